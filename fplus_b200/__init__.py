@@ -1,0 +1,293 @@
+"""fplus_b200 -- the FPLUS C interface on B200, for Python callers (ctypes over libfplus.so).
+
+``libfplus.so`` (built by ``__graft_entry__.build()`` / ``make -C fplus_b200/csrc``) serves the unchanged fplus.h
+interface (analyze / factor / solve) with every numeric step on the GPU.  This module binds it for the tests and the
+benchmark: ``analyze`` -> :class:`Symbolic`, ``Symbolic.factor`` -> :class:`Numeric`, ``Numeric.solve``.  Errors raise
+:class:`FplusError` with the library's code and message.  There is no fallback: a missing library or a failing CUDA call
+raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfplus.so")
+
+FPLUS_OK, FPLUS_ERR_NOMEM, FPLUS_ERR_SINGULAR, FPLUS_ERR_BADARG, FPLUS_ERR_GPU, FPLUS_ERR_INTERNAL = 0, -1, -2, -3, -4, -5
+FPLUS_PIVOT_FULL, FPLUS_PIVOT_PARTIAL, FPLUS_PIVOT_ROOK = 0, 1, 2
+FPLUS_PIVOT_REL_DEFAULT = 1.4901161193847656e-08
+
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class Options(ctypes.Structure):
+    """fplus_options (include/fplus.h), field for field."""
+    _fields_ = [("pin_dense", ctypes.c_int), ("tau_density", ctypes.c_double), ("tau_min_nnz", ctypes.c_int64),
+                ("postorder", ctypes.c_int), ("equilibrate", ctypes.c_int), ("ruiz_max_iter", ctypes.c_int),
+                ("ruiz_tol", ctypes.c_double), ("pivot_rel", ctypes.c_double), ("pivot_strategy", ctypes.c_int),
+                ("drop_tol", ctypes.c_double), ("relax_rows", ctypes.c_int64), ("panel", ctypes.c_int64),
+                ("use_gpu", ctypes.c_int), ("gpu_min_flops", ctypes.c_double), ("verbose", ctypes.c_int)]
+
+
+class Factors(ctypes.Structure):
+    """fplus_factors (include/fplus.h)."""
+    _fields_ = [("n", ctypes.c_int64), ("is_complex", ctypes.c_int), ("csc", ctypes.c_int),
+                ("Lp", _i64p), ("Li", _i64p), ("Lx", ctypes.c_void_p), ("Up", _i64p), ("Ui", _i64p), ("Ux", ctypes.c_void_p),
+                ("p", _i64p), ("q", _i64p), ("nsupernodes", ctypes.c_int64), ("n_pivots_replaced", ctypes.c_int64)]
+
+
+class Info(ctypes.Structure):
+    """fplus_b200_info (include/fplus_b200.h)."""
+    _fields_ = [("n", ctypes.c_int64), ("nfronts", ctypes.c_int64), ("f_dense", ctypes.c_int64), ("attempts", ctypes.c_int),
+                ("ruiz_iters", ctypes.c_int), ("nnz_L", ctypes.c_int64), ("nnz_U", ctypes.c_int64),
+                ("front_flops", ctypes.c_double), ("ms_equil", ctypes.c_double), ("ms_fronts", ctypes.c_double),
+                ("device_bytes", ctypes.c_int64)]
+
+
+# every entry point of include/fplus.h and include/fplus_b200.h (the tests check that each is exported)
+FPLUS_H_SYMBOLS = [
+    "fplus_factors_free", "fplus_analyze", "fplus_analyze_ord", "fplus_symbolic_free", "fplus_symbolic_n",
+    "fplus_symbolic_nnz", "fplus_symbolic_row_perm", "fplus_symbolic_col_perm", "fplus_symbolic_n_dense_rows",
+    "fplus_symbolic_n_dense_cols", "fplus_coletree_postorder", "fplus_default_options", "fplus_analyze_opts",
+    "fplus_factor", "fplus_solve", "fplus_numeric_factors", "fplus_numeric_p", "fplus_numeric_q", "fplus_numeric_Dr",
+    "fplus_numeric_Dc", "fplus_numeric_free",
+]
+FPLUS_B200_H_SYMBOLS = [
+    "fplus_b200_numeric_info", "fplus_b200_use_stream", "fplus_b200_factor_dev", "fplus_b200_solve_dev",
+    "fplus_b200_interior_order", "fplus_b200_plan_size", "fplus_b200_plan_export",
+]
+
+_lib = None
+
+
+def lib():
+    """The loaded libfplus.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FplusError(FPLUS_ERR_INTERNAL, f"{LIB_PATH} is missing: build it with __graft_entry__.build()")
+    L = ctypes.CDLL(LIB_PATH)
+    L.fplus_default_options.argtypes = [ctypes.POINTER(Options)]
+    L.fplus_analyze_opts.argtypes = [ctypes.c_int64, _i64p, _i64p, ctypes.POINTER(Options), ctypes.POINTER(ctypes.c_void_p),
+                                     ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_analyze.argtypes = [ctypes.c_int64, _i64p, _i64p, ctypes.c_int, ctypes.c_double, ctypes.c_int64, ctypes.c_char_p,
+                                ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_analyze_ord.argtypes = [ctypes.c_int64, _i64p, _i64p, ctypes.c_int, ctypes.c_double, ctypes.c_int64,
+                                    ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_symbolic_free.argtypes = [ctypes.c_void_p]
+    for f in ("fplus_symbolic_n", "fplus_symbolic_nnz", "fplus_symbolic_n_dense_rows", "fplus_symbolic_n_dense_cols"):
+        getattr(L, f).argtypes = [ctypes.c_void_p]
+        getattr(L, f).restype = ctypes.c_int64
+    for f in ("fplus_symbolic_row_perm", "fplus_symbolic_col_perm"):
+        getattr(L, f).argtypes = [ctypes.c_void_p]
+        getattr(L, f).restype = _i64p
+    L.fplus_coletree_postorder.argtypes = [ctypes.c_int64, ctypes.c_int64, _i64p, _i64p, _i64p]
+    L.fplus_factor.argtypes = [ctypes.c_void_p, _i64p, _i64p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Options),
+                               ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_b200_factor_dev.argtypes = L.fplus_factor.argtypes
+    L.fplus_solve.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_char_p,
+                              ctypes.c_size_t]
+    L.fplus_b200_solve_dev.argtypes = L.fplus_solve.argtypes
+    L.fplus_numeric_factors.argtypes = [ctypes.c_void_p]
+    L.fplus_numeric_factors.restype = ctypes.POINTER(Factors)
+    for f in ("fplus_numeric_p", "fplus_numeric_q"):
+        getattr(L, f).argtypes = [ctypes.c_void_p]
+        getattr(L, f).restype = _i64p
+    for f in ("fplus_numeric_Dr", "fplus_numeric_Dc"):
+        getattr(L, f).argtypes = [ctypes.c_void_p]
+        getattr(L, f).restype = _dp
+    L.fplus_numeric_free.argtypes = [ctypes.c_void_p]
+    L.fplus_b200_numeric_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(Info)]
+    L.fplus_b200_use_stream.argtypes = [ctypes.c_void_p]
+    L.fplus_b200_interior_order.argtypes = [ctypes.c_int64, _i64p, _i64p, ctypes.c_char_p, ctypes.c_char_p, _i64p]
+    L.fplus_b200_plan_size.argtypes = [ctypes.c_void_p, ctypes.c_int64, _i64p, _i64p, _i64p]
+    L.fplus_b200_plan_export.argtypes = [ctypes.c_void_p, ctypes.c_int64, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p]
+    _lib = L
+    return L
+
+
+class FplusError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"FPLUS error {code}: {msg}")
+        self.code = code
+
+
+def _check(rc, err):
+    if rc != FPLUS_OK:
+        raise FplusError(rc, err.value.decode(errors="replace") if err is not None else "")
+
+
+def _p64(a):
+    return a.ctypes.data_as(_i64p)
+
+
+def default_options(**kw):
+    o = Options()
+    lib().fplus_default_options(ctypes.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def csc_arrays(n, Ap, Ai, Ax=None):
+    Ap = np.ascontiguousarray(Ap, dtype=np.int64)
+    Ai = np.ascontiguousarray(Ai, dtype=np.int64)
+    if Ax is not None:
+        Ax = np.ascontiguousarray(Ax, dtype=np.complex128 if np.iscomplexobj(Ax) else np.float64)
+    return n, Ap, Ai, Ax
+
+
+class Symbolic:
+    """fplus_analyze_opts: the static orders of one pattern (reusable for any values on it)."""
+
+    def __init__(self, n, Ap, Ai, options=None, **kw):
+        n, Ap, Ai, _ = csc_arrays(n, Ap, Ai)
+        self.n, self.Ap, self.Ai = n, Ap, Ai
+        self.options = options if options is not None else default_options(**kw)
+        self._h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        _check(lib().fplus_analyze_opts(n, _p64(Ap), _p64(Ai), ctypes.byref(self.options), ctypes.byref(self._h), err, 512), err)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None and self._h.value:
+            _lib.fplus_symbolic_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    @property
+    def row_perm(self):
+        return np.ctypeslib.as_array(lib().fplus_symbolic_row_perm(self._h), (self.n,)).copy()
+
+    @property
+    def col_perm(self):
+        return np.ctypeslib.as_array(lib().fplus_symbolic_col_perm(self._h), (self.n,)).copy()
+
+    @property
+    def n_dense_rows(self):
+        return int(lib().fplus_symbolic_n_dense_rows(self._h))
+
+    @property
+    def n_dense_cols(self):
+        return int(lib().fplus_symbolic_n_dense_cols(self._h))
+
+    def plan(self, tail=-1):
+        """The multifrontal structure (host only): dict of col_front, parent, col_ptr, cols, nrows, nbord, f_dense."""
+        nf, nct, fd = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().fplus_b200_plan_size(self._h, tail, ctypes.byref(nf), ctypes.byref(nct), ctypes.byref(fd)), None)
+        nf, nct = nf.value, nct.value
+        out = dict(col_front=np.zeros(self.n, np.int64), parent=np.zeros(nf, np.int64), col_ptr=np.zeros(nf + 1, np.int64),
+                   cols=np.zeros(max(nct, 1), np.int64), nrows=np.zeros(nf, np.int64), nbord=np.zeros(nf, np.int64))
+        _check(lib().fplus_b200_plan_export(self._h, tail, *(_p64(out[k]) for k in ("col_front", "parent", "col_ptr", "cols",
+                                                                                   "nrows", "nbord"))), None)
+        out["f_dense"] = fd.value
+        return out
+
+    def factor(self, Ax, options=None, device=False):
+        return Numeric(self, Ax, options, device)
+
+
+class Numeric:
+    """fplus_factor: diag(Dr) A[p,:][:,q] diag(Dc) = L U, the factors in device memory."""
+
+    def __init__(self, sym: Symbolic, Ax, options=None, device=False):
+        self.sym = sym
+        self._h = ctypes.c_void_p()
+        opts = options if options is not None else sym.options
+        err = ctypes.create_string_buffer(512)
+        if device:      # a torch CUDA tensor (float64, or complex128 viewed as float64 pairs)
+            self.is_complex = bool(Ax.is_complex())
+            ptr = ctypes.c_void_p(Ax.data_ptr())
+            rc = lib().fplus_b200_factor_dev(sym._h, _p64(sym.Ap), _p64(sym.Ai), ptr, int(self.is_complex), ctypes.byref(opts),
+                                             ctypes.byref(self._h), err, 512)
+        else:
+            Ax = np.ascontiguousarray(Ax)
+            self.is_complex = np.iscomplexobj(Ax)
+            Ax = Ax.astype(np.complex128 if self.is_complex else np.float64, copy=False)
+            rc = lib().fplus_factor(sym._h, _p64(sym.Ap), _p64(sym.Ai), Ax.ctypes.data_as(ctypes.c_void_p), int(self.is_complex),
+                                    ctypes.byref(opts), ctypes.byref(self._h), err, 512)
+        _check(rc, err)
+        self.n = sym.n
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None and self._h.value:
+            _lib.fplus_numeric_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def solve(self, b, trans=0):
+        """x with op(A) x = b (trans 0: A, 1: A^T, 2: A^H); b of shape (n,) or (n, nrhs)."""
+        b = np.asarray(b)
+        dt = np.complex128 if self.is_complex else np.float64
+        one = b.ndim == 1
+        X = np.array(b.reshape(self.n, -1), dtype=dt, order="F", copy=True)
+        err = ctypes.create_string_buffer(512)
+        _check(lib().fplus_solve(self._h, X.ctypes.data_as(ctypes.c_void_p), X.shape[1], self.n, trans, err, 512), err)
+        return X[:, 0] if one else X
+
+    def solve_device(self, B, trans=0):
+        """In place on a torch CUDA tensor holding nrhs right-hand sides column-major (shape (nrhs, n), contiguous)."""
+        err = ctypes.create_string_buffer(512)
+        nrhs = 1 if B.dim() == 1 else B.shape[0]
+        _check(lib().fplus_b200_solve_dev(self._h, ctypes.c_void_p(B.data_ptr()), nrhs, self.n, trans, err, 512), err)
+        return B
+
+    @property
+    def info(self):
+        I = Info()
+        _check(lib().fplus_b200_numeric_info(self._h, ctypes.byref(I)), None)
+        return {k: getattr(I, k) for k, _ in Info._fields_}
+
+    @property
+    def p(self):
+        return np.ctypeslib.as_array(lib().fplus_numeric_p(self._h), (self.n,)).copy()
+
+    @property
+    def q(self):
+        return np.ctypeslib.as_array(lib().fplus_numeric_q(self._h), (self.n,)).copy()
+
+    @property
+    def Dr(self):
+        return np.ctypeslib.as_array(lib().fplus_numeric_Dr(self._h), (self.n,)).copy()
+
+    @property
+    def Dc(self):
+        return np.ctypeslib.as_array(lib().fplus_numeric_Dc(self._h), (self.n,)).copy()
+
+    def factors(self):
+        """(L, U, p_lu) of the scaled, permuted matrix as scipy CSC matrices (L unit lower in pivot order)."""
+        import scipy.sparse as sp
+        fp = lib().fplus_numeric_factors(self._h)
+        if not fp:
+            raise FplusError(FPLUS_ERR_GPU, "fplus_numeric_factors failed")
+        f = fp.contents
+        n = f.n
+        return (_csc(f.Lp, f.Li, f.Lx, n, f.is_complex), _csc(f.Up, f.Ui, f.Ux, n, f.is_complex),
+                np.ctypeslib.as_array(f.p, (n,)).copy())
+
+
+def _csc(Pp, Pi, Px, n, cplx):
+    import scipy.sparse as sp
+    p = np.ctypeslib.as_array(Pp, (n + 1,)).copy()
+    nnz = int(p[-1])
+    i = np.ctypeslib.as_array(Pi, (max(nnz, 1),))[:nnz].copy()
+    x = np.ctypeslib.as_array(ctypes.cast(Px, _dp), (max(nnz, 1) * (2 if cplx else 1),))[: nnz * (2 if cplx else 1)].copy()
+    if cplx:
+        x = x.view(np.complex128)
+    return sp.csc_matrix((x, i, p), shape=(n, n))
+
+
+def analyze(n, Ap, Ai, options=None, **kw) -> Symbolic:
+    return Symbolic(n, Ap, Ai, options, **kw)
+
+
+def interior_order(n, Ap, Ai, trow=None, tcol=None):
+    n, Ap, Ai, _ = csc_arrays(n, Ap, Ai)
+    perm = np.zeros(n, np.int64)
+    tr = None if trow is None else np.ascontiguousarray(trow, dtype=np.uint8).ctypes.data_as(ctypes.c_char_p)
+    tc = None if tcol is None else np.ascontiguousarray(tcol, dtype=np.uint8).ctypes.data_as(ctypes.c_char_p)
+    _check(lib().fplus_b200_interior_order(n, _p64(Ap), _p64(Ai), tr, tc, _p64(perm)), None)
+    return perm

@@ -1,0 +1,396 @@
+// api.cpp -- the fplus.h entry points of the numeric phase (FPLUS src/numeric.c, src/pipeline.c:84-127) and the
+// fplus_b200.h additions.  The numeric work runs on the GPU (numeric.cu); this file validates, composes the orders and
+// scalings (FPLUS src/numeric.c:71-77), moves data, and materializes host copies of the factors on request.
+#include "internal.hpp"
+#include "numeric.hpp"
+#include "fplus_b200.h"
+#include <algorithm>
+#include <cstring>
+#include <new>
+
+using namespace fpl;
+
+static thread_local cudaStream_t tl_stream = nullptr;
+
+extern "C" void fplus_b200_use_stream(void *stream) { tl_stream = (cudaStream_t)stream; }
+
+struct fplus_numeric {
+    int64_t n = 0;
+    int is_complex = 0;
+    std::shared_ptr<FrontPlan> plan;
+    std::shared_ptr<DevPlan> dplan;
+    std::unique_ptr<DevNum> dev;
+    std::vector<int64_t> p, q, p_lu;
+    std::vector<double> Dr, Dc, Drp, Dcp;
+    fplus_b200_info info{};
+    mutable std::mutex mu;               // solves and the lazy host factors share the device buffers
+    mutable bool have_host = false;
+    mutable fplus_factors f{};
+};
+
+#define CKH(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { errf(err, errlen, "CUDA: %s", cudaGetErrorString(e_)); return FPLUS_ERR_GPU; } } while (0)
+
+// the plan for the symbolic object's current dense-chain hint, and its device copy (built on first use)
+static int get_plan(const fplus_symbolic *sym, int64_t tail, std::shared_ptr<FrontPlan> *plan, std::shared_ptr<DevPlan> *dplan,
+                    char *err, size_t errlen)
+{
+    std::lock_guard<std::mutex> lk(sym->mu);
+    int dev = 0;
+    CKH(cudaGetDevice(&dev));
+    if (tail < sym->tail_hint || sym->tail_hint < 0) { if (tail >= 0) sym->tail_hint = tail; }
+    const int64_t want = sym->tail_hint;
+    if (!sym->plan || sym->plan->f_dense != (want >= 0 && want < sym->n - sym->n_tau_cols ? want : sym->n - sym->n_tau_cols)) {
+        auto P = std::make_shared<FrontPlan>();
+        fplus_symbolic_view v{sym->n, sym->n_tau_rows, sym->n_tau_cols, sym->Bp.data(), sym->Bi.data()};
+        if (build_plan(v, want, 64, 256, *P)) { errf(err, errlen, "out of memory (symbolic structure)"); return FPLUS_ERR_NOMEM; }
+        sym->plan = P;
+        sym->dplan.reset();
+    }
+    if (!sym->dplan || sym->dplan->device != dev) {
+        auto D = std::make_shared<DevPlan>();
+        int rc = dev_upload_plan(sym, *sym->plan, *D, err, errlen);
+        if (rc) return rc;
+        sym->dplan = D;
+    }
+    *plan = sym->plan;
+    *dplan = sym->dplan;
+    return FPLUS_OK;
+}
+
+static int factor_common(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax, int ax_on_device,
+                         int is_complex, const fplus_options *opt, fplus_numeric **out, char *err, size_t errlen)
+{
+    if (!out) { errf(err, errlen, "num is NULL"); return FPLUS_ERR_BADARG; }
+    *out = nullptr;
+    if (!sym) { errf(err, errlen, "sym is NULL"); return FPLUS_ERR_BADARG; }
+    fplus_options d;
+    if (!opt) { fplus_default_options(&d); opt = &d; }
+    // options (FPLUS src/numeric.c:51-57)
+    if (opt->pivot_strategy != FPLUS_PIVOT_PARTIAL && opt->pivot_strategy != FPLUS_PIVOT_ROOK && opt->pivot_strategy != FPLUS_PIVOT_FULL) {
+        errf(err, errlen, "pivot_strategy must be FPLUS_PIVOT_PARTIAL, _ROOK or _FULL (got %d)", opt->pivot_strategy);
+        return FPLUS_ERR_BADARG;
+    }
+    if (!(opt->drop_tol >= 0.0)) { errf(err, errlen, "drop_tol must be >= 0 (got %g)", opt->drop_tol); return FPLUS_ERR_BADARG; }
+    if (opt->pivot_strategy != FPLUS_PIVOT_PARTIAL || opt->drop_tol != 0.0) {
+        errf(err, errlen, "this build factors with partial pivoting and drop_tol 0 only (rook / full pivoting and incomplete LU "
+                          "are not built)");
+        return FPLUS_ERR_BADARG;
+    }
+    if (!(opt->pivot_rel >= 0.0)) { errf(err, errlen, "pivot_rel must be >= 0"); return FPLUS_ERR_BADARG; }
+    const int64_t n = sym->n;
+    // the analysed pattern (FPLUS src/pipeline.c:91-99, 118-123)
+    if (!Ap || (n > 0 && !Ai && Ap[n] > 0)) { errf(err, errlen, "NULL index array"); return FPLUS_ERR_BADARG; }
+    if (Ap[n] != sym->nnz) {
+        errf(err, errlen, "the matrix has %ld nonzeros, the symbolic analysis %ld", (long)Ap[n], (long)sym->nnz);
+        return FPLUS_ERR_BADARG;
+    }
+    int rc = check_compressed(n, Ap, Ai, 1, err, errlen);
+    if (rc) return rc;
+    {
+        // the pattern must be the analysed one: compare with the permuted pattern through the gather map
+        const int64_t *Bp = sym->Bp.data(), *Bsrc = sym->Bsrc.data();
+        const int64_t *cp = sym->col_perm.data();
+        for (int64_t jj = 0; jj < n; jj++) {
+            const int64_t c = cp[jj];
+            if (Ap[c + 1] - Ap[c] != Bp[jj + 1] - Bp[jj] ) { errf(err, errlen, "the pattern differs from the analysed one (column %ld)", (long)c); return FPLUS_ERR_BADARG; }
+        }
+        for (int64_t q = 0; q < sym->nnz; q++) {
+            if (Ai[Bsrc[q]] != sym->row_perm[sym->Bi[q]]) { errf(err, errlen, "the pattern differs from the analysed one (entry %ld)", (long)Bsrc[q]); return FPLUS_ERR_BADARG; }
+        }
+    }
+    if (!ax_on_device) { rc = check_finite(Ap[n], Ax, is_complex, err, errlen); if (rc) return rc; }
+    fplus_numeric *num = new (std::nothrow) fplus_numeric;
+    if (!num) { errf(err, errlen, "out of memory"); return FPLUS_ERR_NOMEM; }
+    std::unique_ptr<fplus_numeric> guard(num);
+    try {
+        num->n = n; num->is_complex = is_complex ? 1 : 0;
+        num->dev.reset(new DevNum);
+        DevNum &N = *num->dev;
+        rc = dev_num_init(N, n, sym->nnz, num->is_complex, err, errlen);
+        if (rc) return rc;
+        if (tl_stream) { cudaStreamDestroy(N.stream); N.stream = tl_stream; N.stream_owned = false; }
+        const size_t bytes = (size_t)sym->nnz * (size_t)N.vs;
+        if (bytes) CKH(cudaMemcpyAsync(N.Ax, Ax, bytes, ax_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, N.stream));
+        std::shared_ptr<FrontPlan> P;
+        std::shared_ptr<DevPlan> D;
+        rc = get_plan(sym, -1, &P, &D, err, errlen);
+        if (rc) return rc;
+        if (ax_on_device) { rc = dev_check_finite(N, err, errlen); if (rc) return rc; }
+        CKH(cudaEventRecord(N.ev0, N.stream));
+        rc = dev_equilibrate(*D, N, opt->equilibrate, opt->ruiz_max_iter, opt->ruiz_tol, err, errlen);
+        if (rc) return rc;
+        CKH(cudaEventRecord(N.ev1, N.stream));
+        CKH(cudaEventSynchronize(N.ev1));
+        float ms = 0;
+        CKH(cudaEventElapsedTime(&ms, N.ev0, N.ev1));
+        num->info.ms_equil = ms;
+        int attempts = 0;
+        for (;;) {
+            attempts++;
+            int64_t border = -1;
+            CKH(cudaEventRecord(N.ev0, N.stream));
+            rc = dev_factor_fronts(*P, *D, N, opt->pivot_rel, &border, err, errlen);
+            if (rc) return rc;
+            CKH(cudaEventRecord(N.ev1, N.stream));
+            CKH(cudaEventSynchronize(N.ev1));
+            CKH(cudaEventElapsedTime(&ms, N.ev0, N.ev1));
+            num->info.ms_fronts = ms;
+            if (border < 0) break;
+            if (attempts >= 3) { errf(err, errlen, "dense-row pivot reported again after the restart (front %ld)", (long)border); return FPLUS_ERR_INTERNAL; }
+            // a dense row was chosen as pivot in front `border`: the dense chain starts at that front
+            rc = get_plan(sym, P->fronts[border].f, &P, &D, err, errlen);
+            if (rc) return rc;
+        }
+        num->plan = P;
+        num->dplan = D;
+        // compose the orders and scalings (FPLUS src/numeric.c:71-77)
+        num->p_lu.resize((size_t)n); num->Drp.resize((size_t)n); num->Dcp.resize((size_t)n);
+        if (n > 0) {
+            CKH(cudaMemcpyAsync(num->p_lu.data(), N.p_lu, (size_t)n * 8, cudaMemcpyDeviceToHost, N.stream));
+            CKH(cudaMemcpyAsync(num->Drp.data(), N.Drp, (size_t)n * 8, cudaMemcpyDeviceToHost, N.stream));
+            CKH(cudaMemcpyAsync(num->Dcp.data(), N.Dcp, (size_t)n * 8, cudaMemcpyDeviceToHost, N.stream));
+            CKH(cudaStreamSynchronize(N.stream));
+        }
+        num->p.resize((size_t)n); num->q.resize((size_t)n); num->Dr.resize((size_t)n); num->Dc.resize((size_t)n);
+        const int64_t *rp = sym->row_perm.data(), *cp = sym->col_perm.data();
+        for (int64_t k = 0; k < n; k++) {
+            num->p[k] = rp[num->p_lu[k]];
+            num->q[k] = cp[k];
+            num->Dr[rp[k]] = num->Drp[k];
+            num->Dc[cp[k]] = num->Dcp[k];
+        }
+        fplus_b200_info &I = num->info;
+        I.n = n; I.nfronts = (int64_t)P->fronts.size(); I.f_dense = P->f_dense; I.attempts = attempts;
+        I.ruiz_iters = N.ruiz_iters;
+        int64_t nl = 0, nu = 0;
+        for (auto &F : P->fronts) {
+            for (int64_t i = 0; i < F.npiv && i < F.nrows; i++) { nl += F.nrows - i; nu += F.ncols - i; }
+        }
+        I.nnz_L = nl; I.nnz_U = nu;
+        I.front_flops = 2.0 * P->flops_real * (is_complex ? 4.0 : 1.0);
+        I.device_bytes = (int64_t)(N.cap_L + N.cap_U + N.cap_cb + N.cap_work + 2 * bytes);
+    } catch (const std::bad_alloc &) {
+        errf(err, errlen, "out of memory");
+        return FPLUS_ERR_NOMEM;
+    }
+    *out = guard.release();
+    return FPLUS_OK;
+}
+
+extern "C" int fplus_factor(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex,
+                            const fplus_options *opt, fplus_numeric **num, char *err, size_t errlen)
+{
+    return factor_common(sym, Ap, Ai, Ax, 0, is_complex, opt, num, err, errlen);
+}
+
+extern "C" int fplus_b200_factor_dev(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax_dev,
+                                     int is_complex, const fplus_options *opt, fplus_numeric **num, char *err, size_t errlen)
+{
+    return factor_common(sym, Ap, Ai, Ax_dev, 1, is_complex, opt, num, err, errlen);
+}
+
+#define SOLVE_GROUP 32
+
+static int solve_common(const fplus_numeric *num, void *b, int64_t nrhs, int64_t ldb, int trans, int on_device, char *err,
+                        size_t errlen)
+{
+    if (!num) { errf(err, errlen, "fplus_solve: num is NULL"); return FPLUS_ERR_BADARG; }
+    const int64_t n = num->n;
+    if (trans < 0 || trans > 2 || nrhs < 0 || ldb < n) { errf(err, errlen, "fplus_solve: bad trans, nrhs or ldb"); return FPLUS_ERR_BADARG; }
+    if (nrhs == 0 || n == 0) return FPLUS_OK;
+    if (!b) { errf(err, errlen, "fplus_solve: b is NULL"); return FPLUS_ERR_BADARG; }
+    std::lock_guard<std::mutex> lk(num->mu);
+    DevNum &N = *num->dev;
+    CKH(cudaSetDevice(N.device));
+    cudaStream_t saved = N.stream;
+    if (tl_stream) N.stream = tl_stream;
+    const size_t vs = (size_t)N.vs;
+    const int64_t g = nrhs < SOLVE_GROUP ? nrhs : SOLVE_GROUP;
+    int rc = FPLUS_OK;
+    if ((rc = dev_ensure_x(N, (size_t)n * (size_t)g * vs, err, errlen))) { N.stream = saved; return rc; }
+    dev_clear_status(N, err, errlen);
+    for (int64_t r0 = 0; r0 < nrhs && rc == FPLUS_OK; r0 += g) {
+        const int64_t m = nrhs - r0 < g ? nrhs - r0 : g;
+        char *bb = (char *)b + (size_t)r0 * (size_t)ldb * vs;
+        cudaError_t e = cudaMemcpy2DAsync(N.xbuf, (size_t)n * vs, bb, (size_t)ldb * vs, (size_t)n * vs, (size_t)m,
+                                          on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, N.stream);
+        if (e != cudaSuccess) { errf(err, errlen, "CUDA: %s", cudaGetErrorString(e)); rc = FPLUS_ERR_GPU; break; }
+        rc = dev_solve(*num->plan, *num->dplan, N, N.xbuf, m, trans, err, errlen);
+        if (rc) break;
+        e = cudaMemcpy2DAsync(bb, (size_t)ldb * vs, N.xbuf, (size_t)n * vs, (size_t)n * vs, (size_t)m,
+                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, N.stream);
+        if (e != cudaSuccess) { errf(err, errlen, "CUDA: %s", cudaGetErrorString(e)); rc = FPLUS_ERR_GPU; break; }
+    }
+    if (rc == FPLUS_OK) {
+        int code = 0; int64_t idx = 0;
+        rc = dev_status(N, &code, &idx, err, errlen);
+        if (rc == FPLUS_OK && code != 0) { errf(err, errlen, "fplus_solve: zero or missing diagonal in U"); rc = FPLUS_ERR_SINGULAR; }
+    }
+    N.stream = saved;
+    return rc;
+}
+
+extern "C" int fplus_solve(const fplus_numeric *num, void *b, int64_t nrhs, int64_t ldb, int trans, char *err, size_t errlen)
+{
+    return solve_common(num, b, nrhs, ldb, trans, 0, err, errlen);
+}
+
+extern "C" int fplus_b200_solve_dev(const fplus_numeric *num, void *b_dev, int64_t nrhs, int64_t ldb, int trans, char *err,
+                                    size_t errlen)
+{
+    return solve_common(num, b_dev, nrhs, ldb, trans, 1, err, errlen);
+}
+
+extern "C" void fplus_factors_free(fplus_factors *f)
+{
+    if (!f) return;
+    free(f->Lp); free(f->Li); free(f->Lx); free(f->Up); free(f->Ui); free(f->Ux); free(f->p); free(f->q);
+    f->Lp = f->Li = f->Up = f->Ui = f->p = f->q = nullptr; f->Lx = f->Ux = nullptr;
+}
+
+extern "C" void fplus_numeric_free(fplus_numeric *num)
+{
+    if (!num) return;
+    fplus_factors_free(&num->f);
+    delete num;
+}
+
+// Host copies of L and U (FPLUS src/factor_sn.c:741-808 layout): L in pivot order with the unit diagonal first and the
+// rows below ascending, U with rows ascending (the diagonal last); the front structure's explicit zeros included.
+static int materialize(const fplus_numeric *num)
+{
+    const FrontPlan &P = *num->plan;
+    DevNum &N = *num->dev;
+    const int64_t n = num->n;
+    const size_t vs = (size_t)N.vs;
+    std::vector<char> La((size_t)P.L_size * vs), Ua((size_t)P.U_size * vs);
+    std::vector<int64_t> rowid((size_t)P.rows_total);
+    if (cudaSetDevice(N.device) != cudaSuccess) return FPLUS_ERR_GPU;
+    if (P.L_size && cudaMemcpy(La.data(), N.Larena, La.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return FPLUS_ERR_GPU;
+    if (P.U_size && cudaMemcpy(Ua.data(), N.Uarena, Ua.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return FPLUS_ERR_GPU;
+    if (P.rows_total && cudaMemcpy(rowid.data(), N.rowid, rowid.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess) return FPLUS_ERR_GPU;
+    std::vector<int64_t> pinv((size_t)(n > 0 ? n : 1));
+    for (int64_t k = 0; k < n; k++) pinv[num->p_lu[k]] = k;
+    fplus_factors &f = num->f;
+    std::memset(&f, 0, sizeof(f));
+    f.n = n; f.is_complex = num->is_complex; f.csc = 1; f.nsupernodes = (int64_t)P.fronts.size();
+    // L
+    int64_t nl = 0;
+    for (auto &F : P.fronts) for (int64_t i = 0; i < F.npiv && i < F.nrows; i++) nl += F.nrows - i;
+    f.Lp = (int64_t *)malloc((size_t)(n + 1) * 8);
+    f.Li = (int64_t *)malloc((size_t)(nl > 0 ? nl : 1) * 8);
+    f.Lx = malloc((size_t)(nl > 0 ? nl : 1) * vs);
+    f.p = (int64_t *)malloc((size_t)(n > 0 ? n : 1) * 8);
+    f.q = (int64_t *)malloc((size_t)(n > 0 ? n : 1) * 8);
+    if (!f.Lp || !f.Li || !f.Lx || !f.p || !f.q) { fplus_factors_free(&f); return FPLUS_ERR_NOMEM; }
+    std::vector<std::pair<int64_t, int64_t>> ord;
+    int64_t o = 0;
+    const double one[2] = {1.0, 0.0};
+    for (auto &F : P.fronts) {
+        for (int64_t i = 0; i < F.npiv && i < F.nrows; i++) {
+            const int64_t k = F.f + i;
+            f.Lp[k] = o;
+            f.Li[o] = k;
+            std::memcpy((char *)f.Lx + (size_t)o * vs, one, vs);
+            o++;
+            ord.clear();
+            for (int64_t r = i + 1; r < F.nrows; r++) ord.emplace_back(pinv[rowid[F.row_off + r]], r);
+            std::sort(ord.begin(), ord.end());
+            for (auto &t : ord) {
+                f.Li[o] = t.first;
+                std::memcpy((char *)f.Lx + (size_t)o * vs, La.data() + (size_t)(F.L_off + t.second + i * F.nrows) * vs, vs);
+                o++;
+            }
+        }
+    }
+    f.Lp[n] = o;
+    // U: per column, the rows of the fronts that hold it, ascending
+    std::vector<int64_t> cnt((size_t)n + 1, 0);
+    for (auto &F : P.fronts)
+        for (int64_t i = 0; i < F.npiv && i < F.nrows; i++)
+            for (int64_t t = i; t < F.ncols; t++) cnt[P.cols[F.col_off + t] + 1]++;
+    for (int64_t j = 0; j < n; j++) cnt[j + 1] += cnt[j];
+    const int64_t nu = cnt[n];
+    f.Up = (int64_t *)malloc((size_t)(n + 1) * 8);
+    f.Ui = (int64_t *)malloc((size_t)(nu > 0 ? nu : 1) * 8);
+    f.Ux = malloc((size_t)(nu > 0 ? nu : 1) * vs);
+    if (!f.Up || !f.Ui || !f.Ux) { fplus_factors_free(&f); return FPLUS_ERR_NOMEM; }
+    std::memcpy(f.Up, cnt.data(), (size_t)(n + 1) * 8);
+    std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+    for (auto &F : P.fronts)      // fronts in increasing pivot order: each column fills in ascending row order
+        for (int64_t i = 0; i < F.npiv && i < F.nrows; i++) {
+            const int64_t k = F.f + i;
+            for (int64_t t = i; t < F.ncols; t++) {
+                const int64_t c = P.cols[F.col_off + t];
+                const int64_t w = fill[c]++;
+                f.Ui[w] = k;
+                const char *src = t < F.npiv ? La.data() + (size_t)(F.L_off + i + t * F.nrows) * vs
+                                             : Ua.data() + (size_t)(F.U_off + i + (t - F.npiv) * F.npiv) * vs;
+                std::memcpy((char *)f.Ux + (size_t)w * vs, src, vs);
+            }
+        }
+    for (int64_t k = 0; k < n; k++) { f.p[k] = num->p_lu[k]; f.q[k] = k; }
+    return FPLUS_OK;
+}
+
+extern "C" const fplus_factors *fplus_numeric_factors(const fplus_numeric *num)
+{
+    std::lock_guard<std::mutex> lk(num->mu);
+    if (!num->have_host) {
+        if (materialize(num) != FPLUS_OK) return nullptr;
+        num->have_host = true;
+    }
+    return &num->f;
+}
+
+extern "C" const int64_t *fplus_numeric_p(const fplus_numeric *num) { return num->p.data(); }
+extern "C" const int64_t *fplus_numeric_q(const fplus_numeric *num) { return num->q.data(); }
+extern "C" const double *fplus_numeric_Dr(const fplus_numeric *num) { return num->Dr.data(); }
+extern "C" const double *fplus_numeric_Dc(const fplus_numeric *num) { return num->Dc.data(); }
+
+extern "C" int fplus_b200_numeric_info(const fplus_numeric *num, fplus_b200_info *info)
+{
+    if (!num || !info) return FPLUS_ERR_BADARG;
+    *info = num->info;
+    return FPLUS_OK;
+}
+
+// ---- host-only views of the multifrontal structure (tests)
+static int plan_for(const fplus_symbolic *sym, int64_t tail, FrontPlan &P)
+{
+    fplus_symbolic_view v{sym->n, sym->n_tau_rows, sym->n_tau_cols, sym->Bp.data(), sym->Bi.data()};
+    return build_plan(v, tail, 64, 256, P) ? FPLUS_ERR_NOMEM : FPLUS_OK;
+}
+
+extern "C" int fplus_b200_plan_size(const fplus_symbolic *sym, int64_t tail, int64_t *nfronts, int64_t *ncols_total, int64_t *f_dense)
+{
+    if (!sym) return FPLUS_ERR_BADARG;
+    FrontPlan P;
+    int rc = plan_for(sym, tail, P);
+    if (rc) return rc;
+    if (nfronts) *nfronts = (int64_t)P.fronts.size();
+    if (ncols_total) *ncols_total = (int64_t)P.cols.size();
+    if (f_dense) *f_dense = P.f_dense;
+    return FPLUS_OK;
+}
+
+extern "C" int fplus_b200_plan_export(const fplus_symbolic *sym, int64_t tail, int64_t *col_front, int64_t *parent,
+                                      int64_t *col_ptr, int64_t *cols, int64_t *nrows, int64_t *nbord)
+{
+    if (!sym) return FPLUS_ERR_BADARG;
+    FrontPlan P;
+    int rc = plan_for(sym, tail, P);
+    if (rc) return rc;
+    const int64_t nf = (int64_t)P.fronts.size();
+    if (col_front) std::memcpy(col_front, P.col_front.data(), (size_t)sym->n * 8);
+    for (int64_t s = 0; s < nf; s++) {
+        const Front &F = P.fronts[s];
+        if (parent) parent[s] = F.parent;
+        if (col_ptr) col_ptr[s] = F.col_off;
+        if (nrows) nrows[s] = F.nrows;
+        if (nbord) nbord[s] = F.nbord;
+    }
+    if (col_ptr) col_ptr[nf] = (int64_t)P.cols.size();
+    if (cols) std::memcpy(cols, P.cols.data(), P.cols.size() * 8);
+    return FPLUS_OK;
+}

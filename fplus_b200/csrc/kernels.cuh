@@ -1,0 +1,659 @@
+// kernels.cuh -- the CUDA kernels of the numeric phase (sm_100a): permutation, Ruiz equilibration, the front kernels
+// of the multifrontal LU (assembly, extend-add, panel with partial pivoting, row swaps, unit-lower TRSM, FP64 tensor-core
+// GEMM, copy-out) and the supernodal triangular sweeps.  Included once, by numeric.cu.
+#pragma once
+#include "dev_common.cuh"
+
+namespace fpl {
+
+// =====================================================================================================================
+// permutation and Ruiz equilibration (FPLUS src/pipeline.c:14-82, src/equil.c:60-183, 186-441)
+// =====================================================================================================================
+
+// Bx[p] = Ax[src[p]]: the values of B = A[row_perm,:][:,col_perm] (the pattern and src come from the analysis)
+template <typename T>
+__global__ void k_gather(T *__restrict__ Bx, const T *__restrict__ Ax, const int64_t *__restrict__ src, int64_t nnz)
+{
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nnz; p += (int64_t)gridDim.x * blockDim.x)
+        Bx[p] = Ax[src[p]];
+}
+
+// the largest |d| and the smallest positive |d| over the raw doubles (range guard, FPLUS src/equil.c:197-206)
+__global__ void k_abs_range(const double *__restrict__ d, int64_t m, DevStatus *st)
+{
+    double amax = 0.0, amin = INFINITY;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x) {
+        double a = fabs(d[q]);
+        amax = fmax(amax, a);
+        if (a > 0.0) amin = fmin(amin, a);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+        amin = fmin(amin, __shfl_xor_sync(0xffffffffu, amin, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&st->amax_bits, dbits(amax));
+        atomicMin(&st->amin_bits, dbits(amin));
+    }
+}
+
+// line maxima of max(|re|, |im|) for the wide-range guard (FPLUS src/equil.c:215-227); lmax: 2n zeroed bit patterns
+template <bool CPLX>
+__global__ void k_line_max(const int64_t *__restrict__ Bp, const int64_t *__restrict__ Bi, const double *__restrict__ d,
+                           int64_t n, unsigned long long *lmax)
+{
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
+        for (int64_t p = Bp[j]; p < Bp[j + 1]; p++) {
+            double a = CPLX ? fmax(fabs(d[2 * p]), fabs(d[2 * p + 1])) : fabs(d[p]);
+            atomicMax(&lmax[Bi[p]], dbits(a));
+            atomicMax(&lmax[n + j], dbits(a));
+        }
+}
+
+__global__ void k_min_pos(const unsigned long long *__restrict__ v, int64_t m, DevStatus *st)
+{
+    double amin = INFINITY;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x) {
+        double a = bitsd(v[q]);
+        if (a > 0.0) amin = fmin(amin, a);
+    }
+    for (int o = 16; o > 0; o >>= 1) amin = fmin(amin, __shfl_xor_sync(0xffffffffu, amin, o));
+    if ((threadIdx.x & 31) == 0) atomicMin(&st->amin_bits, dbits(amin));
+}
+
+__global__ void k_scale_raw(double *d, int64_t m, double sc)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x) d[q] *= sc;
+}
+
+// squared modulus exactly as the reference rounds it: re*re + im*im, two products and a sum, no contraction
+__device__ __forceinline__ double sqmod(double a) { return __dmul_rn(a, a); }
+__device__ __forceinline__ double sqmod(cplx a) { return __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y)); }
+
+// row maxima of |b|^2 (order independent: the maximum of non-negative doubles is their integer maximum)
+template <typename T>
+__global__ void k_ruiz_rowmax(const int64_t *__restrict__ Bi, const T *__restrict__ Bx, int64_t nnz,
+                              unsigned long long *__restrict__ rmax, const DevStatus *st)
+{
+    if (st->done || st->code) return;
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nnz; p += (int64_t)gridDim.x * blockDim.x)
+        atomicMax(&rmax[Bi[p]], dbits(sqmod(Bx[p])));
+}
+
+// zero-row check, residual, row scale 1/sqrt(sqrt(max)), Dr *= scale (FPLUS src/equil.c:80-92)
+__global__ void k_ruiz_rowscale(int64_t n, unsigned long long *__restrict__ rmax, double *__restrict__ Dr, DevStatus *st)
+{
+    if (st->done || st->code) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double m = bitsd(rmax[i]);
+        if (m == 0.0) {           // the smallest zero row wins (the reference reports the first)
+            atomicCAS(&((DevStatus *)st)->code, 0, ST_ZERO_ROW);
+            continue;
+        }
+        double v = 0.5 * fabs(log(m));
+        atomicMax(&st->res_bits, dbits(v));
+        double dr = 1.0 / sqrt(sqrt(m));
+        Dr[i] = __dmul_rn(Dr[i], dr);
+        rmax[i] = dbits(dr);
+    }
+}
+
+// zero-row index: the smallest (second pass so the index is deterministic)
+__global__ void k_first_zero(int64_t n, const unsigned long long *__restrict__ v, DevStatus *st, int code)
+{
+    if (st->code != code) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (bitsd(v[i]) == 0.0) atomicMin((unsigned long long *)&st->idx, (unsigned long long)i);
+}
+
+// per column (a warp each): scale by the row scales, then the column maximum of |b|^2 (FPLUS src/equil.c:93-147)
+template <typename T>
+__global__ void k_ruiz_colpass(const int64_t *__restrict__ Bp, const int64_t *__restrict__ Bi, T *__restrict__ Bx,
+                               int64_t n, const unsigned long long *__restrict__ rscale, unsigned long long *__restrict__ cmax,
+                               const DevStatus *st)
+{
+    if (st->done || st->code) return;
+    const int lane = threadIdx.x & 31;
+    for (int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; j < n; j += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        double cm = 0.0;
+        for (int64_t p = Bp[j] + lane; p < Bp[j + 1]; p += 32) {
+            T v = scal(Bx[p], bitsd(rscale[Bi[p]]));
+            Bx[p] = v;
+            cm = fmax(cm, sqmod(v));
+        }
+        for (int o = 16; o > 0; o >>= 1) cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+        if (lane == 0) cmax[j] = dbits(cm);
+    }
+}
+
+// the zero-column check, residual, column scale, Dc *= scale (FPLUS src/equil.c:148-155)
+__global__ void k_ruiz_colscale(int64_t n, unsigned long long *__restrict__ cmax, double *__restrict__ Dc, DevStatus *st)
+{
+    if (st->done || st->code) return;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        double m = bitsd(cmax[j]);
+        if (m == 0.0) { atomicCAS(&st->code, 0, ST_ZERO_COL); continue; }
+        double v = 0.5 * fabs(log(m));
+        atomicMax(&st->res_bits, dbits(v));
+        double c = 1.0 / sqrt(sqrt(m));
+        Dc[j] = __dmul_rn(Dc[j], c);
+        cmax[j] = dbits(c);
+    }
+}
+
+template <typename T>
+__global__ void k_ruiz_colapply(const int64_t *__restrict__ Bp, T *__restrict__ Bx, int64_t n,
+                                const unsigned long long *__restrict__ cscale, const DevStatus *st)
+{
+    if (st->done || st->code) return;
+    const int lane = threadIdx.x & 31;
+    for (int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; j < n; j += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const double c = bitsd(cscale[j]);
+        for (int64_t p = Bp[j] + lane; p < Bp[j + 1]; p += 32) Bx[p] = scal(Bx[p], c);
+    }
+}
+
+// end of an iteration: count it, stop when the residual is below tol (FPLUS src/equil.c:405-411)
+__global__ void k_ruiz_check(DevStatus *st, double tol)
+{
+    if (st->done || st->code) return;
+    st->iters++;
+    if (bitsd(st->res_bits) < tol) st->done = 1;
+    st->res_bits = 0ull;
+}
+
+__global__ void k_fold(double *Dr, double *Dc, int64_t n, double h)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        Dr[i] *= h; Dc[i] *= h;
+    }
+}
+
+// the largest modulus of each column of the scaled B (the singular-pivot threshold, FPLUS src/factor_sn_panel.inc:50)
+template <typename T>
+__global__ void k_colmax(const int64_t *__restrict__ Bp, const T *__restrict__ Bx, int64_t n, double *__restrict__ cm)
+{
+    const int lane = threadIdx.x & 31;
+    for (int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; j < n; j += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        double m = 0.0;
+        for (int64_t p = Bp[j] + lane; p < Bp[j + 1]; p += 32) m = fmax(m, vabs(Bx[p]));
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0) cm[j] = m;
+    }
+}
+
+// =====================================================================================================================
+// fronts
+// =====================================================================================================================
+
+// original entries into the front's working block; static row ids
+template <typename T>
+__global__ void k_assemble(T *__restrict__ W, const T *__restrict__ Bx, const int64_t *__restrict__ src,
+                           const int64_t *__restrict__ dst, int64_t cnt, int64_t *__restrict__ rowid,
+                           const int64_t *__restrict__ rowinit, int64_t nrows, const DevStatus *st)
+{
+    if (st->code) return;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e = tid; e < cnt; e += stride) W[dst[e]] = Bx[src[e]];
+    for (int64_t i = tid; i < nrows; i += stride) if (rowinit[i] >= 0) rowid[i] = rowinit[i];
+}
+
+// W += the child's contribution block (rows: the child's interior CB rows into its slots, its border rows onto the
+// parent's dense rows; columns through relcol); the child's CB row ids fill the slots
+template <typename T>
+__global__ void k_extend_add(T *__restrict__ W, int64_t ldw, const T *__restrict__ cb, int64_t cbr, int64_t cbc,
+                             int64_t nslot, int64_t slot, int64_t tau_base, const int64_t *__restrict__ relcol,
+                             int64_t *__restrict__ rowid_parent, const int64_t *__restrict__ rowid_child_cb,
+                             const DevStatus *st)
+{
+    if (st->code) return;
+    const int64_t total = cbr * cbc;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = e % cbr, c = e / cbr;
+        const int64_t pr = t < nslot ? slot + t : tau_base + (t - nslot);
+        const int64_t pc = relcol[c];
+        T v = cb[t + c * cbr];
+        T *w = W + pr + pc * ldw;
+        *w = add(*w, v);
+        if (c == 0 && t < nslot) rowid_parent[slot + t] = rowid_child_cb[t];
+    }
+    if (cbc == 0)
+        for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nslot; t += (int64_t)gridDim.x * blockDim.x)
+            rowid_parent[slot + t] = rowid_child_cb[t];
+}
+
+// Partial pivoting on columns [k0, k0 + w) of the working block (rows [k0, nrows)), one CTA: per column, the argmax of
+// the moduli (warp shuffles, then across warps; ties to the smaller row of B), the singular test against pivot_rel *
+// max |B(:, j)|, the border test, the row swap inside the panel (and of the row ids), the division by the pivot and the
+// rank-1 update of the panel's remaining columns.  Swaps are recorded in ipiv for the other columns.
+template <typename T>
+__global__ void __launch_bounds__(512) k_panel(T *__restrict__ W, int64_t ld, int64_t nrows, int64_t nri, int k0, int w,
+                                              int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
+                                              int64_t *__restrict__ rowid, int *__restrict__ ipiv, DevStatus *st,
+                                              int64_t front)
+{
+    __shared__ double s_val[32];
+    __shared__ int64_t s_idx[32], s_rid[32];
+    __shared__ int64_t s_piv;
+    __shared__ T s_row[32];
+    __shared__ int s_stop;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    if (tid == 0) s_stop = st->code != 0;
+    __syncthreads();
+    if (s_stop) return;
+    for (int kk = 0; kk < w; kk++) {
+        const int64_t j = k0 + kk;
+        // argmax over rows [j, nrows)
+        double bv = -1.0; int64_t bi = -1, br = INT64_MAX;
+        for (int64_t i = j + tid; i < nrows; i += blockDim.x) {
+            double a = vabs(W[i + j * ld]);
+            int64_t r = rowid[i];
+            if (a > bv || (a == bv && r < br)) { bv = a; bi = i; br = r; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            int64_t oi = __shfl_xor_sync(0xffffffffu, bi, o), orr = __shfl_xor_sync(0xffffffffu, br, o);
+            if (ov > bv || (ov == bv && orr < br)) { bv = ov; bi = oi; br = orr; }
+        }
+        if (lane == 0) { s_val[warp] = bv; s_idx[warp] = bi; s_rid[warp] = br; }
+        __syncthreads();
+        if (tid == 0) {
+            double v = s_val[0]; int64_t ix = s_idx[0], rr = s_rid[0];
+            for (int q = 1; q < nw; q++)
+                if (s_val[q] > v || (s_val[q] == v && s_rid[q] < rr)) { v = s_val[q]; ix = s_idx[q]; rr = s_rid[q]; }
+            const double thr = pivot_rel * colmax[fcol + j];
+            if (ix < 0 || v <= 0.0 || v < thr) { set_status(st, ST_SINGULAR, fcol + j, v > 0 ? v : 0.0, thr); s_stop = 1; }
+            else if (ix >= nri) { set_status(st, ST_BORDER, front, v, thr); s_stop = 1; }
+            s_piv = ix;
+            if (!s_stop) {
+                ipiv[j] = (int)ix;
+                if (ix != j) { int64_t t = rowid[j]; rowid[j] = rowid[ix]; rowid[ix] = t; }
+            }
+        }
+        __syncthreads();
+        if (s_stop) return;
+        const int64_t p = s_piv;
+        // swap rows j and p inside the panel; keep the pivot row's panel entries in shared memory
+        if (tid < w) {
+            const int64_t c = k0 + tid;
+            T a = W[j + c * ld], b = W[p + c * ld];
+            if (p != j) { W[j + c * ld] = b; W[p + c * ld] = a; }
+            s_row[tid] = p != j ? b : a;
+        }
+        __syncthreads();
+        const T piv = s_row[kk];
+        for (int64_t i = j + 1 + tid; i < nrows; i += blockDim.x) {
+            T l = divv(W[i + j * ld], piv);
+            W[i + j * ld] = l;
+            for (int c = kk + 1; c < w; c++) {
+                T *x = W + i + (k0 + c) * ld;
+                *x = sub(*x, mul(l, s_row[c]));
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// apply the recorded swaps ipiv[k0 .. k0 + cnt) in order to the columns [c0, c1)
+template <typename T>
+__global__ void k_laswp(T *__restrict__ W, int64_t ld, const int *__restrict__ ipiv, int k0, int cnt, int64_t c0, int64_t c1,
+                        const DevStatus *st)
+{
+    if (st->code) return;
+    for (int64_t c = c0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < c1; c += (int64_t)gridDim.x * blockDim.x) {
+        T *col = W + c * ld;
+        for (int k = 0; k < cnt; k++) {
+            const int64_t j = k0 + k, p = ipiv[j];
+            if (p != j) { T t = col[j]; col[j] = col[p]; col[p] = t; }
+        }
+    }
+}
+
+// X <- L^-1 X for the unit lower w x w block L = W[k0.., k0..] and X = rows [k0, k0 + w) of columns [c0, c1)
+template <typename T>
+__global__ void __launch_bounds__(128) k_trsm_unit(T *__restrict__ W, int64_t ld, int k0, int w, int64_t c0, int64_t c1,
+                                                   const DevStatus *st)
+{
+    __shared__ T sL[32][33];
+    if (st->code) return;
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+        int r = e % w, c = e / w;
+        sL[r][c] = W[(k0 + r) + (int64_t)(k0 + c) * ld];
+    }
+    __syncthreads();
+    for (int64_t c = c0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < c1; c += (int64_t)gridDim.x * blockDim.x) {
+        T x[32];
+        T *col = W + k0 + c * ld;
+#pragma unroll
+        for (int i = 0; i < 32; i++) if (i < w) x[i] = col[i];
+#pragma unroll
+        for (int i = 0; i < 32; i++) {
+            if (i >= w) break;
+#pragma unroll
+            for (int r = i + 1; r < 32; r++) if (r < w) x[r] = sub(x[r], mul(sL[r][i], x[i]));
+        }
+#pragma unroll
+        for (int i = 0; i < 32; i++) if (i < w) col[i] = x[i];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// C <- C - A B (column-major; M x K times K x N) on the FP64 tensor cores: mma.sync m8n8k4 f64 (DMMA).  64 x 64 block
+// tiles, 16-deep K slices staged in shared memory, 8 warps of 32 x 16.  Complex: four real products per complex one
+// (Cr += Ar Br - Ai Bi, Ci += Ar Bi + Ai Br), the minus folded into a negated copy of Bi.
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
+constexpr int GBM = 64, GBN = 64, GBK = 16, GPAD = 68;
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_gemm_sub(int64_t M, int64_t N, int64_t K, const T *__restrict__ A, int64_t lda,
+                                                 const T *__restrict__ B, int64_t ldb, T *__restrict__ C, int64_t ldc,
+                                                 const DevStatus *st)
+{
+    constexpr bool CP = VT<T>::cplx_;
+    __shared__ double As[CP ? 2 : 1][GBK][GPAD];
+    __shared__ double Bs[CP ? 3 : 1][GBK][GPAD];
+    if (st->code) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 1, wn = warp >> 1;
+    const int64_t m0 = (int64_t)blockIdx.x * GBM, n0 = (int64_t)blockIdx.y * GBN;
+    double acc[CP ? 2 : 1][4][2][2];
+#pragma unroll
+    for (int z = 0; z < (CP ? 2 : 1); z++)
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++) { acc[z][a][b][0] = 0.0; acc[z][a][b][1] = 0.0; }
+    for (int64_t k0 = 0; k0 < K; k0 += GBK) {
+        // stage A (64 x 16) and B (16 x 64)
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int m = tid & 63, k = (tid >> 6) + 4 * i;
+            const int64_t gm = m0 + m, gk = k0 + k;
+            T v = (gm < M && gk < K) ? A[gm + gk * lda] : VT<T>::zero();
+            if constexpr (CP) { As[0][k][m] = v.x; As[1][k][m] = v.y; } else As[0][k][m] = v;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int k = tid & 15, nn = (tid >> 4) + 16 * i;
+            const int64_t gk = k0 + k, gn = n0 + nn;
+            T v = (gk < K && gn < N) ? B[gk + gn * ldb] : VT<T>::zero();
+            if constexpr (CP) { Bs[0][k][nn] = v.x; Bs[1][k][nn] = v.y; Bs[2][k][nn] = -v.y; } else Bs[0][k][nn] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < GBK; ks += 4) {
+            const int kr = ks + (lane & 3);
+            double ar[4], ai[4], br[2], bi[2], bn[2];
+#pragma unroll
+            for (int a = 0; a < 4; a++) {
+                const int m = wm * 32 + a * 8 + (lane >> 2);
+                ar[a] = As[0][kr][m];
+                if constexpr (CP) ai[a] = As[1][kr][m];
+            }
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                const int nn = wn * 16 + b * 8 + (lane >> 2);
+                br[b] = Bs[0][kr][nn];
+                if constexpr (CP) { bi[b] = Bs[1][kr][nn]; bn[b] = Bs[2][kr][nn]; }
+            }
+#pragma unroll
+            for (int a = 0; a < 4; a++)
+#pragma unroll
+                for (int b = 0; b < 2; b++) {
+                    dmma(acc[0][a][b][0], acc[0][a][b][1], ar[a], br[b]);
+                    if constexpr (CP) {
+                        dmma(acc[0][a][b][0], acc[0][a][b][1], ai[a], bn[b]);
+                        dmma(acc[1][a][b][0], acc[1][a][b][1], ar[a], bi[b]);
+                        dmma(acc[1][a][b][0], acc[1][a][b][1], ai[a], br[b]);
+                    }
+                }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 2; b++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int64_t gm = m0 + wm * 32 + a * 8 + (lane >> 2);
+                const int64_t gn = n0 + wn * 16 + b * 8 + 2 * (lane & 3) + h;
+                if (gm < M && gn < N) {
+                    T *c = C + gm + gn * ldc;
+                    if constexpr (CP) { cplx v = *c; v.x -= acc[0][a][b][h]; v.y -= acc[1][a][b][h]; *c = v; }
+                    else *c -= acc[0][a][b][h];
+                }
+            }
+}
+
+// the factors of the front leave the working block: L (nrows x npiv) and U12 (npiv x ncb) into the arena, the CB into
+// the stack, the pivot rows into p_lu
+template <typename T>
+__global__ void k_copyout(const T *__restrict__ W, int64_t nrows, int64_t ncols, int64_t npiv, T *__restrict__ Lo,
+                          T *__restrict__ Uo, T *__restrict__ CBo, const int64_t *__restrict__ rowid, int64_t f,
+                          int64_t *__restrict__ p_lu, const DevStatus *st)
+{
+    if (st->code) return;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t ncb = ncols - npiv, cbr = nrows > npiv ? nrows - npiv : 0;
+    for (int64_t e = tid; e < nrows * npiv; e += stride) Lo[e] = W[e];
+    for (int64_t e = tid; e < npiv * ncb; e += stride) { int64_t i = e % npiv, c = e / npiv; Uo[e] = W[i + (npiv + c) * nrows]; }
+    for (int64_t e = tid; e < cbr * ncb; e += stride) { int64_t i = e % cbr, c = e / cbr; CBo[e] = W[npiv + i + (npiv + c) * nrows]; }
+    for (int64_t i = tid; i < npiv && i < nrows; i += stride) p_lu[f + i] = rowid[i];
+}
+
+// =====================================================================================================================
+// solves (x column-major n x nrhs; row space: rows of B; column / pivot space: columns of B = pivot steps)
+// =====================================================================================================================
+
+// Wr[r] = Drp[r] * b[row_perm[r]] (trans 0), or Wc[k] = Dcp[k] * b[col_perm[k]] (trans 1, 2)
+template <typename T>
+__global__ void k_rhs_in(T *__restrict__ out, const T *__restrict__ b, int64_t ldb, const int64_t *__restrict__ perm,
+                         const double *__restrict__ scale, int64_t n, int64_t nrhs)
+{
+    const int64_t total = n * nrhs;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        int64_t k = e % n, r = e / n;
+        out[e] = scal(b[perm[k] + r * ldb], scale[k]);
+    }
+}
+
+// x[perm[k]] = scale[sidx[k]] * v[k]  (trans 0: perm = col_perm, sidx = identity; trans 1/2: perm = row_perm o p_lu)
+template <typename T>
+__global__ void k_rhs_out(T *__restrict__ x, int64_t ldx, const T *__restrict__ v, const int64_t *__restrict__ perm,
+                          const int64_t *__restrict__ inner, const double *__restrict__ scale, int64_t n, int64_t nrhs)
+{
+    const int64_t total = n * nrhs;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        int64_t k = e % n, r = e / n;
+        int64_t s = inner ? inner[k] : k;
+        x[perm[s] + r * ldx] = scal(v[e], scale[s]);
+    }
+}
+
+// Y[k] = Wr[p_lu[k]]: the forward result in pivot order
+template <typename T>
+__global__ void k_gather_rows(T *__restrict__ Y, const T *__restrict__ Wr, const int64_t *__restrict__ p_lu, int64_t n, int64_t nrhs)
+{
+    const int64_t total = n * nrhs;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        int64_t k = e % n, r = e / n;
+        Y[e] = Wr[p_lu[k] + r * n];
+    }
+}
+
+// forward sweep with L through one front (one CTA), in row space: for each pivot column i, the rows below it lose
+// L[row, i] times the pivot row's value
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwdL(const T *__restrict__ L, int64_t nrows, int64_t npiv,
+                                              const int64_t *__restrict__ rowid, T *__restrict__ Wr, int64_t n, int64_t nrhs)
+{
+    for (int64_t i = 0; i < npiv && i < nrows; i++) {
+        for (int64_t e = threadIdx.x; e < (nrows - i - 1) * nrhs; e += blockDim.x) {
+            const int64_t rr = i + 1 + e % (nrows - i - 1), r = e / (nrows - i - 1);
+            const T xi = Wr[rowid[i] + r * n];
+            if (is_zero(xi)) continue;
+            T *y = Wr + rowid[rr] + r * n;
+            *y = sub(*y, mul(L[rr + i * nrows], xi));
+        }
+        __syncthreads();
+    }
+}
+
+// backward sweep with U, step 1: partial sums of U12 x_cb over column chunks: part[chunk][i + r * npiv]
+template <typename T>
+__global__ void __launch_bounds__(256) k_u12_gemv(const T *__restrict__ U12, int64_t npiv, int64_t ncb,
+                                                  const int64_t *__restrict__ cbcols, const T *__restrict__ X, int64_t n,
+                                                  int64_t nrhs, int64_t chunk, T *__restrict__ part)
+{
+    const int64_t c0 = blockIdx.x * chunk, c1 = c0 + chunk < ncb ? c0 + chunk : ncb;
+    for (int64_t e = threadIdx.x; e < npiv * nrhs; e += blockDim.x) {
+        const int64_t i = e % npiv, r = e / npiv;
+        T s = VT<T>::zero();
+        for (int64_t c = c0; c < c1; c++) s = add(s, mul(U12[i + c * npiv], X[cbcols[c] + r * n]));
+        part[blockIdx.x * npiv * nrhs + e] = s;
+    }
+}
+
+// backward sweep with U, step 2 (one CTA): x = U11^-1 (y - sum of the partial sums)
+template <typename T>
+__global__ void __launch_bounds__(256) k_bwdU(const T *__restrict__ L, int64_t nrows, int64_t npiv, int64_t f,
+                                              const T *__restrict__ part, int64_t nchunk, const T *__restrict__ Y,
+                                              T *__restrict__ X, int64_t n, int64_t nrhs, DevStatus *st)
+{
+    extern __shared__ unsigned char smem_raw[];
+    T *s = reinterpret_cast<T *>(smem_raw);           // npiv * nrhs
+    for (int64_t e = threadIdx.x; e < npiv * nrhs; e += blockDim.x) {
+        const int64_t i = e % npiv, r = e / npiv;
+        T v = Y[f + i + r * n];
+        for (int64_t q = 0; q < nchunk; q++) v = sub(v, part[q * npiv * nrhs + e]);
+        s[e] = v;
+    }
+    __syncthreads();
+    for (int64_t i = npiv - 1; i >= 0; i--) {
+        const T d = L[i + i * nrows];
+        if (is_zero(d)) { if (threadIdx.x == 0) set_status(st, ST_SOLVE_ZERO, f + i, 0, 0); return; }
+        for (int64_t r = threadIdx.x; r < nrhs; r += blockDim.x) s[i + r * npiv] = divv(s[i + r * npiv], d);
+        __syncthreads();
+        for (int64_t e = threadIdx.x; e < i * nrhs; e += blockDim.x) {
+            const int64_t j = e % i, r = e / i;
+            s[j + r * npiv] = sub(s[j + r * npiv], mul(L[j + i * nrows], s[i + r * npiv]));
+        }
+        __syncthreads();
+    }
+    for (int64_t e = threadIdx.x; e < npiv * nrhs; e += blockDim.x) {
+        const int64_t i = e % npiv, r = e / npiv;
+        X[f + i + r * n] = s[e];
+    }
+}
+
+// transposed solves: forward with U^T (U^H when conj) through one front, step 1 (one CTA): z = U11^-T w[f ..]
+template <typename T, bool CJ>
+__global__ void __launch_bounds__(256) k_fwdUt(const T *__restrict__ L, int64_t nrows, int64_t npiv, int64_t f,
+                                               T *__restrict__ Wc, int64_t n, int64_t nrhs, DevStatus *st)
+{
+    for (int64_t i = 0; i < npiv; i++) {
+        T d = L[i + i * nrows];
+        if (CJ) d = conjv(d);
+        if (is_zero(d)) { if (threadIdx.x == 0) set_status(st, ST_SOLVE_ZERO, f + i, 0, 0); return; }
+        for (int64_t r = threadIdx.x; r < nrhs; r += blockDim.x) Wc[f + i + r * n] = divv(Wc[f + i + r * n], d);
+        __syncthreads();
+        for (int64_t e = threadIdx.x; e < (npiv - i - 1) * nrhs; e += blockDim.x) {
+            const int64_t j = i + 1 + e % (npiv - i - 1), r = e / (npiv - i - 1);
+            T u = L[i + j * nrows];
+            if (CJ) u = conjv(u);
+            Wc[f + j + r * n] = sub(Wc[f + j + r * n], mul(u, Wc[f + i + r * n]));
+        }
+        __syncthreads();
+    }
+}
+
+// step 2 (many CTAs, a warp per CB column): w[cbcol[c]] -= U12[:, c]^T z
+template <typename T, bool CJ>
+__global__ void k_ut_scatter(const T *__restrict__ U12, int64_t npiv, int64_t ncb, const int64_t *__restrict__ cbcols,
+                             int64_t f, T *__restrict__ Wc, int64_t n, int64_t nrhs)
+{
+    const int lane = threadIdx.x & 31;
+    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < ncb; c += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        for (int64_t r = 0; r < nrhs; r++) {
+            T s = VT<T>::zero();
+            for (int64_t i = lane; i < npiv; i += 32) {
+                T u = U12[i + c * npiv];
+                if (CJ) u = conjv(u);
+                s = add(s, mul(u, Wc[f + i + r * n]));
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                if constexpr (VT<T>::cplx_) {
+                    cplx t; t.x = __shfl_xor_sync(0xffffffffu, ((cplx &)s).x, o); t.y = __shfl_xor_sync(0xffffffffu, ((cplx &)s).y, o);
+                    s = add(s, *(T *)&t);
+                } else s = add(s, __shfl_xor_sync(0xffffffffu, s, o));
+            }
+            if (lane == 0) { T *w = Wc + cbcols[c] + r * n; *w = sub(*w, s); }
+        }
+    }
+}
+
+// backward with L^T (L^H) through one front (one CTA): V[f + i] = z_i - sum over the rows below of L[row, i] V[row's step]
+template <typename T, bool CJ>
+__global__ void __launch_bounds__(256) k_bwdLt(const T *__restrict__ L, int64_t nrows, int64_t npiv, int64_t f,
+                                               const int64_t *__restrict__ rowid, const int64_t *__restrict__ pinv,
+                                               const T *__restrict__ Z, T *__restrict__ V, int64_t n, int64_t nrhs)
+{
+    extern __shared__ unsigned char smem_raw[];
+    T *s = reinterpret_cast<T *>(smem_raw);           // npiv * nrhs
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    // s = z - L21^T v_cb (a warp per pivot column)
+    for (int64_t e = warp; e < npiv * nrhs; e += nw) {
+        const int64_t i = e % npiv, r = e / npiv;
+        T acc = VT<T>::zero();
+        for (int64_t rr = npiv + lane; rr < nrows; rr += 32) {
+            T l = L[rr + i * nrows];
+            if (CJ) l = conjv(l);
+            acc = add(acc, mul(l, V[pinv[rowid[rr]] + r * n]));
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            if constexpr (VT<T>::cplx_) {
+                cplx t; t.x = __shfl_xor_sync(0xffffffffu, ((cplx &)acc).x, o); t.y = __shfl_xor_sync(0xffffffffu, ((cplx &)acc).y, o);
+                acc = add(acc, *(T *)&t);
+            } else acc = add(acc, __shfl_xor_sync(0xffffffffu, acc, o));
+        }
+        if (lane == 0) s[e] = sub(Z[f + i + r * n], acc);
+    }
+    __syncthreads();
+    for (int64_t i = npiv - 1; i >= 0; i--) {
+        // s[i] final; s[j] -= L[i, j] s[i] for j < i
+        for (int64_t e = threadIdx.x; e < i * nrhs; e += blockDim.x) {
+            const int64_t j = e % i, r = e / i;
+            T l = L[i + j * nrows];
+            if (CJ) l = conjv(l);
+            s[j + r * npiv] = sub(s[j + r * npiv], mul(l, s[i + r * npiv]));
+        }
+        __syncthreads();
+    }
+    for (int64_t e = threadIdx.x; e < npiv * nrhs; e += blockDim.x) {
+        const int64_t i = e % npiv, r = e / npiv;
+        V[f + i + r * n] = s[e];
+    }
+}
+
+// every value finite: the first non-finite double (by index) is reported
+__global__ void k_check_finite(const double *__restrict__ d, int64_t m, DevStatus *st)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x)
+        if (!isfinite(d[q])) {
+            atomicCAS(&st->code, 0, ST_BAD_VALUE);
+            atomicMin((unsigned long long *)&st->idx, (unsigned long long)q);
+        }
+}
+
+__global__ void k_pinv(const int64_t *__restrict__ p_lu, int64_t *__restrict__ pinv, int64_t n)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) pinv[p_lu[k]] = k;
+}
+
+}  // namespace fpl

@@ -1,0 +1,411 @@
+// numeric.cu -- the device side of fplus_factor / fplus_solve: device copies of the multifrontal plan, the numeric
+// state of one factorization, and the launch sequences.
+#include "numeric.hpp"
+#include "kernels.cuh"
+#include <algorithm>
+#include <cstring>
+#include <cmath>
+
+namespace fpl {
+
+#define CK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { errf(err, errlen, "CUDA: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); return FPLUS_ERR_GPU; } } while (0)
+
+static inline int nblk(int64_t work, int per = 256, int cap = 148 * 16)
+{
+    int64_t b = (work + per - 1) / per;
+    if (b < 1) b = 1;
+    if (b > cap) b = cap;
+    return (int)b;
+}
+
+template <typename T> static int upload(const std::vector<T> &h, T **d, char *err, size_t errlen)
+{
+    *d = nullptr;
+    size_t bytes = (h.empty() ? 1 : h.size()) * sizeof(T);
+    CK(cudaMalloc((void **)d, bytes));
+    if (!h.empty()) CK(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return FPLUS_OK;
+}
+
+DevPlan::~DevPlan()
+{
+    for (void *p : {(void *)cols, (void *)relcol, (void *)rowinit, (void *)asm_src, (void *)asm_dst, (void *)Bp, (void *)Bi,
+                    (void *)Bsrc, (void *)row_perm, (void *)col_perm})
+        if (p) cudaFree(p);
+}
+
+int dev_upload_plan(const fplus_symbolic *S, const FrontPlan &P, DevPlan &D, char *err, size_t errlen)
+{
+    CK(cudaGetDevice(&D.device));
+    int rc;
+    if ((rc = upload(P.cols, &D.cols, err, errlen))) return rc;
+    if ((rc = upload(P.relcol, &D.relcol, err, errlen))) return rc;
+    if ((rc = upload(P.rowinit, &D.rowinit, err, errlen))) return rc;
+    if ((rc = upload(P.asm_src, &D.asm_src, err, errlen))) return rc;
+    if ((rc = upload(P.asm_dst, &D.asm_dst, err, errlen))) return rc;
+    if ((rc = upload(S->Bp, &D.Bp, err, errlen))) return rc;
+    if ((rc = upload(S->Bi, &D.Bi, err, errlen))) return rc;
+    if ((rc = upload(S->Bsrc, &D.Bsrc, err, errlen))) return rc;
+    if ((rc = upload(S->row_perm, &D.row_perm, err, errlen))) return rc;
+    if ((rc = upload(S->col_perm, &D.col_perm, err, errlen))) return rc;
+    return FPLUS_OK;
+}
+
+DevNum::~DevNum()
+{
+    if (device >= 0) cudaSetDevice(device);
+    for (void *p : {(void *)Ax, (void *)Bx, (void *)Drp, (void *)Dcp, (void *)colmax, (void *)Larena, (void *)Uarena,
+                    (void *)cbstack, (void *)work, (void *)rowid, (void *)p_lu, (void *)pinv, (void *)ipiv, (void *)st,
+                    (void *)scratch, (void *)rbuf, (void *)sbuf, (void *)xbuf, (void *)part})
+        if (p) cudaFree(p);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream && stream_owned) cudaStreamDestroy(stream);
+}
+
+static int ensure(void **p, size_t *cap, size_t bytes, char *err, size_t errlen)
+{
+    if (*cap >= bytes && *p) return FPLUS_OK;
+    if (*p) { cudaFree(*p); *p = nullptr; *cap = 0; }
+    CK(cudaMalloc(p, bytes > 0 ? bytes : 16));
+    *cap = bytes;
+    return FPLUS_OK;
+}
+
+int dev_num_init(DevNum &N, int64_t n, int64_t nnz, int cplx, char *err, size_t errlen)
+{
+    N.n = n; N.nnz = nnz; N.cplx = cplx;
+    N.vs = cplx ? 16 : 8;
+    CK(cudaGetDevice(&N.device));
+    CK(cudaStreamCreateWithFlags(&N.stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&N.ev0));
+    CK(cudaEventCreate(&N.ev1));
+    const size_t nn = (size_t)(n > 0 ? n : 1), nz = (size_t)(nnz > 0 ? nnz : 1);
+    CK(cudaMalloc((void **)&N.Ax, nz * N.vs));
+    CK(cudaMalloc((void **)&N.Bx, nz * N.vs));
+    CK(cudaMalloc((void **)&N.Drp, nn * 8));
+    CK(cudaMalloc((void **)&N.Dcp, nn * 8));
+    CK(cudaMalloc((void **)&N.colmax, nn * 8));
+    CK(cudaMalloc((void **)&N.p_lu, nn * 8));
+    CK(cudaMalloc((void **)&N.pinv, nn * 8));
+    CK(cudaMalloc((void **)&N.st, sizeof(DevStatus)));
+    CK(cudaMalloc((void **)&N.scratch, 2 * nn * 8));
+    return FPLUS_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// permutation + Ruiz: Bx = the scaled permuted values, Drp / Dcp, colmax; returns FPLUS_OK or an error
+template <typename T>
+static int run_equil(const DevPlan &D, DevNum &N, int equilibrate, int max_iter, double tol, char *err, size_t errlen)
+{
+    cudaStream_t s = N.stream;
+    const int64_t n = N.n, nnz = N.nnz;
+    T *Bx = (T *)N.Bx;
+    k_gather<T><<<nblk(nnz), 256, 0, s>>>(Bx, (const T *)N.Ax, D.Bsrc, nnz);
+    DevStatus h0;
+    std::memset(&h0, 0, sizeof(h0));
+    h0.amin_bits = 0x7ff0000000000000ull;       // +inf
+    h0.idx = INT64_MAX;                         // the smallest failing index wins
+    CK(cudaMemcpyAsync(N.st, &h0, sizeof(h0), cudaMemcpyHostToDevice, s));
+    std::vector<double> ones((size_t)(n > 0 ? n : 1), 1.0);
+    CK(cudaMemcpyAsync(N.Drp, ones.data(), (size_t)n * 8, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(N.Dcp, ones.data(), (size_t)n * 8, cudaMemcpyHostToDevice, s));
+    if (equilibrate) {
+        // range guard (FPLUS src/equil.c:197-241)
+        const int64_t m = (N.cplx ? 2 : 1) * nnz;
+        k_abs_range<<<nblk(m), 256, 0, s>>>((const double *)Bx, m, N.st);
+        DevStatus h;
+        CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        double amax = bitsd_h(h.amax_bits), amin = bitsd_h(h.amin_bits);
+        int k4 = 0;
+        if (amax > 0.0 && (amax > 0x1p500 || amin < 0x1p-500)) {
+            int emax = std::ilogb(amax), emin = std::ilogb(amin);
+            if (emax - emin > 990) {
+                unsigned long long *lmax = (unsigned long long *)N.scratch;
+                CK(cudaMemsetAsync(lmax, 0, (size_t)(2 * n) * 8, s));
+                if (N.cplx) k_line_max<true><<<nblk(n), 256, 0, s>>>(D.Bp, D.Bi, (const double *)Bx, n, lmax);
+                else k_line_max<false><<<nblk(n), 256, 0, s>>>(D.Bp, D.Bi, (const double *)Bx, n, lmax);
+                unsigned long long inf = 0x7ff0000000000000ull;
+                CK(cudaMemcpyAsync(&N.st->amin_bits, &inf, 8, cudaMemcpyHostToDevice, s));
+                k_min_pos<<<nblk(2 * n), 256, 0, s>>>(lmax, 2 * n, N.st);
+                CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, s));
+                CK(cudaStreamSynchronize(s));
+                double lmin = bitsd_h(h.amin_bits);
+                int elmin = std::ilogb(lmin);
+                if (emax - elmin > 990) {
+                    errf(err, errlen, "line maxima span 2^%d .. 2^%d (entries 2^%d ..): wider than Ruiz equilibration can handle "
+                         "in double precision; factor without equilibration (equilibrate=False)", elmin, emax, emin);
+                    return FPLUS_ERR_BADARG;
+                }
+                emin = elmin;
+            }
+            k4 = -((emax + emin) / 2 / 4) * 4;
+            k_scale_raw<<<nblk(m), 256, 0, s>>>((double *)Bx, m, std::ldexp(1.0, k4));
+        }
+        unsigned long long *rmax = (unsigned long long *)N.scratch, *cmax = rmax + n;
+        for (int it = 0; it < max_iter; it++) {
+            CK(cudaMemsetAsync(rmax, 0, (size_t)n * 8, s));
+            k_ruiz_rowmax<T><<<nblk(nnz), 256, 0, s>>>(D.Bi, Bx, nnz, rmax, N.st);
+            k_ruiz_rowscale<<<nblk(n), 256, 0, s>>>(n, rmax, N.Drp, N.st);
+            k_first_zero<<<nblk(n), 256, 0, s>>>(n, rmax, N.st, ST_ZERO_ROW);
+            k_ruiz_colpass<T><<<nblk(32 * n), 256, 0, s>>>(D.Bp, D.Bi, Bx, n, rmax, cmax, N.st);
+            k_ruiz_colscale<<<nblk(n), 256, 0, s>>>(n, cmax, N.Dcp, N.st);
+            k_first_zero<<<nblk(n), 256, 0, s>>>(n, cmax, N.st, ST_ZERO_COL);
+            k_ruiz_colapply<T><<<nblk(32 * n), 256, 0, s>>>(D.Bp, Bx, n, cmax, N.st);
+            k_ruiz_check<<<1, 1, 0, s>>>(N.st, tol);
+        }
+        if (k4 != 0) k_fold<<<nblk(n), 256, 0, s>>>(N.Drp, N.Dcp, n, std::ldexp(1.0, k4 / 2));
+    }
+    k_colmax<T><<<nblk(32 * n), 256, 0, s>>>(D.Bp, Bx, n, N.colmax);
+    CK(cudaGetLastError());
+    DevStatus h;
+    CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    N.ruiz_iters = h.iters;
+    if (h.code == ST_ZERO_ROW) {
+        errf(err, errlen, "Row %ld of the matrix is entirely zero (structural singularity detected during equilibration).", (long)h.idx);
+        return FPLUS_ERR_SINGULAR;
+    }
+    if (h.code == ST_ZERO_COL) {
+        errf(err, errlen, "Column %ld of the matrix is entirely zero (structural singularity detected during equilibration).", (long)h.idx);
+        return FPLUS_ERR_SINGULAR;
+    }
+    return FPLUS_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// the fronts, in order.  Returns FPLUS_OK, or ST_BORDER through *border_front (>= 0) for a restart with a dense chain.
+template <typename T>
+static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pivot_rel, int64_t *border_front,
+                      char *err, size_t errlen)
+{
+    cudaStream_t s = N.stream;
+    const int64_t vs = N.vs;
+    int rc;
+    *border_front = -1;
+    if ((rc = ensure((void **)&N.Larena, &N.cap_L, (size_t)P.L_size * vs, err, errlen))) return rc;
+    if ((rc = ensure((void **)&N.Uarena, &N.cap_U, (size_t)P.U_size * vs, err, errlen))) return rc;
+    if ((rc = ensure((void **)&N.cbstack, &N.cap_cb, (size_t)P.cb_size * vs, err, errlen))) return rc;
+    if ((rc = ensure((void **)&N.work, &N.cap_work, (size_t)P.work_size * vs, err, errlen))) return rc;
+    if ((rc = ensure((void **)&N.rowid, &N.cap_rowid, (size_t)P.rows_total * 8, err, errlen))) return rc;
+    if ((rc = ensure((void **)&N.ipiv, &N.cap_ipiv, (size_t)(N.n > 0 ? N.n : 1) * 4, err, errlen))) return rc;
+    DevStatus h0;
+    std::memset(&h0, 0, sizeof(h0));
+    CK(cudaMemcpyAsync(N.st, &h0, sizeof(h0), cudaMemcpyHostToDevice, s));
+    T *W = (T *)N.work, *La = (T *)N.Larena, *Ua = (T *)N.Uarena, *CB = (T *)N.cbstack;
+    const T *Bx = (const T *)N.Bx;
+    constexpr int PW = 32;       // panel width
+    const int64_t nf = (int64_t)P.fronts.size();
+    for (int64_t fi = 0; fi < nf; fi++) {
+        const Front &F = P.fronts[fi];
+        const int64_t nr = F.nrows, nc = F.ncols, np = F.npiv, ncb = nc - np;
+        const int64_t ld = nr;
+        if (nr * nc > 0) CK(cudaMemsetAsync(W, 0, (size_t)(nr * nc) * vs, s));
+        {
+            const int64_t cnt = F.asm_end - F.asm_begin;
+            k_assemble<T><<<nblk(std::max(cnt, nr)), 256, 0, s>>>(W, Bx, D.asm_src + F.asm_begin, D.asm_dst + F.asm_begin, cnt,
+                                                                   N.rowid + F.row_off, D.rowinit + F.row_off, nr, N.st);
+        }
+        for (int64_t k = F.child_begin; k < F.child_end; k++) {
+            const Front &G = P.fronts[P.children[k]];
+            const int64_t cbr = std::max<int64_t>(0, G.nrows - G.npiv), cbc = G.ncols - G.npiv;
+            const int64_t nslot = std::max<int64_t>(0, G.nri - G.npiv);
+            if (cbr == 0) continue;
+            k_extend_add<T><<<nblk(std::max(cbr * cbc, nslot)), 256, 0, s>>>(W, ld, CB + G.cb_off, cbr, cbc, nslot, G.slot,
+                                                                            F.tau_base, D.relcol + G.relcol_off,
+                                                                            N.rowid + F.row_off, N.rowid + G.row_off + G.npiv, N.st);
+        }
+        if (np > 0 && nr > 0) {
+            const int64_t npr = std::min(np, nr);
+            // left part: blocked partial-pivot LU of the nrows x npiv pivot block
+            for (int64_t k0 = 0; k0 < npr; k0 += PW) {
+                const int w = (int)std::min<int64_t>(PW, npr - k0);
+                k_panel<T><<<1, 512, 0, s>>>(W, ld, nr, F.nri, (int)k0, w, F.f, N.colmax, pivot_rel, N.rowid + F.row_off,
+                                            N.ipiv + F.f, N.st, fi);
+                // the swaps on the pivot block's other columns
+                if (k0 > 0) k_laswp<T><<<nblk(k0, 128), 128, 0, s>>>(W, ld, N.ipiv + F.f, (int)k0, w, 0, k0, N.st);
+                if (k0 + w < np) {
+                    k_laswp<T><<<nblk(np - k0 - w, 128), 128, 0, s>>>(W, ld, N.ipiv + F.f, (int)k0, w, k0 + w, np, N.st);
+                    k_trsm_unit<T><<<nblk(np - k0 - w, 128), 128, 0, s>>>(W, ld, (int)k0, w, k0 + w, np, N.st);
+                    const int64_t M = nr - k0 - w, Nn = np - k0 - w;
+                    if (M > 0) {
+                        dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((Nn + GBN - 1) / GBN));
+                        k_gemm_sub<T><<<g, 256, 0, s>>>(M, Nn, w, W + (k0 + w) + k0 * ld, ld, W + k0 + (k0 + w) * ld, ld,
+                                                        W + (k0 + w) + (k0 + w) * ld, ld, N.st);
+                    }
+                }
+            }
+            if (ncb > 0) {
+                // right part: the swaps, U12 = L11^-1 A12 (blocked), then the Schur complement CB -= L21 U12
+                k_laswp<T><<<nblk(ncb, 128), 128, 0, s>>>(W, ld, N.ipiv + F.f, 0, (int)npr, np, nc, N.st);
+                for (int64_t k0 = 0; k0 < npr; k0 += PW) {
+                    const int w = (int)std::min<int64_t>(PW, npr - k0);
+                    k_trsm_unit<T><<<nblk(ncb, 128), 128, 0, s>>>(W, ld, (int)k0, w, np, nc, N.st);
+                    const int64_t M = npr - k0 - w;
+                    if (M > 0) {
+                        dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((ncb + GBN - 1) / GBN));
+                        k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, w, W + (k0 + w) + k0 * ld, ld, W + k0 + np * ld, ld,
+                                                        W + (k0 + w) + np * ld, ld, N.st);
+                    }
+                }
+                const int64_t M = nr - np;
+                if (M > 0) {
+                    dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((ncb + GBN - 1) / GBN));
+                    k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, np, W + np, ld, W + np * ld, ld, W + np + np * ld, ld, N.st);
+                }
+            }
+        }
+        k_copyout<T><<<nblk(std::max(nr * np, std::max(np * ncb, std::max<int64_t>(0, nr - np) * ncb))), 256, 0, s>>>(
+            W, nr, nc, np, La + F.L_off, Ua + F.U_off, CB + F.cb_off, N.rowid + F.row_off, F.f, N.p_lu, N.st);
+        if ((fi & 255) == 255) CK(cudaGetLastError());
+    }
+    CK(cudaGetLastError());
+    k_pinv<<<nblk(N.n), 256, 0, s>>>(N.p_lu, N.pinv, N.n);
+    DevStatus h;
+    CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h.code == ST_BORDER) { *border_front = h.idx; return FPLUS_OK; }
+    if (h.code == ST_SINGULAR) {
+        errf(err, errlen, "Near-zero or zero pivot %.6e at step %ld (threshold %.6e). Matrix is singular.", h.best, (long)h.idx, h.thr);
+        return FPLUS_ERR_SINGULAR;
+    }
+    if (h.code != ST_OK) { errf(err, errlen, "factorization: device status %d", h.code); return FPLUS_ERR_INTERNAL; }
+    return FPLUS_OK;
+}
+
+int dev_equilibrate(const DevPlan &D, DevNum &N, int equilibrate, int max_iter, double tol, char *err, size_t errlen)
+{
+    return N.cplx ? run_equil<cplx>(D, N, equilibrate, max_iter, tol, err, errlen)
+                  : run_equil<double>(D, N, equilibrate, max_iter, tol, err, errlen);
+}
+
+int dev_factor_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pivot_rel, int64_t *border_front,
+                      char *err, size_t errlen)
+{
+    return N.cplx ? run_fronts<cplx>(P, D, N, pivot_rel, border_front, err, errlen)
+                  : run_fronts<double>(P, D, N, pivot_rel, border_front, err, errlen);
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// solves on device buffers: x (n x nrhs, ld = n) in, solution out, through the plan's fronts
+template <typename T>
+static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int64_t nrhs, int trans, char *err, size_t errlen)
+{
+    cudaStream_t s = N.stream;
+    const int64_t n = N.n;
+    int rc;
+    const size_t nb = (size_t)(n > 0 ? n : 1) * (size_t)nrhs * sizeof(T);
+    if ((rc = ensure((void **)&N.rbuf, &N.cap_r, nb, err, errlen))) return rc;
+    if ((rc = ensure((void **)&N.sbuf, &N.cap_s, nb, err, errlen))) return rc;
+    const int64_t chunk = 256;
+    int64_t maxpart = 1;
+    for (const Front &F : P.fronts) maxpart = std::max(maxpart, ((F.ncols - F.npiv + chunk - 1) / chunk) * F.npiv);
+    if ((rc = ensure((void **)&N.part, &N.cap_part, (size_t)maxpart * (size_t)nrhs * sizeof(T), err, errlen))) return rc;
+    T *R = (T *)N.rbuf, *S2 = (T *)N.sbuf, *part = (T *)N.part;
+    const T *La = (const T *)N.Larena, *Ua = (const T *)N.Uarena;
+    const int64_t nf = (int64_t)P.fronts.size();
+    const size_t smem = (size_t)P.max_npiv * (size_t)nrhs * sizeof(T);
+    if (smem > 48 * 1024) {
+        CK(cudaFuncSetAttribute(k_bwdU<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CK(cudaFuncSetAttribute(k_bwdLt<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CK(cudaFuncSetAttribute(k_bwdLt<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    if (trans == 0) {
+        // R (row space) = Dr * b[row_perm]; forward with L; S2 = R[p_lu] (pivot order); backward with U into R
+        k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, n, D.row_perm, N.Drp, n, nrhs);
+        for (int64_t fi = 0; fi < nf; fi++) {
+            const Front &F = P.fronts[fi];
+            if (F.npiv == 0 || F.nrows == 0) continue;
+            k_fwdL<T><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs);
+        }
+        k_gather_rows<T><<<nblk(n * nrhs), 256, 0, s>>>(S2, R, N.p_lu, n, nrhs);
+        for (int64_t fi = nf - 1; fi >= 0; fi--) {
+            const Front &F = P.fronts[fi];
+            const int64_t ncb = F.ncols - F.npiv;
+            if (F.npiv == 0) continue;
+            int64_t nchunk = 0;
+            if (ncb > 0) {
+                nchunk = (ncb + chunk - 1) / chunk;
+                k_u12_gemv<T><<<(unsigned)nchunk, 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, R, n, nrhs,
+                                                               chunk, part);
+            }
+            k_bwdU<T><<<1, 256, (size_t)F.npiv * nrhs * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, part, nchunk, S2, R,
+                                                                         n, nrhs, N.st);
+        }
+        // x[col_perm[k]] = Dcp[k] * R[k]
+        k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, R, D.col_perm, nullptr, N.Dcp, n, nrhs);
+    } else {
+        // R (column space) = Dc * b[col_perm]; forward with U^T; backward with L^T into S2 (pivot order)
+        k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, n, D.col_perm, N.Dcp, n, nrhs);
+        const bool cj = trans == 2;
+        for (int64_t fi = 0; fi < nf; fi++) {
+            const Front &F = P.fronts[fi];
+            const int64_t ncb = F.ncols - F.npiv;
+            if (F.npiv == 0) continue;
+            if (cj) k_fwdUt<T, true><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st);
+            else k_fwdUt<T, false><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st);
+            if (ncb > 0) {
+                if (cj) k_ut_scatter<T, true><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, F.f, R, n, nrhs);
+                else k_ut_scatter<T, false><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, F.f, R, n, nrhs);
+            }
+        }
+        for (int64_t fi = nf - 1; fi >= 0; fi--) {
+            const Front &F = P.fronts[fi];
+            if (F.npiv == 0) continue;
+            const size_t sm = (size_t)F.npiv * nrhs * sizeof(T);
+            if (cj) k_bwdLt<T, true><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, N.rowid + F.row_off, N.pinv, R, S2, n, nrhs);
+            else k_bwdLt<T, false><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, N.rowid + F.row_off, N.pinv, R, S2, n, nrhs);
+        }
+        // x[row_perm[p_lu[k]]] = Drp[p_lu[k]] * S2[k]
+        k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, S2, D.row_perm, N.p_lu, N.Drp, n, nrhs);
+    }
+    CK(cudaGetLastError());
+    return FPLUS_OK;
+}
+
+int dev_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, void *x_dev, int64_t nrhs, int trans, char *err, size_t errlen)
+{
+    return N.cplx ? run_solve<cplx>(P, D, N, (cplx *)x_dev, nrhs, trans, err, errlen)
+                  : run_solve<double>(P, D, N, (double *)x_dev, nrhs, trans, err, errlen);
+}
+
+int dev_status(DevNum &N, int *code, int64_t *idx, char *err, size_t errlen)
+{
+    DevStatus h;
+    CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, N.stream));
+    CK(cudaStreamSynchronize(N.stream));
+    *code = h.code; *idx = h.idx;
+    return FPLUS_OK;
+}
+
+int dev_clear_status(DevNum &N, char *err, size_t errlen)
+{
+    DevStatus h0;
+    std::memset(&h0, 0, sizeof(h0));
+    h0.idx = INT64_MAX;
+    CK(cudaMemcpyAsync(N.st, &h0, sizeof(h0), cudaMemcpyHostToDevice, N.stream));
+    return FPLUS_OK;
+}
+
+int dev_ensure_x(DevNum &N, size_t bytes, char *err, size_t errlen)
+{
+    return ensure((void **)&N.xbuf, &N.cap_x, bytes, err, errlen);
+}
+
+int dev_check_finite(DevNum &N, char *err, size_t errlen)
+{
+    const int64_t m = (N.cplx ? 2 : 1) * N.nnz;
+    if (dev_clear_status(N, err, errlen) != FPLUS_OK) return FPLUS_ERR_GPU;
+    k_check_finite<<<nblk(m), 256, 0, N.stream>>>((const double *)N.Ax, m, N.st);
+    DevStatus h;
+    CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, N.stream));
+    CK(cudaStreamSynchronize(N.stream));
+    if (h.code != 0) {
+        errf(err, errlen, "non-finite value in entry %ld", (long)(N.cplx ? h.idx / 2 : h.idx));
+        return FPLUS_ERR_BADARG;
+    }
+    return FPLUS_OK;
+}
+
+}  // namespace fpl

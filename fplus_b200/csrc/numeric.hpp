@@ -1,0 +1,57 @@
+// numeric.hpp -- the device state of the numeric phase and the launch sequences (numeric.cu).
+#pragma once
+#include <cstdint>
+#include <cstring>
+#include <cuda_runtime.h>
+#include "internal.hpp"
+#include "plan.hpp"
+
+namespace fpl {
+
+struct DevStatus;
+
+inline double bitsd_h(unsigned long long b) { double d; std::memcpy(&d, &b, 8); return d; }
+
+// device copies of a plan and of the symbolic object's permutation (read-only, shared by every factorization)
+struct DevPlan {
+    int device = -1;
+    int64_t *cols = nullptr, *relcol = nullptr, *rowinit = nullptr, *asm_src = nullptr, *asm_dst = nullptr;
+    int64_t *Bp = nullptr, *Bi = nullptr, *Bsrc = nullptr, *row_perm = nullptr, *col_perm = nullptr;
+    ~DevPlan();
+};
+
+// the device buffers of one factorization (and of its solves)
+struct DevNum {
+    int device = -1;
+    int64_t n = 0, nnz = 0;
+    int cplx = 0;
+    int64_t vs = 8;
+    cudaStream_t stream = nullptr;
+    bool stream_owned = true;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    void *Ax = nullptr, *Bx = nullptr;
+    double *Drp = nullptr, *Dcp = nullptr, *colmax = nullptr;
+    void *Larena = nullptr, *Uarena = nullptr, *cbstack = nullptr, *work = nullptr;
+    size_t cap_L = 0, cap_U = 0, cap_cb = 0, cap_work = 0, cap_rowid = 0, cap_ipiv = 0;
+    int64_t *rowid = nullptr, *p_lu = nullptr, *pinv = nullptr;
+    int *ipiv = nullptr;
+    DevStatus *st = nullptr;
+    void *scratch = nullptr;
+    void *rbuf = nullptr, *sbuf = nullptr, *xbuf = nullptr, *part = nullptr;
+    size_t cap_r = 0, cap_s = 0, cap_x = 0, cap_part = 0;
+    int ruiz_iters = 0;
+    ~DevNum();
+};
+
+int dev_upload_plan(const fplus_symbolic *S, const FrontPlan &P, DevPlan &D, char *err, size_t errlen);
+int dev_num_init(DevNum &N, int64_t n, int64_t nnz, int cplx, char *err, size_t errlen);
+int dev_equilibrate(const DevPlan &D, DevNum &N, int equilibrate, int max_iter, double tol, char *err, size_t errlen);
+int dev_factor_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pivot_rel, int64_t *border_front,
+                      char *err, size_t errlen);
+int dev_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, void *x_dev, int64_t nrhs, int trans, char *err, size_t errlen);
+int dev_status(DevNum &N, int *code, int64_t *idx, char *err, size_t errlen);
+int dev_clear_status(DevNum &N, char *err, size_t errlen);
+int dev_check_finite(DevNum &N, char *err, size_t errlen);
+int dev_ensure_x(DevNum &N, size_t bytes, char *err, size_t errlen);
+
+}  // namespace fpl

@@ -1,0 +1,60 @@
+/* fplus_b200.h -- additions of the B200 build of FPLUS to the fplus.h interface (libfplus.so).
+ *
+ * fplus.h stays ABI-identical to FPLUS; what this build adds lives here, as new functions: device-resident inputs and
+ * right-hand sides (no host copies in the way), the CUDA stream to run on, factorization statistics, and the pieces of
+ * the symbolic analysis the tests inspect.  None of these has a counterpart in FPLUS unless its comment names one.
+ */
+#ifndef FPLUS_B200_H
+#define FPLUS_B200_H
+
+#include "fplus.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Statistics of one factorization. */
+typedef struct {
+    int64_t n;
+    int64_t nfronts;            /* fronts of the multifrontal structure used */
+    int64_t f_dense;            /* first column of the dense chain (n when there is none) */
+    int     attempts;           /* 1, or 2 when a dense row was chosen as a pivot before the chain and the LU was redone */
+    int     ruiz_iters;         /* Ruiz iterations run */
+    int64_t nnz_L, nnz_U;       /* stored entries (explicit zeros of the front structure included) */
+    double  front_flops;        /* real floating-point operations of the front factorizations (complex: x4) */
+    double  ms_equil;           /* device time: permutation + Ruiz */
+    double  ms_fronts;          /* device time: the fronts (last attempt) */
+    int64_t device_bytes;       /* device memory held by the factorization */
+} fplus_b200_info;
+
+int fplus_b200_numeric_info(const fplus_numeric *num, fplus_b200_info *info);
+
+/* Run this host thread's subsequent fplus_factor / fplus_solve / fplus_b200_* calls on the given CUDA stream
+ * (a cudaStream_t; NULL: each factorization's own stream). */
+void fplus_b200_use_stream(void *stream);
+
+/* fplus_factor with the values already in device memory (Ax_dev: nnz doubles or nnz interleaved complex pairs, the
+ * analysed pattern Ap / Ai on the host).  The values are checked for finiteness on the device. */
+int fplus_b200_factor_dev(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax_dev, int is_complex,
+                          const fplus_options *opt, fplus_numeric **num, char *err, size_t errlen);
+
+/* fplus_solve with the right-hand sides in device memory (column-major, leading dimension ldb >= n), solved in place. */
+int fplus_b200_solve_dev(const fplus_numeric *num, void *b_dev, int64_t nrhs, int64_t ldb, int trans, char *err, size_t errlen);
+
+/* The fill-reducing column order of the interior pattern (the dense rows' entries and the dense columns, given by the
+ * 0/1 masks, left out; empty columns last).  The order fplus_analyze uses before the column-etree postorder. */
+int fplus_b200_interior_order(int64_t n, const int64_t *Ap, const int64_t *Ai, const unsigned char *tau_row_mask,
+                              const unsigned char *tau_col_mask, int64_t *perm);
+
+/* The multifrontal structure of an analysed pattern (host only, no GPU): with a dense chain from column `tail`
+ * (-1: none).  plan_size returns the number of fronts and the total length of the column lists; plan_export fills
+ * col_front[n] (the front of each column), parent[nf], col_ptr[nf + 1] / cols[] (each front's columns: pivot columns
+ * first), nrows[nf] and nbord[nf] (its rows, the border rows among them). */
+int fplus_b200_plan_size(const fplus_symbolic *sym, int64_t tail, int64_t *nfronts, int64_t *ncols_total, int64_t *f_dense);
+int fplus_b200_plan_export(const fplus_symbolic *sym, int64_t tail, int64_t *col_front, int64_t *parent, int64_t *col_ptr,
+                           int64_t *cols, int64_t *nrows, int64_t *nbord);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FPLUS_B200_H */
