@@ -106,9 +106,9 @@ static int factor_common(const fplus_symbolic *sym, const int64_t *Ap, const int
         num->n = n; num->is_complex = is_complex ? 1 : 0;
         num->dev.reset(new DevNum);
         DevNum &N = *num->dev;
+        if (tl_stream) N.stream = tl_stream;
         rc = dev_num_init(N, n, sym->nnz, num->is_complex, err, errlen);
         if (rc) return rc;
-        if (tl_stream) { cudaStreamDestroy(N.stream); N.stream = tl_stream; N.stream_owned = false; }
         const size_t bytes = (size_t)sym->nnz * (size_t)N.vs;
         if (bytes) CKH(cudaMemcpyAsync(N.Ax, Ax, bytes, ax_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, N.stream));
         std::shared_ptr<FrontPlan> P;

@@ -2,6 +2,7 @@
 // of the multifrontal LU (assembly, extend-add, panel with partial pivoting, row swaps, unit-lower TRSM, FP64 tensor-core
 // GEMM, copy-out) and the supernodal triangular sweeps.  Included once, by numeric.cu.
 #pragma once
+#include <climits>
 #include "dev_common.cuh"
 
 namespace fpl {
@@ -101,7 +102,7 @@ __global__ void k_ruiz_rowscale(int64_t n, unsigned long long *__restrict__ rmax
 // zero-row index: the smallest (second pass so the index is deterministic)
 __global__ void k_first_zero(int64_t n, const unsigned long long *__restrict__ v, DevStatus *st, int code)
 {
-    if (st->code != code) return;
+    if (st->code != code || st->done) return;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         if (bitsd(v[i]) == 0.0) atomicMin((unsigned long long *)&st->idx, (unsigned long long)i);
 }
@@ -156,7 +157,8 @@ __global__ void k_ruiz_colapply(const int64_t *__restrict__ Bp, T *__restrict__ 
 // end of an iteration: count it, stop when the residual is below tol (FPLUS src/equil.c:405-411)
 __global__ void k_ruiz_check(DevStatus *st, double tol)
 {
-    if (st->done || st->code) return;
+    if (st->done) return;
+    if (st->code) { st->done = 1; return; }      // an error: later iterations change nothing (the index stays)
     st->iters++;
     if (bitsd(st->res_bits) < tol) st->done = 1;
     st->res_bits = 0ull;
@@ -304,6 +306,7 @@ __global__ void k_laswp(T *__restrict__ W, int64_t ld, const int *__restrict__ i
         T *col = W + c * ld;
         for (int k = 0; k < cnt; k++) {
             const int64_t j = k0 + k, p = ipiv[j];
+            if (p < 0 || p >= ld) continue;       // never written by a panel that stopped: skip
             if (p != j) { T t = col[j]; col[j] = col[p]; col[p] = t; }
         }
     }
@@ -338,7 +341,7 @@ __global__ void __launch_bounds__(128) k_trsm_unit(T *__restrict__ W, int64_t ld
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
-// C <- C - A B (column-major; M x K times K x N) on the FP64 tensor cores: mma.sync m8n8k4 f64 (DMMA).  64 x 64 block
+// Cout <- Cin - A B (column-major; M x K times K x N; Cin's rows optionally gathered through rmap) on the FP64 tensor cores: mma.sync m8n8k4 f64 (DMMA).  64 x 64 block
 // tiles, 16-deep K slices staged in shared memory, 8 warps of 32 x 16.  Complex: four real products per complex one
 // (Cr += Ar Br - Ai Bi, Ci += Ar Bi + Ai Br), the minus folded into a negated copy of Bi.
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
@@ -351,8 +354,8 @@ constexpr int GBM = 64, GBN = 64, GBK = 16, GPAD = 68;
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_gemm_sub(int64_t M, int64_t N, int64_t K, const T *__restrict__ A, int64_t lda,
-                                                 const T *__restrict__ B, int64_t ldb, T *__restrict__ C, int64_t ldc,
-                                                 const DevStatus *st)
+                                                 const T *__restrict__ B, int64_t ldb, const T *Cin, int64_t ldci,
+                                                 const int *__restrict__ rmap, T *Cout, int64_t ldco, const DevStatus *st)
 {
     constexpr bool CP = VT<T>::cplx_;
     __shared__ double As[CP ? 2 : 1][GBK][GPAD];
@@ -424,9 +427,11 @@ __global__ void __launch_bounds__(256) k_gemm_sub(int64_t M, int64_t N, int64_t 
                 const int64_t gm = m0 + wm * 32 + a * 8 + (lane >> 2);
                 const int64_t gn = n0 + wn * 16 + b * 8 + 2 * (lane & 3) + h;
                 if (gm < M && gn < N) {
-                    T *c = C + gm + gn * ldc;
-                    if constexpr (CP) { cplx v = *c; v.x -= acc[0][a][b][h]; v.y -= acc[1][a][b][h]; *c = v; }
-                    else *c -= acc[0][a][b][h];
+                    const int64_t gi = rmap ? (int64_t)rmap[gm] : gm;
+                    T v = Cin[gi + gn * ldci];
+                    if constexpr (CP) { v.x -= acc[0][a][b][h]; v.y -= acc[1][a][b][h]; }
+                    else v -= acc[0][a][b][h];
+                    Cout[gm + gn * ldco] = v;
                 }
             }
 }
@@ -445,6 +450,174 @@ __global__ void k_copyout(const T *__restrict__ W, int64_t nrows, int64_t ncols,
     for (int64_t e = tid; e < npiv * ncb; e += stride) { int64_t i = e % npiv, c = e / npiv; Uo[e] = W[i + (npiv + c) * nrows]; }
     for (int64_t e = tid; e < cbr * ncb; e += stride) { int64_t i = e % cbr, c = e / cbr; CBo[e] = W[npiv + i + (npiv + c) * nrows]; }
     for (int64_t i = tid; i < npiv && i < nrows; i += stride) p_lu[f + i] = rowid[i];
+}
+
+// Partial-pivot LU of a front's pivot block (nrows x npiv, in shared memory, one CTA), without row swaps: a row chosen
+// as the pivot of step j is tagged j and leaves the updates; the others are scaled and updated in place.  Per step the
+// argmax (largest modulus, ties to the smaller row of B) is computed by every warp from shared memory with shuffles, so
+// one barrier per step suffices.  Threads: row i = t % R, column group g = t / R (R = nrows rounded up to a warp).
+// Output, in the final row order (pivot rows by step, then the other rows in their order): the packed L\U block into the
+// arena, the row ids, the pivot rows (p_lu) and the order itself (perm: position -> local row) for the other columns.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_front_lu(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
+                                                   int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
+                                                   int64_t *__restrict__ rowid, T *__restrict__ Lout, int *__restrict__ perm,
+                                                   int64_t *__restrict__ p_lu, DevStatus *st, int64_t front)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *A = reinterpret_cast<T *>(smem_raw);                        // npiv x nrows, column-major: A[c * nrows + i]
+    T *lcol = A + (size_t)npiv * nrows;                            // this step's multipliers
+    int64_t *rid = reinterpret_cast<int64_t *>(lcol + nrows);
+    int *tag = reinterpret_cast<int *>(rid + nrows);
+    int *pos = tag + nrows;
+    __shared__ int s_stop;
+    const int tid = threadIdx.x, lane = tid & 31, nt = blockDim.x;
+    const int R = (nrows + 31) & ~31;
+    const int G = nt >= R ? nt / R : 1;                            // column groups per row
+    const int rstep = nt >= R ? R : nt;                            // row stride of a thread
+    const int my_i = nt >= R ? tid % R : tid, my_g = nt >= R ? tid / R : 0;
+    if (tid == 0) s_stop = st->code != 0;
+    for (int64_t e = tid; e < (int64_t)npiv * nrows; e += nt) {
+        const int i = (int)(e % nrows), c = (int)(e / nrows);
+        A[e] = W[i + c * ld];
+    }
+    for (int i = tid; i < nrows; i += nt) { rid[i] = rowid[i]; tag[i] = INT_MAX; }
+    __syncthreads();
+    if (s_stop) return;
+    const int steps = npiv;
+    for (int j = 0; j < steps; j++) {
+        // argmax over the rows not pivoted before step j (tag >= j; tid 0 tags this step's pivot during the step, which
+        // keeps it a candidate for the warps still searching), the same result in every warp
+        double bv = -1.0; int bi = -1; int64_t br = INT64_MAX;
+        for (int i = lane; i < nrows; i += 32) {
+            if (tag[i] < j) continue;
+            const double a = vabs(A[(size_t)j * nrows + i]);
+            const int64_t r = rid[i];
+            if (a > bv || (a == bv && r < br)) { bv = a; bi = i; br = r; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            const int64_t orr = __shfl_xor_sync(0xffffffffu, br, o);
+            if (ov > bv || (ov == bv && orr < br)) { bv = ov; bi = oi; br = orr; }
+        }
+        const double thr = pivot_rel * colmax[fcol + j];
+        if (bi < 0 || bv <= 0.0 || bv < thr) {
+            if (tid == 0) set_status(st, ST_SINGULAR, fcol + j, bv > 0 ? bv : 0.0, thr);
+            return;
+        }
+        if (bi >= nri) {
+            if (tid == 0) set_status(st, ST_BORDER, front, bv, thr);
+            return;
+        }
+        // the previous step's multipliers into column j - 1 (read by nobody from here on): rows not pivoted up to j - 1
+        if (j > 0 && my_g == 0)
+            for (int i = my_i; i < nrows; i += rstep) if (tag[i] > j - 1) A[(size_t)(j - 1) * nrows + i] = lcol[i];
+        const T piv = A[(size_t)j * nrows + bi];
+        if (tid == 0) tag[bi] = j;
+        for (int i = my_i; i < nrows; i += rstep) {
+            if (i == bi || tag[i] <= j) continue;
+            const T l = divv(A[(size_t)j * nrows + i], piv);
+            for (int c = j + 1 + my_g; c < npiv; c += G) {
+                T *x = A + (size_t)c * nrows + i;
+                *x = sub(*x, mul(l, A[(size_t)c * nrows + bi]));
+            }
+            if (my_g == 0) lcol[i] = l;
+        }
+        __syncthreads();
+    }
+    if (steps > 0 && my_g == 0)
+        for (int i = my_i; i < nrows; i += rstep) if (tag[i] > steps - 1) A[(size_t)(steps - 1) * nrows + i] = lcol[i];
+    // final order: position tag[i] for the pivot rows, then the untagged rows in order (a ballot scan by warp 0)
+    if (tid < 32) {
+        int base = steps;
+        for (int i0 = 0; i0 < nrows; i0 += 32) {
+            const int i = i0 + lane;
+            const bool un = i < nrows && tag[i] >= steps;
+            const unsigned m = __ballot_sync(0xffffffffu, un);
+            if (i < nrows) pos[i] = un ? base + __popc(m & ((1u << lane) - 1u)) : tag[i];
+            base += __popc(m);
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < nrows; i += nt) {
+        const int k = pos[i];
+        perm[k] = i;
+        rowid[k] = rid[i];
+        if (k < steps) p_lu[fcol + k] = rid[i];
+    }
+    for (int64_t e = tid; e < (int64_t)npiv * nrows; e += nt) {
+        const int i = (int)(e % nrows), c = (int)(e / nrows);
+        Lout[pos[i] + (int64_t)c * nrows] = A[e];
+    }
+}
+
+// After the blocked (global-memory) pivoting of a large front's pivot block: the final row order from the swaps, the
+// pivot rows (the swaps already moved the row ids), and the block into the arena
+template <typename T>
+__global__ void k_left_finish(const T *__restrict__ W, int64_t ld, int64_t nrows, int64_t npiv, const int *__restrict__ ipiv,
+                              int *__restrict__ perm, const int64_t *__restrict__ rowid, int64_t f, int64_t *__restrict__ p_lu,
+                              T *__restrict__ Lout, const DevStatus *st)
+{
+    if (st->code) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int64_t i = 0; i < nrows; i++) perm[i] = (int)i;
+        for (int64_t j = 0; j < npiv && j < nrows; j++) { int p = ipiv[j]; int t = perm[j]; perm[j] = perm[p]; perm[p] = t; }
+    }
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e = tid; e < nrows * npiv; e += stride) Lout[e] = W[e % nrows + (e / nrows) * ld];
+    for (int64_t i = tid; i < npiv && i < nrows; i += stride) p_lu[f + i] = rowid[i];
+}
+
+// U12 rows in pivot order: U[i + c * npiv] = W[perm[i] + (npiv + c) * ld]
+template <typename T>
+__global__ void k_u12_gather(const T *__restrict__ W, int64_t ld, int64_t npiv, int64_t ncb, const int *__restrict__ perm,
+                             T *__restrict__ U, const DevStatus *st)
+{
+    if (st->code) return;
+    const int64_t total = npiv * ncb;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e % npiv, c = e / npiv;
+        U[e] = W[perm[i] + (npiv + c) * ld];
+    }
+}
+
+template <typename T> __device__ __forceinline__ T shfl_v(T v, int src);
+template <> __device__ __forceinline__ double shfl_v<double>(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+template <> __device__ __forceinline__ cplx shfl_v<cplx>(cplx v, int src)
+{
+    return cplx{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
+}
+
+// X <- L^-1 X for a unit lower w x w block (w <= 32 RPL) and every column of X (rows [0, w) of each column, ld ldx):
+// a warp per column, RPL rows per lane, the solved entries broadcast by shuffles
+template <typename T, int RPL>
+__global__ void __launch_bounds__(256) k_trsm_warp(T *__restrict__ X, int64_t ldx, int w, int64_t ncols,
+                                                   const T *__restrict__ Lb, int64_t ldl, const DevStatus *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *sL = reinterpret_cast<T *>(smem_raw);          // w x w, column-major, ld w
+    if (st->code) return;
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) sL[e] = Lb[(e % w) + (int64_t)(e / w) * ldl];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5, nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c = wid; c < ncols; c += nwarp) {
+        T *col = X + c * ldx;
+        T x[RPL];
+#pragma unroll
+        for (int q = 0; q < RPL; q++) { const int r = lane + 32 * q; x[q] = r < w ? col[r] : VT<T>::zero(); }
+        for (int i = 0; i < w; i++) {
+            const T xi = shfl_v<T>(x[i >> 5], i & 31);
+#pragma unroll
+            for (int q = 0; q < RPL; q++) {
+                const int r = lane + 32 * q;
+                if (r > i && r < w) x[q] = sub(x[q], mul(sL[r + i * w], xi));
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < RPL; q++) { const int r = lane + 32 * q; if (r < w) col[r] = x[q]; }
+    }
 }
 
 // =====================================================================================================================
@@ -487,6 +660,28 @@ __global__ void k_gather_rows(T *__restrict__ Y, const T *__restrict__ Wr, const
     }
 }
 
+// forward sweep with L through one front in shared memory (one CTA): gather the front's rows of the right-hand sides,
+// eliminate column by column, scatter back
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwdL_smem(const T *__restrict__ L, int64_t nrows, int64_t npiv,
+                                                   const int64_t *__restrict__ rowid, T *__restrict__ Wr, int64_t n, int64_t nrhs)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *v = reinterpret_cast<T *>(smem_raw);           // nrows x nrhs
+    for (int64_t e = threadIdx.x; e < nrows * nrhs; e += blockDim.x) v[e] = Wr[rowid[e % nrows] + (e / nrows) * n];
+    __syncthreads();
+    for (int64_t i = 0; i < npiv && i < nrows; i++) {
+        const int64_t m = nrows - i - 1;
+        for (int64_t e = threadIdx.x; e < m * nrhs; e += blockDim.x) {
+            const int64_t rr = i + 1 + e % m, r = e / m;
+            const T xi = v[i + r * nrows];
+            v[rr + r * nrows] = sub(v[rr + r * nrows], mul(L[rr + i * nrows], xi));
+        }
+        __syncthreads();
+    }
+    for (int64_t e = threadIdx.x; e < nrows * nrhs; e += blockDim.x) Wr[rowid[e % nrows] + (e / nrows) * n] = v[e];
+}
+
 // forward sweep with L through one front (one CTA), in row space: for each pivot column i, the rows below it lose
 // L[row, i] times the pivot row's value
 template <typename T>
@@ -505,18 +700,32 @@ __global__ void __launch_bounds__(256) k_fwdL(const T *__restrict__ L, int64_t n
     }
 }
 
-// backward sweep with U, step 1: partial sums of U12 x_cb over column chunks: part[chunk][i + r * npiv]
+// backward sweep with U, step 1: partial sums of U12 x_cb over column chunks, part[chunk][i + r * npiv]; lanes over the
+// pivot rows (coalesced reads of each U12 column), warps over the chunk's columns, a shared-memory reduction per chunk
 template <typename T>
 __global__ void __launch_bounds__(256) k_u12_gemv(const T *__restrict__ U12, int64_t npiv, int64_t ncb,
                                                   const int64_t *__restrict__ cbcols, const T *__restrict__ X, int64_t n,
                                                   int64_t nrhs, int64_t chunk, T *__restrict__ part)
 {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *red = reinterpret_cast<T *>(smem_raw);         // (blockDim / 32) x npiv
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int64_t c0 = blockIdx.x * chunk, c1 = c0 + chunk < ncb ? c0 + chunk : ncb;
-    for (int64_t e = threadIdx.x; e < npiv * nrhs; e += blockDim.x) {
-        const int64_t i = e % npiv, r = e / npiv;
-        T s = VT<T>::zero();
-        for (int64_t c = c0; c < c1; c++) s = add(s, mul(U12[i + c * npiv], X[cbcols[c] + r * n]));
-        part[blockIdx.x * npiv * nrhs + e] = s;
+    for (int64_t r = 0; r < nrhs; r++) {
+        for (int64_t i0 = 0; i0 < npiv; i0 += 32) {
+            const int64_t i = i0 + lane;
+            T acc = VT<T>::zero();
+            if (i < npiv)
+                for (int64_t c = c0 + warp; c < c1; c += nw) acc = add(acc, mul(U12[i + c * npiv], X[cbcols[c] + r * n]));
+            if (i < npiv) red[warp * npiv + i] = acc;
+        }
+        __syncthreads();
+        for (int64_t i = threadIdx.x; i < npiv; i += blockDim.x) {
+            T s = VT<T>::zero();
+            for (int q = 0; q < nw; q++) s = add(s, red[q * npiv + i]);
+            part[blockIdx.x * npiv * nrhs + i + r * npiv] = s;
+        }
+        __syncthreads();
     }
 }
 
@@ -651,9 +860,21 @@ __global__ void k_check_finite(const double *__restrict__ d, int64_t m, DevStatu
         }
 }
 
-__global__ void k_pinv(const int64_t *__restrict__ p_lu, int64_t *__restrict__ pinv, int64_t n)
+// a front with fewer rows than pivot columns: no pivot for step `step` (unless an earlier failure is recorded)
+__global__ void k_set_singular(DevStatus *st, int64_t step)
 {
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) pinv[p_lu[k]] = k;
+    set_status(st, ST_SINGULAR, step, 0.0, 0.0);
+}
+
+// the inverse pivot order; nothing when the factorization stopped (p_lu is then incomplete), and indices outside [0, n)
+// are never written
+__global__ void k_pinv(const int64_t *__restrict__ p_lu, int64_t *__restrict__ pinv, int64_t n, const DevStatus *st)
+{
+    if (st->code) return;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = p_lu[k];
+        if (r >= 0 && r < n) pinv[r] = k;
+    }
 }
 
 }  // namespace fpl

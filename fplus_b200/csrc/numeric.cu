@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstring>
 #include <cmath>
+#include <mutex>
 
 namespace fpl {
 
@@ -55,12 +56,38 @@ DevNum::~DevNum()
 {
     if (device >= 0) cudaSetDevice(device);
     for (void *p : {(void *)Ax, (void *)Bx, (void *)Drp, (void *)Dcp, (void *)colmax, (void *)Larena, (void *)Uarena,
-                    (void *)cbstack, (void *)work, (void *)rowid, (void *)p_lu, (void *)pinv, (void *)ipiv, (void *)st,
-                    (void *)scratch, (void *)rbuf, (void *)sbuf, (void *)xbuf, (void *)part})
-        if (p) cudaFree(p);
+                    (void *)cbstack, (void *)work, (void *)rowid, (void *)p_lu, (void *)pinv, (void *)ipiv, (void *)perm,
+                    (void *)st, (void *)scratch, (void *)rbuf, (void *)sbuf, (void *)xbuf, (void *)part})
+        if (p) cudaFreeAsync(p, stream);
+    if (stream) cudaStreamSynchronize(stream);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream && stream_owned) cudaStreamDestroy(stream);
+}
+
+// stream-ordered allocation from the device's default pool, which keeps freed memory for reuse (release threshold: no
+// limit), so a refactorization of the same size allocates nothing new
+static int pool_init(int dev, char *err, size_t errlen)
+{
+    static std::mutex mu;
+    static int done[64] = {0};
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 0 || dev >= 64 || done[dev]) return FPLUS_OK;
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t thr = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    done[dev] = 1;
+    return FPLUS_OK;
+}
+
+int ensure_async(DevNum &N, void **p, size_t *cap, size_t bytes, char *err, size_t errlen)
+{
+    if (*cap >= bytes && *p) return FPLUS_OK;
+    if (*p) { CK(cudaFreeAsync(*p, N.stream)); *p = nullptr; *cap = 0; }
+    CK(cudaMallocAsync(p, bytes > 0 ? bytes : 16, N.stream));
+    *cap = bytes;
+    return FPLUS_OK;
 }
 
 static int ensure(void **p, size_t *cap, size_t bytes, char *err, size_t errlen)
@@ -77,19 +104,22 @@ int dev_num_init(DevNum &N, int64_t n, int64_t nnz, int cplx, char *err, size_t 
     N.n = n; N.nnz = nnz; N.cplx = cplx;
     N.vs = cplx ? 16 : 8;
     CK(cudaGetDevice(&N.device));
-    CK(cudaStreamCreateWithFlags(&N.stream, cudaStreamNonBlocking));
+    int rc = pool_init(N.device, err, errlen);
+    if (rc) return rc;
+    if (!N.stream) { CK(cudaStreamCreateWithFlags(&N.stream, cudaStreamNonBlocking)); N.stream_owned = true; }
     CK(cudaEventCreate(&N.ev0));
     CK(cudaEventCreate(&N.ev1));
     const size_t nn = (size_t)(n > 0 ? n : 1), nz = (size_t)(nnz > 0 ? nnz : 1);
-    CK(cudaMalloc((void **)&N.Ax, nz * N.vs));
-    CK(cudaMalloc((void **)&N.Bx, nz * N.vs));
-    CK(cudaMalloc((void **)&N.Drp, nn * 8));
-    CK(cudaMalloc((void **)&N.Dcp, nn * 8));
-    CK(cudaMalloc((void **)&N.colmax, nn * 8));
-    CK(cudaMalloc((void **)&N.p_lu, nn * 8));
-    CK(cudaMalloc((void **)&N.pinv, nn * 8));
-    CK(cudaMalloc((void **)&N.st, sizeof(DevStatus)));
-    CK(cudaMalloc((void **)&N.scratch, 2 * nn * 8));
+    cudaStream_t s = N.stream;
+    CK(cudaMallocAsync((void **)&N.Ax, nz * N.vs, s));
+    CK(cudaMallocAsync((void **)&N.Bx, nz * N.vs, s));
+    CK(cudaMallocAsync((void **)&N.Drp, nn * 8, s));
+    CK(cudaMallocAsync((void **)&N.Dcp, nn * 8, s));
+    CK(cudaMallocAsync((void **)&N.colmax, nn * 8, s));
+    CK(cudaMallocAsync((void **)&N.p_lu, nn * 8, s));
+    CK(cudaMallocAsync((void **)&N.pinv, nn * 8, s));
+    CK(cudaMallocAsync((void **)&N.st, sizeof(DevStatus), s));
+    CK(cudaMallocAsync((void **)&N.scratch, 2 * nn * 8, s));
     return FPLUS_OK;
 }
 
@@ -176,6 +206,9 @@ static int run_equil(const DevPlan &D, DevNum &N, int equilibrate, int max_iter,
 
 // ---------------------------------------------------------------------------------------------------------------------
 // the fronts, in order.  Returns FPLUS_OK, or ST_BORDER through *border_front (>= 0) for a restart with a dense chain.
+static size_t front_lu_smem(int64_t nrows, int64_t npiv, int64_t vs) { return (size_t)(nrows * npiv * vs + nrows * (vs + 16)); }
+static const size_t SMEM_MAX = 220 * 1024;   // dynamic shared memory opt-in, below the 227 KB per-block limit (static smem on top)
+
 template <typename T>
 static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pivot_rel, int64_t *border_front,
                       char *err, size_t errlen)
@@ -184,23 +217,31 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     const int64_t vs = N.vs;
     int rc;
     *border_front = -1;
-    if ((rc = ensure((void **)&N.Larena, &N.cap_L, (size_t)P.L_size * vs, err, errlen))) return rc;
-    if ((rc = ensure((void **)&N.Uarena, &N.cap_U, (size_t)P.U_size * vs, err, errlen))) return rc;
-    if ((rc = ensure((void **)&N.cbstack, &N.cap_cb, (size_t)P.cb_size * vs, err, errlen))) return rc;
-    if ((rc = ensure((void **)&N.work, &N.cap_work, (size_t)P.work_size * vs, err, errlen))) return rc;
-    if ((rc = ensure((void **)&N.rowid, &N.cap_rowid, (size_t)P.rows_total * 8, err, errlen))) return rc;
-    if ((rc = ensure((void **)&N.ipiv, &N.cap_ipiv, (size_t)(N.n > 0 ? N.n : 1) * 4, err, errlen))) return rc;
-    DevStatus h0;
-    std::memset(&h0, 0, sizeof(h0));
-    CK(cudaMemcpyAsync(N.st, &h0, sizeof(h0), cudaMemcpyHostToDevice, s));
+    if ((rc = ensure_async(N, (void **)&N.Larena, &N.cap_L, (size_t)P.L_size * vs, err, errlen))) return rc;
+    if ((rc = ensure_async(N, (void **)&N.Uarena, &N.cap_U, (size_t)P.U_size * vs, err, errlen))) return rc;
+    if ((rc = ensure_async(N, (void **)&N.cbstack, &N.cap_cb, (size_t)P.cb_size * vs, err, errlen))) return rc;
+    if ((rc = ensure_async(N, (void **)&N.work, &N.cap_work, (size_t)P.work_size * vs, err, errlen))) return rc;
+    if ((rc = ensure_async(N, (void **)&N.rowid, &N.cap_rowid, (size_t)P.rows_total * 8, err, errlen))) return rc;
+    if ((rc = ensure_async(N, (void **)&N.ipiv, &N.cap_ipiv, (size_t)(N.n > 0 ? N.n : 1) * 4, err, errlen))) return rc;
+    if ((rc = ensure_async(N, (void **)&N.perm, &N.cap_perm, (size_t)(P.max_nrows > 0 ? P.max_nrows : 1) * 4, err, errlen))) return rc;
+    static thread_local int attr_set = 0;
+    if (!attr_set) {
+        CK(cudaFuncSetAttribute(k_front_lu<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_trsm_warp<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_trsm_warp<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        attr_set = 1;
+    }
+    if ((rc = dev_clear_status(N, err, errlen))) return rc;
     T *W = (T *)N.work, *La = (T *)N.Larena, *Ua = (T *)N.Uarena, *CB = (T *)N.cbstack;
     const T *Bx = (const T *)N.Bx;
-    constexpr int PW = 32;       // panel width
+    constexpr int PW = 32;       // panel width of the blocked path
+    const int TB = VT<T>::cplx_ ? 32 : 64;    // rows per TRSM block of U12
     const int64_t nf = (int64_t)P.fronts.size();
     for (int64_t fi = 0; fi < nf; fi++) {
         const Front &F = P.fronts[fi];
         const int64_t nr = F.nrows, nc = F.ncols, np = F.npiv, ncb = nc - np;
         const int64_t ld = nr;
+        T *Lf = La + F.L_off;
         if (nr * nc > 0) CK(cudaMemsetAsync(W, 0, (size_t)(nr * nc) * vs, s));
         {
             const int64_t cnt = F.asm_end - F.asm_begin;
@@ -216,14 +257,24 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
                                                                             F.tau_base, D.relcol + G.relcol_off,
                                                                             N.rowid + F.row_off, N.rowid + G.row_off + G.npiv, N.st);
         }
-        if (np > 0 && nr > 0) {
+        if (np == 0) continue;
+        if (nr == 0) { k_set_singular<<<1, 1, 0, s>>>(N.st, F.f); continue; }     // no row can take pivot step f
+        // the pivot block: partial-pivot LU, L\U into the arena in the final row order, the order into N.perm
+        const size_t sm = front_lu_smem(nr, np, vs);
+        if (sm <= SMEM_MAX) {
+            const int R = (int)((nr + 31) & ~31);
+            int nt = R;
+            while (nt * 2 <= 1024 && nt * 2 <= R * std::max<int64_t>(1, np / 8)) nt *= 2;
+            if (nt > 1024) nt = 1024;
+            if (nt < 64) nt = 64;
+            k_front_lu<T><<<1, nt, sm, s>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel, N.rowid + F.row_off, Lf,
+                                           N.perm, N.p_lu, N.st, fi);
+        } else {
             const int64_t npr = std::min(np, nr);
-            // left part: blocked partial-pivot LU of the nrows x npiv pivot block
             for (int64_t k0 = 0; k0 < npr; k0 += PW) {
                 const int w = (int)std::min<int64_t>(PW, npr - k0);
                 k_panel<T><<<1, 512, 0, s>>>(W, ld, nr, F.nri, (int)k0, w, F.f, N.colmax, pivot_rel, N.rowid + F.row_off,
                                             N.ipiv + F.f, N.st, fi);
-                // the swaps on the pivot block's other columns
                 if (k0 > 0) k_laswp<T><<<nblk(k0, 128), 128, 0, s>>>(W, ld, N.ipiv + F.f, (int)k0, w, 0, k0, N.st);
                 if (k0 + w < np) {
                     k_laswp<T><<<nblk(np - k0 - w, 128), 128, 0, s>>>(W, ld, N.ipiv + F.f, (int)k0, w, k0 + w, np, N.st);
@@ -231,37 +282,45 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
                     const int64_t M = nr - k0 - w, Nn = np - k0 - w;
                     if (M > 0) {
                         dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((Nn + GBN - 1) / GBN));
+                        T *C = W + (k0 + w) + (k0 + w) * ld;
                         k_gemm_sub<T><<<g, 256, 0, s>>>(M, Nn, w, W + (k0 + w) + k0 * ld, ld, W + k0 + (k0 + w) * ld, ld,
-                                                        W + (k0 + w) + (k0 + w) * ld, ld, N.st);
+                                                        C, ld, nullptr, C, ld, N.st);
                     }
                 }
             }
-            if (ncb > 0) {
-                // right part: the swaps, U12 = L11^-1 A12 (blocked), then the Schur complement CB -= L21 U12
-                k_laswp<T><<<nblk(ncb, 128), 128, 0, s>>>(W, ld, N.ipiv + F.f, 0, (int)npr, np, nc, N.st);
-                for (int64_t k0 = 0; k0 < npr; k0 += PW) {
-                    const int w = (int)std::min<int64_t>(PW, npr - k0);
-                    k_trsm_unit<T><<<nblk(ncb, 128), 128, 0, s>>>(W, ld, (int)k0, w, np, nc, N.st);
-                    const int64_t M = npr - k0 - w;
-                    if (M > 0) {
-                        dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((ncb + GBN - 1) / GBN));
-                        k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, w, W + (k0 + w) + k0 * ld, ld, W + k0 + np * ld, ld,
-                                                        W + (k0 + w) + np * ld, ld, N.st);
-                    }
-                }
-                const int64_t M = nr - np;
-                if (M > 0) {
-                    dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((ncb + GBN - 1) / GBN));
-                    k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, np, W + np, ld, W + np * ld, ld, W + np + np * ld, ld, N.st);
-                }
+            k_left_finish<T><<<nblk(nr * np), 256, 0, s>>>(W, ld, nr, np, N.ipiv + F.f, N.perm, N.rowid + F.row_off, F.f, N.p_lu,
+                                                          Lf, N.st);
+        }
+        if (nr < np) k_set_singular<<<1, 1, 0, s>>>(N.st, F.f + nr);
+        if (ncb == 0) continue;
+        // U12 = L11^-1 A12[perm]: gather the pivot rows into the arena, then blocked TRSM in place
+        T *Uf = Ua + F.U_off;
+        k_u12_gather<T><<<nblk(np * ncb), 256, 0, s>>>(W, ld, np, ncb, N.perm, Uf, N.st);
+        const int64_t npr = std::min(np, nr);
+        for (int64_t k0 = 0; k0 < npr; k0 += TB) {
+            const int w = (int)std::min<int64_t>(TB, npr - k0);
+            const size_t tsm = (size_t)w * w * vs;
+            const int nwarps = (int)std::min<int64_t>(ncb, 148 * 64);
+            const int blocks = (nwarps + 7) / 8;
+            if (w <= 32) k_trsm_warp<T, 1><<<blocks, 256, tsm, s>>>(Uf + k0, np, w, ncb, Lf + k0 + k0 * ld, ld, N.st);
+            else k_trsm_warp<T, 2><<<blocks, 256, tsm, s>>>(Uf + k0, np, w, ncb, Lf + k0 + k0 * ld, ld, N.st);
+            const int64_t M = npr - k0 - w;
+            if (M > 0) {
+                dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((ncb + GBN - 1) / GBN));
+                T *C = Uf + k0 + w;
+                k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, w, Lf + (k0 + w) + k0 * ld, ld, Uf + k0, np, C, np, nullptr, C, np, N.st);
             }
         }
-        k_copyout<T><<<nblk(std::max(nr * np, std::max(np * ncb, std::max<int64_t>(0, nr - np) * ncb))), 256, 0, s>>>(
-            W, nr, nc, np, La + F.L_off, Ua + F.U_off, CB + F.cb_off, N.rowid + F.row_off, F.f, N.p_lu, N.st);
+        // the Schur complement into the CB stack: CB = A22[perm] - L21 U12
+        const int64_t M = nr - np;
+        if (M > 0) {
+            dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((ncb + GBN - 1) / GBN));
+            k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, np, Lf + np, ld, Uf, np, W + np * ld, ld, N.perm + np, CB + F.cb_off, M, N.st);
+        }
         if ((fi & 255) == 255) CK(cudaGetLastError());
     }
     CK(cudaGetLastError());
-    k_pinv<<<nblk(N.n), 256, 0, s>>>(N.p_lu, N.pinv, N.n);
+    k_pinv<<<nblk(N.n), 256, 0, s>>>(N.p_lu, N.pinv, N.n, N.st);
     DevStatus h;
     CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -296,16 +355,21 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
     const int64_t n = N.n;
     int rc;
     const size_t nb = (size_t)(n > 0 ? n : 1) * (size_t)nrhs * sizeof(T);
-    if ((rc = ensure((void **)&N.rbuf, &N.cap_r, nb, err, errlen))) return rc;
-    if ((rc = ensure((void **)&N.sbuf, &N.cap_s, nb, err, errlen))) return rc;
-    const int64_t chunk = 256;
+    if ((rc = ensure_async(N, (void **)&N.rbuf, &N.cap_r, nb, err, errlen))) return rc;
+    if ((rc = ensure_async(N, (void **)&N.sbuf, &N.cap_s, nb, err, errlen))) return rc;
+    auto chunk_of = [](int64_t ncb) { int64_t c = (ncb + 295) / 296; return c < 32 ? (int64_t)32 : c; };
     int64_t maxpart = 1;
-    for (const Front &F : P.fronts) maxpart = std::max(maxpart, ((F.ncols - F.npiv + chunk - 1) / chunk) * F.npiv);
-    if ((rc = ensure((void **)&N.part, &N.cap_part, (size_t)maxpart * (size_t)nrhs * sizeof(T), err, errlen))) return rc;
+    for (const Front &F : P.fronts) {
+        const int64_t ncb = F.ncols - F.npiv;
+        if (ncb > 0) maxpart = std::max(maxpart, ((ncb + chunk_of(ncb) - 1) / chunk_of(ncb)) * F.npiv);
+    }
+    if ((rc = ensure_async(N, (void **)&N.part, &N.cap_part, (size_t)maxpart * (size_t)nrhs * sizeof(T), err, errlen))) return rc;
     T *R = (T *)N.rbuf, *S2 = (T *)N.sbuf, *part = (T *)N.part;
     const T *La = (const T *)N.Larena, *Ua = (const T *)N.Uarena;
     const int64_t nf = (int64_t)P.fronts.size();
     const size_t smem = (size_t)P.max_npiv * (size_t)nrhs * sizeof(T);
+    CK(cudaFuncSetAttribute(k_fwdL_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    CK(cudaFuncSetAttribute(k_u12_gemv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
     if (smem > 48 * 1024) {
         CK(cudaFuncSetAttribute(k_bwdU<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         CK(cudaFuncSetAttribute(k_bwdLt<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -317,7 +381,11 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
         for (int64_t fi = 0; fi < nf; fi++) {
             const Front &F = P.fronts[fi];
             if (F.npiv == 0 || F.nrows == 0) continue;
-            k_fwdL<T><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs);
+            const size_t fsm = (size_t)F.nrows * nrhs * sizeof(T);
+            if (fsm <= 96 * 1024)
+                k_fwdL_smem<T><<<1, 256, fsm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs);
+            else
+                k_fwdL<T><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs);
         }
         k_gather_rows<T><<<nblk(n * nrhs), 256, 0, s>>>(S2, R, N.p_lu, n, nrhs);
         for (int64_t fi = nf - 1; fi >= 0; fi--) {
@@ -326,9 +394,10 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
             if (F.npiv == 0) continue;
             int64_t nchunk = 0;
             if (ncb > 0) {
+                const int64_t chunk = chunk_of(ncb);
                 nchunk = (ncb + chunk - 1) / chunk;
-                k_u12_gemv<T><<<(unsigned)nchunk, 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, R, n, nrhs,
-                                                               chunk, part);
+                k_u12_gemv<T><<<(unsigned)nchunk, 256, (size_t)8 * F.npiv * sizeof(T), s>>>(
+                    Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, R, n, nrhs, chunk, part);
             }
             k_bwdU<T><<<1, 256, (size_t)F.npiv * nrhs * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, part, nchunk, S2, R,
                                                                          n, nrhs, N.st);
@@ -390,7 +459,7 @@ int dev_clear_status(DevNum &N, char *err, size_t errlen)
 
 int dev_ensure_x(DevNum &N, size_t bytes, char *err, size_t errlen)
 {
-    return ensure((void **)&N.xbuf, &N.cap_x, bytes, err, errlen);
+    return ensure_async(N, (void **)&N.xbuf, &N.cap_x, bytes, err, errlen);
 }
 
 int dev_check_finite(DevNum &N, char *err, size_t errlen)

@@ -27,14 +27,15 @@ struct DevNum {
     int cplx = 0;
     int64_t vs = 8;
     cudaStream_t stream = nullptr;
-    bool stream_owned = true;
+    bool stream_owned = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     void *Ax = nullptr, *Bx = nullptr;
     double *Drp = nullptr, *Dcp = nullptr, *colmax = nullptr;
     void *Larena = nullptr, *Uarena = nullptr, *cbstack = nullptr, *work = nullptr;
     size_t cap_L = 0, cap_U = 0, cap_cb = 0, cap_work = 0, cap_rowid = 0, cap_ipiv = 0;
     int64_t *rowid = nullptr, *p_lu = nullptr, *pinv = nullptr;
-    int *ipiv = nullptr;
+    int *ipiv = nullptr, *perm = nullptr;
+    size_t cap_perm = 0;
     DevStatus *st = nullptr;
     void *scratch = nullptr;
     void *rbuf = nullptr, *sbuf = nullptr, *xbuf = nullptr, *part = nullptr;
@@ -53,5 +54,6 @@ int dev_status(DevNum &N, int *code, int64_t *idx, char *err, size_t errlen);
 int dev_clear_status(DevNum &N, char *err, size_t errlen);
 int dev_check_finite(DevNum &N, char *err, size_t errlen);
 int dev_ensure_x(DevNum &N, size_t bytes, char *err, size_t errlen);
+int ensure_async(DevNum &N, void **p, size_t *cap, size_t bytes, char *err, size_t errlen);
 
 }  // namespace fpl

@@ -1,0 +1,141 @@
+"""Parity of the CUDA path (libfplus.so, through the fplus.h C-ABI) with the oracle on the same inputs and orders.
+
+The bar (factor+solve contract): identical pivots; Ruiz scalings Dr, Dc bit-identical; L and U within 1e-12 normwise of
+the oracle's; backward error of the solves at most 1e-14 (1e-13 for the 12-decade-scaled test matrices, whose
+conditioning the reference's own tests grant 1e-12).
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import fplus_b200 as F
+import oracle as O
+from tests.cases import CASES
+
+pytestmark = pytest.mark.gpu
+
+FACTOR_TOL = 1e-12
+
+
+def _rel(A, B):
+    nb = sp.linalg.norm(B)
+    return sp.linalg.norm(A - B) / (nb if nb > 0 else 1.0)
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    import torch
+    assert torch.cuda.is_available(), "the GPU tests need a CUDA device"
+    torch.cuda.init()
+    return torch.device("cuda:0")
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_factor_matches_oracle(gpu, name):
+    n, Ap, Ai, Ax = CASES[name]()
+    S = F.analyze(n, Ap, Ai)
+    N = S.factor(Ax)
+    orc = O.OracleLU(n, Ap, Ai, Ax, S.row_perm, S.col_perm)
+    assert np.array_equal(N.p, orc.p), "pivot order differs from the oracle"
+    assert np.array_equal(N.q, orc.q)
+    assert np.array_equal(N.Dr, orc.Dr) and np.array_equal(N.Dc, orc.Dc), "Ruiz scalings are not bit-identical"
+    L, U, p_lu = N.factors()
+    assert np.array_equal(p_lu, orc.p_lu)
+    assert _rel(L, orc.L) <= FACTOR_TOL, f"L differs by {_rel(L, orc.L):.2e}"
+    assert _rel(U, orc.U) <= FACTOR_TOL, f"U differs by {_rel(U, orc.U):.2e}"
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_solve_backward_error(gpu, name):
+    n, Ap, Ai, Ax = CASES[name]()
+    cplx = np.iscomplexobj(Ax)
+    S = F.analyze(n, Ap, Ai)
+    N = S.factor(Ax)
+    orc = O.OracleLU(n, Ap, Ai, Ax, S.row_perm, S.col_perm)
+    rng = np.random.default_rng(7)
+    nrhs = 3
+    B = rng.standard_normal((n, nrhs)) + (1j * rng.standard_normal((n, nrhs)) if cplx else 0)
+    tol = 1e-13 if name.startswith("hard") else 1e-14
+    for trans in ((0, 1, 2) if cplx else (0, 1)):
+        X = N.solve(B, trans)
+        Xo = orc.solve(B, trans)
+        for r in range(nrhs):
+            be = O.backward_error(n, Ap, Ai, Ax, X[:, r], B[:, r], trans)
+            assert be <= tol, f"trans {trans} rhs {r}: backward error {be:.2e}"
+        d = np.linalg.norm(X - Xo) / np.linalg.norm(Xo)
+        assert d < 1e-8, f"trans {trans}: differs from the oracle's solve by {d:.1e}"
+
+
+def test_dense_row_pivot_restarts_with_chain(gpu):
+    """A dense row chosen as pivot inside the interior fronts: the factorization is redone with the dense chain from that
+    front and the pivots still match the oracle."""
+    n, Ap, Ai, Ax = CASES["pencil_1x64"]()
+    S = F.analyze(n, Ap, Ai)
+    N = S.factor(Ax)
+    info = N.info
+    assert info["attempts"] == 2 and info["f_dense"] < n - S.n_dense_cols
+    N2 = S.factor(Ax * (1 + 0.25j))          # the same pattern again: the chain start is remembered
+    assert N2.info["attempts"] == 1
+    orc = O.OracleLU(n, Ap, Ai, Ax * (1 + 0.25j), S.row_perm, S.col_perm)
+    assert np.array_equal(N2.p, orc.p)
+
+
+def test_several_rhs_and_leading_dimension(gpu):
+    n, Ap, Ai, Ax = CASES["banded_cplx_1200"]()
+    S = F.analyze(n, Ap, Ai)
+    N = S.factor(Ax)
+    rng = np.random.default_rng(3)
+    nrhs, ldb = 37, n + 5                      # more than one group of 32, padded leading dimension
+    Bfull = rng.standard_normal((ldb, nrhs)) + 1j * rng.standard_normal((ldb, nrhs))
+    B = np.asfortranarray(Bfull.copy())
+    import ctypes
+    err = ctypes.create_string_buffer(256)
+    rc = F.lib().fplus_solve(N._h, B.ctypes.data_as(ctypes.c_void_p), nrhs, ldb, 0, err, 256)
+    assert rc == 0, err.value
+    X1 = N.solve(Bfull[:n, :], 0)
+    assert np.array_equal(B[:n, :], X1), "solving with ldb > n changed the result"
+    assert np.array_equal(B[n:, :], Bfull[n:, :]), "rows beyond n were written"
+    cols = np.column_stack([N.solve(Bfull[:n, k], 0) for k in range(nrhs)])
+    assert np.allclose(cols, X1, rtol=0, atol=1e-12 * np.abs(X1).max())
+
+
+def test_singular_matrix_reports_singular(gpu):
+    # [[1, 1], [1, 1]]: an exact LU fails (tests/c/test_fplus.c:226-228)
+    Ap = np.array([0, 2, 4]); Ai = np.array([0, 1, 0, 1]); Ax = np.array([1.0, 1.0, 1.0, 1.0])
+    S = F.analyze(2, Ap, Ai, pin_dense=0, equilibrate=0)
+    with pytest.raises(F.FplusError) as e:
+        S.factor(Ax)
+    assert e.value.code == F.FPLUS_ERR_SINGULAR
+
+
+def test_zero_row_reported_by_equilibration(gpu):
+    # a structurally present but numerically zero row: Ruiz reports it (FPLUS src/equil.c:276-284)
+    Ap = np.array([0, 2, 4]); Ai = np.array([0, 1, 0, 1]); Ax = np.array([1.0, 0.0, 2.0, 0.0])
+    S = F.analyze(2, Ap, Ai)
+    with pytest.raises(F.FplusError) as e:
+        S.factor(Ax)
+    assert e.value.code == F.FPLUS_ERR_SINGULAR and "Row 1" in str(e.value)
+
+
+def test_example_program_values(gpu):
+    """The reference's example (examples/solve.c): x = (1, 1, 1) for A and A^H."""
+    Ap = np.array([0, 2, 5, 7]); Ai = np.array([0, 1, 0, 1, 2, 1, 2])
+    Ax = np.array([4, 1j, 1, 3, 2, 1, 5], dtype=complex)
+    S = F.analyze(3, Ap, Ai)
+    N = S.factor(Ax)
+    assert np.allclose(N.solve(np.array([5, 4 + 1j, 7]), 0), 1.0, atol=1e-14)
+    assert np.allclose(N.solve(np.array([4 - 1j, 6, 6]), 2), 1.0, atol=1e-14)
+
+
+def test_device_resident_entry_points(gpu):
+    import torch
+    n, Ap, Ai, Ax = CASES["convdiff2d_g20"]()
+    S = F.analyze(n, Ap, Ai)
+    Ad = torch.from_numpy(Ax).to(gpu)
+    Nd = S.factor(Ad, device=True)
+    Nh = S.factor(Ax)
+    assert np.array_equal(Nd.p, Nh.p)
+    b = np.random.default_rng(5).standard_normal(n)
+    bd = torch.from_numpy(b.copy()).to(gpu)
+    Nd.solve_device(bd, 0)
+    assert np.array_equal(bd.cpu().numpy(), Nh.solve(b, 0))
