@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Factor + solve benchmark of the FPLUS path on B200 (one JSON line on stdout, rank 0).
+
+Workload (default ``pencil``): the shift-invert pencil A - sigma B, complex128, 8 Fourier modes x 4 fields x 1024
+Chebyshev modes (n = 32,768), banded blocks of half-bandwidth 6, 8 dense tau rows and 8 dense tau columns over all n,
+magnitudes log-uniform in [1e-6, 1e6] with seeded phases, sigma = 0.3 + 1.7i; b ~ N(0, 1) complex, nrhs 1.  ``--workload
+convdiff2d`` runs the 100 x 100 convection-diffusion stencil (n = 10,000, real) instead.  Synthetic, seeded.
+
+One step = fplus_factor (permutation, Ruiz, the multifrontal LU) + fplus_solve on one matrix, the symbolic analysis
+(fplus_analyze_opts: done once per pattern, reported as analyze_ms) reused across steps.  The metric is milliseconds
+per step with the solution at backward error <= 1e-14 (checked after the timed steps; lower is better).
+
+* value -- device-timed (CUDA events on the stream the library runs on) with the matrix and right-hand side resident in
+  HBM (fplus_b200_factor_dev / fplus_b200_solve_dev); L2 flushed (a 512 MiB write) between steps, outside the events.
+* e2e   -- the same step through the public fplus_factor / fplus_solve with pinned host buffers: the host-to-device copy
+  of the values and the right-hand side and the device-to-host copy of the solution are inside the timed region.
+* roofline -- the dominant kernel class of the factorization, from a separate step with the library's per-class CUDA
+  event timing on: achieved algorithmic rate / measured peak.
+* cpu_baseline / --impl reference -- the reference's own CPU build (oracle/_ref/libfplusref.so: the FPLUS sources,
+  OpenMP + OpenBLAS, all host cores) on a bounded sample of the same generator (fewer Fourier modes), scaled to the full
+  workload by n^3 (its relaxed supernodes make this factorization dense; the sample and the factor are reported).
+
+Multi-GPU: one factorization does not shard; N ranks run N independent replicas ("replicas only"); the line reports
+the slowest rank's ms per step divided by N (the job's ms per factorization) with scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def workload(name):
+    from fplus_b200 import workloads as W
+    if name == "pencil":
+        n, Ap, Ai, Ax = W.pencil()
+        desc = {"workload": "pencil A - sigma B, 8 Fourier x 4 fields x 1024 Chebyshev (n=32768), complex128, "
+                            "half-bandwidth 6, 8 dense tau rows + 8 dense tau columns, |a| log-uniform [1e-6, 1e6], "
+                            "sigma=0.3+1.7i", "n": n, "nnz": int(Ap[-1]), "nrhs": 1}
+    elif name == "convdiff2d":
+        n, Ap, Ai, Ax = W.convdiff2d(100, 1)
+        desc = {"workload": "2D convection-diffusion 5-point, 100x100 grid (n=10000), float64", "n": n,
+                "nnz": int(Ap[-1]), "nrhs": 1}
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    b = W.rhs(n, 1, np.iscomplexobj(Ax), 2)[0]
+    return n, Ap, Ai, Ax, b, desc
+
+
+def sample_workload(name):
+    """The bounded CPU-baseline sample: the same generator, fewer Fourier modes (or the full matrix when small)."""
+    from fplus_b200 import workloads as W
+    if name == "pencil":
+        modes = int(os.environ.get("FPLUS_BENCH_REF_MODES", "1"))
+        n, Ap, Ai, Ax = W.pencil(modes=modes)
+        return n, Ap, Ai, Ax, (f"pencil generator with {modes} Fourier mode(s) (n={n}), median of 3; ms scaled by "
+                               f"(32768/{n})^3 -- an underestimate: the reference took 43x longer at 2 modes than at 1")
+    n, Ap, Ai, Ax = W.convdiff2d(100, 1)
+    return n, Ap, Ai, Ax, "the full workload"
+
+
+# ------------------------------------------------------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1])); smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------------------------- peaks
+def fp64_peak_tflops(torch, cplx):
+    """cuBLAS FP64 GEMM throughput on this GPU (the roofline of an FP64 tensor-core kernel: the driver's measured peaks
+    file covers bf16 and HBM only): complex128 (ZGEMM, 8 flops per multiply-add) or float64, 8192^3, best of 5."""
+    dt = torch.complex128 if cplx else torch.float64
+    m = 8192
+    a = torch.randn(m, m, dtype=dt, device="cuda")
+    b = torch.randn(m, m, dtype=dt, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(); torch.matmul(a, b); e1.record(); torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return (8.0 if cplx else 2.0) * m ** 3 / (best * 1e-3) / 1e12
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return json.load(open(p)), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# ------------------------------------------------------------------------------------------------------------- ranks
+def allreduce_max(value: float, device) -> float:
+    """The maximum of a per-rank value over all ranks (every rank gets it); the value itself with one rank."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------------------------------------------------- arms
+def reference_sample(workload_name, reps=1):
+    """The reference CPU build on the bounded sample: (ms per factor+solve, berr, description, threads)."""
+    import oracle as O
+    n, Ap, Ai, Ax, desc = sample_workload(workload_name)
+    import fplus_b200 as F
+    S = F.analyze(n, Ap, Ai)                       # the same static orders for both libraries
+    from fplus_b200 import workloads as W
+    b = W.rhs(n, 1, np.iscomplexobj(Ax), 2)[0]
+    trow = np.zeros(n, np.uint8); trow[S.row_perm[n - S.n_dense_rows:]] = 1
+    tcol = np.zeros(n, np.uint8); tcol[S.col_perm[n - S.n_dense_cols:]] = 1
+    # the reference's analysis with the same fill-reducing order and no postorder: col_perm as given
+    times = []
+    be = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        R = O.RefLU(n, Ap, Ai, Ax, S.col_perm, trow, tcol, postorder=0)
+        x = R.solve(b)
+        times.append((time.perf_counter() - t0) * 1e3)
+        be = O.backward_error(n, Ap, Ai, Ax, x, b)
+        assert np.array_equal(R.col_perm, S.col_perm) and np.array_equal(R.row_perm, S.row_perm)
+        del R
+    scale = (32768.0 / n) ** 3 if workload_name == "pencil" else 1.0
+    threads = os.cpu_count()
+    return float(np.median(times)) * scale, float(np.median(times)), be, desc, threads, scale
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    if not __import__("oracle").have_reference():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfplusref.so was not built (the reference "
+                                                                "sources were absent at build time)"}))
+        return
+    for _ in range(args.warmup and 1):
+        reference_sample(args.workload)
+    ms_list = []
+    for _ in range(args.steps):
+        ms_full, ms_sample, be, desc, threads, scale = reference_sample(args.workload)
+        ms_list.append(ms_full)
+    d = workload(args.workload)[5]
+    ms = float(np.mean(ms_list))
+    line = {"impl": "reference", "metric": "factor+solve ms (berr<=1e-14)", "value": ms, "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128" if args.workload == "pencil" else "f64", "data": "synthetic",
+            "config": d,
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
+                             "sample": f"{desc}; measured {ms_sample:.1f} ms per sample step; berr {be:.2e}"},
+            "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_b200_arm(args, rank, world):
+    import torch
+    import fplus_b200 as F
+    import oracle as O
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n, Ap, Ai, Ax, b, desc = workload(args.workload)
+    cplx = np.iscomplexobj(Ax)
+    t0 = time.perf_counter()
+    S = F.analyze(n, Ap, Ai)
+    analyze_ms = (time.perf_counter() - t0) * 1e3
+    stream = torch.cuda.current_stream()
+    F.lib().fplus_b200_use_stream(ctypes.c_void_p(stream.cuda_stream))
+    Ad = torch.from_numpy(Ax).to(dev)
+    bd0 = torch.from_numpy(np.ascontiguousarray(b)).to(dev)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def dev_step():
+        bd = bd0.clone()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        N = S.factor(Ad, device=True)
+        N.solve_device(bd, 0)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), N, bd
+
+    for _ in range(args.warmup):
+        _, N, _ = dev_step()
+        del N
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    L0 = F.launch_count()
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ms, N, bd = dev_step()
+            times.append(ms)
+            del N
+    torch.cuda.synchronize()
+    launches = F.launch_count() - L0
+    ms_dev = allreduce_max(float(np.mean(times)), dev)
+    x = bd.cpu().numpy()
+    berr = O.backward_error(n, Ap, Ai, Ax, x, b)
+
+    # e2e: the public host API with pinned buffers
+    Ah = torch.from_numpy(Ax).pin_memory()
+    bh = torch.from_numpy(np.ascontiguousarray(b)).pin_memory()
+    Ah_np = Ah.numpy()
+
+    def e2e_step():
+        xb = bh.clone()              # pinned, solved in place
+        xb_np = xb.numpy()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        err = ctypes.create_string_buffer(512)
+        h = ctypes.c_void_p()
+        rc = F.lib().fplus_factor(S._h, F._p64(S.Ap), F._p64(S.Ai), Ah_np.ctypes.data_as(ctypes.c_void_p), int(cplx),
+                                  ctypes.byref(S.options), ctypes.byref(h), err, 512)
+        assert rc == 0, err.value
+        rc = F.lib().fplus_solve(h, xb_np.ctypes.data_as(ctypes.c_void_p), 1, n, 0, err, 512)
+        assert rc == 0, err.value
+        e1.record(stream)
+        e1.synchronize()
+        F.lib().fplus_numeric_free(h)
+        return e0.elapsed_time(e1), xb_np
+    for _ in range(min(args.warmup, 2)):
+        e2e_step()
+    e2e_times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ms, xe = e2e_step()
+        e2e_times.append(ms)
+    ms_e2e = allreduce_max(float(np.mean(e2e_times)), dev)
+    berr_e2e = O.backward_error(n, Ap, Ai, Ax, xe, b)
+    vsz = 16 if cplx else 8
+
+    # roofline: one profiled step, the dominant class
+    F.profile(True)
+    flush.zero_()
+    _, N, _ = dev_step()
+    info = N.info
+    del N
+    prof = {F.PROFILE_CLASSES[c]: F.profile_read(c) for c in F.PROFILE_CLASSES}
+    F.profile(False)
+    dom = max(prof, key=lambda k: prof[k]["ms"])
+    peaks, psrc = measured_peaks()
+    p = prof[dom]
+    if dom == "assemble":
+        achieved = p["bytes"] / (p["ms"] * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "peak_source": f"hbm_gbs ({psrc})"}
+    else:
+        achieved = p["flops"] / (p["ms"] * 1e-3) / 1e12
+        peak = fp64_peak_tflops(torch, cplx) if rank == 0 else float("nan")
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": ("cuBLAS " + ("ZGEMM" if cplx else "DGEMM") + " 8192^3 measured in bench.py (FP64 tensor "
+                                "path; the measured-peaks file has bf16 and HBM only)")}
+    roof.update({"kernel_class": dom, "launches": p["count"], "avg_launch_us": 1e3 * p["ms"] / max(p["count"], 1),
+                 "algorithmic_per_launch": (p["flops"] if dom != "assemble" else p["bytes"]) / max(p["count"], 1),
+                 "traffic": None,
+                 "classes_ms": {k: round(v["ms"], 3) for k, v in prof.items()}})
+
+    if rank != 0:
+        return
+    clocks = clk.summary()
+    cpu = None
+    if __import__("oracle").have_reference() and world == 1 and not args.no_cpu_baseline:
+        ms_full, ms_sample, be_ref, sdesc, threads, scale = reference_sample(args.workload, reps=3)
+        cpu = {"value": ms_full, "unit": "ms", "cores": threads, "kind": "reference",
+               "sample": f"{sdesc}; measured {ms_sample:.1f} ms per factor+solve; berr {be_ref:.2e}"}
+    line = {"metric": "factor+solve ms (berr<=1e-14)", "value": ms_dev / world, "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_dev, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128" if cplx else "f64", "data": "synthetic",
+            "config": dict(desc, **{"parallelism": f"replicas{world}" if world > 1 else "1 GPU",
+                                    "l2": "flushed between steps (512 MiB write)", "analyze_ms": round(analyze_ms, 2),
+                                    "berr": berr, "berr_e2e": berr_e2e, "fronts": info["nfronts"],
+                                    "dense_chain_from": info["f_dense"], "ms_equil": round(info["ms_equil"], 3),
+                                    "ms_fronts": round(info["ms_fronts"], 3), "front_flops": info["front_flops"]}),
+            "e2e": {"value": ms_e2e / world, "unit": "ms", "h2d_bytes_per_step": int(Ap[-1]) * vsz + n * vsz,
+                    "d2h_bytes_per_step": n * vsz},
+            "gpu_launches": int(launches),
+            "clocks": clocks, "roofline": roof, "cpu_baseline": cpu}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="pencil", choices=["pencil", "convdiff2d"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1 and args.impl == "b200":
+        import datetime
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, rank, world)
+        else:
+            run_b200_arm(args, rank, world)
+    finally:
+        if world > 1 and args.impl == "b200":
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

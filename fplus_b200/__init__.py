@@ -58,7 +58,8 @@ FPLUS_H_SYMBOLS = [
 ]
 FPLUS_B200_H_SYMBOLS = [
     "fplus_b200_numeric_info", "fplus_b200_use_stream", "fplus_b200_factor_dev", "fplus_b200_solve_dev",
-    "fplus_b200_interior_order", "fplus_b200_plan_size", "fplus_b200_plan_export",
+    "fplus_b200_interior_order", "fplus_b200_plan_size", "fplus_b200_plan_export", "fplus_b200_launch_count",
+    "fplus_b200_profile", "fplus_b200_profile_read",
 ]
 
 _lib = None
@@ -108,6 +109,9 @@ def lib():
     L.fplus_b200_interior_order.argtypes = [ctypes.c_int64, _i64p, _i64p, ctypes.c_char_p, ctypes.c_char_p, _i64p]
     L.fplus_b200_plan_size.argtypes = [ctypes.c_void_p, ctypes.c_int64, _i64p, _i64p, _i64p]
     L.fplus_b200_plan_export.argtypes = [ctypes.c_void_p, ctypes.c_int64, _i64p, _i64p, _i64p, _i64p, _i64p, _i64p]
+    L.fplus_b200_launch_count.restype = ctypes.c_longlong
+    L.fplus_b200_profile.argtypes = [ctypes.c_int]
+    L.fplus_b200_profile_read.argtypes = [ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_longlong), _dp, _dp]
     _lib = L
     return L
 
@@ -278,6 +282,24 @@ def _csc(Pp, Pi, Px, n, cplx):
     if cplx:
         x = x.view(np.complex128)
     return sp.csc_matrix((x, i, p), shape=(n, n))
+
+
+PROFILE_CLASSES = {0: "schur_gemm", 1: "front_lu", 2: "u12_trsm", 3: "assemble"}
+
+
+def launch_count() -> int:
+    return int(lib().fplus_b200_launch_count())
+
+
+def profile(on: bool):
+    lib().fplus_b200_profile(1 if on else 0)
+
+
+def profile_read(cls: int):
+    ms, fl, by = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    cnt = ctypes.c_longlong()
+    _check(lib().fplus_b200_profile_read(cls, ctypes.byref(ms), ctypes.byref(cnt), ctypes.byref(fl), ctypes.byref(by)), None)
+    return dict(ms=ms.value, count=cnt.value, flops=fl.value, bytes=by.value)
 
 
 def analyze(n, Ap, Ai, options=None, **kw) -> Symbolic:

@@ -394,3 +394,18 @@ extern "C" int fplus_b200_plan_export(const fplus_symbolic *sym, int64_t tail, i
     if (cols) std::memcpy(cols, P.cols.data(), P.cols.size() * 8);
     return FPLUS_OK;
 }
+
+extern "C" long long fplus_b200_launch_count(void) { return launch_count(); }
+
+extern "C" void fplus_b200_profile(int on) { prof_enable(on); }
+
+extern "C" int fplus_b200_profile_read(int cls, double *ms, long long *count, double *flops, double *bytes)
+{
+    if (cls < 0 || cls >= PROF_NCLASS) return FPLUS_ERR_BADARG;
+    ProfClass c = prof_read(cls);
+    if (ms) *ms = c.ms;
+    if (count) *count = c.count;
+    if (flops) *flops = c.flops;
+    if (bytes) *bytes = c.bytes;
+    return FPLUS_OK;
+}

@@ -476,6 +476,7 @@ __global__ void __launch_bounds__(1024) k_front_lu(const T *__restrict__ W, int6
     const int G = nt >= R ? nt / R : 1;                            // column groups per row
     const int rstep = nt >= R ? R : nt;                            // row stride of a thread
     const int my_i = nt >= R ? tid % R : tid, my_g = nt >= R ? tid / R : 0;
+    const bool upd = my_g < G;                                     // threads beyond G whole row groups only search
     if (tid == 0) s_stop = st->code != 0;
     for (int64_t e = tid; e < (int64_t)npiv * nrows; e += nt) {
         const int i = (int)(e % nrows), c = (int)(e / nrows);
@@ -488,10 +489,11 @@ __global__ void __launch_bounds__(1024) k_front_lu(const T *__restrict__ W, int6
     for (int j = 0; j < steps; j++) {
         // argmax over the rows not pivoted before step j (tag >= j; tid 0 tags this step's pivot during the step, which
         // keeps it a candidate for the warps still searching), the same result in every warp
+        // (compared on the squared modulus, which orders as the modulus does up to the rounding of the squares)
         double bv = -1.0; int bi = -1; int64_t br = INT64_MAX;
         for (int i = lane; i < nrows; i += 32) {
             if (tag[i] < j) continue;
-            const double a = vabs(A[(size_t)j * nrows + i]);
+            const double a = sqmod(A[(size_t)j * nrows + i]);
             const int64_t r = rid[i];
             if (a > bv || (a == bv && r < br)) { bv = a; bi = i; br = r; }
         }
@@ -501,6 +503,7 @@ __global__ void __launch_bounds__(1024) k_front_lu(const T *__restrict__ W, int6
             const int64_t orr = __shfl_xor_sync(0xffffffffu, br, o);
             if (ov > bv || (ov == bv && orr < br)) { bv = ov; bi = oi; br = orr; }
         }
+        if (bi >= 0) bv = vabs(A[(size_t)j * nrows + bi]);       // the modulus of the winner, for the singular test
         const double thr = pivot_rel * colmax[fcol + j];
         if (bi < 0 || bv <= 0.0 || bv < thr) {
             if (tid == 0) set_status(st, ST_SINGULAR, fcol + j, bv > 0 ? bv : 0.0, thr);
@@ -513,11 +516,11 @@ __global__ void __launch_bounds__(1024) k_front_lu(const T *__restrict__ W, int6
         // the previous step's multipliers into column j - 1 (read by nobody from here on): rows not pivoted up to j - 1
         if (j > 0 && my_g == 0)
             for (int i = my_i; i < nrows; i += rstep) if (tag[i] > j - 1) A[(size_t)(j - 1) * nrows + i] = lcol[i];
-        const T piv = A[(size_t)j * nrows + bi];
+        const T inv = divv(VT<T>::one(), A[(size_t)j * nrows + bi]);
         if (tid == 0) tag[bi] = j;
-        for (int i = my_i; i < nrows; i += rstep) {
+        for (int i = my_i; upd && i < nrows; i += rstep) {
             if (i == bi || tag[i] <= j) continue;
-            const T l = divv(A[(size_t)j * nrows + i], piv);
+            const T l = mul(A[(size_t)j * nrows + i], inv);
             for (int c = j + 1 + my_g; c < npiv; c += G) {
                 T *x = A + (size_t)c * nrows + i;
                 *x = sub(*x, mul(l, A[(size_t)c * nrows + bi]));
@@ -587,6 +590,42 @@ template <> __device__ __forceinline__ double shfl_v<double>(double v, int src) 
 template <> __device__ __forceinline__ cplx shfl_v<cplx>(cplx v, int src)
 {
     return cplx{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
+}
+
+// U12 = L11^-1 A12[perm] in one pass for npiv <= 32 RPL: a warp per column gathers the pivot rows of the column
+// through perm, solves with the unit lower L11 (shared memory) by shuffles, and writes the U12 column
+template <typename T, int RPL>
+__global__ void __launch_bounds__(256) k_u12_fused(const T *__restrict__ W, int64_t ld, const int *__restrict__ perm,
+                                                   int npiv, int64_t ncb, const T *__restrict__ Lb, int64_t ldl,
+                                                   T *__restrict__ U, const DevStatus *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *sL = reinterpret_cast<T *>(smem_raw);          // npiv x npiv, column-major
+    if (st->code) return;
+    for (int e = threadIdx.x; e < npiv * npiv; e += blockDim.x) sL[e] = Lb[(e % npiv) + (int64_t)(e / npiv) * ldl];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    int src[RPL];
+#pragma unroll
+    for (int q = 0; q < RPL; q++) { const int r = lane + 32 * q; src[q] = r < npiv ? perm[r] : 0; }
+    const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5, nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c = wid; c < ncb; c += nwarp) {
+        const T *col = W + (npiv + c) * ld;
+        T x[RPL];
+#pragma unroll
+        for (int q = 0; q < RPL; q++) { const int r = lane + 32 * q; x[q] = r < npiv ? col[src[q]] : VT<T>::zero(); }
+        for (int i = 0; i < npiv; i++) {
+            const T xi = shfl_v<T>(x[i >> 5], i & 31);
+#pragma unroll
+            for (int q = 0; q < RPL; q++) {
+                const int r = lane + 32 * q;
+                if (r > i && r < npiv) x[q] = sub(x[q], mul(sL[r + i * npiv], xi));
+            }
+        }
+        T *u = U + c * npiv;
+#pragma unroll
+        for (int q = 0; q < RPL; q++) { const int r = lane + 32 * q; if (r < npiv) u[r] = x[q]; }
+    }
 }
 
 // X <- L^-1 X for a unit lower w x w block (w <= 32 RPL) and every column of X (rows [0, w) of each column, ld ldx):
@@ -660,6 +699,39 @@ __global__ void k_gather_rows(T *__restrict__ Y, const T *__restrict__ Wr, const
     }
 }
 
+// forward sweep with L through one front in shared memory (one CTA): gather the front's rows of the right-hand sides;
+// the unit lower L11 solve by a warp per right-hand side (shared-memory column sweep, __syncwarp per step); the L21
+// update by the whole CTA; scatter back
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwdL2(const T *__restrict__ L, int64_t nrows, int64_t npiv,
+                                               const int64_t *__restrict__ rowid, T *__restrict__ Wr, int64_t n, int64_t nrhs)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *v = reinterpret_cast<T *>(smem_raw);           // nrows x nrhs
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int64_t e = threadIdx.x; e < nrows * nrhs; e += blockDim.x) v[e] = Wr[rowid[e % nrows] + (e / nrows) * n];
+    __syncthreads();
+    const int64_t np = npiv < nrows ? npiv : nrows;
+    for (int64_t r = warp; r < nrhs; r += nw) {
+        T *vr = v + r * nrows;
+        for (int64_t i = 0; i < np; i++) {
+            const T xi = vr[i];
+            if (!is_zero(xi))
+                for (int64_t rr = i + 1 + lane; rr < np; rr += 32) vr[rr] = sub(vr[rr], mul(L[rr + i * nrows], xi));
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < (nrows - np) * nrhs; e += blockDim.x) {
+        const int64_t rr = np + e % (nrows - np), r = e / (nrows - np);
+        T acc = VT<T>::zero();
+        for (int64_t i = 0; i < np; i++) acc = add(acc, mul(L[rr + i * nrows], v[i + r * nrows]));
+        v[rr + r * nrows] = sub(v[rr + r * nrows], acc);
+    }
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < nrows * nrhs; e += blockDim.x) Wr[rowid[e % nrows] + (e / nrows) * n] = v[e];
+}
+
 // forward sweep with L through one front in shared memory (one CTA): gather the front's rows of the right-hand sides,
 // eliminate column by column, scatter back
 template <typename T>
@@ -729,14 +801,16 @@ __global__ void __launch_bounds__(256) k_u12_gemv(const T *__restrict__ U12, int
     }
 }
 
-// backward sweep with U, step 2 (one CTA): x = U11^-1 (y - sum of the partial sums)
+// backward sweep with U, step 2 (one CTA): s = y - the partial sums (all threads), then x = U11^-1 s by a warp per
+// right-hand side (column sweep from the last pivot, __syncwarp per step)
 template <typename T>
 __global__ void __launch_bounds__(256) k_bwdU(const T *__restrict__ L, int64_t nrows, int64_t npiv, int64_t f,
                                               const T *__restrict__ part, int64_t nchunk, const T *__restrict__ Y,
                                               T *__restrict__ X, int64_t n, int64_t nrhs, DevStatus *st)
 {
-    extern __shared__ unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     T *s = reinterpret_cast<T *>(smem_raw);           // npiv * nrhs
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int64_t e = threadIdx.x; e < npiv * nrhs; e += blockDim.x) {
         const int64_t i = e % npiv, r = e / npiv;
         T v = Y[f + i + r * n];
@@ -744,20 +818,48 @@ __global__ void __launch_bounds__(256) k_bwdU(const T *__restrict__ L, int64_t n
         s[e] = v;
     }
     __syncthreads();
-    for (int64_t i = npiv - 1; i >= 0; i--) {
-        const T d = L[i + i * nrows];
-        if (is_zero(d)) { if (threadIdx.x == 0) set_status(st, ST_SOLVE_ZERO, f + i, 0, 0); return; }
-        for (int64_t r = threadIdx.x; r < nrhs; r += blockDim.x) s[i + r * npiv] = divv(s[i + r * npiv], d);
-        __syncthreads();
-        for (int64_t e = threadIdx.x; e < i * nrhs; e += blockDim.x) {
-            const int64_t j = e % i, r = e / i;
-            s[j + r * npiv] = sub(s[j + r * npiv], mul(L[j + i * nrows], s[i + r * npiv]));
+    for (int64_t r = warp; r < nrhs; r += nw) {
+        T *sr = s + r * npiv;
+        for (int64_t i = npiv - 1; i >= 0; i--) {
+            const T d = L[i + i * nrows];
+            if (is_zero(d)) { if (lane == 0) set_status(st, ST_SOLVE_ZERO, f + i, 0, 0); break; }
+            const T xi = divv(sr[i], d);
+            __syncwarp();
+            if (lane == 0) sr[i] = xi;
+            for (int64_t j = lane; j < i; j += 32) sr[j] = sub(sr[j], mul(L[j + i * nrows], xi));
+            __syncwarp();
         }
-        __syncthreads();
     }
+    __syncthreads();
     for (int64_t e = threadIdx.x; e < npiv * nrhs; e += blockDim.x) {
         const int64_t i = e % npiv, r = e / npiv;
         X[f + i + r * n] = s[e];
+    }
+}
+
+// transposed solves: forward with U^T (U^H when conj) through one front, step 1 (one CTA): z = U11^-T w[f ..] by a warp
+// per right-hand side
+template <typename T, bool CJ>
+__global__ void __launch_bounds__(256) k_fwdUt2(const T *__restrict__ L, int64_t nrows, int64_t npiv, int64_t f,
+                                                T *__restrict__ Wc, int64_t n, int64_t nrhs, DevStatus *st)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int64_t r = warp; r < nrhs; r += nw) {
+        T *w = Wc + f + r * n;
+        for (int64_t i = 0; i < npiv; i++) {
+            T d = L[i + i * nrows];
+            if (CJ) d = conjv(d);
+            if (is_zero(d)) { if (lane == 0) set_status(st, ST_SOLVE_ZERO, f + i, 0, 0); break; }
+            const T zi = divv(w[i], d);
+            __syncwarp();
+            if (lane == 0) w[i] = zi;
+            for (int64_t j = i + 1 + lane; j < npiv; j += 32) {
+                T u = L[i + j * nrows];
+                if (CJ) u = conjv(u);
+                w[j] = sub(w[j], mul(u, zi));
+            }
+            __syncwarp();
+        }
     }
 }
 
@@ -834,16 +936,20 @@ __global__ void __launch_bounds__(256) k_bwdLt(const T *__restrict__ L, int64_t 
         if (lane == 0) s[e] = sub(Z[f + i + r * n], acc);
     }
     __syncthreads();
-    for (int64_t i = npiv - 1; i >= 0; i--) {
-        // s[i] final; s[j] -= L[i, j] s[i] for j < i
-        for (int64_t e = threadIdx.x; e < i * nrhs; e += blockDim.x) {
-            const int64_t j = e % i, r = e / i;
-            T l = L[i + j * nrows];
-            if (CJ) l = conjv(l);
-            s[j + r * npiv] = sub(s[j + r * npiv], mul(l, s[i + r * npiv]));
+    for (int64_t r = warp; r < nrhs; r += nw) {
+        T *sr = s + r * npiv;
+        for (int64_t i = npiv - 1; i >= 0; i--) {
+            // s[i] final; s[j] -= L[i, j] s[i] for j < i
+            const T vi = sr[i];
+            for (int64_t j = lane; j < i; j += 32) {
+                T l = L[i + j * nrows];
+                if (CJ) l = conjv(l);
+                sr[j] = sub(sr[j], mul(l, vi));
+            }
+            __syncwarp();
         }
-        __syncthreads();
     }
+    __syncthreads();
     for (int64_t e = threadIdx.x; e < npiv * nrhs; e += blockDim.x) {
         const int64_t i = e % npiv, r = e / npiv;
         V[f + i + r * n] = s[e];

@@ -6,8 +6,47 @@
 #include <cstring>
 #include <cmath>
 #include <mutex>
+#include <atomic>
 
 namespace fpl {
+
+static std::atomic<long long> g_launches{0};
+static inline void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(); }
+
+// optional per-class device timing of the factorization's kernels (CUDA events around each launch of a class)
+static std::atomic<int> g_prof{0};
+static std::mutex g_prof_mu;
+static ProfClass g_pc[PROF_NCLASS];
+void prof_enable(int on) { g_prof = on; std::lock_guard<std::mutex> lk(g_prof_mu); for (auto &c : g_pc) c = ProfClass(); }
+ProfClass prof_read(int cls) { std::lock_guard<std::mutex> lk(g_prof_mu); return (cls >= 0 && cls < PROF_NCLASS) ? g_pc[cls] : ProfClass(); }
+
+struct ProfRec { int cls; cudaEvent_t a, b; double flops, bytes; };
+struct Prof {
+    std::vector<ProfRec> recs;
+    bool on = g_prof.load() != 0;
+    void begin(cudaStream_t s, int cls, double flops, double bytes) {
+        if (!on) return;
+        ProfRec r{cls, nullptr, nullptr, flops, bytes};
+        cudaEventCreate(&r.a); cudaEventCreate(&r.b);
+        cudaEventRecord(r.a, s);
+        recs.push_back(r);
+    }
+    void end(cudaStream_t s) { if (on && !recs.empty()) cudaEventRecord(recs.back().b, s); }
+    void flush() {
+        if (!on) return;
+        std::lock_guard<std::mutex> lk(g_prof_mu);
+        for (auto &r : recs) {
+            float ms = 0;
+            if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+                ProfClass &c = g_pc[r.cls];
+                c.ms += ms; c.count++; c.flops += r.flops; c.bytes += r.bytes;
+            }
+            cudaEventDestroy(r.a); cudaEventDestroy(r.b);
+        }
+        recs.clear();
+    }
+};
 
 #define CK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { errf(err, errlen, "CUDA: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); return FPLUS_ERR_GPU; } } while (0)
 
@@ -131,7 +170,7 @@ static int run_equil(const DevPlan &D, DevNum &N, int equilibrate, int max_iter,
     cudaStream_t s = N.stream;
     const int64_t n = N.n, nnz = N.nnz;
     T *Bx = (T *)N.Bx;
-    k_gather<T><<<nblk(nnz), 256, 0, s>>>(Bx, (const T *)N.Ax, D.Bsrc, nnz);
+    k_gather<T><<<nblk(nnz), 256, 0, s>>>(Bx, (const T *)N.Ax, D.Bsrc, nnz), note_launch();
     DevStatus h0;
     std::memset(&h0, 0, sizeof(h0));
     h0.amin_bits = 0x7ff0000000000000ull;       // +inf
@@ -143,7 +182,7 @@ static int run_equil(const DevPlan &D, DevNum &N, int equilibrate, int max_iter,
     if (equilibrate) {
         // range guard (FPLUS src/equil.c:197-241)
         const int64_t m = (N.cplx ? 2 : 1) * nnz;
-        k_abs_range<<<nblk(m), 256, 0, s>>>((const double *)Bx, m, N.st);
+        k_abs_range<<<nblk(m), 256, 0, s>>>((const double *)Bx, m, N.st), note_launch();
         DevStatus h;
         CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
@@ -154,11 +193,11 @@ static int run_equil(const DevPlan &D, DevNum &N, int equilibrate, int max_iter,
             if (emax - emin > 990) {
                 unsigned long long *lmax = (unsigned long long *)N.scratch;
                 CK(cudaMemsetAsync(lmax, 0, (size_t)(2 * n) * 8, s));
-                if (N.cplx) k_line_max<true><<<nblk(n), 256, 0, s>>>(D.Bp, D.Bi, (const double *)Bx, n, lmax);
-                else k_line_max<false><<<nblk(n), 256, 0, s>>>(D.Bp, D.Bi, (const double *)Bx, n, lmax);
+                if (N.cplx) k_line_max<true><<<nblk(n), 256, 0, s>>>(D.Bp, D.Bi, (const double *)Bx, n, lmax), note_launch();
+                else k_line_max<false><<<nblk(n), 256, 0, s>>>(D.Bp, D.Bi, (const double *)Bx, n, lmax), note_launch();
                 unsigned long long inf = 0x7ff0000000000000ull;
                 CK(cudaMemcpyAsync(&N.st->amin_bits, &inf, 8, cudaMemcpyHostToDevice, s));
-                k_min_pos<<<nblk(2 * n), 256, 0, s>>>(lmax, 2 * n, N.st);
+                k_min_pos<<<nblk(2 * n), 256, 0, s>>>(lmax, 2 * n, N.st), note_launch();
                 CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, s));
                 CK(cudaStreamSynchronize(s));
                 double lmin = bitsd_h(h.amin_bits);
@@ -171,23 +210,23 @@ static int run_equil(const DevPlan &D, DevNum &N, int equilibrate, int max_iter,
                 emin = elmin;
             }
             k4 = -((emax + emin) / 2 / 4) * 4;
-            k_scale_raw<<<nblk(m), 256, 0, s>>>((double *)Bx, m, std::ldexp(1.0, k4));
+            k_scale_raw<<<nblk(m), 256, 0, s>>>((double *)Bx, m, std::ldexp(1.0, k4)), note_launch();
         }
         unsigned long long *rmax = (unsigned long long *)N.scratch, *cmax = rmax + n;
         for (int it = 0; it < max_iter; it++) {
             CK(cudaMemsetAsync(rmax, 0, (size_t)n * 8, s));
-            k_ruiz_rowmax<T><<<nblk(nnz), 256, 0, s>>>(D.Bi, Bx, nnz, rmax, N.st);
-            k_ruiz_rowscale<<<nblk(n), 256, 0, s>>>(n, rmax, N.Drp, N.st);
-            k_first_zero<<<nblk(n), 256, 0, s>>>(n, rmax, N.st, ST_ZERO_ROW);
-            k_ruiz_colpass<T><<<nblk(32 * n), 256, 0, s>>>(D.Bp, D.Bi, Bx, n, rmax, cmax, N.st);
-            k_ruiz_colscale<<<nblk(n), 256, 0, s>>>(n, cmax, N.Dcp, N.st);
-            k_first_zero<<<nblk(n), 256, 0, s>>>(n, cmax, N.st, ST_ZERO_COL);
-            k_ruiz_colapply<T><<<nblk(32 * n), 256, 0, s>>>(D.Bp, Bx, n, cmax, N.st);
-            k_ruiz_check<<<1, 1, 0, s>>>(N.st, tol);
+            k_ruiz_rowmax<T><<<nblk(nnz), 256, 0, s>>>(D.Bi, Bx, nnz, rmax, N.st), note_launch();
+            k_ruiz_rowscale<<<nblk(n), 256, 0, s>>>(n, rmax, N.Drp, N.st), note_launch();
+            k_first_zero<<<nblk(n), 256, 0, s>>>(n, rmax, N.st, ST_ZERO_ROW), note_launch();
+            k_ruiz_colpass<T><<<nblk(32 * n), 256, 0, s>>>(D.Bp, D.Bi, Bx, n, rmax, cmax, N.st), note_launch();
+            k_ruiz_colscale<<<nblk(n), 256, 0, s>>>(n, cmax, N.Dcp, N.st), note_launch();
+            k_first_zero<<<nblk(n), 256, 0, s>>>(n, cmax, N.st, ST_ZERO_COL), note_launch();
+            k_ruiz_colapply<T><<<nblk(32 * n), 256, 0, s>>>(D.Bp, Bx, n, cmax, N.st), note_launch();
+            k_ruiz_check<<<1, 1, 0, s>>>(N.st, tol), note_launch();
         }
-        if (k4 != 0) k_fold<<<nblk(n), 256, 0, s>>>(N.Drp, N.Dcp, n, std::ldexp(1.0, k4 / 2));
+        if (k4 != 0) k_fold<<<nblk(n), 256, 0, s>>>(N.Drp, N.Dcp, n, std::ldexp(1.0, k4 / 2)), note_launch();
     }
-    k_colmax<T><<<nblk(32 * n), 256, 0, s>>>(D.Bp, Bx, n, N.colmax);
+    k_colmax<T><<<nblk(32 * n), 256, 0, s>>>(D.Bp, Bx, n, N.colmax), note_launch();
     CK(cudaGetLastError());
     DevStatus h;
     CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -229,6 +268,9 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         CK(cudaFuncSetAttribute(k_front_lu<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_u12_fused<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_u12_fused<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_u12_fused<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         attr_set = 1;
     }
     if ((rc = dev_clear_status(N, err, errlen))) return rc;
@@ -237,16 +279,19 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     constexpr int PW = 32;       // panel width of the blocked path
     const int TB = VT<T>::cplx_ ? 32 : 64;    // rows per TRSM block of U12
     const int64_t nf = (int64_t)P.fronts.size();
+    const double fm = VT<T>::cplx_ ? 8.0 : 2.0;     // flops per multiply-add
+    Prof prof;
     for (int64_t fi = 0; fi < nf; fi++) {
         const Front &F = P.fronts[fi];
         const int64_t nr = F.nrows, nc = F.ncols, np = F.npiv, ncb = nc - np;
         const int64_t ld = nr;
         T *Lf = La + F.L_off;
+        prof.begin(s, PROF_ASM, 0.0, (double)(nr * nc + 2 * (F.asm_end - F.asm_begin)) * vs);
         if (nr * nc > 0) CK(cudaMemsetAsync(W, 0, (size_t)(nr * nc) * vs, s));
         {
             const int64_t cnt = F.asm_end - F.asm_begin;
             k_assemble<T><<<nblk(std::max(cnt, nr)), 256, 0, s>>>(W, Bx, D.asm_src + F.asm_begin, D.asm_dst + F.asm_begin, cnt,
-                                                                   N.rowid + F.row_off, D.rowinit + F.row_off, nr, N.st);
+                                                                   N.rowid + F.row_off, D.rowinit + F.row_off, nr, N.st), note_launch();
         }
         for (int64_t k = F.child_begin; k < F.child_end; k++) {
             const Front &G = P.fronts[P.children[k]];
@@ -255,75 +300,94 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             if (cbr == 0) continue;
             k_extend_add<T><<<nblk(std::max(cbr * cbc, nslot)), 256, 0, s>>>(W, ld, CB + G.cb_off, cbr, cbc, nslot, G.slot,
                                                                             F.tau_base, D.relcol + G.relcol_off,
-                                                                            N.rowid + F.row_off, N.rowid + G.row_off + G.npiv, N.st);
+                                                                            N.rowid + F.row_off, N.rowid + G.row_off + G.npiv, N.st), note_launch();
         }
+        prof.end(s);
         if (np == 0) continue;
-        if (nr == 0) { k_set_singular<<<1, 1, 0, s>>>(N.st, F.f); continue; }     // no row can take pivot step f
+        if (nr == 0) { k_set_singular<<<1, 1, 0, s>>>(N.st, F.f), note_launch(); continue; }     // no row can take pivot step f
         // the pivot block: partial-pivot LU, L\U into the arena in the final row order, the order into N.perm
         const size_t sm = front_lu_smem(nr, np, vs);
+        {
+            double fl = 0;
+            for (int64_t k = 0; k < std::min(np, nr); k++) fl += (double)(nr - k - 1) * (double)(np - k);
+            prof.begin(s, PROF_LU, fm * fl, 2.0 * (double)(nr * np) * vs);
+        }
         if (sm <= SMEM_MAX) {
             const int R = (int)((nr + 31) & ~31);
-            int nt = R;
-            while (nt * 2 <= 1024 && nt * 2 <= R * std::max<int64_t>(1, np / 8)) nt *= 2;
-            if (nt > 1024) nt = 1024;
-            if (nt < 64) nt = 64;
+            int nt = R <= 256 ? 256 : (R < 1024 ? R : 1024);
             k_front_lu<T><<<1, nt, sm, s>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel, N.rowid + F.row_off, Lf,
-                                           N.perm, N.p_lu, N.st, fi);
+                                           N.perm, N.p_lu, N.st, fi), note_launch();
         } else {
             const int64_t npr = std::min(np, nr);
             for (int64_t k0 = 0; k0 < npr; k0 += PW) {
                 const int w = (int)std::min<int64_t>(PW, npr - k0);
                 k_panel<T><<<1, 512, 0, s>>>(W, ld, nr, F.nri, (int)k0, w, F.f, N.colmax, pivot_rel, N.rowid + F.row_off,
-                                            N.ipiv + F.f, N.st, fi);
-                if (k0 > 0) k_laswp<T><<<nblk(k0, 128), 128, 0, s>>>(W, ld, N.ipiv + F.f, (int)k0, w, 0, k0, N.st);
+                                            N.ipiv + F.f, N.st, fi), note_launch();
+                if (k0 > 0) k_laswp<T><<<nblk(k0, 128), 128, 0, s>>>(W, ld, N.ipiv + F.f, (int)k0, w, 0, k0, N.st), note_launch();
                 if (k0 + w < np) {
-                    k_laswp<T><<<nblk(np - k0 - w, 128), 128, 0, s>>>(W, ld, N.ipiv + F.f, (int)k0, w, k0 + w, np, N.st);
-                    k_trsm_unit<T><<<nblk(np - k0 - w, 128), 128, 0, s>>>(W, ld, (int)k0, w, k0 + w, np, N.st);
+                    k_laswp<T><<<nblk(np - k0 - w, 128), 128, 0, s>>>(W, ld, N.ipiv + F.f, (int)k0, w, k0 + w, np, N.st), note_launch();
+                    k_trsm_unit<T><<<nblk(np - k0 - w, 128), 128, 0, s>>>(W, ld, (int)k0, w, k0 + w, np, N.st), note_launch();
                     const int64_t M = nr - k0 - w, Nn = np - k0 - w;
                     if (M > 0) {
                         dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((Nn + GBN - 1) / GBN));
                         T *C = W + (k0 + w) + (k0 + w) * ld;
                         k_gemm_sub<T><<<g, 256, 0, s>>>(M, Nn, w, W + (k0 + w) + k0 * ld, ld, W + k0 + (k0 + w) * ld, ld,
-                                                        C, ld, nullptr, C, ld, N.st);
+                                                        C, ld, nullptr, C, ld, N.st), note_launch();
                     }
                 }
             }
             k_left_finish<T><<<nblk(nr * np), 256, 0, s>>>(W, ld, nr, np, N.ipiv + F.f, N.perm, N.rowid + F.row_off, F.f, N.p_lu,
-                                                          Lf, N.st);
+                                                          Lf, N.st), note_launch();
         }
-        if (nr < np) k_set_singular<<<1, 1, 0, s>>>(N.st, F.f + nr);
+        prof.end(s);
+        if (nr < np) { k_set_singular<<<1, 1, 0, s>>>(N.st, F.f + nr), note_launch(); }
         if (ncb == 0) continue;
         // U12 = L11^-1 A12[perm]: gather the pivot rows into the arena, then blocked TRSM in place
         T *Uf = Ua + F.U_off;
-        k_u12_gather<T><<<nblk(np * ncb), 256, 0, s>>>(W, ld, np, ncb, N.perm, Uf, N.st);
+        prof.begin(s, PROF_U12, fm * (double)np * (double)np / 2.0 * (double)ncb, 3.0 * (double)(np * ncb) * vs);
         const int64_t npr = std::min(np, nr);
+        const int rpl_max = VT<T>::cplx_ ? 2 : 4;        // L11 in shared memory: 64 x 64 complex or 128 x 128 real
+        if (npr == np && np <= 32 * rpl_max) {
+            const size_t tsm = (size_t)np * np * vs;
+            const int nwarps = (int)std::min<int64_t>(ncb, 148 * 64);
+            const int blocks = (nwarps + 7) / 8;
+            if (np <= 32) k_u12_fused<T, 1><<<blocks, 256, tsm, s>>>(W, ld, N.perm, (int)np, ncb, Lf, ld, Uf, N.st), note_launch();
+            else if (np <= 64) k_u12_fused<T, 2><<<blocks, 256, tsm, s>>>(W, ld, N.perm, (int)np, ncb, Lf, ld, Uf, N.st), note_launch();
+            else k_u12_fused<T, 4><<<blocks, 256, tsm, s>>>(W, ld, N.perm, (int)np, ncb, Lf, ld, Uf, N.st), note_launch();
+        } else {
+        k_u12_gather<T><<<nblk(np * ncb), 256, 0, s>>>(W, ld, np, ncb, N.perm, Uf, N.st), note_launch();
         for (int64_t k0 = 0; k0 < npr; k0 += TB) {
             const int w = (int)std::min<int64_t>(TB, npr - k0);
             const size_t tsm = (size_t)w * w * vs;
             const int nwarps = (int)std::min<int64_t>(ncb, 148 * 64);
             const int blocks = (nwarps + 7) / 8;
-            if (w <= 32) k_trsm_warp<T, 1><<<blocks, 256, tsm, s>>>(Uf + k0, np, w, ncb, Lf + k0 + k0 * ld, ld, N.st);
-            else k_trsm_warp<T, 2><<<blocks, 256, tsm, s>>>(Uf + k0, np, w, ncb, Lf + k0 + k0 * ld, ld, N.st);
+            if (w <= 32) k_trsm_warp<T, 1><<<blocks, 256, tsm, s>>>(Uf + k0, np, w, ncb, Lf + k0 + k0 * ld, ld, N.st), note_launch();
+            else k_trsm_warp<T, 2><<<blocks, 256, tsm, s>>>(Uf + k0, np, w, ncb, Lf + k0 + k0 * ld, ld, N.st), note_launch();
             const int64_t M = npr - k0 - w;
             if (M > 0) {
                 dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((ncb + GBN - 1) / GBN));
                 T *C = Uf + k0 + w;
-                k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, w, Lf + (k0 + w) + k0 * ld, ld, Uf + k0, np, C, np, nullptr, C, np, N.st);
+                k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, w, Lf + (k0 + w) + k0 * ld, ld, Uf + k0, np, C, np, nullptr, C, np, N.st), note_launch();
             }
         }
+        }
+        prof.end(s);
         // the Schur complement into the CB stack: CB = A22[perm] - L21 U12
         const int64_t M = nr - np;
         if (M > 0) {
+            prof.begin(s, PROF_SCHUR, fm * (double)M * (double)ncb * (double)np, (double)(2 * M * ncb + M * np + np * ncb) * vs);
             dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((ncb + GBN - 1) / GBN));
-            k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, np, Lf + np, ld, Uf, np, W + np * ld, ld, N.perm + np, CB + F.cb_off, M, N.st);
+            k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, np, Lf + np, ld, Uf, np, W + np * ld, ld, N.perm + np, CB + F.cb_off, M, N.st), note_launch();
+            prof.end(s);
         }
         if ((fi & 255) == 255) CK(cudaGetLastError());
     }
     CK(cudaGetLastError());
-    k_pinv<<<nblk(N.n), 256, 0, s>>>(N.p_lu, N.pinv, N.n, N.st);
+    k_pinv<<<nblk(N.n), 256, 0, s>>>(N.p_lu, N.pinv, N.n, N.st), note_launch();
     DevStatus h;
     CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    prof.flush();
     if (h.code == ST_BORDER) { *border_front = h.idx; return FPLUS_OK; }
     if (h.code == ST_SINGULAR) {
         errf(err, errlen, "Near-zero or zero pivot %.6e at step %ld (threshold %.6e). Matrix is singular.", h.best, (long)h.idx, h.thr);
@@ -368,7 +432,7 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
     const T *La = (const T *)N.Larena, *Ua = (const T *)N.Uarena;
     const int64_t nf = (int64_t)P.fronts.size();
     const size_t smem = (size_t)P.max_npiv * (size_t)nrhs * sizeof(T);
-    CK(cudaFuncSetAttribute(k_fwdL_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    CK(cudaFuncSetAttribute(k_fwdL2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
     CK(cudaFuncSetAttribute(k_u12_gemv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
     if (smem > 48 * 1024) {
         CK(cudaFuncSetAttribute(k_bwdU<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -377,17 +441,17 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
     }
     if (trans == 0) {
         // R (row space) = Dr * b[row_perm]; forward with L; S2 = R[p_lu] (pivot order); backward with U into R
-        k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, n, D.row_perm, N.Drp, n, nrhs);
+        k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, n, D.row_perm, N.Drp, n, nrhs), note_launch();
         for (int64_t fi = 0; fi < nf; fi++) {
             const Front &F = P.fronts[fi];
             if (F.npiv == 0 || F.nrows == 0) continue;
             const size_t fsm = (size_t)F.nrows * nrhs * sizeof(T);
             if (fsm <= 96 * 1024)
-                k_fwdL_smem<T><<<1, 256, fsm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs);
+                k_fwdL2<T><<<1, 256, fsm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs), note_launch();
             else
-                k_fwdL<T><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs);
+                k_fwdL<T><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs), note_launch();
         }
-        k_gather_rows<T><<<nblk(n * nrhs), 256, 0, s>>>(S2, R, N.p_lu, n, nrhs);
+        k_gather_rows<T><<<nblk(n * nrhs), 256, 0, s>>>(S2, R, N.p_lu, n, nrhs), note_launch();
         for (int64_t fi = nf - 1; fi >= 0; fi--) {
             const Front &F = P.fronts[fi];
             const int64_t ncb = F.ncols - F.npiv;
@@ -397,37 +461,37 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
                 const int64_t chunk = chunk_of(ncb);
                 nchunk = (ncb + chunk - 1) / chunk;
                 k_u12_gemv<T><<<(unsigned)nchunk, 256, (size_t)8 * F.npiv * sizeof(T), s>>>(
-                    Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, R, n, nrhs, chunk, part);
+                    Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, R, n, nrhs, chunk, part), note_launch();
             }
             k_bwdU<T><<<1, 256, (size_t)F.npiv * nrhs * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, part, nchunk, S2, R,
-                                                                         n, nrhs, N.st);
+                                                                         n, nrhs, N.st), note_launch();
         }
         // x[col_perm[k]] = Dcp[k] * R[k]
-        k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, R, D.col_perm, nullptr, N.Dcp, n, nrhs);
+        k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, R, D.col_perm, nullptr, N.Dcp, n, nrhs), note_launch();
     } else {
         // R (column space) = Dc * b[col_perm]; forward with U^T; backward with L^T into S2 (pivot order)
-        k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, n, D.col_perm, N.Dcp, n, nrhs);
+        k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, n, D.col_perm, N.Dcp, n, nrhs), note_launch();
         const bool cj = trans == 2;
         for (int64_t fi = 0; fi < nf; fi++) {
             const Front &F = P.fronts[fi];
             const int64_t ncb = F.ncols - F.npiv;
             if (F.npiv == 0) continue;
-            if (cj) k_fwdUt<T, true><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st);
-            else k_fwdUt<T, false><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st);
+            if (cj) k_fwdUt2<T, true><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
+            else k_fwdUt2<T, false><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
             if (ncb > 0) {
-                if (cj) k_ut_scatter<T, true><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, F.f, R, n, nrhs);
-                else k_ut_scatter<T, false><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, F.f, R, n, nrhs);
+                if (cj) k_ut_scatter<T, true><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, F.f, R, n, nrhs), note_launch();
+                else k_ut_scatter<T, false><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, F.f, R, n, nrhs), note_launch();
             }
         }
         for (int64_t fi = nf - 1; fi >= 0; fi--) {
             const Front &F = P.fronts[fi];
             if (F.npiv == 0) continue;
             const size_t sm = (size_t)F.npiv * nrhs * sizeof(T);
-            if (cj) k_bwdLt<T, true><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, N.rowid + F.row_off, N.pinv, R, S2, n, nrhs);
-            else k_bwdLt<T, false><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, N.rowid + F.row_off, N.pinv, R, S2, n, nrhs);
+            if (cj) k_bwdLt<T, true><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, N.rowid + F.row_off, N.pinv, R, S2, n, nrhs), note_launch();
+            else k_bwdLt<T, false><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, N.rowid + F.row_off, N.pinv, R, S2, n, nrhs), note_launch();
         }
         // x[row_perm[p_lu[k]]] = Drp[p_lu[k]] * S2[k]
-        k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, S2, D.row_perm, N.p_lu, N.Drp, n, nrhs);
+        k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, S2, D.row_perm, N.p_lu, N.Drp, n, nrhs), note_launch();
     }
     CK(cudaGetLastError());
     return FPLUS_OK;
@@ -466,7 +530,7 @@ int dev_check_finite(DevNum &N, char *err, size_t errlen)
 {
     const int64_t m = (N.cplx ? 2 : 1) * N.nnz;
     if (dev_clear_status(N, err, errlen) != FPLUS_OK) return FPLUS_ERR_GPU;
-    k_check_finite<<<nblk(m), 256, 0, N.stream>>>((const double *)N.Ax, m, N.st);
+    k_check_finite<<<nblk(m), 256, 0, N.stream>>>((const double *)N.Ax, m, N.st), note_launch();
     DevStatus h;
     CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, N.stream));
     CK(cudaStreamSynchronize(N.stream));

@@ -10,6 +10,14 @@ namespace fpl {
 
 struct DevStatus;
 
+// per-class device timing (fplus_b200_profile): 0 Schur GEMM into the CB, 1 pivot-block LU, 2 U12 (gather + TRSM),
+// 3 assembly and extend-add
+enum { PROF_SCHUR = 0, PROF_LU = 1, PROF_U12 = 2, PROF_ASM = 3, PROF_NCLASS = 4 };
+struct ProfClass { double ms = 0, flops = 0, bytes = 0; long long count = 0; };
+void prof_enable(int on);
+ProfClass prof_read(int cls);
+long long launch_count();
+
 inline double bitsd_h(unsigned long long b) { double d; std::memcpy(&d, &b, 8); return d; }
 
 // device copies of a plan and of the symbolic object's permutation (read-only, shared by every factorization)

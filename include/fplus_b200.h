@@ -54,6 +54,17 @@ int fplus_b200_plan_size(const fplus_symbolic *sym, int64_t tail, int64_t *nfron
 int fplus_b200_plan_export(const fplus_symbolic *sym, int64_t tail, int64_t *col_front, int64_t *parent, int64_t *col_ptr,
                            int64_t *cols, int64_t *nrows, int64_t *nbord);
 
+/* Kernel launches made by this library since it was loaded (all threads). */
+long long fplus_b200_launch_count(void);
+
+/* Device timing of the factorization's kernels by class, for measurement: when on, every launch of a class is bracketed
+ * by CUDA events (a small perturbation; off by default).  Turning it on clears the totals.  Classes: 0 the Schur-
+ * complement GEMM into the contribution block, 1 the pivot-block LU, 2 U12 (gather + TRSM), 3 assembly and extend-add.
+ * profile_read returns the class's total device milliseconds, launches, and the algorithmic flops and bytes of those
+ * launches. */
+void fplus_b200_profile(int on);
+int fplus_b200_profile_read(int cls, double *ms, long long *count, double *flops, double *bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,311 @@
+"""CPU tests (no GPU): the oracle against the reference and the golden fixtures, the host-side analysis against the
+reference's own ordering code, the multifrontal structure against the oracle's factors, the C-ABI library's exports,
+and the host-side argument checks of the boundary."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import fplus_b200 as F
+import oracle as O
+from fplus_b200 import workloads as W
+from tests.cases import CASES
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLD = os.path.join(ROOT, "tests", "golden")
+needs_ref = pytest.mark.skipif(not O.have_reference(), reason="oracle/_ref (the reference build) is not present")
+
+
+def _rel(A, B):
+    return sp.linalg.norm(A - B) / max(sp.linalg.norm(B), 1e-300)
+
+
+def _masks(n, S):
+    tr = np.zeros(n, np.uint8); tr[S.row_perm[n - S.n_dense_rows:]] = 1
+    tc = np.zeros(n, np.uint8); tc[S.col_perm[n - S.n_dense_cols:]] = 1
+    return tr, tc
+
+
+# ------------------------------------------------------------------------------------------------ the library boundary
+def _declared(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fplus_\w+)\s*\(", text)) - {"fplus_symbolic", "fplus_numeric"})
+
+
+def test_library_exports_every_declared_symbol():
+    L = F.lib()
+    declared = _declared("fplus.h") + _declared("fplus_b200.h")
+    missing = [s for s in declared if not hasattr(L, s)]
+    assert not missing, f"declared but not exported: {missing}"
+    assert set(F.FPLUS_H_SYMBOLS) <= set(declared) and set(F.FPLUS_B200_H_SYMBOLS) <= set(declared)
+
+
+def test_options_defaults_match_reference():
+    o = F.default_options()
+    # FPLUS src/numeric.c:15-22
+    assert (o.pin_dense, o.tau_density, o.tau_min_nnz, o.postorder) == (1, 0.5, 10, 1)
+    assert (o.equilibrate, o.ruiz_max_iter, o.ruiz_tol) == (1, 20, 1e-2)
+    assert o.pivot_rel == F.FPLUS_PIVOT_REL_DEFAULT and o.pivot_strategy == F.FPLUS_PIVOT_PARTIAL and o.drop_tol == 0.0
+    assert (o.relax_rows, o.panel, o.use_gpu, o.gpu_min_flops, o.verbose) == (32, 512, 0, 5e7, 0)
+    assert ctypes.sizeof(F.Options) == 112
+
+
+def _factor_rc(S, Ax, cplx, opt=None, Ap=None, Ai=None):
+    err = ctypes.create_string_buffer(256)
+    h = ctypes.c_void_p()
+    Ap = S.Ap if Ap is None else np.ascontiguousarray(Ap, np.int64)
+    Ai = S.Ai if Ai is None else np.ascontiguousarray(Ai, np.int64)
+    Ax = np.ascontiguousarray(Ax)
+    rc = F.lib().fplus_factor(S._h, F._p64(Ap), F._p64(Ai), Ax.ctypes.data_as(ctypes.c_void_p), int(cplx),
+                              ctypes.byref(opt if opt is not None else S.options), ctypes.byref(h), err, 256)
+    return rc, err.value.decode()
+
+
+def test_factor_argument_checks_on_host():
+    n, Ap, Ai, Ax = W.convdiff2d(8, 1)
+    S = F.analyze(n, Ap, Ai)
+    assert _factor_rc(S, Ax, 0, F.default_options(pivot_strategy=7))[0] == F.FPLUS_ERR_BADARG
+    assert _factor_rc(S, Ax, 0, F.default_options(drop_tol=-1.0))[0] == F.FPLUS_ERR_BADARG
+    rc, msg = _factor_rc(S, Ax, 0, F.default_options(pivot_strategy=F.FPLUS_PIVOT_ROOK))
+    assert rc == F.FPLUS_ERR_BADARG and "partial pivoting" in msg
+    assert _factor_rc(S, Ax, 0, F.default_options(drop_tol=1e-3))[0] == F.FPLUS_ERR_BADARG
+    assert _factor_rc(S, Ax, 0, F.default_options(pivot_rel=-1.0))[0] == F.FPLUS_ERR_BADARG
+    bad = Ax.copy(); bad[5] = np.nan
+    rc, msg = _factor_rc(S, bad, 0)
+    assert rc == F.FPLUS_ERR_BADARG and "non-finite" in msg
+    # a different pattern with the same number of entries
+    Ai2 = Ai.copy(); Ai2[Ap[3]] = (Ai2[Ap[3]] + 1) % n
+    A2 = sp.csc_matrix((Ax, Ai2, Ap), shape=(n, n)); A2.sort_indices()
+    if A2.nnz == len(Ax):
+        rc, msg = _factor_rc(S, A2.data, 0, None, A2.indptr, A2.indices)
+        assert rc == F.FPLUS_ERR_BADARG
+    rc, msg = _factor_rc(S, Ax[:-1], 0, None, np.r_[Ap[:-1], Ap[-1] - 1], Ai[:-1])
+    assert rc == F.FPLUS_ERR_BADARG and "nonzeros" in msg
+
+
+def test_analyze_argument_checks():
+    with pytest.raises(F.FplusError) as e:
+        F.analyze(2, np.array([0, 2, 3]), np.array([1, 0, 1]))       # unsorted: not canonical
+    assert e.value.code == F.FPLUS_ERR_BADARG
+    with pytest.raises(F.FplusError) as e:
+        F.analyze(2, np.array([0, 2, 3]), np.array([0, 5, 1]))       # index out of range
+    assert e.value.code == F.FPLUS_ERR_BADARG
+
+
+# ------------------------------------------------------------------------------------------------ the analysis
+@needs_ref
+@pytest.mark.parametrize("name", ["convdiff2d_g20", "pencil_1x64", "hard_real_300", "hard_cplx_300", "banded_cplx_1200"])
+def test_analysis_matches_reference_order_code(name):
+    """Dense-line pinning, the row order and the column-etree postorder against the reference's src/order.c, given the
+    same fill-reducing order (SuiteSparse COLAMD is absent: the order is injected into the reference's code)."""
+    n, Ap, Ai, Ax = CASES[name]()
+    S = F.analyze(n, Ap, Ai)
+    cnt = np.bincount(Ai, minlength=n)
+    thr = max(0.5 * n, 10)
+    tr, tc = (cnt > thr).astype(np.uint8), (np.diff(Ap) > thr).astype(np.uint8)
+    assert S.n_dense_rows == tr.sum() and S.n_dense_cols == tc.sum()
+    perm = F.interior_order(n, Ap, Ai, tr, tc)
+    R = O.RefLU(n, Ap, Ai, None, perm, None, None, postorder=1)
+    assert np.array_equal(R.row_perm, S.row_perm)
+    assert np.array_equal(R.col_perm, S.col_perm)
+
+
+@needs_ref
+def test_coletree_postorder_matches_reference():
+    rng = np.random.default_rng(4)
+    for m, n in ((40, 30), (200, 200), (150, 170)):
+        A = sp.random(m, n, density=0.04, random_state=rng, format="csc")
+        A.sort_indices()
+        Ap, Ai = A.indptr.astype(np.int64), A.indices.astype(np.int64)
+        p1, p2 = np.zeros(n, np.int64), np.zeros(n, np.int64)
+        assert F.lib().fplus_coletree_postorder(m, n, F._p64(Ap), F._p64(Ai), F._p64(p1)) == 0
+        assert O.reference().fplus_coletree_postorder(m, n, F._p64(Ap), F._p64(Ai), F._p64(p2)) == 0
+        assert np.array_equal(p1, p2)
+
+
+def test_interior_order_is_a_fill_reducing_permutation():
+    n, Ap, Ai, Ax = W.convdiff2d(30, 1)
+    perm = F.interior_order(n, Ap, Ai)
+    assert np.array_equal(np.sort(perm), np.arange(n))
+    S = F.analyze(n, Ap, Ai)
+    A = sp.csc_matrix((np.ones(len(Ai)), Ai, Ap), shape=(n, n))
+    fill = lambda cp: O.OracleLU(n, Ap, Ai, Ax, np.arange(n), cp).L.nnz
+    assert fill(S.col_perm) < 0.7 * fill(np.arange(n))            # less fill than the natural (banded) order
+
+
+# ------------------------------------------------------------------------------------------------ the oracle
+@needs_ref
+@pytest.mark.parametrize("name", ["convdiff2d_g20", "convdiff2d_g100", "pencil_1x64", "hard_real_300", "hard_cplx_300",
+                                  "hard_cplx_300_s0", "banded_cplx_1200", "convdiff3d_g12"])
+def test_oracle_matches_reference(name):
+    n, Ap, Ai, Ax = CASES[name]()
+    S = F.analyze(n, Ap, Ai)
+    tr, tc = _masks(n, S)
+    R = O.RefLU(n, Ap, Ai, Ax, S.col_perm, tr, tc, postorder=0)
+    orc = O.OracleLU(n, Ap, Ai, Ax, S.row_perm, S.col_perm)
+    assert np.array_equal(R.p, orc.p)
+    assert np.array_equal(R.Dr, orc.Dr) and np.array_equal(R.Dc, orc.Dc)
+    L, U, p_lu, _ = R.factors()
+    assert np.array_equal(p_lu, orc.p_lu)
+    assert _rel(orc.L, L) < 1e-12 and _rel(orc.U, U) < 1e-12
+    b = np.random.default_rng(3).standard_normal(n) + (1j if np.iscomplexobj(Ax) else 0)
+    for t in ((0, 1, 2) if np.iscomplexobj(Ax) else (0, 1)):
+        x, xr = orc.solve(b, t), R.solve(b, t)
+        assert np.linalg.norm(x - xr) <= 1e-10 * np.linalg.norm(xr)
+
+
+@pytest.mark.parametrize("name", ["relaxed_panel_case50", "relaxed_panel_case3"])
+def test_oracle_against_golden_regression_matrices(name):
+    """The reference's regression matrices (identity orders): the reference keeps the same pivots for every relax /
+    panel combination, and the oracle reproduces them, the scalings bit for bit, and the solution."""
+    z = np.load(os.path.join(GOLD, name + ".npz"))
+    assert bool(z["p_all_equal"])
+    n = int(z["n"])
+    orc = O.OracleLU(n, z["Ap"], z["Ai"], z["Ax"], z["row_perm"], z["col_perm"])
+    assert np.array_equal(orc.p, z["p"])
+    assert np.array_equal(orc.Dr, z["Dr"]) and np.array_equal(orc.Dc, z["Dc"])
+    assert abs(sp.linalg.norm(orc.L) - float(z["L_fro"])) <= 1e-12 * float(z["L_fro"])
+    assert abs(sp.linalg.norm(orc.U) - float(z["U_fro"])) <= 1e-12 * float(z["U_fro"])
+    x = orc.solve(z["b"], 0)
+    assert np.linalg.norm(x - z["x"]) <= 1e-10 * np.linalg.norm(z["x"])
+    assert O.backward_error(n, z["Ap"], z["Ai"], z["Ax"], x, z["b"]) < 1e-13
+
+
+def _golden_generated():
+    z = np.load(os.path.join(GOLD, "generated_cases.npz"))
+    return z, [str(s) for s in z["names"]]
+
+
+@pytest.mark.parametrize("name", ["convdiff2d_g20", "pencil_1x64", "hard_real_300", "hard_cplx_300", "banded_cplx_600"])
+def test_oracle_against_golden_generated(name):
+    z, names = _golden_generated()
+    g = lambda k: z[f"{name}__{k}"]
+    n = int(g("n"))
+    orc = O.OracleLU(n, g("Ap"), g("Ai"), g("Ax"), g("row_perm"), g("col_perm"))
+    assert np.array_equal(orc.p, g("p"))
+    assert np.array_equal(orc.Dr, g("Dr")) and np.array_equal(orc.Dc, g("Dc"))
+    assert abs(sp.linalg.norm(orc.L) - float(g("L_fro"))) <= 1e-12 * float(g("L_fro"))
+    assert abs(sp.linalg.norm(orc.U) - float(g("U_fro"))) <= 1e-12 * float(g("U_fro"))
+    B = g("B")
+    for t in ((0, 1, 2) if np.iscomplexobj(g("Ax")) else (0, 1)):
+        X = orc.solve(B, t)
+        assert np.linalg.norm(X - g(f"X{t}")) <= 1e-10 * np.linalg.norm(g(f"X{t}"))
+    # the analysis of this build reproduces the committed orders
+    S = F.analyze(n, g("Ap"), g("Ai"))
+    assert np.array_equal(S.row_perm, g("row_perm")) and np.array_equal(S.col_perm, g("col_perm"))
+
+
+def test_ruiz_range_guard_known_answers():
+    """tests/c/test_fplus.c:249-266: entries near 1e200 are rescaled by a power of two (scaled to 1 within e^0.01, and
+    Dr A Dc reproduces them); a 1e300 / 1e-300 span is refused."""
+    L = O.restatement()
+    n = 3
+    p = np.array([0, 1, 2, 3], np.int64); i = np.array([0, 1, 2], np.int64)
+    x = np.array([1e200, 1e100, 1e150]); x0 = x.copy()
+    Dr, Dc = np.zeros(3), np.zeros(3)
+    it = ctypes.c_int()
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    rc = L.orc_ruiz(n, F._p64(p), F._p64(i), x.ctypes.data_as(ctypes.c_void_p), 0, 20, 1e-2, dp(Dr), dp(Dc), ctypes.byref(it), None, 0)
+    assert rc == 0
+    assert np.all(np.abs(np.log(np.abs(x))) < 1e-2)
+    assert np.all(np.abs(Dr * x0 * Dc - x) < 1e-14 * np.abs(x))
+    y = np.array([1e300, 1e-300, 1.0])
+    rc = L.orc_ruiz(n, F._p64(p), F._p64(i), y.ctypes.data_as(ctypes.c_void_p), 0, 20, 1e-2, dp(Dr), dp(Dc), ctypes.byref(it), None, 0)
+    assert rc == -3
+    if O.have_reference():
+        R = O.reference()
+        x = x0.copy()
+        Dr2, Dc2 = np.zeros(3), np.zeros(3)
+        assert R.fplus_ruiz(n, F._p64(p), F._p64(i), x.ctypes.data_as(ctypes.c_void_p), 0, 1, 20, 1e-2, 0, dp(Dr2), dp(Dc2), None, 0) == 0
+        x1 = x0.copy()
+        L.orc_ruiz(n, F._p64(p), F._p64(i), x1.ctypes.data_as(ctypes.c_void_p), 0, 20, 1e-2, dp(Dr), dp(Dc), ctypes.byref(it), None, 0)
+        assert np.array_equal(x, x1) and np.array_equal(Dr, Dr2) and np.array_equal(Dc, Dc2)
+
+
+def test_oracle_several_rhs_equal_one_at_a_time():
+    n, Ap, Ai, Ax = CASES["banded_cplx_1200"]()
+    S = F.analyze(n, Ap, Ai)
+    orc = O.OracleLU(n, Ap, Ai, Ax, S.row_perm, S.col_perm)
+    B = np.random.default_rng(1).standard_normal((n, 5)) + 1j
+    X = orc.solve(B, 2)
+    assert np.array_equal(X, np.column_stack([orc.solve(B[:, k], 2) for k in range(5)]))
+
+
+# ------------------------------------------------------------------------------------------------ the front structure
+@pytest.mark.parametrize("name", ["convdiff2d_g20", "convdiff2d_g100", "convdiff3d_g12", "pencil_1x64", "hard_real_300",
+                                  "hard_cplx_300", "banded_cplx_1200"])
+def test_front_structure_contains_the_factors(name):
+    """Every nonzero of the oracle's L and U (same orders, same pivots) lies inside the multifrontal structure: U[k, c]
+    in the columns of the front of k, and each L[row, k]'s row (by its first column) in the subtree of that front.  A
+    dense row pivoted inside a front with border rows needs the dense chain: with the chain started at that front's first
+    column, the containment holds."""
+    n, Ap, Ai, Ax = CASES[name]()
+    S = F.analyze(n, Ap, Ai)
+    orc = O.OracleLU(n, Ap, Ai, Ax, S.row_perm, S.col_perm)
+    mi = n - S.n_dense_rows
+    Bc = orc.B.tocoo()
+    firstcol = np.full(n, n)
+    np.minimum.at(firstcol, Bc.row, Bc.col)
+    p_lu = orc.p_lu
+    Lc, Uc = orc.L.tocoo(), orc.U.tocoo()
+
+    def check(tail):
+        """containment for the pivot steps before the first dense-row pivot in a front with border rows (all steps when
+        there is none); returns that step or None"""
+        P = S.plan(tail)
+        cf, par, cptr, cols, nbord = P["col_front"], P["parent"], P["col_ptr"], P["cols"], P["nbord"]
+        nf = len(par)
+        border = np.nonzero((p_lu >= mi) & (nbord[cf] > 0))[0]
+        kmax = border[0] if len(border) else n
+        first = np.arange(nf)
+        for s in range(nf):
+            if par[s] >= 0:
+                first[par[s]] = min(first[par[s]], first[s])
+        member = sp.csr_matrix((np.ones(len(cols), bool), cols, cptr), shape=(nf, n))
+        u = Uc.row < kmax
+        assert np.all(np.asarray(member[cf[Uc.row[u]], Uc.col[u]]).ravel()), "U entry outside its front's columns"
+        off = (Lc.row != Lc.col) & (Lc.col < kmax)
+        rows = p_lu[Lc.row[off]]
+        ks = Lc.col[off]
+        interior = rows < mi
+        fb = cf[firstcol[rows[interior]]]
+        fk = cf[ks[interior]]
+        assert np.all((first[fk] <= fb) & (fb <= fk)), "L row outside its front's subtree"
+        return border[0] if len(border) else None
+
+    b = check(-1)
+    if b is not None:
+        P = S.plan(-1)
+        s = P["col_front"][b]
+        f0 = int(np.nonzero(P["col_front"] == s)[0][0])
+        assert check(f0) is None
+
+
+# ------------------------------------------------------------------------------------------------ multi-process (gloo)
+def _replica_worker(rank, world, port, out):
+    import torch.distributed as dist
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        out[rank] = bench.allreduce_max(float(10 + rank), "cpu")
+    finally:
+        dist.destroy_process_group()
+
+
+def test_replica_timing_is_the_max_over_ranks():
+    """bench.py --gpus N runs N independent replicas (one factorization does not shard); the reported time is the
+    slowest rank's, reduced the same way on every rank (two gloo ranks on CPU)."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.start_processes(_replica_worker, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
+    assert dict(out) == {0: 11.0, 1: 11.0}
