@@ -350,7 +350,7 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
                  : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
 }
 
-constexpr int GBM = 64, GBN = 64, GBK = 16, GPAD = 68;
+constexpr int GBM = 64, GBN = 64, GBK = 16, GPAD = 68, GBP = 20;   // A staged [k][m] (row 68), B staged [n][k] (row 20)
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_gemm_sub(int64_t M, int64_t N, int64_t K, const T *__restrict__ A, int64_t lda,
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(256) k_gemm_sub(int64_t M, int64_t N, int64_t 
 {
     constexpr bool CP = VT<T>::cplx_;
     __shared__ double As[CP ? 2 : 1][GBK][GPAD];
-    __shared__ double Bs[CP ? 3 : 1][GBK][GPAD];
+    __shared__ double Bs[CP ? 3 : 1][GBN][GBP];
     if (st->code) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 1, wn = warp >> 1;
@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(256) k_gemm_sub(int64_t M, int64_t N, int64_t 
             const int k = tid & 15, nn = (tid >> 4) + 16 * i;
             const int64_t gk = k0 + k, gn = n0 + nn;
             T v = (gk < K && gn < N) ? B[gk + gn * ldb] : VT<T>::zero();
-            if constexpr (CP) { Bs[0][k][nn] = v.x; Bs[1][k][nn] = v.y; Bs[2][k][nn] = -v.y; } else Bs[0][k][nn] = v;
+            if constexpr (CP) { Bs[0][nn][k] = v.x; Bs[1][nn][k] = v.y; Bs[2][nn][k] = -v.y; } else Bs[0][nn][k] = v;
         }
         __syncthreads();
 #pragma unroll
@@ -401,8 +401,8 @@ __global__ void __launch_bounds__(256) k_gemm_sub(int64_t M, int64_t N, int64_t 
 #pragma unroll
             for (int b = 0; b < 2; b++) {
                 const int nn = wn * 16 + b * 8 + (lane >> 2);
-                br[b] = Bs[0][kr][nn];
-                if constexpr (CP) { bi[b] = Bs[1][kr][nn]; bn[b] = Bs[2][kr][nn]; }
+                br[b] = Bs[0][nn][kr];
+                if constexpr (CP) { bi[b] = Bs[1][nn][kr]; bn[b] = Bs[2][nn][kr]; }
             }
 #pragma unroll
             for (int a = 0; a < 4; a++)
@@ -555,6 +555,184 @@ __global__ void __launch_bounds__(1024) k_front_lu(const T *__restrict__ W, int6
     }
 }
 
+// 1 / p for the pivot: conj(p) / |p|^2 with the components scaled by max(|re|, |im|) first (no overflow or underflow of the
+// squares); real: 1 / p
+__device__ __forceinline__ double recip(double p) { return 1.0 / p; }
+__device__ __forceinline__ cplx recip(cplx p)
+{
+    const double q = p.x * p.x + p.y * p.y;
+    if (q > 1e-300 && q < 1e300) { const double d = 1.0 / q; return cplx{p.x * d, -p.y * d}; }
+    const double s = fmax(fabs(p.x), fabs(p.y)), is = 1.0 / s;          // scaled: no overflow or underflow
+    const double a = p.x * is, b = p.y * is, d = 1.0 / (a * a + b * b);
+    return cplx{a * d * is, -b * d * is};
+}
+
+// The pivot of column j among the rows not pivoted before step j (tag >= j), by one warp: each lane's best (largest
+// squared modulus, ties to the smaller row of B) over its rows, the warp's maximum by shuffles, then the winning lane by
+// ballot (exact ties between lanes resolved by the smaller row of B).  Returns the local row, -1 when none.
+template <typename T>
+__device__ __forceinline__ int warp_argmax(const T *__restrict__ col, const int *__restrict__ tag, const int64_t *__restrict__ rid,
+                                           int nrows, int j, int lane)
+{
+    double bv = -1.0; int bi = -1; int64_t br = INT64_MAX;
+    for (int i = lane; i < nrows; i += 32) {
+        if (tag[i] < j) continue;
+        const double a = sqmod(col[i]);
+        const int64_t r = rid[i];
+        if (a > bv || (a == bv && r < br)) { bv = a; bi = i; br = r; }
+    }
+    double m = bv;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    unsigned cand = __ballot_sync(0xffffffffu, bi >= 0 && bv == m);
+    if (cand == 0) return -1;
+    if ((cand & (cand - 1)) != 0) {            // an exact tie between lanes: the smallest row of B among them
+        int64_t rr = (cand >> lane) & 1u ? br : INT64_MAX;
+        for (int o = 16; o > 0; o >>= 1) { int64_t t = __shfl_xor_sync(0xffffffffu, rr, o); rr = t < rr ? t : rr; }
+        cand = __ballot_sync(0xffffffffu, ((cand >> lane) & 1u) && br == rr);
+    }
+    return __shfl_sync(0xffffffffu, bi, __ffs(cand) - 1);
+}
+
+// Partial-pivot LU of a front's pivot block in shared memory, with a pivot warp and one-column look-ahead (one CTA of
+// up to 1024 threads).  Warp 0 owns the critical path: at step j it updates column j + 1 for every row with the step-j
+// multipliers and, in the same pass, finds the pivot of column j + 1 (largest squared modulus, ties to the smaller row
+// of B), then publishes the row and 1 / pivot (double-buffered slots).  The other warps update columns j + 2 .. with the
+// step-j pivot meanwhile, keep the multipliers (double-buffered) and store those of step j - 1 into column j - 1 (no
+// longer read by anyone).  One barrier per step.  No row swaps: the pivot row of step j is tagged j.  The singular test
+// uses the column thresholds staged in shared memory (squared moduli; the modulus itself near the threshold).
+template <typename T>
+__global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
+                                                    int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
+                                                    int64_t *__restrict__ rowid, T *__restrict__ Lout, int *__restrict__ perm,
+                                                    int64_t *__restrict__ p_lu, DevStatus *st, int64_t front)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *A = reinterpret_cast<T *>(smem_raw);                        // npiv x nrows, column-major: A[c * nrows + i]
+    T *lcol = A + (size_t)npiv * nrows;                            // 2 x nrows: multipliers of steps j (j & 1)
+    int64_t *rid = reinterpret_cast<int64_t *>(lcol + 2 * nrows);
+    double *thr = reinterpret_cast<double *>(rid + nrows);         // npiv: pivot_rel * max |B(:, column)|
+    int *tag = reinterpret_cast<int *>(thr + npiv);
+    int *pos = tag + nrows;
+    __shared__ int s_bi[2], s_stop;
+    __shared__ T s_inv[2];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
+    for (int c = 0; c < npiv; c++)
+        for (int i = tid; i < nrows; i += nt) A[(size_t)c * nrows + i] = W[i + (int64_t)c * ld];
+    for (int i = tid; i < nrows; i += nt) { rid[i] = rowid[i]; tag[i] = INT_MAX; }
+    for (int c = tid; c < npiv; c += nt) thr[c] = pivot_rel * colmax[fcol + c];
+    if (tid == 0) s_stop = st->code != 0 ? 3 : 0;
+    __syncthreads();
+    if (s_stop) return;
+    const int nu = nt - 32, ut = tid - 32;                          // update threads: warps 1 ..
+    const int R = (nrows + 31) & ~31;
+    const int G = nu >= R ? nu / R : 1, rstep = nu >= R ? R : nu;
+    const int my_i = ut >= 0 ? (nu >= R ? ut % R : ut) : 0, my_g = ut >= 0 ? (nu >= R ? ut / R : 0) : G;
+    const bool upd = ut >= 0 && my_g < G;
+    // warp 0: decide on the winner (bi, squared modulus bv2) of column j, publish into slot
+    auto decide = [&](int j, int bi, double bv2, int slot) {
+        if (lane != 0) return;
+        const double t = thr[j];
+        int stop = 0;
+        bool sing = bi < 0 || !(bv2 > 0.0);
+        if (!sing && bv2 < 4.0 * t * t) sing = vabs(A[(size_t)j * nrows + bi]) < t;      // near the threshold: the modulus
+        if (sing) { const double bv = bi >= 0 ? vabs(A[(size_t)j * nrows + bi]) : 0.0; set_status(st, ST_SINGULAR, fcol + j, bv, t); stop = 1; }
+        else if (bi >= nri) { set_status(st, ST_BORDER, front, sqrt(bv2), t); stop = 1; }
+        s_bi[slot] = bi;
+        if (!stop) { s_inv[slot] = recip(A[(size_t)j * nrows + bi]); tag[bi] = j; }
+        else s_stop = 1;
+    };
+    auto reduce = [&](double bv, int bi, int64_t br, double *bv2_out) -> int {
+        double m = bv;
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        unsigned cand = __ballot_sync(0xffffffffu, bi >= 0 && bv == m);
+        *bv2_out = m;
+        if (cand == 0) return -1;
+        if ((cand & (cand - 1)) != 0) {
+            int64_t rr = (cand >> lane) & 1u ? br : INT64_MAX;
+            for (int o = 16; o > 0; o >>= 1) { int64_t t = __shfl_xor_sync(0xffffffffu, rr, o); rr = t < rr ? t : rr; }
+            cand = __ballot_sync(0xffffffffu, ((cand >> lane) & 1u) && br == rr);
+        }
+        return __shfl_sync(0xffffffffu, bi, __ffs(cand) - 1);
+    };
+    if (warp == 0) {
+        double bv = -1.0; int bi = -1; int64_t br = INT64_MAX;
+        for (int i = lane; i < nrows; i += 32) {
+            const double a = sqmod(A[i]);
+            const int64_t r = rid[i];
+            if (a > bv || (a == bv && r < br)) { bv = a; bi = i; br = r; }
+        }
+        double m;
+        const int w = reduce(bv, bi, br, &m);
+        decide(0, w, m, 0);
+    }
+    __syncthreads();
+    for (int j = 0; j < npiv; j++) {
+        if (s_stop) return;
+        const int bi = s_bi[j & 1];
+        const T inv = s_inv[j & 1];
+        if (warp == 0) {
+            if (j + 1 < npiv) {
+                // column j + 1 for every row not yet pivoted, and its pivot, in one pass
+                const T pr = A[(size_t)(j + 1) * nrows + bi];
+                const T *cj = A + (size_t)j * nrows;
+                T *cn = A + (size_t)(j + 1) * nrows;
+                double bv = -1.0; int wi = -1; int64_t br = INT64_MAX;
+#pragma unroll 4
+                for (int i = lane; i < nrows; i += 32) {
+                    if (tag[i] <= j) continue;
+                    const T x = sub(cn[i], mul(mul(cj[i], inv), pr));
+                    cn[i] = x;
+                    const double a = sqmod(x);
+                    const int64_t r = rid[i];
+                    if (a > bv || (a == bv && r < br)) { bv = a; wi = i; br = r; }
+                }
+                double m;
+                const int w = reduce(bv, wi, br, &m);
+                decide(j + 1, w, m, (j + 1) & 1);
+            }
+        } else if (upd) {
+            T *lc = lcol + (j & 1) * nrows;
+            const T *lp = lcol + ((j + 1) & 1) * nrows;
+            for (int i = my_i; i < nrows; i += rstep) {
+                if (my_g == 0 && j > 0 && tag[i] >= j) A[(size_t)(j - 1) * nrows + i] = lp[i];   // step j - 1's multiplier
+                if (tag[i] <= j) continue;
+                const T l = mul(A[(size_t)j * nrows + i], inv);
+                if (my_g == 0) lc[i] = l;
+                for (int c = j + 2 + my_g; c < npiv; c += G) {
+                    T *x = A + (size_t)c * nrows + i;
+                    *x = sub(*x, mul(l, A[(size_t)c * nrows + bi]));
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // the last step's multipliers
+    if (upd && my_g == 0 && npiv > 0) {
+        const T *lp = lcol + ((npiv - 1) & 1) * nrows;
+        for (int i = my_i; i < nrows; i += rstep) if (tag[i] >= npiv) A[(size_t)(npiv - 1) * nrows + i] = lp[i];
+    }
+    const int steps = npiv;
+    if (warp == 0) {
+        int base = steps;
+        for (int i0 = 0; i0 < nrows; i0 += 32) {
+            const int i = i0 + lane;
+            const bool un = i < nrows && tag[i] >= steps;
+            const unsigned m = __ballot_sync(0xffffffffu, un);
+            if (i < nrows) pos[i] = un ? base + __popc(m & ((1u << lane) - 1u)) : tag[i];
+            base += __popc(m);
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < nrows; i += nt) {
+        const int k = pos[i];
+        perm[k] = i;
+        rowid[k] = rid[i];
+        if (k < steps) p_lu[fcol + k] = rid[i];
+    }
+    for (int c = 0; c < npiv; c++)
+        for (int i = tid; i < nrows; i += nt) Lout[pos[i] + (int64_t)c * nrows] = A[(size_t)c * nrows + i];
+}
+
 // After the blocked (global-memory) pivoting of a large front's pivot block: the final row order from the swaps, the
 // pivot rows (the swaps already moved the row ids), and the block into the arena
 template <typename T>
@@ -625,6 +803,78 @@ __global__ void __launch_bounds__(256) k_u12_fused(const T *__restrict__ W, int6
         T *u = U + c * npiv;
 #pragma unroll
         for (int q = 0; q < RPL; q++) { const int r = lane + 32 * q; if (r < npiv) u[r] = x[q]; }
+    }
+}
+
+// U12 = L11^-1 A12[perm] for npiv <= 64, by column tiles of 32 in shared memory (persistent CTAs: L11 staged once per
+// CTA): the tile's pivot rows are gathered through perm; then per 16-row block, the diagonal 16 x 16 solve by half-warps
+// (one column each, 16 shuffle steps) and the update of the rows below from shared memory by the whole CTA; the tile
+// leaves for the arena.  The same operations as a blocked forward substitution.
+constexpr int U12_TN = 32, U12_NP = 64, U12_BK = 16;
+template <typename T>
+__global__ void __launch_bounds__(256) k_u12_blk(const T *__restrict__ W, int64_t ld, const int *__restrict__ perm, int npiv,
+                                                 int64_t ncb, const T *__restrict__ Lb, int64_t ldl, T *__restrict__ U,
+                                                 const DevStatus *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *sL = reinterpret_cast<T *>(smem_raw);                 // U12_NP x U12_NP, column-major (ld U12_NP)
+    T *X = sL + U12_NP * U12_NP;                             // U12_NP x U12_TN, column-major (ld U12_NP)
+    __shared__ int sperm[U12_NP];
+    if (st->code) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < U12_NP * U12_NP; e += blockDim.x) {
+        const int r = e % U12_NP, c = e / U12_NP;
+        sL[e] = (r < npiv && c < npiv) ? Lb[r + (int64_t)c * ldl] : VT<T>::zero();
+    }
+    for (int i = tid; i < U12_NP; i += blockDim.x) sperm[i] = i < npiv ? perm[i] : 0;
+    __syncthreads();
+    const int64_t ntile = (ncb + U12_TN - 1) / U12_TN;
+    const int nb = (npiv + U12_BK - 1) / U12_BK;
+    const int half = lane >> 4, hl = lane & 15;
+    for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x) {
+        const int64_t c0 = t * U12_TN;
+        const int tn = (int)(ncb - c0 < U12_TN ? ncb - c0 : U12_TN);
+        for (int e = tid; e < U12_NP * U12_TN; e += blockDim.x) {
+            const int r = e % U12_NP, c = e / U12_NP;
+            X[e] = (r < npiv && c < tn) ? W[sperm[r] + (npiv + c0 + c) * ld] : VT<T>::zero();
+        }
+        __syncthreads();
+        for (int b = 0; b < nb; b++) {
+            const int r0 = b * U12_BK, w = npiv - r0 < U12_BK ? npiv - r0 : U12_BK;
+            // the diagonal block: a half-warp per column (both halves of a warp step through the column pairs together,
+            // so every shuffle has the full warp), lane hl holds row r0 + hl
+            for (int cp = warp; 2 * cp < tn; cp += blockDim.x >> 5) {
+                const int c = 2 * cp + half;
+                const bool act = c < tn;
+                T x = act ? X[r0 + hl + c * U12_NP] : VT<T>::zero();
+                for (int i = 0; i < w; i++) {
+                    T xi;
+                    if constexpr (VT<T>::cplx_) xi = T{__shfl_sync(0xffffffffu, x.x, i, 16), __shfl_sync(0xffffffffu, x.y, i, 16)};
+                    else xi = __shfl_sync(0xffffffffu, x, i, 16);
+                    if (hl > i && hl < w) x = sub(x, mul(sL[r0 + hl + (r0 + i) * U12_NP], xi));
+                }
+                if (act && hl < w) X[r0 + hl + c * U12_NP] = x;
+            }
+            __syncthreads();
+            // the rows below: X[r, c] -= sum_k L[r, r0 + k] X[r0 + k, c]
+            const int rb = r0 + w;
+            if (rb < npiv) {
+                const int mrows = npiv - rb;
+                for (int e = tid; e < mrows * tn; e += blockDim.x) {
+                    const int r = rb + e % mrows, c = e / mrows;
+                    T acc = VT<T>::zero();
+#pragma unroll 4
+                    for (int kk = 0; kk < w; kk++) acc = add(acc, mul(sL[r + (r0 + kk) * U12_NP], X[r0 + kk + c * U12_NP]));
+                    X[r + c * U12_NP] = sub(X[r + c * U12_NP], acc);
+                }
+            }
+            __syncthreads();
+        }
+        for (int e = tid; e < npiv * tn; e += blockDim.x) {
+            const int r = e % npiv, c = e / npiv;
+            U[r + (c0 + c) * (int64_t)npiv] = X[r + c * U12_NP];
+        }
+        __syncthreads();
     }
 }
 

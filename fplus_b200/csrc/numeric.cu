@@ -245,7 +245,7 @@ static int run_equil(const DevPlan &D, DevNum &N, int equilibrate, int max_iter,
 
 // ---------------------------------------------------------------------------------------------------------------------
 // the fronts, in order.  Returns FPLUS_OK, or ST_BORDER through *border_front (>= 0) for a restart with a dense chain.
-static size_t front_lu_smem(int64_t nrows, int64_t npiv, int64_t vs) { return (size_t)(nrows * npiv * vs + nrows * (vs + 16)); }
+static size_t front_lu_smem(int64_t nrows, int64_t npiv, int64_t vs) { return (size_t)(nrows * npiv * vs + nrows * (2 * vs + 16) + npiv * 8); }
 static const size_t SMEM_MAX = 220 * 1024;   // dynamic shared memory opt-in, below the 227 KB per-block limit (static smem on top)
 
 template <typename T>
@@ -266,8 +266,10 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     static thread_local int attr_set = 0;
     if (!attr_set) {
         CK(cudaFuncSetAttribute(k_front_lu<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_front_lu2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_u12_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_u12_fused<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_u12_fused<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_u12_fused<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
@@ -314,8 +316,9 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         }
         if (sm <= SMEM_MAX) {
             const int R = (int)((nr + 31) & ~31);
-            int nt = R <= 256 ? 256 : (R < 1024 ? R : 1024);
-            k_front_lu<T><<<1, nt, sm, s>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel, N.rowid + F.row_off, Lf,
+            int nt = 32 + (R <= 128 ? 4 * R : (R <= 480 ? R : 992));   // the pivot warp + the update warps
+            if (nt > 1024) nt = 1024;
+            k_front_lu2<T><<<1, nt, sm, s>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel, N.rowid + F.row_off, Lf,
                                            N.perm, N.p_lu, N.st, fi), note_launch();
         } else {
             const int64_t npr = std::min(np, nr);
@@ -346,14 +349,11 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         T *Uf = Ua + F.U_off;
         prof.begin(s, PROF_U12, fm * (double)np * (double)np / 2.0 * (double)ncb, 3.0 * (double)(np * ncb) * vs);
         const int64_t npr = std::min(np, nr);
-        const int rpl_max = VT<T>::cplx_ ? 2 : 4;        // L11 in shared memory: 64 x 64 complex or 128 x 128 real
-        if (npr == np && np <= 32 * rpl_max) {
-            const size_t tsm = (size_t)np * np * vs;
-            const int nwarps = (int)std::min<int64_t>(ncb, 148 * 64);
-            const int blocks = (nwarps + 7) / 8;
-            if (np <= 32) k_u12_fused<T, 1><<<blocks, 256, tsm, s>>>(W, ld, N.perm, (int)np, ncb, Lf, ld, Uf, N.st), note_launch();
-            else if (np <= 64) k_u12_fused<T, 2><<<blocks, 256, tsm, s>>>(W, ld, N.perm, (int)np, ncb, Lf, ld, Uf, N.st), note_launch();
-            else k_u12_fused<T, 4><<<blocks, 256, tsm, s>>>(W, ld, N.perm, (int)np, ncb, Lf, ld, Uf, N.st), note_launch();
+        if (npr == np && np <= U12_NP) {
+            // gather + blocked TRSM of 32-column tiles in shared memory; persistent CTAs (L11 staged once per CTA)
+            const size_t tsm = (size_t)(U12_NP * U12_NP + U12_NP * U12_TN) * vs;
+            const int blocks = (int)std::min<int64_t>((ncb + U12_TN - 1) / U12_TN, 2 * 148);
+            k_u12_blk<T><<<blocks, 256, tsm, s>>>(W, ld, N.perm, (int)np, ncb, Lf, ld, Uf, N.st), note_launch();
         } else {
         k_u12_gather<T><<<nblk(np * ncb), 256, 0, s>>>(W, ld, np, ncb, N.perm, Uf, N.st), note_launch();
         for (int64_t k0 = 0; k0 < npr; k0 += TB) {
