@@ -555,6 +555,13 @@ __global__ void __launch_bounds__(1024) k_front_lu(const T *__restrict__ W, int6
     }
 }
 
+template <typename T> __device__ __forceinline__ T shfl_v(T v, int src);
+template <> __device__ __forceinline__ double shfl_v<double>(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+template <> __device__ __forceinline__ cplx shfl_v<cplx>(cplx v, int src)
+{
+    return cplx{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
+}
+
 // 1 / p for the pivot: conj(p) / |p|^2 with the components scaled by max(|re|, |im|) first (no overflow or underflow of the
 // squares); real: 1 / p
 __device__ __forceinline__ double recip(double p) { return 1.0 / p; }
@@ -672,19 +679,37 @@ __global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int
         const T inv = s_inv[j & 1];
         if (warp == 0) {
             if (j + 1 < npiv) {
-                // column j + 1 for every row not yet pivoted, and its pivot, in one pass
+                // column j + 1 for every row not yet pivoted, and its pivot, in one pass: the row slots of a lane are
+                // independent (loads first, then the arithmetic), 4 slots per round
                 const T pr = A[(size_t)(j + 1) * nrows + bi];
                 const T *cj = A + (size_t)j * nrows;
                 T *cn = A + (size_t)(j + 1) * nrows;
                 double bv = -1.0; int wi = -1; int64_t br = INT64_MAX;
-#pragma unroll 4
-                for (int i = lane; i < nrows; i += 32) {
-                    if (tag[i] <= j) continue;
-                    const T x = sub(cn[i], mul(mul(cj[i], inv), pr));
-                    cn[i] = x;
-                    const double a = sqmod(x);
-                    const int64_t r = rid[i];
-                    if (a > bv || (a == bv && r < br)) { bv = a; wi = i; br = r; }
+                for (int i0 = lane; i0 < nrows; i0 += 128) {
+                    T xa[4], xb[4];
+                    bool ok[4];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int i = i0 + 32 * q;
+                        ok[q] = i < nrows && tag[i] > j;
+                        xa[q] = ok[q] ? cj[i] : VT<T>::zero();
+                        xb[q] = ok[q] ? cn[i] : VT<T>::zero();
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const T x = sub(xb[q], mul(mul(xa[q], inv), pr));
+                        xb[q] = x;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int i = i0 + 32 * q;
+                        if (ok[q]) {
+                            cn[i] = xb[q];
+                            const double a = sqmod(xb[q]);
+                            const int64_t r = rid[i];
+                            if (a > bv || (a == bv && r < br)) { bv = a; wi = i; br = r; }
+                        }
+                    }
                 }
                 double m;
                 const int w = reduce(bv, wi, br, &m);
@@ -698,7 +723,18 @@ __global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int
                 if (tag[i] <= j) continue;
                 const T l = mul(A[(size_t)j * nrows + i], inv);
                 if (my_g == 0) lc[i] = l;
-                for (int c = j + 2 + my_g; c < npiv; c += G) {
+                int c = j + 2 + my_g;
+                for (; c + 3 * G < npiv; c += 4 * G) {          // 4 independent columns per round, loads first
+                    T xv[4], pv[4];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        xv[q] = A[(size_t)(c + q * G) * nrows + i];
+                        pv[q] = A[(size_t)(c + q * G) * nrows + bi];
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; q++) A[(size_t)(c + q * G) * nrows + i] = sub(xv[q], mul(l, pv[q]));
+                }
+                for (; c < npiv; c += G) {
                     T *x = A + (size_t)c * nrows + i;
                     *x = sub(*x, mul(l, A[(size_t)c * nrows + bi]));
                 }
@@ -761,13 +797,6 @@ __global__ void k_u12_gather(const T *__restrict__ W, int64_t ld, int64_t npiv, 
         const int64_t i = e % npiv, c = e / npiv;
         U[e] = W[perm[i] + (npiv + c) * ld];
     }
-}
-
-template <typename T> __device__ __forceinline__ T shfl_v(T v, int src);
-template <> __device__ __forceinline__ double shfl_v<double>(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
-template <> __device__ __forceinline__ cplx shfl_v<cplx>(cplx v, int src)
-{
-    return cplx{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
 }
 
 // U12 = L11^-1 A12[perm] in one pass for npiv <= 32 RPL: a warp per column gathers the pivot rows of the column
@@ -1067,13 +1096,18 @@ __global__ void __launch_bounds__(256) k_bwdU(const T *__restrict__ L, int64_t n
         for (int64_t q = 0; q < nchunk; q++) v = sub(v, part[q * npiv * nrhs + e]);
         s[e] = v;
     }
+    T *dinv = s + npiv * nrhs;                        // 1 / U[i, i], computed in parallel
+    for (int64_t i = threadIdx.x; i < npiv; i += blockDim.x) {
+        const T d = L[i + i * nrows];
+        if (is_zero(d)) set_status(st, ST_SOLVE_ZERO, f + i, 0, 0);
+        dinv[i] = is_zero(d) ? VT<T>::zero() : recip(d);
+    }
     __syncthreads();
+    if (st->code == ST_SOLVE_ZERO) return;
     for (int64_t r = warp; r < nrhs; r += nw) {
         T *sr = s + r * npiv;
         for (int64_t i = npiv - 1; i >= 0; i--) {
-            const T d = L[i + i * nrows];
-            if (is_zero(d)) { if (lane == 0) set_status(st, ST_SOLVE_ZERO, f + i, 0, 0); break; }
-            const T xi = divv(sr[i], d);
+            const T xi = mul(sr[i], dinv[i]);
             __syncwarp();
             if (lane == 0) sr[i] = xi;
             for (int64_t j = lane; j < i; j += 32) sr[j] = sub(sr[j], mul(L[j + i * nrows], xi));
@@ -1093,14 +1127,21 @@ template <typename T, bool CJ>
 __global__ void __launch_bounds__(256) k_fwdUt2(const T *__restrict__ L, int64_t nrows, int64_t npiv, int64_t f,
                                                 T *__restrict__ Wc, int64_t n, int64_t nrhs, DevStatus *st)
 {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *dinv = reinterpret_cast<T *>(smem_raw);         // 1 / U[i, i] (conjugated for U^H), computed in parallel
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int64_t i = threadIdx.x; i < npiv; i += blockDim.x) {
+        T d = L[i + i * nrows];
+        if (CJ) d = conjv(d);
+        if (is_zero(d)) set_status(st, ST_SOLVE_ZERO, f + i, 0, 0);
+        dinv[i] = is_zero(d) ? VT<T>::zero() : recip(d);
+    }
+    __syncthreads();
+    if (st->code == ST_SOLVE_ZERO) return;
     for (int64_t r = warp; r < nrhs; r += nw) {
         T *w = Wc + f + r * n;
         for (int64_t i = 0; i < npiv; i++) {
-            T d = L[i + i * nrows];
-            if (CJ) d = conjv(d);
-            if (is_zero(d)) { if (lane == 0) set_status(st, ST_SOLVE_ZERO, f + i, 0, 0); break; }
-            const T zi = divv(w[i], d);
+            const T zi = mul(w[i], dinv[i]);
             __syncwarp();
             if (lane == 0) w[i] = zi;
             for (int64_t j = i + 1 + lane; j < npiv; j += 32) {

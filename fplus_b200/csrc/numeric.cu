@@ -431,7 +431,7 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
     T *R = (T *)N.rbuf, *S2 = (T *)N.sbuf, *part = (T *)N.part;
     const T *La = (const T *)N.Larena, *Ua = (const T *)N.Uarena;
     const int64_t nf = (int64_t)P.fronts.size();
-    const size_t smem = (size_t)P.max_npiv * (size_t)nrhs * sizeof(T);
+    const size_t smem = (size_t)P.max_npiv * (size_t)(nrhs + 1) * sizeof(T);
     CK(cudaFuncSetAttribute(k_fwdL2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
     CK(cudaFuncSetAttribute(k_u12_gemv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
     if (smem > 48 * 1024) {
@@ -463,7 +463,7 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
                 k_u12_gemv<T><<<(unsigned)nchunk, 256, (size_t)8 * F.npiv * sizeof(T), s>>>(
                     Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, R, n, nrhs, chunk, part), note_launch();
             }
-            k_bwdU<T><<<1, 256, (size_t)F.npiv * nrhs * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, part, nchunk, S2, R,
+            k_bwdU<T><<<1, 256, (size_t)F.npiv * (nrhs + 1) * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, part, nchunk, S2, R,
                                                                          n, nrhs, N.st), note_launch();
         }
         // x[col_perm[k]] = Dcp[k] * R[k]
@@ -476,8 +476,8 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
             const Front &F = P.fronts[fi];
             const int64_t ncb = F.ncols - F.npiv;
             if (F.npiv == 0) continue;
-            if (cj) k_fwdUt2<T, true><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
-            else k_fwdUt2<T, false><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
+            if (cj) k_fwdUt2<T, true><<<1, 256, (size_t)F.npiv * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
+            else k_fwdUt2<T, false><<<1, 256, (size_t)F.npiv * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
             if (ncb > 0) {
                 if (cj) k_ut_scatter<T, true><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, F.f, R, n, nrhs), note_launch();
                 else k_ut_scatter<T, false><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, F.f, R, n, nrhs), note_launch();
