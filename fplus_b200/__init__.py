@@ -59,7 +59,7 @@ FPLUS_H_SYMBOLS = [
 FPLUS_B200_H_SYMBOLS = [
     "fplus_b200_numeric_info", "fplus_b200_use_stream", "fplus_b200_factor_dev", "fplus_b200_solve_dev",
     "fplus_b200_interior_order", "fplus_b200_plan_size", "fplus_b200_plan_export", "fplus_b200_launch_count",
-    "fplus_b200_profile", "fplus_b200_profile_read",
+    "fplus_b200_profile", "fplus_b200_profile_read", "fplus_b200_solve_dev_noalloc",
 ]
 
 _lib = None
@@ -95,6 +95,7 @@ def lib():
     L.fplus_solve.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_char_p,
                               ctypes.c_size_t]
     L.fplus_b200_solve_dev.argtypes = L.fplus_solve.argtypes
+    L.fplus_b200_solve_dev_noalloc.argtypes = L.fplus_solve.argtypes
     L.fplus_numeric_factors.argtypes = [ctypes.c_void_p]
     L.fplus_numeric_factors.restype = ctypes.POINTER(Factors)
     for f in ("fplus_numeric_p", "fplus_numeric_q"):

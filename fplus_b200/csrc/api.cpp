@@ -409,3 +409,29 @@ extern "C" int fplus_b200_profile_read(int cls, double *ms, long long *count, do
     if (bytes) *bytes = c.bytes;
     return FPLUS_OK;
 }
+
+// The allocation-free solve: see include/fplus_b200.h.  The status word read afterwards belongs to the factorization.
+extern "C" int fplus_b200_solve_dev_noalloc(const fplus_numeric *num, void *b_dev, int64_t nrhs, int64_t ldb, int trans,
+                                            char *err, size_t errlen)
+{
+    if (!num) { errf(err, errlen, "fplus_b200_solve_dev_noalloc: num is NULL"); return FPLUS_ERR_BADARG; }
+    const int64_t n = num->n;
+    if (trans < 0 || trans > 2 || nrhs < 0 || ldb < n) { errf(err, errlen, "fplus_b200_solve_dev_noalloc: bad trans, nrhs or ldb"); return FPLUS_ERR_BADARG; }
+    if (nrhs == 0 || n == 0) return FPLUS_OK;
+    if (!b_dev) { errf(err, errlen, "fplus_b200_solve_dev_noalloc: b is NULL"); return FPLUS_ERR_BADARG; }
+    std::lock_guard<std::mutex> lk(num->mu);
+    DevNum &N = *num->dev;
+    CKH(cudaSetDevice(N.device));
+    cudaStream_t s = tl_stream ? tl_stream : N.stream;
+    cudaStream_t saved = N.stream;
+    N.stream = s;
+    int rc = dev_clear_status(N, err, errlen);
+    if (rc == FPLUS_OK) rc = dev_solve_noalloc(*num->plan, *num->dplan, N, b_dev, ldb, nrhs, trans, s, err, errlen);
+    if (rc == FPLUS_OK) {
+        int code = 0; int64_t idx = 0;
+        rc = dev_status(N, &code, &idx, err, errlen);
+        if (rc == FPLUS_OK && code != 0) { errf(err, errlen, "fplus_b200_solve_dev_noalloc: zero or missing diagonal in U"); rc = FPLUS_ERR_SINGULAR; }
+    }
+    N.stream = saved;
+    return rc;
+}

@@ -503,6 +503,138 @@ int dev_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, void *x_dev, int6
                   : run_solve<double>(P, D, N, (double *)x_dev, nrhs, trans, err, errlen);
 }
 
+// ---------------------------------------------------------------------------------------------------------------------
+// The allocation-free solve (fplus_b200_solve_dev_noalloc).  The same kernels and launch order as run_solve, in place on
+// the caller's right-hand sides (leading dimension ldx), with the scratch vectors carved from one file-scope device array
+// instead of allocations.  Host code cannot use g_noalloc_scratch's name as a device address (it is a host-side stand-in):
+// the address comes from cudaGetSymbolAddress, once per device, with that device current.  The array keeps the last
+// call's contents; every scratch vector is written before it is read, so nothing needs clearing.  Calls share the array:
+// calls that overlap on the GPU (other streams, other host threads) race.
+static constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)16 << 20;       // 16 MiB per device, held until exit
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+static int noalloc_scratch(void **ptr, char *err, size_t errlen)
+{
+    static std::mutex mu;
+    static void *addr[64] = {nullptr};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) { errf(err, errlen, "device %d out of range", dev); return FPLUS_ERR_GPU; }
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        addr[dev] = p;
+    }
+    *ptr = addr[dev];
+    return FPLUS_OK;
+}
+
+static inline size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+static constexpr int64_t NOALLOC_GROUP = 32;                          // right-hand sides per pass (the solve kernels' width)
+
+template <typename T>
+static int run_solve_noalloc_group(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int64_t ldx, int64_t nrhs,
+                                   int trans, cudaStream_t s, char *err, size_t errlen)
+{
+    const int64_t n = N.n;
+    auto chunk_of = [](int64_t ncb) { int64_t c = (ncb + 295) / 296; return c < 32 ? (int64_t)32 : c; };
+    int64_t maxpart = 1;
+    for (const Front &F : P.fronts) {
+        const int64_t ncb = F.ncols - F.npiv;
+        if (ncb > 0) maxpart = std::max(maxpart, ((ncb + chunk_of(ncb) - 1) / chunk_of(ncb)) * F.npiv);
+    }
+    const size_t vb = round256((size_t)(n > 0 ? n : 1) * (size_t)nrhs * sizeof(T));
+    const size_t pb = round256((size_t)maxpart * (size_t)nrhs * sizeof(T));
+    const size_t need = 2 * vb + pb;
+    if (need > NOALLOC_SCRATCH_BYTES) {
+        errf(err, errlen, "fplus_b200_solve_dev_noalloc: %zu bytes of scratch needed (n = %ld, %ld right-hand sides per "
+             "pass), the fixed maximum is %zu", need, (long)n, (long)nrhs, NOALLOC_SCRATCH_BYTES);
+        return FPLUS_ERR_BADARG;
+    }
+    void *base = nullptr;
+    int rc = noalloc_scratch(&base, err, errlen);
+    if (rc) return rc;
+    T *R = (T *)base, *S2 = (T *)((char *)base + vb), *part = (T *)((char *)base + 2 * vb);
+    const T *La = (const T *)N.Larena, *Ua = (const T *)N.Uarena;
+    const int64_t nf = (int64_t)P.fronts.size();
+    const size_t smem = (size_t)P.max_npiv * (size_t)(nrhs + 1) * sizeof(T);
+    CK(cudaFuncSetAttribute(k_fwdL2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    CK(cudaFuncSetAttribute(k_u12_gemv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+    if (smem > 48 * 1024) {
+        CK(cudaFuncSetAttribute(k_bwdU<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CK(cudaFuncSetAttribute(k_bwdLt<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CK(cudaFuncSetAttribute(k_bwdLt<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    if (trans == 0) {
+        k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, ldx, D.row_perm, N.Drp, n, nrhs), note_launch();
+        for (int64_t fi = 0; fi < nf; fi++) {
+            const Front &F = P.fronts[fi];
+            if (F.npiv == 0 || F.nrows == 0) continue;
+            const size_t fsm = (size_t)F.nrows * nrhs * sizeof(T);
+            if (fsm <= 96 * 1024)
+                k_fwdL2<T><<<1, 256, fsm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs), note_launch();
+            else
+                k_fwdL<T><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs), note_launch();
+        }
+        k_gather_rows<T><<<nblk(n * nrhs), 256, 0, s>>>(S2, R, N.p_lu, n, nrhs), note_launch();
+        for (int64_t fi = nf - 1; fi >= 0; fi--) {
+            const Front &F = P.fronts[fi];
+            const int64_t ncb = F.ncols - F.npiv;
+            if (F.npiv == 0) continue;
+            int64_t nchunk = 0;
+            if (ncb > 0) {
+                const int64_t chunk = chunk_of(ncb);
+                nchunk = (ncb + chunk - 1) / chunk;
+                k_u12_gemv<T><<<(unsigned)nchunk, 256, (size_t)8 * F.npiv * sizeof(T), s>>>(
+                    Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, R, n, nrhs, chunk, part), note_launch();
+            }
+            k_bwdU<T><<<1, 256, (size_t)F.npiv * (nrhs + 1) * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, part, nchunk, S2, R,
+                                                                         n, nrhs, N.st), note_launch();
+        }
+        k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, ldx, R, D.col_perm, nullptr, N.Dcp, n, nrhs), note_launch();
+    } else {
+        k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, ldx, D.col_perm, N.Dcp, n, nrhs), note_launch();
+        const bool cj = trans == 2;
+        for (int64_t fi = 0; fi < nf; fi++) {
+            const Front &F = P.fronts[fi];
+            const int64_t ncb = F.ncols - F.npiv;
+            if (F.npiv == 0) continue;
+            if (cj) k_fwdUt2<T, true><<<1, 256, (size_t)F.npiv * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
+            else k_fwdUt2<T, false><<<1, 256, (size_t)F.npiv * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
+            if (ncb > 0) {
+                if (cj) k_ut_scatter<T, true><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, F.f, R, n, nrhs), note_launch();
+                else k_ut_scatter<T, false><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, F.f, R, n, nrhs), note_launch();
+            }
+        }
+        for (int64_t fi = nf - 1; fi >= 0; fi--) {
+            const Front &F = P.fronts[fi];
+            if (F.npiv == 0) continue;
+            const size_t sm = (size_t)F.npiv * nrhs * sizeof(T);
+            if (cj) k_bwdLt<T, true><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, N.rowid + F.row_off, N.pinv, R, S2, n, nrhs), note_launch();
+            else k_bwdLt<T, false><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, N.rowid + F.row_off, N.pinv, R, S2, n, nrhs), note_launch();
+        }
+        k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, ldx, S2, D.row_perm, N.p_lu, N.Drp, n, nrhs), note_launch();
+    }
+    CK(cudaGetLastError());
+    return FPLUS_OK;
+}
+
+int dev_solve_noalloc(const FrontPlan &P, const DevPlan &D, DevNum &N, void *b_dev, int64_t ldb, int64_t nrhs, int trans,
+                      cudaStream_t s, char *err, size_t errlen)
+{
+    const int64_t g = nrhs < NOALLOC_GROUP ? nrhs : NOALLOC_GROUP;
+    int rc = FPLUS_OK;
+    for (int64_t r0 = 0; r0 < nrhs && rc == FPLUS_OK; r0 += g) {
+        const int64_t m = nrhs - r0 < g ? nrhs - r0 : g;
+        char *bb = (char *)b_dev + (size_t)r0 * (size_t)ldb * (size_t)N.vs;
+        rc = N.cplx ? run_solve_noalloc_group<cplx>(P, D, N, (cplx *)bb, ldb, m, trans, s, err, errlen)
+                    : run_solve_noalloc_group<double>(P, D, N, (double *)bb, ldb, m, trans, s, err, errlen);
+    }
+    return rc;
+}
+
 int dev_status(DevNum &N, int *code, int64_t *idx, char *err, size_t errlen)
 {
     DevStatus h;

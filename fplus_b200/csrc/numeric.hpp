@@ -59,6 +59,8 @@ int dev_factor_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
                       char *err, size_t errlen);
 int dev_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, void *x_dev, int64_t nrhs, int trans, char *err, size_t errlen);
 int dev_status(DevNum &N, int *code, int64_t *idx, char *err, size_t errlen);
+int dev_solve_noalloc(const FrontPlan &P, const DevPlan &D, DevNum &N, void *b_dev, int64_t ldb, int64_t nrhs, int trans,
+                      cudaStream_t s, char *err, size_t errlen);
 int dev_clear_status(DevNum &N, char *err, size_t errlen);
 int dev_check_finite(DevNum &N, char *err, size_t errlen);
 int dev_ensure_x(DevNum &N, size_t bytes, char *err, size_t errlen);

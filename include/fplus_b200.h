@@ -54,6 +54,22 @@ int fplus_b200_plan_size(const fplus_symbolic *sym, int64_t tail, int64_t *nfron
 int fplus_b200_plan_export(const fplus_symbolic *sym, int64_t tail, int64_t *col_front, int64_t *parent, int64_t *col_ptr,
                            int64_t *cols, int64_t *nrows, int64_t *nbord);
 
+/* fplus_b200_solve_dev for callers that cannot allocate device memory.  No counterpart in the reference (FPLUS has no GPU
+ * solve).  Some callers may not call cudaMalloc at solve time: code running inside another runtime that owns the device
+ * memory (a framework's custom operator given only its input and output buffers), latency-critical loops in which an
+ * allocation's implicit device synchronization is not acceptable, and processes run under a fixed device-memory budget.
+ * This entry point allocates nothing: it solves in place on b_dev (nrhs right-hand sides, column-major, leading
+ * dimension ldb >= n), m = min(nrhs, 32) of them per pass, with its scratch vectors taken from one fixed array of
+ * 16 MiB that the library declares in device memory; every GPU that loads the library holds that array until the
+ * process exits.  One pass needs two n x m vectors plus the partial sums of the widest U12 product (a few npiv x m),
+ * each rounded up to 256 bytes: about n <= 32,000 real or 16,000 complex at m = 32, proportionally more with fewer
+ * right-hand sides.  A call that needs more than 16 MiB is rejected, before any work, with FPLUS_ERR_BADARG and a
+ * message giving the size needed.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress): make that first call before any stream capture.  The array is shared by every call on the
+ * device and keeps the last call's contents (every scratch value is written before it is read); calls that overlap on
+ * the GPU (from other streams or host threads) race on it: serialize them. */
+int fplus_b200_solve_dev_noalloc(const fplus_numeric *num, void *b_dev, int64_t nrhs, int64_t ldb, int trans, char *err, size_t errlen);
+
 /* Kernel launches made by this library since it was loaded (all threads). */
 long long fplus_b200_launch_count(void);
 
