@@ -64,6 +64,8 @@ struct DevStatus {
     unsigned long long res_bits;   // max |log| residual of the running iteration (bits of a non-negative double)
     int done, iters;
     unsigned long long amax_bits, amin_bits;
+    unsigned int ticket;           // CTAs of the running fused backward-sweep launch that have finished (0 between launches)
+    int pad2;
 };
 
 __device__ __forceinline__ void set_status(DevStatus *st, int code, long long idx, double best, double thr)

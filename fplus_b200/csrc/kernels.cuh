@@ -555,6 +555,31 @@ __global__ void __launch_bounds__(1024) k_front_lu(const T *__restrict__ W, int6
     }
 }
 
+// asynchronous global -> shared copies of one element (cp.async: all of a thread's copies in flight at once; completed
+// by cp_async_wait_all, then a barrier).  Both addresses aligned to the element size.
+template <typename T> __device__ __forceinline__ void cp_async_el(T *dst, const T *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(T) == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// a load that bypasses L1 (values another CTA wrote during this launch)
+__device__ __forceinline__ double ldcg_v(const double *p) { return __ldcg(p); }
+__device__ __forceinline__ cplx ldcg_v(const cplx *p)
+{
+    const double2 v = __ldcg(reinterpret_cast<const double2 *>(p));
+    return cplx{v.x, v.y};
+}
+
+template <typename T> __device__ __forceinline__ T shfl_xor_v(T v, int m);
+template <> __device__ __forceinline__ double shfl_xor_v<double>(double v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+template <> __device__ __forceinline__ cplx shfl_xor_v<cplx>(cplx v, int m)
+{
+    return cplx{__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m)};
+}
+
 template <typename T> __device__ __forceinline__ T shfl_v(T v, int src);
 template <> __device__ __forceinline__ double shfl_v<double>(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
 template <> __device__ __forceinline__ cplx shfl_v<cplx>(cplx v, int src)
@@ -1011,6 +1036,55 @@ __global__ void __launch_bounds__(256) k_fwdL2(const T *__restrict__ L, int64_t 
     for (int64_t e = threadIdx.x; e < nrows * nrhs; e += blockDim.x) Wr[rowid[e % nrows] + (e / nrows) * n] = v[e];
 }
 
+// forward sweep with L through one front (one CTA, npiv <= 64): copy the front's L block into shared memory (cp.async,
+// all copies in flight at once: the whole nrows x npiv block when `whole`, else the L11 block) while gathering the front's
+// rows of the right-hand sides; the L11 solve by a warp per right-hand side with the vector in registers (rows lane and
+// lane + 32; the pivot value broadcast by shuffle); the L21 update by the whole CTA; scatter back
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwdL3(const T *__restrict__ L, int64_t nrows, int64_t npiv,
+                                               const int64_t *__restrict__ rowid, T *__restrict__ Wr, int64_t n, int64_t nrhs,
+                                               int whole)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *v = reinterpret_cast<T *>(smem_raw);           // nrows x nrhs
+    T *sL = v + nrows * nrhs;                         // whole: nrows x np (ld nrows), else np x np (ld np)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int np = (int)(npiv < nrows ? npiv : nrows);
+    const int64_t ld = whole ? nrows : np;
+    if (whole)
+        for (int64_t e = threadIdx.x; e < nrows * np; e += blockDim.x) cp_async_el(sL + e, L + e);
+    else
+        for (int e = threadIdx.x; e < np * np; e += blockDim.x) cp_async_el(sL + e, L + (e % np) + (int64_t)(e / np) * nrows);
+    for (int64_t e = threadIdx.x; e < nrows * nrhs; e += blockDim.x) v[e] = Wr[rowid[e % nrows] + (e / nrows) * n];
+    cp_async_wait_all();
+    __syncthreads();
+    for (int64_t r = warp; r < nrhs; r += nw) {
+        T *vr = v + r * nrows;
+        T a = lane < np ? vr[lane] : VT<T>::zero();
+        T b = lane + 32 < np ? vr[lane + 32] : VT<T>::zero();
+        for (int i = 0; i < np; i++) {
+            const T xi = shfl_v<T>(i < 32 ? a : b, i & 31);
+            const T *col = sL + i * ld;
+            if (lane > i && lane < np) a = sub(a, mul(col[lane], xi));
+            if (lane + 32 > i && lane + 32 < np) b = sub(b, mul(col[lane + 32], xi));
+        }
+        if (lane < np) vr[lane] = a;
+        if (lane + 32 < np) vr[lane + 32] = b;
+    }
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < (nrows - np) * nrhs; e += blockDim.x) {
+        const int64_t rr = np + e % (nrows - np), r = e / (nrows - np);
+        T acc = VT<T>::zero();
+        if (whole)
+            for (int i = 0; i < np; i++) acc = add(acc, mul(sL[rr + i * nrows], v[i + r * nrows]));
+        else
+            for (int64_t i = 0; i < np; i++) acc = add(acc, mul(L[rr + i * nrows], v[i + r * nrows]));
+        v[rr + r * nrows] = sub(v[rr + r * nrows], acc);
+    }
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < nrows * nrhs; e += blockDim.x) Wr[rowid[e % nrows] + (e / nrows) * n] = v[e];
+}
+
 // forward sweep with L through one front in shared memory (one CTA): gather the front's rows of the right-hand sides,
 // eliminate column by column, scatter back
 template <typename T>
@@ -1118,6 +1192,180 @@ __global__ void __launch_bounds__(256) k_bwdU(const T *__restrict__ L, int64_t n
     for (int64_t e = threadIdx.x; e < npiv * nrhs; e += blockDim.x) {
         const int64_t i = e % npiv, r = e / npiv;
         X[f + i + r * n] = s[e];
+    }
+}
+
+// backward sweep with U through one front, in one launch.  Every CTA forms the partial products U12[:, chunk] x_cb of its
+// chunk of contribution-block columns, for blocks of up to 8 right-hand sides: thread (row i = tid % 64, column group
+// tid / 64) reads U12 in double-buffered batches of 16 columns (32 loads in flight per thread; each U12 entry read once
+// per block of right-hand sides), the x values of a 256-column tile staged in shared memory.  The last CTA to finish (the
+// status word's ticket, after a fence) copies U11 into shared memory (cp.async) while it sums the partials in chunk order,
+// subtracts them from y and solves with U11: a warp per right-hand side with the vector in registers (npiv <= 64), else
+// in shared memory.  The ticket is returned to 0 for the next launch.
+template <typename T>
+__global__ void __launch_bounds__(256) k_bwdU_fused(const T *__restrict__ L, int64_t nrows, int64_t npiv, int64_t f,
+                                                    const T *__restrict__ U12, int64_t ncb, const int64_t *__restrict__ cbcols,
+                                                    int64_t chunk, T *__restrict__ part, const T *__restrict__ Y,
+                                                    T *__restrict__ X, int64_t n, int64_t nrhs, DevStatus *st)
+{
+    constexpr int RB = 8, CT = 256, UB = 16;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int last;
+    const int tid = threadIdx.x, ri = tid & 63, cg = tid >> 6;
+    const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const int64_t G = gridDim.x;
+    const int64_t c0 = blockIdx.x * chunk, c1 = c0 + chunk < ncb ? c0 + chunk : ncb;
+    T *xs = reinterpret_cast<T *>(smem_raw);          // CT x RB
+    T *red = xs + CT * RB;                            // 4 x 64 x RB
+    for (int64_t r0 = 0; r0 < nrhs; r0 += RB) {
+        const int rb = nrhs - r0 < RB ? (int)(nrhs - r0) : RB;
+        for (int64_t i0 = 0; i0 < npiv; i0 += 64) {
+            const int64_t i = i0 + ri;
+            const bool row_ok = i < npiv;
+            T acc[RB];
+#pragma unroll
+            for (int r = 0; r < RB; r++) acc[r] = VT<T>::zero();
+            for (int64_t t0 = c0; t0 < c1; t0 += CT) {
+                const int ct = c1 - t0 < CT ? (int)(c1 - t0) : CT;
+                const T *u = U12 + i + t0 * npiv;
+                T ucur[UB], unext[UB];
+#pragma unroll
+                for (int k = 0; k < UB; k++) {
+                    const int cc = cg + 4 * k;
+                    ucur[k] = row_ok && cc < ct ? u[(int64_t)cc * npiv] : VT<T>::zero();
+                }
+                __syncthreads();
+                for (int e = tid; e < ct * rb; e += blockDim.x) {
+                    const int cc = e % ct, r = e / ct;
+                    xs[cc + r * CT] = X[cbcols[t0 + cc] + (r0 + r) * n];
+                }
+                __syncthreads();
+                for (int kb = 0; kb < ct; kb += 4 * UB) {
+                    const bool more = kb + 4 * UB < ct;
+                    if (more) {
+#pragma unroll
+                        for (int k = 0; k < UB; k++) {
+                            const int cc = kb + 4 * UB + cg + 4 * k;
+                            unext[k] = row_ok && cc < ct ? u[(int64_t)cc * npiv] : VT<T>::zero();
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < UB; k++) {
+                        const int cc = kb + cg + 4 * k;
+                        if (cc < ct) {
+#pragma unroll
+                            for (int r = 0; r < RB; r++)
+                                if (r < rb) acc[r] = add(acc[r], mul(ucur[k], xs[cc + r * CT]));
+                        }
+                    }
+                    if (more) {
+#pragma unroll
+                        for (int k = 0; k < UB; k++) ucur[k] = unext[k];
+                    }
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < RB; r++)
+                if (r < rb) red[(cg * 64 + ri) * RB + r] = acc[r];
+            __syncthreads();
+            for (int e = tid; e < 64 * rb; e += blockDim.x) {
+                const int rr = e & 63, r = e >> 6;
+                if (i0 + rr < npiv) {
+                    T sm = red[rr * RB + r];
+                    sm = add(sm, red[(64 + rr) * RB + r]);
+                    sm = add(sm, red[(128 + rr) * RB + r]);
+                    sm = add(sm, red[(192 + rr) * RB + r]);
+                    part[blockIdx.x * npiv * nrhs + (i0 + rr) + (r0 + r) * npiv] = sm;
+                }
+            }
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) last = atomicAdd(&st->ticket, 1u) == (unsigned)(G - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // the last CTA
+    const int np = (int)npiv;
+    const bool reg = npiv <= 64;
+    const int64_t E = npiv * nrhs;
+    T *s = reinterpret_cast<T *>(smem_raw);           // npiv * nrhs
+    T *dinv = s + E;                                  // npiv
+    T *ps = dinv + npiv;                              // 4 x 64 partial sums
+    T *sU = ps + 256;                                 // U11 (npiv <= 64): sU[j + i * np] = U[j, i]
+    if (reg)
+        for (int e = tid; e < np * np; e += blockDim.x) cp_async_el(sU + e, L + (e % np) + (int64_t)(e / np) * nrows);
+    for (int64_t e0 = 0; e0 < E; e0 += 64) {
+        const int64_t e = e0 + ri;
+        T v = VT<T>::zero();
+        if (e < E) {
+            const T *pp = part + e;
+            for (int64_t q0 = cg; q0 < G; q0 += 4 * UB) {
+                T pv[UB];
+#pragma unroll
+                for (int k = 0; k < UB; k++) {
+                    const int64_t q = q0 + 4 * k;
+                    pv[k] = q < G ? ldcg_v(pp + q * E) : VT<T>::zero();
+                }
+#pragma unroll
+                for (int k = 0; k < UB; k++) v = add(v, pv[k]);
+            }
+        }
+        ps[cg * 64 + ri] = v;
+        __syncthreads();
+        if (tid < 64 && e < E) {
+            const int64_t ii = e % npiv, r = e / npiv;
+            T t = add(add(ps[tid], ps[64 + tid]), add(ps[128 + tid], ps[192 + tid]));
+            s[e] = sub(Y[f + ii + r * n], t);
+        }
+        __syncthreads();
+    }
+    for (int64_t ii = tid; ii < npiv; ii += blockDim.x) {
+        const T d = L[ii + ii * nrows];
+        if (is_zero(d)) set_status(st, ST_SOLVE_ZERO, f + ii, 0, 0);
+        dinv[ii] = is_zero(d) ? VT<T>::zero() : recip(d);
+    }
+    if (tid == 0) st->ticket = 0u;
+    cp_async_wait_all();
+    __syncthreads();
+    if (st->code == ST_SOLVE_ZERO) return;
+    if (reg) {
+        for (int64_t r = warp; r < nrhs; r += nw) {
+            T a = lane < np ? s[lane + r * npiv] : VT<T>::zero();
+            T b = lane + 32 < np ? s[lane + 32 + r * npiv] : VT<T>::zero();
+            for (int ii = np - 1; ii >= 0; ii--) {
+                const T *col = sU + ii * np;
+                const T xi = mul(shfl_v<T>(ii < 32 ? a : b, ii & 31), dinv[ii]);
+                if (ii >= 32) {
+                    if (lane == ii - 32) b = xi;
+                    else if (lane < ii - 32) b = sub(b, mul(col[lane + 32], xi));
+                    a = sub(a, mul(col[lane], xi));
+                } else {
+                    if (lane == ii) a = xi;
+                    else if (lane < ii) a = sub(a, mul(col[lane], xi));
+                }
+            }
+            if (lane < np) X[f + lane + r * n] = a;
+            if (lane + 32 < np) X[f + lane + 32 + r * n] = b;
+        }
+        return;
+    }
+    for (int64_t r = warp; r < nrhs; r += nw) {
+        T *sr = s + r * npiv;
+        for (int64_t ii = npiv - 1; ii >= 0; ii--) {
+            const T xi = mul(sr[ii], dinv[ii]);
+            __syncwarp();
+            if (lane == 0) sr[ii] = xi;
+            for (int64_t j = lane; j < ii; j += 32) sr[j] = sub(sr[j], mul(L[j + ii * nrows], xi));
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (int64_t e = tid; e < npiv * nrhs; e += blockDim.x) {
+        const int64_t ii = e % npiv, r = e / npiv;
+        X[f + ii + r * n] = s[e];
     }
 }
 
@@ -1244,6 +1492,117 @@ __global__ void __launch_bounds__(256) k_bwdLt(const T *__restrict__ L, int64_t 
     for (int64_t e = threadIdx.x; e < npiv * nrhs; e += blockDim.x) {
         const int64_t i = e % npiv, r = e / npiv;
         V[f + i + r * n] = s[e];
+    }
+}
+
+// transposed solves, npiv <= 64 (one CTA): the front's U11 (or L11) block copied transposed into shared memory (ld
+// npiv + 1, so that the transposing stores and the sweep's row reads are free of bank conflicts), then a warp per
+// right-hand side with the vector in registers (rows lane and lane + 32)
+template <typename T, bool CJ>
+__device__ __forceinline__ void stage_transposed(const T *__restrict__ L, int64_t nrows, int np, T *sT)
+{
+    const int ld = np + 1;
+    for (int e = threadIdx.x; e < np * np; e += blockDim.x) {
+        const int row = e % np, col = e / np;
+        T v = L[row + (int64_t)col * nrows];
+        if (CJ) v = conjv(v);
+        sT[col + row * ld] = v;                        // sT[j + i * ld] = block[i, j]
+    }
+}
+
+// forward with U^T (U^H when conj): z_i = w_i / u_ii, then w_j -= u_ij z_i for j > i
+template <typename T, bool CJ>
+__global__ void __launch_bounds__(256) k_fwdUt3(const T *__restrict__ L, int64_t nrows, int64_t npiv, int64_t f,
+                                                T *__restrict__ Wc, int64_t n, int64_t nrhs, DevStatus *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int np = (int)npiv, ld = np + 1;
+    T *sT = reinterpret_cast<T *>(smem_raw);           // np x ld
+    T *dinv = sT + np * ld;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    stage_transposed<T, CJ>(L, nrows, np, sT);
+    for (int i = threadIdx.x; i < np; i += blockDim.x) {
+        T d = L[i + (int64_t)i * nrows];
+        if (CJ) d = conjv(d);
+        if (is_zero(d)) set_status(st, ST_SOLVE_ZERO, f + i, 0, 0);
+        dinv[i] = is_zero(d) ? VT<T>::zero() : recip(d);
+    }
+    __syncthreads();
+    if (st->code == ST_SOLVE_ZERO) return;
+    for (int64_t r = warp; r < nrhs; r += nw) {
+        T *w = Wc + f + r * n;
+        T a = lane < np ? w[lane] : VT<T>::zero();
+        T b = lane + 32 < np ? w[lane + 32] : VT<T>::zero();
+        for (int i = 0; i < np; i++) {
+            const T zi = mul(shfl_v<T>(i < 32 ? a : b, i & 31), dinv[i]);
+            const T *row = sT + i * ld;                 // row[j] = u_ij
+            if (lane == i) a = zi;
+            else if (lane > i && lane < np) a = sub(a, mul(row[lane], zi));
+            if (lane + 32 == i) b = zi;
+            else if (lane + 32 > i && lane + 32 < np) b = sub(b, mul(row[lane + 32], zi));
+        }
+        if (lane < np) w[lane] = a;
+        if (lane + 32 < np) w[lane + 32] = b;
+    }
+}
+
+// w[cbcol[c]] -= U12[:, c]^T z (a warp per CB column; the column's U12 entries loaded once for all right-hand sides)
+template <typename T, bool CJ>
+__global__ void k_ut_scatter2(const T *__restrict__ U12, int64_t npiv, int64_t ncb, const int64_t *__restrict__ cbcols,
+                              int64_t f, T *__restrict__ Wc, int64_t n, int64_t nrhs)
+{
+    const int lane = threadIdx.x & 31;
+    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < ncb; c += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        T u0 = lane < npiv ? U12[lane + c * npiv] : VT<T>::zero();
+        T u1 = lane + 32 < npiv ? U12[lane + 32 + c * npiv] : VT<T>::zero();
+        if (CJ) { u0 = conjv(u0); u1 = conjv(u1); }
+        for (int64_t r = 0; r < nrhs; r++) {
+            const T *z = Wc + f + r * n;
+            T s = lane < npiv ? mul(u0, z[lane]) : VT<T>::zero();
+            if (lane + 32 < npiv) s = add(s, mul(u1, z[lane + 32]));
+            for (int o = 16; o > 0; o >>= 1) s = add(s, shfl_xor_v<T>(s, o));
+            if (lane == 0) { T *w = Wc + cbcols[c] + r * n; *w = sub(*w, s); }
+        }
+    }
+}
+
+// backward with L^T (L^H): s = z - L21^T v_cb (a warp per pivot column and right-hand side), then the unit upper
+// L11^T solve from the last pivot
+template <typename T, bool CJ>
+__global__ void __launch_bounds__(256) k_bwdLt3(const T *__restrict__ L, int64_t nrows, int64_t npiv, int64_t f,
+                                                const int64_t *__restrict__ rowid, const int64_t *__restrict__ pinv,
+                                                const T *__restrict__ Z, T *__restrict__ V, int64_t n, int64_t nrhs)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int np = (int)npiv, ld = np + 1;
+    T *sT = reinterpret_cast<T *>(smem_raw);           // np x ld: sT[j + i * ld] = L11[i, j]
+    T *s = sT + np * ld;                               // np * nrhs
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    stage_transposed<T, CJ>(L, nrows, np, sT);
+    for (int64_t e = warp; e < npiv * nrhs; e += nw) {
+        const int64_t i = e % npiv, r = e / npiv;
+        T acc = VT<T>::zero();
+        for (int64_t rr = npiv + lane; rr < nrows; rr += 32) {
+            T l = L[rr + i * nrows];
+            if (CJ) l = conjv(l);
+            acc = add(acc, mul(l, V[pinv[rowid[rr]] + r * n]));
+        }
+        for (int o = 16; o > 0; o >>= 1) acc = add(acc, shfl_xor_v<T>(acc, o));
+        if (lane == 0) s[e] = sub(Z[f + i + r * n], acc);
+    }
+    __syncthreads();
+    for (int64_t r = warp; r < nrhs; r += nw) {
+        T *sr = s + r * npiv;
+        T a = lane < np ? sr[lane] : VT<T>::zero();
+        T b = lane + 32 < np ? sr[lane + 32] : VT<T>::zero();
+        for (int i = np - 1; i >= 0; i--) {
+            const T vi = shfl_v<T>(i < 32 ? a : b, i & 31);
+            const T *row = sT + i * ld;                 // row[j] = L11[i, j], j < i
+            if (lane < i) a = sub(a, mul(row[lane], vi));
+            if (lane + 32 < i) b = sub(b, mul(row[lane + 32], vi));
+        }
+        if (lane < np) V[f + lane + r * n] = a;
+        if (lane + 32 < np) V[f + lane + 32 + r * n] = b;
     }
 }
 

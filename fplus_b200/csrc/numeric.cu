@@ -421,10 +421,14 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
     const size_t nb = (size_t)(n > 0 ? n : 1) * (size_t)nrhs * sizeof(T);
     if ((rc = ensure_async(N, (void **)&N.rbuf, &N.cap_r, nb, err, errlen))) return rc;
     if ((rc = ensure_async(N, (void **)&N.sbuf, &N.cap_s, nb, err, errlen))) return rc;
+    // fused backward sweep: one CTA per SM at most, each over >= 64 contribution-block columns
+    auto bwd_chunk = [](int64_t ncb) { int64_t c = (ncb + 147) / 148; return c < 128 ? (int64_t)128 : c; };
+    auto bwd_grid = [&](int64_t ncb) { return ncb > 0 ? (ncb + bwd_chunk(ncb) - 1) / bwd_chunk(ncb) : (int64_t)1; };
     auto chunk_of = [](int64_t ncb) { int64_t c = (ncb + 295) / 296; return c < 32 ? (int64_t)32 : c; };
     int64_t maxpart = 1;
     for (const Front &F : P.fronts) {
         const int64_t ncb = F.ncols - F.npiv;
+        maxpart = std::max(maxpart, bwd_grid(ncb) * F.npiv);
         if (ncb > 0) maxpart = std::max(maxpart, ((ncb + chunk_of(ncb) - 1) / chunk_of(ncb)) * F.npiv);
     }
     if ((rc = ensure_async(N, (void **)&N.part, &N.cap_part, (size_t)maxpart * (size_t)nrhs * sizeof(T), err, errlen))) return rc;
@@ -432,8 +436,19 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
     const T *La = (const T *)N.Larena, *Ua = (const T *)N.Uarena;
     const int64_t nf = (int64_t)P.fronts.size();
     const size_t smem = (size_t)P.max_npiv * (size_t)(nrhs + 1) * sizeof(T);
+    const size_t fsmem = std::max((size_t)(256 * 8 + 64 * 4 * 8), (size_t)(P.max_npiv * (nrhs + 1) + 256 + 64 * 64)) * sizeof(T);
+    constexpr size_t FWD_SMEM = 200 * 1024;
     CK(cudaFuncSetAttribute(k_fwdL2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    CK(cudaFuncSetAttribute(k_fwdL3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
     CK(cudaFuncSetAttribute(k_u12_gemv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+    if (fsmem > 48 * 1024) CK(cudaFuncSetAttribute(k_bwdU_fused<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem));
+    {
+        const int t3 = (int)((64 * 65 + 64) * sizeof(T)), b3 = (int)((64 * 65 + 64 * nrhs) * sizeof(T));
+        CK(cudaFuncSetAttribute(k_fwdUt3<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, t3));
+        CK(cudaFuncSetAttribute(k_fwdUt3<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, t3));
+        CK(cudaFuncSetAttribute(k_bwdLt3<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, b3));
+        CK(cudaFuncSetAttribute(k_bwdLt3<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b3));
+    }
     if (smem > 48 * 1024) {
         CK(cudaFuncSetAttribute(k_bwdU<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         CK(cudaFuncSetAttribute(k_bwdLt<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -446,7 +461,13 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
             const Front &F = P.fronts[fi];
             if (F.npiv == 0 || F.nrows == 0) continue;
             const size_t fsm = (size_t)F.nrows * nrhs * sizeof(T);
-            if (fsm <= 96 * 1024)
+            const int64_t np = std::min(F.npiv, F.nrows);
+            const size_t whole_sm = fsm + (size_t)F.nrows * np * sizeof(T), l11_sm = fsm + (size_t)np * np * sizeof(T);
+            if (F.npiv <= 64 && whole_sm <= FWD_SMEM)
+                k_fwdL3<T><<<1, 256, whole_sm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 1), note_launch();
+            else if (F.npiv <= 64 && l11_sm <= FWD_SMEM)
+                k_fwdL3<T><<<1, 256, l11_sm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 0), note_launch();
+            else if (fsm <= 96 * 1024)
                 k_fwdL2<T><<<1, 256, fsm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs), note_launch();
             else
                 k_fwdL<T><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs), note_launch();
@@ -456,15 +477,9 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
             const Front &F = P.fronts[fi];
             const int64_t ncb = F.ncols - F.npiv;
             if (F.npiv == 0) continue;
-            int64_t nchunk = 0;
-            if (ncb > 0) {
-                const int64_t chunk = chunk_of(ncb);
-                nchunk = (ncb + chunk - 1) / chunk;
-                k_u12_gemv<T><<<(unsigned)nchunk, 256, (size_t)8 * F.npiv * sizeof(T), s>>>(
-                    Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, R, n, nrhs, chunk, part), note_launch();
-            }
-            k_bwdU<T><<<1, 256, (size_t)F.npiv * (nrhs + 1) * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, part, nchunk, S2, R,
-                                                                         n, nrhs, N.st), note_launch();
+            k_bwdU_fused<T><<<(unsigned)bwd_grid(ncb), 256, fsmem, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, Ua + F.U_off, ncb,
+                                                                     D.cols + F.col_off + F.npiv, ncb > 0 ? bwd_chunk(ncb) : 0,
+                                                                     part, S2, R, n, nrhs, N.st), note_launch();
         }
         // x[col_perm[k]] = Dcp[k] * R[k]
         k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, R, D.col_perm, nullptr, N.Dcp, n, nrhs), note_launch();
@@ -476,19 +491,31 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
             const Front &F = P.fronts[fi];
             const int64_t ncb = F.ncols - F.npiv;
             if (F.npiv == 0) continue;
-            if (cj) k_fwdUt2<T, true><<<1, 256, (size_t)F.npiv * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
+            const bool small = F.npiv <= 64 && F.npiv <= F.nrows;
+            const size_t tsm = (size_t)(F.npiv * (F.npiv + 1) + F.npiv) * sizeof(T);
+            if (small && cj) k_fwdUt3<T, true><<<1, 256, tsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
+            else if (small) k_fwdUt3<T, false><<<1, 256, tsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
+            else if (cj) k_fwdUt2<T, true><<<1, 256, (size_t)F.npiv * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
             else k_fwdUt2<T, false><<<1, 256, (size_t)F.npiv * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
             if (ncb > 0) {
-                if (cj) k_ut_scatter<T, true><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, F.f, R, n, nrhs), note_launch();
-                else k_ut_scatter<T, false><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, F.f, R, n, nrhs), note_launch();
+                const int64_t* cbc = D.cols + F.col_off + F.npiv;
+                if (F.npiv <= 64 && cj) k_ut_scatter2<T, true><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, cbc, F.f, R, n, nrhs), note_launch();
+                else if (F.npiv <= 64) k_ut_scatter2<T, false><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, cbc, F.f, R, n, nrhs), note_launch();
+                else if (cj) k_ut_scatter<T, true><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, cbc, F.f, R, n, nrhs), note_launch();
+                else k_ut_scatter<T, false><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, cbc, F.f, R, n, nrhs), note_launch();
             }
         }
         for (int64_t fi = nf - 1; fi >= 0; fi--) {
             const Front &F = P.fronts[fi];
             if (F.npiv == 0) continue;
             const size_t sm = (size_t)F.npiv * nrhs * sizeof(T);
-            if (cj) k_bwdLt<T, true><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, N.rowid + F.row_off, N.pinv, R, S2, n, nrhs), note_launch();
-            else k_bwdLt<T, false><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, N.rowid + F.row_off, N.pinv, R, S2, n, nrhs), note_launch();
+            const bool small = F.npiv <= 64 && F.npiv <= F.nrows;
+            const size_t tsm = sm + (size_t)F.npiv * (F.npiv + 1) * sizeof(T);
+            const int64_t *rid = N.rowid + F.row_off;
+            if (small && cj) k_bwdLt3<T, true><<<1, 256, tsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
+            else if (small) k_bwdLt3<T, false><<<1, 256, tsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
+            else if (cj) k_bwdLt<T, true><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
+            else k_bwdLt<T, false><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
         }
         // x[row_perm[p_lu[k]]] = Drp[p_lu[k]] * S2[k]
         k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, S2, D.row_perm, N.p_lu, N.Drp, n, nrhs), note_launch();
