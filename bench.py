@@ -40,11 +40,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 
-def workload(name):
+def workload(name, modes=8):
     from fplus_b200 import workloads as W
     if name == "pencil":
-        n, Ap, Ai, Ax = W.pencil()
-        desc = {"workload": "pencil A - sigma B, 8 Fourier x 4 fields x 1024 Chebyshev (n=32768), complex128, "
+        n, Ap, Ai, Ax = W.pencil(modes=modes)
+        desc = {"workload": f"pencil A - sigma B, {modes} Fourier x 4 fields x 1024 Chebyshev (n={n}), complex128, "
                             "half-bandwidth 6, 8 dense tau rows + 8 dense tau columns, |a| log-uniform [1e-6, 1e6], "
                             "sigma=0.3+1.7i", "n": n, "nnz": int(Ap[-1]), "nrhs": 1}
     elif name == "convdiff2d":
@@ -198,7 +198,7 @@ def run_reference_arm(args, rank, world):
     for _ in range(args.steps):
         ms_full, ms_sample, be, desc, threads, scale = reference_sample(args.workload)
         ms_list.append(ms_full)
-    d = workload(args.workload)[5]
+    d = workload(args.workload, args.modes)[5]
     ms = float(np.mean(ms_list))
     line = {"impl": "reference", "metric": "factor+solve ms (berr<=1e-14)", "value": ms, "unit": "ms", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
@@ -218,7 +218,7 @@ def run_b200_arm(args, rank, world):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    n, Ap, Ai, Ax, b, desc = workload(args.workload)
+    n, Ap, Ai, Ax, b, desc = workload(args.workload, args.modes)
     cplx = np.iscomplexobj(Ax)
     t0 = time.perf_counter()
     S = F.analyze(n, Ap, Ai)
@@ -349,6 +349,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="pencil", choices=["pencil", "convdiff2d"])
+    ap.add_argument("--modes", type=int, default=8,
+                    help="Fourier modes of the pencil workload (8: n = 32768, the benchmark; 1: n = 4096, for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
