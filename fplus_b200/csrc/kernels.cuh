@@ -202,24 +202,24 @@ __global__ void k_assemble(T *__restrict__ W, const T *__restrict__ Bx, const in
 
 // W += the child's contribution block (rows: the child's interior CB rows into its slots, its border rows onto the
 // parent's dense rows; columns through relcol); the child's CB row ids fill the slots
+// (columns [c0, c1) of the CB; the row ids when `rowids`)
 template <typename T>
-__global__ void k_extend_add(T *__restrict__ W, int64_t ldw, const T *__restrict__ cb, int64_t cbr, int64_t cbc,
+__global__ void k_extend_add(T *__restrict__ W, int64_t ldw, const T *__restrict__ cb, int64_t cbr, int64_t c0, int64_t c1,
                              int64_t nslot, int64_t slot, int64_t tau_base, const int64_t *__restrict__ relcol,
-                             int64_t *__restrict__ rowid_parent, const int64_t *__restrict__ rowid_child_cb,
+                             int64_t *__restrict__ rowid_parent, const int64_t *__restrict__ rowid_child_cb, int rowids,
                              const DevStatus *st)
 {
     if (st->code) return;
-    const int64_t total = cbr * cbc;
+    const int64_t total = cbr * (c1 - c0);
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t t = e % cbr, c = e / cbr;
+        const int64_t t = e % cbr, c = c0 + e / cbr;
         const int64_t pr = t < nslot ? slot + t : tau_base + (t - nslot);
         const int64_t pc = relcol[c];
         T v = cb[t + c * cbr];
         T *w = W + pr + pc * ldw;
         *w = add(*w, v);
-        if (c == 0 && t < nslot) rowid_parent[slot + t] = rowid_child_cb[t];
     }
-    if (cbc == 0)
+    if (rowids)
         for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nslot; t += (int64_t)gridDim.x * blockDim.x)
             rowid_parent[slot + t] = rowid_child_cb[t];
 }
@@ -632,11 +632,24 @@ __device__ __forceinline__ int warp_argmax(const T *__restrict__ col, const int 
 // step-j pivot meanwhile, keep the multipliers (double-buffered) and store those of step j - 1 into column j - 1 (no
 // longer read by anyone).  One barrier per step.  No row swaps: the pivot row of step j is tagged j.  The singular test
 // uses the column thresholds staged in shared memory (squared moduli; the modulus itself near the threshold).
+// The sources of a front's pivot block when the LU kernel assembles it itself (instead of reading it from the working
+// block): the original entries of the pivot columns and the pivot-column part of at most one child's contribution block.
+struct PivotAsm {
+    int on;                                  // assemble from these sources
+    const void *cb;                          // the child's CB (cbr x cbc, column-major), or null
+    int64_t cbr, h, nslot, slot, tau_base;   // its rows, its CB columns in the pivot columns (a prefix), row placement
+    const int64_t *relcol, *child_rowid;     // the child's CB columns -> local columns; its CB rows' ids
+    const int64_t *asrc, *adst;              // original entries: B entry -> offset in the block (column-major, ld nrows)
+    int64_t acnt;
+    const void *Bx;
+    const int64_t *rowinit;                  // the entering rows' ids (-1 for rows from children)
+};
+
 template <typename T>
 __global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
                                                     int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
                                                     int64_t *__restrict__ rowid, T *__restrict__ Lout, int *__restrict__ perm,
-                                                    int64_t *__restrict__ p_lu, DevStatus *st, int64_t front)
+                                                    int64_t *__restrict__ p_lu, DevStatus *st, int64_t front, PivotAsm pa)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *A = reinterpret_cast<T *>(smem_raw);                        // npiv x nrows, column-major: A[c * nrows + i]
@@ -648,9 +661,38 @@ __global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int
     __shared__ int s_bi[2], s_stop;
     __shared__ T s_inv[2];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
-    for (int c = 0; c < npiv; c++)
-        for (int i = tid; i < nrows; i += nt) A[(size_t)c * nrows + i] = W[i + (int64_t)c * ld];
-    for (int i = tid; i < nrows; i += nt) { rid[i] = rowid[i]; tag[i] = INT_MAX; }
+    const int ne = npiv * nrows;
+    if (!pa.on) {
+        // the block from the working block, 8 loads in flight per thread
+        for (int e0 = tid; e0 < ne; e0 += 8 * nt) {
+            T v[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) { const int e = e0 + q * nt; v[q] = e < ne ? W[e % nrows + (int64_t)(e / nrows) * ld] : VT<T>::zero(); }
+#pragma unroll
+            for (int q = 0; q < 8; q++) { const int e = e0 + q * nt; if (e < ne) A[e] = v[q]; }
+        }
+        for (int i = tid; i < nrows; i += nt) rid[i] = rowid[i];
+    } else {
+        // assembled here: zero, the original entries, then the child's CB columns added; the row ids
+        for (int e = tid; e < ne; e += nt) A[e] = VT<T>::zero();
+        for (int i = tid; i < nrows; i += nt) rid[i] = pa.rowinit[i];
+        __syncthreads();
+        const T *Bx = reinterpret_cast<const T *>(pa.Bx);
+#pragma unroll 4
+        for (int64_t e = tid; e < pa.acnt; e += nt) A[pa.adst[e]] = Bx[pa.asrc[e]];
+        for (int64_t t = tid; t < pa.nslot; t += nt) rid[pa.slot + t] = pa.child_rowid[t];
+        __syncthreads();
+        const T *cb = reinterpret_cast<const T *>(pa.cb);
+        const int64_t tot = pa.cbr * pa.h;
+#pragma unroll 4
+        for (int64_t e = tid; e < tot; e += nt) {
+            const int64_t t = e % pa.cbr, c = e / pa.cbr;
+            const int64_t pr = t < pa.nslot ? pa.slot + t : pa.tau_base + (t - pa.nslot);
+            T *a = A + pa.relcol[c] * nrows + pr;
+            *a = add(*a, cb[t + c * pa.cbr]);
+        }
+    }
+    for (int i = tid; i < nrows; i += nt) tag[i] = INT_MAX;
     for (int c = tid; c < npiv; c += nt) thr[c] = pivot_rel * colmax[fcol + c];
     if (tid == 0) s_stop = st->code != 0 ? 3 : 0;
     __syncthreads();
@@ -927,6 +969,131 @@ __global__ void __launch_bounds__(256) k_u12_blk(const T *__restrict__ W, int64_
         for (int e = tid; e < npiv * tn; e += blockDim.x) {
             const int r = e % npiv, c = e / npiv;
             U[r + (c0 + c) * (int64_t)npiv] = X[r + c * U12_NP];
+        }
+        __syncthreads();
+    }
+}
+
+// The tail of a front with npiv <= 64 and nrows <= 128, in one pass over its contribution-block columns: for each tile of
+// 32 columns, the tile's rows are gathered in pivot order (perm; the next tile's values are loaded into registers while
+// this one is computed), then per 16-row block of the pivot rows, the diagonal 16 x 16 unit-lower solve by half-warps
+// (one column each, 16 shuffle steps) and the update of every row below, pivot rows and contribution-block rows alike,
+// X[r, c] -= sum_k L[r, k] X[k, c], on the FP64 tensor cores (mma m8n8k4; complex as four real products).  Rows [0, npiv)
+// leave as U12 (into the arena), rows [npiv, nrows) as the contribution block A22[perm] - L21 U12 (into the stack): the
+// blocked forward substitution with [L11; L21] of the front's columns.  L (real and imaginary planes) and the tile live
+// in shared memory with a leading dimension of 132 doubles (4 mod 16: the mma fragments of a half-warp hit 16 banks).
+constexpr int FT_TN = 32, FT_LD = 132, FT_NP = 64, FT_NR = 128, FT_THREADS = 512;
+template <typename T>
+__global__ void __launch_bounds__(FT_THREADS) k_front_tail(const T *__restrict__ W, int64_t ld, const int *__restrict__ perm,
+                                                           int npiv, int nrows, int64_t ncb, int64_t cb0, int64_t cb1,
+                                                           const T *__restrict__ Lb, T *__restrict__ U, T *__restrict__ CB,
+                                                           const DevStatus *st)
+{
+    constexpr bool CP = VT<T>::cplx_;
+    constexpr int PER = FT_NR * FT_TN / FT_THREADS;                // tile values per thread (8)
+    extern __shared__ __align__(16) double ft_smem[];
+    double *sLr = ft_smem;                                          // L[m, k] at k * FT_LD + m
+    double *sLi = sLr + (CP ? FT_NP * FT_LD : 0);
+    double *sXr = sLr + (CP ? 2 : 1) * FT_NP * FT_LD;               // X[r, c] at c * FT_LD + r
+    double *sXi = sXr + (CP ? FT_TN * FT_LD : 0);
+    __shared__ int sperm[FT_NR];
+    if (st->code) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int M = nrows - npiv;
+    for (int e0 = tid; e0 < npiv * nrows; e0 += 8 * FT_THREADS) {     // 8 loads in flight per thread
+        T v[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) { const int e = e0 + q * FT_THREADS; v[q] = e < npiv * nrows ? Lb[e] : VT<T>::zero(); }
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int e = e0 + q * FT_THREADS, m = e % nrows, k = e / nrows;
+            if (e < npiv * nrows) {
+                if constexpr (CP) { sLr[k * FT_LD + m] = v[q].x; sLi[k * FT_LD + m] = v[q].y; } else sLr[k * FT_LD + m] = v[q];
+            }
+        }
+    }
+    for (int i = tid; i < nrows; i += FT_THREADS) sperm[i] = perm[i];
+    __syncthreads();
+    // columns [cb0, cb1) of the contribution block (cb0 a multiple of the tile width)
+    const int64_t t0 = cb0 / FT_TN, ntile = (cb1 + FT_TN - 1) / FT_TN;
+    T pre[PER];
+    auto fetch = [&](int64_t t) {
+        const int64_t c0 = t * FT_TN;
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            const int e = tid + q * FT_THREADS, r = e % FT_NR, c = e / FT_NR;
+            pre[q] = (t < ntile && r < nrows && c0 + c < cb1) ? W[sperm[r] + (npiv + c0 + c) * ld] : VT<T>::zero();
+        }
+    };
+    fetch(t0 + blockIdx.x);
+    const int half = lane >> 4, hl = lane & 15;
+    for (int64_t t = t0 + blockIdx.x; t < ntile; t += gridDim.x) {
+        const int64_t c0 = t * FT_TN;
+        const int tn = (int)(cb1 - c0 < FT_TN ? cb1 - c0 : FT_TN);
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            const int e = tid + q * FT_THREADS, r = e % FT_NR, c = e / FT_NR;
+            if constexpr (CP) { sXr[c * FT_LD + r] = pre[q].x; sXi[c * FT_LD + r] = pre[q].y; } else sXr[c * FT_LD + r] = pre[q];
+        }
+        __syncthreads();
+        fetch(t + gridDim.x);                                       // in flight during this tile
+        for (int kb = 0; kb < npiv; kb += 16) {
+            const int w = npiv - kb < 16 ? npiv - kb : 16;
+            {   // the diagonal block: a half-warp per column, lane hl holds row kb + hl
+                const int c = 2 * warp + half;
+                double xr = hl < w ? sXr[c * FT_LD + kb + hl] : 0.0, xi = CP && hl < w ? sXi[c * FT_LD + kb + hl] : 0.0;
+                for (int i = 0; i < w; i++) {
+                    const double pr = __shfl_sync(0xffffffffu, xr, i, 16);
+                    const double pi = CP ? __shfl_sync(0xffffffffu, xi, i, 16) : 0.0;
+                    if (hl > i && hl < w) {
+                        const double lr = sLr[(kb + i) * FT_LD + kb + hl];
+                        if constexpr (CP) {
+                            const double li = sLi[(kb + i) * FT_LD + kb + hl];
+                            const T x = sub(T{xr, xi}, mul(T{lr, li}, T{pr, pi}));
+                            xr = x.x; xi = x.y;
+                        } else xr = xr - lr * pr;
+                    }
+                }
+                if (hl < w) { sXr[c * FT_LD + kb + hl] = xr; if constexpr (CP) sXi[c * FT_LD + kb + hl] = xi; }
+            }
+            __syncthreads();
+            const int rb = kb + w, R = nrows - rb;
+            if (R > 0) {
+                const int mt = (R + 7) >> 3, nt = (tn + 7) >> 3;
+                for (int p = warp; p < mt * nt; p += FT_THREADS / 32) {
+                    const int m0 = rb + 8 * (p % mt), n0 = 8 * (p / mt);
+                    const int am = m0 + (lane >> 2), bn = n0 + (lane >> 2);
+                    double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;         // re / im accumulators (two columns each)
+                    for (int ks = 0; ks < w; ks += 4) {
+                        const int k = kb + ks + (lane & 3);
+                        const bool kin = ks + (lane & 3) < w;
+                        const double ar = kin && am < nrows ? sLr[k * FT_LD + am] : 0.0;
+                        const double br = kin ? sXr[bn * FT_LD + k] : 0.0;
+                        dmma(a0, a1, ar, br);
+                        if constexpr (CP) {
+                            const double ai = kin && am < nrows ? sLi[k * FT_LD + am] : 0.0;
+                            const double bi = kin ? sXi[bn * FT_LD + k] : 0.0;
+                            dmma(a0, a1, ai, -bi);
+                            dmma(b0, b1, ar, bi);
+                            dmma(b0, b1, ai, br);
+                        }
+                    }
+                    const int cr = m0 + (lane >> 2), cc = n0 + 2 * (lane & 3);
+                    if (cr < nrows) {
+                        sXr[cc * FT_LD + cr] -= a0;
+                        sXr[(cc + 1) * FT_LD + cr] -= a1;
+                        if constexpr (CP) { sXi[cc * FT_LD + cr] -= b0; sXi[(cc + 1) * FT_LD + cr] -= b1; }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        for (int e = tid; e < nrows * tn; e += FT_THREADS) {
+            const int r = e % nrows, c = e / nrows;
+            T v;
+            if constexpr (CP) v = T{sXr[c * FT_LD + r], sXi[c * FT_LD + r]}; else v = sXr[c * FT_LD + r];
+            if (r < npiv) U[r + (c0 + c) * (int64_t)npiv] = v;
+            else CB[(r - npiv) + (c0 + c) * (int64_t)M] = v;
         }
         __syncthreads();
     }

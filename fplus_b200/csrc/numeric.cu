@@ -96,9 +96,14 @@ DevNum::~DevNum()
     if (device >= 0) cudaSetDevice(device);
     for (void *p : {(void *)Ax, (void *)Bx, (void *)Drp, (void *)Dcp, (void *)colmax, (void *)Larena, (void *)Uarena,
                     (void *)cbstack, (void *)work, (void *)rowid, (void *)p_lu, (void *)pinv, (void *)ipiv, (void *)perm,
-                    (void *)st, (void *)scratch, (void *)rbuf, (void *)sbuf, (void *)xbuf, (void *)part})
+                    (void *)st, (void *)scratch, (void *)rbuf, (void *)sbuf, (void *)xbuf, (void *)part, (void *)work2,
+                    (void *)perm2})
         if (p) cudaFreeAsync(p, stream);
     if (stream) cudaStreamSynchronize(stream);
+    if (crit) cudaStreamSynchronize(crit);
+    if (ev_lu) cudaEventDestroy(ev_lu);
+    if (ev_head) cudaEventDestroy(ev_head);
+    if (crit) cudaStreamDestroy(crit);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream && stream_owned) cudaStreamDestroy(stream);
@@ -270,83 +275,205 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_u12_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_front_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_u12_fused<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_u12_fused<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_u12_fused<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         attr_set = 1;
     }
     if ((rc = dev_clear_status(N, err, errlen))) return rc;
-    T *W = (T *)N.work, *La = (T *)N.Larena, *Ua = (T *)N.Uarena, *CB = (T *)N.cbstack;
+    T *La = (T *)N.Larena, *Ua = (T *)N.Uarena, *CB = (T *)N.cbstack;
     const T *Bx = (const T *)N.Bx;
     constexpr int PW = 32;       // panel width of the blocked path
     const int TB = VT<T>::cplx_ ? 32 : 64;    // rows per TRSM block of U12
     const int64_t nf = (int64_t)P.fronts.size();
     const double fm = VT<T>::cplx_ ? 8.0 : 2.0;     // flops per multiply-add
     Prof prof;
+
+    // Chain fronts whose CB goes to the next front run with a one-front look-ahead on two streams.  The critical stream
+    // (high priority) assembles a front's pivot columns and factors its pivot block; the bulk stream (the caller's)
+    // assembles the front's other columns, then, once the pivot block is factored, forms U12 and the CB for the CB
+    // columns that are the parent's pivot columns (the head), signals the critical stream, and forms the rest of the
+    // front's tail while the critical stream moves on to the parent.  Consecutive such fronts alternate between two
+    // working blocks and two row orders.
+    auto head_cols = [&](const Front &G) -> int64_t {       // G's CB columns inside its parent's pivot columns (a prefix), or -1
+        if (G.parent < 0) return 0;
+        const int64_t ncb = G.ncols - G.npiv, pnp = P.fronts[G.parent].npiv;
+        int64_t h = 0;
+        while (h < ncb && P.relcol[G.relcol_off + h] < pnp) h++;
+        for (int64_t c = h; c < ncb; c++) if (P.relcol[G.relcol_off + c] < pnp) return -1;
+        return h;
+    };
+    std::vector<int64_t> hc((size_t)nf, -1);
+    std::vector<char> pipe((size_t)nf, 0);
+    bool any_pipe = false;
     for (int64_t fi = 0; fi < nf; fi++) {
         const Front &F = P.fronts[fi];
-        const int64_t nr = F.nrows, nc = F.ncols, np = F.npiv, ncb = nc - np;
-        const int64_t ld = nr;
-        T *Lf = La + F.L_off;
-        prof.begin(s, PROF_ASM, 0.0, (double)(nr * nc + 2 * (F.asm_end - F.asm_begin)) * vs);
-        if (nr * nc > 0) CK(cudaMemsetAsync(W, 0, (size_t)(nr * nc) * vs, s));
-        {
-            const int64_t cnt = F.asm_end - F.asm_begin;
-            k_assemble<T><<<nblk(std::max(cnt, nr)), 256, 0, s>>>(W, Bx, D.asm_src + F.asm_begin, D.asm_dst + F.asm_begin, cnt,
-                                                                   N.rowid + F.row_off, D.rowinit + F.row_off, nr, N.st), note_launch();
+        hc[fi] = head_cols(F);
+        const int64_t nr = F.nrows, np = F.npiv, ncb = F.ncols - F.npiv;
+        bool ok = F.dense && np > 0 && np <= nr && np <= FT_NP && nr <= FT_NR && front_lu_smem(nr, np, vs) <= SMEM_MAX;
+        ok = ok && (ncb == 0 || (F.parent == fi + 1 && hc[fi] >= 0));
+        for (int64_t k = F.child_begin; ok && k < F.child_end; k++) ok = hc[P.children[k]] >= 0;
+        pipe[fi] = ok;
+        any_pipe = any_pipe || ok;
+    }
+    if (any_pipe) {
+        const size_t wbytes = (size_t)P.work_size * vs;
+        if ((rc = ensure_async(N, (void **)&N.work2, &N.cap_work2, wbytes, err, errlen))) return rc;
+        if ((rc = ensure_async(N, (void **)&N.perm2, &N.cap_perm2, (size_t)(P.max_nrows > 0 ? P.max_nrows : 1) * 4, err, errlen))) return rc;
+        if (!N.crit) {
+            int lo = 0, hi = 0;
+            CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            CK(cudaStreamCreateWithPriority(&N.crit, cudaStreamNonBlocking, hi));
+            CK(cudaEventCreateWithFlags(&N.ev_lu, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&N.ev_head, cudaEventDisableTiming));
         }
+    }
+    cudaStream_t A = N.crit;
+
+    // the assembly of columns [0, npiv) (part 1), the others (part 2), or all (part 0)
+    auto assemble = [&](int64_t fi, T *W, cudaStream_t st, int part) {
+        const Front &F = P.fronts[fi];
+        const int64_t nr = F.nrows, nc = F.ncols, np = F.npiv, ld = nr;
+        const int64_t e0 = part == 2 ? F.asm_mid : F.asm_begin, e1 = part == 1 ? F.asm_mid : F.asm_end;
+        const int64_t z0 = part == 2 ? nr * np : 0, z1 = part == 1 ? nr * np : nr * nc;
+        prof.begin(st, PROF_ASM, 0.0, (double)((z1 - z0) + 2 * (e1 - e0)) * vs);
+        if (z1 > z0) CK(cudaMemsetAsync(W + z0, 0, (size_t)(z1 - z0) * vs, st));
+        const int64_t cnt = e1 - e0, nri = part == 2 ? 0 : nr;
+        if (cnt > 0 || nri > 0)
+            k_assemble<T><<<nblk(std::max(cnt, nri)), 256, 0, st>>>(W, Bx, D.asm_src + e0, D.asm_dst + e0, cnt,
+                                                                    N.rowid + F.row_off, D.rowinit + F.row_off, nri, N.st), note_launch();
         for (int64_t k = F.child_begin; k < F.child_end; k++) {
-            const Front &G = P.fronts[P.children[k]];
+            const int64_t gi = P.children[k];
+            const Front &G = P.fronts[gi];
             const int64_t cbr = std::max<int64_t>(0, G.nrows - G.npiv), cbc = G.ncols - G.npiv;
             const int64_t nslot = std::max<int64_t>(0, G.nri - G.npiv);
             if (cbr == 0) continue;
-            k_extend_add<T><<<nblk(std::max(cbr * cbc, nslot)), 256, 0, s>>>(W, ld, CB + G.cb_off, cbr, cbc, nslot, G.slot,
-                                                                            F.tau_base, D.relcol + G.relcol_off,
-                                                                            N.rowid + F.row_off, N.rowid + G.row_off + G.npiv, N.st), note_launch();
+            const int64_t c0 = part == 2 ? hc[gi] : 0, c1 = part == 1 ? hc[gi] : cbc;
+            const int rowids = part != 2;
+            if (c1 <= c0 && !rowids) continue;
+            k_extend_add<T><<<nblk(std::max(cbr * std::max<int64_t>(c1 - c0, 0), nslot)), 256, 0, st>>>(
+                W, ld, CB + G.cb_off, cbr, c0, std::max(c0, c1), nslot, G.slot, F.tau_base, D.relcol + G.relcol_off,
+                N.rowid + F.row_off, N.rowid + G.row_off + G.npiv, rowids, N.st), note_launch();
         }
-        prof.end(s);
-        if (np == 0) continue;
-        if (nr == 0) { k_set_singular<<<1, 1, 0, s>>>(N.st, F.f), note_launch(); continue; }     // no row can take pivot step f
-        // the pivot block: partial-pivot LU, L\U into the arena in the final row order, the order into N.perm
+        prof.end(st);
+        return FPLUS_OK;
+    };
+    // the pivot block: partial-pivot LU, L\U into the arena in the final row order, the order into perm
+    auto factor_block = [&](int64_t fi, T *W, int *perm, cudaStream_t st, const PivotAsm &pa) {
+        const Front &F = P.fronts[fi];
+        const int64_t nr = F.nrows, np = F.npiv, ld = nr;
+        T *Lf = La + F.L_off;
         const size_t sm = front_lu_smem(nr, np, vs);
         {
             double fl = 0;
             for (int64_t k = 0; k < std::min(np, nr); k++) fl += (double)(nr - k - 1) * (double)(np - k);
-            prof.begin(s, PROF_LU, fm * fl, 2.0 * (double)(nr * np) * vs);
+            prof.begin(st, PROF_LU, fm * fl, 2.0 * (double)(nr * np) * vs);
         }
         if (sm <= SMEM_MAX) {
             const int R = (int)((nr + 31) & ~31);
             int nt = 32 + (R <= 128 ? 4 * R : (R <= 480 ? R : 992));   // the pivot warp + the update warps
             if (nt > 1024) nt = 1024;
-            k_front_lu2<T><<<1, nt, sm, s>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel, N.rowid + F.row_off, Lf,
-                                           N.perm, N.p_lu, N.st, fi), note_launch();
+            k_front_lu2<T><<<1, nt, sm, st>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel, N.rowid + F.row_off, Lf,
+                                            perm, N.p_lu, N.st, fi, pa), note_launch();
         } else {
             const int64_t npr = std::min(np, nr);
             for (int64_t k0 = 0; k0 < npr; k0 += PW) {
                 const int w = (int)std::min<int64_t>(PW, npr - k0);
-                k_panel<T><<<1, 512, 0, s>>>(W, ld, nr, F.nri, (int)k0, w, F.f, N.colmax, pivot_rel, N.rowid + F.row_off,
-                                            N.ipiv + F.f, N.st, fi), note_launch();
-                if (k0 > 0) k_laswp<T><<<nblk(k0, 128), 128, 0, s>>>(W, ld, N.ipiv + F.f, (int)k0, w, 0, k0, N.st), note_launch();
+                k_panel<T><<<1, 512, 0, st>>>(W, ld, nr, F.nri, (int)k0, w, F.f, N.colmax, pivot_rel, N.rowid + F.row_off,
+                                             N.ipiv + F.f, N.st, fi), note_launch();
+                if (k0 > 0) k_laswp<T><<<nblk(k0, 128), 128, 0, st>>>(W, ld, N.ipiv + F.f, (int)k0, w, 0, k0, N.st), note_launch();
                 if (k0 + w < np) {
-                    k_laswp<T><<<nblk(np - k0 - w, 128), 128, 0, s>>>(W, ld, N.ipiv + F.f, (int)k0, w, k0 + w, np, N.st), note_launch();
-                    k_trsm_unit<T><<<nblk(np - k0 - w, 128), 128, 0, s>>>(W, ld, (int)k0, w, k0 + w, np, N.st), note_launch();
+                    k_laswp<T><<<nblk(np - k0 - w, 128), 128, 0, st>>>(W, ld, N.ipiv + F.f, (int)k0, w, k0 + w, np, N.st), note_launch();
+                    k_trsm_unit<T><<<nblk(np - k0 - w, 128), 128, 0, st>>>(W, ld, (int)k0, w, k0 + w, np, N.st), note_launch();
                     const int64_t M = nr - k0 - w, Nn = np - k0 - w;
                     if (M > 0) {
                         dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((Nn + GBN - 1) / GBN));
                         T *C = W + (k0 + w) + (k0 + w) * ld;
-                        k_gemm_sub<T><<<g, 256, 0, s>>>(M, Nn, w, W + (k0 + w) + k0 * ld, ld, W + k0 + (k0 + w) * ld, ld,
-                                                        C, ld, nullptr, C, ld, N.st), note_launch();
+                        k_gemm_sub<T><<<g, 256, 0, st>>>(M, Nn, w, W + (k0 + w) + k0 * ld, ld, W + k0 + (k0 + w) * ld, ld,
+                                                         C, ld, nullptr, C, ld, N.st), note_launch();
                     }
                 }
             }
-            k_left_finish<T><<<nblk(nr * np), 256, 0, s>>>(W, ld, nr, np, N.ipiv + F.f, N.perm, N.rowid + F.row_off, F.f, N.p_lu,
-                                                          Lf, N.st), note_launch();
+            k_left_finish<T><<<nblk(nr * np), 256, 0, st>>>(W, ld, nr, np, N.ipiv + F.f, perm, N.rowid + F.row_off, F.f, N.p_lu,
+                                                           Lf, N.st), note_launch();
         }
-        prof.end(s);
-        if (nr < np) { k_set_singular<<<1, 1, 0, s>>>(N.st, F.f + nr), note_launch(); }
+        prof.end(st);
+        if (nr < np) { k_set_singular<<<1, 1, 0, st>>>(N.st, F.f + nr), note_launch(); }
+        return FPLUS_OK;
+    };
+    // U12 and the CB for CB columns [c0, c1) by the fused tail kernel (at most `cap` CTAs)
+    auto tail = [&](int64_t fi, T *W, const int *perm, cudaStream_t st, int64_t c0, int64_t c1, int cap) {
+        const Front &F = P.fronts[fi];
+        const int64_t nr = F.nrows, np = F.npiv, ncb = F.ncols - F.npiv, M = nr - np;
+        if (c1 <= c0) return FPLUS_OK;
+        prof.begin(st, PROF_SCHUR, fm * ((double)np * (double)np / 2.0 + (double)M * (double)np) * (double)(c1 - c0),
+                   (double)(2 * nr * (c1 - c0) + nr * np) * vs);
+        const size_t fsm = (size_t)(VT<T>::cplx_ ? 2 : 1) * (FT_NP + FT_TN) * FT_LD * sizeof(double);
+        const int blocks = (int)std::min<int64_t>((c1 - c0 + FT_TN - 1) / FT_TN, cap);
+        k_front_tail<T><<<blocks, FT_THREADS, fsm, st>>>(W, nr, perm, (int)np, (int)nr, ncb, c0, c1, La + F.L_off, Ua + F.U_off,
+                                                        CB + F.cb_off, N.st), note_launch();
+        prof.end(st);
+        return FPLUS_OK;
+    };
+
+    bool in_pipe = false;
+    int wsel = 0;
+    for (int64_t fi = 0; fi < nf; fi++) {
+        const Front &F = P.fronts[fi];
+        const int64_t nr = F.nrows, nc = F.ncols, np = F.npiv, ncb = nc - np;
+        if (pipe[fi]) {
+            if (!in_pipe) { CK(cudaEventRecord(N.ev_head, s)); in_pipe = true; }   // the critical stream joins the bulk one
+            T *W = (T *)(wsel ? N.work2 : N.work);
+            int *perm = wsel ? N.perm2 : N.perm;
+            wsel ^= 1;
+            CK(cudaStreamWaitEvent(A, N.ev_head, 0));
+            PivotAsm pa{};
+            if (F.child_end - F.child_begin <= 1) {
+                // the LU kernel assembles the pivot block itself (from at most one child)
+                pa.on = 1;
+                pa.asrc = D.asm_src + F.asm_begin; pa.adst = D.asm_dst + F.asm_begin;
+                pa.acnt = (ncb > 0 ? F.asm_mid : F.asm_end) - F.asm_begin;
+                pa.Bx = Bx; pa.rowinit = D.rowinit + F.row_off; pa.tau_base = F.tau_base;
+                if (F.child_end > F.child_begin) {
+                    const int64_t gi = P.children[F.child_begin];
+                    const Front &G = P.fronts[gi];
+                    pa.cbr = std::max<int64_t>(0, G.nrows - G.npiv);
+                    pa.h = pa.cbr > 0 ? hc[gi] : 0;
+                    pa.nslot = std::max<int64_t>(0, G.nri - G.npiv);
+                    pa.slot = G.slot;
+                    pa.cb = CB + G.cb_off; pa.relcol = D.relcol + G.relcol_off; pa.child_rowid = N.rowid + G.row_off + G.npiv;
+                }
+            } else if ((rc = assemble(fi, W, A, ncb > 0 ? 1 : 0))) return rc;
+            if ((rc = factor_block(fi, W, perm, A, pa))) return rc;
+            CK(cudaEventRecord(N.ev_lu, A));
+            if (ncb > 0 && (rc = assemble(fi, W, s, 2))) return rc;
+            CK(cudaStreamWaitEvent(s, N.ev_lu, 0));
+            if (ncb > 0) {
+                const int64_t h = std::min<int64_t>(ncb, (hc[fi] + FT_TN - 1) / FT_TN * FT_TN);
+                if ((rc = tail(fi, W, perm, s, 0, h, 148))) return rc;
+                CK(cudaEventRecord(N.ev_head, s));
+                if ((rc = tail(fi, W, perm, s, h, ncb, 147))) return rc;      // one SM left for the next pivot block
+            }
+            if ((fi & 255) == 255) CK(cudaGetLastError());
+            continue;
+        }
+        in_pipe = false;       // the bulk stream has waited for the last pivot block of the critical stream
+        T *W = (T *)N.work;
+        T *Lf = La + F.L_off;
+        const int64_t ld = nr;
+        if ((rc = assemble(fi, W, s, 0))) return rc;
+        if (np == 0) continue;
+        if (nr == 0) { k_set_singular<<<1, 1, 0, s>>>(N.st, F.f), note_launch(); continue; }     // no row can take pivot step f
+        if ((rc = factor_block(fi, W, N.perm, s, PivotAsm{}))) return rc;
         if (ncb == 0) continue;
-        // U12 = L11^-1 A12[perm]: gather the pivot rows into the arena, then blocked TRSM in place
         T *Uf = Ua + F.U_off;
+        if (std::min(np, nr) == np && np <= FT_NP && nr <= FT_NR) {
+            if ((rc = tail(fi, W, N.perm, s, 0, ncb, 148))) return rc;
+            if ((fi & 255) == 255) CK(cudaGetLastError());
+            continue;
+        }
+        // U12 = L11^-1 A12[perm]: gather the pivot rows into the arena, then blocked TRSM in place
         prof.begin(s, PROF_U12, fm * (double)np * (double)np / 2.0 * (double)ncb, 3.0 * (double)(np * ncb) * vs);
         const int64_t npr = std::min(np, nr);
         if (npr == np && np <= U12_NP) {

@@ -44,6 +44,12 @@ struct DevNum {
     int64_t *rowid = nullptr, *p_lu = nullptr, *pinv = nullptr;
     int *ipiv = nullptr, *perm = nullptr;
     size_t cap_perm = 0;
+    // the look-ahead over chain fronts: a second working block and row order, the critical stream and its events
+    void *work2 = nullptr;
+    int *perm2 = nullptr;
+    size_t cap_work2 = 0, cap_perm2 = 0;
+    cudaStream_t crit = nullptr;
+    cudaEvent_t ev_lu = nullptr, ev_head = nullptr;
     DevStatus *st = nullptr;
     void *scratch = nullptr;
     void *rbuf = nullptr, *sbuf = nullptr, *xbuf = nullptr, *part = nullptr;

@@ -36,6 +36,7 @@ struct Front {
     int64_t row_off = 0;           // rowinit / device rowid [row_off .. + nrows)
     int64_t relcol_off = 0;        // relcol[relcol_off .. + ncols - npiv): parent local column of each CB column
     int64_t asm_begin = 0, asm_end = 0;
+    int64_t asm_mid = 0;           // [asm_begin, asm_mid): entries in the pivot columns; [asm_mid, asm_end): the others
     int64_t child_begin = 0, child_end = 0;
     int64_t L_off = 0, U_off = 0;  // factor arena (elements): nrows x npiv, npiv x (ncols - npiv)
     int64_t cb_off = 0;            // CB stack (elements): (nrows - npiv) x (ncols - npiv), column-major

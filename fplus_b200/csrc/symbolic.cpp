@@ -262,6 +262,17 @@ int build_plan(const fplus_symbolic_view &S, int64_t f_tail, int64_t nb_chain, i
                 }
         }
         F.asm_end = (int64_t)P.asm_src.size();
+        {   // the pivot-column entries first (a stable partition), so that the pivot block can be assembled on its own
+            std::vector<std::pair<int64_t, int64_t>> head, tail;
+            for (int64_t q = F.asm_begin; q < F.asm_end; q++) {
+                auto e = std::make_pair(P.asm_src[q], P.asm_dst[q]);
+                (P.asm_dst[q] / F.nrows < F.npiv ? head : tail).push_back(e);
+            }
+            int64_t q = F.asm_begin;
+            for (auto &e : head) { P.asm_src[q] = e.first; P.asm_dst[q] = e.second; q++; }
+            F.asm_mid = q;
+            for (auto &e : tail) { P.asm_src[q] = e.first; P.asm_dst[q] = e.second; q++; }
+        }
         for (int64_t t = 0; t < F.ncols; t++) pos[P.cols[F.col_off + t]] = -1;
         // levels
         int lv = 0;
