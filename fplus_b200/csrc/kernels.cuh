@@ -632,6 +632,9 @@ __device__ __forceinline__ int warp_argmax(const T *__restrict__ col, const int 
 // step-j pivot meanwhile, keep the multipliers (double-buffered) and store those of step j - 1 into column j - 1 (no
 // longer read by anyone).  One barrier per step.  No row swaps: the pivot row of step j is tagged j.  The singular test
 // uses the column thresholds staged in shared memory (squared moduli; the modulus itself near the threshold).
+// a named barrier for `count` threads (a multiple of 32); the non-aligned form, so that a warp need not be converged
+__device__ __forceinline__ void named_bar(int id, int count) { asm volatile("barrier.sync %0, %1;" ::"r"(id), "r"(count) : "memory"); }
+
 // The sources of a front's pivot block when the LU kernel assembles it itself (instead of reading it from the working
 // block): the original entries of the pivot columns and the pivot-column part of at most one child's contribution block.
 struct PivotAsm {
@@ -658,7 +661,7 @@ __global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int
     double *thr = reinterpret_cast<double *>(rid + nrows);         // npiv: pivot_rel * max |B(:, column)|
     int *tag = reinterpret_cast<int *>(thr + npiv);
     int *pos = tag + nrows;
-    __shared__ int s_bi[2], s_stop;
+    __shared__ int s_bi[2], s_stv[2], s_stop;                      // s_stv: the stop decision of steps j (j & 1)
     __shared__ T s_inv[2];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
     const int ne = npiv * nrows;
@@ -697,7 +700,14 @@ __global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int
     if (tid == 0) s_stop = st->code != 0 ? 3 : 0;
     __syncthreads();
     if (s_stop) return;
-    const int nu = nt - 32, ut = tid - 32;                          // update threads: warps 1 ..
+    // The SM sub-partition of warp w is w % 4: sub-partition 0 is left to the pivot warp (warps 4, 8, ... leave here),
+    // the update warps run on the other three.  The steps synchronise the remaining warps with a named barrier.
+    if ((warp & 3) == 0 && warp != 0) return;
+    const int nwarp = nt >> 5, nuw = (nwarp - 1) - (nwarp - 1) / 4;
+    const int nact = 32 * (1 + nuw);                                // the pivot warp and the update warps
+    const int uw = warp == 0 ? -1 : (warp >> 2) * 3 + (warp & 3) - 1;
+    const int at = (uw + 1) * 32 + lane;                            // index among the remaining threads
+    const int nu = 32 * nuw, ut = warp == 0 ? -1 : uw * 32 + lane;  // update threads
     const int R = (nrows + 31) & ~31;
     const int G = nu >= R ? nu / R : 1, rstep = nu >= R ? R : nu;
     const int my_i = ut >= 0 ? (nu >= R ? ut % R : ut) : 0, my_g = ut >= 0 ? (nu >= R ? ut / R : 0) : G;
@@ -712,6 +722,7 @@ __global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int
         if (sing) { const double bv = bi >= 0 ? vabs(A[(size_t)j * nrows + bi]) : 0.0; set_status(st, ST_SINGULAR, fcol + j, bv, t); stop = 1; }
         else if (bi >= nri) { set_status(st, ST_BORDER, front, sqrt(bv2), t); stop = 1; }
         s_bi[slot] = bi;
+        s_stv[slot] = stop;
         if (!stop) { s_inv[slot] = recip(A[(size_t)j * nrows + bi]); tag[bi] = j; }
         else s_stop = 1;
     };
@@ -738,10 +749,11 @@ __global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int
         double m;
         const int w = reduce(bv, bi, br, &m);
         decide(0, w, m, 0);
+        __syncwarp();
     }
-    __syncthreads();
+    named_bar(1, nact);
     for (int j = 0; j < npiv; j++) {
-        if (s_stop) return;
+        if (s_stv[j & 1]) return;                                   // decided before the last barrier, seen by all
         const int bi = s_bi[j & 1];
         const T inv = s_inv[j & 1];
         if (warp == 0) {
@@ -781,6 +793,7 @@ __global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int
                 double m;
                 const int w = reduce(bv, wi, br, &m);
                 decide(j + 1, w, m, (j + 1) & 1);
+                __syncwarp();
             }
         } else if (upd) {
             T *lc = lcol + (j & 1) * nrows;
@@ -807,7 +820,7 @@ __global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int
                 }
             }
         }
-        __syncthreads();
+        named_bar(1, nact);
     }
     // the last step's multipliers
     if (upd && my_g == 0 && npiv > 0) {
@@ -825,15 +838,15 @@ __global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int
             base += __popc(m);
         }
     }
-    __syncthreads();
-    for (int i = tid; i < nrows; i += nt) {
+    named_bar(1, nact);
+    for (int i = at; i < nrows; i += nact) {
         const int k = pos[i];
         perm[k] = i;
         rowid[k] = rid[i];
         if (k < steps) p_lu[fcol + k] = rid[i];
     }
     for (int c = 0; c < npiv; c++)
-        for (int i = tid; i < nrows; i += nt) Lout[pos[i] + (int64_t)c * nrows] = A[(size_t)c * nrows + i];
+        for (int i = at; i < nrows; i += nact) Lout[pos[i] + (int64_t)c * nrows] = A[(size_t)c * nrows + i];
 }
 
 // After the blocked (global-memory) pivoting of a large front's pivot block: the final row order from the swaps, the
