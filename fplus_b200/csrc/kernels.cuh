@@ -649,7 +649,7 @@ struct PivotAsm {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
+__global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
                                                     int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
                                                     int64_t *__restrict__ rowid, T *__restrict__ Lout, int *__restrict__ perm,
                                                     int64_t *__restrict__ p_lu, DevStatus *st, int64_t front, PivotAsm pa)
@@ -739,24 +739,104 @@ __global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int
         }
         return __shfl_sync(0xffffffffu, bi, __ffs(cand) - 1);
     };
-    if (warp == 0) {
-        double bv = -1.0; int bi = -1; int64_t br = INT64_MAX;
-        for (int i = lane; i < nrows; i += 32) {
-            const double a = sqmod(A[i]);
-            const int64_t r = rid[i];
-            if (a > bv || (a == bv && r < br)) { bv = a; bi = i; br = r; }
+    if (warp == 0 && nrows <= 128) {
+        // the pivot warp with its rows' state in registers (4 row slots per lane): row ids, not-yet-pivoted flags, and
+        // its own copy of the running column (it computes column j + 1 at step j and uses it as column j at step j + 1)
+        T xc[4];
+        int64_t rr[4];
+        bool al[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int i = lane + 32 * q;
+            al[q] = i < nrows;
+            rr[q] = al[q] ? rid[i] : INT64_MAX;
+            xc[q] = al[q] ? A[i] : VT<T>::zero();
         }
+        auto pick = [&](const T *xv, double *m, T *pv) -> int {      // the warp's winner among the live slots
+            double bv = -1.0; int wi = -1; int64_t br = INT64_MAX; T bx = VT<T>::zero();
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (!al[q]) continue;
+                const double a = sqmod(xv[q]);
+                if (a > bv || (a == bv && rr[q] < br)) { bv = a; wi = lane + 32 * q; br = rr[q]; bx = xv[q]; }
+            }
+            double mm = bv;
+            for (int o = 16; o > 0; o >>= 1) mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+            unsigned cand = __ballot_sync(0xffffffffu, wi >= 0 && bv == mm);
+            *m = mm;
+            if (cand == 0) { *pv = VT<T>::zero(); return -1; }
+            if ((cand & (cand - 1)) != 0) {
+                int64_t r2 = (cand >> lane) & 1u ? br : INT64_MAX;
+                for (int o = 16; o > 0; o >>= 1) { int64_t t = __shfl_xor_sync(0xffffffffu, r2, o); r2 = t < r2 ? t : r2; }
+                cand = __ballot_sync(0xffffffffu, ((cand >> lane) & 1u) && br == r2);
+            }
+            const int wl = __ffs(cand) - 1;
+            *pv = shfl_v<T>(bx, wl);
+            return __shfl_sync(0xffffffffu, wi, wl);
+        };
+        // lane 0 decides with the winner's value pv; 1 / pv to every lane
+        auto decide_v = [&](int j, int bi, double bv2, int slot, T pv) -> T {
+            T inv = VT<T>::zero();
+            if (lane == 0) {
+                const double t = thr[j];
+                int stop = 0;
+                bool sing = bi < 0 || !(bv2 > 0.0);
+                if (!sing && bv2 < 4.0 * t * t) sing = vabs(pv) < t;      // near the threshold: the modulus
+                if (sing) { set_status(st, ST_SINGULAR, fcol + j, bi >= 0 ? vabs(pv) : 0.0, t); stop = 1; }
+                else if (bi >= nri) { set_status(st, ST_BORDER, front, sqrt(bv2), t); stop = 1; }
+                s_bi[slot] = bi;
+                s_stv[slot] = stop;
+                if (!stop) { inv = recip(pv); s_inv[slot] = inv; tag[bi] = j; }
+            }
+            return shfl_v<T>(inv, 0);
+        };
         double m;
-        const int w = reduce(bv, bi, br, &m);
-        decide(0, w, m, 0);
+        T pv;
+        int bi = pick(xc, &m, &pv);
+        T inv = decide_v(0, bi, m, 0, pv);
+#pragma unroll
+        for (int q = 0; q < 4; q++) al[q] = al[q] && lane + 32 * q != bi;
         __syncwarp();
-    }
-    named_bar(1, nact);
-    for (int j = 0; j < npiv; j++) {
-        if (s_stv[j & 1]) return;                                   // decided before the last barrier, seen by all
-        const int bi = s_bi[j & 1];
-        const T inv = s_inv[j & 1];
-        if (warp == 0) {
+        named_bar(1, nact);
+        for (int j = 0; j < npiv; j++) {
+            if (s_stv[j & 1]) return;                               // decided before the last barrier, seen by all
+            if (j + 1 < npiv) {
+                T *cn = A + (size_t)(j + 1) * nrows;
+                const T pr = cn[bi];
+                T xb[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) xb[q] = al[q] ? cn[lane + 32 * q] : VT<T>::zero();
+#pragma unroll
+                for (int q = 0; q < 4; q++) xb[q] = sub(xb[q], mul(mul(xc[q], inv), pr));
+#pragma unroll
+                for (int q = 0; q < 4; q++) if (al[q]) cn[lane + 32 * q] = xb[q];
+                const int w = pick(xb, &m, &pv);
+                inv = decide_v(j + 1, w, m, (j + 1) & 1, pv);
+#pragma unroll
+                for (int q = 0; q < 4; q++) { xc[q] = xb[q]; al[q] = al[q] && lane + 32 * q != w; }
+                bi = w;
+                __syncwarp();
+            }
+            named_bar(1, nact);
+        }
+    } else if (warp == 0) {
+        {
+            double bv = -1.0; int bi = -1; int64_t br = INT64_MAX;
+            for (int i = lane; i < nrows; i += 32) {
+                const double a = sqmod(A[i]);
+                const int64_t r = rid[i];
+                if (a > bv || (a == bv && r < br)) { bv = a; bi = i; br = r; }
+            }
+            double m;
+            const int w = reduce(bv, bi, br, &m);
+            decide(0, w, m, 0);
+            __syncwarp();
+        }
+        named_bar(1, nact);
+        for (int j = 0; j < npiv; j++) {
+            if (s_stv[j & 1]) return;
+            const int bi = s_bi[j & 1];
+            const T inv = s_inv[j & 1];
             if (j + 1 < npiv) {
                 // column j + 1 for every row not yet pivoted, and its pivot, in one pass: the row slots of a lane are
                 // independent (loads first, then the arithmetic), 4 slots per round
@@ -795,32 +875,41 @@ __global__ void __launch_bounds__(1024) k_front_lu2(const T *__restrict__ W, int
                 decide(j + 1, w, m, (j + 1) & 1);
                 __syncwarp();
             }
-        } else if (upd) {
-            T *lc = lcol + (j & 1) * nrows;
-            const T *lp = lcol + ((j + 1) & 1) * nrows;
-            for (int i = my_i; i < nrows; i += rstep) {
-                if (my_g == 0 && j > 0 && tag[i] >= j) A[(size_t)(j - 1) * nrows + i] = lp[i];   // step j - 1's multiplier
-                if (tag[i] <= j) continue;
-                const T l = mul(A[(size_t)j * nrows + i], inv);
-                if (my_g == 0) lc[i] = l;
-                int c = j + 2 + my_g;
-                for (; c + 3 * G < npiv; c += 4 * G) {          // 4 independent columns per round, loads first
-                    T xv[4], pv[4];
+            named_bar(1, nact);
+        }
+    } else {
+        named_bar(1, nact);
+        for (int j = 0; j < npiv; j++) {
+            if (s_stv[j & 1]) return;
+            const int bi = s_bi[j & 1];
+            const T inv = s_inv[j & 1];
+            if (upd) {
+                T *lc = lcol + (j & 1) * nrows;
+                const T *lp = lcol + ((j + 1) & 1) * nrows;
+                for (int i = my_i; i < nrows; i += rstep) {
+                    if (my_g == 0 && j > 0 && tag[i] >= j) A[(size_t)(j - 1) * nrows + i] = lp[i];   // step j - 1's multiplier
+                    if (tag[i] <= j) continue;
+                    const T l = mul(A[(size_t)j * nrows + i], inv);
+                    if (my_g == 0) lc[i] = l;
+                    int c = j + 2 + my_g;
+                    for (; c + 3 * G < npiv; c += 4 * G) {          // 4 independent columns per round, loads first
+                        T xv[4], pv[4];
 #pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        xv[q] = A[(size_t)(c + q * G) * nrows + i];
-                        pv[q] = A[(size_t)(c + q * G) * nrows + bi];
+                        for (int q = 0; q < 4; q++) {
+                            xv[q] = A[(size_t)(c + q * G) * nrows + i];
+                            pv[q] = A[(size_t)(c + q * G) * nrows + bi];
+                        }
+#pragma unroll
+                        for (int q = 0; q < 4; q++) A[(size_t)(c + q * G) * nrows + i] = sub(xv[q], mul(l, pv[q]));
                     }
-#pragma unroll
-                    for (int q = 0; q < 4; q++) A[(size_t)(c + q * G) * nrows + i] = sub(xv[q], mul(l, pv[q]));
-                }
-                for (; c < npiv; c += G) {
-                    T *x = A + (size_t)c * nrows + i;
-                    *x = sub(*x, mul(l, A[(size_t)c * nrows + bi]));
+                    for (; c < npiv; c += G) {
+                        T *x = A + (size_t)c * nrows + i;
+                        *x = sub(*x, mul(l, A[(size_t)c * nrows + bi]));
+                    }
                 }
             }
+            named_bar(1, nact);
         }
-        named_bar(1, nact);
     }
     // the last step's multipliers
     if (upd && my_g == 0 && npiv > 0) {

@@ -372,8 +372,8 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         }
         if (sm <= SMEM_MAX) {
             const int R = (int)((nr + 31) & ~31);
-            int nt = 32 + (R <= 128 ? 4 * R : (R <= 480 ? R : 992));   // the pivot warp + the update warps
-            if (nt > 1024) nt = 1024;
+            int nt = 32 + (R <= 128 ? 4 * R : R);   // the pivot warp + the update warps
+            if (nt > 640) nt = 640;
             k_front_lu2<T><<<1, nt, sm, st>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel, N.rowid + F.row_off, Lf,
                                             perm, N.p_lu, N.st, fi, pa), note_launch();
         } else {
