@@ -1077,7 +1077,7 @@ __global__ void __launch_bounds__(256) k_u12_blk(const T *__restrict__ W, int64_
 }
 
 // The tail of a front with npiv <= 64 and nrows <= 128, in one pass over its contribution-block columns: for each tile of
-// 32 columns, the tile's rows are gathered in pivot order (perm; the next tile's values are loaded into registers while
+// TN columns (32; 8 for the few columns the next pivot block waits for), the tile's rows are gathered in pivot order (perm; the next tile's values are loaded into registers while
 // this one is computed), then per 16-row block of the pivot rows, the diagonal 16 x 16 unit-lower solve by half-warps
 // (one column each, 16 shuffle steps) and the update of every row below, pivot rows and contribution-block rows alike,
 // X[r, c] -= sum_k L[r, k] X[k, c], on the FP64 tensor cores (mma m8n8k4; complex as four real products).  Rows [0, npiv)
@@ -1085,23 +1085,37 @@ __global__ void __launch_bounds__(256) k_u12_blk(const T *__restrict__ W, int64_
 // blocked forward substitution with [L11; L21] of the front's columns.  L (real and imaginary planes) and the tile live
 // in shared memory with a leading dimension of 132 doubles (4 mod 16: the mma fragments of a half-warp hit 16 banks).
 constexpr int FT_TN = 32, FT_LD = 132, FT_NP = 64, FT_NR = 128, FT_THREADS = 512;
-template <typename T>
+template <typename T, int TN>
 __global__ void __launch_bounds__(FT_THREADS) k_front_tail(const T *__restrict__ W, int64_t ld, const int *__restrict__ perm,
                                                            int npiv, int nrows, int64_t ncb, int64_t cb0, int64_t cb1,
                                                            const T *__restrict__ Lb, T *__restrict__ U, T *__restrict__ CB,
                                                            const DevStatus *st)
 {
     constexpr bool CP = VT<T>::cplx_;
-    constexpr int PER = FT_NR * FT_TN / FT_THREADS;                // tile values per thread (8)
+    constexpr int PER = FT_NR * TN / FT_THREADS;                   // tile values per thread
     extern __shared__ __align__(16) double ft_smem[];
     double *sLr = ft_smem;                                          // L[m, k] at k * FT_LD + m
     double *sLi = sLr + (CP ? FT_NP * FT_LD : 0);
     double *sXr = sLr + (CP ? 2 : 1) * FT_NP * FT_LD;               // X[r, c] at c * FT_LD + r
-    double *sXi = sXr + (CP ? FT_TN * FT_LD : 0);
+    double *sXi = sXr + (CP ? TN * FT_LD : 0);
     __shared__ int sperm[FT_NR];
     if (st->code) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int M = nrows - npiv;
+    for (int i = tid; i < nrows; i += FT_THREADS) sperm[i] = perm[i];
+    __syncthreads();
+    // columns [cb0, cb1) of the contribution block (cb0 a multiple of the tile width)
+    const int64_t t0 = cb0 / TN, ntile = (cb1 + TN - 1) / TN;
+    T pre[PER];
+    auto fetch = [&](int64_t t) {
+        const int64_t c0 = t * TN;
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            const int e = tid + q * FT_THREADS, r = e % FT_NR, c = e / FT_NR;
+            pre[q] = (t < ntile && r < nrows && c0 + c < cb1) ? W[sperm[r] + (npiv + c0 + c) * ld] : VT<T>::zero();
+        }
+    };
+    fetch(t0 + blockIdx.x);                                          // in flight while L is staged
     for (int e0 = tid; e0 < npiv * nrows; e0 += 8 * FT_THREADS) {     // 8 loads in flight per thread
         T v[8];
 #pragma unroll
@@ -1114,24 +1128,11 @@ __global__ void __launch_bounds__(FT_THREADS) k_front_tail(const T *__restrict__
             }
         }
     }
-    for (int i = tid; i < nrows; i += FT_THREADS) sperm[i] = perm[i];
     __syncthreads();
-    // columns [cb0, cb1) of the contribution block (cb0 a multiple of the tile width)
-    const int64_t t0 = cb0 / FT_TN, ntile = (cb1 + FT_TN - 1) / FT_TN;
-    T pre[PER];
-    auto fetch = [&](int64_t t) {
-        const int64_t c0 = t * FT_TN;
-#pragma unroll
-        for (int q = 0; q < PER; q++) {
-            const int e = tid + q * FT_THREADS, r = e % FT_NR, c = e / FT_NR;
-            pre[q] = (t < ntile && r < nrows && c0 + c < cb1) ? W[sperm[r] + (npiv + c0 + c) * ld] : VT<T>::zero();
-        }
-    };
-    fetch(t0 + blockIdx.x);
     const int half = lane >> 4, hl = lane & 15;
     for (int64_t t = t0 + blockIdx.x; t < ntile; t += gridDim.x) {
-        const int64_t c0 = t * FT_TN;
-        const int tn = (int)(cb1 - c0 < FT_TN ? cb1 - c0 : FT_TN);
+        const int64_t c0 = t * TN;
+        const int tn = (int)(cb1 - c0 < TN ? cb1 - c0 : TN);
 #pragma unroll
         for (int q = 0; q < PER; q++) {
             const int e = tid + q * FT_THREADS, r = e % FT_NR, c = e / FT_NR;
@@ -1141,7 +1142,7 @@ __global__ void __launch_bounds__(FT_THREADS) k_front_tail(const T *__restrict__
         fetch(t + gridDim.x);                                       // in flight during this tile
         for (int kb = 0; kb < npiv; kb += 16) {
             const int w = npiv - kb < 16 ? npiv - kb : 16;
-            {   // the diagonal block: a half-warp per column, lane hl holds row kb + hl
+            if (2 * warp < TN) {   // the diagonal block: a half-warp per column, lane hl holds row kb + hl
                 const int c = 2 * warp + half;
                 double xr = hl < w ? sXr[c * FT_LD + kb + hl] : 0.0, xi = CP && hl < w ? sXi[c * FT_LD + kb + hl] : 0.0;
                 for (int i = 0; i < w; i++) {

@@ -275,7 +275,8 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_u12_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
-        CK(cudaFuncSetAttribute(k_front_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_front_tail<T, FT_TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_front_tail<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_u12_fused<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_u12_fused<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_u12_fused<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
@@ -403,16 +404,21 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         return FPLUS_OK;
     };
     // U12 and the CB for CB columns [c0, c1) by the fused tail kernel (at most `cap` CTAs)
-    auto tail = [&](int64_t fi, T *W, const int *perm, cudaStream_t st, int64_t c0, int64_t c1, int cap) {
+    auto tail = [&](int64_t fi, T *W, const int *perm, cudaStream_t st, int64_t c0, int64_t c1, int cap, bool narrow) {
         const Front &F = P.fronts[fi];
         const int64_t nr = F.nrows, np = F.npiv, ncb = F.ncols - F.npiv, M = nr - np;
         if (c1 <= c0) return FPLUS_OK;
         prof.begin(st, PROF_SCHUR, fm * ((double)np * (double)np / 2.0 + (double)M * (double)np) * (double)(c1 - c0),
                    (double)(2 * nr * (c1 - c0) + nr * np) * vs);
-        const size_t fsm = (size_t)(VT<T>::cplx_ ? 2 : 1) * (FT_NP + FT_TN) * FT_LD * sizeof(double);
-        const int blocks = (int)std::min<int64_t>((c1 - c0 + FT_TN - 1) / FT_TN, cap);
-        k_front_tail<T><<<blocks, FT_THREADS, fsm, st>>>(W, nr, perm, (int)np, (int)nr, ncb, c0, c1, La + F.L_off, Ua + F.U_off,
-                                                        CB + F.cb_off, N.st), note_launch();
+        const int tn = narrow ? 8 : FT_TN;
+        const size_t fsm = (size_t)(VT<T>::cplx_ ? 2 : 1) * (FT_NP + tn) * FT_LD * sizeof(double);
+        const int blocks = (int)std::min<int64_t>((c1 - c0 + tn - 1) / tn, cap);
+        if (narrow)
+            k_front_tail<T, 8><<<blocks, FT_THREADS, fsm, st>>>(W, nr, perm, (int)np, (int)nr, ncb, c0, c1, La + F.L_off,
+                                                               Ua + F.U_off, CB + F.cb_off, N.st), note_launch();
+        else
+            k_front_tail<T, FT_TN><<<blocks, FT_THREADS, fsm, st>>>(W, nr, perm, (int)np, (int)nr, ncb, c0, c1, La + F.L_off,
+                                                                   Ua + F.U_off, CB + F.cb_off, N.st), note_launch();
         prof.end(st);
         return FPLUS_OK;
     };
@@ -451,9 +457,9 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             CK(cudaStreamWaitEvent(s, N.ev_lu, 0));
             if (ncb > 0) {
                 const int64_t h = std::min<int64_t>(ncb, (hc[fi] + FT_TN - 1) / FT_TN * FT_TN);
-                if ((rc = tail(fi, W, perm, s, 0, h, 148))) return rc;
+                if ((rc = tail(fi, W, perm, s, 0, h, 148, true))) return rc;
                 CK(cudaEventRecord(N.ev_head, s));
-                if ((rc = tail(fi, W, perm, s, h, ncb, 147))) return rc;      // one SM left for the next pivot block
+                if ((rc = tail(fi, W, perm, s, h, ncb, 147, false))) return rc;      // one SM left for the next pivot block
             }
             if ((fi & 255) == 255) CK(cudaGetLastError());
             continue;
@@ -469,7 +475,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         if (ncb == 0) continue;
         T *Uf = Ua + F.U_off;
         if (std::min(np, nr) == np && np <= FT_NP && nr <= FT_NR) {
-            if ((rc = tail(fi, W, N.perm, s, 0, ncb, 148))) return rc;
+            if ((rc = tail(fi, W, N.perm, s, 0, ncb, 148, false))) return rc;
             if ((fi & 255) == 255) CK(cudaGetLastError());
             continue;
         }
