@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstring>
 #include <new>
+#include <thread>
 
 using namespace fpl;
 
@@ -84,20 +85,29 @@ static int factor_common(const fplus_symbolic *sym, const int64_t *Ap, const int
         errf(err, errlen, "the matrix has %ld nonzeros, the symbolic analysis %ld", (long)Ap[n], (long)sym->nnz);
         return FPLUS_ERR_BADARG;
     }
-    int rc = check_compressed(n, Ap, Ai, 1, err, errlen);
-    if (rc) return rc;
-    {
-        // the pattern must be the analysed one: compare with the permuted pattern through the gather map
-        const int64_t *Bp = sym->Bp.data(), *Bsrc = sym->Bsrc.data();
-        const int64_t *cp = sym->col_perm.data();
-        for (int64_t jj = 0; jj < n; jj++) {
-            const int64_t c = cp[jj];
-            if (Ap[c + 1] - Ap[c] != Bp[jj + 1] - Bp[jj] ) { errf(err, errlen, "the pattern differs from the analysed one (column %ld)", (long)c); return FPLUS_ERR_BADARG; }
-        }
-        for (int64_t q = 0; q < sym->nnz; q++) {
-            if (Ai[Bsrc[q]] != sym->row_perm[sym->Bi[q]]) { errf(err, errlen, "the pattern differs from the analysed one (entry %ld)", (long)Bsrc[q]); return FPLUS_ERR_BADARG; }
-        }
+    int rc = FPLUS_OK;
+    // The pattern must be the analysed one (which was checked canonical when analysed).  The column pointers are
+    // compared here; the row indices below, on a host thread while the GPU permutes and equilibrates the values (which
+    // it reads only through the analysed pattern's maps, so a different pattern cannot make it read out of bounds).
+    if (std::memcmp(Ap, sym->Ap0.data(), (size_t)(n + 1) * sizeof(int64_t)) != 0) {
+        rc = check_compressed(n, Ap, Ai, 1, err, errlen);
+        if (rc) return rc;
+        errf(err, errlen, "the pattern differs from the analysed one (column pointers)");
+        return FPLUS_ERR_BADARG;
     }
+
+    // the row indices: compared on another host thread while the values are checked, uploaded, permuted and
+    // equilibrated; a difference takes precedence over any other error
+    int prc = FPLUS_OK;
+    char perr[256] = {0};
+    std::thread checker([&]() {
+        if (sym->nnz > 0 && std::memcmp(Ai, sym->Ai0.data(), (size_t)sym->nnz * sizeof(int64_t)) != 0) {
+            prc = check_compressed(n, Ap, Ai, 1, perr, sizeof perr);
+            if (prc == FPLUS_OK) { errf(perr, sizeof perr, "the pattern differs from the analysed one (row indices)"); prc = FPLUS_ERR_BADARG; }
+        }
+    });
+    auto body = [&]() -> int {
+    int rc = FPLUS_OK;
     if (!ax_on_device) { rc = check_finite(Ap[n], Ax, is_complex, err, errlen); if (rc) return rc; }
     fplus_numeric *num = new (std::nothrow) fplus_numeric;
     if (!num) { errf(err, errlen, "out of memory"); return FPLUS_ERR_NOMEM; }
@@ -119,6 +129,8 @@ static int factor_common(const fplus_symbolic *sym, const int64_t *Ap, const int
         CKH(cudaEventRecord(N.ev0, N.stream));
         rc = dev_equilibrate(*D, N, opt->equilibrate, opt->ruiz_max_iter, opt->ruiz_tol, err, errlen);
         if (rc) return rc;
+        checker.join();
+        if (prc) return prc;
         CKH(cudaEventRecord(N.ev1, N.stream));
         CKH(cudaEventSynchronize(N.ev1));
         float ms = 0;
@@ -175,6 +187,15 @@ static int factor_common(const fplus_symbolic *sym, const int64_t *Ap, const int
     }
     *out = guard.release();
     return FPLUS_OK;
+    };
+    rc = body();
+    if (checker.joinable()) checker.join();
+    if (prc) {
+        if (*out) { delete *out; *out = nullptr; }
+        errf(err, errlen, "%s", perr);
+        return prc;
+    }
+    return rc;
 }
 
 extern "C" int fplus_factor(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex,

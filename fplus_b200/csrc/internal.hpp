@@ -44,6 +44,8 @@ struct fplus_symbolic {
     int64_t n_tau_rows = 0, n_tau_cols = 0;
     // the permuted pattern B = A[row_perm,:][:,col_perm] (canonical CSC) and, per entry of B, its position in A
     std::vector<int64_t> Bp, Bi, Bsrc;
+    // the analysed pattern itself (A's Ap, Ai): a factorization's pattern is compared with it
+    std::vector<int64_t> Ap0, Ai0;
     // the multifrontal structure, built on first use; rebuilt with a dense tail when a dense row is chosen as a pivot
     // before the tail (the pivot order is value dependent); guarded by mu
     mutable std::mutex mu;

@@ -81,11 +81,14 @@ __global__ void k_ruiz_rowmax(const int64_t *__restrict__ Bi, const T *__restric
         atomicMax(&rmax[Bi[p]], dbits(sqmod(Bx[p])));
 }
 
-// zero-row check, residual, row scale 1/sqrt(sqrt(max)), Dr *= scale (FPLUS src/equil.c:80-92)
-__global__ void k_ruiz_rowscale(int64_t n, unsigned long long *__restrict__ rmax, double *__restrict__ Dr, DevStatus *st)
+// zero-row check, residual, row scale 1/sqrt(sqrt(max)), Dr *= scale (FPLUS src/equil.c:80-92); the column maxima of
+// the coming column pass start at zero
+__global__ void k_ruiz_rowscale(int64_t n, unsigned long long *__restrict__ rmax, double *__restrict__ Dr,
+                                unsigned long long *__restrict__ cmax, DevStatus *st)
 {
     if (st->done || st->code) return;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        cmax[i] = 0ull;
         double m = bitsd(rmax[i]);
         if (m == 0.0) {           // the smallest zero row wins (the reference reports the first)
             atomicCAS(&((DevStatus *)st)->code, 0, ST_ZERO_ROW);
@@ -107,23 +110,29 @@ __global__ void k_first_zero(int64_t n, const unsigned long long *__restrict__ v
         if (bitsd(v[i]) == 0.0) atomicMin((unsigned long long *)&st->idx, (unsigned long long)i);
 }
 
-// per column (a warp each): scale by the row scales, then the column maximum of |b|^2 (FPLUS src/equil.c:93-147)
+// Column passes run over column segments of at most COL_SEG entries (seg: column, first entry, end; a warp each), so a
+// dense column is spread over many warps; a segment's maximum joins its column's by an integer atomicMax (the maximum
+// of non-negative doubles is their integer maximum, so the result does not depend on the order).
+constexpr int64_t COL_SEG = 1024;
+
+// scale by the row scales, then the column maximum of |b|^2 (FPLUS src/equil.c:93-147); cmax starts at zero
 template <typename T>
-__global__ void k_ruiz_colpass(const int64_t *__restrict__ Bp, const int64_t *__restrict__ Bi, T *__restrict__ Bx,
-                               int64_t n, const unsigned long long *__restrict__ rscale, unsigned long long *__restrict__ cmax,
+__global__ void k_ruiz_colpass(const int64_t *__restrict__ seg, int64_t nseg, const int64_t *__restrict__ Bi, T *__restrict__ Bx,
+                               const unsigned long long *__restrict__ rscale, unsigned long long *__restrict__ cmax,
                                const DevStatus *st)
 {
     if (st->done || st->code) return;
     const int lane = threadIdx.x & 31;
-    for (int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; j < n; j += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < nseg; g += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int64_t j = seg[3 * g], p1 = seg[3 * g + 2];
         double cm = 0.0;
-        for (int64_t p = Bp[j] + lane; p < Bp[j + 1]; p += 32) {
+        for (int64_t p = seg[3 * g + 1] + lane; p < p1; p += 32) {
             T v = scal(Bx[p], bitsd(rscale[Bi[p]]));
             Bx[p] = v;
             cm = fmax(cm, sqmod(v));
         }
         for (int o = 16; o > 0; o >>= 1) cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, o));
-        if (lane == 0) cmax[j] = dbits(cm);
+        if (lane == 0) atomicMax(&cmax[j], dbits(cm));
     }
 }
 
@@ -143,14 +152,15 @@ __global__ void k_ruiz_colscale(int64_t n, unsigned long long *__restrict__ cmax
 }
 
 template <typename T>
-__global__ void k_ruiz_colapply(const int64_t *__restrict__ Bp, T *__restrict__ Bx, int64_t n,
+__global__ void k_ruiz_colapply(const int64_t *__restrict__ seg, int64_t nseg, T *__restrict__ Bx,
                                 const unsigned long long *__restrict__ cscale, const DevStatus *st)
 {
     if (st->done || st->code) return;
     const int lane = threadIdx.x & 31;
-    for (int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; j < n; j += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const double c = bitsd(cscale[j]);
-        for (int64_t p = Bp[j] + lane; p < Bp[j + 1]; p += 32) Bx[p] = scal(Bx[p], c);
+    for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < nseg; g += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const double c = bitsd(cscale[seg[3 * g]]);
+        const int64_t p1 = seg[3 * g + 2];
+        for (int64_t p = seg[3 * g + 1] + lane; p < p1; p += 32) Bx[p] = scal(Bx[p], c);
     }
 }
 
@@ -172,15 +182,17 @@ __global__ void k_fold(double *Dr, double *Dc, int64_t n, double h)
 }
 
 // the largest modulus of each column of the scaled B (the singular-pivot threshold, FPLUS src/factor_sn_panel.inc:50)
+// (over column segments; cm, the bits of non-negative doubles, starts at zero)
 template <typename T>
-__global__ void k_colmax(const int64_t *__restrict__ Bp, const T *__restrict__ Bx, int64_t n, double *__restrict__ cm)
+__global__ void k_colmax(const int64_t *__restrict__ seg, int64_t nseg, const T *__restrict__ Bx, unsigned long long *__restrict__ cm)
 {
     const int lane = threadIdx.x & 31;
-    for (int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; j < n; j += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < nseg; g += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         double m = 0.0;
-        for (int64_t p = Bp[j] + lane; p < Bp[j + 1]; p += 32) m = fmax(m, vabs(Bx[p]));
+        const int64_t p1 = seg[3 * g + 2];
+        for (int64_t p = seg[3 * g + 1] + lane; p < p1; p += 32) m = fmax(m, vabs(Bx[p]));
         for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if (lane == 0) cm[j] = m;
+        if (lane == 0) atomicMax(&cm[seg[3 * g]], dbits(m));
     }
 }
 

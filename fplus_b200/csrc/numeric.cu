@@ -70,7 +70,7 @@ template <typename T> static int upload(const std::vector<T> &h, T **d, char *er
 DevPlan::~DevPlan()
 {
     for (void *p : {(void *)cols, (void *)relcol, (void *)rowinit, (void *)asm_src, (void *)asm_dst, (void *)Bp, (void *)Bi,
-                    (void *)Bsrc, (void *)row_perm, (void *)col_perm})
+                    (void *)Bsrc, (void *)row_perm, (void *)col_perm, (void *)seg})
         if (p) cudaFree(p);
 }
 
@@ -88,6 +88,15 @@ int dev_upload_plan(const fplus_symbolic *S, const FrontPlan &P, DevPlan &D, cha
     if ((rc = upload(S->Bsrc, &D.Bsrc, err, errlen))) return rc;
     if ((rc = upload(S->row_perm, &D.row_perm, err, errlen))) return rc;
     if ((rc = upload(S->col_perm, &D.col_perm, err, errlen))) return rc;
+    {
+        std::vector<int64_t> seg;
+        for (int64_t j = 0; j < S->n; j++)
+            for (int64_t p0 = S->Bp[j]; p0 < S->Bp[j + 1]; p0 += COL_SEG) {
+                seg.push_back(j); seg.push_back(p0); seg.push_back(std::min<int64_t>(p0 + COL_SEG, S->Bp[j + 1]));
+            }
+        D.nseg = (int64_t)seg.size() / 3;
+        if ((rc = upload(seg, &D.seg, err, errlen))) return rc;
+    }
     return FPLUS_OK;
 }
 
@@ -221,17 +230,18 @@ static int run_equil(const DevPlan &D, DevNum &N, int equilibrate, int max_iter,
         for (int it = 0; it < max_iter; it++) {
             CK(cudaMemsetAsync(rmax, 0, (size_t)n * 8, s));
             k_ruiz_rowmax<T><<<nblk(nnz), 256, 0, s>>>(D.Bi, Bx, nnz, rmax, N.st), note_launch();
-            k_ruiz_rowscale<<<nblk(n), 256, 0, s>>>(n, rmax, N.Drp, N.st), note_launch();
+            k_ruiz_rowscale<<<nblk(n), 256, 0, s>>>(n, rmax, N.Drp, cmax, N.st), note_launch();
             k_first_zero<<<nblk(n), 256, 0, s>>>(n, rmax, N.st, ST_ZERO_ROW), note_launch();
-            k_ruiz_colpass<T><<<nblk(32 * n), 256, 0, s>>>(D.Bp, D.Bi, Bx, n, rmax, cmax, N.st), note_launch();
+            k_ruiz_colpass<T><<<nblk(32 * D.nseg), 256, 0, s>>>(D.seg, D.nseg, D.Bi, Bx, rmax, cmax, N.st), note_launch();
             k_ruiz_colscale<<<nblk(n), 256, 0, s>>>(n, cmax, N.Dcp, N.st), note_launch();
             k_first_zero<<<nblk(n), 256, 0, s>>>(n, cmax, N.st, ST_ZERO_COL), note_launch();
-            k_ruiz_colapply<T><<<nblk(32 * n), 256, 0, s>>>(D.Bp, Bx, n, cmax, N.st), note_launch();
+            k_ruiz_colapply<T><<<nblk(32 * D.nseg), 256, 0, s>>>(D.seg, D.nseg, Bx, cmax, N.st), note_launch();
             k_ruiz_check<<<1, 1, 0, s>>>(N.st, tol), note_launch();
         }
         if (k4 != 0) k_fold<<<nblk(n), 256, 0, s>>>(N.Drp, N.Dcp, n, std::ldexp(1.0, k4 / 2)), note_launch();
     }
-    k_colmax<T><<<nblk(32 * n), 256, 0, s>>>(D.Bp, Bx, n, N.colmax), note_launch();
+    CK(cudaMemsetAsync(N.colmax, 0, (size_t)n * 8, s));
+    k_colmax<T><<<nblk(32 * D.nseg), 256, 0, s>>>(D.seg, D.nseg, Bx, (unsigned long long *)N.colmax), note_launch();
     CK(cudaGetLastError());
     DevStatus h;
     CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -297,20 +307,11 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     // columns that are the parent's pivot columns (the head), signals the critical stream, and forms the rest of the
     // front's tail while the critical stream moves on to the parent.  Consecutive such fronts alternate between two
     // working blocks and two row orders.
-    auto head_cols = [&](const Front &G) -> int64_t {       // G's CB columns inside its parent's pivot columns (a prefix), or -1
-        if (G.parent < 0) return 0;
-        const int64_t ncb = G.ncols - G.npiv, pnp = P.fronts[G.parent].npiv;
-        int64_t h = 0;
-        while (h < ncb && P.relcol[G.relcol_off + h] < pnp) h++;
-        for (int64_t c = h; c < ncb; c++) if (P.relcol[G.relcol_off + c] < pnp) return -1;
-        return h;
-    };
-    std::vector<int64_t> hc((size_t)nf, -1);
+    const std::vector<int64_t> &hc = P.head_cols;
     std::vector<char> pipe((size_t)nf, 0);
     bool any_pipe = false;
     for (int64_t fi = 0; fi < nf; fi++) {
         const Front &F = P.fronts[fi];
-        hc[fi] = head_cols(F);
         const int64_t nr = F.nrows, np = F.npiv, ncb = F.ncols - F.npiv;
         bool ok = F.dense && np > 0 && np <= nr && np <= FT_NP && nr <= FT_NR && front_lu_smem(nr, np, vs) <= SMEM_MAX;
         ok = ok && (ncb == 0 || (F.parent == fi + 1 && hc[fi] >= 0));
@@ -429,11 +430,13 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         const Front &F = P.fronts[fi];
         const int64_t nr = F.nrows, nc = F.ncols, np = F.npiv, ncb = nc - np;
         if (pipe[fi]) {
-            if (!in_pipe) { CK(cudaEventRecord(N.ev_head, s)); in_pipe = true; }   // the critical stream joins the bulk one
+            // critical stream: [pivot-column assembly], LU, then (once the bulk stream has assembled the other
+            // columns) the tail on the CB columns that are the parent's pivot columns; bulk stream: the assembly of the
+            // other columns, then (after the LU) the rest of the tail
+            if (!in_pipe) { CK(cudaEventRecord(N.ev_head, s)); CK(cudaStreamWaitEvent(A, N.ev_head, 0)); in_pipe = true; }
             T *W = (T *)(wsel ? N.work2 : N.work);
             int *perm = wsel ? N.perm2 : N.perm;
             wsel ^= 1;
-            CK(cudaStreamWaitEvent(A, N.ev_head, 0));
             PivotAsm pa{};
             if (F.child_end - F.child_begin <= 1) {
                 // the LU kernel assembles the pivot block itself (from at most one child)
@@ -453,18 +456,20 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             } else if ((rc = assemble(fi, W, A, ncb > 0 ? 1 : 0))) return rc;
             if ((rc = factor_block(fi, W, perm, A, pa))) return rc;
             CK(cudaEventRecord(N.ev_lu, A));
-            if (ncb > 0 && (rc = assemble(fi, W, s, 2))) return rc;
-            CK(cudaStreamWaitEvent(s, N.ev_lu, 0));
             if (ncb > 0) {
-                const int64_t h = std::min<int64_t>(ncb, (hc[fi] + FT_TN - 1) / FT_TN * FT_TN);
-                if ((rc = tail(fi, W, perm, s, 0, h, 148, true))) return rc;
+                if ((rc = assemble(fi, W, s, 2))) return rc;
                 CK(cudaEventRecord(N.ev_head, s));
-                if ((rc = tail(fi, W, perm, s, h, ncb, 147, false))) return rc;      // one SM left for the next pivot block
+                CK(cudaStreamWaitEvent(s, N.ev_lu, 0));
+                const int64_t h = std::min<int64_t>(ncb, (hc[fi] + FT_TN - 1) / FT_TN * FT_TN);
+                // at most 139 CTAs: one SM stays free for the next LU and eight for the next tail head
+                if ((rc = tail(fi, W, perm, s, h, ncb, 139, false))) return rc;
+                CK(cudaStreamWaitEvent(A, N.ev_head, 0));
+                if ((rc = tail(fi, W, perm, A, 0, h, 148, true))) return rc;
             }
             if ((fi & 255) == 255) CK(cudaGetLastError());
             continue;
         }
-        in_pipe = false;       // the bulk stream has waited for the last pivot block of the critical stream
+        if (in_pipe) { CK(cudaEventRecord(N.ev_lu, A)); CK(cudaStreamWaitEvent(s, N.ev_lu, 0)); in_pipe = false; }
         T *W = (T *)N.work;
         T *Lf = La + F.L_off;
         const int64_t ld = nr;
@@ -515,6 +520,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         }
         if ((fi & 255) == 255) CK(cudaGetLastError());
     }
+    if (in_pipe) { CK(cudaEventRecord(N.ev_lu, A)); CK(cudaStreamWaitEvent(s, N.ev_lu, 0)); }    // the bulk stream joins
     CK(cudaGetLastError());
     k_pinv<<<nblk(N.n), 256, 0, s>>>(N.p_lu, N.pinv, N.n, N.st), note_launch();
     DevStatus h;

@@ -25,6 +25,9 @@ struct DevPlan {
     int device = -1;
     int64_t *cols = nullptr, *relcol = nullptr, *rowinit = nullptr, *asm_src = nullptr, *asm_dst = nullptr;
     int64_t *Bp = nullptr, *Bi = nullptr, *Bsrc = nullptr, *row_perm = nullptr, *col_perm = nullptr;
+    // B's columns cut into segments of at most 1024 entries (column, first entry, end), for the column passes
+    int64_t *seg = nullptr;
+    int64_t nseg = 0;
     ~DevPlan();
 };
 

@@ -443,6 +443,8 @@ extern "C" int fplus_analyze_ord(int64_t n, const int64_t *Ap, const int64_t *Ai
         // the permuted pattern B = A[row_perm, :][:, col_perm] (rows ascending in each column) and its gather map
         std::vector<int64_t> inv((size_t)(n > 0 ? n : 1));
         for (int64_t i = 0; i < n; i++) inv[sym->row_perm[i]] = i;
+        sym->Ap0.assign(Ap, Ap + n + 1);
+        sym->Ai0.assign(Ai, Ai + nnz);
         sym->Bp.assign((size_t)n + 1, 0);
         sym->Bi.resize((size_t)nnz);
         sym->Bsrc.resize((size_t)nnz);

@@ -52,6 +52,8 @@ struct FrontPlan {
     std::vector<int64_t> cols, relcol, children, rowinit;
     std::vector<int64_t> asm_src, asm_dst;     // B entry -> offset in the front's working block
     std::vector<int64_t> col_front;            // B column -> front
+    std::vector<int64_t> head_cols;            // per front: how many of its CB columns lie in its parent's pivot columns,
+                                               // which come first (-1: they do not come first; 0 without a parent)
     int64_t L_size = 0, U_size = 0, cb_size = 0, work_size = 0, rows_total = 0;
     int64_t max_nrows = 0, max_ncols = 0, max_npiv = 0;
     double flops_real = 0;         // multiply-adds of the dense fronts (partial factorization), real count

@@ -290,6 +290,16 @@ int build_plan(const fplus_symbolic_view &S, int64_t f_tail, int64_t nb_chain, i
         }
     }
     P.rows_total = (int64_t)P.rowinit.size();
+    P.head_cols.assign(P.fronts.size(), 0);
+    for (size_t g = 0; g < P.fronts.size(); g++) {
+        const Front &G = P.fronts[g];
+        if (G.parent < 0) continue;
+        const int64_t ncb = G.ncols - G.npiv, pnp = P.fronts[(size_t)G.parent].npiv;
+        int64_t h = 0;
+        while (h < ncb && P.relcol[G.relcol_off + h] < pnp) h++;
+        for (int64_t c = h; c < ncb && h >= 0; c++) if (P.relcol[G.relcol_off + c] < pnp) h = -1;
+        P.head_cols[g] = h;
+    }
 
     // ---- factor arena and the CB stack (children's CBs are popped by the parent, in processing order)
     int64_t lo = 0, uo = 0;
