@@ -185,6 +185,71 @@ def reference_sample(workload_name, reps=1):
     return float(np.median(times)) * scale, float(np.median(times)), be, desc, threads, scale
 
 
+def run_profile_once(args):
+    """One factor + solve inside a profiler range (after a warm factorization that caches the plan), then the per-class
+    algorithmic flops and bytes of that factorization (the library's own counts) as one JSON line."""
+    import torch
+    import fplus_b200 as F
+    torch.cuda.init()
+    n, Ap, Ai, Ax, b, desc = workload(args.workload, args.modes)
+    S = F.analyze(n, Ap, Ai)
+    N = S.factor(Ax)
+    N.solve(b)
+    del N
+    torch.cuda.synchronize()
+    F.profile(True)
+    torch.cuda.cudart().cudaProfilerStart()
+    N = S.factor(Ax)
+    N.solve(b)
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStop()
+    prof = {F.PROFILE_CLASSES[c]: F.profile_read(c) for c in F.PROFILE_CLASSES}
+    F.profile(False)
+    print(json.dumps({"profile_once": desc, "classes": prof}))
+
+
+def traffic_ratio(kernel_class):
+    """DRAM bytes per algorithmic byte of a kernel class's launches, from the committed ncu summary of that kernel
+    (profiles/*.md, the line 'dram_to_algorithmic_bytes: R'), or (None, reason)."""
+    name = {"front_lu": "k_front_lu2_pencil_n4096.md", "schur_gemm": "k_front_tail_pencil_n16384.md"}.get(kernel_class)
+    if name is None:
+        return None, "no ncu summary for this class"
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(path):
+            if line.startswith("dram_to_algorithmic_bytes:"):
+                return float(line.split(":", 1)[1]), f"profiles/{name} (ncu dram__bytes_read.sum + dram__bytes_write.sum)"
+    except OSError:
+        pass
+    return None, f"profiles/{name} absent"
+
+
+def run_shift_batch(S, n, modes, count, b):
+    """count shifts A - sigma_k B (sigma_k = 0.3 + 1.7i + 0.1 k) of the pencil on its one analysis: factor + solve one by
+    one, then through fplus_b200_factor_batch / solve_batch (concurrent).  Host wall time around the synchronous calls."""
+    import fplus_b200 as F
+    import oracle as O
+    from fplus_b200 import workloads as W
+    _, Ap, Ai, A0 = W.pencil(modes=modes, sigma=0.0)
+    Bv = A0 - W.pencil(modes=modes, sigma=1.0)[3]           # B's values on A's pattern (the pencil is linear in sigma)
+    Axs = [A0 - (0.3 + 1.7j + 0.1 * k) * Bv for k in range(count)]
+    t0 = time.perf_counter()
+    for Ax in Axs:
+        N = S.factor(Ax)
+        N.solve(b)
+        del N
+    seq = (time.perf_counter() - t0) * 1e3
+    F.solve_batch(F.factor_batch([S] * 2, Axs[:2]), [b, b])          # warm-up of the worker path
+    t0 = time.perf_counter()
+    Ns = F.factor_batch([S] * count, Axs, nworkers=count)
+    Xs = F.solve_batch(Ns, [b] * count, nworkers=count)
+    par = (time.perf_counter() - t0) * 1e3
+    be = max(O.backward_error(n, Ap, Ai, Axs[k], Xs[k], b) for k in range(count))
+    return {"workload": f"{count} shifts sigma_k = 0.3+1.7i+0.1k of the pencil, one analysis, nrhs 1",
+            "ms_per_matrix": par / count, "sequential_ms_per_matrix": seq / count, "speedup": seq / par,
+            "berr_max": be, "timing": "host wall clock around the synchronous fplus calls (host values, e2e)"}
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -214,6 +279,7 @@ def run_b200_arm(args, rank, world):
     import torch
     import fplus_b200 as F
     import oracle as O
+    from fplus_b200 import workloads as W
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -314,10 +380,40 @@ def run_b200_arm(args, rank, world):
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "peak_source": ("cuBLAS " + ("ZGEMM" if cplx else "DGEMM") + " 8192^3 measured in bench.py (FP64 tensor "
                                 "path; the measured-peaks file has bf16 and HBM only)")}
+    ratio, rsrc = traffic_ratio(dom)
     roof.update({"kernel_class": dom, "launches": p["count"], "avg_launch_us": 1e3 * p["ms"] / max(p["count"], 1),
                  "algorithmic_per_launch": (p["flops"] if dom != "assemble" else p["bytes"]) / max(p["count"], 1),
-                 "traffic": None,
+                 "algorithmic_bytes_per_launch": p["bytes"] / max(p["count"], 1),
+                 "traffic": None if ratio is None else ratio * p["bytes"] / max(p["count"], 1),
+                 "traffic_source": rsrc,
                  "classes_ms": {k: round(v["ms"], 3) for k, v in prof.items()}})
+
+    # the solve with 16 right-hand sides (the configuration's second nrhs)
+    solve16 = None
+    if args.workload == "pencil":
+        N16 = S.factor(Ad, device=True)
+        B16 = torch.from_numpy(W.rhs(n, 16, cplx, 5)).to(dev)       # (16, n): column-major n x 16
+        N16.solve_device(B16.clone(), 0)
+        ts = []
+        for _ in range(3):
+            Bc = B16.clone()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            N16.solve_device(Bc, 0)
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        X16 = Bc.cpu().numpy().T
+        B16h = B16.cpu().numpy().T
+        be16 = max(O.backward_error(n, Ap, Ai, Ax, X16[:, r], B16h[:, r]) for r in range(16))
+        solve16 = {"nrhs": 16, "ms": float(np.median(ts)), "berr_max": be16}
+        del N16
+
+    # the batch form: shifts sigma_k of the same pencil on one analysis, factored and solved concurrently
+    batch = None
+    if args.workload == "pencil" and args.batch > 0 and world == 1:
+        batch = run_shift_batch(S, n, args.modes, args.batch, b)
 
     if rank != 0:
         return
@@ -338,7 +434,7 @@ def run_b200_arm(args, rank, world):
             "e2e": {"value": ms_e2e / world, "unit": "ms", "h2d_bytes_per_step": int(Ap[-1]) * vsz + n * vsz,
                     "d2h_bytes_per_step": n * vsz},
             "gpu_launches": int(launches),
-            "clocks": clocks, "roofline": roof, "cpu_baseline": cpu}
+            "clocks": clocks, "roofline": roof, "cpu_baseline": cpu, "solve_nrhs16": solve16, "batch": batch}
     print(json.dumps(line))
 
 
@@ -352,6 +448,10 @@ def main():
     ap.add_argument("--modes", type=int, default=8,
                     help="Fourier modes of the pencil workload (8: n = 32768, the benchmark; 1: n = 4096, for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch", type=int, default=8, help="shifts in the batch measurement (0: none)")
+    ap.add_argument("--profile-once", action="store_true",
+                    help="for ncu --profile-from-start off: one warm factorization, then exactly one factor + solve "
+                         "between cudaProfilerStart / Stop; prints that factorization's algorithmic work per class")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -361,7 +461,9 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        if args.impl == "reference":
+        if args.profile_once:
+            run_profile_once(args)
+        elif args.impl == "reference":
             run_reference_arm(args, rank, world)
         else:
             run_b200_arm(args, rank, world)

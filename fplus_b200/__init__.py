@@ -59,7 +59,8 @@ FPLUS_H_SYMBOLS = [
 FPLUS_B200_H_SYMBOLS = [
     "fplus_b200_numeric_info", "fplus_b200_use_stream", "fplus_b200_factor_dev", "fplus_b200_solve_dev",
     "fplus_b200_interior_order", "fplus_b200_plan_size", "fplus_b200_plan_export", "fplus_b200_launch_count",
-    "fplus_b200_profile", "fplus_b200_profile_read", "fplus_b200_solve_dev_noalloc",
+    "fplus_b200_profile", "fplus_b200_profile_read", "fplus_b200_solve_dev_noalloc", "fplus_b200_factor_batch",
+    "fplus_b200_solve_batch",
 ]
 
 _lib = None
@@ -96,6 +97,11 @@ def lib():
                               ctypes.c_size_t]
     L.fplus_b200_solve_dev.argtypes = L.fplus_solve.argtypes
     L.fplus_b200_solve_dev_noalloc.argtypes = L.fplus_solve.argtypes
+    L.fplus_b200_factor_batch.argtypes = [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_int, ctypes.POINTER(Options), ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_b200_solve_batch.argtypes = [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_numeric_factors.argtypes = [ctypes.c_void_p]
     L.fplus_numeric_factors.restype = ctypes.POINTER(Factors)
     for f in ("fplus_numeric_p", "fplus_numeric_q"):
@@ -218,6 +224,12 @@ class Numeric:
         _check(rc, err)
         self.n = sym.n
 
+    @classmethod
+    def _from_handle(cls, sym, h, is_complex):
+        self = cls.__new__(cls)
+        self.sym, self._h, self.is_complex, self.n = sym, ctypes.c_void_p(h), bool(is_complex), sym.n
+        return self
+
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None and self._h.value:
             _lib.fplus_numeric_free(self._h)
@@ -305,6 +317,45 @@ def profile_read(cls: int):
 
 def analyze(n, Ap, Ai, options=None, **kw) -> Symbolic:
     return Symbolic(n, Ap, Ai, options, **kw)
+
+
+def factor_batch(syms, Axs, options=None, nworkers=8):
+    """fplus_b200_factor_batch: factor matrix k (pattern syms[k], values Axs[k]) for every k, concurrently on the GPU.
+    Returns the list of Numeric objects (raises FplusError with the first failure's code and message)."""
+    count = len(syms)
+    if count != len(Axs):
+        raise FplusError(FPLUS_ERR_BADARG, "syms and Axs differ in length")
+    cplx = any(np.iscomplexobj(a) for a in Axs)
+    vals = [np.ascontiguousarray(a, dtype=np.complex128 if cplx else np.float64) for a in Axs]
+    VP = ctypes.c_void_p * count
+    P64 = _i64p * count
+    hs = (ctypes.c_void_p * count)()
+    rcs = (ctypes.c_int * count)()
+    err = ctypes.create_string_buffer(512)
+    opts = options if options is not None else (syms[0].options if count else Options())
+    rc = lib().fplus_b200_factor_batch(count, VP(*[s._h for s in syms]), P64(*[_p64(s.Ap) for s in syms]),
+                                       P64(*[_p64(s.Ai) for s in syms]), VP(*[v.ctypes.data for v in vals]), int(cplx),
+                                       ctypes.byref(opts), nworkers, hs, rcs, err, 512)
+    out = [Numeric._from_handle(syms[k], hs[k], cplx) if hs[k] else None for k in range(count)]
+    _check(rc, err)
+    return out
+
+
+def solve_batch(nums, bs, trans=0, nworkers=8):
+    """fplus_b200_solve_batch: x_k with op(A_k) x_k = b_k for every k, concurrently; returns the list of solutions."""
+    count = len(nums)
+    Xs = []
+    for N, b in zip(nums, bs):
+        b = np.asarray(b)
+        Xs.append(np.array(b.reshape(N.n, -1), dtype=np.complex128 if N.is_complex else np.float64, order="F", copy=True))
+    VP = ctypes.c_void_p * count
+    I64 = ctypes.c_int64 * count
+    rcs = (ctypes.c_int * count)()
+    err = ctypes.create_string_buffer(512)
+    rc = lib().fplus_b200_solve_batch(count, VP(*[N._h.value for N in nums]), VP(*[X.ctypes.data for X in Xs]),
+                                      I64(*[X.shape[1] for X in Xs]), I64(*[N.n for N in nums]), trans, nworkers, rcs, err, 512)
+    _check(rc, err)
+    return [X[:, 0] if np.asarray(b).ndim == 1 else X for X, b in zip(Xs, bs)]
 
 
 def interior_order(n, Ap, Ai, trow=None, tcol=None):

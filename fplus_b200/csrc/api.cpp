@@ -8,6 +8,9 @@
 #include <cstring>
 #include <new>
 #include <thread>
+#include <string>
+#include <functional>
+#include <atomic>
 
 using namespace fpl;
 
@@ -249,6 +252,68 @@ static int solve_common(const fplus_numeric *num, void *b, int64_t nrhs, int64_t
     }
     N.stream = saved;
     return rc;
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Batches: independent factorizations / solves run concurrently.  Each numeric object has its own CUDA stream (the
+// worker threads leave fplus_b200_use_stream unset), so the pivot-block chains of different matrices, each on one SM,
+// overlap on the GPU, as do their bulk kernels.  The work itself is the single-matrix path: the results are those of
+// fplus_factor / fplus_solve called one by one.
+static int run_batch(int64_t count, int nworkers, const std::function<int(int64_t, char *, size_t)> &job, int *rcs, char *err,
+                     size_t errlen)
+{
+    if (count < 0) { errf(err, errlen, "count must be >= 0"); return FPLUS_ERR_BADARG; }
+    if (nworkers <= 0) nworkers = 8;
+    if (nworkers > count) nworkers = (int)count;
+    std::atomic<int64_t> next{0};
+    std::vector<int> rc_local((size_t)count, FPLUS_OK);
+    std::vector<std::string> msg((size_t)count);
+    auto worker = [&]() {
+        char e[512];
+        for (;;) {
+            const int64_t k = next.fetch_add(1);
+            if (k >= count) break;
+            e[0] = 0;
+            rc_local[(size_t)k] = job(k, e, sizeof e);
+            if (rc_local[(size_t)k]) msg[(size_t)k] = e;
+        }
+    };
+    std::vector<std::thread> pool;
+    try {
+        for (int w = 0; w < nworkers; w++) pool.emplace_back(worker);
+    } catch (...) {
+        for (auto &t : pool) t.join();
+        errf(err, errlen, "could not start the worker threads");
+        return FPLUS_ERR_NOMEM;
+    }
+    for (auto &t : pool) t.join();
+    int rc = FPLUS_OK;
+    for (int64_t k = 0; k < count; k++) {
+        if (rcs) rcs[k] = rc_local[(size_t)k];
+        if (rc == FPLUS_OK && rc_local[(size_t)k]) { rc = rc_local[(size_t)k]; errf(err, errlen, "matrix %ld: %s", (long)k, msg[(size_t)k].c_str()); }
+    }
+    return rc;
+}
+
+extern "C" int fplus_b200_factor_batch(int64_t count, const fplus_symbolic *const *syms, const int64_t *const *Ap,
+                                       const int64_t *const *Ai, const void *const *Ax, int is_complex,
+                                       const fplus_options *opt, int nworkers, fplus_numeric **nums, int *rcs, char *err,
+                                       size_t errlen)
+{
+    if (count > 0 && (!syms || !Ap || !Ai || !Ax || !nums)) { errf(err, errlen, "NULL array"); return FPLUS_ERR_BADARG; }
+    for (int64_t k = 0; k < count; k++) nums[k] = nullptr;
+    return run_batch(count, nworkers, [&](int64_t k, char *e, size_t el) {
+        return factor_common(syms[k], Ap[k], Ai[k], Ax[k], 0, is_complex, opt, &nums[k], e, el);
+    }, rcs, err, errlen);
+}
+
+extern "C" int fplus_b200_solve_batch(int64_t count, fplus_numeric *const *nums, void *const *b, const int64_t *nrhs,
+                                      const int64_t *ldb, int trans, int nworkers, int *rcs, char *err, size_t errlen)
+{
+    if (count > 0 && (!nums || !b || !nrhs || !ldb)) { errf(err, errlen, "NULL array"); return FPLUS_ERR_BADARG; }
+    return run_batch(count, nworkers, [&](int64_t k, char *e, size_t el) {
+        return solve_common(nums[k], b[k], nrhs[k], ldb[k], trans, 0, e, el);
+    }, rcs, err, errlen);
 }
 
 extern "C" int fplus_solve(const fplus_numeric *num, void *b, int64_t nrhs, int64_t ldb, int trans, char *err, size_t errlen)

@@ -1614,23 +1614,22 @@ __global__ void __launch_bounds__(256) k_bwdU_fused(const T *__restrict__ L, int
     __syncthreads();
     if (st->code == ST_SOLVE_ZERO) return;
     if (reg) {
+        // U11's columns scaled by the reciprocal diagonal (off the sweep's chain): s_j -= (U_ji / u_ii) s_i, x = s / u
+        for (int e = tid; e < np * np; e += blockDim.x) sU[e] = mul(sU[e], dinv[e / np]);
+        __syncthreads();
         for (int64_t r = warp; r < nrhs; r += nw) {
             T a = lane < np ? s[lane + r * npiv] : VT<T>::zero();
             T b = lane + 32 < np ? s[lane + 32 + r * npiv] : VT<T>::zero();
             for (int ii = np - 1; ii >= 0; ii--) {
                 const T *col = sU + ii * np;
-                const T xi = mul(shfl_v<T>(ii < 32 ? a : b, ii & 31), dinv[ii]);
+                const T si = shfl_v<T>(ii < 32 ? a : b, ii & 31);
                 if (ii >= 32) {
-                    if (lane == ii - 32) b = xi;
-                    else if (lane < ii - 32) b = sub(b, mul(col[lane + 32], xi));
-                    a = sub(a, mul(col[lane], xi));
-                } else {
-                    if (lane == ii) a = xi;
-                    else if (lane < ii) a = sub(a, mul(col[lane], xi));
-                }
+                    if (lane < ii - 32) b = sub(b, mul(col[lane + 32], si));
+                    a = sub(a, mul(col[lane], si));
+                } else if (lane < ii) a = sub(a, mul(col[lane], si));
             }
-            if (lane < np) X[f + lane + r * n] = a;
-            if (lane + 32 < np) X[f + lane + 32 + r * n] = b;
+            if (lane < np) X[f + lane + r * n] = mul(a, dinv[lane]);
+            if (lane + 32 < np) X[f + lane + 32 + r * n] = mul(b, dinv[lane + 32]);
         }
         return;
     }

@@ -560,7 +560,7 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
     const size_t nb = (size_t)(n > 0 ? n : 1) * (size_t)nrhs * sizeof(T);
     if ((rc = ensure_async(N, (void **)&N.rbuf, &N.cap_r, nb, err, errlen))) return rc;
     if ((rc = ensure_async(N, (void **)&N.sbuf, &N.cap_s, nb, err, errlen))) return rc;
-    // fused backward sweep: one CTA per SM at most, each over >= 64 contribution-block columns
+    // fused backward sweep: one CTA per SM at most, each over >= 128 contribution-block columns
     auto bwd_chunk = [](int64_t ncb) { int64_t c = (ncb + 147) / 148; return c < 128 ? (int64_t)128 : c; };
     auto bwd_grid = [&](int64_t ncb) { return ncb > 0 ? (ncb + bwd_chunk(ncb) - 1) / bwd_chunk(ncb) : (int64_t)1; };
     auto chunk_of = [](int64_t ncb) { int64_t c = (ncb + 295) / 296; return c < 32 ? (int64_t)32 : c; };

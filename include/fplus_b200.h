@@ -54,6 +54,20 @@ int fplus_b200_plan_size(const fplus_symbolic *sym, int64_t tail, int64_t *nfron
 int fplus_b200_plan_export(const fplus_symbolic *sym, int64_t tail, int64_t *col_front, int64_t *parent, int64_t *col_ptr,
                            int64_t *cols, int64_t *nrows, int64_t *nbord);
 
+/* Batches of independent factorizations and solves.  No counterpart in FPLUS (one of the forms the B200 build adds): many
+ * pencils of one problem, or many shifts A - sigma_k B refactored on one analysed pattern.  Matrix k is analysed by
+ * syms[k] (the same object may appear several times), given by Ap[k], Ai[k], Ax[k] (host memory; all real or all
+ * complex); the factorizations run concurrently on `nworkers` host threads (<= 0: 8), each numeric object on its own
+ * CUDA stream, so that the GPU overlaps them.  nums[k] receives the k-th numeric object (NULL if it failed) and rcs[k]
+ * (when rcs is not NULL) its return code; the function returns FPLUS_OK, or the first failing code with its message.
+ * The results are those of fplus_factor / fplus_solve called one by one.  solve_batch solves nums[k] x = b[k] in place
+ * (host buffers, nrhs[k] right-hand sides, leading dimension ldb[k]). */
+int fplus_b200_factor_batch(int64_t count, const fplus_symbolic *const *syms, const int64_t *const *Ap, const int64_t *const *Ai,
+                            const void *const *Ax, int is_complex, const fplus_options *opt, int nworkers, fplus_numeric **nums,
+                            int *rcs, char *err, size_t errlen);
+int fplus_b200_solve_batch(int64_t count, fplus_numeric *const *nums, void *const *b, const int64_t *nrhs, const int64_t *ldb,
+                           int trans, int nworkers, int *rcs, char *err, size_t errlen);
+
 /* fplus_b200_solve_dev for callers that cannot allocate device memory.  No counterpart in the reference (FPLUS has no GPU
  * solve).  Some callers may not call cudaMalloc at solve time: code running inside another runtime that owns the device
  * memory (a framework's custom operator given only its input and output buffers), latency-critical loops in which an

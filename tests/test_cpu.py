@@ -309,3 +309,13 @@ def test_replica_timing_is_the_max_over_ranks():
     out = mgr.dict()
     mp.start_processes(_replica_worker, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
     assert dict(out) == {0: 11.0, 1: 11.0}
+
+
+def test_batch_argument_checks_on_host():
+    """The batch entry points: an empty batch succeeds; NULL arrays are refused before any GPU work."""
+    L = F.lib()
+    err = ctypes.create_string_buffer(256)
+    assert L.fplus_b200_factor_batch(0, None, None, None, None, 0, None, 2, None, None, err, 256) == F.FPLUS_OK
+    assert L.fplus_b200_factor_batch(3, None, None, None, None, 0, None, 2, None, None, err, 256) == F.FPLUS_ERR_BADARG
+    assert L.fplus_b200_solve_batch(0, None, None, None, None, 0, 2, None, err, 256) == F.FPLUS_OK
+    assert L.fplus_b200_solve_batch(2, None, None, None, None, 0, 2, None, err, 256) == F.FPLUS_ERR_BADARG
