@@ -764,7 +764,9 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
             rr[q] = al[q] ? rid[i] : INT64_MAX;
             xc[q] = al[q] ? A[i] : VT<T>::zero();
         }
-        auto pick = [&](const T *xv, double *m, T *pv) -> int {      // the warp's winner among the live slots
+        // the warp's winner among the live slots; every lane also forms 1 / its own candidate while the reduction runs,
+        // and the winner's reciprocal comes back with its value
+        auto pick = [&](const T *xv, double *m, T *pv, T *pinv) -> int {
             double bv = -1.0; int wi = -1; int64_t br = INT64_MAX; T bx = VT<T>::zero();
 #pragma unroll
             for (int q = 0; q < 4; q++) {
@@ -772,11 +774,12 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
                 const double a = sqmod(xv[q]);
                 if (a > bv || (a == bv && rr[q] < br)) { bv = a; wi = lane + 32 * q; br = rr[q]; bx = xv[q]; }
             }
+            const T binv = wi >= 0 && bv > 0.0 ? recip(bx) : VT<T>::zero();
             double mm = bv;
             for (int o = 16; o > 0; o >>= 1) mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, o));
             unsigned cand = __ballot_sync(0xffffffffu, wi >= 0 && bv == mm);
             *m = mm;
-            if (cand == 0) { *pv = VT<T>::zero(); return -1; }
+            if (cand == 0) { *pv = VT<T>::zero(); *pinv = VT<T>::zero(); return -1; }
             if ((cand & (cand - 1)) != 0) {
                 int64_t r2 = (cand >> lane) & 1u ? br : INT64_MAX;
                 for (int o = 16; o > 0; o >>= 1) { int64_t t = __shfl_xor_sync(0xffffffffu, r2, o); r2 = t < r2 ? t : r2; }
@@ -784,11 +787,11 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
             }
             const int wl = __ffs(cand) - 1;
             *pv = shfl_v<T>(bx, wl);
+            *pinv = shfl_v<T>(binv, wl);
             return __shfl_sync(0xffffffffu, wi, wl);
         };
-        // lane 0 decides with the winner's value pv; 1 / pv to every lane
-        auto decide_v = [&](int j, int bi, double bv2, int slot, T pv) -> T {
-            T inv = VT<T>::zero();
+        // lane 0 decides with the winner's value pv and its reciprocal pinv (held by every lane)
+        auto decide_v = [&](int j, int bi, double bv2, int slot, T pv, T pinv) -> T {
             if (lane == 0) {
                 const double t = thr[j];
                 int stop = 0;
@@ -798,14 +801,14 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
                 else if (bi >= nri) { set_status(st, ST_BORDER, front, sqrt(bv2), t); stop = 1; }
                 s_bi[slot] = bi;
                 s_stv[slot] = stop;
-                if (!stop) { inv = recip(pv); s_inv[slot] = inv; tag[bi] = j; }
+                if (!stop) { s_inv[slot] = pinv; tag[bi] = j; }
             }
-            return shfl_v<T>(inv, 0);
+            return pinv;
         };
         double m;
-        T pv;
-        int bi = pick(xc, &m, &pv);
-        T inv = decide_v(0, bi, m, 0, pv);
+        T pv, pinv;
+        int bi = pick(xc, &m, &pv, &pinv);
+        T inv = decide_v(0, bi, m, 0, pv, pinv);
 #pragma unroll
         for (int q = 0; q < 4; q++) al[q] = al[q] && lane + 32 * q != bi;
         __syncwarp();
@@ -822,8 +825,8 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
                 for (int q = 0; q < 4; q++) xb[q] = sub(xb[q], mul(mul(xc[q], inv), pr));
 #pragma unroll
                 for (int q = 0; q < 4; q++) if (al[q]) cn[lane + 32 * q] = xb[q];
-                const int w = pick(xb, &m, &pv);
-                inv = decide_v(j + 1, w, m, (j + 1) & 1, pv);
+                const int w = pick(xb, &m, &pv, &pinv);
+                inv = decide_v(j + 1, w, m, (j + 1) & 1, pv, pinv);
 #pragma unroll
                 for (int q = 0; q < 4; q++) { xc[q] = xb[q]; al[q] = al[q] && lane + 32 * q != w; }
                 bi = w;
@@ -1647,6 +1650,107 @@ __global__ void __launch_bounds__(256) k_bwdU_fused(const T *__restrict__ L, int
     for (int64_t e = tid; e < npiv * nrhs; e += blockDim.x) {
         const int64_t ii = e % npiv, r = e / npiv;
         X[f + ii + r * n] = s[e];
+    }
+}
+
+// Backward sweep through the dense chain (fronts of nb pivots from column f0, each with all columns to its right), one
+// launch per front k, column-oriented: every CTA subtracts U[:, the nb columns of front k + 1] x_{k+1} from its rows of
+// the chain above front k + 1 (each row's U12 entries read once for all right-hand sides; no cross-CTA sums), then the
+// last CTA to finish (the status word's ticket) solves front k's U11 with its now complete rows, the columns of U11
+// scaled by the reciprocal diagonal as in k_bwdU_fused.  jk1 < 0: front k is the last one (no update).
+template <typename T>
+__global__ void __launch_bounds__(256) k_chain_bwd(const T *__restrict__ Ua, const int64_t *__restrict__ cU_off, int64_t f0,
+                                                   int64_t nb, int64_t jk1, int npk1, const T *__restrict__ Lk, int64_t nrowsk,
+                                                   int64_t fk, int npk, T *__restrict__ Y, T *__restrict__ X, int64_t n,
+                                                   int64_t nrhs, DevStatus *st)
+{
+    constexpr int RB = 8;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int last;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    T *xs = reinterpret_cast<T *>(smem_raw);          // npk1 x nrhs: x of front k + 1
+    if (jk1 >= 0) {
+        // four lanes per row, sixteen of front k + 1's columns each (all their loads in flight at once); the lanes' sums
+        // are combined by shuffles in a fixed order
+        const int64_t fk1 = f0 + jk1 * nb, R = fk1 - f0;
+        for (int64_t e = tid; e < npk1 * nrhs; e += blockDim.x) xs[e] = X[fk1 + e % npk1 + (e / npk1) * n];
+        __syncthreads();
+        const int q = lane & 3;
+        const int64_t nwarp_all = (int64_t)gridDim.x * nw;
+        for (int64_t base = (blockIdx.x * (int64_t)nw + warp) * 8; base < R; base += nwarp_all * 8) {
+            const int64_t r = base + (lane >> 2);
+            const bool on = r < R;
+            const int64_t j = on ? r / nb : 0, i = on ? r % nb : 0;
+            const T *u = Ua + cU_off[j] + i + (fk1 - (f0 + j * nb) - nb) * nb;      // U12_j[i, column fk1]
+            T uv[16];
+#pragma unroll
+            for (int c = 0; c < 16; c++) {
+                const int cc = q * 16 + c;
+                uv[c] = on && cc < npk1 ? u[(int64_t)cc * nb] : VT<T>::zero();
+            }
+            for (int64_t r0 = 0; r0 < nrhs; r0 += RB) {
+                const int rb = nrhs - r0 < RB ? (int)(nrhs - r0) : RB;
+                T acc[RB];
+#pragma unroll
+                for (int t = 0; t < RB; t++) acc[t] = VT<T>::zero();
+#pragma unroll
+                for (int c = 0; c < 16; c++) {
+                    const int cc = q * 16 + c;
+                    if (cc < npk1) {
+#pragma unroll
+                        for (int t = 0; t < RB; t++)
+                            if (t < rb) acc[t] = add(acc[t], mul(uv[c], xs[cc + (r0 + t) * npk1]));
+                    }
+                }
+#pragma unroll
+                for (int t = 0; t < RB; t++) {
+                    acc[t] = add(acc[t], shfl_xor_v<T>(acc[t], 1));
+                    acc[t] = add(acc[t], shfl_xor_v<T>(acc[t], 2));
+                }
+                if (on && q == 0) {
+#pragma unroll
+                    for (int t = 0; t < RB; t++)
+                        if (t < rb) { T *y = Y + f0 + r + (r0 + t) * n; *y = sub(*y, acc[t]); }
+                }
+            }
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // the last CTA: front k's rows of Y are complete; x_k = U11^-1 y_k
+    T *s = reinterpret_cast<T *>(smem_raw);           // npk x nrhs
+    T *dinv = s + npk * nrhs;                         // npk
+    T *sU = dinv + npk;                               // npk x npk: sU[j + i * npk] = U[j, i] / U[i, i]
+    for (int e = tid; e < npk * npk; e += blockDim.x) cp_async_el(sU + e, Lk + (e % npk) + (int64_t)(e / npk) * nrowsk);
+    for (int64_t e = tid; e < npk * nrhs; e += blockDim.x) s[e] = ldcg_v(Y + fk + e % npk + (e / npk) * n);
+    for (int i = tid; i < npk; i += blockDim.x) {
+        const T d = Lk[i + (int64_t)i * nrowsk];
+        if (is_zero(d)) set_status(st, ST_SOLVE_ZERO, fk + i, 0, 0);
+        dinv[i] = is_zero(d) ? VT<T>::zero() : recip(d);
+    }
+    if (tid == 0) st->ticket = 0u;
+    cp_async_wait_all();
+    __syncthreads();
+    if (st->code == ST_SOLVE_ZERO) return;
+    for (int e = tid; e < npk * npk; e += blockDim.x) sU[e] = mul(sU[e], dinv[e / npk]);
+    __syncthreads();
+    for (int64_t r = warp; r < nrhs; r += nw) {
+        T a = lane < npk ? s[lane + r * npk] : VT<T>::zero();
+        T b = lane + 32 < npk ? s[lane + 32 + r * npk] : VT<T>::zero();
+        for (int ii = npk - 1; ii >= 0; ii--) {
+            const T *col = sU + ii * npk;
+            const T si = shfl_v<T>(ii < 32 ? a : b, ii & 31);
+            if (ii >= 32) {
+                if (lane < ii - 32) b = sub(b, mul(col[lane + 32], si));
+                a = sub(a, mul(col[lane], si));
+            } else if (lane < ii) a = sub(a, mul(col[lane], si));
+        }
+        if (lane < npk) X[fk + lane + r * n] = mul(a, dinv[lane]);
+        if (lane + 32 < npk) X[fk + lane + 32 + r * n] = mul(b, dinv[lane + 32]);
     }
 }
 

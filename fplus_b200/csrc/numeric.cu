@@ -70,7 +70,7 @@ template <typename T> static int upload(const std::vector<T> &h, T **d, char *er
 DevPlan::~DevPlan()
 {
     for (void *p : {(void *)cols, (void *)relcol, (void *)rowinit, (void *)asm_src, (void *)asm_dst, (void *)Bp, (void *)Bi,
-                    (void *)Bsrc, (void *)row_perm, (void *)col_perm, (void *)seg})
+                    (void *)Bsrc, (void *)row_perm, (void *)col_perm, (void *)seg, (void *)chain_uoff})
         if (p) cudaFree(p);
 }
 
@@ -96,6 +96,25 @@ int dev_upload_plan(const fplus_symbolic *S, const FrontPlan &P, DevPlan &D, cha
             }
         D.nseg = (int64_t)seg.size() / 3;
         if ((rc = upload(seg, &D.seg, err, errlen))) return rc;
+    }
+    {
+        // the dense chain: trailing dense fronts, nb_chain pivots each (the last at most), columns [f, n), no gaps
+        const int64_t nf = (int64_t)P.fronts.size(), nb = P.nb_chain;
+        int64_t c0 = nf;
+        while (c0 > 0 && P.fronts[c0 - 1].dense) c0--;
+        bool ok = nf - c0 >= 2 && nb > 0 && nb <= 64;
+        std::vector<int64_t> uoff;
+        for (int64_t j = c0; ok && j < nf; j++) {
+            const Front &F = P.fronts[j];
+            const bool lastf = j == nf - 1;
+            ok = F.f == P.fronts[c0].f + (j - c0) * nb && (lastf ? F.npiv <= nb : F.npiv == nb) && F.npiv <= F.nrows &&
+                 F.ncols == S->n - F.f;
+            uoff.push_back(F.U_off);
+        }
+        if (ok) {
+            D.chain_begin = c0; D.chain_nb = nb; D.chain_f0 = P.fronts[c0].f;
+            if ((rc = upload(uoff, &D.chain_uoff, err, errlen))) return rc;
+        }
     }
     return FPLUS_OK;
 }
@@ -612,7 +631,24 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
                 k_fwdL<T><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs), note_launch();
         }
         k_gather_rows<T><<<nblk(n * nrhs), 256, 0, s>>>(S2, R, N.p_lu, n, nrhs), note_launch();
-        for (int64_t fi = nf - 1; fi >= 0; fi--) {
+        int64_t fi_end = nf;                   // fronts below the chain: the row-oriented kernel
+        if (D.chain_begin >= 0) {
+            // the dense chain, column-oriented: front k's launch first applies front k + 1's solution to the rows above
+            const int64_t cb = D.chain_begin, nb = D.chain_nb;
+            const size_t csm = std::max((size_t)nb * nrhs, (size_t)(nb * (nrhs + 1) + nb * nb)) * sizeof(T);
+            if (csm > 48 * 1024) CK(cudaFuncSetAttribute(k_chain_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+            for (int64_t fi = nf - 1; fi >= cb; fi--) {
+                const Front &F = P.fronts[fi];
+                const int64_t jk1 = fi + 1 < nf ? fi + 1 - cb : -1;
+                const int npk1 = jk1 >= 0 ? (int)P.fronts[fi + 1].npiv : 0;
+                const int64_t rows = jk1 >= 0 ? jk1 * nb : 0;
+                const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((rows + 63) / 64, 296));   // 64 rows per CTA
+                k_chain_bwd<T><<<grid, 256, csm, s>>>(Ua, D.chain_uoff, D.chain_f0, nb, jk1, npk1, La + F.L_off, F.nrows, F.f,
+                                                      (int)F.npiv, S2, R, n, nrhs, N.st), note_launch();
+            }
+            fi_end = cb;
+        }
+        for (int64_t fi = fi_end - 1; fi >= 0; fi--) {
             const Front &F = P.fronts[fi];
             const int64_t ncb = F.ncols - F.npiv;
             if (F.npiv == 0) continue;

@@ -28,6 +28,10 @@ struct DevPlan {
     // B's columns cut into segments of at most 1024 entries (column, first entry, end), for the column passes
     int64_t *seg = nullptr;
     int64_t nseg = 0;
+    // the dense chain as the column-oriented backward sweep sees it: fronts [chain_begin, nfronts), chain_nb pivots each
+    // (the last one at most), first column chain_f0, their U offsets; chain_begin < 0 when the fronts do not qualify
+    int64_t chain_begin = -1, chain_nb = 0, chain_f0 = 0;
+    int64_t *chain_uoff = nullptr;
     ~DevPlan();
 };
 
