@@ -1326,7 +1326,7 @@ __global__ void __launch_bounds__(256) k_fwdL2(const T *__restrict__ L, int64_t 
 // rows of the right-hand sides; the L11 solve by a warp per right-hand side with the vector in registers (rows lane and
 // lane + 32; the pivot value broadcast by shuffle); the L21 update by the whole CTA; scatter back
 template <typename T>
-__global__ void __launch_bounds__(256) k_fwdL3(const T *__restrict__ L, int64_t nrows, int64_t npiv,
+__global__ void __launch_bounds__(512) k_fwdL3(const T *__restrict__ L, int64_t nrows, int64_t npiv,
                                                const int64_t *__restrict__ rowid, T *__restrict__ Wr, int64_t n, int64_t nrhs,
                                                int whole)
 {
@@ -1659,7 +1659,7 @@ __global__ void __launch_bounds__(256) k_bwdU_fused(const T *__restrict__ L, int
 // last CTA to finish (the status word's ticket) solves front k's U11 with its now complete rows, the columns of U11
 // scaled by the reciprocal diagonal as in k_bwdU_fused.  jk1 < 0: front k is the last one (no update).
 template <typename T>
-__global__ void __launch_bounds__(256) k_chain_bwd(const T *__restrict__ Ua, const int64_t *__restrict__ cU_off, int64_t f0,
+__global__ void __launch_bounds__(512) k_chain_bwd(const T *__restrict__ Ua, const int64_t *__restrict__ cU_off, int64_t f0,
                                                    int64_t nb, int64_t jk1, int npk1, const T *__restrict__ Lk, int64_t nrowsk,
                                                    int64_t fk, int npk, T *__restrict__ Y, T *__restrict__ X, int64_t n,
                                                    int64_t nrhs, DevStatus *st)

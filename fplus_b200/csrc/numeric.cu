@@ -621,10 +621,11 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
             const size_t fsm = (size_t)F.nrows * nrhs * sizeof(T);
             const int64_t np = std::min(F.npiv, F.nrows);
             const size_t whole_sm = fsm + (size_t)F.nrows * np * sizeof(T), l11_sm = fsm + (size_t)np * np * sizeof(T);
+            const int swt = nrhs > 8 ? 512 : 256;        // a warp per right-hand side in the sweeps
             if (F.npiv <= 64 && whole_sm <= FWD_SMEM)
-                k_fwdL3<T><<<1, 256, whole_sm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 1), note_launch();
+                k_fwdL3<T><<<1, swt, whole_sm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 1), note_launch();
             else if (F.npiv <= 64 && l11_sm <= FWD_SMEM)
-                k_fwdL3<T><<<1, 256, l11_sm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 0), note_launch();
+                k_fwdL3<T><<<1, swt, l11_sm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 0), note_launch();
             else if (fsm <= 96 * 1024)
                 k_fwdL2<T><<<1, 256, fsm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs), note_launch();
             else
@@ -642,8 +643,9 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
                 const int64_t jk1 = fi + 1 < nf ? fi + 1 - cb : -1;
                 const int npk1 = jk1 >= 0 ? (int)P.fronts[fi + 1].npiv : 0;
                 const int64_t rows = jk1 >= 0 ? jk1 * nb : 0;
-                const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((rows + 63) / 64, 296));   // 64 rows per CTA
-                k_chain_bwd<T><<<grid, 256, csm, s>>>(Ua, D.chain_uoff, D.chain_f0, nb, jk1, npk1, La + F.L_off, F.nrows, F.f,
+                const int cbt = nrhs > 8 ? 512 : 256;      // a warp per right-hand side in the U11 sweep
+                const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((rows + cbt / 4 - 1) / (cbt / 4), 296));
+                k_chain_bwd<T><<<grid, cbt, csm, s>>>(Ua, D.chain_uoff, D.chain_f0, nb, jk1, npk1, La + F.L_off, F.nrows, F.f,
                                                       (int)F.npiv, S2, R, n, nrhs, N.st), note_launch();
             }
             fi_end = cb;

@@ -164,3 +164,20 @@ def test_batch_factor_and_solve_match_single(gpu):
         assert np.array_equal(Xs[k], X1), f"matrix {k}: solutions differ"
         for r in range(2):
             assert O.backward_error(m[0], m[1], m[2], m[3], Xs[k][:, r], bs[k][:, r]) <= 1e-14
+
+
+def test_chain_solve_many_rhs(gpu):
+    """A pencil (dense chain: the column-oriented backward sweep) with 20 right-hand sides (more than one warp's worth per
+    sweep CTA): every column at backward error <= 1e-14, and each equal within rounding to its own one-column solve."""
+    n, Ap, Ai, Ax = CASES["pencil_2x256"]()
+    S = F.analyze(n, Ap, Ai)
+    N = S.factor(Ax)
+    assert N.info["f_dense"] < n, "the case should factor with a dense chain"
+    rng = np.random.default_rng(9)
+    B = rng.standard_normal((n, 20)) + 1j * rng.standard_normal((n, 20))
+    for trans in (0, 1, 2):
+        X = N.solve(B, trans)
+        for r in range(20):
+            assert O.backward_error(n, Ap, Ai, Ax, X[:, r], B[:, r], trans) <= 1e-14
+        x3 = N.solve(B[:, 3], trans)
+        assert np.allclose(X[:, 3], x3, rtol=0, atol=1e-12 * np.abs(x3).max())
