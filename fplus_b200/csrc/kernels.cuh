@@ -577,6 +577,12 @@ template <typename T> __device__ __forceinline__ void cp_async_el(T *dst, const 
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream serialization may start before the kernel
+// ahead of it in the stream has finished; pdl_wait() blocks until that kernel has completed and its writes are visible
+// (a no-op for a normally launched kernel); pdl_trigger() lets the next such kernel start its own launch.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // a load that bypasses L1 (values another CTA wrote during this launch)
 __device__ __forceinline__ double ldcg_v(const double *p) { return __ldcg(p); }
 __device__ __forceinline__ cplx ldcg_v(const cplx *p)
@@ -678,6 +684,7 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
     const int ne = npiv * nrows;
     if (!pa.on) {
+        pdl_wait();
         // the block from the working block, 8 loads in flight per thread
         for (int e0 = tid; e0 < ne; e0 += 8 * nt) {
             T v[8];
@@ -695,6 +702,7 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
         const T *Bx = reinterpret_cast<const T *>(pa.Bx);
 #pragma unroll 4
         for (int64_t e = tid; e < pa.acnt; e += nt) A[pa.adst[e]] = Bx[pa.asrc[e]];
+        pdl_wait();                                   // the child's CB columns (the launch before) are written
         for (int64_t t = tid; t < pa.nslot; t += nt) rid[pa.slot + t] = pa.child_rowid[t];
         __syncthreads();
         const T *cb = reinterpret_cast<const T *>(pa.cb);
@@ -1114,6 +1122,7 @@ __global__ void __launch_bounds__(FT_THREADS) k_front_tail(const T *__restrict__
     double *sXr = sLr + (CP ? 2 : 1) * FT_NP * FT_LD;               // X[r, c] at c * FT_LD + r
     double *sXi = sXr + (CP ? TN * FT_LD : 0);
     __shared__ int sperm[FT_NR];
+    pdl_trigger();                                   // the next pivot block's LU may start its own set-up
     if (st->code) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int M = nrows - npiv;
@@ -1340,6 +1349,8 @@ __global__ void __launch_bounds__(512) k_fwdL3(const T *__restrict__ L, int64_t 
         for (int64_t e = threadIdx.x; e < nrows * np; e += blockDim.x) cp_async_el(sL + e, L + e);
     else
         for (int e = threadIdx.x; e < np * np; e += blockDim.x) cp_async_el(sL + e, L + (e % np) + (int64_t)(e / np) * nrows);
+    pdl_wait();                                       // the previous front's sweep has written Wr (the L copy runs on)
+    pdl_trigger();
     for (int64_t e = threadIdx.x; e < nrows * nrhs; e += blockDim.x) v[e] = Wr[rowid[e % nrows] + (e / nrows) * n];
     cp_async_wait_all();
     __syncthreads();
@@ -1669,25 +1680,35 @@ __global__ void __launch_bounds__(512) k_chain_bwd(const T *__restrict__ Ua, con
     __shared__ int last;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
     T *xs = reinterpret_cast<T *>(smem_raw);          // npk1 x nrhs: x of front k + 1
+    const int q = lane & 3;
+    const int64_t fk1 = jk1 >= 0 ? f0 + jk1 * nb : 0, R = jk1 >= 0 ? fk1 - f0 : 0;
+    const int64_t nwarp_all = (int64_t)gridDim.x * nw;
+    // four lanes per row, sixteen of front k + 1's columns each (all their loads in flight at once); the lanes' sums
+    // are combined by shuffles in a fixed order.  The first rows' U12 entries are loaded before waiting for the previous
+    // front's launch (U does not change during the solve).
+    T uv[16];
+    auto load_u = [&](int64_t base) {
+        const int64_t r = base + (lane >> 2);
+        const bool on = r < R;
+        const int64_t j = on ? r / nb : 0, i = on ? r % nb : 0;
+        const T *u = Ua + cU_off[j] + i + (fk1 - (f0 + j * nb) - nb) * nb;      // U12_j[i, column fk1]
+#pragma unroll
+        for (int c = 0; c < 16; c++) {
+            const int cc = q * 16 + c;
+            uv[c] = on && cc < npk1 ? u[(int64_t)cc * nb] : VT<T>::zero();
+        }
+    };
+    const int64_t base0 = (blockIdx.x * (int64_t)nw + warp) * 8;
+    if (jk1 >= 0 && base0 < R) load_u(base0);
+    pdl_wait();                                       // the previous front's x is written
+    pdl_trigger();
     if (jk1 >= 0) {
-        // four lanes per row, sixteen of front k + 1's columns each (all their loads in flight at once); the lanes' sums
-        // are combined by shuffles in a fixed order
-        const int64_t fk1 = f0 + jk1 * nb, R = fk1 - f0;
         for (int64_t e = tid; e < npk1 * nrhs; e += blockDim.x) xs[e] = X[fk1 + e % npk1 + (e / npk1) * n];
         __syncthreads();
-        const int q = lane & 3;
-        const int64_t nwarp_all = (int64_t)gridDim.x * nw;
-        for (int64_t base = (blockIdx.x * (int64_t)nw + warp) * 8; base < R; base += nwarp_all * 8) {
+        for (int64_t base = base0; base < R; base += nwarp_all * 8) {
+            if (base != base0) load_u(base);
             const int64_t r = base + (lane >> 2);
             const bool on = r < R;
-            const int64_t j = on ? r / nb : 0, i = on ? r % nb : 0;
-            const T *u = Ua + cU_off[j] + i + (fk1 - (f0 + j * nb) - nb) * nb;      // U12_j[i, column fk1]
-            T uv[16];
-#pragma unroll
-            for (int c = 0; c < 16; c++) {
-                const int cc = q * 16 + c;
-                uv[c] = on && cc < npk1 ? u[(int64_t)cc * nb] : VT<T>::zero();
-            }
             for (int64_t r0 = 0; r0 < nrhs; r0 += RB) {
                 const int rb = nrhs - r0 < RB ? (int)(nrhs - r0) : RB;
                 T acc[RB];

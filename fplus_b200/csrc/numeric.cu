@@ -48,6 +48,20 @@ struct Prof {
     }
 };
 
+// a launch that may begin before the kernel ahead of it in the stream has finished (programmatic dependent launch); the
+// kernel waits (pdl_wait) before it reads that kernel's results
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid; cfg.blockDim = block; cfg.dynamicSmemBytes = smem; cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at; cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 #define CK(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { errf(err, errlen, "CUDA: %s (%s:%d)", cudaGetErrorString(e_), __FILE__, __LINE__); return FPLUS_ERR_GPU; } } while (0)
 
 static inline int nblk(int64_t work, int per = 256, int cap = 148 * 16)
@@ -395,8 +409,13 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             const int R = (int)((nr + 31) & ~31);
             int nt = 32 + (R <= 128 ? 4 * R : R);   // the pivot warp + the update warps
             if (nt > 640) nt = 640;
-            k_front_lu2<T><<<1, nt, sm, st>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel, N.rowid + F.row_off, Lf,
-                                            perm, N.p_lu, N.st, fi, pa), note_launch();
+            if (pa.on) {      // right after the child's tail head on the critical stream: overlap the launch
+                CK(launch_pdl(k_front_lu2<T>, 1, nt, sm, st, (const T *)W, ld, (int)nr, (int)np, (int)F.nri, F.f,
+                              (const double *)N.colmax, pivot_rel, N.rowid + F.row_off, Lf, perm, N.p_lu, N.st, fi, pa));
+                note_launch();
+            } else
+                k_front_lu2<T><<<1, nt, sm, st>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel, N.rowid + F.row_off,
+                                                Lf, perm, N.p_lu, N.st, fi, pa), note_launch();
         } else {
             const int64_t npr = std::min(np, nr);
             for (int64_t k0 = 0; k0 < npr; k0 += PW) {
@@ -622,10 +641,13 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
             const int64_t np = std::min(F.npiv, F.nrows);
             const size_t whole_sm = fsm + (size_t)F.nrows * np * sizeof(T), l11_sm = fsm + (size_t)np * np * sizeof(T);
             const int swt = nrhs > 8 ? 512 : 256;        // a warp per right-hand side in the sweeps
-            if (F.npiv <= 64 && whole_sm <= FWD_SMEM)
-                k_fwdL3<T><<<1, swt, whole_sm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 1), note_launch();
-            else if (F.npiv <= 64 && l11_sm <= FWD_SMEM)
-                k_fwdL3<T><<<1, swt, l11_sm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 0), note_launch();
+            if (F.npiv <= 64 && whole_sm <= FWD_SMEM) {
+                CK(launch_pdl(k_fwdL3<T>, 1, swt, whole_sm, s, La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 1));
+                note_launch();
+            } else if (F.npiv <= 64 && l11_sm <= FWD_SMEM) {
+                CK(launch_pdl(k_fwdL3<T>, 1, swt, l11_sm, s, La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 0));
+                note_launch();
+            }
             else if (fsm <= 96 * 1024)
                 k_fwdL2<T><<<1, 256, fsm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs), note_launch();
             else
@@ -645,8 +667,9 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
                 const int64_t rows = jk1 >= 0 ? jk1 * nb : 0;
                 const int cbt = nrhs > 8 ? 512 : 256;      // a warp per right-hand side in the U11 sweep
                 const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((rows + cbt / 4 - 1) / (cbt / 4), 296));
-                k_chain_bwd<T><<<grid, cbt, csm, s>>>(Ua, D.chain_uoff, D.chain_f0, nb, jk1, npk1, La + F.L_off, F.nrows, F.f,
-                                                      (int)F.npiv, S2, R, n, nrhs, N.st), note_launch();
+                CK(launch_pdl(k_chain_bwd<T>, grid, cbt, csm, s, Ua, D.chain_uoff, D.chain_f0, nb, jk1, npk1, La + F.L_off,
+                              F.nrows, F.f, (int)F.npiv, S2, R, n, nrhs, N.st));
+                note_launch();
             }
             fi_end = cb;
         }
