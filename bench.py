@@ -250,6 +250,34 @@ def run_shift_batch(S, n, modes, count, b):
             "berr_max": be, "timing": "host wall clock around the synchronous fplus calls (host values, e2e)"}
 
 
+def run_pencil_batch(count, nworkers=16):
+    """count independent pencils of uneven size (n log-uniform in [500, 8000], 2-4 dense tau rows / columns), 8
+    right-hand sides each: analysed once each, then factored and solved one by one and through fplus_b200_factor_batch /
+    solve_batch.  Host wall time around the synchronous calls."""
+    import fplus_b200 as F
+    import oracle as O
+    from fplus_b200 import workloads as W
+    mats = W.pencil_batch(count=count)
+    syms = [F.analyze(m[0], m[1], m[2]) for m in mats]
+    rhs = [W.rhs(m[0], 8, True, 7 + k).T.copy(order="F") for k, m in enumerate(mats)]
+    F.solve_batch(F.factor_batch(syms[:4], [m[3] for m in mats[:4]]), rhs[:4])        # warm-up
+    t0 = time.perf_counter()
+    for S, m, b in zip(syms, mats, rhs):
+        N = S.factor(m[3])
+        N.solve(b)
+        del N
+    seq = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    Ns = F.factor_batch(syms, [m[3] for m in mats], nworkers=nworkers)
+    Xs = F.solve_batch(Ns, rhs, nworkers=nworkers)
+    par = (time.perf_counter() - t0) * 1e3
+    be = max(O.backward_error(m[0], m[1], m[2], m[3], X[:, r], b[:, r]) for m, X, b in zip(mats, Xs, rhs) for r in (0, 7))
+    ns = [m[0] for m in mats]
+    return {"workload": f"{count} pencils, n log-uniform in [500, 8000] (sum {sum(ns)}), 8 right-hand sides each",
+            "ms_total": par, "sequential_ms_total": seq, "speedup": seq / par, "berr_max": be, "workers": nworkers,
+            "timing": "host wall clock around the synchronous fplus calls (host values, e2e); analysis excluded"}
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -414,6 +442,9 @@ def run_b200_arm(args, rank, world):
     batch = None
     if args.workload == "pencil" and args.batch > 0 and world == 1:
         batch = run_shift_batch(S, n, args.modes, args.batch, b)
+    batch_pencils = None
+    if args.batch_pencils > 0 and world == 1:
+        batch_pencils = run_pencil_batch(args.batch_pencils)
 
     if rank != 0:
         return
@@ -434,7 +465,8 @@ def run_b200_arm(args, rank, world):
             "e2e": {"value": ms_e2e / world, "unit": "ms", "h2d_bytes_per_step": int(Ap[-1]) * vsz + n * vsz,
                     "d2h_bytes_per_step": n * vsz},
             "gpu_launches": int(launches),
-            "clocks": clocks, "roofline": roof, "cpu_baseline": cpu, "solve_nrhs16": solve16, "batch": batch}
+            "clocks": clocks, "roofline": roof, "cpu_baseline": cpu, "solve_nrhs16": solve16, "batch": batch,
+            "batch_pencils": batch_pencils}
     print(json.dumps(line))
 
 
@@ -449,6 +481,8 @@ def main():
                     help="Fourier modes of the pencil workload (8: n = 32768, the benchmark; 1: n = 4096, for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=8, help="shifts in the batch measurement (0: none)")
+    ap.add_argument("--batch-pencils", type=int, default=128,
+                    help="independent uneven pencils in the second batch measurement (0: none)")
     ap.add_argument("--profile-once", action="store_true",
                     help="for ncu --profile-from-start off: one warm factorization, then exactly one factor + solve "
                          "between cudaProfilerStart / Stop; prints that factorization's algorithmic work per class")

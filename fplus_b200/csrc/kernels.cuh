@@ -1679,7 +1679,10 @@ __global__ void __launch_bounds__(512) k_chain_bwd(const T *__restrict__ Ua, con
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int last;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    T *xs = reinterpret_cast<T *>(smem_raw);          // npk1 x nrhs: x of front k + 1
+    T *xs = reinterpret_cast<T *>(smem_raw);          // x of front k + 1: column cc of rhs t at XS(cc, t)
+    // each 16-column group padded by one element, so that the four lanes of a row (16 columns apart) hit different banks
+    const int xld = npk1 + (npk1 + 15) / 16;
+    auto XS = [&](int cc, int64_t t) -> int64_t { return cc + (cc >> 4) + t * xld; };
     const int q = lane & 3;
     const int64_t fk1 = jk1 >= 0 ? f0 + jk1 * nb : 0, R = jk1 >= 0 ? fk1 - f0 : 0;
     const int64_t nwarp_all = (int64_t)gridDim.x * nw;
@@ -1703,7 +1706,7 @@ __global__ void __launch_bounds__(512) k_chain_bwd(const T *__restrict__ Ua, con
     pdl_wait();                                       // the previous front's x is written
     pdl_trigger();
     if (jk1 >= 0) {
-        for (int64_t e = tid; e < npk1 * nrhs; e += blockDim.x) xs[e] = X[fk1 + e % npk1 + (e / npk1) * n];
+        for (int64_t e = tid; e < npk1 * nrhs; e += blockDim.x) xs[XS((int)(e % npk1), e / npk1)] = X[fk1 + e % npk1 + (e / npk1) * n];
         __syncthreads();
         for (int64_t base = base0; base < R; base += nwarp_all * 8) {
             if (base != base0) load_u(base);
@@ -1720,7 +1723,7 @@ __global__ void __launch_bounds__(512) k_chain_bwd(const T *__restrict__ Ua, con
                     if (cc < npk1) {
 #pragma unroll
                         for (int t = 0; t < RB; t++)
-                            if (t < rb) acc[t] = add(acc[t], mul(uv[c], xs[cc + (r0 + t) * npk1]));
+                            if (t < rb) acc[t] = add(acc[t], mul(uv[c], xs[XS(cc, r0 + t)]));
                     }
                 }
 #pragma unroll

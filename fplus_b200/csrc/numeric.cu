@@ -658,7 +658,7 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
         if (D.chain_begin >= 0) {
             // the dense chain, column-oriented: front k's launch first applies front k + 1's solution to the rows above
             const int64_t cb = D.chain_begin, nb = D.chain_nb;
-            const size_t csm = std::max((size_t)nb * nrhs, (size_t)(nb * (nrhs + 1) + nb * nb)) * sizeof(T);
+            const size_t csm = std::max((size_t)(nb + (nb + 15) / 16) * nrhs, (size_t)(nb * (nrhs + 1) + nb * nb)) * sizeof(T);
             if (csm > 48 * 1024) CK(cudaFuncSetAttribute(k_chain_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
             for (int64_t fi = nf - 1; fi >= cb; fi--) {
                 const Front &F = P.fronts[fi];
