@@ -607,13 +607,14 @@ template <> __device__ __forceinline__ cplx shfl_v<cplx>(cplx v, int src)
 
 // 1 / p for the pivot: conj(p) / |p|^2 with the components scaled by max(|re|, |im|) first (no overflow or underflow of the
 // squares); real: 1 / p
-__device__ __forceinline__ double recip(double p) { return 1.0 / p; }
+// (__drcp_rn: the correctly rounded reciprocal, the same value as the IEEE quotient 1.0 / q)
+__device__ __forceinline__ double recip(double p) { return __drcp_rn(p); }
 __device__ __forceinline__ cplx recip(cplx p)
 {
     const double q = p.x * p.x + p.y * p.y;
-    if (q > 1e-300 && q < 1e300) { const double d = 1.0 / q; return cplx{p.x * d, -p.y * d}; }
-    const double s = fmax(fabs(p.x), fabs(p.y)), is = 1.0 / s;          // scaled: no overflow or underflow
-    const double a = p.x * is, b = p.y * is, d = 1.0 / (a * a + b * b);
+    if (q > 1e-300 && q < 1e300) { const double d = __drcp_rn(q); return cplx{p.x * d, -p.y * d}; }
+    const double s = fmax(fabs(p.x), fabs(p.y)), is = __drcp_rn(s);     // scaled: no overflow or underflow
+    const double a = p.x * is, b = p.y * is, d = __drcp_rn(a * a + b * b);
     return cplx{a * d * is, -b * d * is};
 }
 
@@ -783,10 +784,15 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
                 if (a > bv || (a == bv && rr[q] < br)) { bv = a; wi = lane + 32 * q; br = rr[q]; bx = xv[q]; }
             }
             const T binv = wi >= 0 && bv > 0.0 ? recip(bx) : VT<T>::zero();
-            double mm = bv;
-            for (int o = 16; o > 0; o >>= 1) mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, o));
-            unsigned cand = __ballot_sync(0xffffffffu, wi >= 0 && bv == mm);
-            *m = mm;
+            // the maximum: non-negative doubles order as their bit patterns, so two 32-bit warp reductions (high word,
+            // then the low word among the lanes that hold the high word)
+            const unsigned long long key = wi >= 0 ? (unsigned long long)__double_as_longlong(bv) : 0ull;
+            const unsigned khi = (unsigned)(key >> 32);
+            const unsigned hi = __reduce_max_sync(0xffffffffu, khi);
+            const unsigned lo = __reduce_max_sync(0xffffffffu, khi == hi ? (unsigned)key : 0u);
+            const unsigned long long mk = ((unsigned long long)hi << 32) | lo;
+            unsigned cand = __ballot_sync(0xffffffffu, wi >= 0 && key == mk);
+            *m = cand ? __longlong_as_double((long long)mk) : -1.0;
             if (cand == 0) { *pv = VT<T>::zero(); *pinv = VT<T>::zero(); return -1; }
             if ((cand & (cand - 1)) != 0) {
                 int64_t r2 = (cand >> lane) & 1u ? br : INT64_MAX;
@@ -957,8 +963,7 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
         rowid[k] = rid[i];
         if (k < steps) p_lu[fcol + k] = rid[i];
     }
-    for (int c = 0; c < npiv; c++)
-        for (int i = at; i < nrows; i += nact) Lout[pos[i] + (int64_t)c * nrows] = A[(size_t)c * nrows + i];
+    for (int e = at; e < ne; e += nact) { const int i = e % nrows; Lout[pos[i] + (int64_t)(e / nrows) * nrows] = A[e]; }
 }
 
 // After the blocked (global-memory) pivoting of a large front's pivot block: the final row order from the swaps, the
