@@ -448,124 +448,7 @@ __global__ void __launch_bounds__(256) k_gemm_sub(int64_t M, int64_t N, int64_t 
             }
 }
 
-// the factors of the front leave the working block: L (nrows x npiv) and U12 (npiv x ncb) into the arena, the CB into
-// the stack, the pivot rows into p_lu
-template <typename T>
-__global__ void k_copyout(const T *__restrict__ W, int64_t nrows, int64_t ncols, int64_t npiv, T *__restrict__ Lo,
-                          T *__restrict__ Uo, T *__restrict__ CBo, const int64_t *__restrict__ rowid, int64_t f,
-                          int64_t *__restrict__ p_lu, const DevStatus *st)
-{
-    if (st->code) return;
-    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
-    const int64_t ncb = ncols - npiv, cbr = nrows > npiv ? nrows - npiv : 0;
-    for (int64_t e = tid; e < nrows * npiv; e += stride) Lo[e] = W[e];
-    for (int64_t e = tid; e < npiv * ncb; e += stride) { int64_t i = e % npiv, c = e / npiv; Uo[e] = W[i + (npiv + c) * nrows]; }
-    for (int64_t e = tid; e < cbr * ncb; e += stride) { int64_t i = e % cbr, c = e / cbr; CBo[e] = W[npiv + i + (npiv + c) * nrows]; }
-    for (int64_t i = tid; i < npiv && i < nrows; i += stride) p_lu[f + i] = rowid[i];
-}
 
-// Partial-pivot LU of a front's pivot block (nrows x npiv, in shared memory, one CTA), without row swaps: a row chosen
-// as the pivot of step j is tagged j and leaves the updates; the others are scaled and updated in place.  Per step the
-// argmax (largest modulus, ties to the smaller row of B) is computed by every warp from shared memory with shuffles, so
-// one barrier per step suffices.  Threads: row i = t % R, column group g = t / R (R = nrows rounded up to a warp).
-// Output, in the final row order (pivot rows by step, then the other rows in their order): the packed L\U block into the
-// arena, the row ids, the pivot rows (p_lu) and the order itself (perm: position -> local row) for the other columns.
-template <typename T>
-__global__ void __launch_bounds__(1024) k_front_lu(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
-                                                   int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
-                                                   int64_t *__restrict__ rowid, T *__restrict__ Lout, int *__restrict__ perm,
-                                                   int64_t *__restrict__ p_lu, DevStatus *st, int64_t front)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *A = reinterpret_cast<T *>(smem_raw);                        // npiv x nrows, column-major: A[c * nrows + i]
-    T *lcol = A + (size_t)npiv * nrows;                            // this step's multipliers
-    int64_t *rid = reinterpret_cast<int64_t *>(lcol + nrows);
-    int *tag = reinterpret_cast<int *>(rid + nrows);
-    int *pos = tag + nrows;
-    __shared__ int s_stop;
-    const int tid = threadIdx.x, lane = tid & 31, nt = blockDim.x;
-    const int R = (nrows + 31) & ~31;
-    const int G = nt >= R ? nt / R : 1;                            // column groups per row
-    const int rstep = nt >= R ? R : nt;                            // row stride of a thread
-    const int my_i = nt >= R ? tid % R : tid, my_g = nt >= R ? tid / R : 0;
-    const bool upd = my_g < G;                                     // threads beyond G whole row groups only search
-    if (tid == 0) s_stop = st->code != 0;
-    for (int64_t e = tid; e < (int64_t)npiv * nrows; e += nt) {
-        const int i = (int)(e % nrows), c = (int)(e / nrows);
-        A[e] = W[i + c * ld];
-    }
-    for (int i = tid; i < nrows; i += nt) { rid[i] = rowid[i]; tag[i] = INT_MAX; }
-    __syncthreads();
-    if (s_stop) return;
-    const int steps = npiv;
-    for (int j = 0; j < steps; j++) {
-        // argmax over the rows not pivoted before step j (tag >= j; tid 0 tags this step's pivot during the step, which
-        // keeps it a candidate for the warps still searching), the same result in every warp
-        // (compared on the squared modulus, which orders as the modulus does up to the rounding of the squares)
-        double bv = -1.0; int bi = -1; int64_t br = INT64_MAX;
-        for (int i = lane; i < nrows; i += 32) {
-            if (tag[i] < j) continue;
-            const double a = sqmod(A[(size_t)j * nrows + i]);
-            const int64_t r = rid[i];
-            if (a > bv || (a == bv && r < br)) { bv = a; bi = i; br = r; }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            const int64_t orr = __shfl_xor_sync(0xffffffffu, br, o);
-            if (ov > bv || (ov == bv && orr < br)) { bv = ov; bi = oi; br = orr; }
-        }
-        if (bi >= 0) bv = vabs(A[(size_t)j * nrows + bi]);       // the modulus of the winner, for the singular test
-        const double thr = pivot_rel * colmax[fcol + j];
-        if (bi < 0 || bv <= 0.0 || bv < thr) {
-            if (tid == 0) set_status(st, ST_SINGULAR, fcol + j, bv > 0 ? bv : 0.0, thr);
-            return;
-        }
-        if (bi >= nri) {
-            if (tid == 0) set_status(st, ST_BORDER, front, bv, thr);
-            return;
-        }
-        // the previous step's multipliers into column j - 1 (read by nobody from here on): rows not pivoted up to j - 1
-        if (j > 0 && my_g == 0)
-            for (int i = my_i; i < nrows; i += rstep) if (tag[i] > j - 1) A[(size_t)(j - 1) * nrows + i] = lcol[i];
-        const T inv = divv(VT<T>::one(), A[(size_t)j * nrows + bi]);
-        if (tid == 0) tag[bi] = j;
-        for (int i = my_i; upd && i < nrows; i += rstep) {
-            if (i == bi || tag[i] <= j) continue;
-            const T l = mul(A[(size_t)j * nrows + i], inv);
-            for (int c = j + 1 + my_g; c < npiv; c += G) {
-                T *x = A + (size_t)c * nrows + i;
-                *x = sub(*x, mul(l, A[(size_t)c * nrows + bi]));
-            }
-            if (my_g == 0) lcol[i] = l;
-        }
-        __syncthreads();
-    }
-    if (steps > 0 && my_g == 0)
-        for (int i = my_i; i < nrows; i += rstep) if (tag[i] > steps - 1) A[(size_t)(steps - 1) * nrows + i] = lcol[i];
-    // final order: position tag[i] for the pivot rows, then the untagged rows in order (a ballot scan by warp 0)
-    if (tid < 32) {
-        int base = steps;
-        for (int i0 = 0; i0 < nrows; i0 += 32) {
-            const int i = i0 + lane;
-            const bool un = i < nrows && tag[i] >= steps;
-            const unsigned m = __ballot_sync(0xffffffffu, un);
-            if (i < nrows) pos[i] = un ? base + __popc(m & ((1u << lane) - 1u)) : tag[i];
-            base += __popc(m);
-        }
-    }
-    __syncthreads();
-    for (int i = tid; i < nrows; i += nt) {
-        const int k = pos[i];
-        perm[k] = i;
-        rowid[k] = rid[i];
-        if (k < steps) p_lu[fcol + k] = rid[i];
-    }
-    for (int64_t e = tid; e < (int64_t)npiv * nrows; e += nt) {
-        const int i = (int)(e % nrows), c = (int)(e / nrows);
-        Lout[pos[i] + (int64_t)c * nrows] = A[e];
-    }
-}
 
 // asynchronous global -> shared copies of one element (cp.async: all of a thread's copies in flight at once; completed
 // by cp_async_wait_all, then a barrier).  Both addresses aligned to the element size.
@@ -996,41 +879,6 @@ __global__ void k_u12_gather(const T *__restrict__ W, int64_t ld, int64_t npiv, 
     }
 }
 
-// U12 = L11^-1 A12[perm] in one pass for npiv <= 32 RPL: a warp per column gathers the pivot rows of the column
-// through perm, solves with the unit lower L11 (shared memory) by shuffles, and writes the U12 column
-template <typename T, int RPL>
-__global__ void __launch_bounds__(256) k_u12_fused(const T *__restrict__ W, int64_t ld, const int *__restrict__ perm,
-                                                   int npiv, int64_t ncb, const T *__restrict__ Lb, int64_t ldl,
-                                                   T *__restrict__ U, const DevStatus *st)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *sL = reinterpret_cast<T *>(smem_raw);          // npiv x npiv, column-major
-    if (st->code) return;
-    for (int e = threadIdx.x; e < npiv * npiv; e += blockDim.x) sL[e] = Lb[(e % npiv) + (int64_t)(e / npiv) * ldl];
-    __syncthreads();
-    const int lane = threadIdx.x & 31;
-    int src[RPL];
-#pragma unroll
-    for (int q = 0; q < RPL; q++) { const int r = lane + 32 * q; src[q] = r < npiv ? perm[r] : 0; }
-    const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5, nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t c = wid; c < ncb; c += nwarp) {
-        const T *col = W + (npiv + c) * ld;
-        T x[RPL];
-#pragma unroll
-        for (int q = 0; q < RPL; q++) { const int r = lane + 32 * q; x[q] = r < npiv ? col[src[q]] : VT<T>::zero(); }
-        for (int i = 0; i < npiv; i++) {
-            const T xi = shfl_v<T>(x[i >> 5], i & 31);
-#pragma unroll
-            for (int q = 0; q < RPL; q++) {
-                const int r = lane + 32 * q;
-                if (r > i && r < npiv) x[q] = sub(x[q], mul(sL[r + i * npiv], xi));
-            }
-        }
-        T *u = U + c * npiv;
-#pragma unroll
-        for (int q = 0; q < RPL; q++) { const int r = lane + 32 * q; if (r < npiv) u[r] = x[q]; }
-    }
-}
 
 // U12 = L11^-1 A12[perm] for npiv <= 64, by column tiles of 32 in shared memory (persistent CTAs: L11 staged once per
 // CTA): the tile's pivot rows are gathered through perm; then per 16-row block, the diagonal 16 x 16 solve by half-warps
@@ -1386,27 +1234,6 @@ __global__ void __launch_bounds__(512) k_fwdL3(const T *__restrict__ L, int64_t 
     for (int64_t e = threadIdx.x; e < nrows * nrhs; e += blockDim.x) Wr[rowid[e % nrows] + (e / nrows) * n] = v[e];
 }
 
-// forward sweep with L through one front in shared memory (one CTA): gather the front's rows of the right-hand sides,
-// eliminate column by column, scatter back
-template <typename T>
-__global__ void __launch_bounds__(256) k_fwdL_smem(const T *__restrict__ L, int64_t nrows, int64_t npiv,
-                                                   const int64_t *__restrict__ rowid, T *__restrict__ Wr, int64_t n, int64_t nrhs)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *v = reinterpret_cast<T *>(smem_raw);           // nrows x nrhs
-    for (int64_t e = threadIdx.x; e < nrows * nrhs; e += blockDim.x) v[e] = Wr[rowid[e % nrows] + (e / nrows) * n];
-    __syncthreads();
-    for (int64_t i = 0; i < npiv && i < nrows; i++) {
-        const int64_t m = nrows - i - 1;
-        for (int64_t e = threadIdx.x; e < m * nrhs; e += blockDim.x) {
-            const int64_t rr = i + 1 + e % m, r = e / m;
-            const T xi = v[i + r * nrows];
-            v[rr + r * nrows] = sub(v[rr + r * nrows], mul(L[rr + i * nrows], xi));
-        }
-        __syncthreads();
-    }
-    for (int64_t e = threadIdx.x; e < nrows * nrhs; e += blockDim.x) Wr[rowid[e % nrows] + (e / nrows) * n] = v[e];
-}
 
 // forward sweep with L through one front (one CTA), in row space: for each pivot column i, the rows below it lose
 // L[row, i] times the pivot row's value
@@ -1816,26 +1643,6 @@ __global__ void __launch_bounds__(256) k_fwdUt2(const T *__restrict__ L, int64_t
     }
 }
 
-// transposed solves: forward with U^T (U^H when conj) through one front, step 1 (one CTA): z = U11^-T w[f ..]
-template <typename T, bool CJ>
-__global__ void __launch_bounds__(256) k_fwdUt(const T *__restrict__ L, int64_t nrows, int64_t npiv, int64_t f,
-                                               T *__restrict__ Wc, int64_t n, int64_t nrhs, DevStatus *st)
-{
-    for (int64_t i = 0; i < npiv; i++) {
-        T d = L[i + i * nrows];
-        if (CJ) d = conjv(d);
-        if (is_zero(d)) { if (threadIdx.x == 0) set_status(st, ST_SOLVE_ZERO, f + i, 0, 0); return; }
-        for (int64_t r = threadIdx.x; r < nrhs; r += blockDim.x) Wc[f + i + r * n] = divv(Wc[f + i + r * n], d);
-        __syncthreads();
-        for (int64_t e = threadIdx.x; e < (npiv - i - 1) * nrhs; e += blockDim.x) {
-            const int64_t j = i + 1 + e % (npiv - i - 1), r = e / (npiv - i - 1);
-            T u = L[i + j * nrows];
-            if (CJ) u = conjv(u);
-            Wc[f + j + r * n] = sub(Wc[f + j + r * n], mul(u, Wc[f + i + r * n]));
-        }
-        __syncthreads();
-    }
-}
 
 // step 2 (many CTAs, a warp per CB column): w[cbcol[c]] -= U12[:, c]^T z
 template <typename T, bool CJ>

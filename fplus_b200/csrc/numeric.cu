@@ -313,16 +313,12 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     if ((rc = ensure_async(N, (void **)&N.perm, &N.cap_perm, (size_t)(P.max_nrows > 0 ? P.max_nrows : 1) * 4, err, errlen))) return rc;
     static thread_local int attr_set = 0;
     if (!attr_set) {
-        CK(cudaFuncSetAttribute(k_front_lu<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_front_lu2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_u12_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_front_tail<T, FT_TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_front_tail<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
-        CK(cudaFuncSetAttribute(k_u12_fused<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
-        CK(cudaFuncSetAttribute(k_u12_fused<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
-        CK(cudaFuncSetAttribute(k_u12_fused<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         attr_set = 1;
     }
     if ((rc = dev_clear_status(N, err, errlen))) return rc;
