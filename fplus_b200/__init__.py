@@ -54,7 +54,8 @@ FPLUS_H_SYMBOLS = [
     "fplus_symbolic_nnz", "fplus_symbolic_row_perm", "fplus_symbolic_col_perm", "fplus_symbolic_n_dense_rows",
     "fplus_symbolic_n_dense_cols", "fplus_coletree_postorder", "fplus_default_options", "fplus_analyze_opts",
     "fplus_factor", "fplus_solve", "fplus_numeric_factors", "fplus_numeric_p", "fplus_numeric_q", "fplus_numeric_Dr",
-    "fplus_numeric_Dc", "fplus_numeric_free",
+    "fplus_numeric_Dc", "fplus_numeric_free", "fplus_tri_solve", "fplus_solve_plan_create", "fplus_tri_solve_plan",
+    "fplus_solve_plan_nsupernodes", "fplus_solve_plan_free", "fplus_factor_sn_perm", "fplus_factor_sn_sym", "fplus_ruiz",
 ]
 FPLUS_B200_H_SYMBOLS = [
     "fplus_b200_numeric_info", "fplus_b200_use_stream", "fplus_b200_factor_dev", "fplus_b200_solve_dev",
@@ -119,6 +120,22 @@ def lib():
     L.fplus_b200_launch_count.restype = ctypes.c_longlong
     L.fplus_b200_profile.argtypes = [ctypes.c_int]
     L.fplus_b200_profile_read.argtypes = [ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_longlong), _dp, _dp]
+    L.fplus_factors_free.argtypes = [ctypes.POINTER(Factors)]
+    _lo = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+           ctypes.c_double, ctypes.c_double, ctypes.POINTER(Factors), _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_factor_sn_perm.argtypes = [ctypes.c_int64, _i64p, _i64p, ctypes.c_void_p, ctypes.c_int, _i64p, _i64p] + _lo
+    L.fplus_factor_sn_sym.argtypes = [ctypes.c_void_p, _i64p, _i64p, ctypes.c_void_p, ctypes.c_int] + _lo
+    L.fplus_solve_plan_create.argtypes = [ctypes.c_int64, _i64p, _i64p, _i64p, _i64p, ctypes.POINTER(ctypes.c_void_p),
+                                          ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_tri_solve_plan.argtypes = [ctypes.c_void_p, ctypes.c_int64, _i64p, _i64p, ctypes.c_void_p, _i64p, _i64p,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int]
+    L.fplus_tri_solve.argtypes = [ctypes.c_int64, _i64p, _i64p, ctypes.c_void_p, _i64p, _i64p, ctypes.c_void_p,
+                                  ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    L.fplus_solve_plan_nsupernodes.argtypes = [ctypes.c_void_p]
+    L.fplus_solve_plan_nsupernodes.restype = ctypes.c_int64
+    L.fplus_solve_plan_free.argtypes = [ctypes.c_void_p]
+    L.fplus_ruiz.argtypes = [ctypes.c_int64, _i64p, _i64p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                             ctypes.c_double, ctypes.c_int, _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
     _lib = L
     return L
 
@@ -365,3 +382,207 @@ def interior_order(n, Ap, Ai, trow=None, tcol=None):
     tc = None if tcol is None else np.ascontiguousarray(tcol, dtype=np.uint8).ctypes.data_as(ctypes.c_char_p)
     _check(lib().fplus_b200_interior_order(n, _p64(Ap), _p64(Ai), tr, tc, _p64(perm)), None)
     return perm
+
+
+# ------------------------------------------------------------------------------------------------ the low-level interface
+# The functions of FPLUS's Python extension (_sparse_lu_c.c:634-696) over the same C entry points: factor_sn_perm,
+# solve_plan, lu_solve_plan, lu_solve.  The factor arrays returned by factor_sn_perm are views of the library's own
+# memory (no copy), so that passing them back to solve_plan / lu_solve_plan keeps the pointers the library recognises
+# and the solve runs with the factorization's device copy; the memory is released with the last array.
+
+
+class _FactorsOwner:
+    def __init__(self, f: Factors):
+        self.f = f
+
+    def __del__(self):
+        if _lib is not None:
+            _lib.fplus_factors_free(ctypes.byref(self.f))
+
+
+class _Buf:
+    """An __array_interface__ over library memory that keeps its owner alive while an array uses it."""
+
+    def __init__(self, owner, addr, n, dtype):
+        self._owner = owner
+        self.__array_interface__ = {"data": (addr, False), "shape": (n,), "typestr": np.dtype(dtype).str, "version": 3}
+
+
+def _view(owner, ptr, n, dtype):
+    addr = ctypes.cast(ptr, ctypes.c_void_p).value
+    if n == 0 or not addr:
+        return np.zeros(n, dtype)
+    return np.asarray(_Buf(owner, addr, n, dtype))
+
+
+def _factors_dict(f: Factors):
+    owner = _FactorsOwner(f)
+    n = int(f.n)
+    vt = np.complex128 if f.is_complex else np.float64
+    Lp = _view(owner, f.Lp, n + 1, np.int64)
+    Up = _view(owner, f.Up, n + 1, np.int64)
+    nl, nu = int(Lp[n]) if n >= 0 else 0, int(Up[n]) if n >= 0 else 0
+    return {"L_data": _view(owner, f.Lx, nl, vt), "L_indices": _view(owner, f.Li, nl, np.int64), "L_indptr": Lp,
+            "U_data": _view(owner, f.Ux, nu, vt), "U_indices": _view(owner, f.Ui, nu, np.int64), "U_indptr": Up,
+            "p": _view(owner, f.p, n, np.int64), "q": _view(owner, f.q, n, np.int64), "format": "csc"}
+
+
+def factor_sn_perm(data, indices, indptr, n, row_perm, col_perm, is_complex, equilibrate=1, ruiz_max_iter=20,
+                   ruiz_tol=1e-2, verbose=0, relax_rows=0, panel=1, use_gpu=0, gpu_min_flops=5e7,
+                   pivot_rel=FPLUS_PIVOT_REL_DEFAULT):
+    """fplus_factor_sn_perm: the factors of A[row_perm, :][:, col_perm] with Dr, Dc (permuted order), as a dict with the
+    keys of FPLUS's extension (L_data, L_indices, L_indptr, U_data, U_indices, U_indptr, p, q, format, Dr, Dc)."""
+    Ap = np.ascontiguousarray(indptr, dtype=np.int64)
+    Ai = np.ascontiguousarray(indices, dtype=np.int64)
+    Ax = np.ascontiguousarray(data, dtype=np.complex128 if is_complex else np.float64)
+    rp = np.ascontiguousarray(row_perm, dtype=np.int64)
+    cp = np.ascontiguousarray(col_perm, dtype=np.int64)
+    if Ap.shape[0] != n + 1 or rp.shape[0] != n or cp.shape[0] != n:
+        raise ValueError("factor_sn_perm: indptr must have length n + 1 and the permutations length n")
+    Dr = np.empty(max(n, 1)); Dc = np.empty(max(n, 1))
+    f = Factors()
+    err = ctypes.create_string_buffer(512)
+    rc = lib().fplus_factor_sn_perm(n, _p64(Ap), _p64(Ai), Ax.ctypes.data_as(ctypes.c_void_p), int(bool(is_complex)),
+                                    _p64(rp), _p64(cp), int(equilibrate), int(ruiz_max_iter), float(ruiz_tol), int(verbose),
+                                    int(relax_rows), int(panel), int(use_gpu), float(gpu_min_flops), float(pivot_rel),
+                                    ctypes.byref(f), Dr.ctypes.data_as(_dp), Dc.ctypes.data_as(_dp), err, 512)
+    _check(rc, err)
+    d = _factors_dict(f)
+    d["Dr"], d["Dc"] = Dr[:n], Dc[:n]
+    return d
+
+
+def factor_sn_sym(sym: "Symbolic", data, indices, indptr, is_complex, equilibrate=1, ruiz_max_iter=20, ruiz_tol=1e-2,
+                  verbose=0, relax_rows=0, panel=1, use_gpu=0, gpu_min_flops=5e7, pivot_rel=FPLUS_PIVOT_REL_DEFAULT):
+    """fplus_factor_sn_sym: factor_sn_perm with the orders of an analysis."""
+    n = sym.n
+    Ap = np.ascontiguousarray(indptr, dtype=np.int64)
+    Ai = np.ascontiguousarray(indices, dtype=np.int64)
+    Ax = np.ascontiguousarray(data, dtype=np.complex128 if is_complex else np.float64)
+    Dr = np.empty(max(n, 1)); Dc = np.empty(max(n, 1))
+    f = Factors()
+    err = ctypes.create_string_buffer(512)
+    rc = lib().fplus_factor_sn_sym(sym._h, _p64(Ap), _p64(Ai), Ax.ctypes.data_as(ctypes.c_void_p), int(bool(is_complex)),
+                                   int(equilibrate), int(ruiz_max_iter), float(ruiz_tol), int(verbose), int(relax_rows),
+                                   int(panel), int(use_gpu), float(gpu_min_flops), float(pivot_rel), ctypes.byref(f),
+                                   Dr.ctypes.data_as(_dp), Dc.ctypes.data_as(_dp), err, 512)
+    _check(rc, err)
+    d = _factors_dict(f)
+    d["Dr"], d["Dc"] = Dr[:n], Dc[:n]
+    return d
+
+
+class SolvePlan:
+    """fplus_solve_plan_create on CSC factor patterns; freed with the object."""
+
+    def __init__(self, Lp, Li, Up, Ui):
+        self._keep = [np.ascontiguousarray(a, dtype=np.int64) for a in (Lp, Li, Up, Ui)]
+        Lp, Li, Up, Ui = self._keep
+        self.n = Lp.shape[0] - 1
+        if Up.shape[0] != self.n + 1:
+            raise ValueError("solve_plan: Lp and Up must both have length n + 1")
+        self._h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        _check(lib().fplus_solve_plan_create(self.n, _p64(Lp), _p64(Li), _p64(Up), _p64(Ui), ctypes.byref(self._h), err, 512), err)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib is not None:
+            _lib.fplus_solve_plan_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    @property
+    def nsupernodes(self) -> int:
+        return int(lib().fplus_solve_plan_nsupernodes(self._h))
+
+
+def solve_plan(Lp, Li, Up, Ui) -> SolvePlan:
+    return SolvePlan(Lp, Li, Up, Ui)
+
+
+def _solve_x(b, n, is_complex, name):
+    x = np.array(b, dtype=np.complex128 if is_complex else np.float64, order="F", copy=True)
+    if x.ndim not in (1, 2) or x.shape[0] != n:
+        raise ValueError(f"{name}: b must have shape (n,) or (n, nrhs)")
+    return x
+
+
+def _solve_rc(rc, name):
+    if rc == FPLUS_ERR_SINGULAR:
+        raise FplusError(rc, f"{name}: zero or missing diagonal in U")
+    if rc == FPLUS_ERR_BADARG:
+        raise FplusError(rc, f"{name}: the plan does not match these factors")
+    if rc != FPLUS_OK:
+        raise FplusError(rc, f"{name} failed")
+
+
+def lu_solve_plan(plan: SolvePlan, Lp, Li, Lx, Up, Ui, Ux, b, trans, is_complex):
+    """fplus_tri_solve_plan on a copy of b ((n,) or (n, nrhs)): trans 0 L U x = b, 1 (L U)^T x = b, 2 (L U)^H x = b."""
+    vt = np.complex128 if is_complex else np.float64
+    Lp, Li, Up, Ui = (np.ascontiguousarray(a, dtype=np.int64) for a in (Lp, Li, Up, Ui))
+    Lx, Ux = np.ascontiguousarray(Lx, dtype=vt), np.ascontiguousarray(Ux, dtype=vt)
+    n = Lp.shape[0] - 1
+    x = _solve_x(b, n, is_complex, "lu_solve_plan")
+    nrhs = 1 if x.ndim == 1 else x.shape[1]
+    rc = lib().fplus_tri_solve_plan(plan._h, n, _p64(Lp), _p64(Li), Lx.ctypes.data_as(ctypes.c_void_p), _p64(Up), _p64(Ui),
+                                    Ux.ctypes.data_as(ctypes.c_void_p), x.ctypes.data_as(ctypes.c_void_p), nrhs, n,
+                                    int(trans), int(bool(is_complex)))
+    _solve_rc(rc, "lu_solve_plan")
+    return x
+
+
+def lu_solve(Lp, Li, Lx, Up, Ui, Ux, b, trans, is_complex):
+    """fplus_tri_solve, one right-hand side at a time, on a copy of b."""
+    vt = np.complex128 if is_complex else np.float64
+    Lp, Li, Up, Ui = (np.ascontiguousarray(a, dtype=np.int64) for a in (Lp, Li, Up, Ui))
+    Lx, Ux = np.ascontiguousarray(Lx, dtype=vt), np.ascontiguousarray(Ux, dtype=vt)
+    n = Lp.shape[0] - 1
+    x = _solve_x(b, n, is_complex, "lu_solve")
+    cols = [x] if x.ndim == 1 else [x[:, r] for r in range(x.shape[1])]
+    for c in cols:
+        rc = lib().fplus_tri_solve(n, _p64(Lp), _p64(Li), Lx.ctypes.data_as(ctypes.c_void_p), _p64(Up), _p64(Ui),
+                                   Ux.ctypes.data_as(ctypes.c_void_p), c.ctypes.data_as(ctypes.c_void_p), int(trans),
+                                   int(bool(is_complex)))
+        _solve_rc(rc, "lu_solve")
+    return x
+
+
+def lu_solve_perm(plan: SolvePlan, Lp, Li, Lx, Up, Ui, Ux, b, trans, is_complex, p, q, Dr, Dc):
+    """FPLUS's lu_solve_perm (_sparse_lu_c.c:551-633): the right-hand sides gathered through the row (trans 0) or column
+    permutation with its scaling, the plan's solve, then scattered through the other one with the other scaling
+    (trans 0: w = Dr[p] b[p], x[q] = Dc[q] z; else w = Dc[q] b[q], x[p] = Dr[p] z).  Dr / Dc None: no scaling.
+    b: (n,) or (n, nrhs); returns a new array of b's shape."""
+    vt = np.complex128 if is_complex else np.float64
+    bin_ = np.asarray(b, dtype=vt)
+    n = np.asarray(Lp).shape[0] - 1
+    if trans not in (0, 1, 2):
+        raise ValueError("lu_solve_perm: trans must be 0, 1 or 2")
+    p = np.asarray(p, dtype=np.int64); q = np.asarray(q, dtype=np.int64)
+    if bin_.ndim not in (1, 2) or bin_.shape[0] != n or p.shape[0] != n or q.shape[0] != n \
+            or (Dr is not None and len(Dr) != n) or (Dc is not None and len(Dc) != n):
+        raise ValueError("lu_solve_perm: b must have shape (n,) or (n, nrhs); p, q, Dr, Dc length n")
+    if n and (p.min() < 0 or p.max() >= n or q.min() < 0 or q.max() >= n):
+        raise ValueError("lu_solve_perm: p or q out of range")
+    G, Sc = (p, q) if trans == 0 else (q, p)
+    Dg, Ds = (Dr, Dc) if trans == 0 else (Dc, Dr)
+    B2 = bin_.reshape(n, -1)
+    w = B2[G, :] * (np.asarray(Dg)[G][:, None] if Dg is not None else 1.0)
+    z = lu_solve_plan(plan, Lp, Li, Lx, Up, Ui, Ux, w, trans, is_complex)
+    out = np.empty_like(B2)
+    out[Sc, :] = z * (np.asarray(Ds)[Sc][:, None] if Ds is not None else 1.0)
+    return out.reshape(bin_.shape)
+
+
+def ruiz_equilibrate(data, indices, indptr, n, max_iter, tol, is_complex, verbose=0, is_csc=0):
+    """fplus_ruiz on a copy of data (CSR, or CSC when is_csc), as FPLUS's ruiz_equilibrate: {"Dr", "Dc", "data"} with
+    diag(Dr) A diag(Dc) in data (same indices and indptr)."""
+    Ap = np.ascontiguousarray(indptr, dtype=np.int64)
+    Ai = np.ascontiguousarray(indices, dtype=np.int64)
+    x = np.array(data, dtype=np.complex128 if is_complex else np.float64, copy=True)
+    if Ap.shape[0] != n + 1:
+        raise ValueError("ruiz_equilibrate: indptr must have length n + 1")
+    Dr = np.empty(max(n, 1)); Dc = np.empty(max(n, 1))
+    err = ctypes.create_string_buffer(512)
+    rc = lib().fplus_ruiz(n, _p64(Ap), _p64(Ai), x.ctypes.data_as(ctypes.c_void_p), int(bool(is_complex)), int(bool(is_csc)),
+                          int(max_iter), float(tol), int(verbose), Dr.ctypes.data_as(_dp), Dc.ctypes.data_as(_dp), err, 512)
+    _check(rc, err)
+    return {"Dr": Dr[:n], "Dc": Dc[:n], "data": x}

@@ -11,6 +11,9 @@
 #include <string>
 #include <functional>
 #include <atomic>
+#include <memory>
+#include <vector>
+#include "trisolve.hpp"
 
 using namespace fpl;
 
@@ -216,7 +219,7 @@ extern "C" int fplus_b200_factor_dev(const fplus_symbolic *sym, const int64_t *A
 #define SOLVE_GROUP 32
 
 static int solve_common(const fplus_numeric *num, void *b, int64_t nrhs, int64_t ldb, int trans, int on_device, char *err,
-                        size_t errlen)
+                        size_t errlen, int raw = 0)
 {
     if (!num) { errf(err, errlen, "fplus_solve: num is NULL"); return FPLUS_ERR_BADARG; }
     const int64_t n = num->n;
@@ -239,7 +242,7 @@ static int solve_common(const fplus_numeric *num, void *b, int64_t nrhs, int64_t
         cudaError_t e = cudaMemcpy2DAsync(N.xbuf, (size_t)n * vs, bb, (size_t)ldb * vs, (size_t)n * vs, (size_t)m,
                                           on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, N.stream);
         if (e != cudaSuccess) { errf(err, errlen, "CUDA: %s", cudaGetErrorString(e)); rc = FPLUS_ERR_GPU; break; }
-        rc = dev_solve(*num->plan, *num->dplan, N, N.xbuf, m, trans, err, errlen);
+        rc = dev_solve(*num->plan, *num->dplan, N, N.xbuf, m, trans, err, errlen, raw);
         if (rc) break;
         e = cudaMemcpy2DAsync(bb, (size_t)ldb * vs, N.xbuf, (size_t)n * vs, (size_t)n * vs, (size_t)m,
                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, N.stream);
@@ -327,9 +330,12 @@ extern "C" int fplus_b200_solve_dev(const fplus_numeric *num, void *b_dev, int64
     return solve_common(num, b_dev, nrhs, ldb, trans, 1, err, errlen);
 }
 
+static void low_unregister(const void *Lx);
+
 extern "C" void fplus_factors_free(fplus_factors *f)
 {
     if (!f) return;
+    if (f->Lx) low_unregister(f->Lx);
     free(f->Lp); free(f->Li); free(f->Lx); free(f->Up); free(f->Ui); free(f->Ux); free(f->p); free(f->q);
     f->Lp = f->Li = f->Up = f->Ui = f->p = f->q = nullptr; f->Lx = f->Ux = nullptr;
 }
@@ -520,4 +526,312 @@ extern "C" int fplus_b200_solve_dev_noalloc(const fplus_numeric *num, void *b_de
     }
     N.stream = saved;
     return rc;
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// The low-level interface that FPLUS's Python extension calls (FPLUS include/fplus.h:73-88, 125-134;
+// _sparse_lu_c.c:360, 526): the factorization of A[row_perm, :][:, col_perm] with orders the caller chose, returned as
+// host CSC factors, and triangular solves on CSC factors with a plan.
+//
+// The factorization is fplus_factor's GPU path on a symbolic object made from the given orders (kept in a small cache,
+// so that refactoring with the same orders and pattern reuses its front structure and dense-chain start).  Its device
+// factors stay alive beside the host arrays it returns, in a registry of the most recent DEV_KEEP factorizations: a
+// plan made on those very arrays (the same pointers) solves on the GPU with them, in the coordinates of the permuted
+// matrix.  A solve checks that the arrays are still the ones returned (pointers, sizes and a sample of the values);
+// anything else (factors from elsewhere, copies, modified values, an entry dropped from the registry) takes the
+// level-scheduled GPU sweeps over the arrays passed (trisolve.cu).  fplus_factors_free on the returned struct drops
+// the registry entry; the Python extension frees the arrays itself, so its entries go when the registry is full.
+
+namespace {
+
+constexpr size_t SYM_KEEP = 4, DEV_KEEP = 4;
+constexpr int FP_SAMPLES = 32;
+
+std::mutex g_sym_mu;
+std::vector<std::shared_ptr<fplus_symbolic>> g_syms;        // most recently used last
+
+struct DevFactors {
+    fplus_numeric *num = nullptr;
+    int64_t n = 0, nnzL = 0, nnzU = 0;
+    int is_complex = 0;
+    const int64_t *Lp = nullptr, *Li = nullptr, *Up = nullptr, *Ui = nullptr;
+    const void *Lx = nullptr, *Ux = nullptr;
+    std::vector<unsigned char> fp;                           // sampled values of Lx and Ux
+    ~DevFactors() { fplus_numeric_free(num); }
+};
+std::mutex g_dev_mu;
+std::vector<std::shared_ptr<DevFactors>> g_dev;             // most recent last
+
+void fingerprint(int64_t nnzL, const void *Lx, int64_t nnzU, const void *Ux, size_t vs, std::vector<unsigned char> &out)
+{
+    out.clear();
+    for (int part = 0; part < 2; part++) {
+        const int64_t m = part ? nnzU : nnzL;
+        const unsigned char *x = (const unsigned char *)(part ? Ux : Lx);
+        if (m <= 0) continue;
+        for (int k = 0; k < FP_SAMPLES; k++) {
+            const int64_t q = (int64_t)(((__int128)k * (m - 1)) / (FP_SAMPLES - 1));
+            out.insert(out.end(), x + (size_t)q * vs, x + (size_t)(q + 1) * vs);
+        }
+    }
+}
+
+// the cached symbolic object for these orders and this pattern, or a new one
+int sym_for_orders(int64_t n, const int64_t *Ap, const int64_t *Ai, const int64_t *rp, const int64_t *cp,
+                   std::shared_ptr<fplus_symbolic> *out, char *err, size_t errlen)
+{
+    const int64_t nnz = Ap[n];
+    {
+        std::lock_guard<std::mutex> lk(g_sym_mu);
+        for (size_t k = 0; k < g_syms.size(); k++) {
+            const fplus_symbolic &S = *g_syms[k];
+            if (S.n != n || S.nnz != nnz) continue;
+            if (std::memcmp(S.row_perm.data(), rp, (size_t)n * 8) || std::memcmp(S.col_perm.data(), cp, (size_t)n * 8)) continue;
+            if (std::memcmp(S.Ap0.data(), Ap, (size_t)(n + 1) * 8) || (nnz && std::memcmp(S.Ai0.data(), Ai, (size_t)nnz * 8))) continue;
+            *out = g_syms[k];
+            g_syms.erase(g_syms.begin() + (long)k);
+            g_syms.push_back(*out);
+            return FPLUS_OK;
+        }
+    }
+    fplus_symbolic *s = nullptr;
+    int rc = symbolic_from_orders(n, Ap, Ai, rp, cp, &s, err, errlen);
+    if (rc != FPLUS_OK) return rc;
+    out->reset(s, fplus_symbolic_free);
+    std::lock_guard<std::mutex> lk(g_sym_mu);
+    g_syms.push_back(*out);
+    if (g_syms.size() > SYM_KEEP) g_syms.erase(g_syms.begin());
+    return FPLUS_OK;
+}
+
+// fplus_factor on sym with the low-level arguments; the host factors (FPLUS src/factor_sn.c:741-808 layout, p and q of
+// the permuted matrix) into *out, the scalings in the permuted order into Dr, Dc; the device factors registered
+int low_factor(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex, int equilibrate,
+               int ruiz_max_iter, double ruiz_tol, int verbose, int64_t relax_rows, int64_t panel, int use_gpu,
+               double gpu_min_flops, double pivot_rel, fplus_factors *out, double *Dr, double *Dc, char *err, size_t errlen)
+{
+    fplus_options opt;
+    fplus_default_options(&opt);
+    opt.equilibrate = equilibrate; opt.ruiz_max_iter = ruiz_max_iter; opt.ruiz_tol = ruiz_tol; opt.verbose = verbose;
+    opt.relax_rows = relax_rows; opt.panel = panel; opt.use_gpu = use_gpu; opt.gpu_min_flops = gpu_min_flops;
+    opt.pivot_rel = pivot_rel;
+    fplus_numeric *num = nullptr;
+    int rc = fplus_factor(sym, Ap, Ai, Ax, is_complex, &opt, &num, err, errlen);
+    if (rc != FPLUS_OK) return rc;
+    {
+        std::lock_guard<std::mutex> lk(num->mu);
+        rc = materialize(num);
+        if (rc == FPLUS_OK) { *out = num->f; std::memset(&num->f, 0, sizeof(num->f)); num->have_host = false; }
+    }
+    if (rc != FPLUS_OK) {
+        fplus_numeric_free(num);
+        errf(err, errlen, rc == FPLUS_ERR_NOMEM ? "out of memory" : "reading the factors back failed");
+        return rc;
+    }
+    const int64_t n = num->n;
+    for (int64_t k = 0; k < n; k++) { Dr[k] = num->Drp[k]; Dc[k] = num->Dcp[k]; }
+    auto d = std::make_shared<DevFactors>();
+    d->num = num; d->n = n; d->is_complex = is_complex;
+    d->nnzL = out->Lp[n]; d->nnzU = out->Up[n];
+    d->Lp = out->Lp; d->Li = out->Li; d->Up = out->Up; d->Ui = out->Ui; d->Lx = out->Lx; d->Ux = out->Ux;
+    fingerprint(d->nnzL, d->Lx, d->nnzU, d->Ux, is_complex ? 16 : 8, d->fp);
+    std::shared_ptr<DevFactors> dropped;
+    {
+        std::lock_guard<std::mutex> lk(g_dev_mu);
+        g_dev.push_back(d);
+        if (g_dev.size() > DEV_KEEP) { dropped = g_dev.front(); g_dev.erase(g_dev.begin()); }
+    }
+    return FPLUS_OK;
+}
+
+}  // namespace
+
+static void low_unregister(const void *Lx)
+{
+    std::shared_ptr<DevFactors> dropped;      // released after the lock (its numeric frees device memory)
+    std::lock_guard<std::mutex> lk(g_dev_mu);
+    for (size_t k = 0; k < g_dev.size(); k++)
+        if (g_dev[k]->Lx == Lx) { dropped = g_dev[k]; g_dev.erase(g_dev.begin() + (long)k); break; }
+}
+
+// FPLUS include/fplus.h:125-129, src/pipeline.c:84-111
+extern "C" int fplus_factor_sn_perm(int64_t n, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex,
+                                    const int64_t *row_perm, const int64_t *col_perm, int equilibrate, int ruiz_max_iter,
+                                    double ruiz_tol, int verbose, int64_t relax_rows, int64_t panel, int use_gpu,
+                                    double gpu_min_flops, double pivot_rel, fplus_factors *out, double *Dr, double *Dc,
+                                    char *err, size_t errlen)
+{
+    if (!out) { errf(err, errlen, "out is NULL"); return FPLUS_ERR_BADARG; }
+    std::memset(out, 0, sizeof(*out));
+    int rc = check_compressed(n, Ap, Ai, 1, err, errlen);
+    if (rc == FPLUS_OK && (!row_perm || !col_perm || !Dr || !Dc || (!Ax && Ap[n] > 0))) {
+        errf(err, errlen, "NULL argument");
+        rc = FPLUS_ERR_BADARG;
+    }
+    if (rc == FPLUS_OK) rc = check_perm(n, row_perm, "row_perm", err, errlen);
+    if (rc == FPLUS_OK) rc = check_perm(n, col_perm, "col_perm", err, errlen);
+    if (rc != FPLUS_OK) return rc;
+    std::shared_ptr<fplus_symbolic> sym;
+    if ((rc = sym_for_orders(n, Ap, Ai, row_perm, col_perm, &sym, err, errlen))) return rc;
+    return low_factor(sym.get(), Ap, Ai, Ax, is_complex, equilibrate, ruiz_max_iter, ruiz_tol, verbose, relax_rows, panel,
+                      use_gpu, gpu_min_flops, pivot_rel, out, Dr, Dc, err, errlen);
+}
+
+// FPLUS include/fplus.h:130-134, src/pipeline.c:113-127
+extern "C" int fplus_factor_sn_sym(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex,
+                                   int equilibrate, int ruiz_max_iter, double ruiz_tol, int verbose, int64_t relax_rows,
+                                   int64_t panel, int use_gpu, double gpu_min_flops, double pivot_rel, fplus_factors *out,
+                                   double *Dr, double *Dc, char *err, size_t errlen)
+{
+    if (!out) { errf(err, errlen, "out is NULL"); return FPLUS_ERR_BADARG; }
+    std::memset(out, 0, sizeof(*out));
+    if (!sym || !Ap || !Dr || !Dc) { errf(err, errlen, "NULL argument"); return FPLUS_ERR_BADARG; }
+    if (Ap[sym->n] != sym->nnz) {
+        errf(err, errlen, "the matrix has %ld nonzeros, the symbolic analysis %ld", (long)Ap[sym->n], (long)sym->nnz);
+        return FPLUS_ERR_BADARG;
+    }
+    return low_factor(sym, Ap, Ai, Ax, is_complex, equilibrate, ruiz_max_iter, ruiz_tol, verbose, relax_rows, panel, use_gpu,
+                      gpu_min_flops, pivot_rel, out, Dr, Dc, err, errlen);
+}
+
+struct fplus_solve_plan {
+    int64_t n = 0, nnzL = 0, nnzU = 0, nsn = -1;
+    std::shared_ptr<DevFactors> dev;                 // the registered factorization these arrays came with, if any
+    std::vector<int64_t> udiag;                      // position of U(j, j), -1 when missing
+    std::mutex mu;
+    std::unique_ptr<TriPlan> gen;                    // the level-scheduled sweeps, built when first needed
+};
+
+// FPLUS include/fplus.h:81-83, src/solve_plan.c:81-207
+extern "C" int fplus_solve_plan_create(int64_t n, const int64_t *Lp, const int64_t *Li, const int64_t *Up, const int64_t *Ui,
+                                       fplus_solve_plan **plan, char *err, size_t errlen)
+{
+    if (!plan) { errf(err, errlen, "plan is NULL"); return FPLUS_ERR_BADARG; }
+    *plan = nullptr;
+    int rc = check_compressed(n, Lp, Li, 0, err, errlen);
+    if (rc == FPLUS_OK) rc = check_compressed(n, Up, Ui, 0, err, errlen);
+    if (rc != FPLUS_OK) return rc;
+    fplus_solve_plan *pl = new (std::nothrow) fplus_solve_plan;
+    if (!pl) { errf(err, errlen, "out of memory"); return FPLUS_ERR_NOMEM; }
+    try {
+        pl->n = n; pl->nnzL = Lp[n]; pl->nnzU = Up[n];
+        {
+            std::lock_guard<std::mutex> lk(g_dev_mu);
+            for (auto &d : g_dev)
+                if (d->n == n && d->Lp == Lp && d->Li == Li && d->Up == Up && d->Ui == Ui && d->nnzL == pl->nnzL && d->nnzU == pl->nnzU)
+                    pl->dev = d;
+        }
+        pl->udiag.assign((size_t)(n > 0 ? n : 1), -1);
+        if (pl->dev) {
+            // this library's U: rows ascending in every column, the diagonal last
+            for (int64_t j = 0; j < n; j++) if (Up[j + 1] > Up[j] && Ui[Up[j + 1] - 1] == j) pl->udiag[j] = Up[j + 1] - 1;
+            pl->nsn = (int64_t)pl->dev->num->plan->fronts.size();
+        } else {
+            pl->gen.reset(new TriPlan);
+            tri_plan_build(*pl->gen, n, Lp, Li, Up, Ui);
+            pl->udiag = pl->gen->udiag;
+        }
+    } catch (const std::bad_alloc &) {
+        delete pl;
+        errf(err, errlen, "out of memory");
+        return FPLUS_ERR_NOMEM;
+    }
+    *plan = pl;
+    return FPLUS_OK;
+}
+
+// FPLUS include/fplus.h:84-86, src/solve_plan.c:661-719
+extern "C" int fplus_tri_solve_plan(const fplus_solve_plan *pl, int64_t n, const int64_t *Lp, const int64_t *Li, const void *Lx,
+                                    const int64_t *Up, const int64_t *Ui, const void *Ux, void *x, int64_t nrhs, int64_t ldx,
+                                    int trans, int is_complex)
+{
+    if (!pl || !Lp || !Up || trans < 0 || trans > 2 || n < 0 || nrhs < 0 || ldx < n || n != pl->n || Lp[n] != pl->nnzL ||
+        Up[n] != pl->nnzU)
+        return FPLUS_ERR_BADARG;
+    const size_t vs = is_complex ? 16 : 8;
+    for (int64_t j = 0; j < n; j++) {      // a zero or missing pivot fails before x is touched
+        const int64_t q = pl->udiag[j];
+        if (q < 0) return FPLUS_ERR_SINGULAR;
+        const double *u = (const double *)((const char *)Ux + (size_t)q * vs);
+        if (u[0] == 0.0 && (!is_complex || u[1] == 0.0)) return FPLUS_ERR_SINGULAR;
+    }
+    if (nrhs == 0 || n == 0) return FPLUS_OK;
+    if (!x || !Lx || !Ux) return FPLUS_ERR_BADARG;
+    char err[256] = {0};
+    const DevFactors *d = pl->dev.get();
+    if (d && d->Lp == Lp && d->Li == Li && d->Up == Up && d->Ui == Ui && d->Lx == Lx && d->Ux == Ux && d->is_complex == is_complex) {
+        std::vector<unsigned char> fp;
+        fingerprint(d->nnzL, Lx, d->nnzU, Ux, vs, fp);
+        if (fp == d->fp) return solve_common(d->num, x, nrhs, ldx, trans, 0, err, sizeof(err), 1);
+    }
+    fplus_solve_plan *mp = const_cast<fplus_solve_plan *>(pl);      // the sweeps are built once, under the plan's lock
+    TriPlan *g = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(mp->mu);
+        if (!mp->gen) {
+            try {
+                mp->gen.reset(new TriPlan);
+                tri_plan_build(*mp->gen, n, Lp, Li, Up, Ui);
+            } catch (const std::bad_alloc &) {
+                mp->gen.reset();
+                return FPLUS_ERR_NOMEM;
+            }
+        }
+        g = mp->gen.get();
+    }
+    return tri_plan_solve(*g, Lx, Ux, x, nrhs, ldx, trans, is_complex, tl_stream, err, sizeof(err));
+}
+
+// FPLUS include/fplus.h:87
+extern "C" int64_t fplus_solve_plan_nsupernodes(const fplus_solve_plan *plan) { return plan ? plan->nsn : -1; }
+
+// FPLUS include/fplus.h:88
+extern "C" void fplus_solve_plan_free(fplus_solve_plan *plan) { delete plan; }
+
+// FPLUS include/fplus.h:73-74, src/solve.c:62-74: one right-hand side, through a plan made for the call
+extern "C" int fplus_tri_solve(int64_t n, const int64_t *Lp, const int64_t *Li, const void *Lx, const int64_t *Up,
+                               const int64_t *Ui, const void *Ux, void *x, int trans, int is_complex)
+{
+    if (trans < 0 || trans > 2 || n < 0) return FPLUS_ERR_BADARG;
+    fplus_solve_plan *pl = nullptr;
+    char err[256] = {0};
+    int rc = fplus_solve_plan_create(n, Lp, Li, Up, Ui, &pl, err, sizeof(err));
+    if (rc != FPLUS_OK) return rc;
+    rc = fplus_tri_solve_plan(pl, n, Lp, Li, Lx, Up, Ui, Ux, x, 1, n, trans, is_complex);
+    fplus_solve_plan_free(pl);
+    return rc;
+}
+
+// FPLUS include/fplus.h:66-67, src/equil.c:186-441: Ruiz equilibration in place on a CSC (is_csc) or CSR matrix, on the
+// GPU.  FPLUS computes the same scalings by either route; here a CSR matrix is equilibrated as its CSC form (the device
+// gathers the values into column order and the scaled values are scattered back).
+extern "C" int fplus_ruiz(int64_t n, const int64_t *indptr, const int64_t *indices, void *data, int is_complex, int is_csc,
+                          int max_iter, double tol, int verbose, double *Dr, double *Dc, char *err, size_t errlen)
+{
+    int rc = check_compressed(n, indptr, indices, 0, err, errlen);
+    if (rc == FPLUS_OK && ((!data && indptr[n] > 0) || (n > 0 && (!Dr || !Dc)))) { errf(err, errlen, "NULL argument"); rc = FPLUS_ERR_BADARG; }
+    if (rc == FPLUS_OK) rc = check_finite(indptr[n], data, is_complex, err, errlen);
+    if (rc != FPLUS_OK) return rc;
+    if (n == 0) return FPLUS_OK;
+    const int64_t nnz = indptr[n];
+    const size_t vs = is_complex ? 16 : 8;
+    std::vector<int64_t> Cp((size_t)n + 1, 0), Ci((size_t)(nnz > 0 ? nnz : 1)), src((size_t)(nnz > 0 ? nnz : 1));
+    if (is_csc) {
+        Cp.assign(indptr, indptr + n + 1);
+        for (int64_t k = 0; k < nnz; k++) { Ci[k] = indices[k]; src[k] = k; }
+    } else {
+        for (int64_t k = 0; k < nnz; k++) Cp[indices[k] + 1]++;
+        for (int64_t j = 0; j < n; j++) Cp[j + 1] += Cp[j];
+        std::vector<int64_t> fill(Cp.begin(), Cp.end() - 1);
+        for (int64_t i = 0; i < n; i++)
+            for (int64_t k = indptr[i]; k < indptr[i + 1]; k++) { const int64_t o = fill[indices[k]]++; Ci[o] = i; src[o] = k; }
+    }
+    std::vector<unsigned char> out((size_t)(nnz > 0 ? nnz : 1) * vs);
+    int iters = 0;
+    rc = dev_ruiz_matrix(n, Cp, Ci, src, data, out.data(), is_complex ? 1 : 0, max_iter, tol, Dr, Dc, &iters, tl_stream, err,
+                         errlen);
+    if (rc != FPLUS_OK) return rc;
+    for (int64_t k = 0; k < nnz; k++) std::memcpy((unsigned char *)data + (size_t)src[k] * vs, out.data() + (size_t)k * vs, vs);
+    if (verbose >= 1) { std::printf("[FPLUS] Ruiz: %d iterations (GPU)\n", iters); std::fflush(stdout); }
+    return FPLUS_OK;
 }

@@ -31,6 +31,10 @@ void colamd_order(int64_t m, int64_t n_col, const int64_t *Cp, const int64_t *Ci
 void coletree(int64_t m, int64_t n, const int64_t *Cp, const int64_t *Ci, int64_t *parent);
 void tree_postorder(int64_t n, const int64_t *parent, int64_t *post);
 
+// A symbolic object for the caller's own static orders (the low-level fplus_factor_sn_perm), order.cpp.
+int symbolic_from_orders(int64_t n, const int64_t *Ap, const int64_t *Ai, const int64_t *row_perm, const int64_t *col_perm,
+                         fplus_symbolic **out, char *err, size_t errlen);
+
 struct FrontPlan;     // the multifrontal structure (symbolic.cpp)
 struct DevPlan;       // its device copy (device.cu)
 

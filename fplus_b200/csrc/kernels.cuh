@@ -1114,7 +1114,8 @@ __global__ void __launch_bounds__(256) k_trsm_warp(T *__restrict__ X, int64_t ld
 // solves (x column-major n x nrhs; row space: rows of B; column / pivot space: columns of B = pivot steps)
 // =====================================================================================================================
 
-// Wr[r] = Drp[r] * b[row_perm[r]] (trans 0), or Wc[k] = Dcp[k] * b[col_perm[k]] (trans 1, 2)
+// Wr[r] = Drp[r] * b[row_perm[r]] (trans 0), or Wc[k] = Dcp[k] * b[col_perm[k]] (trans 1, 2); a null perm is the
+// identity and a null scale is 1 (the low-level solve on the factors of the permuted matrix)
 template <typename T>
 __global__ void k_rhs_in(T *__restrict__ out, const T *__restrict__ b, int64_t ldb, const int64_t *__restrict__ perm,
                          const double *__restrict__ scale, int64_t n, int64_t nrhs)
@@ -1122,11 +1123,13 @@ __global__ void k_rhs_in(T *__restrict__ out, const T *__restrict__ b, int64_t l
     const int64_t total = n * nrhs;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
         int64_t k = e % n, r = e / n;
-        out[e] = scal(b[perm[k] + r * ldb], scale[k]);
+        const T v = b[(perm ? perm[k] : k) + r * ldb];
+        out[e] = scale ? scal(v, scale[k]) : v;
     }
 }
 
-// x[perm[k]] = scale[sidx[k]] * v[k]  (trans 0: perm = col_perm, sidx = identity; trans 1/2: perm = row_perm o p_lu)
+// x[perm[k]] = scale[sidx[k]] * v[k]  (trans 0: perm = col_perm, sidx = identity; trans 1/2: perm = row_perm o p_lu);
+// a null perm is the identity and a null scale is 1
 template <typename T>
 __global__ void k_rhs_out(T *__restrict__ x, int64_t ldx, const T *__restrict__ v, const int64_t *__restrict__ perm,
                           const int64_t *__restrict__ inner, const double *__restrict__ scale, int64_t n, int64_t nrhs)
@@ -1135,7 +1138,7 @@ __global__ void k_rhs_out(T *__restrict__ x, int64_t ldx, const T *__restrict__ 
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
         int64_t k = e % n, r = e / n;
         int64_t s = inner ? inner[k] : k;
-        x[perm[s] + r * ldx] = scal(v[e], scale[s]);
+        x[(perm ? perm[s] : s) + r * ldx] = scale ? scal(v[e], scale[s]) : v[e];
     }
 }
 

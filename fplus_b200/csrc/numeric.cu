@@ -13,6 +13,7 @@ namespace fpl {
 static std::atomic<long long> g_launches{0};
 static inline void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 long long launch_count() { return g_launches.load(); }
+void add_launches(long long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
 // optional per-class device timing of the factorization's kernels (CUDA events around each launch of a class)
 static std::atomic<int> g_prof{0};
@@ -88,6 +89,18 @@ DevPlan::~DevPlan()
         if (p) cudaFree(p);
 }
 
+// B's columns cut into segments of at most COL_SEG entries (column, first entry, end), for the column passes
+static int upload_segments(int64_t n, const std::vector<int64_t> &Bp, DevPlan &D, char *err, size_t errlen)
+{
+    std::vector<int64_t> seg;
+    for (int64_t j = 0; j < n; j++)
+        for (int64_t p0 = Bp[j]; p0 < Bp[j + 1]; p0 += COL_SEG) {
+            seg.push_back(j); seg.push_back(p0); seg.push_back(std::min<int64_t>(p0 + COL_SEG, Bp[j + 1]));
+        }
+    D.nseg = (int64_t)seg.size() / 3;
+    return upload(seg, &D.seg, err, errlen);
+}
+
 int dev_upload_plan(const fplus_symbolic *S, const FrontPlan &P, DevPlan &D, char *err, size_t errlen)
 {
     CK(cudaGetDevice(&D.device));
@@ -102,15 +115,7 @@ int dev_upload_plan(const fplus_symbolic *S, const FrontPlan &P, DevPlan &D, cha
     if ((rc = upload(S->Bsrc, &D.Bsrc, err, errlen))) return rc;
     if ((rc = upload(S->row_perm, &D.row_perm, err, errlen))) return rc;
     if ((rc = upload(S->col_perm, &D.col_perm, err, errlen))) return rc;
-    {
-        std::vector<int64_t> seg;
-        for (int64_t j = 0; j < S->n; j++)
-            for (int64_t p0 = S->Bp[j]; p0 < S->Bp[j + 1]; p0 += COL_SEG) {
-                seg.push_back(j); seg.push_back(p0); seg.push_back(std::min<int64_t>(p0 + COL_SEG, S->Bp[j + 1]));
-            }
-        D.nseg = (int64_t)seg.size() / 3;
-        if ((rc = upload(seg, &D.seg, err, errlen))) return rc;
-    }
+    if ((rc = upload_segments(S->n, S->Bp, D, err, errlen))) return rc;
     {
         // the dense chain: trailing dense fronts, nb_chain pivots each (the last at most), columns [f, n), no gaps
         const int64_t nf = (int64_t)P.fronts.size(), nb = P.nb_chain;
@@ -576,6 +581,31 @@ int dev_equilibrate(const DevPlan &D, DevNum &N, int equilibrate, int max_iter, 
                   : run_equil<double>(D, N, equilibrate, max_iter, tol, err, errlen);
 }
 
+int dev_ruiz_matrix(int64_t n, const std::vector<int64_t> &Cp, const std::vector<int64_t> &Ci, const std::vector<int64_t> &src,
+                    const void *x_in, void *x_out, int cplx, int max_iter, double tol, double *Dr, double *Dc, int *iters,
+                    cudaStream_t stream, char *err, size_t errlen)
+{
+    const int64_t nnz = Cp[n];
+    DevPlan D;
+    CK(cudaGetDevice(&D.device));
+    int rc;
+    if ((rc = upload(Cp, &D.Bp, err, errlen)) || (rc = upload(Ci, &D.Bi, err, errlen)) || (rc = upload(src, &D.Bsrc, err, errlen)) ||
+        (rc = upload_segments(n, Cp, D, err, errlen)))
+        return rc;
+    DevNum N;
+    if (stream) N.stream = stream;
+    if ((rc = dev_num_init(N, n, nnz, cplx, err, errlen))) return rc;
+    const size_t bytes = (size_t)nnz * (size_t)N.vs;
+    if (bytes) CK(cudaMemcpyAsync(N.Ax, x_in, bytes, cudaMemcpyHostToDevice, N.stream));
+    if ((rc = dev_equilibrate(D, N, 1, max_iter, tol, err, errlen))) { cudaStreamSynchronize(N.stream); return rc; }
+    if (bytes) CK(cudaMemcpyAsync(x_out, N.Bx, bytes, cudaMemcpyDeviceToHost, N.stream));
+    CK(cudaMemcpyAsync(Dr, N.Drp, (size_t)n * 8, cudaMemcpyDeviceToHost, N.stream));
+    CK(cudaMemcpyAsync(Dc, N.Dcp, (size_t)n * 8, cudaMemcpyDeviceToHost, N.stream));
+    CK(cudaStreamSynchronize(N.stream));
+    *iters = N.ruiz_iters;
+    return FPLUS_OK;
+}
+
 int dev_factor_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pivot_rel, int64_t *border_front,
                       char *err, size_t errlen)
 {
@@ -586,7 +616,8 @@ int dev_factor_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
 // ---------------------------------------------------------------------------------------------------------------------
 // solves on device buffers: x (n x nrhs, ld = n) in, solution out, through the plan's fronts
 template <typename T>
-static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int64_t nrhs, int trans, char *err, size_t errlen)
+static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int64_t nrhs, int trans, int raw, char *err,
+                     size_t errlen)
 {
     cudaStream_t s = N.stream;
     const int64_t n = N.n;
@@ -628,8 +659,10 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
         CK(cudaFuncSetAttribute(k_bwdLt<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     }
     if (trans == 0) {
-        // R (row space) = Dr * b[row_perm]; forward with L; S2 = R[p_lu] (pivot order); backward with U into R
-        k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, n, D.row_perm, N.Drp, n, nrhs), note_launch();
+        // R (row space) = Dr * b[row_perm]; forward with L; S2 = R[p_lu] (pivot order); backward with U into R.  raw:
+        // b is in pivot order (R[i] = b[pinv[i]]), without scaling
+        if (raw) k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, n, N.pinv, nullptr, n, nrhs), note_launch();
+        else k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, n, D.row_perm, N.Drp, n, nrhs), note_launch();
         for (int64_t fi = 0; fi < nf; fi++) {
             const Front &F = P.fronts[fi];
             if (F.npiv == 0 || F.nrows == 0) continue;
@@ -677,11 +710,13 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
                                                                      D.cols + F.col_off + F.npiv, ncb > 0 ? bwd_chunk(ncb) : 0,
                                                                      part, S2, R, n, nrhs, N.st), note_launch();
         }
-        // x[col_perm[k]] = Dcp[k] * R[k]
-        k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, R, D.col_perm, nullptr, N.Dcp, n, nrhs), note_launch();
+        // x[col_perm[k]] = Dcp[k] * R[k]  (raw: x[k] = R[k])
+        k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, R, raw ? nullptr : D.col_perm, nullptr, raw ? nullptr : N.Dcp, n, nrhs),
+            note_launch();
     } else {
-        // R (column space) = Dc * b[col_perm]; forward with U^T; backward with L^T into S2 (pivot order)
-        k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, n, D.col_perm, N.Dcp, n, nrhs), note_launch();
+        // R (column space) = Dc * b[col_perm]; forward with U^T; backward with L^T into S2 (pivot order).  raw: R = b
+        k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, n, raw ? nullptr : D.col_perm, raw ? nullptr : N.Dcp, n, nrhs),
+            note_launch();
         const bool cj = trans == 2;
         for (int64_t fi = 0; fi < nf; fi++) {
             const Front &F = P.fronts[fi];
@@ -713,17 +748,19 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
             else if (cj) k_bwdLt<T, true><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
             else k_bwdLt<T, false><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
         }
-        // x[row_perm[p_lu[k]]] = Drp[p_lu[k]] * S2[k]
-        k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, S2, D.row_perm, N.p_lu, N.Drp, n, nrhs), note_launch();
+        // x[row_perm[p_lu[k]]] = Drp[p_lu[k]] * S2[k]  (raw: x[k] = S2[k], pivot order)
+        if (raw) k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, S2, nullptr, nullptr, nullptr, n, nrhs), note_launch();
+        else k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, S2, D.row_perm, N.p_lu, N.Drp, n, nrhs), note_launch();
     }
     CK(cudaGetLastError());
     return FPLUS_OK;
 }
 
-int dev_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, void *x_dev, int64_t nrhs, int trans, char *err, size_t errlen)
+int dev_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, void *x_dev, int64_t nrhs, int trans, char *err, size_t errlen,
+              int raw)
 {
-    return N.cplx ? run_solve<cplx>(P, D, N, (cplx *)x_dev, nrhs, trans, err, errlen)
-                  : run_solve<double>(P, D, N, (double *)x_dev, nrhs, trans, err, errlen);
+    return N.cplx ? run_solve<cplx>(P, D, N, (cplx *)x_dev, nrhs, trans, raw, err, errlen)
+                  : run_solve<double>(P, D, N, (double *)x_dev, nrhs, trans, raw, err, errlen);
 }
 
 // ---------------------------------------------------------------------------------------------------------------------

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstdint>
 #include <cstring>
+#include <vector>
 #include <cuda_runtime.h>
 #include "internal.hpp"
 #include "plan.hpp"
@@ -17,6 +18,7 @@ struct ProfClass { double ms = 0, flops = 0, bytes = 0; long long count = 0; };
 void prof_enable(int on);
 ProfClass prof_read(int cls);
 long long launch_count();
+void add_launches(long long k);          // kernel launches made outside numeric.cu
 
 inline double bitsd_h(unsigned long long b) { double d; std::memcpy(&d, &b, 8); return d; }
 
@@ -68,9 +70,17 @@ struct DevNum {
 int dev_upload_plan(const fplus_symbolic *S, const FrontPlan &P, DevPlan &D, char *err, size_t errlen);
 int dev_num_init(DevNum &N, int64_t n, int64_t nnz, int cplx, char *err, size_t errlen);
 int dev_equilibrate(const DevPlan &D, DevNum &N, int equilibrate, int max_iter, double tol, char *err, size_t errlen);
+// Ruiz equilibration of a caller's matrix (the public fplus_ruiz): its CSC pattern Cp, Ci and gather map src (CSC entry k
+// holds input value src[k]); x_in host values in the caller's order, x_out the scaled values in CSC order (host)
+int dev_ruiz_matrix(int64_t n, const std::vector<int64_t> &Cp, const std::vector<int64_t> &Ci, const std::vector<int64_t> &src,
+                    const void *x_in, void *x_out, int cplx, int max_iter, double tol, double *Dr, double *Dc, int *iters,
+                    cudaStream_t stream, char *err, size_t errlen);
 int dev_factor_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pivot_rel, int64_t *border_front,
                       char *err, size_t errlen);
-int dev_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, void *x_dev, int64_t nrhs, int trans, char *err, size_t errlen);
+// raw: b and x are in the coordinates of the factors of the permuted matrix (trans 0: b in pivot order, x in column
+// order; trans 1/2 the other way round), without the scalings (the low-level fplus_tri_solve_plan)
+int dev_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, void *x_dev, int64_t nrhs, int trans, char *err, size_t errlen,
+              int raw = 0);
 int dev_status(DevNum &N, int *code, int64_t *idx, char *err, size_t errlen);
 int dev_solve_noalloc(const FrontPlan &P, const DevPlan &D, DevNum &N, void *b_dev, int64_t ldb, int64_t nrhs, int trans,
                       cudaStream_t s, char *err, size_t errlen);

@@ -376,6 +376,66 @@ extern "C" int fplus_b200_interior_order(int64_t n, const int64_t *Ap, const int
     return FPLUS_OK;
 }
 
+namespace fpl {
+
+// The permuted pattern B = A[row_perm, :][:, col_perm] (rows ascending in each column) and its gather map, and the
+// analysed pattern itself; row_perm and col_perm are set.
+static void build_permuted(fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai)
+{
+    const int64_t n = sym->n, nnz = Ap[n];
+    std::vector<int64_t> inv((size_t)(n > 0 ? n : 1));
+    for (int64_t i = 0; i < n; i++) inv[sym->row_perm[i]] = i;
+    sym->Ap0.assign(Ap, Ap + n + 1);
+    sym->Ai0.assign(Ai, Ai + nnz);
+    sym->Bp.assign((size_t)n + 1, 0);
+    sym->Bi.resize((size_t)nnz);
+    sym->Bsrc.resize((size_t)nnz);
+    for (int64_t jj = 0; jj < n; jj++) { int64_t c = sym->col_perm[jj]; sym->Bp[jj + 1] = sym->Bp[jj] + Ap[c + 1] - Ap[c]; }
+    std::vector<std::pair<int64_t, int64_t>> tmp;
+    for (int64_t jj = 0; jj < n; jj++) {
+        int64_t c = sym->col_perm[jj];
+        tmp.clear();
+        for (int64_t q = Ap[c]; q < Ap[c + 1]; q++) tmp.emplace_back(inv[Ai[q]], q);
+        std::sort(tmp.begin(), tmp.end());
+        int64_t o = sym->Bp[jj];
+        for (auto &t : tmp) { sym->Bi[o] = t.first; sym->Bsrc[o] = t.second; o++; }
+    }
+}
+
+// A symbolic object for static orders the caller chose (FPLUS src/pipeline.c:84-111 factors A[row_perm, :][:, col_perm]
+// as given).  The trailing rows of B with more than max(n / 2, 10) entries, and likewise its trailing columns, become
+// the dense (border) lines of the front structure: where the orders come from fplus_analyze these are its dense lines.
+// A dense line elsewhere in the order is an ordinary row or column: correct, but its fronts are wide.
+int symbolic_from_orders(int64_t n, const int64_t *Ap, const int64_t *Ai, const int64_t *row_perm, const int64_t *col_perm,
+                         fplus_symbolic **out, char *err, size_t errlen)
+{
+    *out = nullptr;
+    fplus_symbolic *sym = new (std::nothrow) fplus_symbolic;
+    if (!sym) { errf(err, errlen, "out of memory"); return FPLUS_ERR_NOMEM; }
+    try {
+        const int64_t nnz = Ap[n];
+        sym->n = n; sym->nnz = nnz;
+        sym->row_perm.assign(row_perm, row_perm + n);
+        sym->col_perm.assign(col_perm, col_perm + n);
+        const double thr = std::max(0.5 * (double)n, 10.0);
+        std::vector<int64_t> cnt((size_t)(n > 0 ? n : 1), 0);
+        for (int64_t q = 0; q < nnz; q++) cnt[Ai[q]]++;
+        int64_t ntr = 0, ntc = 0;
+        while (ntr < n && (double)cnt[row_perm[n - 1 - ntr]] > thr) ntr++;
+        while (ntc < n && (double)(Ap[col_perm[n - 1 - ntc] + 1] - Ap[col_perm[n - 1 - ntc]]) > thr) ntc++;
+        sym->n_tau_rows = ntr; sym->n_tau_cols = ntc;
+        build_permuted(sym, Ap, Ai);
+    } catch (const std::bad_alloc &) {
+        delete sym;
+        errf(err, errlen, "out of memory");
+        return FPLUS_ERR_NOMEM;
+    }
+    *out = sym;
+    return FPLUS_OK;
+}
+
+}  // namespace fpl
+
 // FPLUS src/order.c:267-399, with this library's minimum-degree order in place of SuiteSparse's COLAMD / AMD (every
 // `ordering` value runs it: minimum degree on the graph of A^T A is what both orders compute).
 extern "C" int fplus_analyze_ord(int64_t n, const int64_t *Ap, const int64_t *Ai, int pin_dense, double tau_density,
@@ -440,24 +500,7 @@ extern "C" int fplus_analyze_ord(int64_t n, const int64_t *Ap, const int64_t *Ai
             for (int64_t q = 0; q < n; q++) if (!tcol[perm[q]]) sym->col_perm[k++] = perm[q];
             for (int64_t q = 0; q < n; q++) if (tcol[perm[q]]) sym->col_perm[k++] = perm[q];
         }
-        // the permuted pattern B = A[row_perm, :][:, col_perm] (rows ascending in each column) and its gather map
-        std::vector<int64_t> inv((size_t)(n > 0 ? n : 1));
-        for (int64_t i = 0; i < n; i++) inv[sym->row_perm[i]] = i;
-        sym->Ap0.assign(Ap, Ap + n + 1);
-        sym->Ai0.assign(Ai, Ai + nnz);
-        sym->Bp.assign((size_t)n + 1, 0);
-        sym->Bi.resize((size_t)nnz);
-        sym->Bsrc.resize((size_t)nnz);
-        for (int64_t jj = 0; jj < n; jj++) { int64_t c = sym->col_perm[jj]; sym->Bp[jj + 1] = sym->Bp[jj] + Ap[c + 1] - Ap[c]; }
-        std::vector<std::pair<int64_t, int64_t>> tmp;
-        for (int64_t jj = 0; jj < n; jj++) {
-            int64_t c = sym->col_perm[jj];
-            tmp.clear();
-            for (int64_t q = Ap[c]; q < Ap[c + 1]; q++) tmp.emplace_back(inv[Ai[q]], q);
-            std::sort(tmp.begin(), tmp.end());
-            int64_t o = sym->Bp[jj];
-            for (auto &t : tmp) { sym->Bi[o] = t.first; sym->Bsrc[o] = t.second; o++; }
-        }
+        build_permuted(sym, Ap, Ai);
     } catch (const std::bad_alloc &) {
         delete sym;
         errf(err, errlen, "out of memory");

@@ -52,8 +52,36 @@ typedef struct {
     int64_t n_pivots_replaced;
 } fplus_factors;
 
-/* FPLUS include/fplus.h:48 */
+/* FPLUS include/fplus.h:48.  Also releases the device copy of factors returned by fplus_factor_sn_perm / _sym. */
 void fplus_factors_free(fplus_factors *f);
+
+/* ---- the low-level interface (what FPLUS's Python extension calls: _sparse_lu_c.c:360, 526) ---- */
+
+/* FPLUS include/fplus.h:64-67: Ruiz L-inf equilibration in place: data (CSR, or CSC when is_csc) becomes
+ * diag(Dr) A diag(Dc); Dr, Dc (length n) are filled.  Both routes give the same scalings.  On the GPU. */
+int fplus_ruiz(int64_t n, const int64_t *indptr, const int64_t *indices, void *data, int is_complex, int is_csc,
+               int max_iter, double tol, int verbose, double *Dr, double *Dc, char *err, size_t errlen);
+
+/* FPLUS include/fplus.h:73-74: triangular solve in place on x (one right-hand side): trans 0 solves L U x = b, 1
+ * (L U)^T x = b, 2 (L U)^H x = b.  L unit lower (an explicit unit diagonal is skipped), U upper with its diagonal stored.
+ * FPLUS_ERR_SINGULAR for a zero or missing diagonal in U.  On the GPU, through a plan made for the call. */
+int fplus_tri_solve(int64_t n, const int64_t *Lp, const int64_t *Li, const void *Lx, const int64_t *Up, const int64_t *Ui,
+                    const void *Ux, void *x, int trans, int is_complex);
+
+/* FPLUS include/fplus.h:81-88: solve plans.  A plan is made once per factorization from the CSC patterns; then
+ * fplus_tri_solve_plan solves for nrhs right-hand sides stored column-major in x (leading dimension ldx >= n), in place,
+ * with the same factor arrays.  A zero or missing diagonal in U fails (FPLUS_ERR_SINGULAR) before x is touched.  In this
+ * build the solves run on the GPU: for the arrays fplus_factor_sn_perm / _sym returned (the same pointers, the values
+ * unchanged) with the factorization's device copy; for any other CSC factors with level-scheduled sweeps over the arrays
+ * given.  nsupernodes: the fronts of the factorization for the former, -1 for the latter. */
+typedef struct fplus_solve_plan fplus_solve_plan;
+int fplus_solve_plan_create(int64_t n, const int64_t *Lp, const int64_t *Li, const int64_t *Up, const int64_t *Ui,
+                            fplus_solve_plan **plan, char *err, size_t errlen);
+int fplus_tri_solve_plan(const fplus_solve_plan *plan, int64_t n, const int64_t *Lp, const int64_t *Li, const void *Lx,
+                         const int64_t *Up, const int64_t *Ui, const void *Ux, void *x, int64_t nrhs, int64_t ldx,
+                         int trans, int is_complex);
+int64_t fplus_solve_plan_nsupernodes(const fplus_solve_plan *plan);
+void fplus_solve_plan_free(fplus_solve_plan *plan);
 
 /* ---- symbolic analysis (FPLUS include/fplus.h:94-120) ---- */
 typedef struct fplus_symbolic fplus_symbolic;
@@ -78,6 +106,22 @@ const int64_t *fplus_symbolic_row_perm(const fplus_symbolic *sym);   /* A[row_pe
 const int64_t *fplus_symbolic_col_perm(const fplus_symbolic *sym);
 int64_t fplus_symbolic_n_dense_rows(const fplus_symbolic *sym);
 int64_t fplus_symbolic_n_dense_cols(const fplus_symbolic *sym);
+
+/* FPLUS include/fplus.h:125-129: the factorization of A[row_perm, :][:, col_perm] (A canonical CSC): the permuted
+ * matrix, Ruiz (when equilibrate; Dr, Dc of length n filled, in the permuted order), then the LU with partial pivoting.
+ * The host factors in *out and p (q the identity) refer to the permuted matrix; free them with fplus_factors_free.
+ * relax_rows, panel, use_gpu and gpu_min_flops are accepted; the work runs on the GPU as in fplus_factor.  The device
+ * factors are kept with the returned arrays, so that a plan made on those arrays solves with them. */
+int fplus_factor_sn_perm(int64_t n, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex,
+                         const int64_t *row_perm, const int64_t *col_perm,
+                         int equilibrate, int ruiz_max_iter, double ruiz_tol, int verbose,
+                         int64_t relax_rows, int64_t panel, int use_gpu, double gpu_min_flops, double pivot_rel,
+                         fplus_factors *out, double *Dr, double *Dc, char *err, size_t errlen);
+/* FPLUS include/fplus.h:130-134: the same with the orders of a symbolic analysis (the pattern must be the analysed one) */
+int fplus_factor_sn_sym(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex,
+                        int equilibrate, int ruiz_max_iter, double ruiz_tol, int verbose,
+                        int64_t relax_rows, int64_t panel, int use_gpu, double gpu_min_flops, double pivot_rel,
+                        fplus_factors *out, double *Dr, double *Dc, char *err, size_t errlen);
 
 /* FPLUS include/fplus.h:92: postorder of the column elimination tree of the m x n CSC pattern; post[k] = the column placed
  * k-th. */

@@ -319,3 +319,45 @@ def test_batch_argument_checks_on_host():
     assert L.fplus_b200_factor_batch(3, None, None, None, None, 0, None, 2, None, None, err, 256) == F.FPLUS_ERR_BADARG
     assert L.fplus_b200_solve_batch(0, None, None, None, None, 0, 2, None, err, 256) == F.FPLUS_OK
     assert L.fplus_b200_solve_batch(2, None, None, None, None, 0, 2, None, err, 256) == F.FPLUS_ERR_BADARG
+
+
+def test_lowlevel_argument_checks_on_host():
+    """The low-level entry points refuse bad arguments, and a zero or missing diagonal of U, on the host before any
+    GPU work (FPLUS src/pipeline.c:91-99, src/solve_plan.c:664-673, src/solve.c:62-66); a plan on factors this library
+    did not return is host-only until its first solve and reports -1 supernodes."""
+    n, Ap, Ai, Ax = CASES["convdiff2d_g20"]()
+    rp = np.arange(n)
+    bad = rp.copy(); bad[3] = bad[4]
+    with pytest.raises(F.FplusError) as e:
+        F.factor_sn_perm(Ax, Ai, Ap, n, bad, rp, False)
+    assert e.value.code == F.FPLUS_ERR_BADARG
+    with pytest.raises(F.FplusError) as e:
+        F.factor_sn_perm(Ax, Ai[::-1].copy(), Ap, n, rp, rp, False)       # rows not ascending
+    assert e.value.code == F.FPLUS_ERR_BADARG
+    # unit lower L and upper U, one zero on U's diagonal
+    m = 6
+    Lm = sp.csc_matrix(np.tril(np.ones((m, m))))
+    Um = sp.csc_matrix(np.triu(np.ones((m, m)) * 2.0))
+    Lp, Li, Up, Ui = (a.astype(np.int64) for a in (Lm.indptr, Lm.indices, Um.indptr, Um.indices))
+    pl = F.solve_plan(Lp, Li, Up, Ui)
+    assert pl.nsupernodes == -1
+    Ux = Um.data.copy(); Ux[Up[3 + 1] - 1] = 0.0                           # U(3, 3) = 0
+    b = np.arange(1.0, m + 1)
+    with pytest.raises(F.FplusError) as e:
+        F.lu_solve_plan(pl, Lp, Li, Lm.data, Up, Ui, Ux, b, 0, False)
+    assert e.value.code == F.FPLUS_ERR_SINGULAR
+    L = F.lib()
+    x = b.copy()
+    assert L.fplus_tri_solve(m, F._p64(Lp), F._p64(Li), Lm.data.ctypes.data_as(ctypes.c_void_p), F._p64(Up), F._p64(Ui),
+                             Ux.ctypes.data_as(ctypes.c_void_p), x.ctypes.data_as(ctypes.c_void_p), 0, 0) == F.FPLUS_ERR_SINGULAR
+    assert np.array_equal(x, b), "x changed before the singular diagonal was reported"
+    for trans, nrhs, ldx, nn in ((3, 1, m, m), (0, -1, m, m), (0, 1, m - 1, m), (0, 1, m + 1, m + 1)):
+        assert L.fplus_tri_solve_plan(pl._h, nn, F._p64(Lp), F._p64(Li), Lm.data.ctypes.data_as(ctypes.c_void_p), F._p64(Up),
+                                      F._p64(Ui), Um.data.ctypes.data_as(ctypes.c_void_p), x.ctypes.data_as(ctypes.c_void_p),
+                                      nrhs, ldx, trans, 0) == F.FPLUS_ERR_BADARG
+    assert L.fplus_tri_solve(m, F._p64(Lp), F._p64(Li), Lm.data.ctypes.data_as(ctypes.c_void_p), F._p64(Up), F._p64(Ui),
+                             Um.data.ctypes.data_as(ctypes.c_void_p), x.ctypes.data_as(ctypes.c_void_p), 3, 0) == F.FPLUS_ERR_BADARG
+    # nrhs 0 on a plan: nothing to do, no GPU needed
+    assert L.fplus_tri_solve_plan(pl._h, m, F._p64(Lp), F._p64(Li), Lm.data.ctypes.data_as(ctypes.c_void_p), F._p64(Up),
+                                  F._p64(Ui), Um.data.ctypes.data_as(ctypes.c_void_p), x.ctypes.data_as(ctypes.c_void_p),
+                                  0, m, 0, 0) == F.FPLUS_OK
