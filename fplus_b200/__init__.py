@@ -61,7 +61,7 @@ FPLUS_B200_H_SYMBOLS = [
     "fplus_b200_numeric_info", "fplus_b200_use_stream", "fplus_b200_factor_dev", "fplus_b200_solve_dev",
     "fplus_b200_interior_order", "fplus_b200_plan_size", "fplus_b200_plan_export", "fplus_b200_launch_count",
     "fplus_b200_profile", "fplus_b200_profile_read", "fplus_b200_solve_dev_noalloc", "fplus_b200_factor_batch",
-    "fplus_b200_solve_batch",
+    "fplus_b200_solve_batch", "fplus_b200_solve_refine",
 ]
 
 _lib = None
@@ -121,6 +121,9 @@ def lib():
     L.fplus_b200_profile.argtypes = [ctypes.c_int]
     L.fplus_b200_profile_read.argtypes = [ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_longlong), _dp, _dp]
     L.fplus_factors_free.argtypes = [ctypes.POINTER(Factors)]
+    L.fplus_b200_solve_refine.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_double, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
+                                          ctypes.c_size_t]
     _lo = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
            ctypes.c_double, ctypes.c_double, ctypes.POINTER(Factors), _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_factor_sn_perm.argtypes = [ctypes.c_int64, _i64p, _i64p, ctypes.c_void_p, ctypes.c_int, _i64p, _i64p] + _lo
@@ -261,6 +264,22 @@ class Numeric:
         err = ctypes.create_string_buffer(512)
         _check(lib().fplus_solve(self._h, X.ctypes.data_as(ctypes.c_void_p), X.shape[1], self.n, trans, err, 512), err)
         return X[:, 0] if one else X
+
+    def solve_refine(self, b, trans=0, max_iter=10, tol=2.0 ** -52):
+        """fplus_b200_solve_refine: (x, berr, iters), with the componentwise backward error and the corrections applied
+        per right-hand side."""
+        b = np.asarray(b)
+        dt = np.complex128 if self.is_complex else np.float64
+        one = b.ndim == 1
+        X = np.array(b.reshape(self.n, -1), dtype=dt, order="F", copy=True)
+        k = X.shape[1]
+        berr = np.zeros(max(k, 1))
+        iters = np.zeros(max(k, 1), dtype=np.int32)
+        err = ctypes.create_string_buffer(512)
+        _check(lib().fplus_b200_solve_refine(self._h, X.ctypes.data_as(ctypes.c_void_p), k, self.n, trans, int(max_iter),
+                                             float(tol), berr.ctypes.data_as(_dp),
+                                             iters.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), err, 512), err)
+        return (X[:, 0] if one else X), berr[:k], iters[:k]
 
     def solve_device(self, B, trans=0):
         """In place on a torch CUDA tensor holding nrhs right-hand sides column-major (shape (nrhs, n), contiguous)."""

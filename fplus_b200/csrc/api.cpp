@@ -835,3 +835,37 @@ extern "C" int fplus_ruiz(int64_t n, const int64_t *indptr, const int64_t *indic
     if (verbose >= 1) { std::printf("[FPLUS] Ruiz: %d iterations (GPU)\n", iters); std::fflush(stdout); }
     return FPLUS_OK;
 }
+
+// Solve with iterative refinement (include/fplus_b200.h).
+extern "C" int fplus_b200_solve_refine(const fplus_numeric *num, void *b, int64_t nrhs, int64_t ldb, int trans, int max_iter,
+                                       double tol, double *berr, int *iters, char *err, size_t errlen)
+{
+    if (!num) { errf(err, errlen, "fplus_b200_solve_refine: num is NULL"); return FPLUS_ERR_BADARG; }
+    const int64_t n = num->n;
+    if (trans < 0 || trans > 2 || nrhs < 0 || ldb < n || max_iter < 0 || !(tol >= 0.0)) {
+        errf(err, errlen, "fplus_b200_solve_refine: bad trans, nrhs, ldb, max_iter or tol");
+        return FPLUS_ERR_BADARG;
+    }
+    if (nrhs == 0 || n == 0) return FPLUS_OK;
+    if (!b) { errf(err, errlen, "fplus_b200_solve_refine: b is NULL"); return FPLUS_ERR_BADARG; }
+    std::vector<double> be((size_t)nrhs);
+    std::vector<int> it((size_t)nrhs);
+    std::lock_guard<std::mutex> lk(num->mu);
+    DevNum &N = *num->dev;
+    CKH(cudaSetDevice(N.device));
+    cudaStream_t saved = N.stream;
+    if (tl_stream) N.stream = tl_stream;
+    dev_clear_status(N, err, errlen);
+    int rc = dev_solve_refine(*num->plan, *num->dplan, N, b, ldb, nrhs, trans, max_iter, tol, be.data(), it.data(), err, errlen);
+    if (rc == FPLUS_OK) {
+        int code = 0; int64_t idx = 0;
+        rc = dev_status(N, &code, &idx, err, errlen);
+        if (rc == FPLUS_OK && code != 0) { errf(err, errlen, "fplus_b200_solve_refine: zero or missing diagonal in U"); rc = FPLUS_ERR_SINGULAR; }
+    }
+    N.stream = saved;
+    if (rc == FPLUS_OK) {
+        if (berr) std::memcpy(berr, be.data(), (size_t)nrhs * sizeof(double));
+        if (iters) std::memcpy(iters, it.data(), (size_t)nrhs * sizeof(int));
+    }
+    return rc;
+}

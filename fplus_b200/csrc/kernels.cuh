@@ -1857,4 +1857,65 @@ __global__ void k_pinv(const int64_t *__restrict__ p_lu, int64_t *__restrict__ p
     }
 }
 
+// =====================================================================================================================
+// iterative refinement: the residual r = b - op(A) x and the componentwise backward error, in the original coordinates
+// =====================================================================================================================
+
+// the sum over a warp by a fixed butterfly (every lane gets the same result)
+template <typename T> __device__ __forceinline__ T shfl_sum(T v)
+{
+    for (int m = 16; m > 0; m >>= 1) v = add(v, shfl_xor_v<T>(v, m));
+    return v;
+}
+
+// One warp per line of B = A[row_perm, :][:, col_perm]: trans 0 the rows of B (CSR: idx = B's column, the x entry
+// col_perm[idx], the output row row_perm[k]), trans 1 / 2 the columns of B (CSC: idx = B's row, x entry row_perm[idx],
+// the output col_perm[k]; conjugated for 2).  Entry e has the value Ax[src[e]].  The partial sums over the line are
+// added by a fixed butterfly.  r = b - op(A) x; the backward error of right-hand side c, max over lines of
+// |r| / (|op(A)| |x| + |b|) (moduli), goes to bits[c] by atomicMax on its bits (non-negative doubles order as their bits;
+// a zero denominator with a non-zero residual counts as infinity).
+template <typename T, bool CJ>
+__global__ void __launch_bounds__(256) k_resid(const int64_t *__restrict__ ptr, const int64_t *__restrict__ idx,
+                                               const int64_t *__restrict__ src, const T *__restrict__ Ax,
+                                               const int64_t *__restrict__ outmap, const int64_t *__restrict__ inmap,
+                                               const T *__restrict__ x, const T *__restrict__ b, T *__restrict__ r,
+                                               int64_t n, int64_t nrhs, unsigned long long *__restrict__ bits)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t k = w; k < n; k += nw) {
+        const int64_t e0 = ptr[k], e1 = ptr[k + 1], o = outmap[k];
+        for (int64_t c = 0; c < nrhs; c++) {
+            const T *xc = x + c * n;
+            T s = VT<T>::zero();
+            double a = 0.0;
+            for (int64_t e = e0 + lane; e < e1; e += 32) {
+                T v = Ax[src[e]];
+                if (CJ) v = conjv(v);
+                const T xv = xc[inmap[idx[e]]];
+                s = add(s, mul(v, xv));
+                a += vabs(v) * vabs(xv);
+            }
+            s = shfl_sum(s);
+            for (int m = 16; m > 0; m >>= 1) a += __shfl_xor_sync(0xffffffffu, a, m);
+            if (lane == 0) {
+                const T rr = sub(b[o + c * n], s);
+                r[o + c * n] = rr;
+                const double den = a + vabs(b[o + c * n]), num = vabs(rr);
+                const double be = den > 0.0 ? num / den : (num > 0.0 ? __longlong_as_double(0x7ff0000000000000ll) : 0.0);
+                atomicMax(bits + c, dbits(be));
+            }
+        }
+    }
+}
+
+// x += d, or x -= d (undo), over m contiguous entries
+template <typename T>
+__global__ void k_axpy1(T *__restrict__ x, const T *__restrict__ d, int64_t m, int undo)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x)
+        x[e] = undo ? sub(x[e], d[e]) : add(x[e], d[e]);
+}
+
 }  // namespace fpl

@@ -144,7 +144,8 @@ DevNum::~DevNum()
     for (void *p : {(void *)Ax, (void *)Bx, (void *)Drp, (void *)Dcp, (void *)colmax, (void *)Larena, (void *)Uarena,
                     (void *)cbstack, (void *)work, (void *)rowid, (void *)p_lu, (void *)pinv, (void *)ipiv, (void *)perm,
                     (void *)st, (void *)scratch, (void *)rbuf, (void *)sbuf, (void *)xbuf, (void *)part, (void *)work2,
-                    (void *)perm2})
+                    (void *)perm2, (void *)rr_p, (void *)rr_l, (void *)rr_s, (void *)ir_b, (void *)ir_x, (void *)ir_r,
+                    (void *)ir_d, (void *)ir_bits})
         if (p) cudaFreeAsync(p, stream);
     if (stream) cudaStreamSynchronize(stream);
     if (crit) cudaStreamSynchronize(crit);
@@ -931,6 +932,107 @@ int dev_check_finite(DevNum &N, char *err, size_t errlen)
         return FPLUS_ERR_BADARG;
     }
     return FPLUS_OK;
+}
+
+}  // namespace fpl
+
+// ---------------------------------------------------------------------------------------------------------------------
+// iterative refinement (the precision form's driver; here on the FP64 factors)
+namespace fpl {
+
+template <typename T>
+static int run_refine(const FrontPlan &P, const DevPlan &D, DevNum &N, void *bh, int64_t ldb, int64_t nrhs, int trans,
+                      int max_iter, double tol, double *berr, int *iters, char *err, size_t errlen)
+{
+    cudaStream_t s = N.stream;
+    const int64_t n = N.n, nnz = N.nnz;
+    int rc;
+    if (!N.rr_p) {
+        // B's rows from its columns: row k lists (column l, position of the entry in A's values)
+        std::vector<int64_t> Bp((size_t)n + 1), Bi((size_t)(nnz > 0 ? nnz : 1)), Bs((size_t)(nnz > 0 ? nnz : 1));
+        CK(cudaMemcpyAsync(Bp.data(), D.Bp, (size_t)(n + 1) * 8, cudaMemcpyDeviceToHost, s));
+        if (nnz) {
+            CK(cudaMemcpyAsync(Bi.data(), D.Bi, (size_t)nnz * 8, cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(Bs.data(), D.Bsrc, (size_t)nnz * 8, cudaMemcpyDeviceToHost, s));
+        }
+        CK(cudaStreamSynchronize(s));
+        std::vector<int64_t> rp((size_t)n + 1, 0), rl(Bi.size()), rs(Bi.size());
+        for (int64_t e = 0; e < nnz; e++) rp[Bi[e] + 1]++;
+        for (int64_t k = 0; k < n; k++) rp[k + 1] += rp[k];
+        std::vector<int64_t> fill(rp.begin(), rp.end() - 1);
+        for (int64_t l = 0; l < n; l++)
+            for (int64_t e = Bp[l]; e < Bp[l + 1]; e++) { const int64_t o = fill[Bi[e]]++; rl[o] = l; rs[o] = Bs[e]; }
+        if ((rc = ensure_async(N, (void **)&N.rr_p, &N.cap_rrp, rp.size() * 8, err, errlen)) ||
+            (rc = ensure_async(N, (void **)&N.rr_l, &N.cap_rrl, rl.size() * 8, err, errlen)) ||
+            (rc = ensure_async(N, (void **)&N.rr_s, &N.cap_rrs, rs.size() * 8, err, errlen)))
+            return rc;
+        CK(cudaMemcpyAsync(N.rr_p, rp.data(), rp.size() * 8, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(N.rr_l, rl.data(), rl.size() * 8, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(N.rr_s, rs.data(), rs.size() * 8, cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    const int64_t g = nrhs < 32 ? nrhs : 32;
+    const size_t vb = (size_t)n * (size_t)g * sizeof(T);
+    if ((rc = ensure_async(N, &N.ir_b, &N.cap_irb, vb, err, errlen)) || (rc = ensure_async(N, &N.ir_x, &N.cap_irx, vb, err, errlen)) ||
+        (rc = ensure_async(N, &N.ir_r, &N.cap_irr, vb, err, errlen)) || (rc = ensure_async(N, &N.ir_d, &N.cap_ird, vb, err, errlen)) ||
+        (rc = ensure_async(N, (void **)&N.ir_bits, &N.cap_bits, (size_t)g * 8, err, errlen)))
+        return rc;
+    T *Bd = (T *)N.ir_b, *X = (T *)N.ir_x, *R = (T *)N.ir_r, *Dd = (T *)N.ir_d;
+    const bool t0 = trans == 0;
+    const int64_t *ptr = t0 ? N.rr_p : D.Bp, *ix = t0 ? N.rr_l : D.Bi, *src = t0 ? N.rr_s : D.Bsrc;
+    const int64_t *outm = t0 ? D.row_perm : D.col_perm, *inm = t0 ? D.col_perm : D.row_perm;
+    std::vector<double> cur((size_t)g), prev((size_t)g);
+    std::vector<char> want((size_t)g), stopped((size_t)g);
+    const int grid = nblk(n * 32);
+    for (int64_t r0 = 0; r0 < nrhs; r0 += g) {
+        const int64_t m = nrhs - r0 < g ? nrhs - r0 : g;
+        char *bb = (char *)bh + (size_t)r0 * (size_t)ldb * sizeof(T);
+        CK(cudaMemcpy2DAsync(Bd, (size_t)n * sizeof(T), bb, (size_t)ldb * sizeof(T), (size_t)n * sizeof(T), (size_t)m,
+                             cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(X, Bd, (size_t)n * (size_t)m * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        if ((rc = dev_solve(P, D, N, X, m, trans, err, errlen))) return rc;
+        for (int64_t c = 0; c < m; c++) { iters[r0 + c] = 0; stopped[c] = 0; want[c] = 0; }
+        for (int it = 0;; it++) {
+            CK(cudaMemsetAsync(N.ir_bits, 0, (size_t)m * 8, s));
+            if (trans == 2) k_resid<T, true><<<grid, 256, 0, s>>>(ptr, ix, src, (const T *)N.Ax, outm, inm, X, Bd, R, n, m, N.ir_bits);
+            else k_resid<T, false><<<grid, 256, 0, s>>>(ptr, ix, src, (const T *)N.Ax, outm, inm, X, Bd, R, n, m, N.ir_bits);
+            note_launch();
+            CK(cudaMemcpyAsync(cur.data(), N.ir_bits, (size_t)m * 8, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            bool any = false;
+            for (int64_t c = 0; c < m; c++) {
+                if (it > 0 && want[c] && cur[c] > prev[c]) {      // the last correction made it worse: undo it
+                    k_axpy1<T><<<nblk(n), 256, 0, s>>>(X + c * n, Dd + c * n, n, 1), note_launch();
+                    cur[c] = prev[c];
+                    iters[r0 + c]--;
+                    stopped[c] = 1;
+                }
+                // LAPACK's rule (xGERFS): refine while the error is above the target and at least halves
+                want[c] = !stopped[c] && it < max_iter && cur[c] > tol && (it == 0 || 2.0 * cur[c] <= prev[c]);
+                any = any || want[c];
+            }
+            for (int64_t c = 0; c < m; c++) berr[r0 + c] = cur[c];
+            if (!any) break;
+            CK(cudaMemcpyAsync(Dd, R, (size_t)n * (size_t)m * sizeof(T), cudaMemcpyDeviceToDevice, s));
+            for (int64_t c = 0; c < m; c++)
+                if (!want[c]) CK(cudaMemsetAsync(Dd + c * n, 0, (size_t)n * sizeof(T), s));
+                else iters[r0 + c]++;
+            if ((rc = dev_solve(P, D, N, Dd, m, trans, err, errlen))) return rc;
+            k_axpy1<T><<<nblk(n * m), 256, 0, s>>>(X, Dd, n * m, 0), note_launch();
+            prev = cur;
+        }
+        CK(cudaMemcpy2DAsync(bb, (size_t)ldb * sizeof(T), X, (size_t)n * sizeof(T), (size_t)n * sizeof(T), (size_t)m,
+                             cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    return FPLUS_OK;
+}
+
+int dev_solve_refine(const FrontPlan &P, const DevPlan &D, DevNum &N, void *b, int64_t ldb, int64_t nrhs, int trans,
+                     int max_iter, double tol, double *berr, int *iters, char *err, size_t errlen)
+{
+    return N.cplx ? run_refine<cplx>(P, D, N, b, ldb, nrhs, trans, max_iter, tol, berr, iters, err, errlen)
+                  : run_refine<double>(P, D, N, b, ldb, nrhs, trans, max_iter, tol, berr, iters, err, errlen);
 }
 
 }  // namespace fpl

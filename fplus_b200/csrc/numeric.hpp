@@ -64,6 +64,11 @@ struct DevNum {
     void *rbuf = nullptr, *sbuf = nullptr, *xbuf = nullptr, *part = nullptr;
     size_t cap_r = 0, cap_s = 0, cap_x = 0, cap_part = 0;
     int ruiz_iters = 0;
+    // iterative refinement: B's rows (CSR; entry -> position in Ax), built on the first refined solve, and its buffers
+    int64_t *rr_p = nullptr, *rr_l = nullptr, *rr_s = nullptr;
+    void *ir_b = nullptr, *ir_x = nullptr, *ir_r = nullptr, *ir_d = nullptr;
+    unsigned long long *ir_bits = nullptr;
+    size_t cap_rrp = 0, cap_rrl = 0, cap_rrs = 0, cap_irb = 0, cap_irx = 0, cap_irr = 0, cap_ird = 0, cap_bits = 0;
     ~DevNum();
 };
 
@@ -82,6 +87,13 @@ int dev_factor_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
 int dev_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, void *x_dev, int64_t nrhs, int trans, char *err, size_t errlen,
               int raw = 0);
 int dev_status(DevNum &N, int *code, int64_t *idx, char *err, size_t errlen);
+// A solve with iterative refinement in FP64 (b in host memory, ld ldb, nrhs right-hand sides, solved in place): the
+// solve, then corrections x += solve(b - op(A) x) with the residual formed on the device from the factorization's own
+// copy of A, while a right-hand side's componentwise backward error is above tol and at least halves (at most max_iter
+// corrections).  A correction that raised the error is undone.  berr[c] is the final backward error, iters[c] the
+// corrections kept.
+int dev_solve_refine(const FrontPlan &P, const DevPlan &D, DevNum &N, void *b, int64_t ldb, int64_t nrhs, int trans,
+                     int max_iter, double tol, double *berr, int *iters, char *err, size_t errlen);
 int dev_solve_noalloc(const FrontPlan &P, const DevPlan &D, DevNum &N, void *b_dev, int64_t ldb, int64_t nrhs, int trans,
                       cudaStream_t s, char *err, size_t errlen);
 int dev_clear_status(DevNum &N, char *err, size_t errlen);

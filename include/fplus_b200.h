@@ -84,6 +84,16 @@ int fplus_b200_solve_batch(int64_t count, fplus_numeric *const *nums, void *cons
  * the GPU (from other streams or host threads) race on it: serialize them. */
 int fplus_b200_solve_dev_noalloc(const fplus_numeric *num, void *b_dev, int64_t nrhs, int64_t ldb, int trans, char *err, size_t errlen);
 
+/* fplus_solve with iterative refinement in FP64.  No counterpart in FPLUS: the refinement driver of the precision form.
+ * It solves in place on b (host memory, nrhs right-hand sides, column-major, leading dimension ldb >= n), then corrects
+ * x += solve(b - op(A) x) while a right-hand side's componentwise backward error max_i |r_i| / (|op(A)| |x| + |b|)_i is
+ * above tol and at least halves from one correction to the next, at most max_iter times (LAPACK's xGERFS rule).  The
+ * residual is formed on the GPU in FP64 from the factorization's own device copy of A, with a fixed summation order.
+ * berr[k] receives the final backward error and iters[k] the corrections applied to right-hand side k (either may be
+ * NULL).  max_iter 0 gives fplus_solve's result with its backward error. */
+int fplus_b200_solve_refine(const fplus_numeric *num, void *b, int64_t nrhs, int64_t ldb, int trans, int max_iter, double tol,
+                            double *berr, int *iters, char *err, size_t errlen);
+
 /* Kernel launches made by this library since it was loaded (all threads). */
 long long fplus_b200_launch_count(void);
 

@@ -361,3 +361,12 @@ def test_lowlevel_argument_checks_on_host():
     assert L.fplus_tri_solve_plan(pl._h, m, F._p64(Lp), F._p64(Li), Lm.data.ctypes.data_as(ctypes.c_void_p), F._p64(Up),
                                   F._p64(Ui), Um.data.ctypes.data_as(ctypes.c_void_p), x.ctypes.data_as(ctypes.c_void_p),
                                   0, m, 0, 0) == F.FPLUS_OK
+
+
+def test_solve_refine_argument_checks_on_host():
+    """fplus_b200_solve_refine refuses a NULL factorization before any GPU work."""
+    L = F.lib()
+    err = ctypes.create_string_buffer(256)
+    x = np.zeros(4)
+    assert L.fplus_b200_solve_refine(None, x.ctypes.data_as(ctypes.c_void_p), 1, 4, 0, 5, 0.0, None, None, err, 256) \
+        == F.FPLUS_ERR_BADARG
