@@ -223,13 +223,27 @@ __global__ void k_extend_add(T *__restrict__ W, int64_t ldw, const T *__restrict
 {
     if (st->code) return;
     const int64_t total = cbr * (c1 - c0);
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t t = e % cbr, c = c0 + e / cbr;
-        const int64_t pr = t < nslot ? slot + t : tau_base + (t - nslot);
-        const int64_t pc = relcol[c];
-        T v = cb[t + c * cbr];
-        T *w = W + pr + pc * ldw;
-        *w = add(*w, v);
+    if (total < INT_MAX && (int64_t)gridDim.x * blockDim.x < INT_MAX - total) {
+        // 32-bit index arithmetic (a 64-bit division per entry costs more than the entry's memory traffic)
+        const int cb32 = (int)cbr, tot32 = (int)total;
+        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < tot32; e += gridDim.x * blockDim.x) {
+            const int cl = e / cb32, t = e - cl * cb32;
+            const int64_t c = c0 + cl;
+            const int64_t pr = t < nslot ? slot + t : tau_base + (t - nslot);
+            const int64_t pc = relcol[c];
+            T v = cb[t + c * cbr];
+            T *w = W + pr + pc * ldw;
+            *w = add(*w, v);
+        }
+    } else {
+        for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+            const int64_t t = e % cbr, c = c0 + e / cbr;
+            const int64_t pr = t < nslot ? slot + t : tau_base + (t - nslot);
+            const int64_t pc = relcol[c];
+            T v = cb[t + c * cbr];
+            T *w = W + pr + pc * ldw;
+            *w = add(*w, v);
+        }
     }
     if (rowids)
         for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nslot; t += (int64_t)gridDim.x * blockDim.x)
@@ -590,13 +604,14 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
         for (int64_t t = tid; t < pa.nslot; t += nt) rid[pa.slot + t] = pa.child_rowid[t];
         __syncthreads();
         const T *cb = reinterpret_cast<const T *>(pa.cb);
-        const int64_t tot = pa.cbr * pa.h;
+        // the CB's pivot-column part is at most nrows x npiv entries: 32-bit index arithmetic
+        const int cbr = (int)pa.cbr, tot = (int)(pa.cbr * pa.h), nsl = (int)pa.nslot, sl = (int)pa.slot, tb = (int)pa.tau_base;
 #pragma unroll 4
-        for (int64_t e = tid; e < tot; e += nt) {
-            const int64_t t = e % pa.cbr, c = e / pa.cbr;
-            const int64_t pr = t < pa.nslot ? pa.slot + t : pa.tau_base + (t - pa.nslot);
-            T *a = A + pa.relcol[c] * nrows + pr;
-            *a = add(*a, cb[t + c * pa.cbr]);
+        for (int e = tid; e < tot; e += nt) {
+            const int c = e / cbr, t = e - c * cbr;
+            const int pr = t < nsl ? sl + t : tb + (t - nsl);
+            T *a = A + (int)pa.relcol[c] * nrows + pr;
+            *a = add(*a, cb[t + (int64_t)c * cbr]);
         }
     }
     for (int i = tid; i < nrows; i += nt) tag[i] = INT_MAX;
