@@ -61,7 +61,7 @@ FPLUS_B200_H_SYMBOLS = [
     "fplus_b200_numeric_info", "fplus_b200_use_stream", "fplus_b200_factor_dev", "fplus_b200_solve_dev",
     "fplus_b200_interior_order", "fplus_b200_plan_size", "fplus_b200_plan_export", "fplus_b200_launch_count",
     "fplus_b200_profile", "fplus_b200_profile_read", "fplus_b200_solve_dev_noalloc", "fplus_b200_factor_batch",
-    "fplus_b200_solve_batch", "fplus_b200_solve_refine",
+    "fplus_b200_solve_batch", "fplus_b200_solve_refine", "fplus_b200_symbolic_from_orders",
 ]
 
 _lib = None
@@ -121,6 +121,8 @@ def lib():
     L.fplus_b200_profile.argtypes = [ctypes.c_int]
     L.fplus_b200_profile_read.argtypes = [ctypes.c_int, _dp, ctypes.POINTER(ctypes.c_longlong), _dp, _dp]
     L.fplus_factors_free.argtypes = [ctypes.POINTER(Factors)]
+    L.fplus_b200_symbolic_from_orders.argtypes = [ctypes.c_int64, _i64p, _i64p, _i64p, _i64p, ctypes.POINTER(ctypes.c_void_p),
+                                                  ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_solve_refine.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_double, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
                                           ctypes.c_size_t]
@@ -184,6 +186,23 @@ class Symbolic:
         self._h = ctypes.c_void_p()
         err = ctypes.create_string_buffer(512)
         _check(lib().fplus_analyze_opts(n, _p64(Ap), _p64(Ai), ctypes.byref(self.options), ctypes.byref(self._h), err, 512), err)
+
+    @classmethod
+    def from_orders(cls, n, Ap, Ai, row_perm, col_perm):
+        """fplus_b200_symbolic_from_orders: the caller's static orders instead of the analysis."""
+        n, Ap, Ai, _ = csc_arrays(n, Ap, Ai)
+        rp = np.ascontiguousarray(row_perm, dtype=np.int64)
+        cp = np.ascontiguousarray(col_perm, dtype=np.int64)
+        if rp.shape[0] != n or cp.shape[0] != n:
+            raise ValueError("from_orders: the permutations must have length n")
+        self = cls.__new__(cls)
+        self.n, self.Ap, self.Ai = n, Ap, Ai
+        self.options = default_options()
+        self._h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        _check(lib().fplus_b200_symbolic_from_orders(n, _p64(Ap), _p64(Ai), _p64(rp), _p64(cp), ctypes.byref(self._h), err, 512),
+               err)
+        return self
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None and self._h.value:
@@ -605,3 +624,124 @@ def ruiz_equilibrate(data, indices, indptr, n, max_iter, tol, is_complex, verbos
                           int(max_iter), float(tol), int(verbose), Dr.ctypes.data_as(_dp), Dc.ctypes.data_as(_dp), err, 512)
     _check(rc, err)
     return {"Dr": Dr[:n], "Dc": Dc[:n], "data": x}
+
+
+class SparseLU:
+    """FPLUS's SparseLU (sparse_lu_full_pivot.py:680-763) on the GPU: ``SparseLU(A, **kwargs).solve(b, trans)``.
+
+    The keyword arguments are those of FPLUS's sparse_lu_full_pivot.  ``colamd`` (default False, as in FPLUS): the
+    library's fill-reducing analysis with ``pin_dense_rows``, ``tau_density``, ``tau_min_nnz``, the masks, ``postorder``
+    and ``ordering``; without it the identity orders.  ``equilibrate``: True (at most 20 Ruiz iterations), False / 0
+    (none) or an iteration count.  ``pivot_rel`` (None: FPLUS's default).  This build factors exactly with partial
+    pivoting: ``drop_tol`` must be 0 and ``pivot_strategy`` 'partial'.  ``relax_rows``, ``panel``, ``gpu``,
+    ``gpu_min_flops``, ``cache_ordering`` and ``verbose`` are accepted.  The factors stay in device memory and the
+    solves run there; ``L`` and ``U`` are read back on first use.
+    """
+
+    _ORDERINGS = {"colamd": 0, "amd": 1, "amd_ata": 1, "auto": 2}
+
+    def __init__(self, A, *, drop_tol=0.0, equilibrate=True, colamd=False, pin_dense_rows=False, tau_density=0.5,
+                 tau_min_nnz=10, tau_row_mask=None, tau_col_mask=None, pivot_strategy="partial", dtype=None, verbose=0,
+                 relax_rows=0, panel=1, cache_ordering=True, gpu=False, gpu_min_flops=5e7, pivot_rel=None, postorder=True,
+                 ordering="auto"):
+        import scipy.sparse as sp
+        if drop_tol != 0.0:
+            raise ValueError("SparseLU: this build computes the exact factorization (drop_tol must be 0)")
+        if pivot_strategy != "partial":
+            raise ValueError("SparseLU: this build pivots by columns only (pivot_strategy 'partial')")
+        if ordering not in self._ORDERINGS:
+            raise ValueError(f"SparseLU: unknown ordering {ordering!r}")
+        A = A if sp.issparse(A) else sp.csc_matrix(A)
+        if A.shape[0] != A.shape[1]:
+            raise ValueError("SparseLU: A must be square")
+        cplx = np.iscomplexobj(A.data)
+        if dtype is not None and np.dtype(dtype) not in (np.dtype(np.complex128), np.dtype(np.float64)):
+            raise ValueError("SparseLU: this build works in float64 / complex128")
+        if dtype is not None and np.dtype(dtype) == np.dtype(np.complex128):
+            cplx = True
+        A = sp.csc_matrix(A, dtype=np.complex128 if cplx else np.float64)
+        A.sum_duplicates()
+        A.sort_indices()
+        n = A.shape[0]
+        Ap, Ai = A.indptr.astype(np.int64), A.indices.astype(np.int64)
+        if colamd:
+            def mask(m):
+                return None if m is None else np.ascontiguousarray(np.asarray(m, dtype=bool), dtype=np.uint8)
+            sym = Symbolic.__new__(Symbolic)
+            sym.n, sym.Ap, sym.Ai = n, Ap, Ai
+            sym.options = default_options()
+            sym._h = ctypes.c_void_p()
+            err = ctypes.create_string_buffer(512)
+            rm, cm = mask(tau_row_mask), mask(tau_col_mask)
+            _check(lib().fplus_analyze_ord(n, _p64(Ap), _p64(Ai), int(bool(pin_dense_rows)), float(tau_density),
+                                           int(tau_min_nnz), None if rm is None else rm.ctypes.data_as(ctypes.c_char_p),
+                                           None if cm is None else cm.ctypes.data_as(ctypes.c_char_p), int(bool(postorder)),
+                                           self._ORDERINGS[ordering], ctypes.byref(sym._h), err, 512), err)
+        else:
+            sym = Symbolic.from_orders(n, Ap, Ai, np.arange(n), np.arange(n))
+        if equilibrate is True or (not isinstance(equilibrate, bool) and int(equilibrate) < 0):
+            eq, iters = 1, 20
+        elif equilibrate is False or int(equilibrate) == 0:
+            eq, iters = 0, 20
+        else:
+            eq, iters = 1, int(equilibrate)
+        opts = default_options(equilibrate=eq, ruiz_max_iter=iters, verbose=int(verbose), relax_rows=int(relax_rows),
+                               panel=int(panel), use_gpu=int(bool(gpu)), gpu_min_flops=float(gpu_min_flops),
+                               pivot_rel=FPLUS_PIVOT_REL_DEFAULT if pivot_rel is None else float(pivot_rel))
+        self._sym = sym
+        self._num = Numeric(sym, A.data, opts)
+        self._n = n
+        self._is_complex = cplx
+        self._LU = None
+
+    def _factors(self):
+        if self._LU is None:
+            L, U, _ = self._num.factors()
+            self._LU = (L, U)
+        return self._LU
+
+    @property
+    def L(self):
+        """Unit lower-triangular factor (CSC), of diag(Dr) A[perm_r, :][:, perm_c] diag(Dc) = L U."""
+        return self._factors()[0]
+
+    @property
+    def U(self):
+        """Upper-triangular factor (CSC)."""
+        return self._factors()[1]
+
+    @property
+    def perm_r(self):
+        return self._num.p
+
+    @property
+    def perm_c(self):
+        return self._num.q
+
+    @property
+    def Dr(self):
+        return self._num.Dr
+
+    @property
+    def Dc(self):
+        return self._num.Dc
+
+    @property
+    def shape(self):
+        return (self._n, self._n)
+
+    @property
+    def nnz(self):
+        """Stored entries of L and U (explicit zeros of the front structure included)."""
+        info = self._num.info
+        return int(info["nnz_L"] + info["nnz_U"])
+
+    def solve(self, b, trans="N"):
+        """x with A x = b ('N'), A^T x = b ('T') or A^H x = b ('H'); b of shape (n,) or (n, nrhs)."""
+        if trans not in ("N", "T", "H"):
+            raise ValueError("SparseLU.solve: trans must be 'N', 'T' or 'H'")
+        tr = 0 if trans == "N" else (1 if trans == "T" or not self._is_complex else 2)
+        b = np.asarray(b)
+        if np.iscomplexobj(b) and not self._is_complex:
+            return self._num.solve(b.real, tr) + 1j * self._num.solve(b.imag, tr)
+        return self._num.solve(b, tr)

@@ -869,3 +869,17 @@ extern "C" int fplus_b200_solve_refine(const fplus_numeric *num, void *b, int64_
     }
     return rc;
 }
+
+// A symbolic object for static orders the caller chose (include/fplus_b200.h).
+extern "C" int fplus_b200_symbolic_from_orders(int64_t n, const int64_t *Ap, const int64_t *Ai, const int64_t *row_perm,
+                                               const int64_t *col_perm, fplus_symbolic **sym, char *err, size_t errlen)
+{
+    if (!sym) { errf(err, errlen, "sym is NULL"); return FPLUS_ERR_BADARG; }
+    *sym = nullptr;
+    int rc = check_compressed(n, Ap, Ai, 1, err, errlen);
+    if (rc == FPLUS_OK && (!row_perm || !col_perm)) { errf(err, errlen, "NULL permutation"); rc = FPLUS_ERR_BADARG; }
+    if (rc == FPLUS_OK) rc = check_perm(n, row_perm, "row_perm", err, errlen);
+    if (rc == FPLUS_OK) rc = check_perm(n, col_perm, "col_perm", err, errlen);
+    if (rc != FPLUS_OK) return rc;
+    return symbolic_from_orders(n, Ap, Ai, row_perm, col_perm, sym, err, errlen);
+}

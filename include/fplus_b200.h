@@ -13,6 +13,14 @@
 extern "C" {
 #endif
 
+/* A symbolic object for static orders the caller chose, for fplus_factor (whose factors stay in device memory).  FPLUS
+ * takes such orders in fplus_factor_sn_perm only, which returns host factors; this is the same analysis for the
+ * device-resident path (FPLUS's SparseLU without colamd factors in the identity order).  The trailing rows and columns
+ * of A[row_perm, :][:, col_perm] with more than max(n / 2, 10) entries become its dense lines.  Free with
+ * fplus_symbolic_free. */
+int fplus_b200_symbolic_from_orders(int64_t n, const int64_t *Ap, const int64_t *Ai, const int64_t *row_perm,
+                                    const int64_t *col_perm, fplus_symbolic **sym, char *err, size_t errlen);
+
 /* Statistics of one factorization. */
 typedef struct {
     int64_t n;

@@ -370,3 +370,20 @@ def test_solve_refine_argument_checks_on_host():
     x = np.zeros(4)
     assert L.fplus_b200_solve_refine(None, x.ctypes.data_as(ctypes.c_void_p), 1, 4, 0, 5, 0.0, None, None, err, 256) \
         == F.FPLUS_ERR_BADARG
+
+
+def test_sparse_lu_and_orders_checks_on_host():
+    """SparseLU refuses what this build does not compute (incomplete LU, rook / full pivoting) before any GPU work, and
+    fplus_b200_symbolic_from_orders refuses a non-permutation; a valid call analyses on the host only."""
+    n, Ap, Ai, Ax = CASES["convdiff2d_g20"]()
+    A = sp.csc_matrix((Ax, Ai, Ap), shape=(n, n))
+    for kw in (dict(drop_tol=1e-3), dict(pivot_strategy="rook"), dict(pivot_strategy="full"), dict(ordering="nd")):
+        with pytest.raises(ValueError):
+            F.SparseLU(A, **kw)
+    bad = np.arange(n); bad[0] = 1
+    with pytest.raises(F.FplusError) as e:
+        F.Symbolic.from_orders(n, Ap, Ai, bad, np.arange(n))
+    assert e.value.code == F.FPLUS_ERR_BADARG
+    S = F.Symbolic.from_orders(n, Ap, Ai, np.arange(n)[::-1], np.arange(n))
+    assert np.array_equal(S.row_perm, np.arange(n)[::-1]) and S.n_dense_rows == 0
+    assert S.plan()["col_front"].shape == (n,)

@@ -265,3 +265,30 @@ def test_ruiz_range_guard_matches_reference(gpu):
                       1e-2, 0, Dr.ctypes.data_as(F._dp), Dc.ctypes.data_as(F._dp), err, 256)
     assert rc == 0
     assert np.array_equal(got["Dr"], Dr) and np.array_equal(got["Dc"], Dc) and np.array_equal(got["data"], x)
+
+
+@pytest.mark.parametrize("name", ["convdiff2d_g20", "pencil_1x64", "hard_cplx_300"])
+@pytest.mark.parametrize("colamd", [True, False])
+def test_sparse_lu(gpu, name, colamd):
+    """FPLUS's SparseLU interface: with colamd (the analysis' orders) and without (the identity orders, FPLUS's default),
+    perm_r / perm_c and L, U as the oracle's with the same orders, and solves for 'N', 'T', 'H'."""
+    n, Ap, Ai, Ax = CASES[name]()
+    cplx = np.iscomplexobj(Ax)
+    A = sp.csc_matrix((Ax, Ai, Ap), shape=(n, n))
+    lu = F.SparseLU(A, colamd=colamd, pin_dense_rows=True)
+    if colamd:
+        S = F.analyze(n, Ap, Ai)
+        rp, cp = S.row_perm, S.col_perm
+    else:
+        rp = cp = np.arange(n)
+    orc = O.OracleLU(n, Ap, Ai, Ax, rp, cp)
+    assert np.array_equal(lu.perm_r, orc.p) and np.array_equal(lu.perm_c, orc.q)
+    assert _rel(lu.L, orc.L) <= FACTOR_TOL and _rel(lu.U, orc.U) <= FACTOR_TOL
+    assert lu.shape == (n, n) and lu.nnz >= lu.L.nnz
+    B = _rhs(n, 2, cplx, 6)
+    for trans in ("N", "T", "H"):
+        X = lu.solve(B, trans)
+        M = A if trans == "N" else (A.T if trans == "T" else A.conj().T)
+        be = max(np.linalg.norm(B[:, r] - M @ X[:, r]) / (sp.linalg.norm(A) * np.linalg.norm(X[:, r]) + np.linalg.norm(B[:, r]))
+                 for r in range(2))
+        assert be <= 1e-13, f"trans {trans}: backward error {be:.2e}"
