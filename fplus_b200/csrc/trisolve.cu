@@ -299,10 +299,14 @@ int tri_plan_solve(TriPlan &P, const void *Lx, const void *Ux, void *x, int64_t 
     if (n == 0 || nrhs == 0) return FPLUS_OK;
     int dev = 0;
     CKT(cudaGetDevice(&dev));
+    struct Restore {            // the caller's current device again on every return
+        int d;
+        ~Restore() { cudaSetDevice(d); }
+    } restore{dev};
     if (P.device >= 0 && P.device != dev) CKT(cudaSetDevice(P.device));
     if (!P.uploaded) {
-        P.device = dev;
-        CKT(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
+        if (P.device < 0) P.device = dev;
+        if (!P.stream) CKT(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
         int rc;
         if ((rc = upload_sweep(P.lf, err, errlen)) || (rc = upload_sweep(P.ub, err, errlen)) ||
             (rc = upload_sweep(P.utf, err, errlen)) || (rc = upload_sweep(P.ltb, err, errlen)))
@@ -324,7 +328,6 @@ int tri_plan_solve(TriPlan &P, const void *Lx, const void *Ux, void *x, int64_t 
     CKT(cudaGetLastError());
     CKT(cudaMemcpy2DAsync(x, (size_t)ldx * vs, P.d_x, (size_t)n * vs, (size_t)n * vs, (size_t)nrhs, cudaMemcpyDeviceToHost, st));
     CKT(cudaStreamSynchronize(st));
-    if (P.device != dev) CKT(cudaSetDevice(dev));
     return FPLUS_OK;
 }
 
