@@ -387,3 +387,17 @@ def test_sparse_lu_and_orders_checks_on_host():
     S = F.Symbolic.from_orders(n, Ap, Ai, np.arange(n)[::-1], np.arange(n))
     assert np.array_equal(S.row_perm, np.arange(n)[::-1]) and S.n_dense_rows == 0
     assert S.plan()["col_front"].shape == (n,)
+
+
+@pytest.mark.parametrize("name", ["pencil_1x64", "pencil_2x256", "hard_real_300", "convdiff3d_g12"])
+def test_symbolic_from_orders_matches_analysis(name):
+    """Given the analysis' own orders, the symbolic object for caller-given orders (fplus_factor_sn_perm, SparseLU without
+    colamd) finds the same dense lines and builds the same front structure, so both paths factor alike (host only)."""
+    n, Ap, Ai, Ax = CASES[name]()
+    S = F.analyze(n, Ap, Ai)
+    T = F.Symbolic.from_orders(n, Ap, Ai, S.row_perm, S.col_perm)
+    assert (T.n_dense_rows, T.n_dense_cols) == (S.n_dense_rows, S.n_dense_cols)
+    P, Q = S.plan(), T.plan()
+    for k in ("col_front", "parent", "col_ptr", "cols", "nrows", "nbord"):
+        assert np.array_equal(P[k], Q[k]), k
+    assert P["f_dense"] == Q["f_dense"]
