@@ -401,3 +401,22 @@ def test_symbolic_from_orders_matches_analysis(name):
     for k in ("col_front", "parent", "col_ptr", "cols", "nrows", "nbord"):
         assert np.array_equal(P[k], Q[k]), k
     assert P["f_dense"] == Q["f_dense"]
+
+
+def test_ruiz_and_factor_sn_sym_checks_on_host():
+    """fplus_ruiz refuses non-finite values and a row index out of range, and fplus_factor_sn_sym a matrix whose entry count
+    differs from the analysis, before any GPU work (FPLUS src/equil.c:189-192, src/pipeline.c:118-122)."""
+    n, Ap, Ai, Ax = CASES["convdiff2d_g20"]()
+    bad = Ax.copy(); bad[5] = np.nan
+    oob = Ai.copy(); oob[3] = n + 5                     # unsorted rows are accepted (FPLUS checks ranges only)
+    for data, idx in ((bad, Ai), (Ax, oob)):
+        with pytest.raises(F.FplusError) as e:
+            F.ruiz_equilibrate(data, idx, Ap, n, 20, 1e-2, False, 0, 1)
+        assert e.value.code == F.FPLUS_ERR_BADARG
+    out = F.ruiz_equilibrate(np.zeros(0), np.zeros(0, np.int64), np.zeros(1, np.int64), 0, 20, 1e-2, False)
+    assert out["Dr"].shape == (0,)
+    S = F.analyze(n, Ap, Ai)
+    Ap2 = Ap.copy(); Ap2[-1] -= 1
+    with pytest.raises(F.FplusError) as e:
+        F.factor_sn_sym(S, Ax[:-1], Ai[:-1], Ap2, False)
+    assert e.value.code == F.FPLUS_ERR_BADARG and "nonzeros" in str(e.value)
