@@ -262,20 +262,26 @@ static int solve_common(const fplus_numeric *num, void *b, int64_t nrhs, int64_t
 // worker threads leave fplus_b200_use_stream unset), so the pivot-block chains of different matrices, each on one SM,
 // overlap on the GPU, as do their bulk kernels.  The work itself is the single-matrix path: the results are those of
 // fplus_factor / fplus_solve called one by one.
+// The workers take the jobs largest first (cost[k], when given: longest processing time first), so that the large
+// matrices of an uneven batch start early and the small ones fill in around them.  The order changes no result.
 static int run_batch(int64_t count, int nworkers, const std::function<int(int64_t, char *, size_t)> &job, int *rcs, char *err,
-                     size_t errlen)
+                     size_t errlen, const std::vector<double> *cost = nullptr)
 {
     if (count < 0) { errf(err, errlen, "count must be >= 0"); return FPLUS_ERR_BADARG; }
     if (nworkers <= 0) nworkers = 8;
     if (nworkers > count) nworkers = (int)count;
+    std::vector<int64_t> order((size_t)count);
+    for (int64_t k = 0; k < count; k++) order[(size_t)k] = k;
+    if (cost) std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return (*cost)[a] > (*cost)[b]; });
     std::atomic<int64_t> next{0};
     std::vector<int> rc_local((size_t)count, FPLUS_OK);
     std::vector<std::string> msg((size_t)count);
     auto worker = [&]() {
         char e[512];
         for (;;) {
-            const int64_t k = next.fetch_add(1);
-            if (k >= count) break;
+            const int64_t t = next.fetch_add(1);
+            if (t >= count) break;
+            const int64_t k = order[(size_t)t];
             e[0] = 0;
             rc_local[(size_t)k] = job(k, e, sizeof e);
             if (rc_local[(size_t)k]) msg[(size_t)k] = e;
@@ -305,18 +311,30 @@ extern "C" int fplus_b200_factor_batch(int64_t count, const fplus_symbolic *cons
 {
     if (count > 0 && (!syms || !Ap || !Ai || !Ax || !nums)) { errf(err, errlen, "NULL array"); return FPLUS_ERR_BADARG; }
     for (int64_t k = 0; k < count; k++) nums[k] = nullptr;
+    // predicted cost: the front structure's multiply-adds when the pattern has been factored before, else n * nnz
+    std::vector<double> cost(count > 0 ? (size_t)count : 0, 0.0);
+    for (int64_t k = 0; k < count; k++) {
+        const fplus_symbolic *S = syms[k];
+        if (!S) continue;
+        std::lock_guard<std::mutex> lk(S->mu);
+        cost[(size_t)k] = S->plan ? S->plan->flops_real : (double)S->n * (double)S->nnz;
+    }
     return run_batch(count, nworkers, [&](int64_t k, char *e, size_t el) {
         return factor_common(syms[k], Ap[k], Ai[k], Ax[k], 0, is_complex, opt, &nums[k], e, el);
-    }, rcs, err, errlen);
+    }, rcs, err, errlen, &cost);
 }
 
 extern "C" int fplus_b200_solve_batch(int64_t count, fplus_numeric *const *nums, void *const *b, const int64_t *nrhs,
                                       const int64_t *ldb, int trans, int nworkers, int *rcs, char *err, size_t errlen)
 {
     if (count > 0 && (!nums || !b || !nrhs || !ldb)) { errf(err, errlen, "NULL array"); return FPLUS_ERR_BADARG; }
+    // predicted cost: the factor entries read by the sweeps, times the right-hand sides
+    std::vector<double> cost(count > 0 ? (size_t)count : 0, 0.0);
+    for (int64_t k = 0; k < count; k++)
+        if (nums[k]) cost[(size_t)k] = (double)(nums[k]->info.nnz_L + nums[k]->info.nnz_U) * (double)(nrhs[k] > 0 ? nrhs[k] : 0);
     return run_batch(count, nworkers, [&](int64_t k, char *e, size_t el) {
         return solve_common(nums[k], b[k], nrhs[k], ldb[k], trans, 0, e, el);
-    }, rcs, err, errlen);
+    }, rcs, err, errlen, &cost);
 }
 
 extern "C" int fplus_solve(const fplus_numeric *num, void *b, int64_t nrhs, int64_t ldb, int trans, char *err, size_t errlen)
