@@ -311,14 +311,19 @@ extern "C" int fplus_b200_factor_batch(int64_t count, const fplus_symbolic *cons
 {
     if (count > 0 && (!syms || !Ap || !Ai || !Ax || !nums)) { errf(err, errlen, "NULL array"); return FPLUS_ERR_BADARG; }
     for (int64_t k = 0; k < count; k++) nums[k] = nullptr;
-    // predicted cost: the front structure's multiply-adds when the pattern has been factored before, else n * nnz
-    std::vector<double> cost(count > 0 ? (size_t)count : 0, 0.0);
+    // predicted cost, in one unit for the whole batch: the front structures' multiply-adds when every pattern has been
+    // factored before, else n * nnz for every matrix
+    std::vector<double> flops(count > 0 ? (size_t)count : 0, 0.0), nz(flops.size(), 0.0);
+    bool all_planned = true;
     for (int64_t k = 0; k < count; k++) {
         const fplus_symbolic *S = syms[k];
         if (!S) continue;
         std::lock_guard<std::mutex> lk(S->mu);
-        cost[(size_t)k] = S->plan ? S->plan->flops_real : (double)S->n * (double)S->nnz;
+        nz[(size_t)k] = (double)S->n * (double)S->nnz;
+        if (S->plan) flops[(size_t)k] = S->plan->flops_real;
+        else all_planned = false;
     }
+    const std::vector<double> &cost = all_planned ? flops : nz;
     return run_batch(count, nworkers, [&](int64_t k, char *e, size_t el) {
         return factor_common(syms[k], Ap[k], Ai[k], Ax[k], 0, is_complex, opt, &nums[k], e, el);
     }, rcs, err, errlen, &cost);
@@ -555,7 +560,7 @@ extern "C" int fplus_b200_solve_dev_noalloc(const fplus_numeric *num, void *b_de
 // so that refactoring with the same orders and pattern reuses its front structure and dense-chain start).  Its device
 // factors stay alive beside the host arrays it returns, in a registry of the most recent DEV_KEEP factorizations: a
 // plan made on those very arrays (the same pointers) solves on the GPU with them, in the coordinates of the permuted
-// matrix.  A solve checks that the arrays are still the ones returned (pointers, sizes and a sample of the values);
+// matrix.  A solve checks that the arrays are still the ones returned (pointers, sizes and a digest of every byte);
 // anything else (factors from elsewhere, copies, modified values, an entry dropped from the registry) takes the
 // level-scheduled GPU sweeps over the arrays passed (trisolve.cu).  fplus_factors_free on the returned struct drops
 // the registry entry; the Python extension frees the arrays itself, so its entries go when the registry is full.
@@ -563,10 +568,67 @@ extern "C" int fplus_b200_solve_dev_noalloc(const fplus_numeric *num, void *b_de
 namespace {
 
 constexpr size_t SYM_KEEP = 4, DEV_KEEP = 4;
-constexpr int FP_SAMPLES = 32;
 
 std::mutex g_sym_mu;
 std::vector<std::shared_ptr<fplus_symbolic>> g_syms;        // most recently used last
+
+// A 128-bit digest of the factor arrays (Lp, Li, Lx, Up, Ui, Ux: every byte), so that a solve can tell whether the
+// arrays still hold what the factorization returned.  Each array is hashed in 4 MiB chunks (four interleaved
+// multiply-rotate lanes over 8-byte words, finished by a 64-bit avalanche), on up to 16 host threads for large arrays;
+// the chunk hashes are folded in order, so the digest does not depend on the thread count.
+struct Digest {
+    uint64_t a = 0, b = 0;
+    bool operator==(const Digest &o) const { return a == o.a && b == o.b; }
+};
+inline uint64_t rotl64(uint64_t x, int r) { return (x << r) | (x >> (64 - r)); }
+inline uint64_t fmix64(uint64_t k)
+{
+    k ^= k >> 33; k *= 0xff51afd7ed558ccdULL;
+    k ^= k >> 33; k *= 0xc4ceb9fe1a85ec53ULL;
+    k ^= k >> 33;
+    return k;
+}
+uint64_t hash_words(const uint64_t *w, size_t nw, uint64_t seed)
+{
+    const uint64_t K1 = 0x87c37b91114253d5ULL, K2 = 0x4cf5ad432745937fULL;
+    uint64_t h[4] = {seed, seed ^ K1, seed ^ K2, seed ^ (K1 + K2)};
+    size_t i = 0;
+    for (; i + 4 <= nw; i += 4)
+        for (int l = 0; l < 4; l++) h[l] = rotl64(h[l] + w[i + l] * K1, 31) * K2;
+    for (; i < nw; i++) h[0] = rotl64(h[0] + w[i] * K1, 31) * K2;
+    return fmix64(h[0] ^ rotl64(h[1], 17) ^ rotl64(h[2], 29) ^ rotl64(h[3], 43) ^ (uint64_t)nw);
+}
+void digest_bytes(const void *p, size_t bytes, Digest &d)
+{
+    const size_t nw = bytes / 8, CH = (size_t)1 << 19;       // 4 MiB chunks of 8-byte words (sizes are multiples of 8)
+    const size_t nch = (nw + CH - 1) / CH;
+    std::vector<uint64_t> hc(nch, 0);
+    const uint64_t *w = (const uint64_t *)p;
+    auto run = [&](size_t c0, size_t c1) {
+        for (size_t c = c0; c < c1; c++) hc[c] = hash_words(w + c * CH, std::min(CH, nw - c * CH), 0x9e3779b97f4a7c15ULL + c);
+    };
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t nt = std::min<size_t>(std::min<size_t>(hw ? hw : 1, 16), nch >= 8 ? nch / 4 : 1);
+    if (nt <= 1) run(0, nch);
+    else {
+        std::vector<std::thread> th;
+        const size_t per = (nch + nt - 1) / nt;
+        try {
+            for (size_t t = 0; t < nt; t++) th.emplace_back(run, std::min(nch, t * per), std::min(nch, (t + 1) * per));
+        } catch (...) {
+            for (auto &x : th) x.join();
+            th.clear();
+            run(0, nch);
+        }
+        for (auto &x : th) x.join();
+    }
+    for (size_t c = 0; c < nch; c++) {
+        d.a = fmix64(d.a ^ hc[c]) + (uint64_t)c;
+        d.b = rotl64(d.b, 23) ^ fmix64(hc[c] + d.b * 0x9e3779b97f4a7c15ULL);
+    }
+    d.a = fmix64(d.a ^ (uint64_t)bytes);
+    d.b = fmix64(d.b + (uint64_t)bytes);
+}
 
 struct DevFactors {
     fplus_numeric *num = nullptr;
@@ -574,24 +636,24 @@ struct DevFactors {
     int is_complex = 0;
     const int64_t *Lp = nullptr, *Li = nullptr, *Up = nullptr, *Ui = nullptr;
     const void *Lx = nullptr, *Ux = nullptr;
-    std::vector<unsigned char> fp;                           // sampled values of Lx and Ux
+    Digest fp;                                               // digest of the six arrays as returned
     ~DevFactors() { fplus_numeric_free(num); }
 };
 std::mutex g_dev_mu;
 std::vector<std::shared_ptr<DevFactors>> g_dev;             // most recent last
 
-void fingerprint(int64_t nnzL, const void *Lx, int64_t nnzU, const void *Ux, size_t vs, std::vector<unsigned char> &out)
+Digest fingerprint(int64_t n, const int64_t *Lp, const int64_t *Li, const void *Lx, const int64_t *Up, const int64_t *Ui,
+                   const void *Ux, size_t vs)
 {
-    out.clear();
-    for (int part = 0; part < 2; part++) {
-        const int64_t m = part ? nnzU : nnzL;
-        const unsigned char *x = (const unsigned char *)(part ? Ux : Lx);
-        if (m <= 0) continue;
-        for (int k = 0; k < FP_SAMPLES; k++) {
-            const int64_t q = (int64_t)(((__int128)k * (m - 1)) / (FP_SAMPLES - 1));
-            out.insert(out.end(), x + (size_t)q * vs, x + (size_t)(q + 1) * vs);
-        }
-    }
+    Digest d;
+    const int64_t nnzL = Lp[n], nnzU = Up[n];
+    digest_bytes(Lp, (size_t)(n + 1) * 8, d);
+    digest_bytes(Li, (size_t)nnzL * 8, d);
+    digest_bytes(Lx, (size_t)nnzL * vs, d);
+    digest_bytes(Up, (size_t)(n + 1) * 8, d);
+    digest_bytes(Ui, (size_t)nnzU * 8, d);
+    digest_bytes(Ux, (size_t)nnzU * vs, d);
+    return d;
 }
 
 // the cached symbolic object for these orders and this pattern, or a new one
@@ -652,7 +714,7 @@ int low_factor(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, 
     d->num = num; d->n = n; d->is_complex = is_complex;
     d->nnzL = out->Lp[n]; d->nnzU = out->Up[n];
     d->Lp = out->Lp; d->Li = out->Li; d->Up = out->Up; d->Ui = out->Ui; d->Lx = out->Lx; d->Ux = out->Ux;
-    fingerprint(d->nnzL, d->Lx, d->nnzU, d->Ux, is_complex ? 16 : 8, d->fp);
+    d->fp = fingerprint(n, d->Lp, d->Li, d->Lx, d->Up, d->Ui, d->Ux, is_complex ? 16 : 8);
     std::shared_ptr<DevFactors> dropped;
     {
         std::lock_guard<std::mutex> lk(g_dev_mu);
@@ -767,6 +829,7 @@ extern "C" int fplus_tri_solve_plan(const fplus_solve_plan *pl, int64_t n, const
         Up[n] != pl->nnzU)
         return FPLUS_ERR_BADARG;
     const size_t vs = is_complex ? 16 : 8;
+    if (n > 0 && !Ux) return FPLUS_ERR_BADARG;
     for (int64_t j = 0; j < n; j++) {      // a zero or missing pivot fails before x is touched
         const int64_t q = pl->udiag[j];
         if (q < 0) return FPLUS_ERR_SINGULAR;
@@ -778,9 +841,7 @@ extern "C" int fplus_tri_solve_plan(const fplus_solve_plan *pl, int64_t n, const
     char err[256] = {0};
     const DevFactors *d = pl->dev.get();
     if (d && d->Lp == Lp && d->Li == Li && d->Up == Up && d->Ui == Ui && d->Lx == Lx && d->Ux == Ux && d->is_complex == is_complex) {
-        std::vector<unsigned char> fp;
-        fingerprint(d->nnzL, Lx, d->nnzU, Ux, vs, fp);
-        if (fp == d->fp) return solve_common(d->num, x, nrhs, ldx, trans, 0, err, sizeof(err), 1);
+        if (fingerprint(n, Lp, Li, Lx, Up, Ui, Ux, vs) == d->fp) return solve_common(d->num, x, nrhs, ldx, trans, 0, err, sizeof(err), 1);
     }
     fplus_solve_plan *mp = const_cast<fplus_solve_plan *>(pl);      // the sweeps are built once, under the plan's lock
     TriPlan *g = nullptr;

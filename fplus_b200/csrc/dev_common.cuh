@@ -45,6 +45,60 @@ __device__ __forceinline__ cplx divv(cplx a, cplx b)
     return cplx{(a.x * r + a.y) / d, (a.y * r - a.x) / d};
 }
 
+// ---------------------------------------------------------------------------------------------------------------------
+// Pivot keys.  Partial pivoting picks the largest modulus (FPLUS src/factor_sn_panel.inc:225-231 compares fabs / cabs).
+// The key of a value is an unsigned integer that orders values as their moduli do, with no overflow or underflow:
+//   real     the bits of |x| (non-negative doubles order as their bit patterns); exact
+//   complex  |x|^2 = m * 2^E (m in [1, 2)) packed as (E + 1023 + PIVKEY_OFF) << 50 | the top 50 fraction bits of m.
+//            Where |x|^2 is a normal double in [2^-1000, 2^1000] that is the double's own bits shifted right by two
+//            (plus the offset); elsewhere the components are first scaled by a power of two (exact), so both routes
+//            give the same key.  E ranges over [-2148, 2048], so the packed exponent fits 13 bits.
+// Zero and NaN have key 0; an infinite modulus the largest key.
+constexpr unsigned long long PIVKEY_OFF = 1200ull;
+constexpr unsigned long long PIVKEY_INF = 8191ull << 50;
+
+__device__ __forceinline__ unsigned long long pivkey(double a)
+{
+    const double m = fabs(a);
+    return m == m ? (unsigned long long)__double_as_longlong(m) : 0ull;
+}
+static __device__ __noinline__ unsigned long long pivkey_wide(double re, double im)
+{
+    const double ax = fabs(re), ay = fabs(im);
+    if (!(ax == ax) || !(ay == ay)) return 0ull;
+    const double s = fmax(ax, ay);
+    if (s == 0.0) return 0ull;
+    if (isinf(s)) return PIVKEY_INF;
+    int e = 0, f = 0;
+    frexp(s, &e);                                                  // s = (0.5 .. 1) * 2^e
+    const double xs = ldexp(ax, -e), ys = ldexp(ay, -e);           // exact (a component far below the other may round)
+    const double q = __dadd_rn(__dmul_rn(xs, xs), __dmul_rn(ys, ys));   // |x|^2 * 2^(-2e), in [0.25, 2)
+    const double m = frexp(q, &f);                                 // q = m * 2^f, m in [0.5, 1)
+    const long long E = (long long)f + 2LL * e - 1;                // |x|^2 = (2m) * 2^E
+    const unsigned long long frac = (unsigned long long)__double_as_longlong(2.0 * m) & ((1ull << 52) - 1);
+    return ((unsigned long long)(E + 1023 + (long long)PIVKEY_OFF) << 50) | (frac >> 2);
+}
+__device__ __forceinline__ unsigned long long pivkey(cplx a)
+{
+    const double q = __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y));
+    if (q >= 0x1p-1000 && q <= 0x1p1000) return ((unsigned long long)__double_as_longlong(q) >> 2) + (PIVKEY_OFF << 50);
+    return pivkey_wide(a.x, a.y);
+}
+// the key of a value of modulus t >= 0
+template <typename T> __device__ __forceinline__ unsigned long long pivkey_of_modulus(double t);
+template <> __device__ __forceinline__ unsigned long long pivkey_of_modulus<double>(double t) { return pivkey(t); }
+template <> __device__ __forceinline__ unsigned long long pivkey_of_modulus<cplx>(double t) { return pivkey(cplx{t, 0.0}); }
+
+// the largest 64-bit key over the warp: two 32-bit reductions (the high word, then the low word among the lanes that hold
+// the high word)
+__device__ __forceinline__ unsigned long long warp_max_key(unsigned long long key)
+{
+    const unsigned khi = (unsigned)(key >> 32);
+    const unsigned hi = __reduce_max_sync(0xffffffffu, khi);
+    const unsigned lo = __reduce_max_sync(0xffffffffu, khi == hi ? (unsigned)key : 0u);
+    return ((unsigned long long)hi << 32) | lo;
+}
+
 // device status word: the first failure wins (code, then the smallest step / index)
 enum : int {
     ST_OK = 0,

@@ -515,39 +515,13 @@ __device__ __forceinline__ cplx recip(cplx p)
     return cplx{a * d * is, -b * d * is};
 }
 
-// The pivot of column j among the rows not pivoted before step j (tag >= j), by one warp: each lane's best (largest
-// squared modulus, ties to the smaller row of B) over its rows, the warp's maximum by shuffles, then the winning lane by
-// ballot (exact ties between lanes resolved by the smaller row of B).  Returns the local row, -1 when none.
-template <typename T>
-__device__ __forceinline__ int warp_argmax(const T *__restrict__ col, const int *__restrict__ tag, const int64_t *__restrict__ rid,
-                                           int nrows, int j, int lane)
-{
-    double bv = -1.0; int bi = -1; int64_t br = INT64_MAX;
-    for (int i = lane; i < nrows; i += 32) {
-        if (tag[i] < j) continue;
-        const double a = sqmod(col[i]);
-        const int64_t r = rid[i];
-        if (a > bv || (a == bv && r < br)) { bv = a; bi = i; br = r; }
-    }
-    double m = bv;
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    unsigned cand = __ballot_sync(0xffffffffu, bi >= 0 && bv == m);
-    if (cand == 0) return -1;
-    if ((cand & (cand - 1)) != 0) {            // an exact tie between lanes: the smallest row of B among them
-        int64_t rr = (cand >> lane) & 1u ? br : INT64_MAX;
-        for (int o = 16; o > 0; o >>= 1) { int64_t t = __shfl_xor_sync(0xffffffffu, rr, o); rr = t < rr ? t : rr; }
-        cand = __ballot_sync(0xffffffffu, ((cand >> lane) & 1u) && br == rr);
-    }
-    return __shfl_sync(0xffffffffu, bi, __ffs(cand) - 1);
-}
-
 // Partial-pivot LU of a front's pivot block in shared memory, with a pivot warp and one-column look-ahead (one CTA of
 // up to 1024 threads).  Warp 0 owns the critical path: at step j it updates column j + 1 for every row with the step-j
-// multipliers and, in the same pass, finds the pivot of column j + 1 (largest squared modulus, ties to the smaller row
-// of B), then publishes the row and 1 / pivot (double-buffered slots).  The other warps update columns j + 2 .. with the
-// step-j pivot meanwhile, keep the multipliers (double-buffered) and store those of step j - 1 into column j - 1 (no
-// longer read by anyone).  One barrier per step.  No row swaps: the pivot row of step j is tagged j.  The singular test
-// uses the column thresholds staged in shared memory (squared moduli; the modulus itself near the threshold).
+// multipliers and, in the same pass, finds the pivot of column j + 1 (the largest pivot key, i.e. modulus, ties to the
+// smaller row of B), then publishes the row and 1 / pivot (double-buffered slots).  The other warps update columns
+// j + 2 .. with the step-j pivot meanwhile, keep the multipliers (double-buffered) and store those of step j - 1 into
+// column j - 1 (no longer read by anyone).  One barrier per step.  No row swaps: the pivot row of step j is tagged j.
+// The singular test uses the column thresholds staged in shared memory (keys; the modulus itself near the threshold).
 // a named barrier for `count` threads (a multiple of 32); the non-aligned form, so that a warp need not be converged
 __device__ __forceinline__ void named_bar(int id, int count) { asm volatile("barrier.sync %0, %1;" ::"r"(id), "r"(count) : "memory"); }
 
@@ -631,25 +605,32 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
     const int G = nu >= R ? nu / R : 1, rstep = nu >= R ? R : nu;
     const int my_i = ut >= 0 ? (nu >= R ? ut % R : ut) : 0, my_g = ut >= 0 ? (nu >= R ? ut / R : 0) : G;
     const bool upd = ut >= 0 && my_g < G;
-    // warp 0: decide on the winner (bi, squared modulus bv2) of column j, publish into slot
-    auto decide = [&](int j, int bi, double bv2, int slot) {
+    // The singular test of the reference (FPLUS src/factor_sn_panel.inc:232-233): no candidate, a zero modulus, or a
+    // modulus below t = pivot_rel * max |B(:, column)|.  A key at or above the key of 2t is clear of the threshold; below
+    // it the modulus itself is compared.
+    auto singular = [&](int bi, unsigned long long key, double t, T pv) -> bool {
+        if (bi < 0 || key == 0ull) return true;
+        return key < pivkey_of_modulus<T>(2.0 * t) && vabs(pv) < t;
+    };
+    // warp 0: decide on the winner (bi, pivot key) of column j, publish into slot
+    auto decide = [&](int j, int bi, unsigned long long key, int slot) {
         if (lane != 0) return;
         const double t = thr[j];
         int stop = 0;
-        bool sing = bi < 0 || !(bv2 > 0.0);
-        if (!sing && bv2 < 4.0 * t * t) sing = vabs(A[(size_t)j * nrows + bi]) < t;      // near the threshold: the modulus
-        if (sing) { const double bv = bi >= 0 ? vabs(A[(size_t)j * nrows + bi]) : 0.0; set_status(st, ST_SINGULAR, fcol + j, bv, t); stop = 1; }
-        else if (bi >= nri) { set_status(st, ST_BORDER, front, sqrt(bv2), t); stop = 1; }
+        const T pv = bi >= 0 ? A[(size_t)j * nrows + bi] : VT<T>::zero();
+        if (singular(bi, key, t, pv)) { set_status(st, ST_SINGULAR, fcol + j, bi >= 0 ? vabs(pv) : 0.0, t); stop = 1; }
+        else if (bi >= nri) { set_status(st, ST_BORDER, front, vabs(pv), t); stop = 1; }
         s_bi[slot] = bi;
         s_stv[slot] = stop;
-        if (!stop) { s_inv[slot] = recip(A[(size_t)j * nrows + bi]); tag[bi] = j; }
+        if (!stop) { s_inv[slot] = recip(pv); tag[bi] = j; }
         else s_stop = 1;
     };
-    auto reduce = [&](double bv, int bi, int64_t br, double *bv2_out) -> int {
-        double m = bv;
-        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-        unsigned cand = __ballot_sync(0xffffffffu, bi >= 0 && bv == m);
-        *bv2_out = m;
+    // the warp's winner: the largest key, ties to the smaller row of B
+    auto reduce = [&](unsigned long long bk, int bi, int64_t br, unsigned long long *key_out) -> int {
+        const unsigned long long key = bi >= 0 ? bk : 0ull;
+        const unsigned long long m = warp_max_key(key);
+        unsigned cand = __ballot_sync(0xffffffffu, bi >= 0 && key == m);
+        *key_out = m;
         if (cand == 0) return -1;
         if ((cand & (cand - 1)) != 0) {
             int64_t rr = (cand >> lane) & 1u ? br : INT64_MAX;
@@ -673,24 +654,19 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
         }
         // the warp's winner among the live slots; every lane also forms 1 / its own candidate while the reduction runs,
         // and the winner's reciprocal comes back with its value
-        auto pick = [&](const T *xv, double *m, T *pv, T *pinv) -> int {
-            double bv = -1.0; int wi = -1; int64_t br = INT64_MAX; T bx = VT<T>::zero();
+        auto pick = [&](const T *xv, unsigned long long *m, T *pv, T *pinv) -> int {
+            long long bk = -1; int wi = -1; int64_t br = INT64_MAX; T bx = VT<T>::zero();
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 if (!al[q]) continue;
-                const double a = sqmod(xv[q]);
-                if (a > bv || (a == bv && rr[q] < br)) { bv = a; wi = lane + 32 * q; br = rr[q]; bx = xv[q]; }
+                const long long a = (long long)pivkey(xv[q]);       // keys are below 2^63
+                if (a > bk || (a == bk && rr[q] < br)) { bk = a; wi = lane + 32 * q; br = rr[q]; bx = xv[q]; }
             }
-            const T binv = wi >= 0 && bv > 0.0 ? recip(bx) : VT<T>::zero();
-            // the maximum: non-negative doubles order as their bit patterns, so two 32-bit warp reductions (high word,
-            // then the low word among the lanes that hold the high word)
-            const unsigned long long key = wi >= 0 ? (unsigned long long)__double_as_longlong(bv) : 0ull;
-            const unsigned khi = (unsigned)(key >> 32);
-            const unsigned hi = __reduce_max_sync(0xffffffffu, khi);
-            const unsigned lo = __reduce_max_sync(0xffffffffu, khi == hi ? (unsigned)key : 0u);
-            const unsigned long long mk = ((unsigned long long)hi << 32) | lo;
+            const T binv = wi >= 0 && bk > 0 ? recip(bx) : VT<T>::zero();
+            const unsigned long long key = wi >= 0 ? (unsigned long long)bk : 0ull;
+            const unsigned long long mk = warp_max_key(key);
             unsigned cand = __ballot_sync(0xffffffffu, wi >= 0 && key == mk);
-            *m = cand ? __longlong_as_double((long long)mk) : -1.0;
+            *m = mk;
             if (cand == 0) { *pv = VT<T>::zero(); *pinv = VT<T>::zero(); return -1; }
             if ((cand & (cand - 1)) != 0) {
                 int64_t r2 = (cand >> lane) & 1u ? br : INT64_MAX;
@@ -703,21 +679,19 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
             return __shfl_sync(0xffffffffu, wi, wl);
         };
         // lane 0 decides with the winner's value pv and its reciprocal pinv (held by every lane)
-        auto decide_v = [&](int j, int bi, double bv2, int slot, T pv, T pinv) -> T {
+        auto decide_v = [&](int j, int bi, unsigned long long key, int slot, T pv, T pinv) -> T {
             if (lane == 0) {
                 const double t = thr[j];
                 int stop = 0;
-                bool sing = bi < 0 || !(bv2 > 0.0);
-                if (!sing && bv2 < 4.0 * t * t) sing = vabs(pv) < t;      // near the threshold: the modulus
-                if (sing) { set_status(st, ST_SINGULAR, fcol + j, bi >= 0 ? vabs(pv) : 0.0, t); stop = 1; }
-                else if (bi >= nri) { set_status(st, ST_BORDER, front, sqrt(bv2), t); stop = 1; }
+                if (singular(bi, key, t, pv)) { set_status(st, ST_SINGULAR, fcol + j, bi >= 0 ? vabs(pv) : 0.0, t); stop = 1; }
+                else if (bi >= nri) { set_status(st, ST_BORDER, front, vabs(pv), t); stop = 1; }
                 s_bi[slot] = bi;
                 s_stv[slot] = stop;
                 if (!stop) { s_inv[slot] = pinv; tag[bi] = j; }
             }
             return pinv;
         };
-        double m;
+        unsigned long long m;
         T pv, pinv;
         int bi = pick(xc, &m, &pv, &pinv);
         T inv = decide_v(0, bi, m, 0, pv, pinv);
@@ -748,14 +722,14 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
         }
     } else if (warp == 0) {
         {
-            double bv = -1.0; int bi = -1; int64_t br = INT64_MAX;
+            long long bk = -1; int bi = -1; int64_t br = INT64_MAX;
             for (int i = lane; i < nrows; i += 32) {
-                const double a = sqmod(A[i]);
+                const long long a = (long long)pivkey(A[i]);
                 const int64_t r = rid[i];
-                if (a > bv || (a == bv && r < br)) { bv = a; bi = i; br = r; }
+                if (a > bk || (a == bk && r < br)) { bk = a; bi = i; br = r; }
             }
-            double m;
-            const int w = reduce(bv, bi, br, &m);
+            unsigned long long m;
+            const int w = reduce((unsigned long long)bk, bi, br, &m);
             decide(0, w, m, 0);
             __syncwarp();
         }
@@ -770,7 +744,7 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
                 const T pr = A[(size_t)(j + 1) * nrows + bi];
                 const T *cj = A + (size_t)j * nrows;
                 T *cn = A + (size_t)(j + 1) * nrows;
-                double bv = -1.0; int wi = -1; int64_t br = INT64_MAX;
+                long long bk = -1; int wi = -1; int64_t br = INT64_MAX;
                 for (int i0 = lane; i0 < nrows; i0 += 128) {
                     T xa[4], xb[4];
                     bool ok[4];
@@ -791,14 +765,14 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
                         const int i = i0 + 32 * q;
                         if (ok[q]) {
                             cn[i] = xb[q];
-                            const double a = sqmod(xb[q]);
+                            const long long a = (long long)pivkey(xb[q]);
                             const int64_t r = rid[i];
-                            if (a > bv || (a == bv && r < br)) { bv = a; wi = i; br = r; }
+                            if (a > bk || (a == bk && r < br)) { bk = a; wi = i; br = r; }
                         }
                     }
                 }
-                double m;
-                const int w = reduce(bv, wi, br, &m);
+                unsigned long long m;
+                const int w = reduce((unsigned long long)bk, wi, br, &m);
                 decide(j + 1, w, m, (j + 1) & 1);
                 __syncwarp();
             }

@@ -765,9 +765,11 @@ int dev_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, void *x_dev, int6
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
-// The allocation-free solve (fplus_b200_solve_dev_noalloc).  The same kernels and launch order as run_solve, in place on
-// the caller's right-hand sides (leading dimension ldx), with the scratch vectors carved from one file-scope device array
-// instead of allocations.  Host code cannot use g_noalloc_scratch's name as a device address (it is a host-side stand-in):
+// The allocation-free solve (fplus_b200_solve_dev_noalloc), in place on the caller's right-hand sides (leading dimension
+// ldx), with the scratch vectors carved from one file-scope device array instead of allocations.  It runs the unfused
+// sweep kernels (k_fwdL / k_fwdL2, k_u12_gemv + k_bwdU, k_fwdUt2, k_ut_scatter, k_bwdLt), whose scratch is two vectors
+// and the U12 partial sums, not run_solve's fused and chain kernels; its results agree with run_solve's to rounding
+// (the sums run in another order), not bit for bit, and it is slower on the dense chain.  Host code cannot use g_noalloc_scratch's name as a device address (it is a host-side stand-in):
 // the address comes from cudaGetSymbolAddress, once per device, with that device current.  The array keeps the last
 // call's contents; every scratch vector is written before it is read, so nothing needs clearing.  Calls share the array:
 // calls that overlap on the GPU (other streams, other host threads) race.

@@ -204,10 +204,12 @@ void tri_plan_build(TriPlan &P, int64_t n, const int64_t *Lp, const int64_t *Li,
 
 #define CKT(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { errf(err, errlen, "CUDA: %s", cudaGetErrorString(e_)); return FPLUS_ERR_GPU; } } while (0)
 
+// (a buffer left from an earlier, failed upload is freed first, so a retry does not leak it)
 template <typename I>
 static int upload(I **d, const std::vector<I> &h, char *err, size_t errlen)
 {
     const size_t b = std::max<size_t>(h.size(), 1) * sizeof(I);
+    if (*d) { cudaFree(*d); *d = nullptr; }
     CKT(cudaMalloc((void **)d, b));
     if (!h.empty()) CKT(cudaMemcpy(*d, h.data(), h.size() * sizeof(I), cudaMemcpyHostToDevice));
     return FPLUS_OK;

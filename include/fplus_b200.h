@@ -89,7 +89,8 @@ int fplus_b200_solve_batch(int64_t count, fplus_numeric *const *nums, void *cons
  * message giving the size needed.  The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress): make that first call before any stream capture.  The array is shared by every call on the
  * device and keeps the last call's contents (every scratch value is written before it is read); calls that overlap on
- * the GPU (from other streams or host threads) race on it: serialize them. */
+ * the GPU (from other streams or host threads) race on it: serialize them.  It runs the unfused sweep kernels, whose
+ * scratch is smallest, so its solutions agree with fplus_b200_solve_dev's to rounding, not bit for bit. */
 int fplus_b200_solve_dev_noalloc(const fplus_numeric *num, void *b_dev, int64_t nrhs, int64_t ldb, int trans, char *err, size_t errlen);
 
 /* fplus_solve with iterative refinement in FP64.  No counterpart in FPLUS: the refinement driver of the precision form.

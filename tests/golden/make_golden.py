@@ -91,7 +91,7 @@ def panel_cases(src):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FPLUS_REFERENCE", "/root/reference")
     if not O.have_reference():
         raise SystemExit("oracle/_ref/libfplusref.so is missing: make -C oracle ref")
     for name, rec in panel_cases(src).items():
