@@ -16,9 +16,13 @@ per step with the solution at backward error <= 1e-14 (checked after the timed s
   of the values and the right-hand side and the device-to-host copy of the solution are inside the timed region.
 * roofline -- the dominant kernel class of the factorization, from a separate step with the library's per-class CUDA
   event timing on: achieved algorithmic rate / measured peak.
-* cpu_baseline / --impl reference -- the reference's own CPU build (oracle/_ref/libfplusref.so: the FPLUS sources,
-  OpenMP + OpenBLAS, all host cores) on a bounded sample of the same generator (fewer Fourier modes), scaled to the full
-  workload by n^3 (its relaxed supernodes make this factorization dense; the sample and the factor are reported).
+* cpu_baseline -- the reference's own CPU build (oracle/_ref/libfplusref.so: the FPLUS sources, OpenMP + OpenBLAS, all
+  host threads) timed on a bounded sample of the same generator (1 Fourier mode, n = 4096), reported as measured.
+* c1_pair -- the 100 x 100 stencil (the reference's CPU-runnable configuration) in full on both sides: this library's
+  device and end-to-end times, the reference at all host threads and at 1 thread.
+* --impl reference -- the reference's CPU build on this arm's configuration, with the static orders of
+  tests/golden/orders.npz (libfplus.so is not loaded).  The stencil runs in full; for the pencil the arm prints the
+  unavailable line with the reference's measured times on the same generator at 1 and 2 Fourier modes.
 
 Multi-GPU: one factorization does not shard; N ranks run N independent replicas ("replicas only"); the line reports
 the slowest rank's ms per step divided by N (the job's ms per factorization) with scaling "weak".
@@ -58,16 +62,42 @@ def workload(name, modes=8):
     return n, Ap, Ai, Ax, b, desc
 
 
-def sample_workload(name):
-    """The bounded CPU-baseline sample: the same generator, fewer Fourier modes (or the full matrix when small)."""
+def load_orders(name, Ap, Ai):
+    """The committed static orders of a workload (tests/golden/orders.npz, written by tests/golden/make_orders.py from
+    this library's analysis): the reference's arm injects them into the reference's own fplus_analyze without loading
+    libfplus.so.  (row_perm, col_perm, dense-row mask, dense-column mask)."""
+    z = np.load(os.path.join(ROOT, "tests", "golden", "orders.npz"))
+    chk = np.array([int(Ap[-1]), int(np.sum(Ap, dtype=np.int64)), int(np.sum(Ai * (np.arange(Ai.size) % 7 + 1), dtype=np.int64))])
+    if not np.array_equal(chk, z[name + "__pattern"]):
+        raise SystemExit(f"orders.npz: the pattern of {name} has changed (rerun tests/golden/make_orders.py)")
+    return z[name + "__row_perm"], z[name + "__col_perm"], z[name + "__trow"], z[name + "__tcol"]
+
+
+def reference_time(name, gen, reps):
+    """The reference's CPU build (oracle/_ref/libfplusref.so: the FPLUS sources, OpenMP + OpenBLAS) on one workload,
+    factor + solve per step (its analysis done once, outside the timing, on the committed orders): (median ms, berr,
+    n).  Threads: OMP_NUM_THREADS / OPENBLAS_NUM_THREADS as set by the caller, else all host cores."""
+    import oracle as O
     from fplus_b200 import workloads as W
-    if name == "pencil":
-        modes = int(os.environ.get("FPLUS_BENCH_REF_MODES", "1"))
-        n, Ap, Ai, Ax = W.pencil(modes=modes)
-        return n, Ap, Ai, Ax, (f"pencil generator with {modes} Fourier mode(s) (n={n}), median of 3; ms scaled by "
-                               f"(32768/{n})^3 -- an underestimate: the reference took 43x longer at 2 modes than at 1")
-    n, Ap, Ai, Ax = W.convdiff2d(100, 1)
-    return n, Ap, Ai, Ax, "the full workload"
+    n, Ap, Ai, Ax = gen()
+    rp, cp, trow, tcol = load_orders(name, Ap, Ai)
+    b = W.rhs(n, 1, np.iscomplexobj(Ax), 2)[0]
+    R = O.RefLU(n, Ap, Ai, None, cp, trow, tcol, postorder=0)        # the injected order, no postorder: cp as given
+    assert np.array_equal(R.row_perm, rp) and np.array_equal(R.col_perm, cp)
+    times, be = [], None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        R.refactor(Ax)
+        x = R.solve(b)
+        times.append((time.perf_counter() - t0) * 1e3)
+        be = O.backward_error(n, Ap, Ai, Ax, x, b)
+    del R
+    return float(np.median(times)), be, n
+
+
+def ref_threads():
+    t = os.environ.get("OMP_NUM_THREADS")
+    return int(t) if t and t.isdigit() else os.cpu_count()
 
 
 # ------------------------------------------------------------------------------------------------------------- clocks
@@ -160,32 +190,6 @@ def allreduce_max(value: float, device) -> float:
 
 
 # ------------------------------------------------------------------------------------------------------------- arms
-def reference_sample(workload_name, reps=1):
-    """The reference CPU build on the bounded sample: (ms per factor+solve, berr, description, threads)."""
-    import oracle as O
-    n, Ap, Ai, Ax, desc = sample_workload(workload_name)
-    import fplus_b200 as F
-    S = F.analyze(n, Ap, Ai)                       # the same static orders for both libraries
-    from fplus_b200 import workloads as W
-    b = W.rhs(n, 1, np.iscomplexobj(Ax), 2)[0]
-    trow = np.zeros(n, np.uint8); trow[S.row_perm[n - S.n_dense_rows:]] = 1
-    tcol = np.zeros(n, np.uint8); tcol[S.col_perm[n - S.n_dense_cols:]] = 1
-    # the reference's analysis with the same fill-reducing order and no postorder: col_perm as given
-    times = []
-    be = None
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        R = O.RefLU(n, Ap, Ai, Ax, S.col_perm, trow, tcol, postorder=0)
-        x = R.solve(b)
-        times.append((time.perf_counter() - t0) * 1e3)
-        be = O.backward_error(n, Ap, Ai, Ax, x, b)
-        assert np.array_equal(R.col_perm, S.col_perm) and np.array_equal(R.row_perm, S.row_perm)
-        del R
-    scale = (32768.0 / n) ** 3 if workload_name == "pencil" else 1.0
-    threads = os.cpu_count()
-    return float(np.median(times)) * scale, float(np.median(times)), be, desc, threads, scale
-
-
 def run_profile_once(args):
     """One factor + solve inside a profiler range (after a warm factorization that caches the plan), then the per-class
     algorithmic flops and bytes of that factorization (the library's own counts) as one JSON line."""
@@ -210,19 +214,15 @@ def run_profile_once(args):
 
 
 def traffic_ratio(kernel_class):
-    """DRAM bytes per algorithmic byte of a kernel class's launches, from the committed ncu summary of that kernel
-    (profiles/*.md, the line 'dram_to_algorithmic_bytes: R'), or (None, reason)."""
-    name = {"front_lu": "k_front_lu2_pencil_n4096.md", "schur_gemm": "k_front_tail_pencil_n16384.md"}.get(kernel_class)
-    if name is None:
-        return None, "no ncu summary for this class"
-    path = os.path.join(ROOT, "profiles", name)
+    """DRAM bytes per algorithmic byte of a kernel class's launches, from profiles/traffic.json (the ratio measured by an
+    ncu capture of that kernel; the capture's summary is named there), or (None, reason)."""
     try:
-        for line in open(path):
-            if line.startswith("dram_to_algorithmic_bytes:"):
-                return float(line.split(":", 1)[1]), f"profiles/{name} (ncu dram__bytes_read.sum + dram__bytes_write.sum)"
-    except OSError:
-        pass
-    return None, f"profiles/{name} absent"
+        t = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["classes"].get(kernel_class)
+    except (OSError, ValueError, KeyError):
+        return None, "profiles/traffic.json absent"
+    if not t:
+        return None, "no ncu capture of this class"
+    return float(t["dram_to_algorithmic_bytes"]), f"{t['summary']} (ncu dram__bytes_read.sum + dram__bytes_write.sum)"
 
 
 def run_shift_batch(S, n, modes, count, b):
@@ -280,28 +280,117 @@ def run_pencil_batch(count, nworkers=16):
 
 
 def run_reference_arm(args, rank, world):
+    """The reference's own CPU implementation on this arm's configuration (rank 0 only).  The 100 x 100 stencil runs in
+    full.  The benchmark pencil (n = 32,768) does not finish within this arm's few-minute bound on the host cores: the arm
+    times the reference on the same generator with 1 and 2 Fourier modes and prints the unavailable line with those
+    measured times as the reason (no extrapolation)."""
     if rank != 0:
         return
     if not __import__("oracle").have_reference():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfplusref.so was not built (the reference "
                                                                 "sources were absent at build time)"}))
         return
-    for _ in range(args.warmup and 1):
-        reference_sample(args.workload)
-    ms_list = []
-    for _ in range(args.steps):
-        ms_full, ms_sample, be, desc, threads, scale = reference_sample(args.workload)
-        ms_list.append(ms_full)
+    from fplus_b200 import workloads as W
+    threads = ref_threads()
+    if args.workload == "pencil":
+        t1, be1, n1 = reference_time("pencil_m1", lambda: W.pencil(modes=1), 1)
+        t2, be2, n2 = reference_time("pencil_m2", lambda: W.pencil(modes=2), 1)
+        print(json.dumps({"impl": "reference", "unavailable": (
+            f"the reference's CPU factor+solve of the benchmark pencil (8 Fourier modes, n=32768) does not finish within "
+            f"this arm's few-minute bound: measured here on {threads} host threads, the same generator took {t1:.0f} ms at "
+            f"1 mode (n={n1}, berr {be1:.1e}) and {t2:.0f} ms at 2 modes (n={n2}, berr {be2:.1e}), {t2 / t1:.0f}x for 2x n"),
+            "samples": {"pencil_m1": {"n": n1, "ms": t1, "berr": be1}, "pencil_m2": {"n": n2, "ms": t2, "berr": be2},
+                        "threads": threads}}))
+        return
+    gen = lambda: W.convdiff2d(100, 1)
+    for _ in range(max(args.warmup, 0)):
+        reference_time("convdiff2d_g100", gen, 1)
+    ms, be, n = reference_time("convdiff2d_g100", gen, max(args.steps, 1))
     d = workload(args.workload, args.modes)[5]
-    ms = float(np.mean(ms_list))
     line = {"impl": "reference", "metric": "factor+solve ms (berr<=1e-14)", "value": ms, "unit": "ms", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c128" if args.workload == "pencil" else "f64", "data": "synthetic",
-            "config": d,
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": d,
             "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
-                             "sample": f"{desc}; measured {ms_sample:.1f} ms per sample step; berr {be:.2e}"},
+                             "sample": f"the full workload, median of {max(args.steps, 1)} factor+solve steps; berr {be:.2e}"},
             "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def reference_subprocess(workload_name, steps, threads=None):
+    """bench.py --impl reference in a child process (so OMP_NUM_THREADS applies from the start); its JSON line."""
+    env = dict(os.environ)
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        env.pop(k, None)
+    if threads:
+        env["OMP_NUM_THREADS"] = env["OPENBLAS_NUM_THREADS"] = str(threads)
+    out = subprocess.run([sys.executable, os.path.abspath(__file__), "--impl", "reference", "--workload", workload_name,
+                          "--steps", str(steps), "--warmup", "1"], env=env, capture_output=True, text=True, timeout=900)
+    for line in out.stdout.splitlines()[::-1]:
+        if line.startswith("{"):
+            return json.loads(line)
+    return {"unavailable": (out.stderr or "no output")[-300:]}
+
+
+def run_c1_pair(stream, dev, steps=10, warmup=3):
+    """The 100 x 100 stencil (n = 10,000, the reference's CPU-runnable configuration) in full on both sides: this
+    library's device and end-to-end times and the reference's CPU build at all host cores and at 1 thread, each its
+    median over `steps` factor+solve steps, the analysis done once beforehand on both sides (the same orders)."""
+    import torch
+    import fplus_b200 as F
+    import oracle as O
+    from fplus_b200 import workloads as W
+    n, Ap, Ai, Ax = W.convdiff2d(100, 1)
+    b = W.rhs(n, 1, False, 2)[0]
+    S = F.analyze(n, Ap, Ai)
+    rp, cp, _, _ = load_orders("convdiff2d_g100", Ap, Ai)
+    same_orders = bool(np.array_equal(S.row_perm, rp) and np.array_equal(S.col_perm, cp))
+    Ad = torch.from_numpy(Ax).to(dev)
+    bd0 = torch.from_numpy(b).to(dev)
+    Ah = torch.from_numpy(Ax).pin_memory().numpy()
+    bh = torch.from_numpy(b).pin_memory()
+
+    def dev_step():
+        bd = bd0.clone()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        N = S.factor(Ad, device=True)
+        N.solve_device(bd, 0)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), bd
+
+    def e2e_step():
+        xb = bh.clone().numpy()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        N = S.factor(Ah)
+        err = ctypes.create_string_buffer(512)
+        rc = F.lib().fplus_solve(N._h, xb.ctypes.data_as(ctypes.c_void_p), 1, n, 0, err, 512)
+        assert rc == 0, err.value
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), xb
+    for _ in range(warmup):
+        dev_step(); e2e_step()
+    td, te = [], []
+    for _ in range(steps):
+        ms, bd = dev_step(); td.append(ms)
+        ms, xe = e2e_step(); te.append(ms)
+    berr = O.backward_error(n, Ap, Ai, Ax, bd.cpu().numpy(), b)
+    berr_e2e = O.backward_error(n, Ap, Ai, Ax, xe, b)
+    ref_all = reference_subprocess("convdiff2d", 5)
+    ref_one = reference_subprocess("convdiff2d", 5, threads=1)
+    out = {"workload": "2D convection-diffusion 5-point, 100x100 grid (n=10000, 49600 entries), float64, nrhs 1",
+           "same_orders": same_orders, "gpu_ms": float(np.median(td)), "gpu_e2e_ms": float(np.median(te)),
+           "berr": berr, "berr_e2e": berr_e2e, "steps": steps,
+           "reference_ms_all_threads": ref_all.get("value"), "reference_threads": ref_all.get("cpu_baseline", {}).get("cores"),
+           "reference_ms_1_thread": ref_one.get("value"),
+           "reference_berr": ref_all.get("cpu_baseline", {}).get("sample")}
+    best = [v for v in (ref_all.get("value"), ref_one.get("value")) if v]
+    if best:
+        out["reference_ms_best"] = min(best)
+        out["e2e_speedup_vs_reference_best"] = min(best) / out["gpu_e2e_ms"]
+    return out
 
 
 def run_b200_arm(args, rank, world):
@@ -446,15 +535,26 @@ def run_b200_arm(args, rank, world):
     batch_pencils = None
     if args.batch_pencils > 0 and world == 1:
         batch_pencils = run_pencil_batch(args.batch_pencils)
+    c1_pair = None
+    if world == 1 and not args.no_cpu_baseline and __import__("oracle").have_reference():
+        c1_pair = run_c1_pair(stream, dev)
 
     if rank != 0:
         return
     clocks = clk.summary()
     cpu = None
     if __import__("oracle").have_reference() and world == 1 and not args.no_cpu_baseline:
-        ms_full, ms_sample, be_ref, sdesc, threads, scale = reference_sample(args.workload, reps=3)
-        cpu = {"value": ms_full, "unit": "ms", "cores": threads, "kind": "reference",
-               "sample": f"{sdesc}; measured {ms_sample:.1f} ms per factor+solve; berr {be_ref:.2e}"}
+        if args.workload == "pencil":
+            ms_s, be_ref, n_s = reference_time("pencil_m1", lambda: W.pencil(modes=1), 3)
+            cpu = {"value": ms_s, "unit": "ms", "cores": ref_threads(), "kind": "reference", "scaled": False,
+                   "sample": (f"the same pencil generator with 1 Fourier mode (n={n_s}) instead of 8 (n={n}): the "
+                              f"reference's factor+solve, median of 3, berr {be_ref:.2e}; measured, not scaled to n={n} "
+                              "(the full size does not finish within minutes; c1_pair compares both in full on the "
+                              "CPU-runnable configuration)")}
+        else:
+            ms_s, be_ref, n_s = reference_time("convdiff2d_g100", lambda: W.convdiff2d(100, 1), 5)
+            cpu = {"value": ms_s, "unit": "ms", "cores": ref_threads(), "kind": "reference", "scaled": False,
+                   "sample": f"the full workload, median of 5 factor+solve steps, berr {be_ref:.2e}"}
     line = {"metric": "factor+solve ms (berr<=1e-14)", "value": ms_dev / world, "unit": "ms", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_dev, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128" if cplx else "f64", "data": "synthetic",
@@ -467,7 +567,7 @@ def run_b200_arm(args, rank, world):
                     "d2h_bytes_per_step": n * vsz},
             "gpu_launches": int(launches),
             "clocks": clocks, "roofline": roof, "cpu_baseline": cpu, "solve_nrhs16": solve16, "batch": batch,
-            "batch_pencils": batch_pencils}
+            "batch_pencils": batch_pencils, "c1_pair": c1_pair}
     print(json.dumps(line))
 
 

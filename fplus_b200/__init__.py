@@ -61,7 +61,7 @@ FPLUS_B200_H_SYMBOLS = [
     "fplus_b200_numeric_info", "fplus_b200_use_stream", "fplus_b200_factor_dev", "fplus_b200_solve_dev",
     "fplus_b200_interior_order", "fplus_b200_plan_size", "fplus_b200_plan_export", "fplus_b200_launch_count",
     "fplus_b200_profile", "fplus_b200_profile_read", "fplus_b200_solve_dev_noalloc", "fplus_b200_factor_batch",
-    "fplus_b200_solve_batch", "fplus_b200_solve_refine", "fplus_b200_symbolic_from_orders",
+    "fplus_b200_solve_batch", "fplus_b200_solve_refine", "fplus_b200_symbolic_from_orders", "fplus_b200_factor_norms",
 ]
 
 _lib = None
@@ -123,6 +123,7 @@ def lib():
     L.fplus_factors_free.argtypes = [ctypes.POINTER(Factors)]
     L.fplus_b200_symbolic_from_orders.argtypes = [ctypes.c_int64, _i64p, _i64p, _i64p, _i64p, ctypes.POINTER(ctypes.c_void_p),
                                                   ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_b200_factor_norms.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_solve_refine.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_double, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
                                           ctypes.c_size_t]
@@ -306,6 +307,13 @@ class Numeric:
         nrhs = 1 if B.dim() == 1 else B.shape[0]
         _check(lib().fplus_b200_solve_dev(self._h, ctypes.c_void_p(B.data_ptr()), nrhs, self.n, trans, err, 512), err)
         return B
+
+    def factor_norms(self):
+        """fplus_b200_factor_norms: (||L||_F, ||U||_F) computed on the GPU from the device factors."""
+        lf, uf = ctypes.c_double(), ctypes.c_double()
+        err = ctypes.create_string_buffer(512)
+        _check(lib().fplus_b200_factor_norms(self._h, ctypes.byref(lf), ctypes.byref(uf), err, 512), err)
+        return lf.value, uf.value
 
     @property
     def info(self):

@@ -470,6 +470,19 @@ extern "C" int fplus_b200_numeric_info(const fplus_numeric *num, fplus_b200_info
     return FPLUS_OK;
 }
 
+extern "C" int fplus_b200_factor_norms(const fplus_numeric *num, double *L_fro, double *U_fro, char *err, size_t errlen)
+{
+    if (!num || !L_fro || !U_fro) { errf(err, errlen, "NULL argument"); return FPLUS_ERR_BADARG; }
+    std::lock_guard<std::mutex> lk(num->mu);
+    DevNum &N = *num->dev;
+    CKH(cudaSetDevice(N.device));
+    cudaStream_t saved = N.stream;
+    if (tl_stream) N.stream = tl_stream;
+    const int rc = dev_factor_norms(*num->plan, N, L_fro, U_fro, err, errlen);
+    N.stream = saved;
+    return rc;
+}
+
 // ---- host-only views of the multifrontal structure (tests)
 static int plan_for(const fplus_symbolic *sym, int64_t tail, FrontPlan &P)
 {

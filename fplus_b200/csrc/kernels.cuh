@@ -1907,4 +1907,48 @@ __global__ void k_axpy1(T *__restrict__ x, const T *__restrict__ d, int64_t m, i
         x[e] = undo ? sub(x[e], d[e]) : add(x[e], d[e]);
 }
 
+// ---------------------------------------------------------------------------------------------------------------------
+// Frobenius norms of the factors straight from the arenas, in two passes so that no square overflows or underflows:
+// PASS 0 the largest modulus of each factor (integer maxima of the bits), PASS 1 the sum of (|x| / max)^2.  In a front's
+// nrows x npiv block of the L arena (rows in the final order) an entry below the diagonal (row > column) belongs to L,
+// one on or above it to U (U11); every entry of the U arena belongs to U (U12).  L's unit diagonal is added on the host.
+// acc: [0] bits of max |L| (starts at 1.0: the unit diagonal), [1] bits of max |U|, [2] sum for L, [3] sum for U.
+// fr: (L_off, nrows, npiv) per front; one CTA per front.
+template <typename T, int PASS>
+__global__ void k_lblock_norm(const T *__restrict__ La, const int64_t *__restrict__ fr, unsigned long long *acc)
+{
+    const int64_t off = fr[3 * blockIdx.x], nr = fr[3 * blockIdx.x + 1], np = fr[3 * blockIdx.x + 2];
+    const double sl = PASS ? 1.0 / bitsd(acc[0]) : 0.0;
+    const double mu = PASS ? bitsd(acc[1]) : 0.0, su = PASS ? (mu > 0.0 ? 1.0 / mu : 1.0) : 0.0;
+    double a0 = 0.0, a1 = 0.0;
+    for (int64_t e = threadIdx.x; e < nr * np; e += blockDim.x) {
+        const int64_t i = e % nr, c = e / nr;
+        const double v = vabs(La[off + e]);
+        if (i > c) { if (PASS) { const double t = v * sl; a0 += t * t; } else a0 = fmax(a0, v); }
+        else if (i < np) { if (PASS) { const double t = v * su; a1 += t * t; } else a1 = fmax(a1, v); }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double b0 = __shfl_xor_sync(0xffffffffu, a0, o), b1 = __shfl_xor_sync(0xffffffffu, a1, o);
+        a0 = PASS ? a0 + b0 : fmax(a0, b0);
+        a1 = PASS ? a1 + b1 : fmax(a1, b1);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (PASS) { atomicAdd((double *)&acc[2], a0); atomicAdd((double *)&acc[3], a1); }
+        else { atomicMax(&acc[0], dbits(a0)); atomicMax(&acc[1], dbits(a1)); }
+    }
+}
+
+template <typename T, int PASS>
+__global__ void k_flat_norm(const T *__restrict__ U, int64_t m, unsigned long long *acc)
+{
+    const double mu = PASS ? bitsd(acc[1]) : 0.0, su = PASS ? (mu > 0.0 ? 1.0 / mu : 1.0) : 0.0;
+    double a = 0.0;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x) {
+        const double v = vabs(U[e]);
+        if (PASS) { const double t = v * su; a += t * t; } else a = fmax(a, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) { const double b = __shfl_xor_sync(0xffffffffu, a, o); a = PASS ? a + b : fmax(a, b); }
+    if ((threadIdx.x & 31) == 0) { if (PASS) atomicAdd((double *)&acc[3], a); else atomicMax(&acc[1], dbits(a)); }
+}
+
 }  // namespace fpl

@@ -145,7 +145,7 @@ DevNum::~DevNum()
                     (void *)cbstack, (void *)work, (void *)rowid, (void *)p_lu, (void *)pinv, (void *)ipiv, (void *)perm,
                     (void *)st, (void *)scratch, (void *)rbuf, (void *)sbuf, (void *)xbuf, (void *)part, (void *)work2,
                     (void *)perm2, (void *)rr_p, (void *)rr_l, (void *)rr_s, (void *)ir_b, (void *)ir_x, (void *)ir_r,
-                    (void *)ir_d, (void *)ir_bits})
+                    (void *)ir_d, (void *)ir_bits, scratch_norm})
         if (p) cudaFreeAsync(p, stream);
     if (stream) cudaStreamSynchronize(stream);
     if (crit) cudaStreamSynchronize(crit);
@@ -896,6 +896,42 @@ int dev_solve_noalloc(const FrontPlan &P, const DevPlan &D, DevNum &N, void *b_d
                     : run_solve_noalloc_group<double>(P, D, N, (double *)bb, ldb, m, trans, s, err, errlen);
     }
     return rc;
+}
+
+// ||L||_F and ||U||_F of the device factors (the unit diagonal of L included)
+template <typename T>
+static int run_factor_norms(const FrontPlan &P, DevNum &N, double *lfro, double *ufro, char *err, size_t errlen)
+{
+    cudaStream_t s = N.stream;
+    const int64_t nf = (int64_t)P.fronts.size();
+    std::vector<int64_t> fr((size_t)std::max<int64_t>(nf, 1) * 3, 0);
+    for (int64_t k = 0; k < nf; k++) {
+        fr[3 * k] = P.fronts[k].L_off; fr[3 * k + 1] = P.fronts[k].nrows; fr[3 * k + 2] = P.fronts[k].npiv;
+    }
+    int rc;
+    if ((rc = ensure_async(N, &N.scratch_norm, &N.cap_norm, fr.size() * 8 + 64, err, errlen))) return rc;
+    unsigned long long *acc = (unsigned long long *)N.scratch_norm;
+    int64_t *dfr = (int64_t *)((char *)N.scratch_norm + 64);
+    const unsigned long long init[4] = {0x3ff0000000000000ull, 0ull, 0ull, 0ull};    // 1.0, 0, 0.0, 0.0
+    CK(cudaMemcpyAsync(acc, init, sizeof init, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(dfr, fr.data(), fr.size() * 8, cudaMemcpyHostToDevice, s));
+    const T *La = (const T *)N.Larena, *Ua = (const T *)N.Uarena;
+    if (nf > 0) k_lblock_norm<T, 0><<<(unsigned)nf, 256, 0, s>>>(La, dfr, acc), note_launch();
+    if (P.U_size > 0) k_flat_norm<T, 0><<<nblk(P.U_size), 256, 0, s>>>(Ua, P.U_size, acc), note_launch();
+    if (nf > 0) k_lblock_norm<T, 1><<<(unsigned)nf, 256, 0, s>>>(La, dfr, acc), note_launch();
+    if (P.U_size > 0) k_flat_norm<T, 1><<<nblk(P.U_size), 256, 0, s>>>(Ua, P.U_size, acc), note_launch();
+    unsigned long long h[4];
+    CK(cudaMemcpyAsync(h, acc, sizeof h, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const double ml = bitsd_h(h[0]), mu = bitsd_h(h[1]), sl = bitsd_h(h[2]), su = bitsd_h(h[3]);
+    *lfro = ml * std::sqrt(sl + (double)N.n / (ml * ml));
+    *ufro = mu * std::sqrt(su);
+    return FPLUS_OK;
+}
+
+int dev_factor_norms(const FrontPlan &P, DevNum &N, double *lfro, double *ufro, char *err, size_t errlen)
+{
+    return N.cplx ? run_factor_norms<cplx>(P, N, lfro, ufro, err, errlen) : run_factor_norms<double>(P, N, lfro, ufro, err, errlen);
 }
 
 int dev_status(DevNum &N, int *code, int64_t *idx, char *err, size_t errlen)

@@ -61,6 +61,8 @@ struct DevNum {
     cudaEvent_t ev_lu = nullptr, ev_head = nullptr;
     DevStatus *st = nullptr;
     void *scratch = nullptr;
+    void *scratch_norm = nullptr;
+    size_t cap_norm = 0;
     void *rbuf = nullptr, *sbuf = nullptr, *xbuf = nullptr, *part = nullptr;
     size_t cap_r = 0, cap_s = 0, cap_x = 0, cap_part = 0;
     int ruiz_iters = 0;
@@ -97,6 +99,8 @@ int dev_solve_refine(const FrontPlan &P, const DevPlan &D, DevNum &N, void *b, i
 int dev_solve_noalloc(const FrontPlan &P, const DevPlan &D, DevNum &N, void *b_dev, int64_t ldb, int64_t nrhs, int trans,
                       cudaStream_t s, char *err, size_t errlen);
 int dev_clear_status(DevNum &N, char *err, size_t errlen);
+// ||L||_F and ||U||_F of the device factors (L with its unit diagonal), from the arenas
+int dev_factor_norms(const FrontPlan &P, DevNum &N, double *lfro, double *ufro, char *err, size_t errlen);
 int dev_check_finite(DevNum &N, char *err, size_t errlen);
 int dev_ensure_x(DevNum &N, size_t bytes, char *err, size_t errlen);
 int ensure_async(DevNum &N, void **p, size_t *cap, size_t bytes, char *err, size_t errlen);

@@ -76,6 +76,11 @@ int fplus_b200_factor_batch(int64_t count, const fplus_symbolic *const *syms, co
 int fplus_b200_solve_batch(int64_t count, fplus_numeric *const *nums, void *const *b, const int64_t *nrhs, const int64_t *ldb,
                            int trans, int nworkers, int *rcs, char *err, size_t errlen);
 
+/* The Frobenius norms of the factors, L (unit diagonal included) and U, computed on the GPU from the device factors
+ * (the sums are scaled by each factor's largest modulus, so they neither overflow nor underflow).  No counterpart in
+ * FPLUS; it lets a caller check factors too large to read back to the host (for instance against a stored oracle). */
+int fplus_b200_factor_norms(const fplus_numeric *num, double *L_fro, double *U_fro, char *err, size_t errlen);
+
 /* fplus_b200_solve_dev for callers that cannot allocate device memory.  No counterpart in the reference (FPLUS has no GPU
  * solve).  Some callers may not call cudaMalloc at solve time: code running inside another runtime that owns the device
  * memory (a framework's custom operator given only its input and output buffers), latency-critical loops in which an

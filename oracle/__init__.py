@@ -95,6 +95,18 @@ class OracleLU:
             x = x.view(np.complex128)
         return sp.csc_matrix((x, i, p), shape=(n, n))
 
+    def _fro(self, fp, fx):
+        L = restatement()
+        nnz = int(np.ctypeslib.as_array(getattr(L, fp)(self._h), (self.n + 1,))[-1])
+        raw = np.ctypeslib.as_array(ctypes.cast(getattr(L, fx)(self._h), _dp), (max(nnz, 1) * (2 if self.cplx else 1),))
+        v = raw[: nnz * (2 if self.cplx else 1)]
+        m = float(np.abs(v).max()) if v.size else 0.0
+        return m * float(np.linalg.norm(v / m)) if m > 0 else 0.0        # scaled: the squares neither overflow nor underflow
+
+    def fro_norms(self):
+        """(||L||_F, ||U||_F) straight from the factor arrays (no copies: for factors too large to convert)."""
+        return self._fro("orc_Lp", "orc_Lx"), self._fro("orc_Up", "orc_Ux")
+
     @property
     def L(self):
         return self._csc("orc_Lp", "orc_Li", "orc_Lx")
@@ -241,6 +253,22 @@ class RefLU:
             self.rc, self.err = rc, err.value.decode(errors="replace")
             if rc != 0:
                 raise RuntimeError(f"reference factor failed ({rc}): {self.err}")
+
+    def refactor(self, Ax):
+        """fplus_factor of new values on this analysis (the previous factorization is freed first)."""
+        L = reference()
+        if self._num.value:
+            L.fplus_numeric_free(self._num)
+            self._num = ctypes.c_void_p()
+        Ap, Ai = self._keep[0], self._keep[1]
+        self.cplx = np.iscomplexobj(Ax)
+        Ax = np.ascontiguousarray(Ax)
+        self._keep[2] = Ax
+        err = ctypes.create_string_buffer(512)
+        rc = L.fplus_factor(self._sym, Ap.ctypes.data_as(_i64p), Ai.ctypes.data_as(_i64p), Ax.ctypes.data_as(ctypes.c_void_p),
+                            int(self.cplx), ctypes.byref(self.opt), ctypes.byref(self._num), err, 512)
+        if rc != 0:
+            raise RuntimeError(f"reference factor failed ({rc}): {err.value}")
 
     def __del__(self):
         L = _ref

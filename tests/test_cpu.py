@@ -420,3 +420,45 @@ def test_ruiz_and_factor_sn_sym_checks_on_host():
     with pytest.raises(F.FplusError) as e:
         F.factor_sn_sym(S, Ax[:-1], Ai[:-1], Ap2, False)
     assert e.value.code == F.FPLUS_ERR_BADARG and "nonzeros" in str(e.value)
+
+
+# ------------------------------------------------------------------------------------ fixtures the GPU tests rely on
+@pytest.mark.parametrize("name", ["pencil_m1", "pencil_m8", "convdiff2d_g100"])
+def test_committed_orders_are_the_analysis(name):
+    """tests/golden/orders.npz (the static orders the benchmark's reference arm injects) equals this build's analysis."""
+    gens = {"pencil_m1": lambda: W.pencil(modes=1), "pencil_m8": lambda: W.pencil(), "convdiff2d_g100": lambda: W.convdiff2d(100, 1)}
+    z = np.load(os.path.join(GOLD, "orders.npz"))
+    n, Ap, Ai, _ = gens[name]()
+    S = F.analyze(n, Ap, Ai)
+    tr, tc = _masks(n, S)
+    assert np.array_equal(S.row_perm, z[name + "__row_perm"]) and np.array_equal(S.col_perm, z[name + "__col_perm"])
+    assert np.array_equal(tr, z[name + "__trow"]) and np.array_equal(tc, z[name + "__tcol"])
+
+
+@pytest.mark.parametrize("name", ["pencil_n32768", "convdiff3d_g32"])
+def test_big_fixtures_orders_and_generator(name):
+    """The full-size fixtures of the GPU tests: the generator still makes the stored matrix and the analysis still gives
+    the stored orders (the oracle's outputs in them were computed on those orders)."""
+    z = np.load(os.path.join(GOLD, name + ".npz"))
+    n, Ap, Ai, Ax = W.pencil() if name.startswith("pencil") else W.convdiff3d(32, 3)
+    a = np.asarray(Ax)
+    cs = np.array([a.real.sum(), (a.imag.sum() if np.iscomplexobj(a) else 0.0), np.abs(a).max(), float(a.size)])
+    assert np.allclose(cs, z["checksum"], rtol=1e-13, atol=0)
+    S = F.analyze(n, Ap, Ai)
+    assert np.array_equal(S.row_perm, z["row_perm"]) and np.array_equal(S.col_perm, z["col_perm"])
+    assert z["berr"] <= 1e-14
+
+
+@needs_ref
+@pytest.mark.parametrize("scale", [1e-170, 1e160])
+def test_oracle_matches_reference_at_extreme_magnitudes(scale):
+    """Without equilibration, values whose squared moduli underflow or overflow: the oracle picks the reference's pivots
+    (both compare cabs), which pins the GPU test of the same matrices."""
+    from tests.cases import hard_matrix
+    n, Ap, Ai, Ax = hard_matrix(300, True, 0.0, 13)
+    Ax = Ax * scale
+    S = F.analyze(n, Ap, Ai, equilibrate=0)
+    tr, tc = _masks(n, S)
+    R = O.RefLU(n, Ap, Ai, Ax, S.col_perm, tr, tc, postorder=0, equilibrate=0)
+    orc = O.OracleLU(n, Ap, Ai, Ax, S.row_perm, S.col_perm, equilibrate=0)
+    assert np.array_equal(R.p, orc.p)
