@@ -17,6 +17,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfplus.so")
 
 FPLUS_OK, FPLUS_ERR_NOMEM, FPLUS_ERR_SINGULAR, FPLUS_ERR_BADARG, FPLUS_ERR_GPU, FPLUS_ERR_INTERNAL = 0, -1, -2, -3, -4, -5
+# the precision form's Schur-update arithmetic (fplus_b200_factor_prec)
+PREC_FP64, PREC_FP32, PREC_BF16X3, PREC_TF32 = 0, 1, 2, 3
 FPLUS_PIVOT_FULL, FPLUS_PIVOT_PARTIAL, FPLUS_PIVOT_ROOK = 0, 1, 2
 FPLUS_PIVOT_REL_DEFAULT = 1.4901161193847656e-08
 
@@ -45,7 +47,8 @@ class Info(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int64), ("nfronts", ctypes.c_int64), ("f_dense", ctypes.c_int64), ("attempts", ctypes.c_int),
                 ("ruiz_iters", ctypes.c_int), ("nnz_L", ctypes.c_int64), ("nnz_U", ctypes.c_int64),
                 ("front_flops", ctypes.c_double), ("ms_equil", ctypes.c_double), ("ms_fronts", ctypes.c_double),
-                ("device_bytes", ctypes.c_int64)]
+                ("device_bytes", ctypes.c_int64), ("precision", ctypes.c_int), ("reserved", ctypes.c_int),
+                ("tc_updates", ctypes.c_int64), ("tc_flops", ctypes.c_double)]
 
 
 # every entry point of include/fplus.h and include/fplus_b200.h (the tests check that each is exported)
@@ -62,6 +65,7 @@ FPLUS_B200_H_SYMBOLS = [
     "fplus_b200_interior_order", "fplus_b200_plan_size", "fplus_b200_plan_export", "fplus_b200_launch_count",
     "fplus_b200_profile", "fplus_b200_profile_read", "fplus_b200_solve_dev_noalloc", "fplus_b200_factor_batch",
     "fplus_b200_solve_batch", "fplus_b200_solve_refine", "fplus_b200_symbolic_from_orders", "fplus_b200_factor_norms",
+    "fplus_b200_factor_prec", "fplus_b200_schur_update",
 ]
 
 _lib = None
@@ -94,6 +98,9 @@ def lib():
     L.fplus_factor.argtypes = [ctypes.c_void_p, _i64p, _i64p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Options),
                                ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_factor_dev.argtypes = L.fplus_factor.argtypes
+    L.fplus_b200_factor_prec.argtypes = [ctypes.c_void_p, _i64p, _i64p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Options),
+                                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p,
+                                         ctypes.c_size_t]
     L.fplus_solve.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_char_p,
                               ctypes.c_size_t]
     L.fplus_b200_solve_dev.argtypes = L.fplus_solve.argtypes
@@ -123,6 +130,10 @@ def lib():
     L.fplus_factors_free.argtypes = [ctypes.POINTER(Factors)]
     L.fplus_b200_symbolic_from_orders.argtypes = [ctypes.c_int64, _i64p, _i64p, _i64p, _i64p, ctypes.POINTER(ctypes.c_void_p),
                                                   ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_b200_schur_update.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                          ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                          ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                          ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_factor_norms.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_solve_refine.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_double, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
@@ -238,14 +249,15 @@ class Symbolic:
         out["f_dense"] = fd.value
         return out
 
-    def factor(self, Ax, options=None, device=False):
-        return Numeric(self, Ax, options, device)
+    def factor(self, Ax, options=None, device=False, precision=0):
+        """fplus_factor (precision 0), or the precision form (PREC_FP32, PREC_BF16X3, PREC_TF32: fplus_b200_factor_prec)."""
+        return Numeric(self, Ax, options, device, precision)
 
 
 class Numeric:
     """fplus_factor: diag(Dr) A[p,:][:,q] diag(Dc) = L U, the factors in device memory."""
 
-    def __init__(self, sym: Symbolic, Ax, options=None, device=False):
+    def __init__(self, sym: Symbolic, Ax, options=None, device=False, precision=0):
         self.sym = sym
         self._h = ctypes.c_void_p()
         opts = options if options is not None else sym.options
@@ -253,14 +265,20 @@ class Numeric:
         if device:      # a torch CUDA tensor (float64, or complex128 viewed as float64 pairs)
             self.is_complex = bool(Ax.is_complex())
             ptr = ctypes.c_void_p(Ax.data_ptr())
-            rc = lib().fplus_b200_factor_dev(sym._h, _p64(sym.Ap), _p64(sym.Ai), ptr, int(self.is_complex), ctypes.byref(opts),
-                                             ctypes.byref(self._h), err, 512)
         else:
             Ax = np.ascontiguousarray(Ax)
             self.is_complex = np.iscomplexobj(Ax)
             Ax = Ax.astype(np.complex128 if self.is_complex else np.float64, copy=False)
-            rc = lib().fplus_factor(sym._h, _p64(sym.Ap), _p64(sym.Ai), Ax.ctypes.data_as(ctypes.c_void_p), int(self.is_complex),
-                                    ctypes.byref(opts), ctypes.byref(self._h), err, 512)
+            ptr = Ax.ctypes.data_as(ctypes.c_void_p)
+        if precision:
+            rc = lib().fplus_b200_factor_prec(sym._h, _p64(sym.Ap), _p64(sym.Ai), ptr, int(self.is_complex), ctypes.byref(opts),
+                                              int(precision), int(bool(device)), ctypes.byref(self._h), err, 512)
+        elif device:
+            rc = lib().fplus_b200_factor_dev(sym._h, _p64(sym.Ap), _p64(sym.Ai), ptr, int(self.is_complex), ctypes.byref(opts),
+                                             ctypes.byref(self._h), err, 512)
+        else:
+            rc = lib().fplus_factor(sym._h, _p64(sym.Ap), _p64(sym.Ai), ptr, int(self.is_complex), ctypes.byref(opts),
+                                    ctypes.byref(self._h), err, 512)
         _check(rc, err)
         self.n = sym.n
 

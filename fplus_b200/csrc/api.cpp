@@ -14,6 +14,7 @@
 #include <memory>
 #include <vector>
 #include "trisolve.hpp"
+#include "schur_tc.hpp"
 
 using namespace fpl;
 
@@ -65,10 +66,12 @@ static int get_plan(const fplus_symbolic *sym, int64_t tail, std::shared_ptr<Fro
 }
 
 static int factor_common(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax, int ax_on_device,
-                         int is_complex, const fplus_options *opt, fplus_numeric **out, char *err, size_t errlen)
+                         int is_complex, const fplus_options *opt, fplus_numeric **out, char *err, size_t errlen,
+                         int prec = FPLUS_B200_PREC_FP64)
 {
     if (!out) { errf(err, errlen, "num is NULL"); return FPLUS_ERR_BADARG; }
     *out = nullptr;
+    if (prec < FPLUS_B200_PREC_FP64 || prec > FPLUS_B200_PREC_TF32) { errf(err, errlen, "unknown precision %d", prec); return FPLUS_ERR_BADARG; }
     if (!sym) { errf(err, errlen, "sym is NULL"); return FPLUS_ERR_BADARG; }
     fplus_options d;
     if (!opt) { fplus_default_options(&d); opt = &d; }
@@ -123,6 +126,7 @@ static int factor_common(const fplus_symbolic *sym, const int64_t *Ap, const int
         num->dev.reset(new DevNum);
         DevNum &N = *num->dev;
         if (tl_stream) N.stream = tl_stream;
+        N.prec = prec;
         rc = dev_num_init(N, n, sym->nnz, num->is_complex, err, errlen);
         if (rc) return rc;
         const size_t bytes = (size_t)sym->nnz * (size_t)N.vs;
@@ -186,7 +190,10 @@ static int factor_common(const fplus_symbolic *sym, const int64_t *Ap, const int
         }
         I.nnz_L = nl; I.nnz_U = nu;
         I.front_flops = 2.0 * P->flops_real * (is_complex ? 4.0 : 1.0);
-        I.device_bytes = (int64_t)(N.cap_L + N.cap_U + N.cap_cb + N.cap_work + 2 * bytes);
+        I.device_bytes = (int64_t)(N.cap_L + N.cap_U + N.cap_cb + N.cap_work + N.cap_work2 + N.cap_tcws + 2 * bytes);
+        I.precision = prec;
+        I.tc_updates = N.tc_updates;
+        I.tc_flops = N.tc_flops;
     } catch (const std::bad_alloc &) {
         errf(err, errlen, "out of memory");
         return FPLUS_ERR_NOMEM;
@@ -214,6 +221,50 @@ extern "C" int fplus_b200_factor_dev(const fplus_symbolic *sym, const int64_t *A
                                      int is_complex, const fplus_options *opt, fplus_numeric **num, char *err, size_t errlen)
 {
     return factor_common(sym, Ap, Ai, Ax_dev, 1, is_complex, opt, num, err, errlen);
+}
+
+extern "C" int fplus_b200_factor_prec(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax,
+                                      int is_complex, const fplus_options *opt, int precision, int ax_on_device,
+                                      fplus_numeric **num, char *err, size_t errlen)
+{
+    return factor_common(sym, Ap, Ai, Ax, ax_on_device ? 1 : 0, is_complex, opt, num, err, errlen, precision);
+}
+
+extern "C" int fplus_b200_schur_update(int precision, int is_complex, int64_t M, int64_t N, int64_t K, const void *A, int64_t lda,
+                                       const void *B, int64_t ldb, const void *Cin, int64_t ldci, const int *rmap, void *Cout,
+                                       int64_t ldco, void *stream, char *err, size_t errlen)
+{
+    if (precision < FPLUS_B200_PREC_FP32 || precision > FPLUS_B200_PREC_TF32) { errf(err, errlen, "precision must be FP32, BF16X3 or TF32"); return FPLUS_ERR_BADARG; }
+    if (!A || !B || !Cin || !Cout || lda < M || ldb < K || ldci < 1 || ldco < M || !schur_tc_supported(M, N, K, is_complex ? 1 : 0)) {
+        errf(err, errlen, "fplus_b200_schur_update: bad arguments or a shape below one 128 x 256 tile");
+        return FPLUS_ERR_BADARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t wsb = schur_tc_workspace(precision, M, N, K, is_complex ? 1 : 0);
+    void *ws = nullptr;
+    unsigned *derr = nullptr;
+    CKH(cudaMallocAsync(&ws, wsb, s));
+    cudaError_t e = cudaMallocAsync((void **)&derr, sizeof(unsigned), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(derr, 0, sizeof(unsigned), s);
+    int rc = FPLUS_OK;
+    if (e != cudaSuccess) { errf(err, errlen, "CUDA: %s", cudaGetErrorString(e)); rc = FPLUS_ERR_GPU; }
+    else {
+        const int trc = schur_tc(precision, is_complex ? 1 : 0, M, N, K, (const double *)A, lda, (const double *)B, ldb,
+                                 (const double *)Cin, ldci, rmap, (double *)Cout, ldco, ws, wsb, derr, s);
+        unsigned herr = 0;
+        if (trc != 0) { errf(err, errlen, "fplus_b200_schur_update: launch failed (%d)", trc); rc = FPLUS_ERR_GPU; }
+        else {
+            add_launches(3);
+            e = cudaMemcpyAsync(&herr, derr, sizeof herr, cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) { errf(err, errlen, "CUDA: %s", cudaGetErrorString(e)); rc = FPLUS_ERR_GPU; }
+            else if (herr) { errf(err, errlen, "fplus_b200_schur_update: a wait timed out (status %u)", herr); rc = FPLUS_ERR_GPU; }
+        }
+    }
+    cudaFreeAsync(ws, s);
+    if (derr) cudaFreeAsync(derr, s);
+    cudaStreamSynchronize(s);
+    return rc;
 }
 
 #define SOLVE_GROUP 32

@@ -119,7 +119,7 @@ struct DevStatus {
     int done, iters;
     unsigned long long amax_bits, amin_bits;
     unsigned int ticket;           // CTAs of the running fused backward-sweep launch that have finished (0 between launches)
-    int pad2;
+    unsigned int tc_err;           // a tensor-core Schur update whose wait ran out of time (bits, see schur_tc.hpp)
 };
 
 __device__ __forceinline__ void set_status(DevStatus *st, int code, long long idx, double best, double thr)

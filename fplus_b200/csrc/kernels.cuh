@@ -1229,6 +1229,57 @@ __global__ void __launch_bounds__(512) k_fwdL3(const T *__restrict__ L, int64_t 
 
 // forward sweep with L through one front (one CTA), in row space: for each pivot column i, the rows below it lose
 // L[row, i] times the pivot row's value
+// The forward sweep through a large front in two launches.  k_fwdL11 (one CTA): the pivot rows' values are gathered
+// (rowid), solved with the unit-lower L11 (a warp per right-hand side, the rows of a step spread over the lanes),
+// written back and copied to xs (np x nrhs, ld np).  k_fwdL21 (many CTAs, a thread per row below the pivots): the rows
+// rr >= np take y[rr] -= sum_i L[rr, i] xs[i] with L read down its columns (coalesced) and xs staged in shared memory
+// (np * nrhs values).  The same operations as one front's forward substitution, the L21 product spread over the GPU.
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwdL11(const T *__restrict__ L, int64_t nrows, int64_t np,
+                                                const int64_t *__restrict__ rowid, T *__restrict__ Wr, int64_t n, int64_t nrhs,
+                                                T *__restrict__ xs)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *v = reinterpret_cast<T *>(smem_raw);           // np x nrhs
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int64_t e = threadIdx.x; e < np * nrhs; e += blockDim.x) v[e] = Wr[rowid[e % np] + (e / np) * n];
+    __syncthreads();
+    for (int64_t r = warp; r < nrhs; r += nw) {
+        T *vr = v + r * np;
+        for (int64_t i = 0; i < np; i++) {
+            const T xi = vr[i];
+            if (!is_zero(xi))
+                for (int64_t rr = i + 1 + lane; rr < np; rr += 32) vr[rr] = sub(vr[rr], mul(L[rr + i * nrows], xi));
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (int64_t e = threadIdx.x; e < np * nrhs; e += blockDim.x) {
+        Wr[rowid[e % np] + (e / np) * n] = v[e];
+        xs[e] = v[e];
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_fwdL21(const T *__restrict__ L, int64_t nrows, int64_t np,
+                                                const int64_t *__restrict__ rowid, T *__restrict__ Wr, int64_t n, int64_t nrhs,
+                                                const T *__restrict__ xs)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *x = reinterpret_cast<T *>(smem_raw);           // np x nrhs
+    for (int64_t e = threadIdx.x; e < np * nrhs; e += blockDim.x) x[e] = xs[e];
+    __syncthreads();
+    const int64_t rr = np + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (rr >= nrows) return;
+    const int64_t o = rowid[rr];
+    for (int64_t r = 0; r < nrhs; r++) {
+        const T *xr = x + r * np;
+        T acc = VT<T>::zero();
+        for (int64_t i = 0; i < np; i++) acc = add(acc, mul(L[rr + i * nrows], xr[i]));
+        Wr[o + r * n] = sub(Wr[o + r * n], acc);
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_fwdL(const T *__restrict__ L, int64_t nrows, int64_t npiv,
                                               const int64_t *__restrict__ rowid, T *__restrict__ Wr, int64_t n, int64_t nrhs)
@@ -1949,6 +2000,39 @@ __global__ void k_flat_norm(const T *__restrict__ U, int64_t m, unsigned long lo
     }
     for (int o = 16; o > 0; o >>= 1) { const double b = __shfl_xor_sync(0xffffffffu, a, o); a = PASS ? a + b : fmax(a, b); }
     if ((threadIdx.x & 31) == 0) { if (PASS) atomicAdd((double *)&acc[3], a); else atomicMax(&acc[1], dbits(a)); }
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// GMRES-IR helpers (one right-hand side at a time).  part[v * gridDim.x + chunk] = the sum over the chunk of
+// conj(V_v) w (V column-major n x nv); a fixed-order tree in shared memory, the chunks summed in order on the host, so the
+// products do not depend on scheduling.  Block 256.
+template <typename T>
+__global__ void __launch_bounds__(256) k_vdots(const T *__restrict__ V, int64_t n, const T *__restrict__ w, T *__restrict__ part)
+{
+    __shared__ T red[256];
+    const int v = blockIdx.y;
+    const T *Vv = V + (int64_t)v * n;
+    T s = VT<T>::zero();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        s = add(s, mul(conjv(Vv[i]), w[i]));
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] = add(red[threadIdx.x], red[threadIdx.x + h]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[(int64_t)v * gridDim.x + blockIdx.x] = red[0];
+}
+
+// w -= sum_v V_v h[v] (nv columns of V, h in device memory); with scale: then w *= scale
+template <typename T>
+__global__ void k_vupdate(const T *__restrict__ V, int64_t n, int nv, const T *__restrict__ h, T *__restrict__ w, double scale)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        T s = w[i];
+        for (int v = 0; v < nv; v++) s = sub(s, mul(V[(int64_t)v * n + i], h[v]));
+        w[i] = scal(s, scale);
+    }
 }
 
 }  // namespace fpl

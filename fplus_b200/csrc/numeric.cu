@@ -2,11 +2,13 @@
 // state of one factorization, and the launch sequences.
 #include "numeric.hpp"
 #include "kernels.cuh"
+#include "schur_tc.hpp"
 #include <algorithm>
 #include <cstring>
 #include <cmath>
 #include <mutex>
 #include <atomic>
+#include <complex>
 
 namespace fpl {
 
@@ -145,7 +147,7 @@ DevNum::~DevNum()
                     (void *)cbstack, (void *)work, (void *)rowid, (void *)p_lu, (void *)pinv, (void *)ipiv, (void *)perm,
                     (void *)st, (void *)scratch, (void *)rbuf, (void *)sbuf, (void *)xbuf, (void *)part, (void *)work2,
                     (void *)perm2, (void *)rr_p, (void *)rr_l, (void *)rr_s, (void *)ir_b, (void *)ir_x, (void *)ir_r,
-                    (void *)ir_d, (void *)ir_bits, scratch_norm})
+                    (void *)ir_d, (void *)ir_bits, scratch_norm, tcws, gm_buf})
         if (p) cudaFreeAsync(p, stream);
     if (stream) cudaStreamSynchronize(stream);
     if (crit) cudaStreamSynchronize(crit);
@@ -301,6 +303,10 @@ static int run_equil(const DevPlan &D, DevNum &N, int equilibrate, int max_iter,
 // the fronts, in order.  Returns FPLUS_OK, or ST_BORDER through *border_front (>= 0) for a restart with a dense chain.
 static size_t front_lu_smem(int64_t nrows, int64_t npiv, int64_t vs) { return (size_t)(nrows * npiv * vs + nrows * (2 * vs + 16) + npiv * 8); }
 static const size_t SMEM_MAX = 220 * 1024;   // dynamic shared memory opt-in, below the 227 KB per-block limit (static smem on top)
+// the precision form takes a Schur update to the tensor cores from this size on (smaller ones stay FP64: they are cheap,
+// and a 128 x 256 tile would be mostly padding)
+static const int64_t TC_MIN_ROWS = 128, TC_MIN_COLS = 256;
+static const double TC_MIN_MADDS = 1 << 24;
 
 template <typename T>
 static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pivot_rel, int64_t *border_front,
@@ -328,6 +334,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         attr_set = 1;
     }
     if ((rc = dev_clear_status(N, err, errlen))) return rc;
+    N.tc_updates = 0; N.tc_flops = 0;
     T *La = (T *)N.Larena, *Ua = (T *)N.Uarena, *CB = (T *)N.cbstack;
     const T *Bx = (const T *)N.Bx;
     constexpr int PW = 32;       // panel width of the blocked path
@@ -550,12 +557,26 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         }
         }
         prof.end(s);
-        // the Schur complement into the CB stack: CB = A22[perm] - L21 U12
+        // the Schur complement into the CB stack: CB = A22[perm] - L21 U12 (the precision form: on the tcgen05 tensor
+        // cores in reduced precision for the large updates; FP64 DMMA otherwise)
         const int64_t M = nr - np;
         if (M > 0) {
             prof.begin(s, PROF_SCHUR, fm * (double)M * (double)ncb * (double)np, (double)(2 * M * ncb + M * np + np * ncb) * vs);
-            dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((ncb + GBN - 1) / GBN));
-            k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, np, Lf + np, ld, Uf, np, W + np * ld, ld, N.perm + np, CB + F.cb_off, M, N.st), note_launch();
+            const bool tc = N.prec != PREC_FP64 && M >= TC_MIN_ROWS && ncb >= TC_MIN_COLS &&
+                            (double)M * (double)ncb * (double)np >= TC_MIN_MADDS && schur_tc_supported(M, ncb, np, VT<T>::cplx_);
+            int trc = 1;
+            if (tc) {
+                const size_t wsb = schur_tc_workspace(N.prec, M, ncb, np, VT<T>::cplx_);
+                if ((rc = ensure_async(N, &N.tcws, &N.cap_tcws, wsb, err, errlen))) return rc;
+                trc = schur_tc(N.prec, VT<T>::cplx_, M, ncb, np, (const double *)(Lf + np), ld, (const double *)Uf, np,
+                               (const double *)(W + np * ld), ld, N.perm + np, (double *)(CB + F.cb_off), M, N.tcws, N.cap_tcws,
+                               &N.st->tc_err, s);
+                if (trc == 0) { note_launch(); add_launches(2); N.tc_updates++; N.tc_flops += fm * (double)M * (double)ncb * (double)np; }
+            }
+            if (trc != 0) {
+                dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((ncb + GBN - 1) / GBN));
+                k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, np, Lf + np, ld, Uf, np, W + np * ld, ld, N.perm + np, CB + F.cb_off, M, N.st), note_launch();
+            }
             prof.end(s);
         }
         if ((fi & 255) == 255) CK(cudaGetLastError());
@@ -567,6 +588,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     prof.flush();
+    if (h.tc_err) { errf(err, errlen, "factorization: a tensor-core Schur update timed out (status %u)", h.tc_err); return FPLUS_ERR_GPU; }
     if (h.code == ST_BORDER) { *border_front = h.idx; return FPLUS_OK; }
     if (h.code == ST_SINGULAR) {
         errf(err, errlen, "Near-zero or zero pivot %.6e at step %ld (threshold %.6e). Matrix is singular.", h.best, (long)h.idx, h.thr);
@@ -645,6 +667,8 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
     constexpr size_t FWD_SMEM = 200 * 1024;
     CK(cudaFuncSetAttribute(k_fwdL2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
     CK(cudaFuncSetAttribute(k_fwdL3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
+    CK(cudaFuncSetAttribute(k_fwdL11<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
+    CK(cudaFuncSetAttribute(k_fwdL21<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
     CK(cudaFuncSetAttribute(k_u12_gemv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
     if (fsmem > 48 * 1024) CK(cudaFuncSetAttribute(k_bwdU_fused<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem));
     {
@@ -678,8 +702,14 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
                 CK(launch_pdl(k_fwdL3<T>, 1, swt, l11_sm, s, La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 0));
                 note_launch();
             }
-            else if (fsm <= 96 * 1024)
-                k_fwdL2<T><<<1, 256, fsm, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs), note_launch();
+            else if ((size_t)np * nrhs * sizeof(T) <= FWD_SMEM) {
+                // a large front: the L11 solve, then the L21 product over many CTAs (xs in the partial-sum buffer)
+                const size_t xsm = (size_t)np * nrhs * sizeof(T);
+                k_fwdL11<T><<<1, 256, xsm, s>>>(La + F.L_off, F.nrows, np, N.rowid + F.row_off, R, n, nrhs, part), note_launch();
+                if (F.nrows > np)
+                    k_fwdL21<T><<<(unsigned)((F.nrows - np + 255) / 256), 256, xsm, s>>>(La + F.L_off, F.nrows, np,
+                                                                                      N.rowid + F.row_off, R, n, nrhs, part), note_launch();
+            }
             else
                 k_fwdL<T><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs), note_launch();
         }
@@ -978,6 +1008,151 @@ int dev_check_finite(DevNum &N, char *err, size_t errlen)
 // iterative refinement (the precision form's driver; here on the FP64 factors)
 namespace fpl {
 
+using Hc = std::complex<double>;
+static inline Hc toH(double v) { return Hc(v, 0.0); }
+static inline Hc toH(const cplx &v) { return Hc(v.x, v.y); }
+template <typename T> static inline T fromH(Hc h);
+template <> inline double fromH<double>(Hc h) { return h.real(); }
+template <> inline cplx fromH<cplx>(Hc h) { return cplx{h.real(), h.imag()}; }
+
+// GMRES-IR (Carson and Higham, SIAM J. Sci. Comput. 40(2), 2018) for one right-hand side, when classic refinement has
+// stalled: x is corrected by x += d, d from GMRES (restart GM_RESTART) on the preconditioned correction equation
+// M^-1 op(A) d = M^-1 r, where M = the factorization's own LU (whatever the precision of its updates) and the residual
+// r = b - op(A) x, the matrix products, the Arnoldi process (classical Gram-Schmidt applied twice) and the update are
+// FP64.  A cycle ends when the preconditioned residual has dropped by GM_INNER_TOL.  Stops when the componentwise
+// backward error is at most tol, after max_solves applications of M^-1, or when a cycle does not lower the error (that
+// cycle is undone).  On return *be is the backward error of x and *solves the applications of M^-1 made.
+constexpr int GM_RESTART = 30, GM_CHUNKS = 64;
+constexpr double GM_INNER_TOL = 1e-12;
+
+template <typename T>
+static int gmres_ir_column(const FrontPlan &P, const DevPlan &D, DevNum &N, T *x, const T *b, int trans, int max_solves,
+                           double tol, double *be, int *solves, char *err, size_t errlen)
+{
+    cudaStream_t s = N.stream;
+    const int64_t n = N.n;
+    constexpr int RS = GM_RESTART;
+    const size_t need = sizeof(T) * ((size_t)n * (RS + 1) + 3 * (size_t)n + (RS + 1) + (size_t)(RS + 1) * GM_CHUNKS);
+    int rc;
+    if ((rc = ensure_async(N, &N.gm_buf, &N.cap_gm, need, err, errlen))) return rc;
+    T *V = (T *)N.gm_buf, *w = V + (size_t)n * (RS + 1), *r = w + n, *zero = r + n, *hd = zero + n, *part = hd + (RS + 1);
+    CK(cudaMemsetAsync(zero, 0, (size_t)n * sizeof(T), s));
+    const bool t0 = trans == 0;
+    const int64_t *ptr = t0 ? N.rr_p : D.Bp, *ix = t0 ? N.rr_l : D.Bi, *src = t0 ? N.rr_s : D.Bsrc;
+    const int64_t *outm = t0 ? D.row_perm : D.col_perm, *inm = t0 ? D.col_perm : D.row_perm;
+    const int grid = nblk(n * 32);
+    // out = bv - op(A) xv, with the componentwise backward error of xv when err_out
+    auto resid = [&](const T *xv, const T *bv, T *out, double *err_out) -> int {
+        CK(cudaMemsetAsync(N.ir_bits, 0, 8, s));
+        if (trans == 2) k_resid<T, true><<<grid, 256, 0, s>>>(ptr, ix, src, (const T *)N.Ax, outm, inm, xv, bv, out, n, 1, N.ir_bits);
+        else k_resid<T, false><<<grid, 256, 0, s>>>(ptr, ix, src, (const T *)N.Ax, outm, inm, xv, bv, out, n, 1, N.ir_bits);
+        note_launch();
+        if (err_out) {
+            unsigned long long bits = 0;
+            CK(cudaMemcpyAsync(&bits, N.ir_bits, 8, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            *err_out = bitsd_h(bits);
+        }
+        return FPLUS_OK;
+    };
+    // h[v] = conj(V_v) . wv for v < nv
+    std::vector<T> hp((size_t)(RS + 1) * GM_CHUNKS);
+    auto dots = [&](const T *Vb, int nv, const T *wv, std::vector<Hc> &h) -> int {
+        k_vdots<T><<<dim3(GM_CHUNKS, (unsigned)nv), 256, 0, s>>>(Vb, n, wv, part), note_launch();
+        CK(cudaMemcpyAsync(hp.data(), part, (size_t)nv * GM_CHUNKS * sizeof(T), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        h.assign((size_t)nv, Hc(0.0, 0.0));
+        for (int v = 0; v < nv; v++)
+            for (int c = 0; c < GM_CHUNKS; c++) h[(size_t)v] += toH(hp[(size_t)v * GM_CHUNKS + c]);
+        return FPLUS_OK;
+    };
+    std::vector<T> hu((size_t)RS + 1);
+    // wv = (wv - sum_v V_v h[v]) * scale
+    auto update = [&](const T *Vb, int nv, const std::vector<Hc> &h, T *wv, double scale) -> int {
+        for (int v = 0; v < nv; v++) hu[(size_t)v] = fromH<T>(h[(size_t)v]);
+        if (nv > 0) CK(cudaMemcpyAsync(hd, hu.data(), (size_t)nv * sizeof(T), cudaMemcpyHostToDevice, s));
+        k_vupdate<T><<<nblk(n), 256, 0, s>>>(Vb, n, nv, hd, wv, scale), note_launch();
+        if (nv > 0) CK(cudaStreamSynchronize(s));        // hu is reused by the next call
+        return FPLUS_OK;
+    };
+    const std::vector<Hc> none;
+    double e = 0.0;
+    if ((rc = resid(x, b, r, &e))) return rc;
+    int used = 0;
+    while (e > tol && used < max_solves) {
+        // v0 = M^-1 r / beta
+        CK(cudaMemcpyAsync(V, r, (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        if ((rc = dev_solve(P, D, N, V, 1, trans, err, errlen))) return rc;
+        used++;
+        std::vector<Hc> hh, h2;
+        if ((rc = dots(V, 1, V, hh))) return rc;
+        const double beta = std::sqrt(hh[0].real());
+        if (!(beta > 0.0) || !std::isfinite(beta)) break;
+        if ((rc = update(V, 0, none, V, 1.0 / beta))) return rc;
+        std::vector<std::vector<Hc>> H((size_t)RS, std::vector<Hc>((size_t)RS + 1, Hc(0.0, 0.0)));   // H[j] = column j
+        std::vector<double> cs((size_t)RS, 0.0);
+        std::vector<Hc> sn((size_t)RS), g((size_t)RS + 1, Hc(0.0, 0.0));
+        g[0] = Hc(beta, 0.0);
+        int k = 0;          // the basis vectors in use
+        for (int j = 0; j < RS && used < max_solves; j++) {
+            T *vn = V + (size_t)(j + 1) * n;
+            if ((rc = resid(V + (size_t)j * n, zero, vn, nullptr))) return rc;      // vn = -op(A) v_j
+            if ((rc = dev_solve(P, D, N, vn, 1, trans, err, errlen))) return rc;
+            used++;
+            if ((rc = update(V, 0, none, vn, -1.0))) return rc;                  // vn = M^-1 op(A) v_j
+            if ((rc = dots(V, j + 1, vn, hh)) || (rc = update(V, j + 1, hh, vn, 1.0))) return rc;
+            if ((rc = dots(V, j + 1, vn, h2)) || (rc = update(V, j + 1, h2, vn, 1.0))) return rc;
+            std::vector<Hc> &Hj = H[(size_t)j];
+            for (int i = 0; i <= j; i++) Hj[(size_t)i] = hh[(size_t)i] + h2[(size_t)i];
+            std::vector<Hc> nn;
+            if ((rc = dots(vn, 1, vn, nn))) return rc;
+            const double hn = std::sqrt(std::max(nn[0].real(), 0.0));
+            Hj[(size_t)j + 1] = Hc(hn, 0.0);
+            if (hn > 0.0 && (rc = update(V, 0, none, vn, 1.0 / hn))) return rc;
+            for (int i = 0; i < j; i++) {      // the earlier rotations
+                const Hc a = Hj[(size_t)i], bb = Hj[(size_t)i + 1];
+                Hj[(size_t)i] = cs[(size_t)i] * a + sn[(size_t)i] * bb;
+                Hj[(size_t)i + 1] = -std::conj(sn[(size_t)i]) * a + cs[(size_t)i] * bb;
+            }
+            // the rotation that zeroes H(j + 1, j)
+            const Hc a = Hj[(size_t)j], bb = Hj[(size_t)j + 1];
+            const double aa = std::abs(a), rr = std::hypot(aa, std::abs(bb));
+            if (rr == 0.0) { cs[(size_t)j] = 1.0; sn[(size_t)j] = 0.0; }
+            else if (aa == 0.0) { cs[(size_t)j] = 0.0; sn[(size_t)j] = std::conj(bb) / std::abs(bb); }
+            else { cs[(size_t)j] = aa / rr; sn[(size_t)j] = (a / aa) * std::conj(bb) / rr; }
+            Hj[(size_t)j] = cs[(size_t)j] * a + sn[(size_t)j] * bb;
+            Hj[(size_t)j + 1] = 0.0;
+            g[(size_t)j + 1] = -std::conj(sn[(size_t)j]) * g[(size_t)j];
+            g[(size_t)j] = cs[(size_t)j] * g[(size_t)j];
+            k = j + 1;
+            if (std::abs(g[(size_t)j + 1]) <= GM_INNER_TOL * beta || hn == 0.0) break;
+        }
+        if (k == 0) break;
+        // y = H(0:k, 0:k) \ g(0:k); w = V y; x += w
+        std::vector<Hc> y((size_t)k);
+        for (int i = k - 1; i >= 0; i--) {
+            Hc t = g[(size_t)i];
+            for (int c = i + 1; c < k; c++) t -= H[(size_t)c][(size_t)i] * y[(size_t)c];
+            y[(size_t)i] = t / H[(size_t)i][(size_t)i];
+        }
+        for (auto &v : y) v = -v;
+        CK(cudaMemsetAsync(w, 0, (size_t)n * sizeof(T), s));
+        if ((rc = update(V, k, y, w, 1.0))) return rc;
+        k_axpy1<T><<<nblk(n), 256, 0, s>>>(x, w, n, 0), note_launch();
+        double e2 = 0.0;
+        if ((rc = resid(x, b, r, &e2))) return rc;
+        if (!(e2 < e)) {                          // no progress: undo the cycle and stop
+            k_axpy1<T><<<nblk(n), 256, 0, s>>>(x, w, n, 1), note_launch();
+            if ((rc = resid(x, b, r, nullptr))) return rc;
+            break;
+        }
+        e = e2;
+    }
+    *be = e;
+    *solves = used;
+    return FPLUS_OK;
+}
+
 template <typename T>
 static int run_refine(const FrontPlan &P, const DevPlan &D, DevNum &N, void *bh, int64_t ldb, int64_t nrhs, int trans,
                       int max_iter, double tol, double *berr, int *iters, char *err, size_t errlen)
@@ -1058,6 +1233,18 @@ static int run_refine(const FrontPlan &P, const DevPlan &D, DevNum &N, void *bh,
             if ((rc = dev_solve(P, D, N, Dd, m, trans, err, errlen))) return rc;
             k_axpy1<T><<<nblk(n * m), 256, 0, s>>>(X, Dd, n * m, 0), note_launch();
             prev = cur;
+        }
+        // classic refinement stalled above the target: GMRES-IR for those right-hand sides, within the same budget of
+        // max_iter solves per right-hand side (at least 2 GMRES cycles' worth)
+        for (int64_t c = 0; c < m; c++) {
+            if (!(berr[r0 + c] > tol) || !std::isfinite(berr[r0 + c])) continue;
+            const int budget = max_iter > 0 ? std::max(max_iter, 2 * GM_RESTART + 2) - iters[r0 + c] : 0;
+            if (budget <= 0) continue;
+            double be = berr[r0 + c];
+            int used = 0;
+            if ((rc = gmres_ir_column<T>(P, D, N, X + c * n, Bd + c * n, trans, budget, tol, &be, &used, err, errlen))) return rc;
+            berr[r0 + c] = be;
+            iters[r0 + c] += used;
         }
         CK(cudaMemcpy2DAsync(bb, (size_t)ldb * sizeof(T), X, (size_t)n * sizeof(T), (size_t)n * sizeof(T), (size_t)m,
                              cudaMemcpyDeviceToHost, s));

@@ -63,6 +63,15 @@ struct DevNum {
     void *scratch = nullptr;
     void *scratch_norm = nullptr;
     size_t cap_norm = 0;
+    // the precision form: the arithmetic of the large fronts' Schur updates (schur_tc.hpp), their operand workspace, and
+    // the updates that ran on the tensor cores in the last factorization
+    int prec = 0;
+    void *gm_buf = nullptr;        // GMRES-IR: the Krylov basis and its vectors
+    size_t cap_gm = 0;
+    void *tcws = nullptr;
+    size_t cap_tcws = 0;
+    long long tc_updates = 0;
+    double tc_flops = 0;
     void *rbuf = nullptr, *sbuf = nullptr, *xbuf = nullptr, *part = nullptr;
     size_t cap_r = 0, cap_s = 0, cap_x = 0, cap_part = 0;
     int ruiz_iters = 0;

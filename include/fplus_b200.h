@@ -33,6 +33,10 @@ typedef struct {
     double  ms_equil;           /* device time: permutation + Ruiz */
     double  ms_fronts;          /* device time: the fronts (last attempt) */
     int64_t device_bytes;       /* device memory held by the factorization */
+    int     precision;          /* FPLUS_B200_PREC_* of the Schur-complement updates (fplus_b200_factor_prec) */
+    int     reserved;
+    int64_t tc_updates;         /* Schur updates that ran on the tcgen05 tensor cores in reduced precision */
+    double  tc_flops;           /* their real floating-point operations (complex: x4) */
 } fplus_b200_info;
 
 int fplus_b200_numeric_info(const fplus_numeric *num, fplus_b200_info *info);
@@ -45,6 +49,35 @@ void fplus_b200_use_stream(void *stream);
  * analysed pattern Ap / Ai on the host).  The values are checked for finiteness on the device. */
 int fplus_b200_factor_dev(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax_dev, int is_complex,
                           const fplus_options *opt, fplus_numeric **num, char *err, size_t errlen);
+
+/* The precision form (no counterpart in FPLUS, which factors in FP64 only): fplus_factor (ax_on_device = 0) or
+ * fplus_b200_factor_dev (1) with the Schur-complement updates of the large fronts (at least 128 x 256 contribution
+ * blocks) on the tcgen05 tensor cores in reduced precision, FP32 accumulation:
+ *   FPLUS_B200_PREC_FP32    operands split into two TF32 parts, three products: FP32-level accuracy
+ *   FPLUS_B200_PREC_BF16X3  operands split into two BF16 parts, three products
+ *   FPLUS_B200_PREC_TF32    one TF32 part, one product
+ * FPLUS_B200_PREC_FP64 is fplus_factor itself.  Ruiz scaling, the pivot search and pivot-block factorization, the
+ * triangular solves for U12 and every smaller update stay FP64, as do the stored factors.  The pivots are those of the
+ * reduced-precision elimination (they can differ from FP64's where candidates are close); solve with
+ * fplus_b200_solve_refine to bring the solution back to FP64 accuracy.  The operands of the reduced-precision products
+ * must lie within FP32's range (Ruiz scaling, the default, ensures that for the matrices FPLUS targets). */
+#define FPLUS_B200_PREC_FP64   0
+#define FPLUS_B200_PREC_FP32   1
+#define FPLUS_B200_PREC_BF16X3 2
+#define FPLUS_B200_PREC_TF32   3
+int fplus_b200_factor_prec(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex,
+                           const fplus_options *opt, int precision, int ax_on_device, fplus_numeric **num, char *err,
+                           size_t errlen);
+
+/* The precision form's Schur-complement update on device buffers, as the factorization runs it on a large front:
+ * Cout[i, j] = Cin[rmap[i], j] - sum_k A[i, k] B[k, j] (rmap NULL: Cin[i, j]) for i < M, j < N, with A (M x K, lda), B
+ * (K x N, ldb), Cin (ldci), Cout (ldco) FP64 column-major device arrays (is_complex: interleaved double pairs) and the
+ * product in precision FPLUS_B200_PREC_FP32, _BF16X3 or _TF32 on the tcgen05 tensor cores.  M >= 128 and N >= 256
+ * (N >= 128 complex).  Runs on `stream` (a cudaStream_t, NULL: the default stream) and waits for it; the workspace is
+ * allocated and freed on the stream.  No counterpart in FPLUS. */
+int fplus_b200_schur_update(int precision, int is_complex, int64_t M, int64_t N, int64_t K, const void *A, int64_t lda,
+                            const void *B, int64_t ldb, const void *Cin, int64_t ldci, const int *rmap, void *Cout, int64_t ldco,
+                            void *stream, char *err, size_t errlen);
 
 /* fplus_solve with the right-hand sides in device memory (column-major, leading dimension ldb >= n), solved in place. */
 int fplus_b200_solve_dev(const fplus_numeric *num, void *b_dev, int64_t nrhs, int64_t ldb, int trans, char *err, size_t errlen);
@@ -103,8 +136,12 @@ int fplus_b200_solve_dev_noalloc(const fplus_numeric *num, void *b_dev, int64_t 
  * x += solve(b - op(A) x) while a right-hand side's componentwise backward error max_i |r_i| / (|op(A)| |x| + |b|)_i is
  * above tol and at least halves from one correction to the next, at most max_iter times (LAPACK's xGERFS rule).  The
  * residual is formed on the GPU in FP64 from the factorization's own device copy of A, with a fixed summation order.
- * berr[k] receives the final backward error and iters[k] the corrections applied to right-hand side k (either may be
- * NULL).  max_iter 0 gives fplus_solve's result with its backward error. */
+ * A right-hand side whose refinement stalls above tol (a factorization from fplus_b200_factor_prec on an ill-conditioned
+ * matrix) continues with GMRES-IR: restarted GMRES (30 vectors, classical Gram-Schmidt applied twice, all in FP64) on
+ * the correction equation preconditioned by the factorization, M^-1 op(A) d = M^-1 r, until tol is met, a cycle does
+ * not lower the error, or max(max_iter, 62) applications of the factors in all.  berr[k] receives the final backward
+ * error and iters[k] the applications of the factors after the first solve for right-hand side k (either may be NULL).
+ * max_iter 0 gives fplus_solve's result with its backward error. */
 int fplus_b200_solve_refine(const fplus_numeric *num, void *b, int64_t nrhs, int64_t ldb, int trans, int max_iter, double tol,
                             double *berr, int *iters, char *err, size_t errlen);
 

@@ -462,3 +462,56 @@ def test_oracle_matches_reference_at_extreme_magnitudes(scale):
     R = O.RefLU(n, Ap, Ai, Ax, S.col_perm, tr, tc, postorder=0, equilibrate=0)
     orc = O.OracleLU(n, Ap, Ai, Ax, S.row_perm, S.col_perm, equilibrate=0)
     assert np.array_equal(R.p, orc.p)
+
+
+# -------------------------------------------------------------------------------- the batch form across GPUs (gloo, CPU)
+def _lpt_worker(rank, world, port, costs, out):
+    import torch.distributed as dist
+    from fplus_b200 import shard
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        parts = shard.lpt_partition(costs, world)
+        mine = parts[rank]
+        # each rank "processes" its share (the sum of its costs stands for its device time) and the results are gathered
+        res = shard.gather_results({"rank": rank, "jobs": mine, "load": float(sum(costs[k] for k in mine))})
+        out[rank] = res
+    finally:
+        dist.destroy_process_group()
+
+
+def test_lpt_partition_properties():
+    from fplus_b200 import shard
+    rng = np.random.default_rng(4)
+    n = np.exp(rng.uniform(np.log(500), np.log(8000), 512)).astype(int)
+    costs = [shard.pencil_cost(int(k), 20 * int(k)) for k in n]
+    for parts in (1, 2, 3, 8):
+        p = shard.lpt_partition(costs, parts)
+        flat = sorted(k for q in p for k in q)
+        assert flat == list(range(len(costs)))
+        loads = [sum(costs[k] for k in q) for q in p]
+        assert max(loads) <= 4.0 / 3.0 * max(sum(costs) / parts, max(costs)) + 1e-6      # Graham's bound
+        for q in p:
+            assert all(costs[q[i]] >= costs[q[i + 1]] for i in range(len(q) - 1))    # largest first within a rank
+
+
+def test_lpt_sharding_over_two_gloo_ranks():
+    """The pencils of the batch form split across two ranks with no data exchange: both ranks compute the same
+    partition, the shares are disjoint and complete, and the gathered loads are balanced."""
+    import socket
+    import torch.multiprocessing as mp
+    from fplus_b200 import shard
+    rng = np.random.default_rng(5)
+    costs = [float(c) for c in rng.uniform(1.0, 100.0, 64)]
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.start_processes(_lpt_worker, args=(2, port, costs, out), nprocs=2, join=True, start_method="spawn")
+    r0, r1 = out[0], out[1]
+    assert r0 == r1                                                       # every rank holds every rank's result
+    jobs = sorted(r0[0]["jobs"] + r0[1]["jobs"])
+    assert jobs == list(range(64))
+    assert set(r0[0]["jobs"]).isdisjoint(r0[1]["jobs"])
+    assert abs(r0[0]["load"] - r0[1]["load"]) <= max(costs)
+    assert shard.lpt_partition(costs, 2) == [r0[0]["jobs"], r0[1]["jobs"]]
