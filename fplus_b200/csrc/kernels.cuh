@@ -838,6 +838,238 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
     for (int e = at; e < ne; e += nact) { const int i = e % nrows; Lout[pos[i] + (int64_t)(e / nrows) * nrows] = A[e]; }
 }
 
+// Blocked partial-pivot LU of a front's pivot block in shared memory (nrows <= 128, npiv <= 64; one CTA of LU3_THREADS):
+// the same elimination as k_front_lu2 in panels of LU3_PB columns with a one-panel look-ahead.
+//   warp 0 (the panel warp)  factors panel p = columns [c0, c1) with its rows in registers (row i in lane i % 32, slot
+//                            i / 32): per column, the pivot (largest key, ties to the smaller row of B), the singular and
+//                            border tests, the multipliers, and the update of the panel's later columns; no block barrier
+//                            inside a panel.  Then the panel goes back to shared memory, with a copy of its multipliers
+//                            in which every row already pivoted reads zero (Lm, double-buffered by panel parity).
+//   warps 1.. (the workers)  for the columns after the panel, first the next panel's, then the rest: the pivot rows' U
+//                            values by forward substitution with the panel's unit-lower L11 (a thread per column), then
+//                            every row's update A[c][i] -= sum_k Lm[k][i] U[k][c].  As soon as the next panel's columns
+//                            are done, warp 0 moves on to it while the workers finish the rest.
+// Rows are never swapped: the pivot row of step j is tagged j, as in k_front_lu2, and the final order is formed at the end.
+// Decisions to stop (singular column, dense-row pivot) are made by warp 0 before a panel's barrier and read by every warp
+// after it.  Named barriers: 1 (all, a panel is factored), 2 (all, the next panel's columns are updated), 3 (workers).
+constexpr int LU3_PB = 8, LU3_THREADS = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(LU3_THREADS) k_front_lu3(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
+                                                           int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
+                                                           int64_t *__restrict__ rowid, T *__restrict__ Lout, int *__restrict__ perm,
+                                                           int64_t *__restrict__ p_lu, DevStatus *st, int64_t front, PivotAsm pa)
+{
+    constexpr int PB = LU3_PB;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *A = reinterpret_cast<T *>(smem_raw);                        // npiv x nrows, column-major: A[c * nrows + i]
+    T *Lm = A + (size_t)npiv * nrows;                              // 2 x PB x nrows: masked multipliers of a panel
+    int64_t *rid = reinterpret_cast<int64_t *>(Lm + 2 * PB * nrows);
+    double *thr = reinterpret_cast<double *>(rid + nrows);         // npiv: pivot_rel * max |B(:, column)|
+    int *tag = reinterpret_cast<int *>(thr + npiv);
+    int *pos = tag + nrows;
+    int *piv = pos + nrows;                                        // npiv: the pivot row (local) of each step
+    __shared__ int s_stop;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
+    const int ne = npiv * nrows;
+    if (!pa.on) {
+        pdl_wait();
+        for (int e0 = tid; e0 < ne; e0 += 8 * nt) {
+            T v[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) { const int e = e0 + q * nt; v[q] = e < ne ? W[e % nrows + (int64_t)(e / nrows) * ld] : VT<T>::zero(); }
+#pragma unroll
+            for (int q = 0; q < 8; q++) { const int e = e0 + q * nt; if (e < ne) A[e] = v[q]; }
+        }
+        for (int i = tid; i < nrows; i += nt) rid[i] = rowid[i];
+    } else {
+        for (int e = tid; e < ne; e += nt) A[e] = VT<T>::zero();
+        for (int i = tid; i < nrows; i += nt) rid[i] = pa.rowinit[i];
+        __syncthreads();
+        const T *Bx = reinterpret_cast<const T *>(pa.Bx);
+#pragma unroll 4
+        for (int64_t e = tid; e < pa.acnt; e += nt) A[pa.adst[e]] = Bx[pa.asrc[e]];
+        pdl_wait();
+        for (int64_t t = tid; t < pa.nslot; t += nt) rid[pa.slot + t] = pa.child_rowid[t];
+        __syncthreads();
+        const T *cb = reinterpret_cast<const T *>(pa.cb);
+        const int cbr = (int)pa.cbr, tot = (int)(pa.cbr * pa.h), nsl = (int)pa.nslot, sl = (int)pa.slot, tb = (int)pa.tau_base;
+#pragma unroll 4
+        for (int e = tid; e < tot; e += nt) {
+            const int c = e / cbr, t = e - c * cbr;
+            const int pr = t < nsl ? sl + t : tb + (t - nsl);
+            T *a = A + (int)pa.relcol[c] * nrows + pr;
+            *a = add(*a, cb[t + (int64_t)c * cbr]);
+        }
+    }
+    for (int i = tid; i < nrows; i += nt) tag[i] = INT_MAX;
+    for (int c = tid; c < npiv; c += nt) thr[c] = pivot_rel * colmax[fcol + c];
+    if (tid == 0) s_stop = st->code != 0 ? 3 : 0;
+    __syncthreads();
+    if (s_stop) return;
+    const int npan = (npiv + PB - 1) / PB;
+    if (warp == 0) {
+        int64_t rr[4];
+        bool al[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int i = lane + 32 * q;
+            al[q] = i < nrows;
+            rr[q] = al[q] ? rid[i] : INT64_MAX;
+        }
+        for (int p = 0; p < npan; p++) {
+            const int c0 = p * PB, w = npiv - c0 < PB ? npiv - c0 : PB;
+            T x[4][PB];
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+#pragma unroll
+                for (int k = 0; k < PB; k++) {
+                    const int i = lane + 32 * q;
+                    x[q][k] = (i < nrows && k < w) ? A[(size_t)(c0 + k) * nrows + i] : VT<T>::zero();
+                }
+            int stop = 0;
+#pragma unroll
+            for (int k = 0; k < PB; k++) {
+                if (k >= w) break;
+                const int j = c0 + k;
+                // the pivot: each lane's best live slot, then the warp's largest key (ties: the smaller row of B)
+                long long bk = -1; int wi = -1; int64_t br = INT64_MAX;
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    if (!al[q]) continue;
+                    const long long a = (long long)pivkey(x[q][k]);
+                    if (a > bk || (a == bk && rr[q] < br)) { bk = a; wi = lane + 32 * q; br = rr[q]; }
+                }
+                const unsigned long long key = wi >= 0 ? (unsigned long long)bk : 0ull;
+                const unsigned long long mk = warp_max_key(key);
+                unsigned cand = __ballot_sync(0xffffffffu, wi >= 0 && key == mk);
+                int bi = -1;
+                if (cand != 0) {
+                    if ((cand & (cand - 1)) != 0) {
+                        int64_t r2 = (cand >> lane) & 1u ? br : INT64_MAX;
+                        for (int o = 16; o > 0; o >>= 1) { const int64_t t = __shfl_xor_sync(0xffffffffu, r2, o); r2 = t < r2 ? t : r2; }
+                        cand = __ballot_sync(0xffffffffu, ((cand >> lane) & 1u) && br == r2);
+                    }
+                    bi = __shfl_sync(0xffffffffu, wi, __ffs(cand) - 1);
+                }
+                // the pivot row's values in this panel's columns, from the lane that holds it
+                const int ql = bi >= 0 ? bi >> 5 : 0, ol = bi >= 0 ? bi & 31 : 0;
+                T prow[PB];
+#pragma unroll
+                for (int k2 = 0; k2 < PB; k2++) {
+                    T mine = x[0][k2];
+#pragma unroll
+                    for (int q = 1; q < 4; q++) if (q == ql) mine = x[q][k2];
+                    prow[k2] = shfl_v<T>(mine, ol);
+                }
+                const T pv = prow[k];
+                if (lane == 0) {
+                    const double t = thr[j];
+                    const bool sing = bi < 0 || mk == 0ull || (mk < pivkey_of_modulus<T>(2.0 * t) && vabs(pv) < t);
+                    if (sing) { set_status(st, ST_SINGULAR, fcol + j, bi >= 0 ? vabs(pv) : 0.0, t); stop = 1; }
+                    else if (bi >= nri) { set_status(st, ST_BORDER, front, vabs(pv), t); stop = 1; }
+                    if (!stop) { tag[bi] = j; piv[j] = bi; }
+                }
+                stop = __shfl_sync(0xffffffffu, stop, 0);
+                if (stop) break;
+                const T inv = recip(pv);
+                if (lane == ol) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) if (q == ql) al[q] = false;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    if (!al[q]) continue;
+                    const T l = mul(x[q][k], inv);
+                    x[q][k] = l;
+#pragma unroll
+                    for (int k2 = k + 1; k2 < PB; k2++) if (k2 < w) x[q][k2] = sub(x[q][k2], mul(l, prow[k2]));
+                }
+            }
+            // the panel back to shared memory; the multipliers of the rows still live (zero for every pivoted row)
+            T *Lb = Lm + (size_t)(p & 1) * PB * nrows;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int i = lane + 32 * q;
+                if (i >= nrows) continue;
+#pragma unroll
+                for (int k = 0; k < PB; k++) {
+                    if (k >= w) break;
+                    A[(size_t)(c0 + k) * nrows + i] = x[q][k];
+                    Lb[(size_t)k * nrows + i] = al[q] ? x[q][k] : VT<T>::zero();
+                }
+            }
+            if (lane == 0 && stop) s_stop = 1;
+            __syncwarp();
+            named_bar(1, nt);
+            if (s_stop) return;
+            if (p + 1 < npan) named_bar(2, nt);
+        }
+    } else {
+        const int wt = tid - 32, nwt = nt - 32;
+        for (int p = 0; p < npan; p++) {
+            named_bar(1, nt);
+            if (s_stop) return;
+            const int c0 = p * PB, w = npiv - c0 < PB ? npiv - c0 : PB, c1 = c0 + w;
+            const int c2 = c1 + PB < npiv ? c1 + PB : npiv;
+            const T *Lb = Lm + (size_t)(p & 1) * PB * nrows;
+            for (int part = 0; part < 2; part++) {
+                const int ca = part ? c2 : c1, cb = part ? npiv : c2;
+                if (ca < cb) {
+                    // U rows of the panel's pivots in columns [ca, cb): forward substitution with L11 (a thread per column)
+                    for (int c = ca + wt; c < cb; c += nwt) {
+                        T u[PB];
+#pragma unroll
+                        for (int k = 0; k < PB; k++) {
+                            if (k >= w) break;
+                            const int pr = piv[c0 + k];
+                            T v = A[(size_t)c * nrows + pr];
+#pragma unroll
+                            for (int m = 0; m < PB; m++) if (m < k) v = sub(v, mul(A[(size_t)(c0 + m) * nrows + pr], u[m]));
+                            u[k] = v;
+                            A[(size_t)c * nrows + pr] = v;
+                        }
+                    }
+                    named_bar(3, nwt);
+                    // every row: A[c][i] -= sum_k Lm[k][i] U[k][c] (the pivoted rows' Lm is zero: they are left alone)
+                    const int tot = (cb - ca) * nrows;
+                    for (int e = wt; e < tot; e += nwt) {
+                        const int c = ca + e / nrows, i = e - (e / nrows) * nrows;
+                        T acc = VT<T>::zero();
+#pragma unroll
+                        for (int k = 0; k < PB; k++) {
+                            if (k >= w) break;
+                            acc = add(acc, mul(Lb[(size_t)k * nrows + i], A[(size_t)c * nrows + piv[c0 + k]]));
+                        }
+                        if (!is_zero(acc)) A[(size_t)c * nrows + i] = sub(A[(size_t)c * nrows + i], acc);
+                    }
+                }
+                if (part == 0 && p + 1 < npan) named_bar(2, nt);
+            }
+        }
+    }
+    __syncthreads();
+    const int steps = npiv;
+    if (warp == 0) {
+        int base = steps;
+        for (int i0 = 0; i0 < nrows; i0 += 32) {
+            const int i = i0 + lane;
+            const bool un = i < nrows && tag[i] >= steps;
+            const unsigned m = __ballot_sync(0xffffffffu, un);
+            if (i < nrows) pos[i] = un ? base + __popc(m & ((1u << lane) - 1u)) : tag[i];
+            base += __popc(m);
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < nrows; i += nt) {
+        const int k = pos[i];
+        perm[k] = i;
+        rowid[k] = rid[i];
+        if (k < steps) p_lu[fcol + k] = rid[i];
+    }
+    for (int e = tid; e < ne; e += nt) { const int i = e % nrows; Lout[pos[i] + (int64_t)(e / nrows) * nrows] = A[e]; }
+}
+
 // After the blocked (global-memory) pivoting of a large front's pivot block: the final row order from the swaps, the
 // pivot rows (the swaps already moved the row ids), and the block into the arena
 template <typename T>

@@ -302,6 +302,15 @@ static int run_equil(const DevPlan &D, DevNum &N, int equilibrate, int max_iter,
 // ---------------------------------------------------------------------------------------------------------------------
 // the fronts, in order.  Returns FPLUS_OK, or ST_BORDER through *border_front (>= 0) for a restart with a dense chain.
 static size_t front_lu_smem(int64_t nrows, int64_t npiv, int64_t vs) { return (size_t)(nrows * npiv * vs + nrows * (2 * vs + 16) + npiv * 8); }
+// k_front_lu3: the block, two panels of masked multipliers, row ids, tags, positions, thresholds and pivot rows
+static size_t front_lu3_smem(int64_t nrows, int64_t npiv, int64_t vs)
+{
+    return (size_t)(nrows * npiv * vs + 2 * LU3_PB * nrows * vs + nrows * 16 + npiv * 12);
+}
+static bool use_lu3(int64_t nrows, int64_t npiv, int64_t vs)
+{
+    return nrows <= 128 && npiv <= 64 && npiv <= nrows && front_lu3_smem(nrows, npiv, vs) <= 220 * 1024;
+}
 static const size_t SMEM_MAX = 220 * 1024;   // dynamic shared memory opt-in, below the 227 KB per-block limit (static smem on top)
 // the precision form takes a Schur update to the tensor cores from this size on (smaller ones stay FP64: they are cheap,
 // and a 128 x 256 tile would be mostly padding)
@@ -326,6 +335,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     static thread_local int attr_set = 0;
     if (!attr_set) {
         CK(cudaFuncSetAttribute(k_front_lu2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_front_lu3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_u12_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
@@ -414,7 +424,16 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             for (int64_t k = 0; k < std::min(np, nr); k++) fl += (double)(nr - k - 1) * (double)(np - k);
             prof.begin(st, PROF_LU, fm * fl, 2.0 * (double)(nr * np) * vs);
         }
-        if (sm <= SMEM_MAX) {
+        if (use_lu3(nr, np, vs)) {
+            const size_t sm3 = front_lu3_smem(nr, np, vs);
+            if (pa.on) {
+                CK(launch_pdl(k_front_lu3<T>, 1, LU3_THREADS, sm3, st, (const T *)W, ld, (int)nr, (int)np, (int)F.nri, F.f,
+                              (const double *)N.colmax, pivot_rel, N.rowid + F.row_off, Lf, perm, N.p_lu, N.st, fi, pa));
+                note_launch();
+            } else
+                k_front_lu3<T><<<1, LU3_THREADS, sm3, st>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel,
+                                                            N.rowid + F.row_off, Lf, perm, N.p_lu, N.st, fi, pa), note_launch();
+        } else if (sm <= SMEM_MAX) {
             const int R = (int)((nr + 31) & ~31);
             int nt = 32 + (R <= 128 ? 4 * R : R);   // the pivot warp + the update warps
             if (nt > 640) nt = 640;
