@@ -225,6 +225,71 @@ def traffic_ratio(kernel_class):
     return float(t["dram_to_algorithmic_bytes"]), f"{t['summary']} (ncu dram__bytes_read.sum + dram__bytes_write.sum)"
 
 
+def run_precision_form(stream, dev, g=80, reps=2):
+    """The precision form on the 3D convection-diffusion stencil (g^3 unknowns; g = 80: n = 512,000, the precision
+    configuration): for each Schur-update arithmetic (FP64 = the plain form, FP32 = split TF32 x3, BF16X3, TF32), the
+    device time of the factorization (values resident in HBM) and of the refined solve to a componentwise backward
+    error of 2^-52 (classic refinement, GMRES-IR where it stalls; host right-hand side in and solution out), the normwise
+    backward error, the forward difference from the FP64 solution, and the tensor-core share of the factorization's flops.
+    Timed on the library's stream with CUDA events, median of `reps` after one warm-up each."""
+    import torch
+    import fplus_b200 as F
+    import oracle as O
+    from fplus_b200 import workloads as W
+    t0 = time.perf_counter()
+    n, Ap, Ai, Ax = W.convdiff3d(g, 3)
+    S = F.analyze(n, Ap, Ai)
+    analyze_ms = (time.perf_counter() - t0) * 1e3
+    b = W.rhs(n, 1, False, 2)[0]
+    Ad = torch.from_numpy(Ax).to(dev)
+    out = {"workload": f"3D convection-diffusion 7-point, {g}^3 grid (n={n}, {int(Ap[-1])} entries), float64, nrhs 1",
+           "analyze_ms": round(analyze_ms, 1), "forms": {}}
+    x64 = None
+    names = {F.PREC_FP64: "fp64", F.PREC_FP32: "fp32_split_tf32x3", F.PREC_BF16X3: "bf16x3", F.PREC_TF32: "tf32"}
+    for prec in (F.PREC_FP64, F.PREC_FP32, F.PREC_BF16X3, F.PREC_TF32):
+        rec = {"factor_ms": [], "solve_ms": []}
+        for r in range(reps + 1):
+            torch.cuda.synchronize()
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            N = S.factor(Ad, device=True, precision=prec)
+            e1.record(stream)
+            x, berr, it = N.solve_refine(b, 0, max_iter=40, tol=2.0 ** -52)
+            e2.record(stream)
+            e2.synchronize()
+            if r > 0:
+                rec["factor_ms"].append(e0.elapsed_time(e1))
+                rec["solve_ms"].append(e1.elapsed_time(e2))
+            info = N.info
+            del N
+        f_ms, s_ms = float(np.median(rec["factor_ms"])), float(np.median(rec["solve_ms"]))
+        be = O.backward_error(n, Ap, Ai, Ax, x, b)
+        if prec == F.PREC_FP64:
+            x64 = x.copy()
+        d = {"factor_ms": f_ms, "refined_solve_ms": s_ms, "total_ms": f_ms + s_ms, "corrections": int(it[0]),
+             "berr_componentwise": float(berr[0]), "berr": be,
+             "forward_diff_vs_fp64": float(np.linalg.norm(x - x64) / np.linalg.norm(x64)),
+             "tc_updates": int(info["tc_updates"]), "tc_flop_share": float(info["tc_flops"] / max(info["front_flops"], 1.0)),
+             "front_flops": info["front_flops"], "device_GB": round(info["device_bytes"] / 1e9, 2)}
+        if prec != F.PREC_FP64:
+            # the Schur class's device time in one profiled factorization: the tensor-core updates' algorithmic rate
+            F.profile(True)
+            N = S.factor(Ad, device=True, precision=prec)
+            torch.cuda.synchronize()
+            pr = F.profile_read(0)
+            F.profile(False)
+            del N
+            d["schur_ms"] = pr["ms"]
+            d["schur_tflops_fp64_equivalent"] = pr["flops"] / max(pr["ms"], 1e-9) / 1e9
+        out["forms"][names[prec]] = d
+    base = out["forms"]["fp64"]["total_ms"]
+    for k, v in out["forms"].items():
+        v["speedup_vs_fp64"] = base / v["total_ms"] if v["berr"] <= 1e-14 else None
+    ok = [v["total_ms"] for k, v in out["forms"].items() if k != "fp64" and v["berr"] <= 1e-14]
+    out["best_mixed_speedup_vs_plain"] = base / min(ok) if ok else None
+    return out
+
+
 def run_shift_batch(S, n, modes, count, b):
     """count shifts A - sigma_k B (sigma_k = 0.3 + 1.7i + 0.1 k) of the pencil on its one analysis: factor + solve one by
     one, then through fplus_b200_factor_batch / solve_batch (concurrent).  Host wall time around the synchronous calls."""
@@ -538,6 +603,9 @@ def run_b200_arm(args, rank, world):
     c1_pair = None
     if world == 1 and not args.no_cpu_baseline and __import__("oracle").have_reference():
         c1_pair = run_c1_pair(stream, dev)
+    precision = None
+    if world == 1 and args.precision_grid > 0:
+        precision = run_precision_form(stream, dev, args.precision_grid)
 
     if rank != 0:
         return
@@ -567,7 +635,7 @@ def run_b200_arm(args, rank, world):
                     "d2h_bytes_per_step": n * vsz},
             "gpu_launches": int(launches),
             "clocks": clocks, "roofline": roof, "cpu_baseline": cpu, "solve_nrhs16": solve16, "batch": batch,
-            "batch_pencils": batch_pencils, "c1_pair": c1_pair}
+            "batch_pencils": batch_pencils, "c1_pair": c1_pair, "precision_form": precision}
     print(json.dumps(line))
 
 
@@ -581,6 +649,8 @@ def main():
     ap.add_argument("--modes", type=int, default=8,
                     help="Fourier modes of the pencil workload (8: n = 32768, the benchmark; 1: n = 4096, for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision-grid", type=int, default=80,
+                    help="grid of the 3D stencil of the precision-form measurement (80: n = 512,000; 0: none)")
     ap.add_argument("--batch", type=int, default=8, help="shifts in the batch measurement (0: none)")
     ap.add_argument("--batch-pencils", type=int, default=128,
                     help="independent uneven pencils in the second batch measurement (0: none)")

@@ -59,6 +59,7 @@ FPLUS_H_SYMBOLS = [
     "fplus_factor", "fplus_solve", "fplus_numeric_factors", "fplus_numeric_p", "fplus_numeric_q", "fplus_numeric_Dr",
     "fplus_numeric_Dc", "fplus_numeric_free", "fplus_tri_solve", "fplus_solve_plan_create", "fplus_tri_solve_plan",
     "fplus_solve_plan_nsupernodes", "fplus_solve_plan_free", "fplus_factor_sn_perm", "fplus_factor_sn_sym", "fplus_ruiz",
+    "fplus_factor_sn", "fplus_factor_row", "fplus_factor_row_perm", "fplus_factor_row_sym",
 ]
 FPLUS_B200_H_SYMBOLS = [
     "fplus_b200_numeric_info", "fplus_b200_use_stream", "fplus_b200_factor_dev", "fplus_b200_solve_dev",
@@ -142,6 +143,9 @@ def lib():
            ctypes.c_double, ctypes.c_double, ctypes.POINTER(Factors), _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_factor_sn_perm.argtypes = [ctypes.c_int64, _i64p, _i64p, ctypes.c_void_p, ctypes.c_int, _i64p, _i64p] + _lo
     L.fplus_factor_sn_sym.argtypes = [ctypes.c_void_p, _i64p, _i64p, ctypes.c_void_p, ctypes.c_int] + _lo
+    L.fplus_factor_sn.argtypes = [ctypes.c_int64, _i64p, _i64p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int64,
+                                  ctypes.c_int64, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.POINTER(Factors),
+                                  ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_solve_plan_create.argtypes = [ctypes.c_int64, _i64p, _i64p, _i64p, _i64p, ctypes.POINTER(ctypes.c_void_p),
                                           ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_tri_solve_plan.argtypes = [ctypes.c_void_p, ctypes.c_int64, _i64p, _i64p, ctypes.c_void_p, _i64p, _i64p,

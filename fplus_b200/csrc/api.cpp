@@ -821,6 +821,82 @@ extern "C" int fplus_factor_sn_perm(int64_t n, const int64_t *Ap, const int64_t 
                       use_gpu, gpu_min_flops, pivot_rel, out, Dr, Dc, err, errlen);
 }
 
+// FPLUS include/fplus.h:54-56, src/factor_sn.c:609-660: partial-pivot LU of the matrix as given (no permutation, no
+// equilibration), q the identity.  The input need not be canonical (the reference checks it with canonical = 0): rows are
+// sorted within each column and repeated entries summed (the reference accumulates them when it scatters a column), then
+// the factorization is fplus_factor_sn_perm's on identity orders, so its device factors serve plans on the returned arrays.
+extern "C" int fplus_factor_sn(int64_t n, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex, int verbose,
+                               int64_t relax_rows, int64_t panel, int use_gpu, double gpu_min_flops, double pivot_rel,
+                               fplus_factors *out, char *err, size_t errlen)
+{
+    if (!out) { errf(err, errlen, "out is NULL"); return FPLUS_ERR_BADARG; }
+    std::memset(out, 0, sizeof(*out));
+    if (!(pivot_rel >= 0.0)) { errf(err, errlen, "pivot_rel must be >= 0"); return FPLUS_ERR_BADARG; }
+    int rc = check_compressed(n, Ap, Ai, 0, err, errlen);
+    if (rc != FPLUS_OK) return rc;
+    if (!Ax && Ap[n] > 0) { errf(err, errlen, "NULL argument"); return FPLUS_ERR_BADARG; }
+    if ((rc = check_finite(Ap[n], Ax, is_complex, err, errlen))) return rc;
+    const size_t vs = is_complex ? 16 : 8;
+    try {
+        std::vector<int64_t> Cp((size_t)n + 1, 0), Ci, ord;
+        std::vector<unsigned char> Cx;
+        Ci.reserve((size_t)Ap[n]);
+        Cx.reserve((size_t)Ap[n] * vs);
+        for (int64_t j = 0; j < n; j++) {
+            ord.clear();
+            for (int64_t q = Ap[j]; q < Ap[j + 1]; q++) ord.push_back(q);
+            std::stable_sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) { return Ai[a] < Ai[b]; });
+            for (size_t t = 0; t < ord.size(); t++) {
+                const double *v = (const double *)((const char *)Ax + (size_t)ord[t] * vs);
+                if (t > 0 && Ai[ord[t]] == Ai[ord[t - 1]]) {           // a repeated entry: summed into the previous one
+                    double *w = (double *)(Cx.data() + Cx.size() - vs);
+                    w[0] += v[0];
+                    if (is_complex) w[1] += v[1];
+                    continue;
+                }
+                Ci.push_back(Ai[ord[t]]);
+                Cx.insert(Cx.end(), (const unsigned char *)v, (const unsigned char *)v + vs);
+            }
+            Cp[(size_t)j + 1] = (int64_t)Ci.size();
+        }
+        std::vector<int64_t> id((size_t)(n > 0 ? n : 1));
+        for (int64_t k = 0; k < n; k++) id[(size_t)k] = k;
+        std::vector<double> Dr((size_t)(n > 0 ? n : 1)), Dc((size_t)(n > 0 ? n : 1));
+        return fplus_factor_sn_perm(n, Cp.data(), Ci.data(), Cx.data(), is_complex, id.data(), id.data(), 0, 20, 1e-2, verbose,
+                                    relax_rows, panel, use_gpu, gpu_min_flops, pivot_rel, out, Dr.data(), Dc.data(), err, errlen);
+    } catch (const std::bad_alloc &) {
+        errf(err, errlen, "out of memory");
+        return FPLUS_ERR_NOMEM;
+    }
+}
+
+// FPLUS include/fplus.h:60-62, 139-147: the row kernel (rook / full pivoting, incomplete LU) is not built in this
+// library; these entry points exist so that programs linked against FPLUS resolve, and refuse every call.
+static int row_kernel_absent(fplus_factors *out, char *err, size_t errlen)
+{
+    if (out) std::memset(out, 0, sizeof(*out));
+    errf(err, errlen, "the row kernel (rook / full pivoting, incomplete LU) is not built in this library: use partial "
+                      "pivoting (fplus_factor_sn*, fplus_factor)");
+    return FPLUS_ERR_BADARG;
+}
+extern "C" int fplus_factor_row(int64_t, const int64_t *, const int64_t *, const void *, double, int, int, int, double,
+                                fplus_factors *out, char *err, size_t errlen)
+{
+    return row_kernel_absent(out, err, errlen);
+}
+extern "C" int fplus_factor_row_perm(int64_t, const int64_t *, const int64_t *, const void *, int, const int64_t *,
+                                     const int64_t *, int, int, double, int, double, int, double, fplus_factors *out, double *,
+                                     double *, char *err, size_t errlen)
+{
+    return row_kernel_absent(out, err, errlen);
+}
+extern "C" int fplus_factor_row_sym(const fplus_symbolic *, const int64_t *, const int64_t *, const void *, int, int, int,
+                                    double, int, double, int, double, fplus_factors *out, double *, double *, char *err,
+                                    size_t errlen)
+{
+    return row_kernel_absent(out, err, errlen);
+}
+
 // FPLUS include/fplus.h:130-134, src/pipeline.c:113-127
 extern "C" int fplus_factor_sn_sym(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex,
                                    int equilibrate, int ruiz_max_iter, double ruiz_tol, int verbose, int64_t relax_rows,

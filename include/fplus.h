@@ -57,6 +57,25 @@ void fplus_factors_free(fplus_factors *f);
 
 /* ---- the low-level interface (what FPLUS's Python extension calls: _sparse_lu_c.c:360, 526) ---- */
 
+/* FPLUS include/fplus.h:54-56: the LU with partial pivoting of the matrix as given (no permutation, no equilibration; q
+ * the identity).  The CSC input is checked but need not be sorted: repeated entries of a column are summed.
+ * relax_rows, panel, use_gpu and gpu_min_flops are accepted; the work runs on the GPU as fplus_factor_sn_perm's with
+ * identity orders. */
+int fplus_factor_sn(int64_t n, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex, int verbose,
+                    int64_t relax_rows, int64_t panel, int use_gpu, double gpu_min_flops, double pivot_rel,
+                    fplus_factors *out, char *err, size_t errlen);
+
+/* FPLUS include/fplus.h:60-62, 139-147: the row kernel (full, partial or rook pivoting on CSR input, incomplete LU).  Not
+ * built in this library: every call returns FPLUS_ERR_BADARG with a message (partial pivoting is fplus_factor_sn*). */
+int fplus_factor_row(int64_t n, const int64_t *indptr, const int64_t *indices, const void *data, double drop_tol,
+                     int is_complex, int verbose, int pivot_strategy, double pivot_rel,
+                     fplus_factors *out, char *err, size_t errlen);
+int fplus_factor_row_perm(int64_t n, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex,
+                          const int64_t *row_perm, const int64_t *col_perm,
+                          int equilibrate, int ruiz_max_iter, double ruiz_tol, int verbose,
+                          double drop_tol, int pivot_strategy, double pivot_rel,
+                          fplus_factors *out, double *Dr, double *Dc, char *err, size_t errlen);
+
 /* FPLUS include/fplus.h:64-67: Ruiz L-inf equilibration in place: data (CSR, or CSC when is_csc) becomes
  * diag(Dr) A diag(Dc); Dr, Dc (length n) are filled.  Both routes give the same scalings.  On the GPU. */
 int fplus_ruiz(int64_t n, const int64_t *indptr, const int64_t *indices, void *data, int is_complex, int is_csc,
@@ -122,6 +141,12 @@ int fplus_factor_sn_sym(const fplus_symbolic *sym, const int64_t *Ap, const int6
                         int equilibrate, int ruiz_max_iter, double ruiz_tol, int verbose,
                         int64_t relax_rows, int64_t panel, int use_gpu, double gpu_min_flops, double pivot_rel,
                         fplus_factors *out, double *Dr, double *Dc, char *err, size_t errlen);
+
+/* FPLUS include/fplus.h:144-147: the row kernel on a symbolic analysis's orders; not built (FPLUS_ERR_BADARG) */
+int fplus_factor_row_sym(const fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex,
+                         int equilibrate, int ruiz_max_iter, double ruiz_tol, int verbose,
+                         double drop_tol, int pivot_strategy, double pivot_rel,
+                         fplus_factors *out, double *Dr, double *Dc, char *err, size_t errlen);
 
 /* FPLUS include/fplus.h:92: postorder of the column elimination tree of the m x n CSC pattern; post[k] = the column placed
  * k-th. */
