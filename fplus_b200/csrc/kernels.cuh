@@ -1885,6 +1885,138 @@ __global__ void __launch_bounds__(512) k_chain_bwd(const T *__restrict__ Ua, con
     }
 }
 
+// The backward sweep through the dense chain by blocks of CHB fronts (the fronts [k0, k1), chain indices), two launches
+// per block, the blocks from the last one up.  Rows and columns are relative to the chain's first column f0; front j
+// owns rows [j nb, (j + 1) nb) and its U12 row i, column c sits at Ua[cU_off[j] + i + (c - j nb - nb) nb].
+//   k_chain_diag (one CTA)   for k = k1 - 1 down to k0: y_k -= U[front k rows, columns of fronts (k, k1)] x, then
+//                            x_k = U11_k^-1 y_k (U11 in the top rows of front k's L block, scaled by the reciprocal
+//                            diagonal; a warp per right-hand side, as in k_chain_bwd's last CTA)
+//   k_chain_bulk (full grid) every row above the block: y_r -= U[r, the block's columns] x_block, four lanes per row
+//                            (each a quarter of the columns, 16 loads in flight), combined by shuffles in a fixed order
+// Every entry of U12 in the chain is read once per group of right-hand sides, and the serial part per block is only the
+// block's own triangle.
+constexpr int CHB = 4;
+
+template <typename T>
+__global__ void __launch_bounds__(512) k_chain_diag(const T *__restrict__ Ua, const int64_t *__restrict__ cU_off,
+                                                    const int64_t *__restrict__ cL_off, const int64_t *__restrict__ cnrow,
+                                                    const T *__restrict__ La, int64_t f0, int64_t nb, int64_t k0, int64_t k1,
+                                                    int64_t ncols_chain, T *__restrict__ Y, T *__restrict__ X, int64_t n,
+                                                    int64_t nrhs, DevStatus *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *s = reinterpret_cast<T *>(smem_raw);          // nb x nrhs: y_k
+    T *dinv = s + nb * nrhs;                          // nb
+    T *sU = dinv + nb;                                // nb x nb: sU[j + i * nb] = U[j, i] / U[i, i]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    pdl_wait();
+    pdl_trigger();
+    if (st->code) return;
+    for (int64_t k = k1 - 1; k >= k0; k--) {
+        const int64_t fk = k * nb, npk = (fk + nb <= ncols_chain ? nb : ncols_chain - fk);
+        const T *Lk = La + cL_off[k];
+        const int64_t nrk = cnrow[k];
+        // the rows of front k against the block's solved columns after it, (k, k1): four lanes per row
+        const int64_t ca = fk + nb, cb = (k1 * nb < ncols_chain ? k1 * nb : ncols_chain), nc = cb > ca ? cb - ca : 0;
+        if (nc > 0) {
+            const int64_t tot = (npk * 4 + 31) / 32 * 32;     // whole warps: every lane takes part in the shuffles
+            for (int64_t e = tid; e < tot; e += blockDim.x) {
+                const bool on = e < npk * 4;
+                const int64_t i = on ? e >> 2 : 0;
+                const int qq = (int)(e & 3);
+                const T *u = Ua + cU_off[k] + i;
+                for (int64_t r = 0; r < nrhs; r++) {
+                    T acc = VT<T>::zero();
+                    if (on)
+                        for (int64_t c = ca + qq; c < cb; c += 4) acc = add(acc, mul(u[(c - fk - nb) * nb], X[f0 + c + r * n]));
+                    acc = add(acc, shfl_xor_v<T>(acc, 1));
+                    acc = add(acc, shfl_xor_v<T>(acc, 2));
+                    if (on && qq == 0) { T *y = Y + f0 + fk + i + r * n; *y = sub(*y, acc); }
+                }
+            }
+            __syncthreads();
+        }
+        // x_k = U11^-1 y_k
+        for (int e = tid; e < npk * npk; e += blockDim.x) sU[e] = Lk[(e % npk) + (int64_t)(e / npk) * nrk];
+        for (int64_t e = tid; e < npk * nrhs; e += blockDim.x) s[e] = Y[f0 + fk + e % npk + (e / npk) * n];
+        for (int i = tid; i < npk; i += blockDim.x) {
+            const T d = Lk[i + (int64_t)i * nrk];
+            if (is_zero(d)) set_status(st, ST_SOLVE_ZERO, f0 + fk + i, 0, 0);
+            dinv[i] = is_zero(d) ? VT<T>::zero() : recip(d);
+        }
+        __syncthreads();
+        if (st->code == ST_SOLVE_ZERO) return;
+        for (int e = tid; e < npk * npk; e += blockDim.x) sU[e] = mul(sU[e], dinv[e / npk]);
+        __syncthreads();
+        for (int64_t r = warp; r < nrhs; r += nw) {
+            T a = lane < npk ? s[lane + r * npk] : VT<T>::zero();
+            T b = lane + 32 < npk ? s[lane + 32 + r * npk] : VT<T>::zero();
+            for (int ii = (int)npk - 1; ii >= 0; ii--) {
+                const T *col = sU + ii * npk;
+                const T si = shfl_v<T>(ii < 32 ? a : b, ii & 31);
+                if (ii >= 32) {
+                    if (lane < ii - 32) b = sub(b, mul(col[lane + 32], si));
+                    a = sub(a, mul(col[lane], si));
+                } else if (lane < ii) a = sub(a, mul(col[lane], si));
+            }
+            if (lane < npk) X[f0 + fk + lane + r * n] = mul(a, dinv[lane]);
+            if (lane + 32 < npk) X[f0 + fk + lane + 32 + r * n] = mul(b, dinv[lane + 32]);
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_chain_bulk(const T *__restrict__ Ua, const int64_t *__restrict__ cU_off, int64_t f0,
+                                                    int64_t nb, int64_t k0, int64_t k1, int64_t ncols_chain,
+                                                    T *__restrict__ Y, const T *__restrict__ X, int64_t n, int64_t nrhs)
+{
+    constexpr int RB = 8;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *xs = reinterpret_cast<T *>(smem_raw);          // the block's x: column c (relative) of rhs t at c + t * nc
+    const int tid = threadIdx.x, lane = tid & 31, q = lane & 3;
+    const int64_t ca = k0 * nb, cb = (k1 * nb < ncols_chain ? k1 * nb : ncols_chain), nc = cb - ca;
+    const int64_t R = k0 * nb;                        // every row above the block
+    pdl_wait();
+    pdl_trigger();
+    for (int64_t e = tid; e < nc * nrhs; e += blockDim.x) xs[e] = X[f0 + ca + e % nc + (e / nc) * n];
+    __syncthreads();
+    const int64_t r = blockIdx.x * (int64_t)(blockDim.x >> 2) + (tid >> 2);
+    const bool on = r < R;
+    const int64_t j = on ? r / nb : 0, i = on ? r % nb : 0;
+    const T *u = Ua + (on ? cU_off[j] : 0) + i + (ca - j * nb - nb) * nb;      // U12_j[i, column ca]
+    for (int64_t r0 = 0; r0 < nrhs; r0 += RB) {
+        const int rb = nrhs - r0 < RB ? (int)(nrhs - r0) : RB;
+        T acc[RB];
+#pragma unroll
+        for (int t = 0; t < RB; t++) acc[t] = VT<T>::zero();
+        if (on) {
+            for (int64_t c0 = q * 16; c0 < nc; c0 += 64) {
+                T uv[16];
+#pragma unroll
+                for (int c = 0; c < 16; c++) uv[c] = c0 + c < nc ? u[(c0 + c) * nb] : VT<T>::zero();
+#pragma unroll
+                for (int c = 0; c < 16; c++) {
+                    if (c0 + c >= nc) break;
+#pragma unroll
+                    for (int t = 0; t < RB; t++)
+                        if (t < rb) acc[t] = add(acc[t], mul(uv[c], xs[c0 + c + (r0 + t) * nc]));
+                }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < RB; t++) {
+            acc[t] = add(acc[t], shfl_xor_v<T>(acc[t], 1));
+            acc[t] = add(acc[t], shfl_xor_v<T>(acc[t], 2));
+        }
+        if (on && q == 0) {
+#pragma unroll
+            for (int t = 0; t < RB; t++)
+                if (t < rb) { T *y = Y + f0 + r + (r0 + t) * n; *y = sub(*y, acc[t]); }
+        }
+    }
+}
+
 // transposed solves: forward with U^T (U^H when conj) through one front, step 1 (one CTA): z = U11^-T w[f ..] by a warp
 // per right-hand side
 template <typename T, bool CJ>

@@ -87,7 +87,8 @@ template <typename T> static int upload(const std::vector<T> &h, T **d, char *er
 DevPlan::~DevPlan()
 {
     for (void *p : {(void *)cols, (void *)relcol, (void *)rowinit, (void *)asm_src, (void *)asm_dst, (void *)Bp, (void *)Bi,
-                    (void *)Bsrc, (void *)row_perm, (void *)col_perm, (void *)seg, (void *)chain_uoff})
+                    (void *)Bsrc, (void *)row_perm, (void *)col_perm, (void *)seg, (void *)chain_uoff, (void *)chain_loff,
+                    (void *)chain_nrow})
         if (p) cudaFree(p);
 }
 
@@ -124,17 +125,21 @@ int dev_upload_plan(const fplus_symbolic *S, const FrontPlan &P, DevPlan &D, cha
         int64_t c0 = nf;
         while (c0 > 0 && P.fronts[c0 - 1].dense) c0--;
         bool ok = nf - c0 >= 2 && nb > 0 && nb <= 64;
-        std::vector<int64_t> uoff;
+        std::vector<int64_t> uoff, loff, nrow;
         for (int64_t j = c0; ok && j < nf; j++) {
             const Front &F = P.fronts[j];
             const bool lastf = j == nf - 1;
             ok = F.f == P.fronts[c0].f + (j - c0) * nb && (lastf ? F.npiv <= nb : F.npiv == nb) && F.npiv <= F.nrows &&
                  F.ncols == S->n - F.f;
             uoff.push_back(F.U_off);
+            loff.push_back(F.L_off);
+            nrow.push_back(F.nrows);
         }
         if (ok) {
             D.chain_begin = c0; D.chain_nb = nb; D.chain_f0 = P.fronts[c0].f;
             if ((rc = upload(uoff, &D.chain_uoff, err, errlen))) return rc;
+            if ((rc = upload(loff, &D.chain_loff, err, errlen))) return rc;
+            if ((rc = upload(nrow, &D.chain_nrow, err, errlen))) return rc;
         }
     }
     return FPLUS_OK;
@@ -739,17 +744,27 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
             const int64_t cb = D.chain_begin, nb = D.chain_nb;
             const size_t csm = std::max((size_t)(nb + (nb + 15) / 16) * nrhs, (size_t)(nb * (nrhs + 1) + nb * nb)) * sizeof(T);
             if (csm > 48 * 1024) CK(cudaFuncSetAttribute(k_chain_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
-            for (int64_t fi = nf - 1; fi >= cb; fi--) {
-                const Front &F = P.fronts[fi];
-                const int64_t jk1 = fi + 1 < nf ? fi + 1 - cb : -1;
-                const int npk1 = jk1 >= 0 ? (int)P.fronts[fi + 1].npiv : 0;
-                const int64_t rows = jk1 >= 0 ? jk1 * nb : 0;
-                const int cbt = nrhs > 8 ? 512 : 256;      // a warp per right-hand side in the U11 sweep
-                const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((rows + cbt / 4 - 1) / (cbt / 4), 296));
-                CK(launch_pdl(k_chain_bwd<T>, grid, cbt, csm, s, Ua, D.chain_uoff, D.chain_f0, nb, jk1, npk1, La + F.L_off,
-                              F.nrows, F.f, (int)F.npiv, S2, R, n, nrhs, N.st));
+            // blocks of CHB fronts from the last: the block's own triangle on one CTA (k_chain_diag), then every row above
+            // it against the block's columns on the whole GPU (k_chain_bulk)
+            const int64_t nch = nf - cb, ncc = n - D.chain_f0;
+            const size_t dsm = (size_t)(nb * (nrhs + 1) + nb * nb) * sizeof(T);
+            const size_t bsm = (size_t)(CHB * nb) * (size_t)nrhs * sizeof(T);
+            CK(cudaFuncSetAttribute(k_chain_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(dsm, (size_t)48 * 1024)));
+            CK(cudaFuncSetAttribute(k_chain_bulk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(bsm, (size_t)48 * 1024)));
+            for (int64_t k1 = nch; k1 > 0; k1 -= CHB) {
+                const int64_t k0 = std::max<int64_t>(0, k1 - CHB);
+                CK(launch_pdl(k_chain_diag<T>, 1, 512, dsm, s, (const T *)Ua, (const int64_t *)D.chain_uoff,
+                              (const int64_t *)D.chain_loff, (const int64_t *)D.chain_nrow, (const T *)La, D.chain_f0, nb, k0, k1,
+                              ncc, S2, R, n, nrhs, N.st));
                 note_launch();
+                if (k0 > 0) {
+                    const int64_t rows = k0 * nb;
+                    CK(launch_pdl(k_chain_bulk<T>, (int)((rows + 63) / 64), 256, bsm, s, (const T *)Ua, (const int64_t *)D.chain_uoff,
+                                  D.chain_f0, nb, k0, k1, ncc, S2, (const T *)R, n, nrhs));
+                    note_launch();
+                }
             }
+            (void)csm;
             fi_end = cb;
         }
         for (int64_t fi = fi_end - 1; fi >= 0; fi--) {

@@ -34,6 +34,7 @@ struct DevPlan {
     // (the last one at most), first column chain_f0, their U offsets; chain_begin < 0 when the fronts do not qualify
     int64_t chain_begin = -1, chain_nb = 0, chain_f0 = 0;
     int64_t *chain_uoff = nullptr;
+    int64_t *chain_loff = nullptr, *chain_nrow = nullptr;     // each chain front's L block (U11 in its top rows), rows
     ~DevPlan();
 };
 
