@@ -290,58 +290,83 @@ def run_precision_form(stream, dev, g=80, reps=2):
     return out
 
 
-def run_shift_batch(S, n, modes, count, b):
-    """count shifts A - sigma_k B (sigma_k = 0.3 + 1.7i + 0.1 k) of the pencil on its one analysis: factor + solve one by
-    one, then through fplus_b200_factor_batch / solve_batch (concurrent).  Host wall time around the synchronous calls."""
+def run_shift_batch(S, n, modes, count, b, wave=8):
+    """count shifts A - sigma_k B (sigma_k = 0.3 + 1.7i + 0.1 k) of the benchmark pencil on its one analysis, nrhs 1:
+    factored and solved through fplus_b200_factor_batch / solve_batch in waves of `wave` matrices (each factorization of
+    this pencil holds about 9 GB of device memory), against the same calls one matrix at a time on the first `wave`
+    shifts.  Device time: fplus_b200_batch_span_ms (CUDA events on the jobs' own streams, from the first factorization's
+    start to the last solve's end), summed over the waves."""
     import fplus_b200 as F
     import oracle as O
     from fplus_b200 import workloads as W
     _, Ap, Ai, A0 = W.pencil(modes=modes, sigma=0.0)
     Bv = A0 - W.pencil(modes=modes, sigma=1.0)[3]           # B's values on A's pattern (the pencil is linear in sigma)
-    Axs = [A0 - (0.3 + 1.7j + 0.1 * k) * Bv for k in range(count)]
-    t0 = time.perf_counter()
-    for Ax in Axs:
-        N = S.factor(Ax)
+    sig = [0.3 + 1.7j + 0.1 * k for k in range(count)]
+    seq = []
+    for k in range(min(wave, count) + 1):
+        N = S.factor(A0 - sig[k % count] * Bv)
         N.solve(b)
+        if k > 0:                                        # the first one warms up
+            seq.append(F.batch_span_ms([N]))
         del N
-    seq = (time.perf_counter() - t0) * 1e3
-    F.solve_batch(F.factor_batch([S] * 2, Axs[:2]), [b, b])          # warm-up of the worker path
-    t0 = time.perf_counter()
-    Ns = F.factor_batch([S] * count, Axs, nworkers=count)
-    Xs = F.solve_batch(Ns, [b] * count, nworkers=count)
-    par = (time.perf_counter() - t0) * 1e3
-    be = max(O.backward_error(n, Ap, Ai, Axs[k], Xs[k], b) for k in range(count))
-    return {"workload": f"{count} shifts sigma_k = 0.3+1.7i+0.1k of the pencil, one analysis, nrhs 1",
-            "ms_per_matrix": par / count, "sequential_ms_per_matrix": seq / count, "speedup": seq / par,
-            "berr_max": be, "timing": "host wall clock around the synchronous fplus calls (host values, e2e)"}
+    F.solve_batch(F.factor_batch([S] * 2, [A0 - sig[0] * Bv, A0 - sig[1] * Bv]), [b, b])     # warm-up of the workers
+    spans, be, wall = [], 0.0, 0.0
+    for w0 in range(0, count, wave):
+        ks = list(range(w0, min(count, w0 + wave)))
+        Axs = [A0 - sig[k] * Bv for k in ks]
+        t0 = time.perf_counter()
+        Ns = F.factor_batch([S] * len(ks), Axs, nworkers=len(ks))
+        Xs = F.solve_batch(Ns, [b] * len(ks), nworkers=len(ks))
+        wall += time.perf_counter() - t0
+        spans.append(F.batch_span_ms(Ns))
+        be = max(be, max(O.backward_error(n, Ap, Ai, Axs[i], Xs[i], b) for i in range(len(ks))))
+        del Ns
+    dev = float(sum(spans))
+    one = float(np.median(seq))
+    return {"workload": f"{count} shifts sigma_k = 0.3+1.7i+0.1k of the benchmark pencil (n={n}), one analysis, nrhs 1, "
+                        f"in waves of {wave}", "device_ms_total": dev, "device_ms_per_matrix": dev / count,
+            "one_by_one_device_ms_per_matrix": one, "speedup_per_matrix": one / (dev / count), "berr_max": be,
+            "host_wall_ms_total": wall * 1e3,
+            "timing": "CUDA events on the jobs' streams (fplus_b200_batch_span_ms); values and right-hand sides from host memory"}
 
 
-def run_pencil_batch(count, nworkers=16):
+def run_pencil_batch(count, nworkers=32):
     """count independent pencils of uneven size (n log-uniform in [500, 8000], 2-4 dense tau rows / columns), 8
-    right-hand sides each: analysed once each, then factored and solved one by one and through fplus_b200_factor_batch /
-    solve_batch.  Host wall time around the synchronous calls."""
+    right-hand sides each: analysed once each (not timed), then factored and solved one by one and through
+    fplus_b200_factor_batch / solve_batch.  Device time from CUDA events on the jobs' own streams
+    (fplus_b200_batch_span_ms); the one-by-one figure is the sum of each matrix's own span."""
+    from concurrent.futures import ThreadPoolExecutor
     import fplus_b200 as F
     import oracle as O
     from fplus_b200 import workloads as W
     mats = W.pencil_batch(count=count)
-    syms = [F.analyze(m[0], m[1], m[2]) for m in mats]
+    with ThreadPoolExecutor(16) as ex:
+        syms = list(ex.map(lambda m: F.analyze(m[0], m[1], m[2]), mats))
     rhs = [W.rhs(m[0], 8, True, 7 + k).T.copy(order="F") for k, m in enumerate(mats)]
-    F.solve_batch(F.factor_batch(syms[:4], [m[3] for m in mats[:4]]), rhs[:4])        # warm-up
+    F.solve_batch(F.factor_batch(syms[:4], [m[3] for m in mats[:4]]), rhs[:4])        # warm-up (and the dense-chain starts)
+    # every pattern factored once, so that a restart for a dense-row pivot is not part of either timing
+    for S, m in zip(syms, mats):
+        S.factor(m[3])
+    seq = 0.0
     t0 = time.perf_counter()
     for S, m, b in zip(syms, mats, rhs):
         N = S.factor(m[3])
         N.solve(b)
+        seq += F.batch_span_ms([N])
         del N
-    seq = (time.perf_counter() - t0) * 1e3
+    seq_wall = (time.perf_counter() - t0) * 1e3
     t0 = time.perf_counter()
     Ns = F.factor_batch(syms, [m[3] for m in mats], nworkers=nworkers)
     Xs = F.solve_batch(Ns, rhs, nworkers=nworkers)
-    par = (time.perf_counter() - t0) * 1e3
+    wall = (time.perf_counter() - t0) * 1e3
+    dev = F.batch_span_ms(Ns)
     be = max(O.backward_error(m[0], m[1], m[2], m[3], X[:, r], b[:, r]) for m, X, b in zip(mats, Xs, rhs) for r in (0, 7))
     ns = [m[0] for m in mats]
-    return {"workload": f"{count} pencils, n log-uniform in [500, 8000] (sum {sum(ns)}), 8 right-hand sides each",
-            "ms_total": par, "sequential_ms_total": seq, "speedup": seq / par, "berr_max": be, "workers": nworkers,
-            "timing": "host wall clock around the synchronous fplus calls (host values, e2e); analysis excluded"}
+    return {"workload": f"{count} pencils, n log-uniform in [500, 8000] (sum {sum(ns)}), complex128, 8 right-hand sides each",
+            "device_ms_total": dev, "one_by_one_device_ms_total": seq, "speedup": seq / dev, "berr_max": be,
+            "workers": nworkers, "host_wall_ms_total": wall, "one_by_one_host_wall_ms_total": seq_wall,
+            "timing": "CUDA events on the jobs' streams (fplus_b200_batch_span_ms); analysis excluded; values and right-hand "
+                      "sides from host memory"}
 
 
 def run_reference_arm(args, rank, world):
@@ -651,8 +676,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision-grid", type=int, default=80,
                     help="grid of the 3D stencil of the precision-form measurement (80: n = 512,000; 0: none)")
-    ap.add_argument("--batch", type=int, default=8, help="shifts in the batch measurement (0: none)")
-    ap.add_argument("--batch-pencils", type=int, default=128,
+    ap.add_argument("--batch", type=int, default=64, help="shifts of the pencil in the batch measurement (0: none)")
+    ap.add_argument("--batch-pencils", type=int, default=512,
                     help="independent uneven pencils in the second batch measurement (0: none)")
     ap.add_argument("--profile-once", action="store_true",
                     help="for ncu --profile-from-start off: one warm factorization, then exactly one factor + solve "

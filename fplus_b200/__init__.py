@@ -66,7 +66,7 @@ FPLUS_B200_H_SYMBOLS = [
     "fplus_b200_interior_order", "fplus_b200_plan_size", "fplus_b200_plan_export", "fplus_b200_launch_count",
     "fplus_b200_profile", "fplus_b200_profile_read", "fplus_b200_solve_dev_noalloc", "fplus_b200_factor_batch",
     "fplus_b200_solve_batch", "fplus_b200_solve_refine", "fplus_b200_symbolic_from_orders", "fplus_b200_factor_norms",
-    "fplus_b200_factor_prec", "fplus_b200_schur_update",
+    "fplus_b200_factor_prec", "fplus_b200_schur_update", "fplus_b200_batch_span_ms",
 ]
 
 _lib = None
@@ -135,6 +135,7 @@ def lib():
                                           ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                           ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                           ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_b200_batch_span_ms.argtypes = [ctypes.c_int64, ctypes.c_void_p, _dp, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_factor_norms.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_solve_refine.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_double, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p,
@@ -441,6 +442,15 @@ def solve_batch(nums, bs, trans=0, nworkers=8):
                                       I64(*[X.shape[1] for X in Xs]), I64(*[N.n for N in nums]), trans, nworkers, rcs, err, 512)
     _check(rc, err)
     return [X[:, 0] if np.asarray(b).ndim == 1 else X for X, b in zip(Xs, bs)]
+
+
+def batch_span_ms(nums):
+    """fplus_b200_batch_span_ms: the device time from the first factorization's start to the last solve's end."""
+    arr = (ctypes.c_void_p * len(nums))(*[N._h.value for N in nums])
+    ms = ctypes.c_double()
+    err = ctypes.create_string_buffer(512)
+    _check(lib().fplus_b200_batch_span_ms(len(nums), arr, ctypes.byref(ms), err, 512), err)
+    return ms.value
 
 
 def interior_order(n, Ap, Ai, trow=None, tcol=None):

@@ -129,6 +129,7 @@ static int factor_common(const fplus_symbolic *sym, const int64_t *Ap, const int
         N.prec = prec;
         rc = dev_num_init(N, n, sym->nnz, num->is_complex, err, errlen);
         if (rc) return rc;
+        CKH(cudaEventRecord(N.ev_begin, N.stream));
         const size_t bytes = (size_t)sym->nnz * (size_t)N.vs;
         if (bytes) CKH(cudaMemcpyAsync(N.Ax, Ax, bytes, ax_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, N.stream));
         std::shared_ptr<FrontPlan> P;
@@ -300,12 +301,36 @@ static int solve_common(const fplus_numeric *num, void *b, int64_t nrhs, int64_t
         if (e != cudaSuccess) { errf(err, errlen, "CUDA: %s", cudaGetErrorString(e)); rc = FPLUS_ERR_GPU; break; }
     }
     if (rc == FPLUS_OK) {
+        cudaEventRecord(N.ev_done, N.stream);
         int code = 0; int64_t idx = 0;
         rc = dev_status(N, &code, &idx, err, errlen);
         if (rc == FPLUS_OK && code != 0) { errf(err, errlen, "fplus_solve: zero or missing diagonal in U"); rc = FPLUS_ERR_SINGULAR; }
     }
     N.stream = saved;
     return rc;
+}
+
+// the device time from the earliest factorization start to the latest solve end over a batch (events on the jobs' own
+// streams, read after they have completed)
+extern "C" int fplus_b200_batch_span_ms(int64_t count, fplus_numeric *const *nums, double *ms, char *err, size_t errlen)
+{
+    if (!nums || !ms || count < 1) { errf(err, errlen, "bad arguments"); return FPLUS_ERR_BADARG; }
+    cudaEvent_t ref = nullptr;
+    double lo = 0, hi = 0;
+    for (int64_t k = 0; k < count; k++) {
+        if (!nums[k] || !nums[k]->dev) { errf(err, errlen, "matrix %ld: no factorization", (long)k); return FPLUS_ERR_BADARG; }
+        DevNum &N = *nums[k]->dev;
+        CKH(cudaEventSynchronize(N.ev_begin));
+        CKH(cudaEventSynchronize(N.ev_done));
+        if (!ref) ref = N.ev_begin;
+        float a = 0, b = 0;
+        CKH(cudaEventElapsedTime(&a, ref, N.ev_begin));
+        CKH(cudaEventElapsedTime(&b, ref, N.ev_done));
+        if (k == 0 || a < lo) lo = a;
+        if (k == 0 || b > hi) hi = b;
+    }
+    *ms = hi - lo;
+    return FPLUS_OK;
 }
 
 // ---------------------------------------------------------------------------------------------------------------------

@@ -156,6 +156,8 @@ DevNum::~DevNum()
         if (p) cudaFreeAsync(p, stream);
     if (stream) cudaStreamSynchronize(stream);
     if (crit) cudaStreamSynchronize(crit);
+    if (ev_begin) cudaEventDestroy(ev_begin);
+    if (ev_done) cudaEventDestroy(ev_done);
     if (ev_lu) cudaEventDestroy(ev_lu);
     if (ev_head) cudaEventDestroy(ev_head);
     if (crit) cudaStreamDestroy(crit);
@@ -208,6 +210,8 @@ int dev_num_init(DevNum &N, int64_t n, int64_t nnz, int cplx, char *err, size_t 
     if (!N.stream) { CK(cudaStreamCreateWithFlags(&N.stream, cudaStreamNonBlocking)); N.stream_owned = true; }
     CK(cudaEventCreate(&N.ev0));
     CK(cudaEventCreate(&N.ev1));
+    CK(cudaEventCreate(&N.ev_begin));
+    CK(cudaEventCreate(&N.ev_done));
     const size_t nn = (size_t)(n > 0 ? n : 1), nz = (size_t)(nnz > 0 ? nnz : 1);
     cudaStream_t s = N.stream;
     CK(cudaMallocAsync((void **)&N.Ax, nz * N.vs, s));

@@ -47,6 +47,7 @@ struct DevNum {
     cudaStream_t stream = nullptr;
     bool stream_owned = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev_begin = nullptr, ev_done = nullptr;   // the first operation of the factorization, the end of the last solve
     void *Ax = nullptr, *Bx = nullptr;
     double *Drp = nullptr, *Dcp = nullptr, *colmax = nullptr;
     void *Larena = nullptr, *Uarena = nullptr, *cbstack = nullptr, *work = nullptr;

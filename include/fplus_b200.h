@@ -114,6 +114,10 @@ int fplus_b200_solve_batch(int64_t count, fplus_numeric *const *nums, void *cons
  * FPLUS; it lets a caller check factors too large to read back to the host (for instance against a stored oracle). */
 int fplus_b200_factor_norms(const fplus_numeric *num, double *L_fro, double *U_fro, char *err, size_t errlen);
 
+/* The device time of a batch: from the earliest start of the factorizations nums[0 .. count) (their first operation) to
+ * the latest end of their last solves, from CUDA events on their own streams (no host timing).  No counterpart in FPLUS. */
+int fplus_b200_batch_span_ms(int64_t count, fplus_numeric *const *nums, double *ms, char *err, size_t errlen);
+
 /* fplus_b200_solve_dev for callers that cannot allocate device memory.  No counterpart in the reference (FPLUS has no GPU
  * solve).  Some callers may not call cudaMalloc at solve time: code running inside another runtime that owns the device
  * memory (a framework's custom operator given only its input and output buffers), latency-critical loops in which an
