@@ -66,7 +66,9 @@ FPLUS_B200_H_SYMBOLS = [
     "fplus_b200_interior_order", "fplus_b200_plan_size", "fplus_b200_plan_export", "fplus_b200_launch_count",
     "fplus_b200_profile", "fplus_b200_profile_read", "fplus_b200_solve_dev_noalloc", "fplus_b200_factor_batch",
     "fplus_b200_solve_batch", "fplus_b200_solve_refine", "fplus_b200_symbolic_from_orders", "fplus_b200_factor_norms",
-    "fplus_b200_factor_prec", "fplus_b200_schur_update", "fplus_b200_batch_span_ms",
+    "fplus_b200_factor_prec", "fplus_b200_schur_update", "fplus_b200_batch_span_ms", "fplus_b200_graph_create",
+    "fplus_b200_graph_values", "fplus_b200_graph_rhs", "fplus_b200_graph_launch", "fplus_b200_graph_status",
+    "fplus_b200_graph_free", "fplus_b200_graph_upload", "fplus_b200_graph_download",
 ]
 
 _lib = None
@@ -135,6 +137,17 @@ def lib():
                                           ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                           ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                           ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_b200_graph_create.argtypes = [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_void_p), ctypes.c_char_p, ctypes.c_size_t]
+    for f in ("fplus_b200_graph_values", "fplus_b200_graph_rhs"):
+        getattr(L, f).argtypes = [ctypes.c_void_p, ctypes.c_int64]
+        getattr(L, f).restype = ctypes.c_void_p
+    L.fplus_b200_graph_launch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_b200_graph_status.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_b200_graph_free.argtypes = [ctypes.c_void_p]
+    L.fplus_b200_graph_upload.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p,
+                                          ctypes.c_size_t]
+    L.fplus_b200_graph_download.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_batch_span_ms.argtypes = [ctypes.c_int64, ctypes.c_void_p, _dp, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_factor_norms.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_solve_refine.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
@@ -442,6 +455,52 @@ def solve_batch(nums, bs, trans=0, nworkers=8):
                                       I64(*[X.shape[1] for X in Xs]), I64(*[N.n for N in nums]), trans, nworkers, rcs, err, 512)
     _check(rc, err)
     return [X[:, 0] if np.asarray(b).ndim == 1 else X for X, b in zip(Xs, bs)]
+
+
+class BatchGraph:
+    """fplus_b200_graph_*: the refactorization and solve of many factored matrices captured as one CUDA graph.  The
+    Numeric objects must outlive the graph (it keeps references)."""
+
+    def __init__(self, nums, nrhs, trans=0):
+        self.nums = list(nums)
+        self.nrhs = [int(r) for r in (nrhs if hasattr(nrhs, "__len__") else [nrhs] * len(self.nums))]
+        self._h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        arr = (ctypes.c_void_p * len(self.nums))(*[N._h.value for N in self.nums])
+        nr = (ctypes.c_int64 * len(self.nums))(*self.nrhs)
+        _check(lib().fplus_b200_graph_create(len(self.nums), arr, nr, int(trans), ctypes.byref(self._h), err, 512), err)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None and self._h.value:
+            _lib.fplus_b200_graph_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def upload(self, k, Ax=None, b=None):
+        N = self.nums[k]
+        dt = np.complex128 if N.is_complex else np.float64
+        a = None if Ax is None else np.ascontiguousarray(Ax, dtype=dt)
+        bb = None if b is None else np.asfortranarray(np.asarray(b, dtype=dt).reshape(N.n, -1))
+        err = ctypes.create_string_buffer(512)
+        _check(lib().fplus_b200_graph_upload(self._h, k, None if a is None else a.ctypes.data_as(ctypes.c_void_p),
+                                             None if bb is None else bb.ctypes.data_as(ctypes.c_void_p), err, 512), err)
+
+    def launch(self, stream=None):
+        err = ctypes.create_string_buffer(512)
+        _check(lib().fplus_b200_graph_launch(self._h, None if stream is None else ctypes.c_void_p(stream), err, 512), err)
+
+    def status(self):
+        """Waits for the graph; the per-matrix codes (0, FPLUS_ERR_SINGULAR, FPLUS_ERR_BADARG, FPLUS_ERR_GPU)."""
+        rcs = (ctypes.c_int * len(self.nums))()
+        err = ctypes.create_string_buffer(512)
+        lib().fplus_b200_graph_status(self._h, rcs, err, 512)
+        return list(rcs)
+
+    def download(self, k):
+        N = self.nums[k]
+        X = np.zeros((N.n, self.nrhs[k]), dtype=np.complex128 if N.is_complex else np.float64, order="F")
+        err = ctypes.create_string_buffer(512)
+        _check(lib().fplus_b200_graph_download(self._h, k, X.ctypes.data_as(ctypes.c_void_p), err, 512), err)
+        return X
 
 
 def batch_span_ms(nums):

@@ -31,6 +31,8 @@ struct fplus_numeric {
     std::vector<int64_t> p, q, p_lu;
     std::vector<double> Dr, Dc, Drp, Dcp;
     fplus_b200_info info{};
+    int equilibrate = 1, ruiz_max_iter = 20;   // the options the factorization ran with (a captured refactorization reuses them)
+    double ruiz_tol = 1e-2, pivot_rel = 0.0;
     mutable std::mutex mu;               // solves and the lazy host factors share the device buffers
     mutable bool have_host = false;
     mutable fplus_factors f{};
@@ -123,6 +125,8 @@ static int factor_common(const fplus_symbolic *sym, const int64_t *Ap, const int
     std::unique_ptr<fplus_numeric> guard(num);
     try {
         num->n = n; num->is_complex = is_complex ? 1 : 0;
+        num->equilibrate = opt->equilibrate; num->ruiz_max_iter = opt->ruiz_max_iter; num->ruiz_tol = opt->ruiz_tol;
+        num->pivot_rel = opt->pivot_rel;
         num->dev.reset(new DevNum);
         DevNum &N = *num->dev;
         if (tl_stream) N.stream = tl_stream;
@@ -309,6 +313,168 @@ static int solve_common(const fplus_numeric *num, void *b, int64_t nrhs, int64_t
     N.stream = saved;
     return rc;
 }
+
+// ---------------------------------------------------------------------------------------------------------------------
+// The batch form as one CUDA graph: the refactorization (new values on the same patterns) and solve of many matrices,
+// captured once from their own launch sequences and replayed.  Each matrix's work is captured on its own stream, forked
+// from and joined to a capture stream, so the graph's branches are independent and run concurrently.
+struct fplus_b200_graph {
+    std::vector<fplus_numeric *> nums;
+    std::vector<int64_t> nrhs;
+    std::vector<void *> rhs;                 // n x nrhs[k] device buffers
+    int trans = 0;
+    int device = 0;
+    cudaStream_t s0 = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> joins;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t launched = nullptr;
+    ~fplus_b200_graph()
+    {
+        cudaSetDevice(device);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (auto e : joins) if (e) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        for (void *p : rhs) if (p) cudaFree(p);
+        if (s0) cudaStreamDestroy(s0);
+    }
+};
+
+extern "C" int fplus_b200_graph_create(int64_t count, fplus_numeric *const *nums, const int64_t *nrhs, int trans,
+                                       fplus_b200_graph **out, char *err, size_t errlen)
+{
+    if (!out) { errf(err, errlen, "graph is NULL"); return FPLUS_ERR_BADARG; }
+    *out = nullptr;
+    if (count < 1 || !nums || !nrhs || trans < 0 || trans > 2) { errf(err, errlen, "bad arguments"); return FPLUS_ERR_BADARG; }
+    std::unique_ptr<fplus_b200_graph> g(new (std::nothrow) fplus_b200_graph);
+    if (!g) { errf(err, errlen, "out of memory"); return FPLUS_ERR_NOMEM; }
+    g->trans = trans;
+    for (int64_t k = 0; k < count; k++) {
+        if (!nums[k] || !nums[k]->dev || nrhs[k] < 1) { errf(err, errlen, "matrix %ld: no factorization or nrhs < 1", (long)k); return FPLUS_ERR_BADARG; }
+        if (k > 0 && nums[k]->dev->device != nums[0]->dev->device) { errf(err, errlen, "the matrices are on different devices"); return FPLUS_ERR_BADARG; }
+        for (int64_t j = 0; j < k; j++) if (nums[j] == nums[k]) { errf(err, errlen, "matrix %ld appears twice", (long)k); return FPLUS_ERR_BADARG; }
+    }
+    g->device = nums[0]->dev->device;
+    CKH(cudaSetDevice(g->device));
+    CKH(cudaStreamCreateWithFlags(&g->s0, cudaStreamNonBlocking));
+    CKH(cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming));
+    int rc = FPLUS_OK;
+    // every buffer sized beforehand: one uncaptured solve per matrix with its right-hand side count
+    for (int64_t k = 0; k < count && rc == FPLUS_OK; k++) {
+        fplus_numeric *num = nums[k];
+        DevNum &N = *num->dev;
+        g->nums.push_back(num);
+        g->nrhs.push_back(nrhs[k]);
+        void *b = nullptr;
+        const size_t bytes = (size_t)num->n * (size_t)nrhs[k] * (size_t)N.vs;
+        CKH(cudaMalloc(&b, bytes > 0 ? bytes : 16));
+        g->rhs.push_back(b);
+        CKH(cudaMemsetAsync(b, 0, bytes, N.stream));
+        rc = dev_solve(*num->plan, *num->dplan, N, b, nrhs[k], trans, err, errlen);
+        if (rc == FPLUS_OK) CKH(cudaStreamSynchronize(N.stream));
+        cudaEvent_t e = nullptr;
+        CKH(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        g->joins.push_back(e);
+    }
+    if (rc) return rc;
+    CKH(cudaStreamBeginCapture(g->s0, cudaStreamCaptureModeThreadLocal));
+    cudaError_t ce = cudaEventRecord(g->fork, g->s0);
+    for (int64_t k = 0; k < count && rc == FPLUS_OK && ce == cudaSuccess; k++) {
+        fplus_numeric *num = nums[k];
+        DevNum &N = *num->dev;
+        if ((ce = cudaStreamWaitEvent(N.stream, g->fork, 0)) != cudaSuccess) break;
+        N.capture = 1;
+        rc = dev_equilibrate(*num->dplan, N, num->equilibrate, num->ruiz_max_iter, num->ruiz_tol, err, errlen);
+        int64_t border = -1;
+        if (rc == FPLUS_OK) rc = dev_factor_fronts(*num->plan, *num->dplan, N, num->pivot_rel, &border, err, errlen);
+        if (rc == FPLUS_OK) rc = dev_solve(*num->plan, *num->dplan, N, g->rhs[(size_t)k], nrhs[k], trans, err, errlen);
+        N.capture = 0;
+        if (rc == FPLUS_OK && (ce = cudaEventRecord(g->joins[(size_t)k], N.stream)) == cudaSuccess)
+            ce = cudaStreamWaitEvent(g->s0, g->joins[(size_t)k], 0);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(g->s0, &graph);
+    g->graph = graph;
+    if (rc) return rc;
+    if (ce != cudaSuccess || ee != cudaSuccess) {
+        errf(err, errlen, "CUDA graph capture: %s", cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+        return FPLUS_ERR_GPU;
+    }
+    CKH(cudaGraphInstantiate(&g->exec, g->graph, 0));
+    *out = g.release();
+    return FPLUS_OK;
+}
+
+extern "C" void *fplus_b200_graph_values(fplus_b200_graph *g, int64_t k)
+{
+    return g && k >= 0 && k < (int64_t)g->nums.size() ? g->nums[(size_t)k]->dev->Ax : nullptr;
+}
+
+extern "C" void *fplus_b200_graph_rhs(fplus_b200_graph *g, int64_t k)
+{
+    return g && k >= 0 && k < (int64_t)g->rhs.size() ? g->rhs[(size_t)k] : nullptr;
+}
+
+extern "C" int fplus_b200_graph_upload(fplus_b200_graph *g, int64_t k, const void *Ax, const void *b, char *err, size_t errlen)
+{
+    if (!g || k < 0 || k >= (int64_t)g->nums.size()) { errf(err, errlen, "bad graph or index"); return FPLUS_ERR_BADARG; }
+    CKH(cudaSetDevice(g->device));
+    const fplus_numeric *num = g->nums[(size_t)k];
+    const DevNum &N = *num->dev;
+    if (Ax) CKH(cudaMemcpyAsync(N.Ax, Ax, (size_t)N.nnz * (size_t)N.vs, cudaMemcpyHostToDevice, g->s0));
+    if (b) CKH(cudaMemcpyAsync(g->rhs[(size_t)k], b, (size_t)num->n * (size_t)g->nrhs[(size_t)k] * (size_t)N.vs,
+                               cudaMemcpyHostToDevice, g->s0));
+    return FPLUS_OK;
+}
+
+extern "C" int fplus_b200_graph_download(fplus_b200_graph *g, int64_t k, void *x, char *err, size_t errlen)
+{
+    if (!g || !x || k < 0 || k >= (int64_t)g->nums.size()) { errf(err, errlen, "bad graph, index or buffer"); return FPLUS_ERR_BADARG; }
+    CKH(cudaSetDevice(g->device));
+    const fplus_numeric *num = g->nums[(size_t)k];
+    CKH(cudaMemcpyAsync(x, g->rhs[(size_t)k], (size_t)num->n * (size_t)g->nrhs[(size_t)k] * (size_t)num->dev->vs,
+                        cudaMemcpyDeviceToHost, g->launched ? g->launched : g->s0));
+    CKH(cudaStreamSynchronize(g->launched ? g->launched : g->s0));
+    return FPLUS_OK;
+}
+
+extern "C" int fplus_b200_graph_launch(fplus_b200_graph *g, void *stream, char *err, size_t errlen)
+{
+    if (!g || !g->exec) { errf(err, errlen, "graph is NULL"); return FPLUS_ERR_BADARG; }
+    CKH(cudaSetDevice(g->device));
+    g->launched = stream ? (cudaStream_t)stream : g->s0;
+    if (g->launched != g->s0) {           // after the uploads made on the graph's stream
+        CKH(cudaEventRecord(g->fork, g->s0));
+        CKH(cudaStreamWaitEvent(g->launched, g->fork, 0));
+    }
+    CKH(cudaGraphLaunch(g->exec, g->launched));
+    return FPLUS_OK;
+}
+
+extern "C" int fplus_b200_graph_status(fplus_b200_graph *g, int *rcs, char *err, size_t errlen)
+{
+    if (!g) { errf(err, errlen, "graph is NULL"); return FPLUS_ERR_BADARG; }
+    CKH(cudaSetDevice(g->device));
+    CKH(cudaStreamSynchronize(g->launched ? g->launched : g->s0));
+    int rc = FPLUS_OK;
+    for (size_t k = 0; k < g->nums.size(); k++) {
+        int r = FPLUS_OK;
+        const int qrc = dev_status_rc(*g->nums[k]->dev, &r, err, errlen);
+        if (qrc) return qrc;
+        if (rcs) rcs[k] = r;
+        if (rc == FPLUS_OK && r != FPLUS_OK) {
+            rc = r;
+            errf(err, errlen, "matrix %ld: %s", (long)k, r == FPLUS_ERR_SINGULAR ? "singular" :
+                 r == FPLUS_ERR_GPU ? "a tensor-core update timed out" :
+                 "needs the uncaptured path (a dense-row pivot at a new place, or values beyond the range guard)");
+        }
+    }
+    return rc;
+}
+
+extern "C" void fplus_b200_graph_free(fplus_b200_graph *g) { delete g; }
 
 // the device time from the earliest factorization start to the latest solve end over a batch (events on the jobs' own
 // streams, read after they have completed)

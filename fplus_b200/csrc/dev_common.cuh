@@ -108,6 +108,7 @@ enum : int {
     ST_ZERO_COL = 4,       // Ruiz: column idx entirely zero
     ST_SOLVE_ZERO = 5,     // a zero diagonal of U in a solve
     ST_BAD_VALUE = 6,      // a non-finite input value at idx
+    ST_RANGE = 7,          // a captured factorization met values beyond 2^+-500 (the range guard needs the host path)
 };
 struct DevStatus {
     int code;

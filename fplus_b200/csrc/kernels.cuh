@@ -2314,6 +2314,27 @@ __global__ void __launch_bounds__(256) k_resid(const int64_t *__restrict__ ptr, 
     }
 }
 
+// ---- the captured (graph) form of the factorization: set-up done on the device instead of by host copies
+// the status word cleared (idx: the largest index, so that the smallest failing one wins)
+__global__ void k_clear_status(DevStatus *st, int range_guard)
+{
+    DevStatus h{};
+    h.idx = INT64_MAX;
+    if (range_guard) h.amin_bits = 0x7ff0000000000000ull;
+    *st = h;
+}
+__global__ void k_fill(double *a, int64_t m, double v)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x) a[q] = v;
+}
+// after k_abs_range: values whose range the host-side guard would rescale (FPLUS src/equil.c:197-241) cannot take the
+// captured path, which has no host decision; they are reported (ST_RANGE) and the caller factors them the usual way
+__global__ void k_range_flag(DevStatus *st)
+{
+    const double amax = bitsd(st->amax_bits), amin = bitsd(st->amin_bits);
+    if (amax > 0.0 && (amax > 0x1p500 || amin < 0x1p-500)) atomicCAS(&st->code, 0, ST_RANGE);
+}
+
 // x += d, or x -= d (undo), over m contiguous entries
 template <typename T>
 __global__ void k_axpy1(T *__restrict__ x, const T *__restrict__ d, int64_t m, int undo)

@@ -184,6 +184,11 @@ static int pool_init(int dev, char *err, size_t errlen)
 
 int ensure_async(DevNum &N, void **p, size_t *cap, size_t bytes, char *err, size_t errlen)
 {
+    if (N.capture) {                      // a captured sequence must not allocate: the buffers are sized beforehand
+        if ((*p && *cap >= bytes) || bytes == 0) return FPLUS_OK;
+        errf(err, errlen, "a captured factorization or solve needs a larger buffer (%zu > %zu bytes)", bytes, *cap);
+        return FPLUS_ERR_INTERNAL;
+    }
     if (*cap >= bytes && *p) return FPLUS_OK;
     if (*p) { CK(cudaFreeAsync(*p, N.stream)); *p = nullptr; *cap = 0; }
     CK(cudaMallocAsync(p, bytes > 0 ? bytes : 16, N.stream));
@@ -235,6 +240,34 @@ static int run_equil(const DevPlan &D, DevNum &N, int equilibrate, int max_iter,
     const int64_t n = N.n, nnz = N.nnz;
     T *Bx = (T *)N.Bx;
     k_gather<T><<<nblk(nnz), 256, 0, s>>>(Bx, (const T *)N.Ax, D.Bsrc, nnz), note_launch();
+    if (N.capture) {
+        // the same steps without host copies or decisions: the set-up on the device, every Ruiz iteration launched (the
+        // kernels do nothing once the iteration has converged), values the range guard would rescale reported
+        k_clear_status<<<1, 1, 0, s>>>(N.st, 1), note_launch();
+        k_fill<<<nblk(n), 256, 0, s>>>(N.Drp, n, 1.0), note_launch();
+        k_fill<<<nblk(n), 256, 0, s>>>(N.Dcp, n, 1.0), note_launch();
+        if (equilibrate) {
+            const int64_t m = (N.cplx ? 2 : 1) * nnz;
+            k_abs_range<<<nblk(m), 256, 0, s>>>((const double *)Bx, m, N.st), note_launch();
+            k_range_flag<<<1, 1, 0, s>>>(N.st), note_launch();
+            unsigned long long *rmax = (unsigned long long *)N.scratch, *cmax = rmax + n;
+            for (int it = 0; it < max_iter; it++) {
+                CK(cudaMemsetAsync(rmax, 0, (size_t)n * 8, s));
+                k_ruiz_rowmax<T><<<nblk(nnz), 256, 0, s>>>(D.Bi, Bx, nnz, rmax, N.st), note_launch();
+                k_ruiz_rowscale<<<nblk(n), 256, 0, s>>>(n, rmax, N.Drp, cmax, N.st), note_launch();
+                k_first_zero<<<nblk(n), 256, 0, s>>>(n, rmax, N.st, ST_ZERO_ROW), note_launch();
+                k_ruiz_colpass<T><<<nblk(32 * D.nseg), 256, 0, s>>>(D.seg, D.nseg, D.Bi, Bx, rmax, cmax, N.st), note_launch();
+                k_ruiz_colscale<<<nblk(n), 256, 0, s>>>(n, cmax, N.Dcp, N.st), note_launch();
+                k_first_zero<<<nblk(n), 256, 0, s>>>(n, cmax, N.st, ST_ZERO_COL), note_launch();
+                k_ruiz_colapply<T><<<nblk(32 * D.nseg), 256, 0, s>>>(D.seg, D.nseg, Bx, cmax, N.st), note_launch();
+                k_ruiz_check<<<1, 1, 0, s>>>(N.st, tol), note_launch();
+            }
+        }
+        CK(cudaMemsetAsync(N.colmax, 0, (size_t)n * 8, s));
+        k_colmax<T><<<nblk(32 * D.nseg), 256, 0, s>>>(D.seg, D.nseg, Bx, (unsigned long long *)N.colmax), note_launch();
+        CK(cudaGetLastError());
+        return FPLUS_OK;
+    }
     DevStatus h0;
     std::memset(&h0, 0, sizeof(h0));
     h0.amin_bits = 0x7ff0000000000000ull;       // +inf
@@ -352,7 +385,8 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         CK(cudaFuncSetAttribute(k_front_tail<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         attr_set = 1;
     }
-    if ((rc = dev_clear_status(N, err, errlen))) return rc;
+    // (captured: the status was cleared where the captured equilibration began, and must keep what it reported)
+    if (!N.capture && (rc = dev_clear_status(N, err, errlen))) return rc;
     N.tc_updates = 0; N.tc_flops = 0;
     T *La = (T *)N.Larena, *Ua = (T *)N.Uarena, *CB = (T *)N.cbstack;
     const T *Bx = (const T *)N.Bx;
@@ -612,6 +646,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     if (in_pipe) { CK(cudaEventRecord(N.ev_lu, A)); CK(cudaStreamWaitEvent(s, N.ev_lu, 0)); }    // the bulk stream joins
     CK(cudaGetLastError());
     k_pinv<<<nblk(N.n), 256, 0, s>>>(N.p_lu, N.pinv, N.n, N.st), note_launch();
+    if (N.capture) return FPLUS_OK;              // the status is read after the graph has run
     DevStatus h;
     CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -1011,8 +1046,20 @@ int dev_status(DevNum &N, int *code, int64_t *idx, char *err, size_t errlen)
     return FPLUS_OK;
 }
 
+int dev_status_rc(DevNum &N, int *rc, char *err, size_t errlen)
+{
+    DevStatus h;
+    CK(cudaMemcpy(&h, N.st, sizeof h, cudaMemcpyDeviceToHost));
+    if (h.tc_err) *rc = FPLUS_ERR_GPU;
+    else if (h.code == ST_SINGULAR || h.code == ST_ZERO_ROW || h.code == ST_ZERO_COL || h.code == ST_SOLVE_ZERO) *rc = FPLUS_ERR_SINGULAR;
+    else if (h.code != ST_OK) *rc = FPLUS_ERR_BADARG;
+    else *rc = FPLUS_OK;
+    return FPLUS_OK;
+}
+
 int dev_clear_status(DevNum &N, char *err, size_t errlen)
 {
+    if (N.capture) { k_clear_status<<<1, 1, 0, N.stream>>>(N.st, 0), note_launch(); return FPLUS_OK; }
     DevStatus h0;
     std::memset(&h0, 0, sizeof(h0));
     h0.idx = INT64_MAX;

@@ -68,6 +68,7 @@ struct DevNum {
     // the precision form: the arithmetic of the large fronts' Schur updates (schur_tc.hpp), their operand workspace, and
     // the updates that ran on the tensor cores in the last factorization
     int prec = 0;
+    int capture = 0;               // the launches are being captured into a CUDA graph: no host copies, waits or decisions
     void *gm_buf = nullptr;        // GMRES-IR: the Krylov basis and its vectors
     size_t cap_gm = 0;
     void *tcws = nullptr;
@@ -110,6 +111,10 @@ int dev_solve_refine(const FrontPlan &P, const DevPlan &D, DevNum &N, void *b, i
 int dev_solve_noalloc(const FrontPlan &P, const DevPlan &D, DevNum &N, void *b_dev, int64_t ldb, int64_t nrhs, int trans,
                       cudaStream_t s, char *err, size_t errlen);
 int dev_clear_status(DevNum &N, char *err, size_t errlen);
+// after a captured factorization and solve: *rc = FPLUS_OK, FPLUS_ERR_SINGULAR (no admissible pivot, a zero line or a
+// zero diagonal), FPLUS_ERR_GPU (a tensor-core wait ran out) or FPLUS_ERR_BADARG (a dense-row pivot where the plan had
+// none, or the range guard); waits for the status word
+int dev_status_rc(DevNum &N, int *rc, char *err, size_t errlen);
 // ||L||_F and ||U||_F of the device factors (L with its unit diagonal), from the arenas
 int dev_factor_norms(const FrontPlan &P, DevNum &N, double *lfro, double *ufro, char *err, size_t errlen);
 int dev_check_finite(DevNum &N, char *err, size_t errlen);

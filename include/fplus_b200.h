@@ -114,6 +114,32 @@ int fplus_b200_solve_batch(int64_t count, fplus_numeric *const *nums, void *cons
  * FPLUS; it lets a caller check factors too large to read back to the host (for instance against a stored oracle). */
 int fplus_b200_factor_norms(const fplus_numeric *num, double *L_fro, double *U_fro, char *err, size_t errlen);
 
+/* The batch form as one CUDA graph (no counterpart in FPLUS).  fplus_b200_graph_create captures, for every matrix k,
+ * the refactorization of new values on its pattern (the permutation, Ruiz, the fronts) and the solve of nrhs[k]
+ * right-hand sides with op = trans, each matrix on its own stream as an independent branch of one graph; nums[k] must
+ * be a factorization (fplus_factor / _dev / _prec) on the current device, and stays owned by the caller (free the graph
+ * first).  Capture needs no host decision: every Ruiz iteration is launched (they stop on the device once converged).
+ * Between launches, write matrix k's values (nnz entries, in A's order, as for fplus_factor) into
+ * fplus_b200_graph_values(g, k) and its right-hand sides (n x nrhs[k], column-major, ld n) into
+ * fplus_b200_graph_rhs(g, k), both device memory; fplus_b200_graph_launch replays the graph on `stream` (NULL: the
+ * graph's own stream); fplus_b200_graph_status waits for it and gives each matrix's code in rcs (FPLUS_OK,
+ * FPLUS_ERR_SINGULAR, or FPLUS_ERR_BADARG for values that need the uncaptured path: a dense row chosen as a pivot where
+ * the pattern's last factorization had none, or entries beyond 2^+-500 that the Ruiz range guard would rescale).  The
+ * solutions are then in the right-hand-side buffers.  After a replay the numeric objects' host-side accessors
+ * (fplus_numeric_p, _Dr, _factors, ...) still describe the factorization made before the capture. */
+typedef struct fplus_b200_graph fplus_b200_graph;
+int fplus_b200_graph_create(int64_t count, fplus_numeric *const *nums, const int64_t *nrhs, int trans, fplus_b200_graph **graph,
+                            char *err, size_t errlen);
+void *fplus_b200_graph_values(fplus_b200_graph *graph, int64_t k);
+void *fplus_b200_graph_rhs(fplus_b200_graph *graph, int64_t k);
+/* Host-memory conveniences: copy matrix k's values and / or right-hand sides (either may be NULL) into the graph's buffers
+ * on the graph's stream (launch orders after them); copy matrix k's solutions out after fplus_b200_graph_status. */
+int fplus_b200_graph_upload(fplus_b200_graph *graph, int64_t k, const void *Ax, const void *b, char *err, size_t errlen);
+int fplus_b200_graph_download(fplus_b200_graph *graph, int64_t k, void *x, char *err, size_t errlen);
+int fplus_b200_graph_launch(fplus_b200_graph *graph, void *stream, char *err, size_t errlen);
+int fplus_b200_graph_status(fplus_b200_graph *graph, int *rcs, char *err, size_t errlen);
+void fplus_b200_graph_free(fplus_b200_graph *graph);
+
 /* The device time of a batch: from the earliest start of the factorizations nums[0 .. count) (their first operation) to
  * the latest end of their last solves, from CUDA events on their own streams (no host timing).  No counterpart in FPLUS. */
 int fplus_b200_batch_span_ms(int64_t count, fplus_numeric *const *nums, double *ms, char *err, size_t errlen);
