@@ -68,7 +68,7 @@ FPLUS_B200_H_SYMBOLS = [
     "fplus_b200_solve_batch", "fplus_b200_solve_refine", "fplus_b200_symbolic_from_orders", "fplus_b200_factor_norms",
     "fplus_b200_factor_prec", "fplus_b200_schur_update", "fplus_b200_batch_span_ms", "fplus_b200_graph_create",
     "fplus_b200_graph_values", "fplus_b200_graph_rhs", "fplus_b200_graph_launch", "fplus_b200_graph_status",
-    "fplus_b200_graph_free", "fplus_b200_graph_upload", "fplus_b200_graph_download",
+    "fplus_b200_graph_free", "fplus_b200_graph_upload", "fplus_b200_graph_download", "fplus_b200_autotune",
 ]
 
 _lib = None
@@ -148,6 +148,8 @@ def lib():
     L.fplus_b200_graph_upload.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p,
                                           ctypes.c_size_t]
     L.fplus_b200_graph_download.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_b200_autotune.argtypes = [ctypes.c_void_p, _i64p, _i64p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Options),
+                                      ctypes.c_int, _i64p, _i64p, _dp, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_batch_span_ms.argtypes = [ctypes.c_int64, ctypes.c_void_p, _dp, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_factor_norms.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_solve_refine.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
@@ -266,6 +268,19 @@ class Symbolic:
                                                                                    "nrows", "nbord"))), None)
         out["f_dense"] = fd.value
         return out
+
+    def autotune(self, Ax, precision=0, options=None):
+        """fplus_b200_autotune: time each front shape on these values and keep the fastest; (width, nb, ms)."""
+        Ax = np.ascontiguousarray(Ax)
+        cplx = np.iscomplexobj(Ax)
+        Ax = Ax.astype(np.complex128 if cplx else np.float64, copy=False)
+        w, nb, ms = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_double()
+        err = ctypes.create_string_buffer(512)
+        opts = options if options is not None else self.options
+        _check(lib().fplus_b200_autotune(self._h, _p64(self.Ap), _p64(self.Ai), Ax.ctypes.data_as(ctypes.c_void_p), int(cplx),
+                                         ctypes.byref(opts), int(precision), ctypes.byref(w), ctypes.byref(nb),
+                                         ctypes.byref(ms), err, 512), err)
+        return w.value, nb.value, ms.value
 
     def factor(self, Ax, options=None, device=False, precision=0):
         """fplus_factor (precision 0), or the precision form (PREC_FP32, PREC_BF16X3, PREC_TF32: fplus_b200_factor_prec)."""

@@ -49,10 +49,11 @@ static int get_plan(const fplus_symbolic *sym, int64_t tail, std::shared_ptr<Fro
     CKH(cudaGetDevice(&dev));
     if (tail < sym->tail_hint || sym->tail_hint < 0) { if (tail >= 0) sym->tail_hint = tail; }
     const int64_t want = sym->tail_hint;
-    if (!sym->plan || sym->plan->f_dense != (want >= 0 && want < sym->n - sym->n_tau_cols ? want : sym->n - sym->n_tau_cols)) {
+    if (!sym->plan || sym->plan->f_dense != (want >= 0 && want < sym->n - sym->n_tau_cols ? want : sym->n - sym->n_tau_cols) ||
+        sym->plan->max_width != sym->max_width || sym->plan->nb_chain != sym->nb_chain) {
         auto P = std::make_shared<FrontPlan>();
         fplus_symbolic_view v{sym->n, sym->n_tau_rows, sym->n_tau_cols, sym->Bp.data(), sym->Bi.data()};
-        if (build_plan(v, want, 64, 256, *P)) { errf(err, errlen, "out of memory (symbolic structure)"); return FPLUS_ERR_NOMEM; }
+        if (build_plan(v, want, sym->nb_chain, sym->max_width, *P)) { errf(err, errlen, "out of memory (symbolic structure)"); return FPLUS_ERR_NOMEM; }
         sym->plan = P;
         sym->dplan.reset();
     }
@@ -270,6 +271,56 @@ extern "C" int fplus_b200_schur_update(int precision, int is_complex, int64_t M,
     if (derr) cudaFreeAsync(derr, s);
     cudaStreamSynchronize(s);
     return rc;
+}
+
+// The front-shape autotuner: factor the given values with each candidate shape (at most 128, 256 or 512 pivot columns per
+// front; for a pattern with a dense chain also 32 or 64 pivots per chain front), timed on the device (permutation,
+// Ruiz and the fronts, CUDA events), and keep the fastest in the symbolic object for every later factorization of the
+// pattern.  Each candidate is timed twice, the better time kept.  The pivots do not depend on the shape.
+extern "C" int fplus_b200_autotune(fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex,
+                                   const fplus_options *opt, int precision, int64_t *best_width, int64_t *best_nb,
+                                   double *best_ms, char *err, size_t errlen)
+{
+    if (!sym) { errf(err, errlen, "sym is NULL"); return FPLUS_ERR_BADARG; }
+    const int64_t widths[3] = {128, 256, 512}, nbs[2] = {32, 64};
+    const int64_t w0 = sym->max_width, b0 = sym->nb_chain;
+    int64_t bw = w0, bb = b0;
+    double bms = -1.0;
+    bool chain = false;
+    for (int wi = 0; wi < 3; wi++) {
+        for (int bi = 0; bi < 2; bi++) {
+            if (bi == 0 && !chain && wi > 0) continue;          // the chain size matters only with a dense chain
+            {
+                std::lock_guard<std::mutex> lk(sym->mu);
+                sym->max_width = widths[wi];
+                sym->nb_chain = nbs[bi];
+            }
+            double t = -1.0;
+            for (int rep = 0; rep < 2; rep++) {
+                fplus_numeric *num = nullptr;
+                const int rc = factor_common(sym, Ap, Ai, Ax, 0, is_complex, opt, &num, err, errlen, precision);
+                if (rc != FPLUS_OK) {
+                    std::lock_guard<std::mutex> lk(sym->mu);
+                    sym->max_width = w0; sym->nb_chain = b0;
+                    return rc;
+                }
+                const double ms = num->info.ms_equil + num->info.ms_fronts;
+                chain = chain || num->info.f_dense < num->n;
+                fplus_numeric_free(num);
+                if (t < 0 || ms < t) t = ms;
+            }
+            if (bms < 0 || t < bms) { bms = t; bw = widths[wi]; bb = nbs[bi]; }
+        }
+    }
+    {
+        std::lock_guard<std::mutex> lk(sym->mu);
+        sym->max_width = bw;
+        sym->nb_chain = bb;
+    }
+    if (best_width) *best_width = bw;
+    if (best_nb) *best_nb = bb;
+    if (best_ms) *best_ms = bms;
+    return FPLUS_OK;
 }
 
 #define SOLVE_GROUP 32

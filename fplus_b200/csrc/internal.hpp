@@ -54,6 +54,9 @@ struct fplus_symbolic {
     // before the tail (the pivot order is value dependent); guarded by mu
     mutable std::mutex mu;
     mutable int64_t tail_hint = -1;       // first column of the dense tail last needed (-1: none)
+    // the front structure's shape: at most max_width pivot columns per front, nb_chain per dense-chain front (the
+    // autotuner, fplus_b200_autotune, may change them)
+    mutable int64_t max_width = 256, nb_chain = 64;
     mutable std::shared_ptr<fpl::FrontPlan> plan;
     mutable std::shared_ptr<fpl::DevPlan> dplan;
 };
