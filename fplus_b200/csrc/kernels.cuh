@@ -2017,6 +2017,38 @@ __global__ void __launch_bounds__(256) k_chain_bulk(const T *__restrict__ Ua, co
     }
 }
 
+// the sum over a warp by a fixed butterfly (every lane gets the same result)
+template <typename T> __device__ __forceinline__ T shfl_sum(T v)
+{
+    for (int m = 16; m > 0; m >>= 1) v = add(v, shfl_xor_v<T>(v, m));
+    return v;
+}
+
+// The L21^T product of a large front's transposed backward sweep over many CTAs: CTA c sums its chunk of rows,
+// part[c][r][i] = sum over rows rr of its chunk of L[rr, i] (conjugated for CJ) v[pinv[rowid[rr]], r], a warp per pivot
+// column with its lanes down the rows (coalesced) and a fixed butterfly; k_bwdLt adds the chunks in order.
+template <typename T, bool CJ>
+__global__ void __launch_bounds__(256) k_ltdot(const T *__restrict__ L, int64_t nrows, int64_t npiv,
+                                               const int64_t *__restrict__ rowid, const int64_t *__restrict__ pinv,
+                                               const T *__restrict__ V, int64_t n, int64_t nrhs, int64_t chunk,
+                                               T *__restrict__ part)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int64_t r0 = npiv + blockIdx.x * chunk, r1 = r0 + chunk < nrows ? r0 + chunk : nrows;
+    T *pc = part + (int64_t)blockIdx.x * npiv * nrhs;
+    for (int64_t e = warp; e < npiv * nrhs; e += nw) {
+        const int64_t i = e % npiv, r = e / npiv;
+        T acc = VT<T>::zero();
+        for (int64_t rr = r0 + lane; rr < r1; rr += 32) {
+            T l = L[rr + i * nrows];
+            if (CJ) l = conjv(l);
+            acc = add(acc, mul(l, V[pinv[rowid[rr]] + r * n]));
+        }
+        acc = shfl_sum(acc);
+        if (lane == 0) pc[e] = acc;
+    }
+}
+
 // transposed solves: forward with U^T (U^H when conj) through one front, step 1 (one CTA): z = U11^-T w[f ..] by a warp
 // per right-hand side
 template <typename T, bool CJ>
@@ -2080,13 +2112,21 @@ __global__ void k_ut_scatter(const T *__restrict__ U12, int64_t npiv, int64_t nc
 template <typename T, bool CJ>
 __global__ void __launch_bounds__(256) k_bwdLt(const T *__restrict__ L, int64_t nrows, int64_t npiv, int64_t f,
                                                const int64_t *__restrict__ rowid, const int64_t *__restrict__ pinv,
-                                               const T *__restrict__ Z, T *__restrict__ V, int64_t n, int64_t nrhs)
+                                               const T *__restrict__ Z, T *__restrict__ V, int64_t n, int64_t nrhs,
+                                               const T *__restrict__ part = nullptr, int nch = 0)
 {
     extern __shared__ unsigned char smem_raw[];
     T *s = reinterpret_cast<T *>(smem_raw);           // npiv * nrhs
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    // s = z - L21^T v_cb (a warp per pivot column)
-    for (int64_t e = warp; e < npiv * nrhs; e += nw) {
+    // s = z - L21^T v_cb: summed here from the partial sums of k_ltdot (in chunk order), or a warp per pivot column
+    if (part) {
+        for (int64_t e = threadIdx.x; e < npiv * nrhs; e += blockDim.x) {
+            T acc = VT<T>::zero();
+            for (int c = 0; c < nch; c++) acc = add(acc, part[(int64_t)c * npiv * nrhs + e]);
+            s[e] = sub(Z[f + e % npiv + (e / npiv) * n], acc);
+        }
+    }
+    for (int64_t e = warp; !part && e < npiv * nrhs; e += nw) {
         const int64_t i = e % npiv, r = e / npiv;
         T acc = VT<T>::zero();
         for (int64_t rr = npiv + lane; rr < nrows; rr += 32) {
@@ -2265,12 +2305,6 @@ __global__ void k_pinv(const int64_t *__restrict__ p_lu, int64_t *__restrict__ p
 // iterative refinement: the residual r = b - op(A) x and the componentwise backward error, in the original coordinates
 // =====================================================================================================================
 
-// the sum over a warp by a fixed butterfly (every lane gets the same result)
-template <typename T> __device__ __forceinline__ T shfl_sum(T v)
-{
-    for (int m = 16; m > 0; m >>= 1) v = add(v, shfl_xor_v<T>(v, m));
-    return v;
-}
 
 // One warp per line of B = A[row_perm, :][:, col_perm]: trans 0 the rows of B (CSR: idx = B's column, the x entry
 // col_perm[idx], the output row row_perm[k]), trans 1 / 2 the columns of B (CSC: idx = B's row, x entry row_perm[idx],

@@ -716,10 +716,14 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
     auto bwd_grid = [&](int64_t ncb) { return ncb > 0 ? (ncb + bwd_chunk(ncb) - 1) / bwd_chunk(ncb) : (int64_t)1; };
     auto chunk_of = [](int64_t ncb) { int64_t c = (ncb + 295) / 296; return c < 32 ? (int64_t)32 : c; };
     int64_t maxpart = 1;
+    // the L21^T partial sums of a large front's transposed sweep: at most LT_CH chunks of rows
+    constexpr int64_t LT_CH = 148;
+    auto lt_chunk = [](int64_t rows) { int64_t c = (rows + LT_CH - 1) / LT_CH; return c < 256 ? (int64_t)256 : c; };
     for (const Front &F : P.fronts) {
         const int64_t ncb = F.ncols - F.npiv;
         maxpart = std::max(maxpart, bwd_grid(ncb) * F.npiv);
         if (ncb > 0) maxpart = std::max(maxpart, ((ncb + chunk_of(ncb) - 1) / chunk_of(ncb)) * F.npiv);
+        if (F.nrows > F.npiv) maxpart = std::max(maxpart, ((F.nrows - F.npiv + lt_chunk(F.nrows - F.npiv) - 1) / lt_chunk(F.nrows - F.npiv)) * F.npiv);
     }
     if ((rc = ensure_async(N, (void **)&N.part, &N.cap_part, (size_t)maxpart * (size_t)nrhs * sizeof(T), err, errlen))) return rc;
     T *R = (T *)N.rbuf, *S2 = (T *)N.sbuf, *part = (T *)N.part;
@@ -847,8 +851,17 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
             const bool small = F.npiv <= 64 && F.npiv <= F.nrows;
             const size_t tsm = sm + (size_t)F.npiv * (F.npiv + 1) * sizeof(T);
             const int64_t *rid = N.rowid + F.row_off;
+            const int64_t rows21 = F.nrows - F.npiv;
             if (small && cj) k_bwdLt3<T, true><<<1, 256, tsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
             else if (small) k_bwdLt3<T, false><<<1, 256, tsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
+            else if (rows21 > 1024) {
+                // a large front: the L21^T product over many CTAs, then the sum and the L11^T solve on one
+                const int64_t ch = lt_chunk(rows21), nch = (rows21 + ch - 1) / ch;
+                if (cj) k_ltdot<T, true><<<(unsigned)nch, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, rid, N.pinv, S2, n, nrhs, ch, part), note_launch();
+                else k_ltdot<T, false><<<(unsigned)nch, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, rid, N.pinv, S2, n, nrhs, ch, part), note_launch();
+                if (cj) k_bwdLt<T, true><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs, part, (int)nch), note_launch();
+                else k_bwdLt<T, false><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs, part, (int)nch), note_launch();
+            }
             else if (cj) k_bwdLt<T, true><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
             else k_bwdLt<T, false><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
         }

@@ -214,3 +214,20 @@ def test_solve_refine(gpu, name):
             c0, cr = _cw_berr(M, X0[:, r], B[:, r]), _cw_berr(M, Xr[:, r], B[:, r])
             assert bz[r] <= max(2 * c0, 1e-15) and c0 <= max(2 * bz[r], 1e-15), f"device {bz[r]:.2e} vs numpy {c0:.2e}"
             assert cr <= max(1e-15, 2 * c0), f"trans {trans} rhs {r}: refined {cr:.2e}, unrefined {c0:.2e}"
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_large_fronts_all_solve_directions(gpu, cplx):
+    """A 32^3 stencil (fronts of up to 256 pivots and thousands of rows: the multi-CTA forward and transposed sweeps):
+    every direction solves to a backward error <= 1e-14 and agrees with the oracle's solve."""
+    n, Ap, Ai, Ax = W.convdiff3d(32, 3)
+    if cplx:
+        Ax = Ax + 0.25j * np.random.default_rng(9).uniform(-1, 1, Ax.size)
+    S = F.analyze(n, Ap, Ai)
+    N = S.factor(Ax)
+    B = W.rhs(n, 2, cplx, 8).T.copy(order="F")
+    for trans in ((0, 1, 2) if cplx else (0, 1)):
+        X = N.solve(B, trans)
+        for r in range(2):
+            be = O.backward_error(n, Ap, Ai, Ax, X[:, r], B[:, r], trans)
+            assert be <= 1e-14, f"trans {trans} rhs {r}: backward error {be:.2e}"
