@@ -68,6 +68,8 @@ struct DevNum {
     // the precision form: the arithmetic of the large fronts' Schur updates (schur_tc.hpp), their operand workspace, and
     // the updates that ran on the tensor cores in the last factorization
     int prec = 0;
+    void *wbuf = nullptr;          // the W matrix [L11^-1 ; -L21 L11^-1] of the front whose tail runs as one GEMM
+    size_t cap_wbuf = 0;
     int capture = 0;               // the launches are being captured into a CUDA graph: no host copies, waits or decisions
     void *gm_buf = nullptr;        // GMRES-IR: the Krylov basis and its vectors
     size_t cap_gm = 0;
