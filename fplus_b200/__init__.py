@@ -69,6 +69,7 @@ FPLUS_B200_H_SYMBOLS = [
     "fplus_b200_factor_prec", "fplus_b200_schur_update", "fplus_b200_batch_span_ms", "fplus_b200_graph_create",
     "fplus_b200_graph_values", "fplus_b200_graph_rhs", "fplus_b200_graph_launch", "fplus_b200_graph_status",
     "fplus_b200_graph_free", "fplus_b200_graph_upload", "fplus_b200_graph_download", "fplus_b200_autotune",
+    "fplus_b200_set_front_shape",
 ]
 
 _lib = None
@@ -148,6 +149,7 @@ def lib():
     L.fplus_b200_graph_upload.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p,
                                           ctypes.c_size_t]
     L.fplus_b200_graph_download.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+    L.fplus_b200_set_front_shape.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
     L.fplus_b200_autotune.argtypes = [ctypes.c_void_p, _i64p, _i64p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Options),
                                       ctypes.c_int, _i64p, _i64p, _dp, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_batch_span_ms.argtypes = [ctypes.c_int64, ctypes.c_void_p, _dp, ctypes.c_char_p, ctypes.c_size_t]
@@ -268,6 +270,10 @@ class Symbolic:
                                                                                    "nrows", "nbord"))), None)
         out["f_dense"] = fd.value
         return out
+
+    def set_front_shape(self, max_width=256, nb_chain=64, lu_variant=2):
+        """fplus_b200_set_front_shape."""
+        _check(lib().fplus_b200_set_front_shape(self._h, int(max_width), int(nb_chain), int(lu_variant)), None)
 
     def autotune(self, Ax, precision=0, options=None):
         """fplus_b200_autotune: time each front shape on these values and keep the fastest; (width, nb, ms)."""

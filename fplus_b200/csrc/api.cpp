@@ -132,6 +132,10 @@ static int factor_common(const fplus_symbolic *sym, const int64_t *Ap, const int
         DevNum &N = *num->dev;
         if (tl_stream) N.stream = tl_stream;
         N.prec = prec;
+        {
+            std::lock_guard<std::mutex> lk(sym->mu);
+            N.lu_variant = sym->lu_variant;
+        }
         rc = dev_num_init(N, n, sym->nnz, num->is_complex, err, errlen);
         if (rc) return rc;
         CKH(cudaEventRecord(N.ev_begin, N.stream));
@@ -273,6 +277,18 @@ extern "C" int fplus_b200_schur_update(int precision, int is_complex, int64_t M,
     return rc;
 }
 
+// the front shape chosen by the caller (what fplus_b200_autotune sets), for every later factorization on sym
+extern "C" int fplus_b200_set_front_shape(fplus_symbolic *sym, int64_t max_width, int64_t nb_chain, int lu_variant)
+{
+    if (!sym || max_width < 16 || max_width > 4096 || nb_chain < 8 || nb_chain > 64 || (lu_variant != 2 && lu_variant != 3))
+        return FPLUS_ERR_BADARG;
+    std::lock_guard<std::mutex> lk(sym->mu);
+    sym->max_width = max_width;
+    sym->nb_chain = nb_chain;
+    sym->lu_variant = lu_variant;
+    return FPLUS_OK;
+}
+
 // The front-shape autotuner: factor the given values with each candidate shape (at most 128, 256 or 512 pivot columns per
 // front; for a pattern with a dense chain also 32 or 64 pivots per chain front), timed on the device (permutation,
 // Ruiz and the fronts, CUDA events), and keep the fastest in the symbolic object for every later factorization of the
@@ -284,24 +300,29 @@ extern "C" int fplus_b200_autotune(fplus_symbolic *sym, const int64_t *Ap, const
     if (!sym) { errf(err, errlen, "sym is NULL"); return FPLUS_ERR_BADARG; }
     const int64_t widths[3] = {128, 256, 512}, nbs[2] = {32, 64};
     const int64_t w0 = sym->max_width, b0 = sym->nb_chain;
+    const int l0 = sym->lu_variant;
     int64_t bw = w0, bb = b0;
+    int bl = l0;
     double bms = -1.0;
     bool chain = false;
-    for (int wi = 0; wi < 3; wi++) {
-        for (int bi = 0; bi < 2; bi++) {
-            if (bi == 0 && !chain && wi > 0) continue;          // the chain size matters only with a dense chain
-            {
-                std::lock_guard<std::mutex> lk(sym->mu);
-                sym->max_width = widths[wi];
-                sym->nb_chain = nbs[bi];
-            }
+    // the front shapes with the pivot-block LU of a barrier per step, then the best shape with the blocked LU
+    for (int ci = 0; ci < 7; ci++) {
+        const int wi = ci < 6 ? ci / 2 : -1, bi = ci < 6 ? ci % 2 : -1;
+        if (ci < 6 && bi == 0 && !chain && wi > 0) continue;      // the chain size matters only with a dense chain
+        {
+            std::lock_guard<std::mutex> lk(sym->mu);
+            sym->max_width = ci < 6 ? widths[wi] : bw;
+            sym->nb_chain = ci < 6 ? nbs[bi] : bb;
+            sym->lu_variant = ci < 6 ? 2 : 3;
+        }
+        {
             double t = -1.0;
             for (int rep = 0; rep < 2; rep++) {
                 fplus_numeric *num = nullptr;
                 const int rc = factor_common(sym, Ap, Ai, Ax, 0, is_complex, opt, &num, err, errlen, precision);
                 if (rc != FPLUS_OK) {
                     std::lock_guard<std::mutex> lk(sym->mu);
-                    sym->max_width = w0; sym->nb_chain = b0;
+                    sym->max_width = w0; sym->nb_chain = b0; sym->lu_variant = l0;
                     return rc;
                 }
                 const double ms = num->info.ms_equil + num->info.ms_fronts;
@@ -309,13 +330,17 @@ extern "C" int fplus_b200_autotune(fplus_symbolic *sym, const int64_t *Ap, const
                 fplus_numeric_free(num);
                 if (t < 0 || ms < t) t = ms;
             }
-            if (bms < 0 || t < bms) { bms = t; bw = widths[wi]; bb = nbs[bi]; }
+            if (bms < 0 || t < bms) {
+                bms = t;
+                if (ci < 6) { bw = widths[wi]; bb = nbs[bi]; bl = 2; } else bl = 3;
+            }
         }
     }
     {
         std::lock_guard<std::mutex> lk(sym->mu);
         sym->max_width = bw;
         sym->nb_chain = bb;
+        sym->lu_variant = bl;
     }
     if (best_width) *best_width = bw;
     if (best_nb) *best_nb = bb;

@@ -2076,13 +2076,24 @@ __global__ void __launch_bounds__(512) k_chain_diag(const T *__restrict__ Ua, co
                 const int64_t i = on ? e >> 2 : 0;
                 const int qq = (int)(e & 3);
                 const T *u = Ua + cU_off[k] + i;
-                for (int64_t r = 0; r < nrhs; r++) {
-                    T acc = VT<T>::zero();
+                for (int64_t r0 = 0; r0 < nrhs; r0 += 8) {     // eight right-hand sides per pass: each u entry used 8 times
+                    const int rb = nrhs - r0 < 8 ? (int)(nrhs - r0) : 8;
+                    T acc[8];
+#pragma unroll
+                    for (int t = 0; t < 8; t++) acc[t] = VT<T>::zero();
                     if (on)
-                        for (int64_t c = ca + qq; c < cb; c += 4) acc = add(acc, mul(u[(c - fk - nb) * nb], X[f0 + c + r * n]));
-                    acc = add(acc, shfl_xor_v<T>(acc, 1));
-                    acc = add(acc, shfl_xor_v<T>(acc, 2));
-                    if (on && qq == 0) { T *y = Y + f0 + fk + i + r * n; *y = sub(*y, acc); }
+                        for (int64_t c = ca + qq; c < cb; c += 4) {
+                            const T uv = u[(c - fk - nb) * nb];
+#pragma unroll
+                            for (int t = 0; t < 8; t++)
+                                if (t < rb) acc[t] = add(acc[t], mul(uv, X[f0 + c + (r0 + t) * n]));
+                        }
+#pragma unroll
+                    for (int t = 0; t < 8; t++) {
+                        acc[t] = add(acc[t], shfl_xor_v<T>(acc[t], 1));
+                        acc[t] = add(acc[t], shfl_xor_v<T>(acc[t], 2));
+                        if (on && qq == 0 && t < rb) { T *y = Y + f0 + fk + i + (r0 + t) * n; *y = sub(*y, acc[t]); }
+                    }
                 }
             }
             __syncthreads();
@@ -2136,16 +2147,19 @@ __global__ void __launch_bounds__(256) k_chain_bulk(const T *__restrict__ Ua, co
     const bool on = r < R;
     const int64_t j = on ? r / nb : 0, i = on ? r % nb : 0;
     const T *u = Ua + (on ? cU_off[j] : 0) + i + (ca - j * nb - nb) * nb;      // U12_j[i, column ca]
-    for (int64_t r0 = 0; r0 < nrhs; r0 += RB) {
-        const int rb = nrhs - r0 < RB ? (int)(nrhs - r0) : RB;
-        T acc[RB];
+    // 64 columns per round (16 per lane, all loaded at once, then used for every right-hand side); the row's partial
+    // sums of a round go into y after it (y stays in L2)
+    for (int64_t cr = 0; cr < nc; cr += 64) {
+        const int64_t c0 = cr + q * 16;
+        T uv[16];
 #pragma unroll
-        for (int t = 0; t < RB; t++) acc[t] = VT<T>::zero();
-        if (on) {
-            for (int64_t c0 = q * 16; c0 < nc; c0 += 64) {
-                T uv[16];
+        for (int c = 0; c < 16; c++) uv[c] = on && c0 + c < nc ? u[(c0 + c) * nb] : VT<T>::zero();
+        for (int64_t r0 = 0; r0 < nrhs; r0 += RB) {
+            const int rb = nrhs - r0 < RB ? (int)(nrhs - r0) : RB;
+            T acc[RB];
 #pragma unroll
-                for (int c = 0; c < 16; c++) uv[c] = c0 + c < nc ? u[(c0 + c) * nb] : VT<T>::zero();
+            for (int t = 0; t < RB; t++) acc[t] = VT<T>::zero();
+            if (on) {
 #pragma unroll
                 for (int c = 0; c < 16; c++) {
                     if (c0 + c >= nc) break;
@@ -2154,16 +2168,16 @@ __global__ void __launch_bounds__(256) k_chain_bulk(const T *__restrict__ Ua, co
                         if (t < rb) acc[t] = add(acc[t], mul(uv[c], xs[c0 + c + (r0 + t) * nc]));
                 }
             }
-        }
 #pragma unroll
-        for (int t = 0; t < RB; t++) {
-            acc[t] = add(acc[t], shfl_xor_v<T>(acc[t], 1));
-            acc[t] = add(acc[t], shfl_xor_v<T>(acc[t], 2));
-        }
-        if (on && q == 0) {
+            for (int t = 0; t < RB; t++) {
+                acc[t] = add(acc[t], shfl_xor_v<T>(acc[t], 1));
+                acc[t] = add(acc[t], shfl_xor_v<T>(acc[t], 2));
+            }
+            if (on && q == 0) {
 #pragma unroll
-            for (int t = 0; t < RB; t++)
-                if (t < rb) { T *y = Y + f0 + r + (r0 + t) * n; *y = sub(*y, acc[t]); }
+                for (int t = 0; t < RB; t++)
+                    if (t < rb) { T *y = Y + f0 + r + (r0 + t) * n; *y = sub(*y, acc[t]); }
+            }
         }
     }
 }

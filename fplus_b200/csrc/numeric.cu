@@ -469,7 +469,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             for (int64_t k = 0; k < std::min(np, nr); k++) fl += (double)(nr - k - 1) * (double)(np - k);
             prof.begin(st, PROF_LU, fm * fl, 2.0 * (double)(nr * np) * vs);
         }
-        if (use_lu3(nr, np, vs)) {
+        if (N.lu_variant == 3 && use_lu3(nr, np, vs)) {
             const size_t sm3 = front_lu3_smem(nr, np, vs);
             if (pa.on) {
                 CK(launch_pdl(k_front_lu3<T>, 1, LU3_THREADS, sm3, st, (const T *)W, ld, (int)nr, (int)np, (int)F.nri, F.f,

@@ -142,12 +142,18 @@ void fplus_b200_graph_free(fplus_b200_graph *graph);
 
 /* The front-shape autotuner (no counterpart in FPLUS): factors the given values once per candidate shape of the
  * multifrontal structure (at most 128, 256 or 512 pivot columns per front, the panel width of the large fronts' Schur
- * updates; for a pattern with a dense chain also 32 or 64 pivots per chain front), each timed on the device twice
- * (permutation, Ruiz and the fronts), in the given precision (FPLUS_B200_PREC_*), and keeps the fastest in sym for every
- * later factorization on it.  The pivots do not depend on the shape.  best_width, best_nb, best_ms may be NULL. */
+ * updates; for a pattern with a dense chain also 32 or 64 pivots per chain front), then the best shape with the blocked
+ * pivot-block LU, each timed on the device twice (permutation, Ruiz and the fronts), in the given precision
+ * (FPLUS_B200_PREC_*), and keeps the fastest in sym for every later factorization on it.  The pivots do not depend on the shape.  best_width, best_nb, best_ms may be NULL. */
 int fplus_b200_autotune(fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex,
                         const fplus_options *opt, int precision, int64_t *best_width, int64_t *best_nb, double *best_ms,
                         char *err, size_t errlen);
+
+/* The front shape of every later factorization on sym, chosen by the caller instead of the autotuner: at most max_width
+ * pivot columns per front (16 .. 4096), nb_chain pivots per dense-chain front (8 .. 64), and the pivot-block LU of the
+ * small fronts (2: one barrier per pivot step; 3: blocked 8-column panels).  The pivots do not depend on these.  No
+ * counterpart in FPLUS. */
+int fplus_b200_set_front_shape(fplus_symbolic *sym, int64_t max_width, int64_t nb_chain, int lu_variant);
 
 /* The device time of a batch: from the earliest start of the factorizations nums[0 .. count) (their first operation) to
  * the latest end of their last solves, from CUDA events on their own streams (no host timing).  No counterpart in FPLUS. */

@@ -231,3 +231,16 @@ def test_large_fronts_all_solve_directions(gpu, cplx):
         for r in range(2):
             be = O.backward_error(n, Ap, Ai, Ax, X[:, r], B[:, r], trans)
             assert be <= 1e-14, f"trans {trans} rhs {r}: backward error {be:.2e}"
+
+
+@pytest.mark.parametrize("name", ["pencil_1x64", "pencil_2x256", "banded_cplx_1200", "convdiff3d_g12", "hard_cplx_300"])
+def test_blocked_pivot_block_lu_matches_oracle(gpu, name):
+    """The blocked pivot-block LU (k_front_lu3, the autotuner's other choice) gives the oracle's pivots and factors."""
+    n, Ap, Ai, Ax = CASES[name]()
+    S = F.analyze(n, Ap, Ai)
+    S.set_front_shape(256, 64, 3)
+    N = S.factor(Ax)
+    orc = O.OracleLU(n, Ap, Ai, Ax, S.row_perm, S.col_perm)
+    assert np.array_equal(N.p, orc.p)
+    L, U, _ = N.factors()
+    assert _rel(L, orc.L) <= FACTOR_TOL and _rel(U, orc.U) <= FACTOR_TOL

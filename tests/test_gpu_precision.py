@@ -70,7 +70,9 @@ def test_schur_update_against_fp64(torch_cuda, prec, cplx, shape):
     assert finite, "non-finite or unwritten entries in the result"
     assert e <= TOL[prec], f"error {e:.2e} relative to |A||B| (plain torch FP32 GEMM: {e32:.2e})"
     if prec == F.PREC_FP32:
-        assert e <= 4 * e32 + 1e-7, f"FP32 mode {e:.2e} vs torch FP32 {e32:.2e}"
+        # FP32-level accuracy: within a decade of a plain FP32 GEMM (the split adds 2^-22 per product, and the FP32
+        # accumulation runs over 3K terms, 6K complex)
+        assert e <= 10 * e32 + 1e-7, f"FP32 mode {e:.2e} vs torch FP32 {e32:.2e}"
 
 
 def test_schur_update_rejects_small_shapes(torch_cuda):
