@@ -99,6 +99,19 @@ __device__ __forceinline__ unsigned long long warp_max_key(unsigned long long ke
     return ((unsigned long long)hi << 32) | lo;
 }
 
+// 1 / p for the pivot: conj(p) / |p|^2 with the components scaled by max(|re|, |im|) first (no overflow or underflow of the
+// squares); real: 1 / p
+// (__drcp_rn: the correctly rounded reciprocal, the same value as the IEEE quotient 1.0 / q)
+__device__ __forceinline__ double recip(double p) { return __drcp_rn(p); }
+__device__ __forceinline__ cplx recip(cplx p)
+{
+    const double q = p.x * p.x + p.y * p.y;
+    if (q > 1e-300 && q < 1e300) { const double d = __drcp_rn(q); return cplx{p.x * d, -p.y * d}; }
+    const double s = fmax(fabs(p.x), fabs(p.y)), is = __drcp_rn(s);     // scaled: no overflow or underflow
+    const double a = p.x * is, b = p.y * is, d = __drcp_rn(a * a + b * b);
+    return cplx{a * d * is, -b * d * is};
+}
+
 // device status word: the first failure wins (code, then the smallest step / index)
 enum : int {
     ST_OK = 0,

@@ -3,6 +3,7 @@
 // GEMM, copy-out) and the supernodal triangular sweeps.  Included once, by numeric.cu.
 #pragma once
 #include <climits>
+#include <cooperative_groups.h>
 #include "dev_common.cuh"
 
 namespace fpl {
@@ -322,6 +323,132 @@ __global__ void __launch_bounds__(512) k_panel(T *__restrict__ W, int64_t ld, in
     }
 }
 
+// The same partial pivoting of panel [k0, k0 + w) for a tall front, on many CTAs at once (a cooperative launch, one CTA
+// per SM): CTA b owns a contiguous range of the rows at positions >= k0.  Per column j: every CTA finds the best of its
+// rows not yet chosen (largest pivot key, ties to the smaller row of B) and posts it (double-buffered by column
+// parity); one grid-wide barrier; every CTA takes the same winner p from the posts, applies the same singular / border
+// decision (a stop ends every CTA at the same column), reads row p's remaining panel entries and updates its own rows
+// (the multiplier, then the rank-1 update of the panel's later columns).  Rows are not moved inside the panel: the
+// chosen rows are marked (ptag), and at the end CTA 0 turns the choices into the interchanges the swapping form would
+// have made (ipiv[j] = the position of the chosen row at step j) and swaps the row ids the same way; the caller then
+// applies ipiv to the panel's own columns too (k_laswp), which leaves exactly the swapping form's result.  ptag holds 0
+// for every row on entry and on exit.
+struct PanelCand { unsigned long long key; long long rid; long long row; };
+
+template <typename T>
+__global__ void __launch_bounds__(512) k_panel_coop(T *__restrict__ W, int64_t ld, int64_t nrows, int64_t nri, int k0, int w,
+                                                   int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
+                                                   int64_t *__restrict__ rowid, int *__restrict__ ipiv, int64_t *__restrict__ chosen,
+                                                   unsigned char *__restrict__ ptag, PanelCand *__restrict__ cand, DevStatus *st,
+                                                   int64_t front)
+{
+    namespace cg = cooperative_groups;
+    cg::grid_group grid = cg::this_grid();
+    __shared__ unsigned long long s_key[16];
+    __shared__ long long s_rid[16], s_row[16];
+    __shared__ long long s_p;
+    __shared__ int s_stop;
+    __shared__ T s_prow[32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const int G = gridDim.x, b = blockIdx.x;
+    const int64_t span = nrows - k0, per = (span + G - 1) / G;
+    const int64_t r_lo = k0 + b * per, r_hi = r_lo + per < nrows ? r_lo + per : nrows;
+    if (st->code) return;                                 // read once, before any barrier: the same for every CTA
+    for (int kk = 0; kk < w; kk++) {
+        const int64_t j = k0 + kk;
+        // 1. the best of this CTA's live rows in column j
+        long long bk = -1; long long brid = LLONG_MAX, brow = -1;
+        for (int64_t i = r_lo + tid; i < r_hi; i += blockDim.x) {
+            if (ptag[i]) continue;
+            const long long a = (long long)pivkey(W[i + j * ld]);
+            const long long r = rowid[i];
+            if (a > bk || (a == bk && r < brid)) { bk = a; brid = r; brow = i; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const long long ok = __shfl_xor_sync(0xffffffffu, bk, o), orid = __shfl_xor_sync(0xffffffffu, brid, o),
+                            orow = __shfl_xor_sync(0xffffffffu, brow, o);
+            if (ok > bk || (ok == bk && orid < brid)) { bk = ok; brid = orid; brow = orow; }
+        }
+        if (lane == 0) { s_key[warp] = (unsigned long long)bk; s_rid[warp] = brid; s_row[warp] = brow; }
+        __syncthreads();
+        if (tid == 0) {
+            long long k2 = (long long)s_key[0], r2 = s_rid[0], w2 = s_row[0];
+            for (int q = 1; q < nw; q++)
+                if ((long long)s_key[q] > k2 || ((long long)s_key[q] == k2 && s_rid[q] < r2)) { k2 = (long long)s_key[q]; r2 = s_rid[q]; w2 = s_row[q]; }
+            PanelCand c; c.key = (unsigned long long)k2; c.rid = r2; c.row = w2;     // key -1 (all ones): no live row
+            cand[(kk & 1) * G + b] = c;
+        }
+        grid.sync();
+        // 2. the winner, the same in every CTA
+        if (tid == 0) {
+            long long k2 = -1, r2 = LLONG_MAX, p = -1;
+            for (int q = 0; q < G; q++) {
+                const PanelCand c = cand[(kk & 1) * G + q];
+                const long long ck = (long long)c.key;
+                if (c.row < 0) continue;
+                if (ck > k2 || (ck == k2 && c.rid < r2)) { k2 = ck; r2 = c.rid; p = c.row; }
+            }
+            const double t = pivot_rel * colmax[fcol + j];
+            int stop = 0;
+            const T pv = p >= 0 ? W[p + j * ld] : VT<T>::zero();
+            if (p < 0 || k2 <= 0 || ((unsigned long long)k2 < pivkey_of_modulus<T>(2.0 * t) && vabs(pv) < t)) {
+                if (b == 0) set_status(st, ST_SINGULAR, fcol + j, p >= 0 ? vabs(pv) : 0.0, t);
+                stop = 1;
+            } else if (p >= nri) {
+                if (b == 0) set_status(st, ST_BORDER, front, vabs(pv), t);
+                stop = 1;
+            }
+            s_stop = stop;
+            s_p = p;
+            if (!stop) {
+                if (b == 0) chosen[kk] = p;
+                if (p >= r_lo && p < r_hi) ptag[p] = 1;   // its owner marks it (only the owner reads its rows' marks)
+            }
+        }
+        __syncthreads();
+        if (s_stop) return;                               // every CTA decides the same at the same column
+        const int64_t p = s_p;
+        if (tid < w - kk) s_prow[tid] = W[p + (k0 + kk + tid) * ld];
+        __syncthreads();
+        // 3. this CTA's live rows: the multiplier and the update of the panel's later columns
+        const T inv = recip(s_prow[0]);
+        for (int64_t i = r_lo + tid; i < r_hi; i += blockDim.x) {
+            if (ptag[i]) continue;
+            const T l = mul(W[i + j * ld], inv);
+            W[i + j * ld] = l;
+            for (int c = 1; c < w - kk; c++) {
+                T *x = W + i + (j + c) * ld;
+                *x = sub(*x, mul(l, s_prow[c]));
+            }
+        }
+    }
+    grid.sync();                                          // every update is done before the choices are turned into swaps
+    if (b == 0 && tid == 0) {
+        // the interchanges of the swapping form: at step t the row chosen sits at position pos(chosen[t]); track the rows
+        // moved so far (at most 2w) in a short list
+        long long mv_row[64], mv_pos[64];
+        int nmv = 0;
+        auto pos_of = [&](long long r) { for (int q = 0; q < nmv; q++) if (mv_row[q] == r) return mv_pos[q]; return r; };
+        auto at_pos = [&](long long ps) { for (int q = 0; q < nmv; q++) if (mv_pos[q] == ps) return mv_row[q]; return ps; };
+        auto set_pos = [&](long long r, long long ps) {
+            for (int q = 0; q < nmv; q++) if (mv_row[q] == r) { mv_pos[q] = ps; return; }
+            mv_row[nmv] = r; mv_pos[nmv] = ps; nmv++;
+        };
+        for (int t = 0; t < w; t++) {
+            const long long jj = k0 + t, r = chosen[t];
+            const long long q = pos_of(r);
+            ipiv[jj] = (int)q;
+            if (q != jj) {
+                const long long x = at_pos(jj);
+                set_pos(x, q);
+                set_pos(r, jj);
+                const int64_t tr = rowid[jj]; rowid[jj] = rowid[q]; rowid[q] = tr;
+            }
+        }
+        for (int t = 0; t < w; t++) ptag[chosen[t]] = 0;
+    }
+}
+
 // apply the recorded swaps ipiv[k0 .. k0 + cnt) in order to the columns [c0, c1)
 template <typename T>
 __global__ void k_laswp(T *__restrict__ W, int64_t ld, const int *__restrict__ ipiv, int k0, int cnt, int64_t c0, int64_t c1,
@@ -502,18 +629,6 @@ template <> __device__ __forceinline__ cplx shfl_v<cplx>(cplx v, int src)
     return cplx{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
 }
 
-// 1 / p for the pivot: conj(p) / |p|^2 with the components scaled by max(|re|, |im|) first (no overflow or underflow of the
-// squares); real: 1 / p
-// (__drcp_rn: the correctly rounded reciprocal, the same value as the IEEE quotient 1.0 / q)
-__device__ __forceinline__ double recip(double p) { return __drcp_rn(p); }
-__device__ __forceinline__ cplx recip(cplx p)
-{
-    const double q = p.x * p.x + p.y * p.y;
-    if (q > 1e-300 && q < 1e300) { const double d = __drcp_rn(q); return cplx{p.x * d, -p.y * d}; }
-    const double s = fmax(fabs(p.x), fabs(p.y)), is = __drcp_rn(s);     // scaled: no overflow or underflow
-    const double a = p.x * is, b = p.y * is, d = __drcp_rn(a * a + b * b);
-    return cplx{a * d * is, -b * d * is};
-}
 
 // Partial-pivot LU of a front's pivot block in shared memory, with a pivot warp and one-column look-ahead (one CTA of
 // up to 1024 threads).  Warp 0 owns the critical path: at step j it updates column j + 1 for every row with the step-j

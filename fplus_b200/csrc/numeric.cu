@@ -152,7 +152,7 @@ DevNum::~DevNum()
                     (void *)cbstack, (void *)work, (void *)rowid, (void *)p_lu, (void *)pinv, (void *)ipiv, (void *)perm,
                     (void *)st, (void *)scratch, (void *)rbuf, (void *)sbuf, (void *)xbuf, (void *)part, (void *)work2,
                     (void *)perm2, (void *)rr_p, (void *)rr_l, (void *)rr_s, (void *)ir_b, (void *)ir_x, (void *)ir_r,
-                    (void *)ir_d, (void *)ir_bits, scratch_norm, tcws, gm_buf, wbuf})
+                    (void *)ir_d, (void *)ir_bits, scratch_norm, tcws, gm_buf, wbuf, coopbuf})
         if (p) cudaFreeAsync(p, stream);
     if (stream) cudaStreamSynchronize(stream);
     if (crit) cudaStreamSynchronize(crit);
@@ -357,6 +357,8 @@ static const size_t SMEM_MAX = 220 * 1024;   // dynamic shared memory opt-in, be
 // the precision form takes a Schur update to the tensor cores from this size on (smaller ones stay FP64: they are cheap,
 // and a 128 x 256 tile would be mostly padding)
 static const int64_t TC_MIN_ROWS = 128, TC_MIN_COLS = 256;
+// panels of fronts with more rows than this are pivoted on every SM at once (k_panel_coop)
+static const int64_t COOP_ROWS = 2048;
 static const double TC_MIN_MADDS = 1 << 24;
 
 template <typename T>
@@ -393,6 +395,19 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     T *La = (T *)N.Larena, *Ua = (T *)N.Uarena, *CB = (T *)N.cbstack;
     const T *Bx = (const T *)N.Bx;
     constexpr int PW = 32;       // panel width of the blocked path
+    // the cooperative panel's buffer and grid (one CTA per SM, if the kernel fits one per SM)
+    static thread_local int coop_grid_cached = -1;
+    if (coop_grid_cached < 0) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_panel_coop<T>, 512, 0) != cudaSuccess) { per = 0; (void)cudaGetLastError(); }
+        coop_grid_cached = per >= 1 ? sms : 0;
+    }
+    const int coop_grid = coop_grid_cached;
+    if (P.max_nrows > COOP_ROWS &&
+        (rc = ensure_async(N, &N.coopbuf, &N.cap_coop, (size_t)((P.max_nrows + 255) & ~(int64_t)255) + PW * 8 +
+                                                          (size_t)2 * 160 * sizeof(PanelCand), err, errlen))) return rc;
     const int TB = VT<T>::cplx_ ? 32 : 64;    // rows per TRSM block of U12
     const int64_t nf = (int64_t)P.fronts.size();
     const double fm = VT<T>::cplx_ ? 8.0 : 2.0;     // flops per multiply-add
@@ -491,10 +506,36 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
                                                 Lf, perm, N.p_lu, N.st, fi, pa), note_launch();
         } else {
             const int64_t npr = std::min(np, nr);
+            // tall panels on many SMs at once (a cooperative launch); the marks start cleared
+            const bool coop = nr > COOP_ROWS && coop_grid > 1;
+            unsigned char *ptag = (unsigned char *)N.coopbuf;
+            int64_t *chosen = (int64_t *)((char *)N.coopbuf + ((P.max_nrows + 255) & ~(int64_t)255));
+            PanelCand *cand = (PanelCand *)(chosen + PW);
+            if (coop) CK(cudaMemsetAsync(ptag, 0, (size_t)nr, st));
             for (int64_t k0 = 0; k0 < npr; k0 += PW) {
                 const int w = (int)std::min<int64_t>(PW, npr - k0);
-                k_panel<T><<<1, 512, 0, st>>>(W, ld, nr, F.nri, (int)k0, w, F.f, N.colmax, pivot_rel, N.rowid + F.row_off,
-                                             N.ipiv + F.f, N.st, fi), note_launch();
+                bool done = false;
+                if (coop && nr - k0 > COOP_ROWS) {
+                    const int G = (int)std::min<int64_t>(coop_grid, (nr - k0 + 255) / 256);
+                    int64_t *rid = N.rowid + F.row_off;
+                    int *ip = N.ipiv + F.f;
+                    int k0i = (int)k0, wi = w;
+                    int64_t fcol = F.f, nri = F.nri, frow = fi, ldl = ld, nrl = nr;
+                    const double *cm = N.colmax;
+                    double prel = pivot_rel;
+                    DevStatus *stp = N.st;
+                    T *Wp = W;
+                    void *args[] = {&Wp, &ldl, &nrl, &nri, &k0i, &wi, &fcol, &cm, &prel, &rid, &ip, &chosen, &ptag, &cand, &stp, &frow};
+                    if (cudaLaunchCooperativeKernel((const void *)k_panel_coop<T>, G, 512, args, 0, st) == cudaSuccess) {
+                        note_launch();
+                        // the panel's own columns take the interchanges too
+                        k_laswp<T><<<nblk(w, 128), 128, 0, st>>>(W, ld, N.ipiv + F.f, (int)k0, w, k0, k0 + w, N.st), note_launch();
+                        done = true;
+                    } else (void)cudaGetLastError();
+                }
+                if (!done)
+                    k_panel<T><<<1, 512, 0, st>>>(W, ld, nr, F.nri, (int)k0, w, F.f, N.colmax, pivot_rel, N.rowid + F.row_off,
+                                                 N.ipiv + F.f, N.st, fi), note_launch();
                 if (k0 > 0) k_laswp<T><<<nblk(k0, 128), 128, 0, st>>>(W, ld, N.ipiv + F.f, (int)k0, w, 0, k0, N.st), note_launch();
                 if (k0 + w < np) {
                     k_laswp<T><<<nblk(np - k0 - w, 128), 128, 0, st>>>(W, ld, N.ipiv + F.f, (int)k0, w, k0 + w, np, N.st), note_launch();

@@ -68,6 +68,8 @@ struct DevNum {
     // the precision form: the arithmetic of the large fronts' Schur updates (schur_tc.hpp), their operand workspace, and
     // the updates that ran on the tensor cores in the last factorization
     int prec = 0;
+    void *coopbuf = nullptr;       // the cooperative panel: row marks (max_nrows bytes), the choices, the CTAs' posts
+    size_t cap_coop = 0;
     void *wbuf = nullptr;          // the W matrix [L11^-1 ; -L21 L11^-1] of the front whose tail runs as one GEMM
     size_t cap_wbuf = 0;
     int lu_variant = 2;            // the pivot-block LU kernel of the small fronts (k_front_lu2 or k_front_lu3)
