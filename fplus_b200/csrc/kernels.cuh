@@ -1732,6 +1732,66 @@ __global__ void __launch_bounds__(512) k_fwdL3(const T *__restrict__ L, int64_t 
 // written back and copied to xs (np x nrhs, ld np).  k_fwdL21 (many CTAs, a thread per row below the pivots): the rows
 // rr >= np take y[rr] -= sum_i L[rr, i] xs[i] with L read down its columns (coalesced) and xs staged in shared memory
 // (np * nrhs values).  The same operations as one front's forward substitution, the L21 product spread over the GPU.
+// A triangular solve of a large front's pivot block on the vector x (np x nrhs, ld np, shared memory) by blocks of 64:
+// each diagonal block staged in shared memory (sT, 64 x 64) and solved with the block's rows in two registers per lane (a
+// warp per right-hand side), then the other rows updated by the block's solved values (L read down its columns).
+// Lower (UPPER false): the unit-lower L11, forward.  Upper: U11 with its diagonal, backward (a zero diagonal entry is
+// reported as ST_SOLVE_ZERO).  The block is L[r + c * ld] (the front's L block: U11 on and above the diagonal).
+template <typename T, bool UPPER>
+__device__ void blk_trisolve(const T *__restrict__ L, int64_t ld, int np, T *x, int64_t nrhs, T *sT, T *dinv, DevStatus *st,
+                             int64_t f)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const int nb = (np + 63) / 64;
+    for (int bb = 0; bb < nb; bb++) {
+        const int bi = UPPER ? nb - 1 - bb : bb;
+        const int r0 = bi * 64, w = np - r0 < 64 ? np - r0 : 64;
+        for (int e = tid; e < w * w; e += blockDim.x) {
+            const int i = e % w, k = e / w;
+            sT[i + k * 64] = L[(r0 + i) + (int64_t)(r0 + k) * ld];
+        }
+        if (UPPER)
+            for (int i = tid; i < w; i += blockDim.x) {
+                const T d = L[(r0 + i) + (int64_t)(r0 + i) * ld];
+                if (is_zero(d)) set_status(st, ST_SOLVE_ZERO, f + r0 + i, 0, 0);
+                dinv[i] = is_zero(d) ? VT<T>::zero() : recip(d);
+            }
+        __syncthreads();
+        if (UPPER && st->code == ST_SOLVE_ZERO) return;
+        for (int64_t r = warp; r < nrhs; r += nw) {
+            T *xr = x + r * np + r0;
+            T a = lane < w ? xr[lane] : VT<T>::zero(), b = lane + 32 < w ? xr[lane + 32] : VT<T>::zero();
+            if (!UPPER) {
+                for (int i = 0; i < w; i++) {
+                    const T xi = shfl_v<T>(i < 32 ? a : b, i & 31);
+                    if (lane > i && lane < w) a = sub(a, mul(sT[lane + i * 64], xi));
+                    if (lane + 32 > i && lane + 32 < w) b = sub(b, mul(sT[lane + 32 + i * 64], xi));
+                }
+            } else {
+                for (int i = w - 1; i >= 0; i--) {
+                    const T xi = mul(shfl_v<T>(i < 32 ? a : b, i & 31), dinv[i]);
+                    if (lane == (i & 31)) { if (i < 32) a = xi; else b = xi; }
+                    if (lane < i) a = sub(a, mul(sT[lane + i * 64], xi));
+                    if (lane + 32 < i) b = sub(b, mul(sT[lane + 32 + i * 64], xi));
+                }
+            }
+            if (lane < w) xr[lane] = a;
+            if (lane + 32 < w) xr[lane + 32] = b;
+        }
+        __syncthreads();
+        const int o0 = UPPER ? 0 : r0 + w, o1 = UPPER ? r0 : np;
+        if (o1 > o0)
+            for (int64_t e = tid; e < (int64_t)(o1 - o0) * nrhs; e += blockDim.x) {
+                const int row = o0 + (int)(e % (o1 - o0));
+                const int64_t r = e / (o1 - o0);
+                T acc = VT<T>::zero();
+                for (int k = 0; k < w; k++) acc = add(acc, mul(L[row + (int64_t)(r0 + k) * ld], x[r * np + r0 + k]));
+                x[r * np + row] = sub(x[r * np + row], acc);
+            }
+        __syncthreads();
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_fwdL11(const T *__restrict__ L, int64_t nrows, int64_t np,
                                                 const int64_t *__restrict__ rowid, T *__restrict__ Wr, int64_t n, int64_t nrhs,
@@ -1739,19 +1799,10 @@ __global__ void __launch_bounds__(256) k_fwdL11(const T *__restrict__ L, int64_t
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *v = reinterpret_cast<T *>(smem_raw);           // np x nrhs
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    T *sT = v + np * nrhs;                            // 64 x 64
     for (int64_t e = threadIdx.x; e < np * nrhs; e += blockDim.x) v[e] = Wr[rowid[e % np] + (e / np) * n];
     __syncthreads();
-    for (int64_t r = warp; r < nrhs; r += nw) {
-        T *vr = v + r * np;
-        for (int64_t i = 0; i < np; i++) {
-            const T xi = vr[i];
-            if (!is_zero(xi))
-                for (int64_t rr = i + 1 + lane; rr < np; rr += 32) vr[rr] = sub(vr[rr], mul(L[rr + i * nrows], xi));
-            __syncwarp();
-        }
-    }
-    __syncthreads();
+    blk_trisolve<T, false>(L, nrows, (int)np, v, nrhs, sT, nullptr, nullptr, 0);
     for (int64_t e = threadIdx.x; e < np * nrhs; e += blockDim.x) {
         Wr[rowid[e % np] + (e / np) * n] = v[e];
         xs[e] = v[e];
@@ -1871,6 +1922,28 @@ __global__ void __launch_bounds__(256) k_bwdU(const T *__restrict__ L, int64_t n
 // status word's ticket, after a fence) copies U11 into shared memory (cp.async) while it sums the partials in chunk order,
 // subtracts them from y and solves with U11: a warp per right-hand side with the vector in registers (npiv <= 64), else
 // in shared memory.  The ticket is returned to 0 for the next launch.
+// The backward sweep through a large front (npiv > 64): y = Y[f ..] minus the U12 partial sums of k_u12_gemv (in chunk
+// order), then U11 by 64-row blocks (blk_trisolve)
+template <typename T>
+__global__ void __launch_bounds__(256) k_bwdU_blk(const T *__restrict__ L, int64_t nrows, int64_t npiv, int64_t f,
+                                                  const T *__restrict__ part, int64_t nchunk, const T *__restrict__ Y,
+                                                  T *__restrict__ X, int64_t n, int64_t nrhs, DevStatus *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *s = reinterpret_cast<T *>(smem_raw);           // npiv * nrhs
+    T *sT = s + npiv * nrhs;                          // 64 x 64
+    T *dinv = sT + 64 * 64;                           // 64
+    for (int64_t e = threadIdx.x; e < npiv * nrhs; e += blockDim.x) {
+        T v = Y[f + e % npiv + (e / npiv) * n];
+        for (int64_t q = 0; q < nchunk; q++) v = sub(v, part[q * npiv * nrhs + e]);
+        s[e] = v;
+    }
+    __syncthreads();
+    blk_trisolve<T, true>(L, nrows, (int)npiv, s, nrhs, sT, dinv, st, f);
+    if (st->code == ST_SOLVE_ZERO) return;
+    for (int64_t e = threadIdx.x; e < npiv * nrhs; e += blockDim.x) X[f + e % npiv + (e / npiv) * n] = s[e];
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_bwdU_fused(const T *__restrict__ L, int64_t nrows, int64_t npiv, int64_t f,
                                                     const T *__restrict__ U12, int64_t ncb, const int64_t *__restrict__ cbcols,

@@ -834,10 +834,12 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
                 CK(launch_pdl(k_fwdL3<T>, 1, swt, l11_sm, s, La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 0));
                 note_launch();
             }
-            else if ((size_t)np * nrhs * sizeof(T) <= FWD_SMEM) {
-                // a large front: the L11 solve, then the L21 product over many CTAs (xs in the partial-sum buffer)
+            else if ((size_t)(np * nrhs + 64 * 64) * sizeof(T) <= FWD_SMEM) {
+                // a large front: the L11 solve by 64-row blocks, then the L21 product over many CTAs (xs in the partial-sum
+                // buffer)
                 const size_t xsm = (size_t)np * nrhs * sizeof(T);
-                k_fwdL11<T><<<1, 256, xsm, s>>>(La + F.L_off, F.nrows, np, N.rowid + F.row_off, R, n, nrhs, part), note_launch();
+                k_fwdL11<T><<<1, 256, xsm + 64 * 64 * sizeof(T), s>>>(La + F.L_off, F.nrows, np, N.rowid + F.row_off, R, n, nrhs,
+                                                                       part), note_launch();
                 if (F.nrows > np)
                     k_fwdL21<T><<<(unsigned)((F.nrows - np + 255) / 256), 256, xsm, s>>>(La + F.L_off, F.nrows, np,
                                                                                       N.rowid + F.row_off, R, n, nrhs, part), note_launch();
@@ -875,10 +877,24 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
             (void)csm;
             fi_end = cb;
         }
+        CK(cudaFuncSetAttribute(k_bwdU_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
         for (int64_t fi = fi_end - 1; fi >= 0; fi--) {
             const Front &F = P.fronts[fi];
             const int64_t ncb = F.ncols - F.npiv;
             if (F.npiv == 0) continue;
+            const size_t bsm = (size_t)(F.npiv * nrhs + 64 * 64 + 64) * sizeof(T);
+            if (F.npiv > 64 && F.npiv <= F.nrows && bsm <= FWD_SMEM) {
+                // a large front: the U12 product over many CTAs, then U11 by 64-row blocks
+                int64_t nchunk = 0;
+                if (ncb > 0) {
+                    const int64_t chunk = chunk_of(ncb);
+                    nchunk = (ncb + chunk - 1) / chunk;
+                    k_u12_gemv<T><<<(unsigned)nchunk, 256, (size_t)8 * F.npiv * sizeof(T), s>>>(
+                        Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, R, n, nrhs, chunk, part), note_launch();
+                }
+                k_bwdU_blk<T><<<1, 256, bsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, part, nchunk, S2, R, n, nrhs, N.st), note_launch();
+                continue;
+            }
             k_bwdU_fused<T><<<(unsigned)bwd_grid(ncb), 256, fsmem, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, Ua + F.U_off, ncb,
                                                                      D.cols + F.col_off + F.npiv, ncb > 0 ? bwd_chunk(ncb) : 0,
                                                                      part, S2, R, n, nrhs, N.st), note_launch();
