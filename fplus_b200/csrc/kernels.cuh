@@ -524,23 +524,39 @@ __global__ void __launch_bounds__(256) k_gemm_sub(int64_t M, int64_t N, int64_t 
         for (int a = 0; a < 4; a++)
 #pragma unroll
             for (int b = 0; b < 2; b++) { acc[z][a][b][0] = 0.0; acc[z][a][b][1] = 0.0; }
-    for (int64_t k0 = 0; k0 < K; k0 += GBK) {
-        // stage A (64 x 16) and B (16 x 64)
+    // the next K slice is loaded into registers while the current one is multiplied
+    T pa[4], pb[4];
+    auto load_slice = [&](int64_t k0) {
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             const int m = tid & 63, k = (tid >> 6) + 4 * i;
             const int64_t gm = m0 + m, gk = k0 + k;
-            T v = (gm < M && gk < K) ? A[gm + gk * lda] : VT<T>::zero();
-            if constexpr (CP) { As[0][k][m] = v.x; As[1][k][m] = v.y; } else As[0][k][m] = v;
+            pa[i] = (gm < M && gk < K) ? A[gm + gk * lda] : VT<T>::zero();
         }
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             const int k = tid & 15, nn = (tid >> 4) + 16 * i;
             const int64_t gk = k0 + k, gn = n0 + nn;
-            T v = (gk < K && gn < N) ? B[gk + gn * ldb] : VT<T>::zero();
+            pb[i] = (gk < K && gn < N) ? B[gk + gn * ldb] : VT<T>::zero();
+        }
+    };
+    load_slice(0);
+    for (int64_t k0 = 0; k0 < K; k0 += GBK) {
+        // stage A (64 x 16) and B (16 x 64) from the registers, then load the next slice
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int m = tid & 63, k = (tid >> 6) + 4 * i;
+            const T v = pa[i];
+            if constexpr (CP) { As[0][k][m] = v.x; As[1][k][m] = v.y; } else As[0][k][m] = v;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int k = tid & 15, nn = (tid >> 4) + 16 * i;
+            const T v = pb[i];
             if constexpr (CP) { Bs[0][nn][k] = v.x; Bs[1][nn][k] = v.y; Bs[2][nn][k] = -v.y; } else Bs[0][nn][k] = v;
         }
         __syncthreads();
+        if (k0 + GBK < K) load_slice(k0 + GBK);
 #pragma unroll
         for (int ks = 0; ks < GBK; ks += 4) {
             const int kr = ks + (lane & 3);
@@ -1417,157 +1433,6 @@ __global__ void __launch_bounds__(FT_THREADS) k_front_tail(const T *__restrict__
 
 // X <- L^-1 X for a unit lower w x w block (w <= 32 RPL) and every column of X (rows [0, w) of each column, ld ldx):
 // a warp per column, RPL rows per lane, the solved entries broadcast by shuffles
-// The tail of a front as one GEMM per column tile.  k_front_winv (one CTA) forms, from the front's factored pivot block
-// (the L arena block: L11 unit lower in its top np rows, L21 below, rows in the final order),
-//     Wm = [ L11^-1 ; -L21 L11^-1 ]      (nrows x npiv, column-major, ld nrows),
-// L11^-1 by columns (four lanes per column, a fixed-order butterfly for each entry), then the product.  k_front_tail_w
-// then computes, for every tile of TN contribution-block columns with the tile's rows gathered in pivot order (perm),
-//     [ U12 ; CB ] = Wm A12[perm] + [ 0 ; A22[perm] ]
-// on the FP64 tensor cores (mma m8n8k4; complex as four real products), a warp per 8-row block over all the tile's
-// columns, the accumulators initialised with A22 for the contribution-block rows, and U12 and the CB written from the
-// accumulators.  No serial triangular solve and one barrier pair per tile.  Mathematically the forward substitution of
-// k_front_tail; the products are summed in another order.
-template <typename T>
-__global__ void __launch_bounds__(256) k_front_winv(const T *__restrict__ Lb, int nrows, int npiv, T *__restrict__ Wm,
-                                                    const DevStatus *st)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *sL = reinterpret_cast<T *>(smem_raw);          // nrows x npiv: the L block (ld nrows)
-    T *sI = sL + (size_t)nrows * npiv;                // npiv x npiv: L11^-1 (ld npiv)
-    if (st->code) return;
-    const int tid = threadIdx.x, lane = tid & 31;
-    for (int e = tid; e < nrows * npiv; e += blockDim.x) sL[e] = Lb[e];
-    for (int e = tid; e < npiv * npiv; e += blockDim.x) sI[e] = (e % npiv == e / npiv) ? VT<T>::one() : VT<T>::zero();
-    __syncthreads();
-    // column j of L11^-1: x_i = -sum_{k in [j, i)} L[i, k] x_k for i > j, by the four lanes q = tid & 3 of column j
-    const int q = tid & 3, j = tid >> 2;
-    for (int i = 1; i < npiv; i++) {
-        T acc = VT<T>::zero();
-        if (j < i && j < npiv)
-            for (int k = j + q; k < i; k += 4) acc = add(acc, mul(sL[i + k * nrows], sI[k + j * npiv]));
-        acc = add(acc, shfl_xor_v<T>(acc, 1));
-        acc = add(acc, shfl_xor_v<T>(acc, 2));
-        if (j < i && j < npiv && q == 0) sI[i + j * npiv] = sub(VT<T>::zero(), acc);
-        __syncthreads();
-    }
-    (void)lane;
-    // Wm: the top rows L11^-1, the others -L21 L11^-1 (L11^-1 lower triangular: k >= c)
-    for (int e = tid; e < nrows * npiv; e += blockDim.x) {
-        const int r = e % nrows, c = e / nrows;
-        T v;
-        if (r < npiv) v = sI[r + c * npiv];
-        else {
-            T acc = VT<T>::zero();
-            for (int k = c; k < npiv; k++) acc = add(acc, mul(sL[r + k * nrows], sI[k + c * npiv]));
-            v = sub(VT<T>::zero(), acc);
-        }
-        Wm[e] = v;
-    }
-}
-
-template <typename T, int TN>
-__global__ void __launch_bounds__(FT_THREADS) k_front_tail_w(const T *__restrict__ W, int64_t ld, const int *__restrict__ perm,
-                                                             int npiv, int nrows, int64_t cb0, int64_t cb1,
-                                                             const T *__restrict__ Wm, T *__restrict__ U, T *__restrict__ CB,
-                                                             const DevStatus *st)
-{
-    constexpr bool CP = VT<T>::cplx_;
-    constexpr int PER = FT_NR * TN / FT_THREADS;                   // tile values per thread
-    constexpr int NB = TN / 8;                                      // 8-column blocks per tile
-    extern __shared__ __align__(16) double ft_smem[];
-    double *sWr = ft_smem;                                          // Wm[m, k] at k * FT_LD + m
-    double *sWi = sWr + (CP ? FT_NP * FT_LD : 0);
-    double *sXr = sWr + (CP ? 2 : 1) * FT_NP * FT_LD;               // X[r, c] at c * FT_LD + r
-    double *sXi = sXr + (CP ? TN * FT_LD : 0);
-    __shared__ int sperm[FT_NR];
-    if (st->code) return;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int M = nrows - npiv;
-    for (int i = tid; i < nrows; i += FT_THREADS) sperm[i] = perm[i];
-    __syncthreads();
-    const int64_t t0 = cb0 / TN, ntile = (cb1 + TN - 1) / TN;
-    T pre[PER];
-    auto fetch = [&](int64_t t) {
-        const int64_t c0 = t * TN;
-#pragma unroll
-        for (int qq = 0; qq < PER; qq++) {
-            const int e = tid + qq * FT_THREADS, r = e % FT_NR, c = e / FT_NR;
-            pre[qq] = (t < ntile && r < nrows && c0 + c < cb1) ? W[sperm[r] + (npiv + c0 + c) * ld] : VT<T>::zero();
-        }
-    };
-    fetch(t0 + blockIdx.x);                                          // in flight while Wm is staged
-    for (int e0 = tid; e0 < npiv * nrows; e0 += 8 * FT_THREADS) {
-        T v[8];
-#pragma unroll
-        for (int qq = 0; qq < 8; qq++) { const int e = e0 + qq * FT_THREADS; v[qq] = e < npiv * nrows ? Wm[e] : VT<T>::zero(); }
-#pragma unroll
-        for (int qq = 0; qq < 8; qq++) {
-            const int e = e0 + qq * FT_THREADS, m = e % nrows, k = e / nrows;
-            if (e < npiv * nrows) {
-                if constexpr (CP) { sWr[k * FT_LD + m] = v[qq].x; sWi[k * FT_LD + m] = v[qq].y; } else sWr[k * FT_LD + m] = v[qq];
-            }
-        }
-    }
-    const int mt = (nrows + 7) >> 3;
-    for (int64_t t = t0 + blockIdx.x; t < ntile; t += gridDim.x) {
-        const int64_t c0 = t * TN;
-        const int tn = (int)(cb1 - c0 < TN ? cb1 - c0 : TN);
-        __syncthreads();                                             // the previous tile's reads are done
-#pragma unroll
-        for (int qq = 0; qq < PER; qq++) {
-            const int e = tid + qq * FT_THREADS, r = e % FT_NR, c = e / FT_NR;
-            if constexpr (CP) { sXr[c * FT_LD + r] = pre[qq].x; sXi[c * FT_LD + r] = pre[qq].y; } else sXr[c * FT_LD + r] = pre[qq];
-        }
-        __syncthreads();
-        fetch(t + gridDim.x);                                        // in flight during this tile
-        if (warp < mt) {
-            const int m0 = 8 * warp, am = m0 + (lane >> 2);
-            const int cr = am, ccb = 2 * (lane & 3);
-            double a[NB][2], b[NB][2];                               // re / im accumulators of each 8-column block
-#pragma unroll
-            for (int nb = 0; nb < NB; nb++) {
-                const int cc = 8 * nb + ccb;
-                const bool cbrow = cr >= npiv && cr < nrows;          // contribution-block rows start from A22
-                a[nb][0] = cbrow ? sXr[cc * FT_LD + cr] : 0.0;
-                a[nb][1] = cbrow ? sXr[(cc + 1) * FT_LD + cr] : 0.0;
-                b[nb][0] = CP && cbrow ? sXi[cc * FT_LD + cr] : 0.0;
-                b[nb][1] = CP && cbrow ? sXi[(cc + 1) * FT_LD + cr] : 0.0;
-            }
-            for (int ks = 0; ks < npiv; ks += 4) {
-                const int k = ks + (lane & 3);
-                const bool kin = k < npiv;
-                const double ar = kin && am < nrows ? sWr[k * FT_LD + am] : 0.0;
-                const double ai = CP && kin && am < nrows ? sWi[k * FT_LD + am] : 0.0;
-#pragma unroll
-                for (int nb = 0; nb < NB; nb++) {
-                    const int bn = 8 * nb + (lane >> 2);
-                    const double br = kin ? sXr[bn * FT_LD + k] : 0.0;
-                    dmma(a[nb][0], a[nb][1], ar, br);
-                    if constexpr (CP) {
-                        const double bi = kin ? sXi[bn * FT_LD + k] : 0.0;
-                        dmma(a[nb][0], a[nb][1], ai, -bi);
-                        dmma(b[nb][0], b[nb][1], ar, bi);
-                        dmma(b[nb][0], b[nb][1], ai, br);
-                    }
-                }
-            }
-            if (cr < nrows) {
-#pragma unroll
-                for (int nb = 0; nb < NB; nb++)
-#pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        const int cc = 8 * nb + ccb + h;
-                        if (cc >= tn) continue;
-                        T v;
-                        if constexpr (CP) v = T{a[nb][h], b[nb][h]}; else v = a[nb][h];
-                        if (cr < npiv) U[cr + (c0 + cc) * (int64_t)npiv] = v;
-                        else CB[(cr - npiv) + (c0 + cc) * (int64_t)M] = v;
-                    }
-            }
-        }
-    }
-}
-
 template <typename T, int RPL>
 __global__ void __launch_bounds__(256) k_trsm_warp(T *__restrict__ X, int64_t ldx, int w, int64_t ncols,
                                                    const T *__restrict__ Lb, int64_t ldl, const DevStatus *st)

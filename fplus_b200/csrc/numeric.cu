@@ -152,7 +152,7 @@ DevNum::~DevNum()
                     (void *)cbstack, (void *)work, (void *)rowid, (void *)p_lu, (void *)pinv, (void *)ipiv, (void *)perm,
                     (void *)st, (void *)scratch, (void *)rbuf, (void *)sbuf, (void *)xbuf, (void *)part, (void *)work2,
                     (void *)perm2, (void *)rr_p, (void *)rr_l, (void *)rr_s, (void *)ir_b, (void *)ir_x, (void *)ir_r,
-                    (void *)ir_d, (void *)ir_bits, scratch_norm, tcws, gm_buf, wbuf, coopbuf})
+                    (void *)ir_d, (void *)ir_bits, scratch_norm, tcws, gm_buf, coopbuf})
         if (p) cudaFreeAsync(p, stream);
     if (stream) cudaStreamSynchronize(stream);
     if (crit) cudaStreamSynchronize(crit);
@@ -385,8 +385,6 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         CK(cudaFuncSetAttribute(k_u12_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_front_tail<T, FT_TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_front_tail<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
-        CK(cudaFuncSetAttribute(k_front_tail_w<T, FT_TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
-        CK(cudaFuncSetAttribute(k_front_winv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         attr_set = 1;
     }
     // (captured: the status was cleared where the captured equilibration began, and must keep what it reported)
@@ -556,28 +554,6 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         if (nr < np) { k_set_singular<<<1, 1, 0, st>>>(N.st, F.f + nr), note_launch(); }
         return FPLUS_OK;
     };
-    // the W form of the tail (k_front_winv + k_front_tail_w) for the bulk of a front's columns: one buffer for W, used
-    // in stream order on the stream that runs the tail
-    if ((rc = ensure_async(N, &N.wbuf, &N.cap_wbuf, (size_t)std::max<int64_t>(1, std::min<int64_t>(P.max_nrows, FT_NR) *
-                                                                                   std::min<int64_t>(P.max_npiv, FT_NP)) * vs,
-                           err, errlen))) return rc;
-    auto tail_w = [&](int64_t fi, T *W, const int *perm, cudaStream_t st, int64_t c0, int64_t c1, int cap) {
-        const Front &F = P.fronts[fi];
-        const int64_t nr = F.nrows, np = F.npiv, M = nr - np;
-        if (c1 <= c0) return FPLUS_OK;
-        // algorithmic work as for the forward substitution (the W form multiplies the full np x np L11^-1: more
-        // arithmetic on the tensor pipe than counted here)
-        prof.begin(st, PROF_SCHUR, fm * ((double)np * (double)np / 2.0 + (double)M * (double)np) * (double)(c1 - c0),
-                   (double)(2 * nr * (c1 - c0) + nr * np) * vs);
-        const size_t wsm = (size_t)(nr * np + np * np) * vs;
-        k_front_winv<T><<<1, 256, wsm, st>>>(La + F.L_off, (int)nr, (int)np, (T *)N.wbuf, N.st), note_launch();
-        const size_t fsm = (size_t)(VT<T>::cplx_ ? 2 : 1) * (FT_NP + FT_TN) * FT_LD * sizeof(double);
-        const int blocks = (int)std::min<int64_t>((c1 - c0 + FT_TN - 1) / FT_TN, cap);
-        k_front_tail_w<T, FT_TN><<<blocks, FT_THREADS, fsm, st>>>(W, nr, perm, (int)np, (int)nr, c0, c1, (const T *)N.wbuf,
-                                                                  Ua + F.U_off, CB + F.cb_off, N.st), note_launch();
-        prof.end(st);
-        return FPLUS_OK;
-    };
     // U12 and the CB for CB columns [c0, c1) by the fused tail kernel (at most `cap` CTAs)
     auto tail = [&](int64_t fi, T *W, const int *perm, cudaStream_t st, int64_t c0, int64_t c1, int cap, bool narrow) {
         const Front &F = P.fronts[fi];
@@ -636,7 +612,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
                 CK(cudaStreamWaitEvent(s, N.ev_lu, 0));
                 const int64_t h = std::min<int64_t>(ncb, (hc[fi] + FT_TN - 1) / FT_TN * FT_TN);
                 // at most 139 CTAs: one SM stays free for the next LU and eight for the next tail head
-                if ((rc = tail_w(fi, W, perm, s, h, ncb, 139))) return rc;
+                if ((rc = tail(fi, W, perm, s, h, ncb, 139, false))) return rc;
                 CK(cudaStreamWaitEvent(A, N.ev_head, 0));
                 if ((rc = tail(fi, W, perm, A, 0, h, 148, true))) return rc;
             }
@@ -654,7 +630,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         if (ncb == 0) continue;
         T *Uf = Ua + F.U_off;
         if (std::min(np, nr) == np && np <= FT_NP && nr <= FT_NR) {
-            if ((rc = tail_w(fi, W, N.perm, s, 0, ncb, 148))) return rc;
+            if ((rc = tail(fi, W, N.perm, s, 0, ncb, 148, false))) return rc;
             if ((fi & 255) == 255) CK(cudaGetLastError());
             continue;
         }

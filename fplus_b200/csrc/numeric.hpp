@@ -70,8 +70,6 @@ struct DevNum {
     int prec = 0;
     void *coopbuf = nullptr;       // the cooperative panel: row marks (max_nrows bytes), the choices, the CTAs' posts
     size_t cap_coop = 0;
-    void *wbuf = nullptr;          // the W matrix [L11^-1 ; -L21 L11^-1] of the front whose tail runs as one GEMM
-    size_t cap_wbuf = 0;
     int lu_variant = 2;            // the pivot-block LU kernel of the small fronts (k_front_lu2 or k_front_lu3)
     int capture = 0;               // the launches are being captured into a CUDA graph: no host copies, waits or decisions
     void *gm_buf = nullptr;        // GMRES-IR: the Krylov basis and its vectors
