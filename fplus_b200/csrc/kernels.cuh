@@ -1209,9 +1209,11 @@ __global__ void k_left_finish(const T *__restrict__ W, int64_t ld, int64_t nrows
                               T *__restrict__ Lout, const DevStatus *st)
 {
     if (st->code) return;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        for (int64_t i = 0; i < nrows; i++) perm[i] = (int)i;
-        for (int64_t j = 0; j < npiv && j < nrows; j++) { int p = ipiv[j]; int t = perm[j]; perm[j] = perm[p]; perm[p] = t; }
+    if (blockIdx.x == 0) {          // the identity by the whole first CTA, then the interchanges in order by one thread
+        for (int64_t i = threadIdx.x; i < nrows; i += blockDim.x) perm[i] = (int)i;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int64_t j = 0; j < npiv && j < nrows; j++) { int p = ipiv[j]; int t = perm[j]; perm[j] = perm[p]; perm[p] = t; }
     }
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t e = tid; e < nrows * npiv; e += stride) Lout[e] = W[e % nrows + (e / nrows) * ld];
