@@ -537,6 +537,10 @@ def run_b200_arm(args, rank, world):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     F.lib().fplus_b200_use_stream(ctypes.c_void_p(stream.cuda_stream))
+    # the front shape for this pattern, picked once by the library's autotuner (untimed, like the analysis)
+    t0 = time.perf_counter()
+    tuned = S.autotune(Ax) if not args.no_autotune else None
+    autotune_ms = (time.perf_counter() - t0) * 1e3
     Ad = torch.from_numpy(Ax).to(dev)
     bd0 = torch.from_numpy(np.ascontiguousarray(b)).to(dev)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -691,6 +695,9 @@ def run_b200_arm(args, rank, world):
             "scaling": "weak", "vs_baseline": None, "dtype": "c128" if cplx else "f64", "data": "synthetic",
             "config": dict(desc, **{"parallelism": f"replicas{world}" if world > 1 else "1 GPU",
                                     "l2": "flushed between steps (512 MiB write)", "analyze_ms": round(analyze_ms, 2),
+                                    "front_shape": None if tuned is None else {"max_width": tuned[0], "nb_chain": tuned[1],
+                                                                                "lu_kernel": tuned[2],
+                                                                                "autotune_ms": round(autotune_ms, 1)},
                                     "berr": berr, "berr_e2e": berr_e2e, "fronts": info["nfronts"],
                                     "dense_chain_from": info["f_dense"], "ms_equil": round(info["ms_equil"], 3),
                                     "ms_fronts": round(info["ms_fronts"], 3), "front_flops": info["front_flops"]}),
@@ -712,6 +719,7 @@ def main():
     ap.add_argument("--modes", type=int, default=8,
                     help="Fourier modes of the pencil workload (8: n = 32768, the benchmark; 1: n = 4096, for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default front shape (no fplus_b200_autotune)")
     ap.add_argument("--precision-grid", type=int, default=80,
                     help="grid of the 3D stencil of the precision-form measurement (80: n = 512,000; 0: none)")
     ap.add_argument("--batch", type=int, default=64, help="shifts of the pencil in the batch measurement (0: none)")

@@ -151,7 +151,8 @@ def lib():
     L.fplus_b200_graph_download.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_set_front_shape.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
     L.fplus_b200_autotune.argtypes = [ctypes.c_void_p, _i64p, _i64p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Options),
-                                      ctypes.c_int, _i64p, _i64p, _dp, ctypes.c_char_p, ctypes.c_size_t]
+                                      ctypes.c_int, _i64p, _i64p, ctypes.POINTER(ctypes.c_int), _dp, ctypes.c_char_p,
+                                      ctypes.c_size_t]
     L.fplus_b200_batch_span_ms.argtypes = [ctypes.c_int64, ctypes.c_void_p, _dp, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_factor_norms.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_char_p, ctypes.c_size_t]
     L.fplus_b200_solve_refine.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
@@ -276,17 +277,17 @@ class Symbolic:
         _check(lib().fplus_b200_set_front_shape(self._h, int(max_width), int(nb_chain), int(lu_variant)), None)
 
     def autotune(self, Ax, precision=0, options=None):
-        """fplus_b200_autotune: time each front shape on these values and keep the fastest; (width, nb, ms)."""
+        """fplus_b200_autotune: time each front shape on these values and keep the fastest; (width, nb, lu, ms)."""
         Ax = np.ascontiguousarray(Ax)
         cplx = np.iscomplexobj(Ax)
         Ax = Ax.astype(np.complex128 if cplx else np.float64, copy=False)
-        w, nb, ms = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_double()
+        w, nb, lu, ms = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int(), ctypes.c_double()
         err = ctypes.create_string_buffer(512)
         opts = options if options is not None else self.options
         _check(lib().fplus_b200_autotune(self._h, _p64(self.Ap), _p64(self.Ai), Ax.ctypes.data_as(ctypes.c_void_p), int(cplx),
                                          ctypes.byref(opts), int(precision), ctypes.byref(w), ctypes.byref(nb),
-                                         ctypes.byref(ms), err, 512), err)
-        return w.value, nb.value, ms.value
+                                         ctypes.byref(lu), ctypes.byref(ms), err, 512), err)
+        return w.value, nb.value, lu.value, ms.value
 
     def factor(self, Ax, options=None, device=False, precision=0):
         """fplus_factor (precision 0), or the precision form (PREC_FP32, PREC_BF16X3, PREC_TF32: fplus_b200_factor_prec)."""

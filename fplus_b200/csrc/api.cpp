@@ -295,7 +295,7 @@ extern "C" int fplus_b200_set_front_shape(fplus_symbolic *sym, int64_t max_width
 // pattern.  Each candidate is timed twice, the better time kept.  The pivots do not depend on the shape.
 extern "C" int fplus_b200_autotune(fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex,
                                    const fplus_options *opt, int precision, int64_t *best_width, int64_t *best_nb,
-                                   double *best_ms, char *err, size_t errlen)
+                                   int *best_lu, double *best_ms, char *err, size_t errlen)
 {
     if (!sym) { errf(err, errlen, "sym is NULL"); return FPLUS_ERR_BADARG; }
     const int64_t widths[3] = {128, 256, 512}, nbs[2] = {32, 64};
@@ -344,6 +344,7 @@ extern "C" int fplus_b200_autotune(fplus_symbolic *sym, const int64_t *Ap, const
     }
     if (best_width) *best_width = bw;
     if (best_nb) *best_nb = bb;
+    if (best_lu) *best_lu = bl;
     if (best_ms) *best_ms = bms;
     return FPLUS_OK;
 }

@@ -146,8 +146,8 @@ void fplus_b200_graph_free(fplus_b200_graph *graph);
  * pivot-block LU, each timed on the device twice (permutation, Ruiz and the fronts), in the given precision
  * (FPLUS_B200_PREC_*), and keeps the fastest in sym for every later factorization on it.  The pivots do not depend on the shape.  best_width, best_nb, best_ms may be NULL. */
 int fplus_b200_autotune(fplus_symbolic *sym, const int64_t *Ap, const int64_t *Ai, const void *Ax, int is_complex,
-                        const fplus_options *opt, int precision, int64_t *best_width, int64_t *best_nb, double *best_ms,
-                        char *err, size_t errlen);
+                        const fplus_options *opt, int precision, int64_t *best_width, int64_t *best_nb, int *best_lu,
+                        double *best_ms, char *err, size_t errlen);
 
 /* The front shape of every later factorization on sym, chosen by the caller instead of the autotuner: at most max_width
  * pivot columns per front (16 .. 4096), nb_chain pivots per dense-chain front (8 .. 64), and the pivot-block LU of the
