@@ -418,7 +418,7 @@ def _csc(Pp, Pi, Px, n, cplx):
     return sp.csc_matrix((x, i, p), shape=(n, n))
 
 
-PROFILE_CLASSES = {0: "schur_gemm", 1: "front_lu", 2: "u12_trsm", 3: "assemble"}
+PROFILE_CLASSES = {0: "schur_gemm", 1: "front_lu", 2: "u12_trsm", 3: "assemble", 4: "front_lu_tall"}
 
 
 def launch_count() -> int:

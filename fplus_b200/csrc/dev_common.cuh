@@ -112,6 +112,26 @@ __device__ __forceinline__ cplx recip(cplx p)
     return cplx{a * d * is, -b * d * is};
 }
 
+// a load that bypasses L1 (values another CTA wrote during this launch)
+__device__ __forceinline__ double ldcg_v(const double *p) { return __ldcg(p); }
+__device__ __forceinline__ cplx ldcg_v(const cplx *p)
+{
+    const double2 v = __ldcg(reinterpret_cast<const double2 *>(p));
+    return cplx{v.x, v.y};
+}
+// a counter read with acquire semantics, and an increment with release semantics (GPU scope): the writes the
+// incrementing thread made, or saw through a barrier, before the increment are visible to a thread whose acquire reads it
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void red_release_add_u32(unsigned *p, unsigned v)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // device status word: the first failure wins (code, then the smallest step / index)
 enum : int {
     ST_OK = 0,
@@ -122,6 +142,7 @@ enum : int {
     ST_SOLVE_ZERO = 5,     // a zero diagonal of U in a solve
     ST_BAD_VALUE = 6,      // a non-finite input value at idx
     ST_RANGE = 7,          // a captured factorization met values beyond 2^+-500 (the range guard needs the host path)
+    ST_WAIT = 8,           // a wait of a multi-CTA pivot search for the other CTAs' candidates ran out of time
 };
 struct DevStatus {
     int code;

@@ -323,129 +323,350 @@ __global__ void __launch_bounds__(512) k_panel(T *__restrict__ W, int64_t ld, in
     }
 }
 
-// The same partial pivoting of panel [k0, k0 + w) for a tall front, on many CTAs at once (a cooperative launch, one CTA
-// per SM): CTA b owns a contiguous range of the rows at positions >= k0.  Per column j: every CTA finds the best of its
-// rows not yet chosen (largest pivot key, ties to the smaller row of B) and posts it (double-buffered by column
-// parity); one grid-wide barrier; every CTA takes the same winner p from the posts, applies the same singular / border
-// decision (a stop ends every CTA at the same column), reads row p's remaining panel entries and updates its own rows
-// (the multiplier, then the rank-1 update of the panel's later columns).  Rows are not moved inside the panel: the
-// chosen rows are marked (ptag), and at the end CTA 0 turns the choices into the interchanges the swapping form would
-// have made (ipiv[j] = the position of the chosen row at step j) and swaps the row ids the same way; the caller then
-// applies ipiv to the panel's own columns too (k_laswp), which leaves exactly the swapping form's result.  ptag holds 0
-// for every row on entry and on exit.
-struct PanelCand { unsigned long long key; long long rid; long long row; };
+// The partial-pivot LU of a tall front's pivot block (nrows x npiv, too large for one CTA's shared memory) in one launch
+// over G CTAs resident at once: one thread-block cluster (G <= MC_CMAX: the CTAs exchange their candidates through
+// distributed shared memory and the cluster barrier), or a cooperative launch (G up to one CTA per SM: the candidates go
+// through global memory and a counter that every CTA increments).  CTA b owns the rows [b * per, b * per + per) and
+// keeps its rows' values of the current 32-column panel in shared memory.  Per pivot column j:
+//   1. each CTA finds the best of its live rows (the largest pivot key, ties to the smaller row of B) and posts it: the
+//      key, the row of B, the position and the row's panel values (cluster: into every CTA's shared memory; grid: into
+//      its global slot, then a release increment of the counter);
+//   2. after the barrier (the cluster barrier; grid: the counter reaching G (j + 1), a bounded wait) every CTA takes the
+//      same winner, applies the same singular / border decision (a stop ends every CTA at the same column), keeps the
+//      winner's panel values (row j of L11\U11) and updates its live rows: the multiplier, then the rank-1 update of the
+//      panel's later columns.
+// After a panel every CTA forms U12 = L11^-1 A12 for the panel's pivot rows (read from W: their owners wrote them before
+// posting the panel's first column), by column chunks and redundantly, and applies A22 -= L21 U12 to its own live rows;
+// one CTA per chunk keeps U12 in Ub for the final block.  Rows never move: the pivot rows are marked, and k_mc_order /
+// k_mc_lout turn the choices (chosen[j] = the position of step j's pivot row) into the final row order (the pivot rows
+// in step order, then the others in their order) and the block in that order.  The operations on every value are those
+// of the swapping form (the same multipliers, the same forward substitution order), so the factors agree with it.
+// The posts alternate by the column's parity.  Grid form: sync[0] is the exit ticket, sync[1] the counter; the last CTA
+// to finish resets both, so they start at zero at the next launch (a CUDA graph replay included).
+constexpr int MC_THREADS = 512, MC_PW = 32, MC_LB = MC_PW + 1, MC_CMAX = 16;
+constexpr unsigned MC_SPIN = 1u << 22;         // polls of the counter before the wait gives up (about a second)
+template <typename T> struct __align__(16) McSlot {
+    long long key, rid, pos, pad;
+    T v[MC_PW];
+};
+template <typename T> __host__ __device__ constexpr int mc_cw() { return VT<T>::cplx_ ? 64 : 128; }
+// shared memory of k_block_lu_mc for `per` rows per CTA (cl: the cluster form's posts too)
+template <typename T> __host__ __device__ constexpr size_t mc_smem(int per, bool cl)
+{
+    return (size_t)(MC_PW * per + MC_PW * MC_LB + MC_PW * mc_cw<T>()) * sizeof(T) +
+           (cl ? (size_t)2 * MC_CMAX * sizeof(McSlot<T>) : 0) + (size_t)per * 8 + (size_t)((per + 15) & ~15);
+}
 
-template <typename T>
-__global__ void __launch_bounds__(512) k_panel_coop(T *__restrict__ W, int64_t ld, int64_t nrows, int64_t nri, int k0, int w,
-                                                   int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
-                                                   int64_t *__restrict__ rowid, int *__restrict__ ipiv, int64_t *__restrict__ chosen,
-                                                   unsigned char *__restrict__ ptag, PanelCand *__restrict__ cand, DevStatus *st,
-                                                   int64_t front)
+template <typename T, bool CL>
+__global__ void __launch_bounds__(MC_THREADS) k_block_lu_mc(T *W, int64_t ld, int nrows, int npiv, int nri, int per,
+                                                          int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
+                                                          const int64_t *__restrict__ rowid, int64_t *__restrict__ chosen,
+                                                          T *__restrict__ Ub, McSlot<T> *gslots, unsigned int *sync,
+                                                          DevStatus *st, int64_t front)
 {
     namespace cg = cooperative_groups;
-    cg::grid_group grid = cg::this_grid();
-    __shared__ unsigned long long s_key[16];
-    __shared__ long long s_rid[16], s_row[16];
-    __shared__ long long s_p;
-    __shared__ int s_stop;
-    __shared__ T s_prow[32];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    constexpr int CW = mc_cw<T>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *S = reinterpret_cast<T *>(smem_raw);              // the panel: S[c * per + r], own row r, panel column c
+    T *Lb = S + MC_PW * per;                             // the panel's pivot rows: Lb[k * MC_LB + c] (L11 \ U11)
+    T *Uc = Lb + MC_PW * MC_LB;                          // a chunk of U12: Uc[k * CW + c]
+    McSlot<T> *cs = reinterpret_cast<McSlot<T> *>(Uc + MC_PW * CW);    // cluster form: the posts, [parity][CTA]
+    long long *rid_s = reinterpret_cast<long long *>(reinterpret_cast<unsigned char *>(cs) +
+                                                     (CL ? (size_t)2 * MC_CMAX * sizeof(McSlot<T>) : 0));
+    unsigned char *live = reinterpret_cast<unsigned char *>(rid_s + per);
+    __shared__ long long s_k[16], s_r[16], s_p[16];
+    __shared__ int s_q[16];
+    __shared__ int s_piv[MC_PW];
+    __shared__ double s_thr[MC_PW];
+    __shared__ int s_stop, s_wait;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = MC_THREADS / 32;
     const int G = gridDim.x, b = blockIdx.x;
-    const int64_t span = nrows - k0, per = (span + G - 1) / G;
-    const int64_t r_lo = k0 + b * per, r_hi = r_lo + per < nrows ? r_lo + per : nrows;
-    if (st->code) return;                                 // read once, before any barrier: the same for every CTA
-    for (int kk = 0; kk < w; kk++) {
-        const int64_t j = k0 + kk;
-        // 1. the best of this CTA's live rows in column j
-        long long bk = -1; long long brid = LLONG_MAX, brow = -1;
-        for (int64_t i = r_lo + tid; i < r_hi; i += blockDim.x) {
-            if (ptag[i]) continue;
-            const long long a = (long long)pivkey(W[i + j * ld]);
-            const long long r = rowid[i];
-            if (a > bk || (a == bk && r < brid)) { bk = a; brid = r; brow = i; }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const long long ok = __shfl_xor_sync(0xffffffffu, bk, o), orid = __shfl_xor_sync(0xffffffffu, brid, o),
-                            orow = __shfl_xor_sync(0xffffffffu, brow, o);
-            if (ok > bk || (ok == bk && orid < brid)) { bk = ok; brid = orid; brow = orow; }
-        }
-        if (lane == 0) { s_key[warp] = (unsigned long long)bk; s_rid[warp] = brid; s_row[warp] = brow; }
-        __syncthreads();
-        if (tid == 0) {
-            long long k2 = (long long)s_key[0], r2 = s_rid[0], w2 = s_row[0];
-            for (int q = 1; q < nw; q++)
-                if ((long long)s_key[q] > k2 || ((long long)s_key[q] == k2 && s_rid[q] < r2)) { k2 = (long long)s_key[q]; r2 = s_rid[q]; w2 = s_row[q]; }
-            PanelCand c; c.key = (unsigned long long)k2; c.rid = r2; c.row = w2;     // key -1 (all ones): no live row
-            cand[(kk & 1) * G + b] = c;
-        }
-        grid.sync();
-        // 2. the winner, the same in every CTA
-        if (tid == 0) {
-            long long k2 = -1, r2 = LLONG_MAX, p = -1;
-            for (int q = 0; q < G; q++) {
-                const PanelCand c = cand[(kk & 1) * G + q];
-                const long long ck = (long long)c.key;
-                if (c.row < 0) continue;
-                if (ck > k2 || (ck == k2 && c.rid < r2)) { k2 = ck; r2 = c.rid; p = c.row; }
-            }
-            const double t = pivot_rel * colmax[fcol + j];
-            int stop = 0;
-            const T pv = p >= 0 ? W[p + j * ld] : VT<T>::zero();
-            if (p < 0 || k2 <= 0 || ((unsigned long long)k2 < pivkey_of_modulus<T>(2.0 * t) && vabs(pv) < t)) {
-                if (b == 0) set_status(st, ST_SINGULAR, fcol + j, p >= 0 ? vabs(pv) : 0.0, t);
-                stop = 1;
-            } else if (p >= nri) {
-                if (b == 0) set_status(st, ST_BORDER, front, vabs(pv), t);
-                stop = 1;
-            }
-            s_stop = stop;
-            s_p = p;
-            if (!stop) {
-                if (b == 0) chosen[kk] = p;
-                if (p >= r_lo && p < r_hi) ptag[p] = 1;   // its owner marks it (only the owner reads its rows' marks)
-            }
+    const int r_lo = b * per, r_hi = r_lo + per < nrows ? r_lo + per : nrows, nmine = r_hi > r_lo ? r_hi - r_lo : 0;
+    const int npr = npiv < nrows ? npiv : nrows;
+    if (tid == 0) { s_stop = st->code != 0; s_wait = 0; }
+    for (int r = tid; r < per; r += MC_THREADS) {
+        live[r] = r < nmine;
+        rid_s[r] = r < nmine ? rowid[r_lo + r] : LLONG_MAX;
+    }
+    if constexpr (CL) {
+        // every CTA of the cluster starts from CTA 0's reading of the status word (the barrier counts must agree)
+        cg::this_cluster().sync();
+        if (tid == 0) s_stop = *cg::this_cluster().map_shared_rank(&s_stop, 0);
+    }
+    __syncthreads();
+    auto better = [](long long k, long long r, long long bk, long long br) { return k > bk || (k == bk && r < br); };
+    for (int p0 = 0; p0 < npr && !s_stop; p0 += MC_PW) {
+        const int w = npr - p0 < MC_PW ? npr - p0 : MC_PW;
+        if (tid < w) s_thr[tid] = pivot_rel * colmax[fcol + p0 + tid];
+        for (int e = tid; e < w * nmine; e += MC_THREADS) {
+            const int c = e / nmine, r = e - c * nmine;
+            S[c * per + r] = W[(r_lo + r) + (int64_t)(p0 + c) * ld];
         }
         __syncthreads();
-        if (s_stop) return;                               // every CTA decides the same at the same column
-        const int64_t p = s_p;
-        if (tid < w - kk) s_prow[tid] = W[p + (k0 + kk + tid) * ld];
-        __syncthreads();
-        // 3. this CTA's live rows: the multiplier and the update of the panel's later columns
-        const T inv = recip(s_prow[0]);
-        for (int64_t i = r_lo + tid; i < r_hi; i += blockDim.x) {
-            if (ptag[i]) continue;
-            const T l = mul(W[i + j * ld], inv);
-            W[i + j * ld] = l;
-            for (int c = 1; c < w - kk; c++) {
-                T *x = W + i + (j + c) * ld;
-                *x = sub(*x, mul(l, s_prow[c]));
+        for (int kk = 0; kk < w; kk++) {
+            const int j = p0 + kk, par = j & 1;
+            // 1. the best of this CTA's live rows in column j, posted
+            long long bk = -1, brid = LLONG_MAX, brow = -1;
+            for (int r = tid; r < nmine; r += MC_THREADS) {
+                if (!live[r]) continue;
+                const long long key = (long long)pivkey(S[kk * per + r]);
+                if (better(key, rid_s[r], bk, brid)) { bk = key; brid = rid_s[r]; brow = r; }
             }
+            for (int o = 16; o > 0; o >>= 1) {
+                const long long ok = __shfl_xor_sync(0xffffffffu, bk, o), orr = __shfl_xor_sync(0xffffffffu, brid, o),
+                                ow = __shfl_xor_sync(0xffffffffu, brow, o);
+                if (better(ok, orr, bk, brid)) { bk = ok; brid = orr; brow = ow; }
+            }
+            if (lane == 0) { s_k[warp] = bk; s_r[warp] = brid; s_p[warp] = brow; }
+            __syncthreads();
+            if (warp == 0) {
+                bk = lane < nw ? s_k[lane] : -1; brid = lane < nw ? s_r[lane] : LLONG_MAX; brow = lane < nw ? s_p[lane] : -1;
+                for (int o = 16; o > 0; o >>= 1) {
+                    const long long ok = __shfl_xor_sync(0xffffffffu, bk, o), orr = __shfl_xor_sync(0xffffffffu, brid, o),
+                                    ow = __shfl_xor_sync(0xffffffffu, brow, o);
+                    if (better(ok, orr, bk, brid)) { bk = ok; brid = orr; brow = ow; }
+                }
+                const T v = (lane < w && brow >= 0) ? S[lane * per + brow] : VT<T>::zero();
+                const long long pos = brow >= 0 ? r_lo + brow : -1;
+                if constexpr (CL) {
+                    cg::cluster_group cl = cg::this_cluster();
+                    for (int d = 0; d < G; d++) {
+                        McSlot<T> *dst = cl.map_shared_rank(cs + par * MC_CMAX + b, d);
+                        if (lane < w) dst->v[lane] = v;
+                        if (lane == 0) { dst->key = bk; dst->rid = brid; dst->pos = pos; }
+                    }
+                } else {
+                    McSlot<T> *my = gslots + (size_t)par * G + b;
+                    if (lane < w) my->v[lane] = v;
+                    if (lane == 0) { my->key = bk; my->rid = brid; my->pos = pos; }
+                    __syncwarp();
+                    if (lane == 0) red_release_add_u32(sync + 1, 1u);
+                }
+            }
+            // 2. the barrier, then the same winner in every CTA
+            long long gk = -1, gr = LLONG_MAX, gp = -1;
+            int gq = -1;
+            if constexpr (CL) {
+                cg::this_cluster().sync();
+            } else {
+                if (tid == 0) {
+                    const unsigned target = (unsigned)G * (unsigned)(j + 1);
+                    unsigned it = 0;
+                    while (ld_acquire_u32(sync + 1) < target && ++it < MC_SPIN) {}
+                    if (it >= MC_SPIN) s_wait = 1;
+                }
+                __syncthreads();
+                if (tid < G && !s_wait) {
+                    const McSlot<T> *c = gslots + (size_t)par * G + tid;
+                    gk = __ldcg(&c->key); gr = __ldcg(&c->rid); gp = __ldcg(&c->pos); gq = tid;
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    const long long ok = __shfl_xor_sync(0xffffffffu, gk, o), orr = __shfl_xor_sync(0xffffffffu, gr, o),
+                                    op = __shfl_xor_sync(0xffffffffu, gp, o);
+                    const int oq = __shfl_xor_sync(0xffffffffu, gq, o);
+                    if (op >= 0 && (gp < 0 || better(ok, orr, gk, gr))) { gk = ok; gr = orr; gp = op; gq = oq; }
+                }
+                if (lane == 0) { s_k[warp] = gk; s_r[warp] = gr; s_p[warp] = gp; s_q[warp] = gq; }
+                __syncthreads();
+            }
+            if (warp == 0) {
+                if constexpr (CL) {
+                    if (lane < G) {
+                        const McSlot<T> *c = cs + par * MC_CMAX + lane;
+                        gk = c->key; gr = c->rid; gp = c->pos; gq = lane;
+                    }
+                } else {
+                    gk = lane < nw ? s_k[lane] : -1; gr = lane < nw ? s_r[lane] : LLONG_MAX;
+                    gp = lane < nw ? s_p[lane] : -1; gq = lane < nw ? s_q[lane] : -1;
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    const long long ok = __shfl_xor_sync(0xffffffffu, gk, o), orr = __shfl_xor_sync(0xffffffffu, gr, o),
+                                    op = __shfl_xor_sync(0xffffffffu, gp, o);
+                    const int oq = __shfl_xor_sync(0xffffffffu, gq, o);
+                    if (op >= 0 && (gp < 0 || better(ok, orr, gk, gr))) { gk = ok; gr = orr; gp = op; gq = oq; }
+                }
+                // the winner's panel values: row j of L11 \ U11
+                T v = VT<T>::zero();
+                if (gq >= 0 && lane < w) {
+                    if constexpr (CL) v = cs[par * MC_CMAX + gq].v[lane];
+                    else v = ldcg_v(&gslots[(size_t)par * G + gq].v[lane]);
+                }
+                if (lane < w) Lb[kk * MC_LB + lane] = v;
+                T pv;
+                if constexpr (VT<T>::cplx_) pv = T{__shfl_sync(0xffffffffu, v.x, kk), __shfl_sync(0xffffffffu, v.y, kk)};
+                else pv = __shfl_sync(0xffffffffu, v, kk);
+                if (lane == 0) {
+                    int stop = 0;
+                    if (s_wait) {
+                        set_status(st, ST_WAIT, front, 0.0, 0.0);
+                        stop = 1;
+                    } else {
+                        const double t = s_thr[kk];
+                        if (gp < 0 || gk <= 0 || ((unsigned long long)gk < pivkey_of_modulus<T>(2.0 * t) && vabs(pv) < t)) {
+                            if (b == 0) set_status(st, ST_SINGULAR, fcol + j, gp >= 0 ? vabs(pv) : 0.0, t);
+                            stop = 1;
+                        } else if (gp >= nri) {
+                            if (b == 0) set_status(st, ST_BORDER, front, vabs(pv), t);
+                            stop = 1;
+                        }
+                    }
+                    s_stop = stop;
+                    if (!stop) {
+                        if (b == 0) chosen[j] = gp;
+                        if (gp >= r_lo && gp < r_hi) live[gp - r_lo] = 0;     // its owner takes it out of the search
+                        s_piv[kk] = (int)gp;
+                    }
+                }
+            }
+            __syncthreads();
+            if (s_stop) break;
+            // 3. this CTA's live rows: the multiplier, then the update of the panel's later columns
+            const T inv = recip(Lb[kk * MC_LB + kk]);
+            for (int r = tid; r < nmine; r += MC_THREADS) {
+                if (!live[r]) continue;
+                const T l = mul(S[kk * per + r], inv);
+                S[kk * per + r] = l;
+                for (int c = kk + 1; c < w; c++) S[c * per + r] = sub(S[c * per + r], mul(l, Lb[kk * MC_LB + c]));
+            }
+            __syncthreads();
+        }
+        if (s_stop) break;
+        for (int e = tid; e < w * nmine; e += MC_THREADS) {
+            const int c = e / nmine, r = e - c * nmine;
+            W[(r_lo + r) + (int64_t)(p0 + c) * ld] = S[c * per + r];
+        }
+        // the trailing columns [p0 + w, npiv) by chunks
+        for (int c0 = p0 + w; c0 < npiv; c0 += CW) {
+            const int cw = npiv - c0 < CW ? npiv - c0 : CW;
+            for (int e = tid; e < w * cw; e += MC_THREADS) {
+                const int k = e % w, c = e / w;
+                Uc[k * CW + c] = ldcg_v(W + s_piv[k] + (int64_t)(c0 + c) * ld);
+            }
+            __syncthreads();
+            // U12 = L11^-1 A12: a thread per column, 8-row blocks in registers (the order of a forward substitution)
+            for (int c = tid; c < cw; c += MC_THREADS) {
+                for (int r0 = 0; r0 < w; r0 += 8) {
+                    T y[8];
+#pragma unroll
+                    for (int q = 0; q < 8; q++) y[q] = r0 + q < w ? Uc[(r0 + q) * CW + c] : VT<T>::zero();
+                    for (int i = 0; i < r0; i++) {
+                        const T xi = Uc[i * CW + c];
+#pragma unroll
+                        for (int q = 0; q < 8; q++) y[q] = sub(y[q], mul(Lb[(r0 + q) * MC_LB + i], xi));
+                    }
+#pragma unroll
+                    for (int q = 1; q < 8; q++)
+#pragma unroll
+                        for (int qq = 0; qq < q; qq++) y[q] = sub(y[q], mul(Lb[(r0 + q) * MC_LB + r0 + qq], y[qq]));
+#pragma unroll
+                    for (int q = 0; q < 8; q++) if (r0 + q < w) Uc[(r0 + q) * CW + c] = y[q];
+                }
+            }
+            __syncthreads();
+            if (b == (c0 / CW) % G)
+                for (int e = tid; e < w * cw; e += MC_THREADS) {
+                    const int k = e % w, c = e / w;
+                    Ub[(p0 + k) + (int64_t)(c0 + c) * npiv] = Uc[k * CW + c];
+                }
+            // A22 -= L21 U12 on this CTA's live rows: 4 x 4 tiles per thread
+            const int tr = (nmine + 3) >> 2, tc = (cw + 3) >> 2;
+            for (int t = tid; t < tr * tc; t += MC_THREADS) {
+                const int rb = (t % tr) * 4, cb = (t / tr) * 4;
+                T acc[4][4];
+#pragma unroll
+                for (int a = 0; a < 4; a++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++) acc[a][q] = VT<T>::zero();
+                for (int k = 0; k < w; k++) {
+                    T lv[4], uv[4];
+#pragma unroll
+                    for (int a = 0; a < 4; a++) lv[a] = rb + a < nmine ? S[k * per + rb + a] : VT<T>::zero();
+#pragma unroll
+                    for (int q = 0; q < 4; q++) uv[q] = cb + q < cw ? Uc[k * CW + cb + q] : VT<T>::zero();
+#pragma unroll
+                    for (int a = 0; a < 4; a++)
+#pragma unroll
+                        for (int q = 0; q < 4; q++) acc[a][q] = add(acc[a][q], mul(lv[a], uv[q]));
+                }
+#pragma unroll
+                for (int a = 0; a < 4; a++) {
+                    const int r = rb + a;
+                    if (r >= nmine || !live[r]) continue;
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        if (cb + q < cw) {
+                            T *x = W + (r_lo + r) + (int64_t)(c0 + cb + q) * ld;
+                            *x = sub(*x, acc[a][q]);
+                        }
+                }
+            }
+            __syncthreads();
         }
     }
-    grid.sync();                                          // every update is done before the choices are turned into swaps
-    if (b == 0 && tid == 0) {
-        // the interchanges of the swapping form: at step t the row chosen sits at position pos(chosen[t]); track the rows
-        // moved so far (at most 2w) in a short list
-        long long mv_row[64], mv_pos[64];
-        int nmv = 0;
-        auto pos_of = [&](long long r) { for (int q = 0; q < nmv; q++) if (mv_row[q] == r) return mv_pos[q]; return r; };
-        auto at_pos = [&](long long ps) { for (int q = 0; q < nmv; q++) if (mv_pos[q] == ps) return mv_row[q]; return ps; };
-        auto set_pos = [&](long long r, long long ps) {
-            for (int q = 0; q < nmv; q++) if (mv_row[q] == r) { mv_pos[q] = ps; return; }
-            mv_row[nmv] = r; mv_pos[nmv] = ps; nmv++;
-        };
-        for (int t = 0; t < w; t++) {
-            const long long jj = k0 + t, r = chosen[t];
-            const long long q = pos_of(r);
-            ipiv[jj] = (int)q;
-            if (q != jj) {
-                const long long x = at_pos(jj);
-                set_pos(x, q);
-                set_pos(r, jj);
-                const int64_t tr = rowid[jj]; rowid[jj] = rowid[q]; rowid[q] = tr;
-            }
+    __syncthreads();
+    if constexpr (CL) {
+        cg::this_cluster().sync();            // no CTA leaves while another may still write its shared memory
+    } else if (tid == 0) {
+        __threadfence();
+        if (atomicAdd(sync, 1u) == (unsigned)(G - 1)) {   // the last CTA out resets the counter and the ticket
+            sync[1] = 0u;
+            __threadfence();
+            sync[0] = 0u;
         }
-        for (int t = 0; t < w; t++) ptag[chosen[t]] = 0;
+    }
+}
+
+// After k_block_lu_mc (one CTA of 1024 threads): the final row order of the front (the pivot rows in step order, then
+// the other rows in their order) into perm, the front's row ids in that order, and the pivot rows' rows of B into p_lu.
+// mark / rid_tmp: scratch of nrows entries.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_mc_order(int nrows, int npr, const int64_t *__restrict__ chosen,
+                                                   int64_t *__restrict__ rowid, int *__restrict__ perm, int64_t f,
+                                                   int64_t *__restrict__ p_lu, int *__restrict__ mark,
+                                                   int64_t *__restrict__ rid_tmp, const DevStatus *st)
+{
+    __shared__ int s_cnt[1024];
+    if (st->code) return;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int i = tid; i < nrows; i += nt) mark[i] = -1;
+    __syncthreads();
+    for (int k = tid; k < npr; k += nt) mark[chosen[k]] = k;
+    __syncthreads();
+    const int seg = (nrows + nt - 1) / nt, lo = tid * seg < nrows ? tid * seg : nrows, hi = lo + seg < nrows ? lo + seg : nrows;
+    int cnt = 0;
+    for (int i = lo; i < hi; i++) cnt += mark[i] < 0;
+    s_cnt[tid] = cnt;
+    __syncthreads();
+    for (int o = 1; o < nt; o <<= 1) {              // inclusive scan of the counts
+        const int v = tid >= o ? s_cnt[tid - o] : 0;
+        __syncthreads();
+        s_cnt[tid] += v;
+        __syncthreads();
+    }
+    int pos = npr + s_cnt[tid] - cnt;
+    for (int i = lo; i < hi; i++) {
+        const int k = mark[i] < 0 ? pos++ : mark[i];
+        perm[k] = i;
+        rid_tmp[k] = rowid[i];
+    }
+    __syncthreads();
+    for (int k = tid; k < nrows; k += nt) {
+        rowid[k] = rid_tmp[k];
+        if (k < npr) p_lu[f + k] = rid_tmp[k];
+    }
+}
+
+// the pivot block in the final row order into the arena: row k of L \ U takes W's row perm[k], except the pivot rows'
+// entries right of their own panel, which are U12 (Ub)
+template <typename T>
+__global__ void k_mc_lout(const T *__restrict__ W, int64_t ld, int64_t nrows, int64_t npiv, int64_t npr,
+                          const int *__restrict__ perm, const T *__restrict__ Ub, T *__restrict__ Lout, const DevStatus *st)
+{
+    if (st->code) return;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nrows * npiv; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = e % nrows, c = e / nrows;
+        const int64_t pend = k < npr ? ((k / MC_PW + 1) * MC_PW < npr ? (k / MC_PW + 1) * MC_PW : npr) : 0;
+        Lout[e] = (k < npr && c >= pend) ? Ub[k + c * npiv] : W[perm[k] + c * ld];
     }
 }
 
@@ -623,13 +844,6 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
-// a load that bypasses L1 (values another CTA wrote during this launch)
-__device__ __forceinline__ double ldcg_v(const double *p) { return __ldcg(p); }
-__device__ __forceinline__ cplx ldcg_v(const cplx *p)
-{
-    const double2 v = __ldcg(reinterpret_cast<const double2 *>(p));
-    return cplx{v.x, v.y};
-}
 
 template <typename T> __device__ __forceinline__ T shfl_xor_v(T v, int m);
 template <> __device__ __forceinline__ double shfl_xor_v<double>(double v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }

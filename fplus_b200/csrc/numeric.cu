@@ -357,8 +357,6 @@ static const size_t SMEM_MAX = 220 * 1024;   // dynamic shared memory opt-in, be
 // the precision form takes a Schur update to the tensor cores from this size on (smaller ones stay FP64: they are cheap,
 // and a 128 x 256 tile would be mostly padding)
 static const int64_t TC_MIN_ROWS = 128, TC_MIN_COLS = 256;
-// panels of fronts with more rows than this are pivoted on every SM at once (k_panel_coop)
-static const int64_t COOP_ROWS = 2048;
 static const double TC_MIN_MADDS = 1 << 24;
 
 template <typename T>
@@ -393,19 +391,55 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     T *La = (T *)N.Larena, *Ua = (T *)N.Uarena, *CB = (T *)N.cbstack;
     const T *Bx = (const T *)N.Bx;
     constexpr int PW = 32;       // panel width of the blocked path
-    // the cooperative panel's buffer and grid (one CTA per SM, if the kernel fits one per SM)
-    static thread_local int coop_grid_cached = -1;
-    if (coop_grid_cached < 0) {
-        int dev = 0, sms = 0, per = 0;
+    // the multi-CTA pivot-block LU (k_block_lu_mc): one cluster of up to mc_cl CTAs, or a cooperative launch of up to one
+    // CTA per SM (mc_sms); its buffer: the grid form's posts (two per CTA), its ticket and counter, the choices, U12 of
+    // the pivot rows, and two row scratches
+    const int per_max = VT<T>::cplx_ ? 256 : 512;
+    static thread_local int mc_sms = -1, mc_cl = 0;
+    if (mc_sms < 0) {
+        int dev = 0, sms = 0, k = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_panel_coop<T>, 512, 0) != cudaSuccess) { per = 0; (void)cudaGetLastError(); }
-        coop_grid_cached = per >= 1 ? sms : 0;
+        if (cudaFuncSetAttribute(k_block_lu_mc<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, k_block_lu_mc<T, false>, MC_THREADS, mc_smem<T>(per_max, false)) != cudaSuccess)
+            k = 0;
+        (void)cudaGetLastError();
+        mc_sms = k >= 1 ? sms : 0;
+        // the largest cluster the device places with the cluster form's largest shared memory
+        if (cudaFuncSetAttribute(k_block_lu_mc<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX) == cudaSuccess &&
+            cudaFuncSetAttribute(k_block_lu_mc<T, true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+            for (int csz = MC_CMAX; csz >= 4 && mc_cl == 0; csz /= 2) {
+                cudaLaunchConfig_t oc = {};
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeClusterDimension;
+                at[0].val.clusterDim.x = (unsigned)csz; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+                oc.gridDim = dim3((unsigned)csz); oc.blockDim = dim3(MC_THREADS); oc.dynamicSmemBytes = mc_smem<T>(per_max, true);
+                oc.attrs = at; oc.numAttrs = 1;
+                int ncl = 0;
+                if (cudaOccupancyMaxActiveClusters(&ncl, (const void *)k_block_lu_mc<T, true>, &oc) == cudaSuccess && ncl >= 1) mc_cl = csz;
+            }
+        }
+        (void)cudaGetLastError();
     }
-    const int coop_grid = coop_grid_cached;
-    if (P.max_nrows > COOP_ROWS &&
-        (rc = ensure_async(N, &N.coopbuf, &N.cap_coop, (size_t)((P.max_nrows + 255) & ~(int64_t)255) + PW * 8 +
-                                                          (size_t)2 * 160 * sizeof(PanelCand), err, errlen))) return rc;
+    auto r256 = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t mc_slots = r256((size_t)2 * (mc_sms > 0 ? mc_sms : 1) * sizeof(McSlot<T>)), mc_tk = 256,
+                 mc_ch = r256((size_t)(P.max_npiv > 0 ? P.max_npiv : 1) * 8),
+                 mc_ub = r256((size_t)(P.max_npiv > 0 ? P.max_npiv : 1) * (P.max_npiv > 0 ? P.max_npiv : 1) * vs),
+                 mc_mark = r256((size_t)(P.max_nrows > 0 ? P.max_nrows : 1) * 4), mc_rid = r256((size_t)(P.max_nrows > 0 ? P.max_nrows : 1) * 8);
+    bool any_mc = false;
+    for (const Front &F : P.fronts)
+        if (front_lu_smem(F.nrows, F.npiv, vs) > SMEM_MAX) { any_mc = true; break; }
+    any_mc = any_mc && (mc_sms > 0 || mc_cl > 0);
+    if (any_mc) {
+        if ((rc = ensure_async(N, &N.coopbuf, &N.cap_coop, mc_slots + mc_tk + mc_ch + mc_ub + mc_mark + mc_rid, err, errlen))) return rc;
+        CK(cudaMemsetAsync((char *)N.coopbuf + mc_slots, 0, mc_tk, s));      // the ticket and the counter start at zero
+    }
+    McSlot<T> *mc_slot = (McSlot<T> *)N.coopbuf;
+    unsigned int *mc_sync = (unsigned int *)((char *)N.coopbuf + mc_slots);
+    int64_t *mc_chosen = (int64_t *)((char *)N.coopbuf + mc_slots + mc_tk);
+    T *mc_U = (T *)((char *)N.coopbuf + mc_slots + mc_tk + mc_ch);
+    int *mc_markp = (int *)((char *)N.coopbuf + mc_slots + mc_tk + mc_ch + mc_ub);
+    int64_t *mc_ridp = (int64_t *)((char *)N.coopbuf + mc_slots + mc_tk + mc_ch + mc_ub + mc_mark);
     const int TB = VT<T>::cplx_ ? 32 : 64;    // rows per TRSM block of U12
     const int64_t nf = (int64_t)P.fronts.size();
     const double fm = VT<T>::cplx_ ? 8.0 : 2.0;     // flops per multiply-add
@@ -480,9 +514,9 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         {
             double fl = 0;
             for (int64_t k = 0; k < std::min(np, nr); k++) fl += (double)(nr - k - 1) * (double)(np - k);
-            prof.begin(st, PROF_LU, fm * fl, 2.0 * (double)(nr * np) * vs);
+            prof.begin(st, sm <= SMEM_MAX ? PROF_LU : PROF_LU_TALL, fm * fl, 2.0 * (double)(nr * np) * vs);
         }
-        if (N.lu_variant == 3 && use_lu3(nr, np, vs)) {
+        if ((N.lu_variant & 3) == 3 && use_lu3(nr, np, vs)) {
             const size_t sm3 = front_lu3_smem(nr, np, vs);
             if (pa.on) {
                 CK(launch_pdl(k_front_lu3<T>, 1, LU3_THREADS, sm3, st, (const T *)W, ld, (int)nr, (int)np, (int)F.nri, F.f,
@@ -504,51 +538,72 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
                                                 Lf, perm, N.p_lu, N.st, fi, pa), note_launch();
         } else {
             const int64_t npr = std::min(np, nr);
-            // tall panels on many SMs at once (a cooperative launch); the marks start cleared
-            const bool coop = nr > COOP_ROWS && coop_grid > 1;
-            unsigned char *ptag = (unsigned char *)N.coopbuf;
-            int64_t *chosen = (int64_t *)((char *)N.coopbuf + ((P.max_nrows + 255) & ~(int64_t)255));
-            PanelCand *cand = (PanelCand *)(chosen + PW);
-            if (coop) CK(cudaMemsetAsync(ptag, 0, (size_t)nr, st));
-            for (int64_t k0 = 0; k0 < npr; k0 += PW) {
-                const int w = (int)std::min<int64_t>(PW, npr - k0);
-                bool done = false;
-                if (coop && nr - k0 > COOP_ROWS) {
-                    const int G = (int)std::min<int64_t>(coop_grid, (nr - k0 + 255) / 256);
-                    int64_t *rid = N.rowid + F.row_off;
-                    int *ip = N.ipiv + F.f;
-                    int k0i = (int)k0, wi = w;
-                    int64_t fcol = F.f, nri = F.nri, frow = fi, ldl = ld, nrl = nr;
+            // the multi-CTA pivoting in one launch, when the rows fit the CTAs (at most per_max rows each): one cluster
+            // when it holds them, else a cooperative launch
+            bool done = false;
+            if (any_mc && !(N.lu_variant & 4)) {
+                const bool cl = mc_cl > 0 && nr <= (int64_t)mc_cl * per_max;
+                int G = cl ? (int)std::min<int64_t>(mc_cl, std::max<int64_t>(2, (nr + 255) / 256))
+                           : (int)std::min<int64_t>(mc_sms, std::max<int64_t>(1, (nr + 63) / 64));
+                if ((nr + G - 1) / G > per_max) G = (int)((nr + per_max - 1) / per_max);
+                const int per = (int)((nr + G - 1) / G);
+                const int64_t *rid = N.rowid + F.row_off;
+                cudaError_t le = cudaErrorInvalidValue;
+                if (cl && G <= mc_cl) {
+                    cudaLaunchConfig_t cfg = {};
+                    cudaLaunchAttribute at[1];
+                    at[0].id = cudaLaunchAttributeClusterDimension;
+                    at[0].val.clusterDim.x = (unsigned)G; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+                    cfg.gridDim = dim3((unsigned)G); cfg.blockDim = dim3(MC_THREADS); cfg.dynamicSmemBytes = mc_smem<T>(per, true);
+                    cfg.stream = st; cfg.attrs = at; cfg.numAttrs = 1;
+                    le = cudaLaunchKernelEx(&cfg, k_block_lu_mc<T, true>, W, ld, (int)nr, (int)np, (int)F.nri, per, F.f,
+                                            (const double *)N.colmax, pivot_rel, rid, mc_chosen, mc_U, mc_slot, mc_sync, N.st, fi);
+                } else if (!cl && mc_sms > 0 && G <= mc_sms) {
+                    T *Wp = W;
+                    int64_t ldl = ld, fcol = F.f, frow = fi;
+                    int nri_ = (int)nr, npi = (int)np, nrii = (int)F.nri, peri = per;
                     const double *cm = N.colmax;
                     double prel = pivot_rel;
+                    int64_t *chs = mc_chosen;
+                    T *ub = mc_U;
+                    McSlot<T> *sl = mc_slot;
+                    unsigned int *sy = mc_sync;
                     DevStatus *stp = N.st;
-                    T *Wp = W;
-                    void *args[] = {&Wp, &ldl, &nrl, &nri, &k0i, &wi, &fcol, &cm, &prel, &rid, &ip, &chosen, &ptag, &cand, &stp, &frow};
-                    if (cudaLaunchCooperativeKernel((const void *)k_panel_coop<T>, G, 512, args, 0, st) == cudaSuccess) {
-                        note_launch();
-                        // the panel's own columns take the interchanges too
-                        k_laswp<T><<<nblk(w, 128), 128, 0, st>>>(W, ld, N.ipiv + F.f, (int)k0, w, k0, k0 + w, N.st), note_launch();
-                        done = true;
-                    } else (void)cudaGetLastError();
+                    void *args[] = {&Wp, &ldl, &nri_, &npi, &nrii, &peri, &fcol, &cm, &prel, &rid, &chs, &ub, &sl, &sy, &stp, &frow};
+                    le = cudaLaunchCooperativeKernel((const void *)k_block_lu_mc<T, false>, G, MC_THREADS, args,
+                                                     mc_smem<T>(per, false), st);
                 }
-                if (!done)
+                if (le == cudaSuccess) {
+                    note_launch();
+                    k_mc_order<T><<<1, 1024, 0, st>>>((int)nr, (int)npr, mc_chosen, N.rowid + F.row_off, perm, F.f, N.p_lu,
+                                                      mc_markp, mc_ridp, N.st), note_launch();
+                    k_mc_lout<T><<<nblk(nr * np), 256, 0, st>>>(W, ld, nr, np, npr, perm, mc_U, Lf, N.st), note_launch();
+                    done = true;
+                } else (void)cudaGetLastError();
+            }
+            if (!done) {
+                // one CTA per 32-column panel, then the swaps, the unit-lower solve and the update of the block's later
+                // columns
+                for (int64_t k0 = 0; k0 < npr; k0 += PW) {
+                    const int w = (int)std::min<int64_t>(PW, npr - k0);
                     k_panel<T><<<1, 512, 0, st>>>(W, ld, nr, F.nri, (int)k0, w, F.f, N.colmax, pivot_rel, N.rowid + F.row_off,
                                                  N.ipiv + F.f, N.st, fi), note_launch();
-                if (k0 > 0) k_laswp<T><<<nblk(k0, 128), 128, 0, st>>>(W, ld, N.ipiv + F.f, (int)k0, w, 0, k0, N.st), note_launch();
-                if (k0 + w < np) {
-                    k_laswp<T><<<nblk(np - k0 - w, 128), 128, 0, st>>>(W, ld, N.ipiv + F.f, (int)k0, w, k0 + w, np, N.st), note_launch();
-                    k_trsm_unit<T><<<nblk(np - k0 - w, 128), 128, 0, st>>>(W, ld, (int)k0, w, k0 + w, np, N.st), note_launch();
-                    const int64_t M = nr - k0 - w, Nn = np - k0 - w;
-                    if (M > 0) {
-                        dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((Nn + GBN - 1) / GBN));
-                        T *C = W + (k0 + w) + (k0 + w) * ld;
-                        k_gemm_sub<T><<<g, 256, 0, st>>>(M, Nn, w, W + (k0 + w) + k0 * ld, ld, W + k0 + (k0 + w) * ld, ld,
-                                                         C, ld, nullptr, C, ld, N.st), note_launch();
+                    if (k0 > 0) k_laswp<T><<<nblk(k0, 128), 128, 0, st>>>(W, ld, N.ipiv + F.f, (int)k0, w, 0, k0, N.st), note_launch();
+                    if (k0 + w < np) {
+                        k_laswp<T><<<nblk(np - k0 - w, 128), 128, 0, st>>>(W, ld, N.ipiv + F.f, (int)k0, w, k0 + w, np, N.st), note_launch();
+                        k_trsm_unit<T><<<nblk(np - k0 - w, 128), 128, 0, st>>>(W, ld, (int)k0, w, k0 + w, np, N.st), note_launch();
+                        const int64_t M = nr - k0 - w, Nn = np - k0 - w;
+                        if (M > 0) {
+                            dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((Nn + GBN - 1) / GBN));
+                            T *C = W + (k0 + w) + (k0 + w) * ld;
+                            k_gemm_sub<T><<<g, 256, 0, st>>>(M, Nn, w, W + (k0 + w) + k0 * ld, ld, W + k0 + (k0 + w) * ld, ld,
+                                                             C, ld, nullptr, C, ld, N.st), note_launch();
+                        }
                     }
                 }
+                k_left_finish<T><<<nblk(nr * np), 256, 0, st>>>(W, ld, nr, np, N.ipiv + F.f, perm, N.rowid + F.row_off, F.f, N.p_lu,
+                                                               Lf, N.st), note_launch();
             }
-            k_left_finish<T><<<nblk(nr * np), 256, 0, st>>>(W, ld, nr, np, N.ipiv + F.f, perm, N.rowid + F.row_off, F.f, N.p_lu,
-                                                           Lf, N.st), note_launch();
         }
         prof.end(st);
         if (nr < np) { k_set_singular<<<1, 1, 0, st>>>(N.st, F.f + nr), note_launch(); }
@@ -693,6 +748,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     CK(cudaStreamSynchronize(s));
     prof.flush();
     if (h.tc_err) { errf(err, errlen, "factorization: a tensor-core Schur update timed out (status %u)", h.tc_err); return FPLUS_ERR_GPU; }
+    if (h.code == ST_WAIT) { errf(err, errlen, "factorization: a multi-CTA pivot search in front %ld timed out", (long)h.idx); return FPLUS_ERR_GPU; }
     if (h.code == ST_BORDER) { *border_front = h.idx; return FPLUS_OK; }
     if (h.code == ST_SINGULAR) {
         errf(err, errlen, "Near-zero or zero pivot %.6e at step %ld (threshold %.6e). Matrix is singular.", h.best, (long)h.idx, h.thr);
@@ -1120,7 +1176,7 @@ int dev_status_rc(DevNum &N, int *rc, char *err, size_t errlen)
 {
     DevStatus h;
     CK(cudaMemcpy(&h, N.st, sizeof h, cudaMemcpyDeviceToHost));
-    if (h.tc_err) *rc = FPLUS_ERR_GPU;
+    if (h.tc_err || h.code == ST_WAIT) *rc = FPLUS_ERR_GPU;
     else if (h.code == ST_SINGULAR || h.code == ST_ZERO_ROW || h.code == ST_ZERO_COL || h.code == ST_SOLVE_ZERO) *rc = FPLUS_ERR_SINGULAR;
     else if (h.code != ST_OK) *rc = FPLUS_ERR_BADARG;
     else *rc = FPLUS_OK;

@@ -13,7 +13,7 @@ struct DevStatus;
 
 // per-class device timing (fplus_b200_profile): 0 Schur GEMM into the CB, 1 pivot-block LU, 2 U12 (gather + TRSM),
 // 3 assembly and extend-add
-enum { PROF_SCHUR = 0, PROF_LU = 1, PROF_U12 = 2, PROF_ASM = 3, PROF_NCLASS = 4 };
+enum { PROF_SCHUR = 0, PROF_LU = 1, PROF_U12 = 2, PROF_ASM = 3, PROF_LU_TALL = 4, PROF_NCLASS = 5 };
 struct ProfClass { double ms = 0, flops = 0, bytes = 0; long long count = 0; };
 void prof_enable(int on);
 ProfClass prof_read(int cls);
@@ -68,9 +68,10 @@ struct DevNum {
     // the precision form: the arithmetic of the large fronts' Schur updates (schur_tc.hpp), their operand workspace, and
     // the updates that ran on the tensor cores in the last factorization
     int prec = 0;
-    void *coopbuf = nullptr;       // the cooperative panel: row marks (max_nrows bytes), the choices, the CTAs' posts
+    void *coopbuf = nullptr;       // the multi-CTA pivot-block LU: the CTAs' posts, the ticket, the choices, U12, row scratch
     size_t cap_coop = 0;
-    int lu_variant = 2;            // the pivot-block LU kernel of the small fronts (k_front_lu2 or k_front_lu3)
+    int lu_variant = 2;            // the small fronts' pivot-block LU (2: k_front_lu2, 3: k_front_lu3); + 4: the tall
+                                   // blocks by one CTA per 32-column panel instead of k_block_lu_mc
     int capture = 0;               // the launches are being captured into a CUDA graph: no host copies, waits or decisions
     void *gm_buf = nullptr;        // GMRES-IR: the Krylov basis and its vectors
     size_t cap_gm = 0;

@@ -151,8 +151,9 @@ int fplus_b200_autotune(fplus_symbolic *sym, const int64_t *Ap, const int64_t *A
 
 /* The front shape of every later factorization on sym, chosen by the caller instead of the autotuner: at most max_width
  * pivot columns per front (16 .. 4096), nb_chain pivots per dense-chain front (8 .. 64), and the pivot-block LU of the
- * small fronts (2: one barrier per pivot step; 3: blocked 8-column panels).  The pivots do not depend on these.  No
- * counterpart in FPLUS. */
+ * small fronts (2: one barrier per pivot step; 3: blocked 8-column panels), plus 4 to pivot the pivot blocks too large
+ * for one CTA by one CTA per 32-column panel instead of all SMs in one launch (6, 7).  The pivots do not depend on these.
+ * No counterpart in FPLUS. */
 int fplus_b200_set_front_shape(fplus_symbolic *sym, int64_t max_width, int64_t nb_chain, int lu_variant);
 
 /* The device time of a batch: from the earliest start of the factorizations nums[0 .. count) (their first operation) to
@@ -195,8 +196,8 @@ long long fplus_b200_launch_count(void);
 
 /* Device timing of the factorization's kernels by class, for measurement: when on, every launch of a class is bracketed
  * by CUDA events (a small perturbation; off by default).  Turning it on clears the totals.  Classes: 0 the Schur-
- * complement GEMM into the contribution block, 1 the pivot-block LU, 2 U12 (gather + TRSM), 3 assembly and extend-add.
- * profile_read returns the class's total device milliseconds, launches, and the algorithmic flops and bytes of those
+ * complement GEMM into the contribution block, 1 the pivot-block LU of the fronts one CTA holds, 2 U12 (gather + TRSM),
+ * 3 assembly and extend-add, 4 the pivot-block LU of the taller fronts (all SMs in one launch).  profile_read returns the class's total device milliseconds, launches, and the algorithmic flops and bytes of those
  * launches. */
 void fplus_b200_profile(int on);
 int fplus_b200_profile_read(int cls, double *ms, long long *count, double *flops, double *bytes);

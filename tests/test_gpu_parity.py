@@ -244,3 +244,26 @@ def test_blocked_pivot_block_lu_matches_oracle(gpu, name):
     assert np.array_equal(N.p, orc.p)
     L, U, _ = N.factors()
     assert _rel(L, orc.L) <= FACTOR_TOL and _rel(U, orc.U) <= FACTOR_TOL
+
+
+@pytest.mark.parametrize("variant", [2, 6])
+@pytest.mark.parametrize("cplx", [False, True])
+def test_tall_pivot_blocks_match_oracle(gpu, cplx, variant):
+    """Pivot blocks too large for one CTA (a 20^3 / 16^3 stencil: 256 pivots, hundreds to thousands of rows), pivoted by
+    all SMs in one launch (k_block_lu_mc, variant 2) and by one CTA per 32-column panel (variant 6): the oracle's pivots,
+    and L and U within 1e-12."""
+    g = 16 if cplx else 20
+    n, Ap, Ai, Ax = W.convdiff3d(g, 3)
+    if cplx:
+        Ax = Ax + 0.25j * np.random.default_rng(21).uniform(-1, 1, Ax.size)
+    S = F.analyze(n, Ap, Ai)
+    S.set_front_shape(256, 64, variant)
+    N = S.factor(Ax)
+    orc = O.OracleLU(n, Ap, Ai, Ax, S.row_perm, S.col_perm)
+    assert np.array_equal(N.p, orc.p), "pivot order differs from the oracle"
+    lo, uo = orc.fro_norms()
+    lf, uf = N.factor_norms()
+    assert abs(lf - lo) <= 1e-12 * lo and abs(uf - uo) <= 1e-12 * uo
+    b = W.rhs(n, 1, cplx, 4)[0]
+    x = N.solve(b)
+    assert O.backward_error(n, Ap, Ai, Ax, x, b) <= 1e-14
