@@ -5,6 +5,7 @@
 #include <climits>
 #include <cooperative_groups.h>
 #include "dev_common.cuh"
+#include "plan.hpp"
 
 namespace fpl {
 
@@ -1820,25 +1821,37 @@ __global__ void __launch_bounds__(512) k_fwdL3(const T *__restrict__ L, int64_t 
 // reported as ST_SOLVE_ZERO).  The block is L[r + c * ld] (the front's L block: U11 on and above the diagonal).
 template <typename T, bool UPPER>
 __device__ void blk_trisolve(const T *__restrict__ L, int64_t ld, int np, T *x, int64_t nrhs, T *sT, T *dinv, DevStatus *st,
-                             int64_t f)
+                             int64_t f, int *zflag = nullptr)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
     const int nb = (np + 63) / 64;
     for (int bb = 0; bb < nb; bb++) {
         const int bi = UPPER ? nb - 1 - bb : bb;
         const int r0 = bi * 64, w = np - r0 < 64 ? np - r0 : 64;
-        for (int e = tid; e < w * w; e += blockDim.x) {
-            const int i = e % w, k = e / w;
-            sT[i + k * 64] = L[(r0 + i) + (int64_t)(r0 + k) * ld];
+        // the diagonal block into shared memory, eight loads in flight per thread
+        for (int e0 = tid; e0 < w * w; e0 += 8 * blockDim.x) {
+            T lv[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const int e = e0 + q * blockDim.x;
+                lv[q] = e < w * w ? L[(r0 + e % w) + (int64_t)(r0 + e / w) * ld] : VT<T>::zero();
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const int e = e0 + q * blockDim.x;
+                if (e < w * w) sT[e % w + (e / w) * 64] = lv[q];
+            }
         }
         if (UPPER)
             for (int i = tid; i < w; i += blockDim.x) {
                 const T d = L[(r0 + i) + (int64_t)(r0 + i) * ld];
-                if (is_zero(d)) set_status(st, ST_SOLVE_ZERO, f + r0 + i, 0, 0);
+                if (is_zero(d)) { set_status(st, ST_SOLVE_ZERO, f + r0 + i, 0, 0); if (zflag) *zflag = 1; }
                 dinv[i] = is_zero(d) ? VT<T>::zero() : recip(d);
             }
         __syncthreads();
-        if (UPPER && st->code == ST_SOLVE_ZERO) return;
+        // zflag (shared, cleared by the caller): this front's own zero diagonal, the same answer for every thread while
+        // other CTAs may be writing the status word
+        if (UPPER && (zflag ? *zflag != 0 : st->code == ST_SOLVE_ZERO)) return;
         for (int64_t r = warp; r < nrhs; r += nw) {
             T *xr = x + r * np + r0;
             T a = lane < w ? xr[lane] : VT<T>::zero(), b = lane + 32 < w ? xr[lane + 32] : VT<T>::zero();
@@ -1865,8 +1878,17 @@ __device__ void blk_trisolve(const T *__restrict__ L, int64_t ld, int np, T *x, 
             for (int64_t e = tid; e < (int64_t)(o1 - o0) * nrhs; e += blockDim.x) {
                 const int row = o0 + (int)(e % (o1 - o0));
                 const int64_t r = e / (o1 - o0);
+                const T *Lr = L + row + (int64_t)r0 * ld;
+                const T *xr = x + r * np + r0;
                 T acc = VT<T>::zero();
-                for (int k = 0; k < w; k++) acc = add(acc, mul(L[row + (int64_t)(r0 + k) * ld], x[r * np + r0 + k]));
+                for (int k0 = 0; k0 < w; k0 += 16) {         // sixteen loads of L in flight, the sum in k order
+                    T lv[16];
+#pragma unroll
+                    for (int q = 0; q < 16; q++) lv[q] = k0 + q < w ? Lr[(int64_t)(k0 + q) * ld] : VT<T>::zero();
+#pragma unroll
+                    for (int q = 0; q < 16; q++)
+                        if (k0 + q < w) acc = add(acc, mul(lv[q], xr[k0 + q]));
+                }
                 x[r * np + row] = sub(x[r * np + row], acc);
             }
         __syncthreads();
@@ -2885,6 +2907,484 @@ __global__ void k_vupdate(const T *__restrict__ V, int64_t n, int nv, const T *_
         T s = w[i];
         for (int v = 0; v < nv; v++) s = sub(s, mul(V[(int64_t)v * n + i], h[v]));
         w[i] = scal(s, scale);
+    }
+}
+
+// =====================================================================================================================
+// the level-scheduled solve
+// =====================================================================================================================
+// The fronts of one level of the tree (the same height above the leaves) are independent in every sweep, so each sweep
+// runs level by level: one launch for the level's small fronts (a CTA each), the others front by front.  The two
+// forward sweeps pass contribution vectors up the tree instead of scattering into a global vector, so no two fronts of a
+// level write the same entry and every sum is taken in a fixed order: front f's vector occupies the entries [row_off,
+// row_off + nrows) (the L sweep: its rows in their final order) or [col_off, col_off + ncols) (the U^T sweep: its
+// columns) of a buffer VB laid out one right-hand side after another (stride: the plan's total front rows, or its total
+// front columns).  A front's vector entry gathers the right-hand side where the row (column) enters the tree, then, in
+// the children's order, the children's contribution entries that land on it (the lists rsp/rsi over the plan's rows,
+// csp/csi over its columns).
+constexpr int SV_RC = 8;              // right-hand sides per pass of the one-CTA sweep kernels
+constexpr int SV_THREADS = 256;
+
+// L sweep (trans 0) of a level's small fronts, a CTA each: the front's vector in its final row order (position k holds
+// initial row perm[k]: the entering row's right-hand side, then the children's entries that land on it), x = L11^-1 v
+// (the pivot rows, into Y in pivot order), then the contribution u = v[np:] - L21 x into VB
+template <typename T>
+__global__ void __launch_bounds__(SV_THREADS) k_sv_fwdL(const SvFront *__restrict__ fr, const int *__restrict__ list,
+                                                        const T *__restrict__ La, const int64_t *__restrict__ rowinit,
+                                                        const int *__restrict__ permall, const int64_t *__restrict__ rsp,
+                                                        const int64_t *__restrict__ rsi, const T *__restrict__ R,
+                                                        T *__restrict__ Y, T *__restrict__ VB, int64_t vstride, int64_t n,
+                                                        int nrhs)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const SvFront F = fr[list[blockIdx.x]];
+    const int nr = (int)F.nr, np = (int)(F.np < F.nr ? F.np : F.nr), nri = (int)F.nri, tid = threadIdx.x;
+    T *v = reinterpret_cast<T *>(smem_raw);          // nr x SV_RC (ld nr)
+    T *x = v + nr * SV_RC;                           // np x SV_RC (ld np)
+    T *sT = x + np * SV_RC;                          // 64 x np
+    const T *L = La + F.L_off;
+    const int *perm = permall + F.row_off;
+    pdl_wait();
+    pdl_trigger();
+    for (int r0 = 0; r0 < nrhs; r0 += SV_RC) {
+        const int rc = nrhs - r0 < SV_RC ? nrhs - r0 : SV_RC;
+        for (int e = tid; e < nr * rc; e += SV_THREADS) {
+            const int k = e % nr, r = e / nr, i = F.np > 0 ? perm[k] : k;     // (a front without pivots keeps its order)
+            const int64_t g = F.row_off + i, ri = rowinit[g];
+            T val = (i < nri && ri >= 0) ? R[ri + (int64_t)(r0 + r) * n] : VT<T>::zero();
+            for (int64_t q = rsp[g]; q < rsp[g + 1]; q++) val = add(val, VB[rsi[q] + (int64_t)(r0 + r) * vstride]);
+            v[k + r * nr] = val;
+        }
+        __syncthreads();
+        for (int e = tid; e < np * rc; e += SV_THREADS) x[e] = v[e % np + (e / np) * nr];
+        __syncthreads();
+        blk_trisolve<T, false>(L, nr, np, x, rc, sT, nullptr, nullptr, 0);
+        for (int e = tid; e < np * rc; e += SV_THREADS) Y[F.f + e % np + (int64_t)(r0 + e / np) * n] = x[e];
+        const int m = nr - np;
+        for (int e = tid; e < m * rc; e += SV_THREADS) {
+            const int t = e % m, r = e / m;
+            T acc = VT<T>::zero();
+            for (int k0 = 0; k0 < np; k0 += 8) {
+                T lv[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++) lv[q] = k0 + q < np ? L[np + t + (int64_t)(k0 + q) * nr] : VT<T>::zero();
+#pragma unroll
+                for (int q = 0; q < 8; q++)
+                    if (k0 + q < np) acc = add(acc, mul(lv[q], x[k0 + q + r * np]));
+            }
+            VB[F.row_off + np + t + (int64_t)(r0 + r) * vstride] = sub(v[np + t + r * nr], acc);
+        }
+        __syncthreads();
+    }
+}
+
+// a larger front's vector (the L sweep), in its final row order, into its own entries of VB
+template <typename T>
+__global__ void k_sv_gatherL(int64_t row_off, int64_t nr, int64_t nri, const int64_t *__restrict__ rowinit,
+                             const int *__restrict__ perm, const int64_t *__restrict__ rsp, const int64_t *__restrict__ rsi,
+                             const T *__restrict__ R, T *__restrict__ VB, int64_t vstride, int64_t n, int64_t nrhs)
+{
+    // perm == nullptr: a front without pivots, in its initial order
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nr * nrhs; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = e % nr, r = e / nr, i = perm ? perm[k] : k, g = row_off + i, ri = rowinit[g];
+        T val = (i < nri && ri >= 0) ? R[ri + r * n] : VT<T>::zero();
+        for (int64_t q = rsp[g]; q < rsp[g + 1]; q++) val = add(val, VB[rsi[q] + r * vstride]);
+        VB[row_off + k + r * vstride] = val;
+    }
+}
+
+// R[rowid[k]] = the front's vector entry k (its rows in their final order): a front's gathered vector into the row-space
+// vector, for the sequential sweep that takes over from it
+template <typename T>
+__global__ void k_sv_toR(const T *__restrict__ Vf, int64_t vstride, int64_t nr, const int64_t *__restrict__ rowid,
+                         T *__restrict__ R, int64_t n, int64_t nrhs)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nr * nrhs; e += (int64_t)gridDim.x * blockDim.x)
+        R[rowid[e % nr] + (e / nr) * n] = Vf[e % nr + (e / nr) * vstride];
+}
+
+// Y[j] = R[p_lu[j]] for the pivots j in [j0, n)
+template <typename T>
+__global__ void k_gather_range(T *__restrict__ Y, const T *__restrict__ R, const int64_t *__restrict__ p_lu, int64_t j0,
+                               int64_t n, int64_t nrhs)
+{
+    const int64_t m = n - j0;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m * nrhs; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t j = j0 + e % m, r = e / m;
+        Y[j + r * n] = R[p_lu[j] + r * n];
+    }
+}
+
+// Y[f + k] = the front's solved pivot entries (rows [0, np) of its VB vector)
+template <typename T>
+__global__ void k_sv_put(const T *__restrict__ Vf, int64_t vstride, int64_t np, T *__restrict__ Y, int64_t f, int64_t n,
+                         int64_t nrhs)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < np * nrhs; e += (int64_t)gridDim.x * blockDim.x)
+        Y[f + e % np + (e / np) * n] = Vf[e % np + (e / np) * vstride];
+}
+
+// U sweep (trans 0) of a level's small fronts, a CTA each: x = U11^-1 (y - U12 x[CB columns]) (the CB columns' x from
+// the fronts above, already solved)
+template <typename T>
+__global__ void __launch_bounds__(SV_THREADS) k_sv_bwdU(const SvFront *__restrict__ fr, const int *__restrict__ list,
+                                                        const T *__restrict__ La, const T *__restrict__ Ua,
+                                                        const int64_t *__restrict__ cols, const T *__restrict__ Y,
+                                                        T *__restrict__ X, int64_t n, int nrhs, DevStatus *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_zero;
+    const SvFront F = fr[list[blockIdx.x]];
+    const int np = (int)F.np, ncb = (int)(F.nc - F.np), tid = threadIdx.x;
+    T *x = reinterpret_cast<T *>(smem_raw);          // np x SV_RC
+    T *sT = x + np * SV_RC;                          // 64 x np
+    T *dinv = sT + 64 * np;                          // 64
+    const T *U12 = Ua + F.U_off;
+    const int64_t *cb = cols + F.col_off + np;
+    pdl_wait();
+    pdl_trigger();
+    for (int r0 = 0; r0 < nrhs; r0 += SV_RC) {
+        const int rc = nrhs - r0 < SV_RC ? nrhs - r0 : SV_RC;
+        for (int e = tid; e < np * rc; e += SV_THREADS) {
+            const int i = e % np, r = e / np;
+            const T *xr = X + (int64_t)(r0 + r) * n;
+            T acc = VT<T>::zero();
+            for (int t = 0; t < ncb; t++) acc = add(acc, mul(U12[i + (int64_t)t * np], xr[cb[t]]));
+            x[e] = sub(Y[F.f + i + (int64_t)(r0 + r) * n], acc);
+        }
+        if (tid == 0) s_zero = 0;
+        __syncthreads();
+        blk_trisolve<T, true>(La + F.L_off, F.nr, np, x, rc, sT, dinv, st, F.f, &s_zero);
+        if (s_zero) return;
+        for (int e = tid; e < np * rc; e += SV_THREADS) X[F.f + e % np + (int64_t)(r0 + e / np) * n] = x[e];
+        __syncthreads();
+    }
+}
+
+// U^T sweep (trans 1; 2 with conj) of a level's small fronts (npiv <= 64), a CTA each: the front's column vector (the
+// pivot columns' right-hand side, then the children's entries that land on each column), y = U11^-T w[:np] (into R),
+// then the contribution u = w[np:] - U12^T y into VB
+template <typename T, bool CJ>
+__global__ void __launch_bounds__(SV_THREADS) k_sv_fwdUt(const SvFront *__restrict__ fr, const int *__restrict__ list,
+                                                         const T *__restrict__ La, const T *__restrict__ Ua,
+                                                         const int64_t *__restrict__ csp, const int64_t *__restrict__ csi,
+                                                         T *__restrict__ R, T *__restrict__ VB, int64_t vstride, int64_t n,
+                                                         int nrhs, DevStatus *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_zero;
+    const SvFront F = fr[list[blockIdx.x]];
+    const int np = (int)F.np, nc = (int)F.nc, ncb = nc - np, ld = np + 1, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5, nw = SV_THREADS / 32;
+    T *w = reinterpret_cast<T *>(smem_raw);          // nc x SV_RC (ld nc)
+    T *sT = w + nc * SV_RC;                          // np x ld: sT[j + i * ld] = U11[i, j] (conj)
+    T *dinv = sT + np * ld;
+    const T *L = La + F.L_off, *U12 = Ua + F.U_off;
+    if (tid == 0) s_zero = 0;
+    stage_transposed<T, CJ>(L, F.nr, np, sT);
+    __syncthreads();
+    for (int i = tid; i < np; i += SV_THREADS) {
+        T d = L[i + (int64_t)i * F.nr];
+        if (CJ) d = conjv(d);
+        if (is_zero(d)) { set_status(st, ST_SOLVE_ZERO, F.f + i, 0, 0); s_zero = 1; }
+        dinv[i] = is_zero(d) ? VT<T>::zero() : recip(d);
+    }
+    pdl_wait();
+    pdl_trigger();
+    __syncthreads();
+    if (s_zero) return;
+    for (int r0 = 0; r0 < nrhs; r0 += SV_RC) {
+        const int rc = nrhs - r0 < SV_RC ? nrhs - r0 : SV_RC;
+        for (int e = tid; e < nc * rc; e += SV_THREADS) {
+            const int c = e % nc, r = e / nc;
+            const int64_t g = F.col_off + c;
+            T val = c < np ? R[F.f + c + (int64_t)(r0 + r) * n] : VT<T>::zero();
+            for (int64_t q = csp[g]; q < csp[g + 1]; q++) val = add(val, VB[csi[q] + (int64_t)(r0 + r) * vstride]);
+            w[c + r * nc] = val;
+        }
+        __syncthreads();
+        for (int r = warp; r < rc; r += nw) {
+            T *wr = w + r * nc;
+            T a = lane < np ? wr[lane] : VT<T>::zero();
+            T b = lane + 32 < np ? wr[lane + 32] : VT<T>::zero();
+            for (int i = 0; i < np; i++) {
+                const T zi = mul(shfl_v<T>(i < 32 ? a : b, i & 31), dinv[i]);
+                const T *row = sT + i * ld;             // row[j] = u_ij
+                if (lane == i) a = zi;
+                else if (lane > i && lane < np) a = sub(a, mul(row[lane], zi));
+                if (lane + 32 == i) b = zi;
+                else if (lane + 32 > i && lane + 32 < np) b = sub(b, mul(row[lane + 32], zi));
+            }
+            if (lane < np) wr[lane] = a;
+            if (lane + 32 < np) wr[lane + 32] = b;
+        }
+        __syncthreads();
+        for (int e = tid; e < np * rc; e += SV_THREADS) R[F.f + e % np + (int64_t)(r0 + e / np) * n] = w[e % np + (e / np) * nc];
+        for (int t = warp; t < ncb; t += nw) {
+            T u0 = lane < np ? U12[lane + (int64_t)t * np] : VT<T>::zero();
+            T u1 = lane + 32 < np ? U12[lane + 32 + (int64_t)t * np] : VT<T>::zero();
+            if (CJ) { u0 = conjv(u0); u1 = conjv(u1); }
+            for (int r = 0; r < rc; r++) {
+                const T *z = w + r * nc;
+                T s = lane < np ? mul(u0, z[lane]) : VT<T>::zero();
+                if (lane + 32 < np) s = add(s, mul(u1, z[lane + 32]));
+                for (int o = 16; o > 0; o >>= 1) s = add(s, shfl_xor_v<T>(s, o));
+                if (lane == 0) VB[F.col_off + np + t + (int64_t)(r0 + r) * vstride] = sub(z[np + t], s);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// a larger front's column vector (the U^T sweep): the pivot columns' entries into R[f ..], the others into its own
+// entries of VB
+template <typename T>
+__global__ void k_sv_gatherU(int64_t f, int64_t np, int64_t nc, int64_t col_off, const int64_t *__restrict__ csp,
+                             const int64_t *__restrict__ csi, T *__restrict__ R, T *__restrict__ VB, int64_t vstride, int64_t n,
+                             int64_t nrhs)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nc * nrhs; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = e % nc, r = e / nc, g = col_off + c;
+        T val = c < np ? R[f + c + r * n] : VT<T>::zero();
+        for (int64_t q = csp[g]; q < csp[g + 1]; q++) val = add(val, VB[csi[q] + r * vstride]);
+        if (c < np) R[f + c + r * n] = val;
+        else VB[col_off + c + r * vstride] = val;
+    }
+}
+
+// a larger front's contribution (the U^T sweep): u[t] = w[np + t] - sum_k U12[k, t] y[k] (conj), a warp per column
+template <typename T, bool CJ>
+__global__ void k_sv_utcb(const T *__restrict__ U12, int64_t npiv, int64_t ncb, int64_t f, const T *__restrict__ R,
+                          T *__restrict__ VBc, int64_t vstride, int64_t n, int64_t nrhs)
+{
+    const int lane = threadIdx.x & 31;
+    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < ncb; c += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        for (int64_t r = 0; r < nrhs; r++) {
+            const T *z = R + f + r * n;
+            T s = VT<T>::zero();
+            for (int64_t k = lane; k < npiv; k += 32) {
+                T u = U12[k + c * npiv];
+                if (CJ) u = conjv(u);
+                s = k < 32 ? mul(u, z[k]) : add(s, mul(u, z[k]));
+            }
+            for (int o = 16; o > 0; o >>= 1) s = add(s, shfl_xor_v<T>(s, o));
+            if (lane == 0) VBc[c + r * vstride] = sub(VBc[c + r * vstride], s);
+        }
+    }
+}
+
+// L^T sweep (trans 1; 2 with conj) of a level's small fronts (npiv <= 64), a CTA each: x = L11^-T (y - L21^T x[CB rows])
+// (the CB rows' x, in pivot order through pinv, from the fronts above, already solved)
+template <typename T, bool CJ>
+__global__ void __launch_bounds__(SV_THREADS) k_sv_bwdLt(const SvFront *__restrict__ fr, const int *__restrict__ list,
+                                                         const T *__restrict__ La, const int64_t *__restrict__ rowid_all,
+                                                         const int64_t *__restrict__ pinv, const T *__restrict__ Z,
+                                                         T *__restrict__ V, int64_t n, int nrhs)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const SvFront F = fr[list[blockIdx.x]];
+    const int np = (int)F.np, nr = (int)F.nr, ld = np + 1, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5, nw = SV_THREADS / 32;
+    T *sT = reinterpret_cast<T *>(smem_raw);          // np x ld: sT[j + i * ld] = L11[i, j] (conj)
+    T *s = sT + np * ld;                              // np x SV_RC
+    const T *L = La + F.L_off;
+    const int64_t *rowid = rowid_all + F.row_off;
+    stage_transposed<T, CJ>(L, nr, np, sT);
+    pdl_wait();
+    pdl_trigger();
+    __syncthreads();
+    for (int r0 = 0; r0 < nrhs; r0 += SV_RC) {
+        const int rc = nrhs - r0 < SV_RC ? nrhs - r0 : SV_RC;
+        for (int e = warp; e < np * rc; e += nw) {
+            const int i = e % np, r = e / np;
+            T acc = VT<T>::zero();
+            for (int rr = np + lane; rr < nr; rr += 32) {
+                T l = L[rr + (int64_t)i * nr];
+                if (CJ) l = conjv(l);
+                acc = add(acc, mul(l, V[pinv[rowid[rr]] + (int64_t)(r0 + r) * n]));
+            }
+            for (int o = 16; o > 0; o >>= 1) acc = add(acc, shfl_xor_v<T>(acc, o));
+            if (lane == 0) s[e] = sub(Z[F.f + i + (int64_t)(r0 + r) * n], acc);
+        }
+        __syncthreads();
+        for (int r = warp; r < rc; r += nw) {
+            T *sr = s + r * np;
+            T a = lane < np ? sr[lane] : VT<T>::zero();
+            T b = lane + 32 < np ? sr[lane + 32] : VT<T>::zero();
+            for (int i = np - 1; i >= 0; i--) {
+                const T vi = shfl_v<T>(i < 32 ? a : b, i & 31);
+                const T *row = sT + i * ld;             // row[j] = L11[i, j], j < i
+                if (lane < i) a = sub(a, mul(row[lane], vi));
+                if (lane + 32 < i) b = sub(b, mul(row[lane + 32], vi));
+            }
+            if (lane < np) V[F.f + lane + (int64_t)(r0 + r) * n] = a;
+            if (lane + 32 < np) V[F.f + lane + 32 + (int64_t)(r0 + r) * n] = b;
+        }
+        __syncthreads();
+    }
+}
+
+// The larger fronts of a level in the trans-0 sweeps, all in each launch (blockIdx.y: the front in the level's list).
+// L sweep, 1: the fronts' vectors in their final row order into VB
+template <typename T>
+__global__ void k_svb_gatherL(const SvFront *__restrict__ fr, const int *__restrict__ list, const int64_t *__restrict__ rowinit,
+                              const int *__restrict__ permall, const int64_t *__restrict__ rsp, const int64_t *__restrict__ rsi,
+                              const T *__restrict__ R, T *__restrict__ VB, int64_t vstride, int64_t n, int64_t nrhs)
+{
+    const SvFront F = fr[list[blockIdx.y]];
+    const int *perm = permall + F.row_off;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < F.nr * nrhs; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = e % F.nr, r = e / F.nr, i = F.np > 0 ? perm[k] : k, g = F.row_off + i, ri = rowinit[g];
+        T val = (i < F.nri && ri >= 0) ? R[ri + r * n] : VT<T>::zero();
+        for (int64_t q = rsp[g]; q < rsp[g + 1]; q++) val = add(val, VB[rsi[q] + r * vstride]);
+        VB[F.row_off + k + r * vstride] = val;
+    }
+}
+
+// L sweep, 2: x = L11^-1 v[:np], a CTA per front, rcb right-hand sides per pass; x into VB (in place) and into Y in
+// pivot order
+template <typename T>
+__global__ void __launch_bounds__(256) k_svb_L11(const SvFront *__restrict__ fr, const int *__restrict__ list,
+                                                 const T *__restrict__ La, T *__restrict__ VB, int64_t vstride,
+                                                 T *__restrict__ Y, int64_t n, int nrhs, int rcb)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const SvFront F = fr[list[blockIdx.x]];
+    const int np = (int)(F.np < F.nr ? F.np : F.nr), tid = threadIdx.x;
+    if (np == 0) return;
+    T *x = reinterpret_cast<T *>(smem_raw);          // np x rcb
+    T *sT = x + (int64_t)np * rcb;                   // 64 x 64
+    for (int r0 = 0; r0 < nrhs; r0 += rcb) {
+        const int rc = nrhs - r0 < rcb ? nrhs - r0 : rcb;
+        for (int e = tid; e < np * rc; e += blockDim.x) x[e] = VB[F.row_off + e % np + (int64_t)(r0 + e / np) * vstride];
+        __syncthreads();
+        blk_trisolve<T, false>(La + F.L_off, F.nr, np, x, rc, sT, nullptr, nullptr, 0);
+        for (int e = tid; e < np * rc; e += blockDim.x) {
+            const int k = e % np;
+            const int64_t r = r0 + e / np;
+            VB[F.row_off + k + r * vstride] = x[e];
+            Y[F.f + k + r * n] = x[e];
+        }
+        __syncthreads();
+    }
+}
+
+// L sweep, 3: u = v[np:] - L21 x on 256 rows per CTA (x from VB), rc2 right-hand sides per pass over L
+template <typename T>
+__global__ void __launch_bounds__(256) k_svb_L21(const SvFront *__restrict__ fr, const int *__restrict__ list,
+                                                 const T *__restrict__ La, T *__restrict__ VB, int64_t vstride, int nrhs, int rc2)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const SvFront F = fr[list[blockIdx.y]];
+    const int np = (int)(F.np < F.nr ? F.np : F.nr), tid = threadIdx.x;
+    const int64_t rows = F.nr - np, row0 = (int64_t)blockIdx.x * 256;
+    if (np == 0 || row0 >= rows) return;
+    T *xs = reinterpret_cast<T *>(smem_raw);         // np x rc2
+    const T *L = La + F.L_off;
+    const int64_t rr = np + row0 + tid;
+    for (int r0 = 0; r0 < nrhs; r0 += rc2) {
+        const int rc = nrhs - r0 < rc2 ? nrhs - r0 : rc2;
+        for (int e = tid; e < np * rc; e += blockDim.x) xs[e] = VB[F.row_off + e % np + (int64_t)(r0 + e / np) * vstride];
+        __syncthreads();
+        if (rr < F.nr) {
+            T acc[SV_RC];
+#pragma unroll
+            for (int r = 0; r < SV_RC; r++) acc[r] = VT<T>::zero();
+            for (int k0 = 0; k0 < np; k0 += 8) {
+                T lv[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++) lv[q] = k0 + q < np ? L[rr + (int64_t)(k0 + q) * F.nr] : VT<T>::zero();
+#pragma unroll
+                for (int q = 0; q < 8; q++)
+                    if (k0 + q < np)
+#pragma unroll
+                        for (int r = 0; r < SV_RC; r++)
+                            if (r < rc) acc[r] = add(acc[r], mul(lv[q], xs[k0 + q + r * np]));
+            }
+#pragma unroll
+            for (int r = 0; r < SV_RC; r++)
+                if (r < rc) {
+                    T *o = VB + F.row_off + rr + (int64_t)(r0 + r) * vstride;
+                    *o = sub(*o, acc[r]);
+                }
+        }
+        __syncthreads();
+    }
+}
+
+// U sweep, 1: the partial products U12 x[CB columns] of chunk blockIdx.x of a front's CB columns (F.nch chunks), a
+// thread per row of U12, into part (the front's partial sums start at F.poff * nrhs)
+template <typename T>
+__global__ void __launch_bounds__(256) k_svb_u12(const SvFront *__restrict__ fr, const int *__restrict__ list,
+                                                 const T *__restrict__ Ua, const int64_t *__restrict__ cols,
+                                                 const T *__restrict__ X, int64_t n, int nrhs, T *__restrict__ part)
+{
+    const SvFront F = fr[list[blockIdx.y]];
+    if (blockIdx.x >= F.nch || F.np == 0) return;
+    const int64_t np = F.np, ncb = F.nc - F.np, chunk = (ncb + F.nch - 1) / F.nch;
+    const int64_t c0 = blockIdx.x * chunk, c1 = c0 + chunk < ncb ? c0 + chunk : ncb;
+    const T *U12 = Ua + F.U_off;
+    const int64_t *cb = cols + F.col_off + np;
+    T *pp = part + F.poff * nrhs + (int64_t)blockIdx.x * np * nrhs;
+    for (int r0 = 0; r0 < nrhs; r0 += SV_RC) {
+        const int rc = nrhs - r0 < SV_RC ? nrhs - r0 : SV_RC;
+        for (int64_t i = threadIdx.x; i < np; i += blockDim.x) {
+            T acc[SV_RC];
+#pragma unroll
+            for (int r = 0; r < SV_RC; r++) acc[r] = VT<T>::zero();
+            for (int64_t k0 = c0; k0 < c1; k0 += 8) {
+                T uv[8];
+                int64_t cc[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const bool ok = k0 + q < c1;
+                    uv[q] = ok ? U12[i + (k0 + q) * np] : VT<T>::zero();
+                    cc[q] = ok ? cb[k0 + q] : 0;
+                }
+#pragma unroll
+                for (int q = 0; q < 8; q++)
+                    if (k0 + q < c1)
+#pragma unroll
+                        for (int r = 0; r < SV_RC; r++)
+                            if (r < rc) acc[r] = add(acc[r], mul(uv[q], X[cc[q] + (int64_t)(r0 + r) * n]));
+            }
+#pragma unroll
+            for (int r = 0; r < SV_RC; r++)
+                if (r < rc) pp[i + (int64_t)(r0 + r) * np] = acc[r];
+        }
+    }
+}
+
+// U sweep, 2: x = U11^-1 (y - the partial products, in chunk order), a CTA per front, rcb right-hand sides per pass
+template <typename T>
+__global__ void __launch_bounds__(256) k_svb_bwdU(const SvFront *__restrict__ fr, const int *__restrict__ list,
+                                                  const T *__restrict__ La, const T *__restrict__ part, const T *__restrict__ Y,
+                                                  T *__restrict__ X, int64_t n, int nrhs, int rcb, DevStatus *st)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_zero;
+    const SvFront F = fr[list[blockIdx.x]];
+    const int np = (int)F.np, tid = threadIdx.x;
+    if (np == 0) return;
+    T *x = reinterpret_cast<T *>(smem_raw);          // np x rcb
+    T *sT = x + (int64_t)np * rcb;                   // 64 x 64
+    T *dinv = sT + 64 * 64;                          // 64
+    const T *pp = part + F.poff * nrhs;
+    for (int r0 = 0; r0 < nrhs; r0 += rcb) {
+        const int rc = nrhs - r0 < rcb ? nrhs - r0 : rcb;
+        for (int e = tid; e < np * rc; e += blockDim.x) {
+            const int i = e % np;
+            const int64_t r = r0 + e / np;
+            T v = Y[F.f + i + r * n];
+            for (int64_t q = 0; q < F.nch; q++) v = sub(v, pp[q * np * nrhs + i + r * np]);
+            x[e] = v;
+        }
+        if (tid == 0) s_zero = 0;
+        __syncthreads();
+        blk_trisolve<T, true>(La + F.L_off, F.nr, np, x, rc, sT, dinv, st, F.f, &s_zero);
+        if (s_zero) return;
+        for (int e = tid; e < np * rc; e += blockDim.x) X[F.f + e % np + (int64_t)(r0 + e / np) * n] = x[e];
+        __syncthreads();
     }
 }
 

@@ -88,7 +88,8 @@ DevPlan::~DevPlan()
 {
     for (void *p : {(void *)cols, (void *)relcol, (void *)rowinit, (void *)asm_src, (void *)asm_dst, (void *)Bp, (void *)Bi,
                     (void *)Bsrc, (void *)row_perm, (void *)col_perm, (void *)seg, (void *)chain_uoff, (void *)chain_loff,
-                    (void *)chain_nrow})
+                    (void *)chain_nrow, (void *)sv, (void *)sv_rows, (void *)sv_cols, (void *)rsp, (void *)rsi, (void *)csp,
+                    (void *)csi, (void *)iota, (void *)sv_brows, (void *)sv_bcols})
         if (p) cudaFree(p);
 }
 
@@ -102,6 +103,129 @@ static int upload_segments(int64_t n, const std::vector<int64_t> &Bp, DevPlan &D
         }
     D.nseg = (int64_t)seg.size() / 3;
     return upload(seg, &D.seg, err, errlen);
+}
+
+// The level-scheduled solve's structures.  A front is small for the row sweeps (L, L^T) when one CTA holds its vector
+// for SV_RC right-hand sides and its pivot block is at most 64 wide and 512 KB (complex), and small for the column sweeps
+// (U, U^T) likewise with its columns and U12; the dense chain's fronts, which the U sweep takes by its own kernels, go
+// with the larger fronts in the column sweeps.
+static const int64_t SV_MAXDIM = 768, SV_MAXNP = 64, SV_MAXBLK = 32768;
+static int upload_solve_levels(const FrontPlan &P, DevPlan &D, char *err, size_t errlen)
+{
+    const int64_t nf = (int64_t)P.fronts.size(), nlev = P.nlevels > 0 ? P.nlevels : 1;
+    std::vector<SvFront> sv((size_t)(nf > 0 ? nf : 1));
+    std::vector<std::vector<int64_t>> lr((size_t)nlev), lc((size_t)nlev);
+    D.big_rows.assign((size_t)nlev, {});
+    D.big_cols.assign((size_t)nlev, {});
+    D.sv_rows_maxnr.assign((size_t)nlev, 0); D.sv_rows_maxnp.assign((size_t)nlev, 0);
+    D.sv_cols_maxnc.assign((size_t)nlev, 0); D.sv_cols_maxnp.assign((size_t)nlev, 0);
+    for (int64_t fi = 0; fi < nf; fi++) {
+        const Front &F = P.fronts[fi];
+        sv[(size_t)fi] = SvFront{F.f, F.npiv, F.nrows, F.nri, F.ncols, F.L_off, F.U_off, F.row_off, F.col_off, 0, 0};
+        const size_t L = (size_t)F.level;
+        const int64_t ncb = F.ncols - F.npiv;
+        const bool base = F.npiv <= SV_MAXNP && F.npiv <= F.nrows;
+        const bool rsmall = base && F.nrows <= SV_MAXDIM && F.nrows * F.npiv <= SV_MAXBLK;
+        const bool csmall = base && F.ncols <= SV_MAXDIM && F.npiv * ncb <= SV_MAXBLK && !(D.chain_begin >= 0 && fi >= D.chain_begin);
+        if (rsmall) {
+            lr[L].push_back(fi);
+            D.sv_rows_maxnr[L] = std::max(D.sv_rows_maxnr[L], F.nrows);
+            D.sv_rows_maxnp[L] = std::max(D.sv_rows_maxnp[L], F.npiv);
+        } else D.big_rows[L].push_back(fi);
+        if (csmall) {
+            lc[L].push_back(fi);
+            D.sv_cols_maxnc[L] = std::max(D.sv_cols_maxnc[L], F.ncols);
+            D.sv_cols_maxnp[L] = std::max(D.sv_cols_maxnp[L], F.npiv);
+        } else D.big_cols[L].push_back(fi);
+    }
+    // the larger fronts of the trans-0 sweeps: device lists by level; the U sweep's CB-column chunks (at most 296, at least
+    // 32 columns each) and each front's first partial sum within its level
+    std::vector<int> brows_list, bcols_list;
+    D.sv_brows_ptr.assign(1, 0); D.sv_bcols_ptr.assign(1, 0);
+    D.brows_maxnr.assign((size_t)nlev, 0); D.brows_maxnp.assign((size_t)nlev, 0); D.brows_maxm.assign((size_t)nlev, 0);
+    D.bcols_maxnp.assign((size_t)nlev, 0); D.bcols_maxnch.assign((size_t)nlev, 0);
+    D.part_need = 1;
+    for (int64_t L = 0; L < nlev; L++) {
+        for (int64_t fi : D.big_rows[(size_t)L]) {
+            const Front &F = P.fronts[(size_t)fi];
+            if (F.nrows == 0) continue;
+            const int64_t np = std::min(F.npiv, F.nrows);
+            brows_list.push_back((int)fi);
+            D.brows_maxnr[(size_t)L] = std::max(D.brows_maxnr[(size_t)L], F.nrows);
+            D.brows_maxnp[(size_t)L] = std::max(D.brows_maxnp[(size_t)L], np);
+            D.brows_maxm[(size_t)L] = std::max(D.brows_maxm[(size_t)L], F.nrows - np);
+        }
+        int64_t poff = 0;
+        for (int64_t fi : D.big_cols[(size_t)L]) {
+            const Front &F = P.fronts[(size_t)fi];
+            if (F.npiv == 0 || (D.chain_begin >= 0 && fi >= D.chain_begin)) continue;
+            const int64_t ncb = F.ncols - F.npiv;
+            const int64_t chunk = ncb > 0 ? std::max<int64_t>(32, (ncb + 295) / 296) : 1;
+            const int64_t nch = ncb > 0 ? (ncb + chunk - 1) / chunk : 0;
+            sv[(size_t)fi].nch = nch;
+            sv[(size_t)fi].poff = poff;
+            poff += nch * F.npiv;
+            bcols_list.push_back((int)fi);
+            D.bcols_maxnp[(size_t)L] = std::max(D.bcols_maxnp[(size_t)L], F.npiv);
+            D.bcols_maxnch[(size_t)L] = std::max(D.bcols_maxnch[(size_t)L], nch);
+        }
+        D.part_need = std::max(D.part_need, poff);
+        D.sv_brows_ptr.push_back((int64_t)brows_list.size());
+        D.sv_bcols_ptr.push_back((int64_t)bcols_list.size());
+    }
+    if (brows_list.empty()) brows_list.push_back(0);
+    if (bcols_list.empty()) bcols_list.push_back(0);
+    std::vector<int> rows_list, cols_list;
+    D.sv_rows_ptr.assign(1, 0); D.sv_cols_ptr.assign(1, 0);
+    for (int64_t L = 0; L < nlev; L++) {
+        for (int64_t fi : lr[(size_t)L]) rows_list.push_back((int)fi);
+        for (int64_t fi : lc[(size_t)L]) cols_list.push_back((int)fi);
+        D.sv_rows_ptr.push_back((int64_t)rows_list.size());
+        D.sv_cols_ptr.push_back((int64_t)cols_list.size());
+    }
+    if (rows_list.empty()) rows_list.push_back(0);
+    if (cols_list.empty()) cols_list.push_back(0);
+    // the children's contribution entries on each plan row and column, in the children's order
+    D.vrow = P.rows_total;
+    D.vcol = (int64_t)P.cols.size();
+    std::vector<int64_t> rsp((size_t)D.vrow + 1, 0), csp((size_t)D.vcol + 1, 0);
+    auto each_entry = [&](auto fn) {
+        for (int64_t fi = 0; fi < nf; fi++) {
+            const Front &F = P.fronts[fi];
+            for (int64_t k = F.child_begin; k < F.child_end; k++) {
+                const Front &G = P.fronts[(size_t)P.children[(size_t)k]];
+                const int64_t cbr = std::max<int64_t>(0, G.nrows - G.npiv), nslot = std::max<int64_t>(0, G.nri - G.npiv);
+                for (int64_t t = 0; t < cbr; t++) {
+                    const int64_t i = t < nslot ? G.slot + t : F.tau_base + (t - nslot);
+                    fn(0, F.row_off + i, G.row_off + G.npiv + t);
+                }
+                for (int64_t t = 0; t < G.ncols - G.npiv; t++) fn(1, F.col_off + P.relcol[(size_t)(G.relcol_off + t)], G.col_off + G.npiv + t);
+            }
+        }
+    };
+    each_entry([&](int kind, int64_t at, int64_t) { (kind ? csp : rsp)[(size_t)at + 1]++; });
+    for (size_t i = 1; i < rsp.size(); i++) rsp[i] += rsp[i - 1];
+    for (size_t i = 1; i < csp.size(); i++) csp[i] += csp[i - 1];
+    std::vector<int64_t> rsi((size_t)std::max<int64_t>(1, rsp.back())), csi((size_t)std::max<int64_t>(1, csp.back()));
+    std::vector<int64_t> rfill(rsp.begin(), rsp.end() - 1), cfill(csp.begin(), csp.end() - 1);
+    each_entry([&](int kind, int64_t at, int64_t src) {
+        if (kind) csi[(size_t)cfill[(size_t)at]++] = src;
+        else rsi[(size_t)rfill[(size_t)at]++] = src;
+    });
+    std::vector<int64_t> iota((size_t)std::max<int64_t>(1, P.max_nrows));
+    for (size_t i = 0; i < iota.size(); i++) iota[i] = (int64_t)i;
+    int rc;
+    if ((rc = upload(sv, &D.sv, err, errlen))) return rc;
+    if ((rc = upload(rows_list, &D.sv_rows, err, errlen))) return rc;
+    if ((rc = upload(brows_list, &D.sv_brows, err, errlen))) return rc;
+    if ((rc = upload(bcols_list, &D.sv_bcols, err, errlen))) return rc;
+    if ((rc = upload(cols_list, &D.sv_cols, err, errlen))) return rc;
+    if ((rc = upload(rsp, &D.rsp, err, errlen))) return rc;
+    if ((rc = upload(rsi, &D.rsi, err, errlen))) return rc;
+    if ((rc = upload(csp, &D.csp, err, errlen))) return rc;
+    if ((rc = upload(csi, &D.csi, err, errlen))) return rc;
+    if ((rc = upload(iota, &D.iota, err, errlen))) return rc;
+    return FPLUS_OK;
 }
 
 int dev_upload_plan(const fplus_symbolic *S, const FrontPlan &P, DevPlan &D, char *err, size_t errlen)
@@ -142,6 +266,7 @@ int dev_upload_plan(const fplus_symbolic *S, const FrontPlan &P, DevPlan &D, cha
             if ((rc = upload(nrow, &D.chain_nrow, err, errlen))) return rc;
         }
     }
+    if ((rc = upload_solve_levels(P, D, err, errlen))) return rc;
     return FPLUS_OK;
 }
 
@@ -152,7 +277,7 @@ DevNum::~DevNum()
                     (void *)cbstack, (void *)work, (void *)rowid, (void *)p_lu, (void *)pinv, (void *)ipiv, (void *)perm,
                     (void *)st, (void *)scratch, (void *)rbuf, (void *)sbuf, (void *)xbuf, (void *)part, (void *)work2,
                     (void *)perm2, (void *)rr_p, (void *)rr_l, (void *)rr_s, (void *)ir_b, (void *)ir_x, (void *)ir_r,
-                    (void *)ir_d, (void *)ir_bits, scratch_norm, tcws, gm_buf, coopbuf})
+                    (void *)ir_d, (void *)ir_bits, scratch_norm, tcws, gm_buf, coopbuf, (void *)permall, vbuf})
         if (p) cudaFreeAsync(p, stream);
     if (stream) cudaStreamSynchronize(stream);
     if (crit) cudaStreamSynchronize(crit);
@@ -373,7 +498,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     if ((rc = ensure_async(N, (void **)&N.work, &N.cap_work, (size_t)P.work_size * vs, err, errlen))) return rc;
     if ((rc = ensure_async(N, (void **)&N.rowid, &N.cap_rowid, (size_t)P.rows_total * 8, err, errlen))) return rc;
     if ((rc = ensure_async(N, (void **)&N.ipiv, &N.cap_ipiv, (size_t)(N.n > 0 ? N.n : 1) * 4, err, errlen))) return rc;
-    if ((rc = ensure_async(N, (void **)&N.perm, &N.cap_perm, (size_t)(P.max_nrows > 0 ? P.max_nrows : 1) * 4, err, errlen))) return rc;
+    if ((rc = ensure_async(N, (void **)&N.permall, &N.cap_permall, (size_t)(P.rows_total > 0 ? P.rows_total : 1) * 4, err, errlen))) return rc;
     static thread_local int attr_set = 0;
     if (!attr_set) {
         CK(cudaFuncSetAttribute(k_front_lu2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
@@ -466,7 +591,6 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     if (any_pipe) {
         const size_t wbytes = (size_t)P.work_size * vs;
         if ((rc = ensure_async(N, (void **)&N.work2, &N.cap_work2, wbytes, err, errlen))) return rc;
-        if ((rc = ensure_async(N, (void **)&N.perm2, &N.cap_perm2, (size_t)(P.max_nrows > 0 ? P.max_nrows : 1) * 4, err, errlen))) return rc;
         if (!N.crit) {
             int lo = 0, hi = 0;
             CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
@@ -640,7 +764,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             // other columns, then (after the LU) the rest of the tail
             if (!in_pipe) { CK(cudaEventRecord(N.ev_head, s)); CK(cudaStreamWaitEvent(A, N.ev_head, 0)); in_pipe = true; }
             T *W = (T *)(wsel ? N.work2 : N.work);
-            int *perm = wsel ? N.perm2 : N.perm;
+            int *perm = N.permall + F.row_off;
             wsel ^= 1;
             PivotAsm pa{};
             if (F.child_end - F.child_begin <= 1) {
@@ -681,11 +805,11 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         if ((rc = assemble(fi, W, s, 0))) return rc;
         if (np == 0) continue;
         if (nr == 0) { k_set_singular<<<1, 1, 0, s>>>(N.st, F.f), note_launch(); continue; }     // no row can take pivot step f
-        if ((rc = factor_block(fi, W, N.perm, s, PivotAsm{}))) return rc;
+        if ((rc = factor_block(fi, W, N.permall + F.row_off, s, PivotAsm{}))) return rc;
         if (ncb == 0) continue;
         T *Uf = Ua + F.U_off;
         if (std::min(np, nr) == np && np <= FT_NP && nr <= FT_NR) {
-            if ((rc = tail(fi, W, N.perm, s, 0, ncb, 148, false))) return rc;
+            if ((rc = tail(fi, W, N.permall + F.row_off, s, 0, ncb, 148, false))) return rc;
             if ((fi & 255) == 255) CK(cudaGetLastError());
             continue;
         }
@@ -696,9 +820,9 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             // gather + blocked TRSM of 32-column tiles in shared memory; persistent CTAs (L11 staged once per CTA)
             const size_t tsm = (size_t)(U12_NP * U12_NP + U12_NP * U12_TN) * vs;
             const int blocks = (int)std::min<int64_t>((ncb + U12_TN - 1) / U12_TN, 2 * 148);
-            k_u12_blk<T><<<blocks, 256, tsm, s>>>(W, ld, N.perm, (int)np, ncb, Lf, ld, Uf, N.st), note_launch();
+            k_u12_blk<T><<<blocks, 256, tsm, s>>>(W, ld, N.permall + F.row_off, (int)np, ncb, Lf, ld, Uf, N.st), note_launch();
         } else {
-        k_u12_gather<T><<<nblk(np * ncb), 256, 0, s>>>(W, ld, np, ncb, N.perm, Uf, N.st), note_launch();
+        k_u12_gather<T><<<nblk(np * ncb), 256, 0, s>>>(W, ld, np, ncb, N.permall + F.row_off, Uf, N.st), note_launch();
         for (int64_t k0 = 0; k0 < npr; k0 += TB) {
             const int w = (int)std::min<int64_t>(TB, npr - k0);
             const size_t tsm = (size_t)w * w * vs;
@@ -727,13 +851,13 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
                 const size_t wsb = schur_tc_workspace(N.prec, M, ncb, np, VT<T>::cplx_);
                 if ((rc = ensure_async(N, &N.tcws, &N.cap_tcws, wsb, err, errlen))) return rc;
                 trc = schur_tc(N.prec, VT<T>::cplx_, M, ncb, np, (const double *)(Lf + np), ld, (const double *)Uf, np,
-                               (const double *)(W + np * ld), ld, N.perm + np, (double *)(CB + F.cb_off), M, N.tcws, N.cap_tcws,
+                               (const double *)(W + np * ld), ld, N.permall + F.row_off + np, (double *)(CB + F.cb_off), M, N.tcws, N.cap_tcws,
                                &N.st->tc_err, s);
                 if (trc == 0) { note_launch(); add_launches(2); N.tc_updates++; N.tc_flops += fm * (double)M * (double)ncb * (double)np; }
             }
             if (trc != 0) {
                 dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((ncb + GBN - 1) / GBN));
-                k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, np, Lf + np, ld, Uf, np, W + np * ld, ld, N.perm + np, CB + F.cb_off, M, N.st), note_launch();
+                k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, np, Lf + np, ld, Uf, np, W + np * ld, ld, N.permall + F.row_off + np, CB + F.cb_off, M, N.st), note_launch();
             }
             prof.end(s);
         }
@@ -799,8 +923,8 @@ int dev_factor_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
 // ---------------------------------------------------------------------------------------------------------------------
 // solves on device buffers: x (n x nrhs, ld = n) in, solution out, through the plan's fronts
 template <typename T>
-static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int64_t nrhs, int trans, int raw, char *err,
-                     size_t errlen)
+static int run_solve_block(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int64_t nrhs, int trans, int raw,
+                           char *err, size_t errlen)
 {
     cudaStream_t s = N.stream;
     const int64_t n = N.n;
@@ -822,10 +946,30 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
         if (ncb > 0) maxpart = std::max(maxpart, ((ncb + chunk_of(ncb) - 1) / chunk_of(ncb)) * F.npiv);
         if (F.nrows > F.npiv) maxpart = std::max(maxpart, ((F.nrows - F.npiv + lt_chunk(F.nrows - F.npiv) - 1) / lt_chunk(F.nrows - F.npiv)) * F.npiv);
     }
+    maxpart = std::max(maxpart, D.part_need);
     if ((rc = ensure_async(N, (void **)&N.part, &N.cap_part, (size_t)maxpart * (size_t)nrhs * sizeof(T), err, errlen))) return rc;
-    T *R = (T *)N.rbuf, *S2 = (T *)N.sbuf, *part = (T *)N.part;
+    // the contribution vectors of the level-scheduled forward sweeps (rows or columns of every front, per right-hand side)
+    const size_t vbytes = (size_t)std::max<int64_t>(1, std::max(D.vrow, D.vcol)) * (size_t)nrhs * sizeof(T);
+    if ((rc = ensure_async(N, &N.vbuf, &N.cap_vb, vbytes, err, errlen))) return rc;
+    T *R = (T *)N.rbuf, *S2 = (T *)N.sbuf, *part = (T *)N.part, *VB = (T *)N.vbuf;
     const T *La = (const T *)N.Larena, *Ua = (const T *)N.Uarena;
     const int64_t nf = (int64_t)P.fronts.size();
+    const int64_t nlev = (int64_t)D.sv_rows_ptr.size() - 1;
+    {
+        static thread_local bool sv_attr = false;
+        if (!sv_attr) {
+            CK(cudaFuncSetAttribute(k_sv_fwdL<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+            CK(cudaFuncSetAttribute(k_sv_bwdU<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+            CK(cudaFuncSetAttribute(k_sv_fwdUt<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+            CK(cudaFuncSetAttribute(k_sv_fwdUt<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+            CK(cudaFuncSetAttribute(k_sv_bwdLt<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+            CK(cudaFuncSetAttribute(k_sv_bwdLt<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+            CK(cudaFuncSetAttribute(k_svb_L11<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+            CK(cudaFuncSetAttribute(k_svb_L21<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+            CK(cudaFuncSetAttribute(k_svb_bwdU<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+            sv_attr = true;
+        }
+    }
     const size_t smem = (size_t)P.max_npiv * (size_t)(nrhs + 1) * sizeof(T);
     const size_t fsmem = std::max((size_t)(256 * 8 + 64 * 4 * 8), (size_t)(P.max_npiv * (nrhs + 1) + 256 + 64 * 64)) * sizeof(T);
     constexpr size_t FWD_SMEM = 200 * 1024;
@@ -852,34 +996,76 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
         // b is in pivot order (R[i] = b[pinv[i]]), without scaling
         if (raw) k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, n, N.pinv, nullptr, n, nrhs), note_launch();
         else k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, n, D.row_perm, N.Drp, n, nrhs), note_launch();
-        for (int64_t fi = 0; fi < nf; fi++) {
-            const Front &F = P.fronts[fi];
-            if (F.npiv == 0 || F.nrows == 0) continue;
-            const size_t fsm = (size_t)F.nrows * nrhs * sizeof(T);
-            const int64_t np = std::min(F.npiv, F.nrows);
-            const size_t whole_sm = fsm + (size_t)F.nrows * np * sizeof(T), l11_sm = fsm + (size_t)np * np * sizeof(T);
-            const int swt = nrhs > 8 ? 512 : 256;        // a warp per right-hand side in the sweeps
-            if (F.npiv <= 64 && whole_sm <= FWD_SMEM) {
-                CK(launch_pdl(k_fwdL3<T>, 1, swt, whole_sm, s, La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 1));
-                note_launch();
-            } else if (F.npiv <= 64 && l11_sm <= FWD_SMEM) {
-                CK(launch_pdl(k_fwdL3<T>, 1, swt, l11_sm, s, La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 0));
+        // the L sweep by levels (leaves first): the level's small fronts in one launch (a CTA each), then its larger
+        // fronts together (their vectors gathered into VB, then the L11 solves and the L21 products there); y into S2 in
+        // pivot order.  The dense chain (the levels above the tree, a front each) sequentially in the row-space vector:
+        // its first front's gathered vector into R, then front after front (the next launch overlapping the previous).
+        const int64_t chain_lv = D.chain_begin >= 0 ? (int64_t)P.fronts[(size_t)D.chain_begin].level : nlev;
+        for (int64_t lv = 0; lv < chain_lv; lv++) {
+            const int64_t a0 = D.sv_rows_ptr[(size_t)lv], a1 = D.sv_rows_ptr[(size_t)lv + 1];
+            if (a1 > a0) {
+                const int64_t mnr = D.sv_rows_maxnr[(size_t)lv], mnp = D.sv_rows_maxnp[(size_t)lv];
+                const size_t sm = (size_t)(mnr * SV_RC + mnp * SV_RC + 64 * mnp) * sizeof(T);
+                CK(launch_pdl(k_sv_fwdL<T>, (int)(a1 - a0), SV_THREADS, sm, s, (const SvFront *)D.sv, (const int *)(D.sv_rows + a0),
+                              La, (const int64_t *)D.rowinit, (const int *)N.permall, (const int64_t *)D.rsp,
+                              (const int64_t *)D.rsi, (const T *)R, S2, VB, D.vrow, n, (int)nrhs));
                 note_launch();
             }
-            else if ((size_t)(np * nrhs + 64 * 64) * sizeof(T) <= FWD_SMEM) {
-                // a large front: the L11 solve by 64-row blocks, then the L21 product over many CTAs (xs in the partial-sum
-                // buffer)
-                const size_t xsm = (size_t)np * nrhs * sizeof(T);
-                k_fwdL11<T><<<1, 256, xsm + 64 * 64 * sizeof(T), s>>>(La + F.L_off, F.nrows, np, N.rowid + F.row_off, R, n, nrhs,
-                                                                       part), note_launch();
-                if (F.nrows > np)
-                    k_fwdL21<T><<<(unsigned)((F.nrows - np + 255) / 256), 256, xsm, s>>>(La + F.L_off, F.nrows, np,
-                                                                                      N.rowid + F.row_off, R, n, nrhs, part), note_launch();
+            // the level's larger fronts together: their vectors, the L11 solves (a CTA each), the L21 products
+            const int64_t b0 = D.sv_brows_ptr[(size_t)lv], b1 = D.sv_brows_ptr[(size_t)lv + 1];
+            if (b1 > b0) {
+                const unsigned nb = (unsigned)(b1 - b0);
+                const int *bl = D.sv_brows + b0;
+                const int64_t mnr = D.brows_maxnr[(size_t)lv], mnp = D.brows_maxnp[(size_t)lv], mm = D.brows_maxm[(size_t)lv];
+                const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((mnr * nrhs + 255) / 256,
+                                                                                     std::max<int64_t>(1, 2368 / (int64_t)nb)));
+                k_svb_gatherL<T><<<dim3(gx, nb), 256, 0, s>>>(D.sv, bl, D.rowinit, N.permall, D.rsp, D.rsi, R, VB, D.vrow, n,
+                                                              nrhs), note_launch();
+                if (mnp > 0) {
+                    const int rcb = (int)std::max<int64_t>(1, std::min<int64_t>(nrhs, (int64_t)((SMEM_MAX - 64 * 64 * sizeof(T)) /
+                                                                                                 ((size_t)mnp * sizeof(T)))));
+                    k_svb_L11<T><<<nb, 256, ((size_t)mnp * rcb + 64 * 64) * sizeof(T), s>>>(D.sv, bl, La, VB, D.vrow, S2, n,
+                                                                                              (int)nrhs, rcb), note_launch();
+                    if (mm > 0) {
+                        const int rc2 = (int)std::max<int64_t>(1, std::min<int64_t>(SV_RC, (int64_t)(SMEM_MAX / ((size_t)mnp * sizeof(T)))));
+                        k_svb_L21<T><<<dim3((unsigned)((mm + 255) / 256), nb), 256, (size_t)mnp * rc2 * sizeof(T), s>>>(
+                            D.sv, bl, La, VB, D.vrow, (int)nrhs, rc2), note_launch();
+                    }
+                }
             }
-            else
-                k_fwdL<T><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs), note_launch();
         }
-        k_gather_rows<T><<<nblk(n * nrhs), 256, 0, s>>>(S2, R, N.p_lu, n, nrhs), note_launch();
+        if (D.chain_begin >= 0) {
+            const Front &C = P.fronts[(size_t)D.chain_begin];
+            k_sv_gatherL<T><<<nblk(C.nrows * nrhs), 256, 0, s>>>(C.row_off, C.nrows, C.nri, D.rowinit,
+                                                                 C.npiv > 0 ? N.permall + C.row_off : nullptr, D.rsp, D.rsi, R, VB,
+                                                                 D.vrow, n, nrhs), note_launch();
+            k_sv_toR<T><<<nblk(C.nrows * nrhs), 256, 0, s>>>(VB + C.row_off, D.vrow, C.nrows, N.rowid + C.row_off, R, n, nrhs),
+                note_launch();
+            for (int64_t fi = D.chain_begin; fi < nf; fi++) {
+                const Front &F = P.fronts[(size_t)fi];
+                if (F.npiv == 0 || F.nrows == 0) continue;
+                const size_t fsm = (size_t)F.nrows * nrhs * sizeof(T);
+                const int64_t np = std::min(F.npiv, F.nrows);
+                const size_t whole_sm = fsm + (size_t)F.nrows * np * sizeof(T), l11_sm = fsm + (size_t)np * np * sizeof(T);
+                const int swt = nrhs > 8 ? 512 : 256;        // a warp per right-hand side in the sweeps
+                if (F.npiv <= 64 && whole_sm <= FWD_SMEM) {
+                    CK(launch_pdl(k_fwdL3<T>, 1, swt, whole_sm, s, La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 1));
+                    note_launch();
+                } else if (F.npiv <= 64 && l11_sm <= FWD_SMEM) {
+                    CK(launch_pdl(k_fwdL3<T>, 1, swt, l11_sm, s, La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs, 0));
+                    note_launch();
+                } else if ((size_t)(np * nrhs + 64 * 64) * sizeof(T) <= FWD_SMEM) {
+                    const size_t xsm = (size_t)np * nrhs * sizeof(T);
+                    k_fwdL11<T><<<1, 256, xsm + 64 * 64 * sizeof(T), s>>>(La + F.L_off, F.nrows, np, N.rowid + F.row_off, R, n, nrhs,
+                                                                           part), note_launch();
+                    if (F.nrows > np)
+                        k_fwdL21<T><<<(unsigned)((F.nrows - np + 255) / 256), 256, xsm, s>>>(La + F.L_off, F.nrows, np,
+                                                                                          N.rowid + F.row_off, R, n, nrhs, part), note_launch();
+                } else
+                    k_fwdL<T><<<1, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, N.rowid + F.row_off, R, n, nrhs), note_launch();
+            }
+            k_gather_range<T><<<nblk((n - C.f) * nrhs), 256, 0, s>>>(S2, R, N.p_lu, C.f, n, nrhs), note_launch();
+        }
         int64_t fi_end = nf;                   // fronts below the chain: the row-oriented kernel
         if (D.chain_begin >= 0) {
             // the dense chain, column-oriented: front k's launch first applies front k + 1's solution to the rows above
@@ -910,26 +1096,30 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
             fi_end = cb;
         }
         CK(cudaFuncSetAttribute(k_bwdU_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
-        for (int64_t fi = fi_end - 1; fi >= 0; fi--) {
-            const Front &F = P.fronts[fi];
-            const int64_t ncb = F.ncols - F.npiv;
-            if (F.npiv == 0) continue;
-            const size_t bsm = (size_t)(F.npiv * nrhs + 64 * 64 + 64) * sizeof(T);
-            if (F.npiv > 64 && F.npiv <= F.nrows && bsm <= FWD_SMEM) {
-                // a large front: the U12 product over many CTAs, then U11 by 64-row blocks
-                int64_t nchunk = 0;
-                if (ncb > 0) {
-                    const int64_t chunk = chunk_of(ncb);
-                    nchunk = (ncb + chunk - 1) / chunk;
-                    k_u12_gemv<T><<<(unsigned)nchunk, 256, (size_t)8 * F.npiv * sizeof(T), s>>>(
-                        Ua + F.U_off, F.npiv, ncb, D.cols + F.col_off + F.npiv, R, n, nrhs, chunk, part), note_launch();
-                }
-                k_bwdU_blk<T><<<1, 256, bsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, part, nchunk, S2, R, n, nrhs, N.st), note_launch();
-                continue;
+        // the U sweep below the chain by levels (roots first): the level's small fronts in one launch (a CTA each), then
+        // its larger fronts together
+        for (int64_t lv = nlev - 1; lv >= 0; lv--) {
+            const int64_t a0 = D.sv_cols_ptr[(size_t)lv], a1 = D.sv_cols_ptr[(size_t)lv + 1];
+            if (a1 > a0) {
+                const int64_t mnp = D.sv_cols_maxnp[(size_t)lv];
+                const size_t sm = (size_t)(mnp * SV_RC + 64 * mnp + 64) * sizeof(T);
+                CK(launch_pdl(k_sv_bwdU<T>, (int)(a1 - a0), SV_THREADS, sm, s, (const SvFront *)D.sv, (const int *)(D.sv_cols + a0),
+                              La, Ua, (const int64_t *)D.cols, (const T *)S2, R, n, (int)nrhs, N.st));
+                note_launch();
             }
-            k_bwdU_fused<T><<<(unsigned)bwd_grid(ncb), 256, fsmem, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, Ua + F.U_off, ncb,
-                                                                     D.cols + F.col_off + F.npiv, ncb > 0 ? bwd_chunk(ncb) : 0,
-                                                                     part, S2, R, n, nrhs, N.st), note_launch();
+            // the level's larger fronts together: the U12 partial products, then the U11 solves (a CTA each)
+            const int64_t b0 = D.sv_bcols_ptr[(size_t)lv], b1 = D.sv_bcols_ptr[(size_t)lv + 1];
+            if (b1 > b0) {
+                const unsigned nb = (unsigned)(b1 - b0);
+                const int *bl = D.sv_bcols + b0;
+                const int64_t mnp = D.bcols_maxnp[(size_t)lv], mch = D.bcols_maxnch[(size_t)lv];
+                if (mch > 0)
+                    k_svb_u12<T><<<dim3((unsigned)mch, nb), 256, 0, s>>>(D.sv, bl, Ua, D.cols, R, n, (int)nrhs, part), note_launch();
+                const int rcb = (int)std::max<int64_t>(1, std::min<int64_t>(nrhs, (int64_t)((SMEM_MAX - (64 * 64 + 64) * sizeof(T)) /
+                                                                                             ((size_t)mnp * sizeof(T)))));
+                k_svb_bwdU<T><<<nb, 256, ((size_t)mnp * rcb + 64 * 64 + 64) * sizeof(T), s>>>(D.sv, bl, La, part, S2, R, n,
+                                                                                               (int)nrhs, rcb, N.st), note_launch();
+            }
         }
         // x[col_perm[k]] = Dcp[k] * R[k]  (raw: x[k] = R[k])
         k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, R, raw ? nullptr : D.col_perm, nullptr, raw ? nullptr : N.Dcp, n, nrhs),
@@ -939,50 +1129,98 @@ static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int
         k_rhs_in<T><<<nblk(n * nrhs), 256, 0, s>>>(R, xb, n, raw ? nullptr : D.col_perm, raw ? nullptr : N.Dcp, n, nrhs),
             note_launch();
         const bool cj = trans == 2;
-        for (int64_t fi = 0; fi < nf; fi++) {
-            const Front &F = P.fronts[fi];
-            const int64_t ncb = F.ncols - F.npiv;
-            if (F.npiv == 0) continue;
-            const bool small = F.npiv <= 64 && F.npiv <= F.nrows;
-            const size_t tsm = (size_t)(F.npiv * (F.npiv + 1) + F.npiv) * sizeof(T);
-            if (small && cj) k_fwdUt3<T, true><<<1, 256, tsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
-            else if (small) k_fwdUt3<T, false><<<1, 256, tsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
-            else if (cj) k_fwdUt2<T, true><<<1, 256, (size_t)F.npiv * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
-            else k_fwdUt2<T, false><<<1, 256, (size_t)F.npiv * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
-            if (ncb > 0) {
-                const int64_t* cbc = D.cols + F.col_off + F.npiv;
-                if (F.npiv <= 64 && cj) k_ut_scatter2<T, true><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, cbc, F.f, R, n, nrhs), note_launch();
-                else if (F.npiv <= 64) k_ut_scatter2<T, false><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, cbc, F.f, R, n, nrhs), note_launch();
-                else if (cj) k_ut_scatter<T, true><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, cbc, F.f, R, n, nrhs), note_launch();
-                else k_ut_scatter<T, false><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, cbc, F.f, R, n, nrhs), note_launch();
+        // the U^T sweep by levels (leaves first): the level's small fronts in one launch, the others front by front (their
+        // column vector gathered: the pivot columns into R, the others into VB; the U11^T solve in R; the contribution)
+        for (int64_t lv = 0; lv < nlev; lv++) {
+            const int64_t a0 = D.sv_cols_ptr[(size_t)lv], a1 = D.sv_cols_ptr[(size_t)lv + 1];
+            if (a1 > a0) {
+                const int64_t mnc = D.sv_cols_maxnc[(size_t)lv], mnp = D.sv_cols_maxnp[(size_t)lv];
+                const size_t sm = (size_t)(mnc * SV_RC + mnp * (mnp + 1) + mnp) * sizeof(T);
+                if (cj)
+                    CK(launch_pdl(k_sv_fwdUt<T, true>, (int)(a1 - a0), SV_THREADS, sm, s, (const SvFront *)D.sv,
+                                  (const int *)(D.sv_cols + a0), La, Ua, (const int64_t *)D.csp, (const int64_t *)D.csi, R, VB,
+                                  D.vcol, n, (int)nrhs, N.st));
+                else
+                    CK(launch_pdl(k_sv_fwdUt<T, false>, (int)(a1 - a0), SV_THREADS, sm, s, (const SvFront *)D.sv,
+                                  (const int *)(D.sv_cols + a0), La, Ua, (const int64_t *)D.csp, (const int64_t *)D.csi, R, VB,
+                                  D.vcol, n, (int)nrhs, N.st));
+                note_launch();
+            }
+            for (int64_t fi : D.big_cols[(size_t)lv]) {
+                const Front &F = P.fronts[(size_t)fi];
+                const int64_t ncb = F.ncols - F.npiv;
+                k_sv_gatherU<T><<<nblk(F.ncols * nrhs), 256, 0, s>>>(F.f, F.npiv, F.ncols, F.col_off, D.csp, D.csi, R, VB, D.vcol,
+                                                                     n, nrhs), note_launch();
+                if (F.npiv == 0) continue;
+                const bool small = F.npiv <= 64 && F.npiv <= F.nrows;
+                const size_t tsm = (size_t)(F.npiv * (F.npiv + 1) + F.npiv) * sizeof(T);
+                if (small && cj) k_fwdUt3<T, true><<<1, 256, tsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
+                else if (small) k_fwdUt3<T, false><<<1, 256, tsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
+                else if (cj) k_fwdUt2<T, true><<<1, 256, (size_t)F.npiv * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
+                else k_fwdUt2<T, false><<<1, 256, (size_t)F.npiv * sizeof(T), s>>>(La + F.L_off, F.nrows, F.npiv, F.f, R, n, nrhs, N.st), note_launch();
+                if (ncb > 0) {
+                    T *Vc = VB + F.col_off + F.npiv;
+                    if (cj) k_sv_utcb<T, true><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, F.f, R, Vc, D.vcol, n, nrhs), note_launch();
+                    else k_sv_utcb<T, false><<<nblk(32 * ncb), 256, 0, s>>>(Ua + F.U_off, F.npiv, ncb, F.f, R, Vc, D.vcol, n, nrhs), note_launch();
+                }
             }
         }
-        for (int64_t fi = nf - 1; fi >= 0; fi--) {
-            const Front &F = P.fronts[fi];
-            if (F.npiv == 0) continue;
-            const size_t sm = (size_t)F.npiv * nrhs * sizeof(T);
-            const bool small = F.npiv <= 64 && F.npiv <= F.nrows;
-            const size_t tsm = sm + (size_t)F.npiv * (F.npiv + 1) * sizeof(T);
-            const int64_t *rid = N.rowid + F.row_off;
-            const int64_t rows21 = F.nrows - F.npiv;
-            if (small && cj) k_bwdLt3<T, true><<<1, 256, tsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
-            else if (small) k_bwdLt3<T, false><<<1, 256, tsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
-            else if (rows21 > 1024) {
-                // a large front: the L21^T product over many CTAs, then the sum and the L11^T solve on one
-                const int64_t ch = lt_chunk(rows21), nch = (rows21 + ch - 1) / ch;
-                if (cj) k_ltdot<T, true><<<(unsigned)nch, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, rid, N.pinv, S2, n, nrhs, ch, part), note_launch();
-                else k_ltdot<T, false><<<(unsigned)nch, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, rid, N.pinv, S2, n, nrhs, ch, part), note_launch();
-                if (cj) k_bwdLt<T, true><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs, part, (int)nch), note_launch();
-                else k_bwdLt<T, false><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs, part, (int)nch), note_launch();
+        // the L^T sweep by levels (roots first): the level's small fronts in one launch, the others front by front
+        for (int64_t lv = nlev - 1; lv >= 0; lv--) {
+            const int64_t a0 = D.sv_rows_ptr[(size_t)lv], a1 = D.sv_rows_ptr[(size_t)lv + 1];
+            if (a1 > a0) {
+                const int64_t mnp = D.sv_rows_maxnp[(size_t)lv];
+                const size_t sm = (size_t)(mnp * (mnp + 1) + mnp * SV_RC) * sizeof(T);
+                if (cj)
+                    CK(launch_pdl(k_sv_bwdLt<T, true>, (int)(a1 - a0), SV_THREADS, sm, s, (const SvFront *)D.sv,
+                                  (const int *)(D.sv_rows + a0), La, (const int64_t *)N.rowid, (const int64_t *)N.pinv, (const T *)R,
+                                  S2, n, (int)nrhs));
+                else
+                    CK(launch_pdl(k_sv_bwdLt<T, false>, (int)(a1 - a0), SV_THREADS, sm, s, (const SvFront *)D.sv,
+                                  (const int *)(D.sv_rows + a0), La, (const int64_t *)N.rowid, (const int64_t *)N.pinv, (const T *)R,
+                                  S2, n, (int)nrhs));
+                note_launch();
             }
-            else if (cj) k_bwdLt<T, true><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
-            else k_bwdLt<T, false><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
+            for (int64_t fi : D.big_rows[(size_t)lv]) {
+                const Front &F = P.fronts[(size_t)fi];
+                if (F.npiv == 0) continue;
+                const size_t sm = (size_t)F.npiv * nrhs * sizeof(T);
+                const bool small = F.npiv <= 64 && F.npiv <= F.nrows;
+                const size_t tsm = sm + (size_t)F.npiv * (F.npiv + 1) * sizeof(T);
+                const int64_t *rid = N.rowid + F.row_off;
+                const int64_t rows21 = F.nrows - F.npiv;
+                if (small && cj) k_bwdLt3<T, true><<<1, 256, tsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
+                else if (small) k_bwdLt3<T, false><<<1, 256, tsm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
+                else if (rows21 > 1024) {
+                    // a large front: the L21^T product over many CTAs, then the sum and the L11^T solve on one
+                    const int64_t ch = lt_chunk(rows21), nch = (rows21 + ch - 1) / ch;
+                    if (cj) k_ltdot<T, true><<<(unsigned)nch, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, rid, N.pinv, S2, n, nrhs, ch, part), note_launch();
+                    else k_ltdot<T, false><<<(unsigned)nch, 256, 0, s>>>(La + F.L_off, F.nrows, F.npiv, rid, N.pinv, S2, n, nrhs, ch, part), note_launch();
+                    if (cj) k_bwdLt<T, true><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs, part, (int)nch), note_launch();
+                    else k_bwdLt<T, false><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs, part, (int)nch), note_launch();
+                }
+                else if (cj) k_bwdLt<T, true><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
+                else k_bwdLt<T, false><<<1, 256, sm, s>>>(La + F.L_off, F.nrows, F.npiv, F.f, rid, N.pinv, R, S2, n, nrhs), note_launch();
+            }
         }
         // x[row_perm[p_lu[k]]] = Drp[p_lu[k]] * S2[k]  (raw: x[k] = S2[k], pivot order)
         if (raw) k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, S2, nullptr, nullptr, nullptr, n, nrhs), note_launch();
         else k_rhs_out<T><<<nblk(n * nrhs), 256, 0, s>>>(xb, n, S2, D.row_perm, N.p_lu, N.Drp, n, nrhs), note_launch();
     }
     CK(cudaGetLastError());
+    return FPLUS_OK;
+}
+
+// at most SOLVE_BLOCK right-hand sides per pass (the sweeps' buffers grow with the count)
+static constexpr int64_t SOLVE_BLOCK = 32;
+template <typename T>
+static int run_solve(const FrontPlan &P, const DevPlan &D, DevNum &N, T *xb, int64_t nrhs, int trans, int raw, char *err,
+                     size_t errlen)
+{
+    for (int64_t r0 = 0; r0 < nrhs; r0 += SOLVE_BLOCK) {
+        const int rc = run_solve_block(P, D, N, xb + r0 * N.n, std::min(SOLVE_BLOCK, nrhs - r0), trans, raw, err, errlen);
+        if (rc) return rc;
+    }
     return FPLUS_OK;
 }
 

@@ -35,6 +35,23 @@ struct DevPlan {
     int64_t chain_begin = -1, chain_nb = 0, chain_f0 = 0;
     int64_t *chain_uoff = nullptr;
     int64_t *chain_loff = nullptr, *chain_nrow = nullptr;     // each chain front's L block (U11 in its top rows), rows
+    // the level-scheduled solve: every front's descriptor; per level (ascending height) the fronts the one-CTA kernels
+    // take, as device lists (sv_rows: the L and L^T sweeps; sv_cols: the U and U^T sweeps) with host ranges and the
+    // level's largest sizes, and the others as host lists; the lists of the children's contribution entries landing on
+    // each plan row (rsp/rsi) and plan column (csp/csi); 0 .. max_nrows - 1
+    SvFront *sv = nullptr;
+    int *sv_rows = nullptr, *sv_cols = nullptr;
+    std::vector<int64_t> sv_rows_ptr, sv_cols_ptr;
+    std::vector<int64_t> sv_rows_maxnr, sv_rows_maxnp, sv_cols_maxnc, sv_cols_maxnp;
+    std::vector<std::vector<int64_t>> big_rows, big_cols;
+    // the trans-0 sweeps' larger fronts as device lists by level (brows: the L sweep; bcols: the U sweep below the dense
+    // chain), with host ranges and the level's largest sizes; the partial sums a level's U sweep needs (per right-hand side)
+    int *sv_brows = nullptr, *sv_bcols = nullptr;
+    std::vector<int64_t> sv_brows_ptr, sv_bcols_ptr;
+    std::vector<int64_t> brows_maxnr, brows_maxnp, brows_maxm, bcols_maxnp, bcols_maxnch;
+    int64_t part_need = 0;
+    int64_t *rsp = nullptr, *rsi = nullptr, *csp = nullptr, *csi = nullptr, *iota = nullptr;
+    int64_t vrow = 0, vcol = 0;              // the plan's total front rows, total front columns
     ~DevPlan();
 };
 
@@ -55,6 +72,10 @@ struct DevNum {
     int64_t *rowid = nullptr, *p_lu = nullptr, *pinv = nullptr;
     int *ipiv = nullptr, *perm = nullptr;
     size_t cap_perm = 0;
+    int *permall = nullptr;        // every front's final row order (position -> initial local row), kept for the solves
+    size_t cap_permall = 0;
+    void *vbuf = nullptr;          // the level-scheduled solve's contribution vectors
+    size_t cap_vb = 0;
     // the look-ahead over chain fronts: a second working block and row order, the critical stream and its events
     void *work2 = nullptr;
     int *perm2 = nullptr;

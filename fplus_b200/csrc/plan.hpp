@@ -60,6 +60,13 @@ struct FrontPlan {
     int nlevels = 0;
 };
 
+// a front as the level-scheduled solve kernels read it (pivot columns [f, f + np), nr rows of which nri above the border,
+// nc columns; its L block, its U12 block, its first entry in the plan's row and column arrays)
+struct SvFront {
+    long long f, np, nr, nri, nc, L_off, U_off, row_off, col_off;
+    long long nch, poff;           // the U sweep of a larger front: CB-column chunks, first partial sum (per right-hand side)
+};
+
 struct fplus_symbolic_view {
     int64_t n, ntr, ntc;
     const int64_t *Bp, *Bi;
