@@ -885,10 +885,10 @@ struct PivotAsm {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
-                                                    int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
-                                                    int64_t *__restrict__ rowid, T *__restrict__ Lout, int *__restrict__ perm,
-                                                    int64_t *__restrict__ p_lu, DevStatus *st, int64_t front, PivotAsm pa)
+__device__ __forceinline__ void front_lu2_body(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
+                                               int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
+                                               int64_t *__restrict__ rowid, T *__restrict__ Lout, int *__restrict__ perm,
+                                               int64_t *__restrict__ p_lu, DevStatus *st, int64_t front, const PivotAsm &pa)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *A = reinterpret_cast<T *>(smem_raw);                        // npiv x nrows, column-major: A[c * nrows + i]
@@ -1182,6 +1182,15 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
         if (k < steps) p_lu[fcol + k] = rid[i];
     }
     for (int e = at; e < ne; e += nact) { const int i = e % nrows; Lout[pos[i] + (int64_t)(e / nrows) * nrows] = A[e]; }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
+                                                    int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
+                                                    int64_t *__restrict__ rowid, T *__restrict__ Lout, int *__restrict__ perm,
+                                                    int64_t *__restrict__ p_lu, DevStatus *st, int64_t front, PivotAsm pa)
+{
+    front_lu2_body<T>(W, ld, nrows, npiv, nri, fcol, colmax, pivot_rel, rowid, Lout, perm, p_lu, st, front, pa);
 }
 
 // Blocked partial-pivot LU of a front's pivot block in shared memory (nrows <= 128, npiv <= 64; one CTA of LU3_THREADS):
@@ -1531,10 +1540,9 @@ __global__ void __launch_bounds__(256) k_u12_blk(const T *__restrict__ W, int64_
 // in shared memory with a leading dimension of 132 doubles (4 mod 16: the mma fragments of a half-warp hit 16 banks).
 constexpr int FT_TN = 32, FT_LD = 132, FT_NP = 64, FT_NR = 128, FT_THREADS = 512;
 template <typename T, int TN>
-__global__ void __launch_bounds__(FT_THREADS) k_front_tail(const T *__restrict__ W, int64_t ld, const int *__restrict__ perm,
-                                                           int npiv, int nrows, int64_t ncb, int64_t cb0, int64_t cb1,
-                                                           const T *__restrict__ Lb, T *__restrict__ U, T *__restrict__ CB,
-                                                           const DevStatus *st)
+__device__ __forceinline__ void front_tail_body(const T *__restrict__ W, int64_t ld, const int *__restrict__ perm, int npiv,
+                                                int nrows, int64_t ncb, int64_t cb0, int64_t cb1, const T *__restrict__ Lb,
+                                                T *__restrict__ U, T *__restrict__ CB, const DevStatus *st, int bid, int nbk)
 {
     constexpr bool CP = VT<T>::cplx_;
     constexpr int PER = FT_NR * TN / FT_THREADS;                   // tile values per thread
@@ -1561,7 +1569,7 @@ __global__ void __launch_bounds__(FT_THREADS) k_front_tail(const T *__restrict__
             pre[q] = (t < ntile && r < nrows && c0 + c < cb1) ? W[sperm[r] + (npiv + c0 + c) * ld] : VT<T>::zero();
         }
     };
-    fetch(t0 + blockIdx.x);                                          // in flight while L is staged
+    fetch(t0 + bid);                                          // in flight while L is staged
     for (int e0 = tid; e0 < npiv * nrows; e0 += 8 * FT_THREADS) {     // 8 loads in flight per thread
         T v[8];
 #pragma unroll
@@ -1576,7 +1584,7 @@ __global__ void __launch_bounds__(FT_THREADS) k_front_tail(const T *__restrict__
     }
     __syncthreads();
     const int half = lane >> 4, hl = lane & 15;
-    for (int64_t t = t0 + blockIdx.x; t < ntile; t += gridDim.x) {
+    for (int64_t t = t0 + bid; t < ntile; t += nbk) {
         const int64_t c0 = t * TN;
         const int tn = (int)(cb1 - c0 < TN ? cb1 - c0 : TN);
 #pragma unroll
@@ -1585,7 +1593,7 @@ __global__ void __launch_bounds__(FT_THREADS) k_front_tail(const T *__restrict__
             if constexpr (CP) { sXr[c * FT_LD + r] = pre[q].x; sXi[c * FT_LD + r] = pre[q].y; } else sXr[c * FT_LD + r] = pre[q];
         }
         __syncthreads();
-        fetch(t + gridDim.x);                                       // in flight during this tile
+        fetch(t + nbk);                                       // in flight during this tile
         for (int kb = 0; kb < npiv; kb += 16) {
             const int w = npiv - kb < 16 ? npiv - kb : 16;
             if (2 * warp < TN) {   // the diagonal block: a half-warp per column, lane hl holds row kb + hl
@@ -1646,6 +1654,15 @@ __global__ void __launch_bounds__(FT_THREADS) k_front_tail(const T *__restrict__
         }
         __syncthreads();
     }
+}
+
+template <typename T, int TN>
+__global__ void __launch_bounds__(FT_THREADS) k_front_tail(const T *__restrict__ W, int64_t ld, const int *__restrict__ perm,
+                                                           int npiv, int nrows, int64_t ncb, int64_t cb0, int64_t cb1,
+                                                           const T *__restrict__ Lb, T *__restrict__ U, T *__restrict__ CB,
+                                                           const DevStatus *st)
+{
+    front_tail_body<T, TN>(W, ld, perm, npiv, nrows, ncb, cb0, cb1, Lb, U, CB, st, (int)blockIdx.x, (int)gridDim.x);
 }
 
 // X <- L^-1 X for a unit lower w x w block (w <= 32 RPL) and every column of X (rows [0, w) of each column, ld ldx):
