@@ -281,7 +281,7 @@ extern "C" int fplus_b200_schur_update(int precision, int is_complex, int64_t M,
 extern "C" int fplus_b200_set_front_shape(fplus_symbolic *sym, int64_t max_width, int64_t nb_chain, int lu_variant)
 {
     if (!sym || max_width < 16 || max_width > 4096 || nb_chain < 8 || nb_chain > 64 ||
-        (lu_variant != 2 && lu_variant != 3 && lu_variant != 6 && lu_variant != 7))
+        ((lu_variant & 3) != 2 && (lu_variant & 3) != 3) || (lu_variant & ~15) != 0)
         return FPLUS_ERR_BADARG;
     std::lock_guard<std::mutex> lk(sym->mu);
     sym->max_width = max_width;

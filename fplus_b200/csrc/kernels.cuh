@@ -3405,4 +3405,74 @@ __global__ void __launch_bounds__(256) k_svb_bwdU(const SvFront *__restrict__ fr
     }
 }
 
+// =====================================================================================================================
+// the batched fronts of the factorization: one launch per level for each of assembly, pivot-block LU and tail
+// =====================================================================================================================
+// Assembly of a level's batched fronts, a CTA each, into their own working blocks (zeroed beforehand): the original
+// entries and the entering rows' ids, then the children's contribution blocks one child after another (the order of the
+// front-by-front assembly) with the children's CB row ids into their slots
+template <typename T>
+__global__ void __launch_bounds__(256) k_bat_assemble(const FcFront *__restrict__ fc, const int *__restrict__ list,
+                                                      const int64_t *__restrict__ children, T *__restrict__ Wbase,
+                                                      const T *__restrict__ Bx, const int64_t *__restrict__ asm_src,
+                                                      const int64_t *__restrict__ asm_dst, const int64_t *__restrict__ rowinit,
+                                                      int64_t *__restrict__ rowid_all, const int64_t *__restrict__ relcol,
+                                                      const T *__restrict__ CBA, const DevStatus *st)
+{
+    if (st->code) return;
+    const FcFront F = fc[list[blockIdx.x]];
+    T *W = Wbase + F.wofs;
+    const int tid = threadIdx.x, nr = (int)F.nr;
+    int64_t *rowid = rowid_all + F.row_off;
+    for (int64_t e = F.asm_begin + tid; e < F.asm_end; e += blockDim.x) W[asm_dst[e]] = Bx[asm_src[e]];
+    for (int i = tid; i < nr; i += blockDim.x) if (rowinit[F.row_off + i] >= 0) rowid[i] = rowinit[F.row_off + i];
+    __syncthreads();
+    for (int64_t k = F.child_begin; k < F.child_end; k++) {
+        const FcFront G = fc[children[k]];
+        const int cbr = (int)(G.nr - G.np), cbc = (int)(G.nc - G.np), nslot = (int)(G.nri - G.np > 0 ? G.nri - G.np : 0);
+        const T *cb = CBA + G.cbofs;
+        const int64_t *rc = relcol + G.relcol_off;
+        for (int e = tid; e < cbr * cbc; e += blockDim.x) {
+            const int c = e / cbr, t = e - c * cbr;
+            const int64_t pr = t < nslot ? G.slot + t : F.tau_base + (t - nslot);
+            T *w = W + pr + rc[c] * nr;
+            *w = add(*w, cb[e]);
+        }
+        for (int t = tid; t < nslot; t += blockDim.x) rowid[G.slot + t] = rowid_all[G.row_off + G.np + t];
+        __syncthreads();
+    }
+}
+
+// the pivot-block LU of a level's batched fronts, a CTA each (the body of k_front_lu2)
+template <typename T>
+__global__ void __launch_bounds__(640) k_bat_lu2(const FcFront *__restrict__ fc, const int *__restrict__ list,
+                                                 const T *__restrict__ Wbase, const double *__restrict__ colmax, double pivot_rel,
+                                                 int64_t *__restrict__ rowid_all, T *__restrict__ La, int *__restrict__ permall,
+                                                 int64_t *__restrict__ p_lu, DevStatus *st)
+{
+    const int fi = list[blockIdx.x];
+    const FcFront F = fc[fi];
+    PivotAsm pa;
+    pa.on = 0;
+    front_lu2_body<T>(Wbase + F.wofs, F.nr, (int)F.nr, (int)F.np, (int)F.nri, F.f, colmax, pivot_rel, rowid_all + F.row_off,
+                      La + F.L_off, permall + F.row_off, p_lu, st, fi, pa);
+}
+
+// U12 and the contribution block of a level's batched fronts (blockIdx.y: the front; blockIdx.x: its CTAs over the
+// 32-column tiles; the body of k_front_tail)
+template <typename T, int TN>
+__global__ void __launch_bounds__(FT_THREADS) k_bat_tail(const FcFront *__restrict__ fc, const int *__restrict__ list,
+                                                         const T *__restrict__ Wbase, const int *__restrict__ permall,
+                                                         const T *__restrict__ La, T *__restrict__ Ua, T *__restrict__ CBA,
+                                                         const DevStatus *st)
+{
+    const FcFront F = fc[list[blockIdx.y]];
+    const int64_t ncb = F.nc - F.np;
+    const int64_t ntile = (ncb + TN - 1) / TN;
+    if (ncb <= 0 || blockIdx.x >= ntile) return;
+    const int nbk = (int)(gridDim.x < ntile ? gridDim.x : ntile);
+    front_tail_body<T, TN>(Wbase + F.wofs, F.nr, permall + F.row_off, (int)F.np, (int)F.nr, ncb, 0, ncb, La + F.L_off,
+                           Ua + F.U_off, CBA + F.cbofs, st, (int)blockIdx.x, nbk);
+}
+
 }  // namespace fpl

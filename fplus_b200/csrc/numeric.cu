@@ -89,7 +89,7 @@ DevPlan::~DevPlan()
     for (void *p : {(void *)cols, (void *)relcol, (void *)rowinit, (void *)asm_src, (void *)asm_dst, (void *)Bp, (void *)Bi,
                     (void *)Bsrc, (void *)row_perm, (void *)col_perm, (void *)seg, (void *)chain_uoff, (void *)chain_loff,
                     (void *)chain_nrow, (void *)sv, (void *)sv_rows, (void *)sv_cols, (void *)rsp, (void *)rsi, (void *)csp,
-                    (void *)csi, (void *)iota, (void *)sv_brows, (void *)sv_bcols})
+                    (void *)csi, (void *)iota, (void *)sv_brows, (void *)sv_bcols, (void *)fc, (void *)children, (void *)bs_list})
         if (p) cudaFree(p);
 }
 
@@ -228,6 +228,68 @@ static int upload_solve_levels(const FrontPlan &P, DevPlan &D, char *err, size_t
     return FPLUS_OK;
 }
 
+// The factorization's batched fronts (DevPlan): an interior front with 1..64 pivots, at most 128 rows and no more pivots
+// than rows, whose children are all batched.
+static const int64_t BS_MAXNR = 128, BS_MAXNP = 64;
+static int upload_batched_fronts(const FrontPlan &P, DevPlan &D, char *err, size_t errlen)
+{
+    const int64_t nf = (int64_t)P.fronts.size(), nlev = P.nlevels > 0 ? P.nlevels : 1;
+    D.is_bs.assign((size_t)nf, 0);
+    D.bs_cbofs.assign((size_t)nf, 0);
+    std::vector<FcFront> fc((size_t)(nf > 0 ? nf : 1));
+    std::vector<std::vector<int64_t>> lists((size_t)nlev);
+    D.bs_maxnr.assign((size_t)nlev, 0); D.bs_maxnp.assign((size_t)nlev, 0); D.bs_maxtiles.assign((size_t)nlev, 0);
+    D.bs_wsz.assign((size_t)nlev, 0);
+    D.bs_lu_flops.assign((size_t)nlev, 0); D.bs_tail_flops.assign((size_t)nlev, 0);
+    D.bs_asm_bytes.assign((size_t)nlev, 0); D.bs_lu_bytes.assign((size_t)nlev, 0); D.bs_tail_bytes.assign((size_t)nlev, 0);
+    int64_t cbo = 0;
+    for (int64_t fi = 0; fi < nf; fi++) {
+        const Front &F = P.fronts[(size_t)fi];
+        bool ok = !F.dense && F.npiv >= 1 && F.npiv <= BS_MAXNP && F.nrows <= BS_MAXNR && F.npiv <= F.nrows;
+        for (int64_t k = F.child_begin; ok && k < F.child_end; k++) ok = D.is_bs[(size_t)P.children[(size_t)k]] != 0;
+        const int64_t ncb = F.ncols - F.npiv, M = F.nrows - F.npiv;
+        FcFront &c = fc[(size_t)fi];
+        c = FcFront{F.f, F.npiv, F.nrows, F.nri, F.ncols, F.L_off, F.U_off, F.row_off, F.relcol_off, F.asm_begin, F.asm_end,
+                    F.child_begin, F.child_end, F.slot, F.tau_base, 0, 0};
+        if (!ok) continue;
+        D.is_bs[(size_t)fi] = 1;
+        const size_t L = (size_t)F.level;
+        lists[L].push_back(fi);
+        c.wofs = D.bs_wsz[L];
+        D.bs_wsz[L] += F.nrows * F.ncols;
+        c.cbofs = cbo;
+        D.bs_cbofs[(size_t)fi] = cbo;
+        cbo += M * ncb;
+        D.bs_maxnr[L] = std::max(D.bs_maxnr[L], F.nrows);
+        D.bs_maxnp[L] = std::max(D.bs_maxnp[L], F.npiv);
+        D.bs_maxtiles[L] = std::max<int64_t>(D.bs_maxtiles[L], (ncb + 31) / 32);
+        double fl = 0;
+        for (int64_t k = 0; k < F.npiv; k++) fl += (double)(F.nrows - k - 1) * (double)(F.npiv - k);
+        D.bs_lu_flops[L] += fl;
+        D.bs_tail_flops[L] += ((double)F.npiv * (double)F.npiv / 2.0 + (double)M * (double)F.npiv) * (double)ncb;
+        D.bs_asm_bytes[L] += (double)(F.nrows * F.ncols + 2 * (F.asm_end - F.asm_begin));
+        D.bs_lu_bytes[L] += 2.0 * (double)(F.nrows * F.npiv);
+        D.bs_tail_bytes[L] += (double)(2 * F.nrows * ncb + F.nrows * F.npiv);
+    }
+    D.bs_cb = cbo;
+    D.bs_ws = 0;
+    std::vector<int> list;
+    D.bs_ptr.assign(1, 0);
+    for (int64_t L = 0; L < nlev; L++) {
+        for (int64_t fi : lists[(size_t)L]) list.push_back((int)fi);
+        D.bs_ptr.push_back((int64_t)list.size());
+        D.bs_ws = std::max(D.bs_ws, D.bs_wsz[(size_t)L]);
+    }
+    if (list.empty()) list.push_back(0);
+    std::vector<int64_t> ch(P.children.begin(), P.children.end());
+    if (ch.empty()) ch.push_back(0);
+    int rc;
+    if ((rc = upload(fc, &D.fc, err, errlen))) return rc;
+    if ((rc = upload(ch, &D.children, err, errlen))) return rc;
+    if ((rc = upload(list, &D.bs_list, err, errlen))) return rc;
+    return FPLUS_OK;
+}
+
 int dev_upload_plan(const fplus_symbolic *S, const FrontPlan &P, DevPlan &D, char *err, size_t errlen)
 {
     CK(cudaGetDevice(&D.device));
@@ -267,6 +329,7 @@ int dev_upload_plan(const fplus_symbolic *S, const FrontPlan &P, DevPlan &D, cha
         }
     }
     if ((rc = upload_solve_levels(P, D, err, errlen))) return rc;
+    if ((rc = upload_batched_fronts(P, D, err, errlen))) return rc;
     return FPLUS_OK;
 }
 
@@ -277,7 +340,7 @@ DevNum::~DevNum()
                     (void *)cbstack, (void *)work, (void *)rowid, (void *)p_lu, (void *)pinv, (void *)ipiv, (void *)perm,
                     (void *)st, (void *)scratch, (void *)rbuf, (void *)sbuf, (void *)xbuf, (void *)part, (void *)work2,
                     (void *)perm2, (void *)rr_p, (void *)rr_l, (void *)rr_s, (void *)ir_b, (void *)ir_x, (void *)ir_r,
-                    (void *)ir_d, (void *)ir_bits, scratch_norm, tcws, gm_buf, coopbuf, (void *)permall, vbuf})
+                    (void *)ir_d, (void *)ir_bits, scratch_norm, tcws, gm_buf, coopbuf, (void *)permall, vbuf, bsw, bscb})
         if (p) cudaFreeAsync(p, stream);
     if (stream) cudaStreamSynchronize(stream);
     if (crit) cudaStreamSynchronize(crit);
@@ -486,7 +549,7 @@ static const double TC_MIN_MADDS = 1 << 24;
 
 template <typename T>
 static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pivot_rel, int64_t *border_front,
-                      char *err, size_t errlen)
+                      char *err, size_t errlen, bool batch = true)
 {
     cudaStream_t s = N.stream;
     const int64_t vs = N.vs;
@@ -508,6 +571,8 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         CK(cudaFuncSetAttribute(k_u12_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_front_tail<T, FT_TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_front_tail<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_bat_lu2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_bat_tail<T, FT_TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         attr_set = 1;
     }
     // (captured: the status was cleared where the captured equilibration began, and must keep what it reported)
@@ -601,6 +666,17 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     }
     cudaStream_t A = N.crit;
 
+    // the batched fronts (variant + 8 or the blocked small-front LU turn them off): their contribution blocks live in
+    // their own arena
+    const bool bs_on = batch && D.bs_ptr.size() > 1 && D.bs_ptr.back() > 0 && !(N.lu_variant & 8) && (N.lu_variant & 3) != 3;
+    T *CBA = nullptr;
+    if (bs_on) {
+        if ((rc = ensure_async(N, &N.bsw, &N.cap_bsw, (size_t)std::max<int64_t>(1, D.bs_ws) * vs, err, errlen))) return rc;
+        if ((rc = ensure_async(N, &N.bscb, &N.cap_bscb, (size_t)std::max<int64_t>(1, D.bs_cb) * vs, err, errlen))) return rc;
+        CBA = (T *)N.bscb;
+    }
+    auto cb_of = [&](int64_t gi) -> T * { return bs_on && D.is_bs[(size_t)gi] ? CBA + D.bs_cbofs[(size_t)gi] : CB + P.fronts[(size_t)gi].cb_off; };
+
     // the assembly of columns [0, npiv) (part 1), the others (part 2), or all (part 0)
     auto assemble = [&](int64_t fi, T *W, cudaStream_t st, int part) {
         const Front &F = P.fronts[fi];
@@ -623,7 +699,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             const int rowids = part != 2;
             if (c1 <= c0 && !rowids) continue;
             k_extend_add<T><<<nblk(std::max(cbr * std::max<int64_t>(c1 - c0, 0), nslot)), 256, 0, st>>>(
-                W, ld, CB + G.cb_off, cbr, c0, std::max(c0, c1), nslot, G.slot, F.tau_base, D.relcol + G.relcol_off,
+                W, ld, cb_of(gi), cbr, c0, std::max(c0, c1), nslot, G.slot, F.tau_base, D.relcol + G.relcol_off,
                 N.rowid + F.row_off, N.rowid + G.row_off + G.npiv, rowids, N.st), note_launch();
         }
         prof.end(st);
@@ -753,11 +829,44 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         return FPLUS_OK;
     };
 
+    // the batched fronts first, level by level: the working blocks zeroed, then one launch each for the assembly, the
+    // pivot-block LU and the tail of every batched front of the level (their children are batched and done)
+    if (bs_on) {
+        T *Wb = (T *)N.bsw;
+        const int64_t nlev = (int64_t)D.bs_ptr.size() - 1;
+        const size_t fsm = (size_t)(VT<T>::cplx_ ? 2 : 1) * (FT_NP + FT_TN) * FT_LD * sizeof(double);
+        for (int64_t lv = 0; lv < nlev; lv++) {
+            const int64_t a0 = D.bs_ptr[(size_t)lv], a1 = D.bs_ptr[(size_t)lv + 1];
+            if (a1 <= a0) continue;
+            const unsigned cnt = (unsigned)(a1 - a0);
+            const int *bl = D.bs_list + a0;
+            prof.begin(s, PROF_ASM, 0.0, D.bs_asm_bytes[(size_t)lv] * (double)vs);
+            CK(cudaMemsetAsync(Wb, 0, (size_t)D.bs_wsz[(size_t)lv] * vs, s));
+            k_bat_assemble<T><<<cnt, 256, 0, s>>>(D.fc, bl, D.children, Wb, Bx, D.asm_src, D.asm_dst, D.rowinit, N.rowid, D.relcol,
+                                                  CBA, N.st), note_launch();
+            prof.end(s);
+            const int R = (int)((D.bs_maxnr[(size_t)lv] + 31) & ~31);
+            int nt = 32 + (R <= 128 ? 4 * R : R);
+            if (nt > 640) nt = 640;
+            prof.begin(s, PROF_LU, fm * D.bs_lu_flops[(size_t)lv], D.bs_lu_bytes[(size_t)lv] * (double)vs);
+            k_bat_lu2<T><<<cnt, nt, front_lu_smem(D.bs_maxnr[(size_t)lv], D.bs_maxnp[(size_t)lv], vs), s>>>(
+                D.fc, bl, Wb, N.colmax, pivot_rel, N.rowid, La, N.permall, N.p_lu, N.st), note_launch();
+            prof.end(s);
+            if (D.bs_maxtiles[(size_t)lv] > 0) {
+                prof.begin(s, PROF_SCHUR, fm * D.bs_tail_flops[(size_t)lv], D.bs_tail_bytes[(size_t)lv] * (double)vs);
+                k_bat_tail<T, FT_TN><<<dim3((unsigned)std::min<int64_t>(D.bs_maxtiles[(size_t)lv], 148), cnt), FT_THREADS, fsm, s>>>(
+                    D.fc, bl, Wb, N.permall, La, Ua, CBA, N.st), note_launch();
+                prof.end(s);
+            }
+        }
+    }
+
     bool in_pipe = false;
     int wsel = 0;
     for (int64_t fi = 0; fi < nf; fi++) {
         const Front &F = P.fronts[fi];
         const int64_t nr = F.nrows, nc = F.ncols, np = F.npiv, ncb = nc - np;
+        if (bs_on && D.is_bs[(size_t)fi]) continue;
         if (pipe[fi]) {
             // critical stream: [pivot-column assembly], LU, then (once the bulk stream has assembled the other
             // columns) the tail on the CB columns that are the parent's pivot columns; bulk stream: the assembly of the
@@ -780,7 +889,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
                     pa.h = pa.cbr > 0 ? hc[gi] : 0;
                     pa.nslot = std::max<int64_t>(0, G.nri - G.npiv);
                     pa.slot = G.slot;
-                    pa.cb = CB + G.cb_off; pa.relcol = D.relcol + G.relcol_off; pa.child_rowid = N.rowid + G.row_off + G.npiv;
+                    pa.cb = cb_of(gi); pa.relcol = D.relcol + G.relcol_off; pa.child_rowid = N.rowid + G.row_off + G.npiv;
                 }
             } else if ((rc = assemble(fi, W, A, ncb > 0 ? 1 : 0))) return rc;
             if ((rc = factor_block(fi, W, perm, A, pa))) return rc;
@@ -871,6 +980,11 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     CK(cudaMemcpyAsync(&h, N.st, sizeof(h), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     prof.flush();
+    // A pivot event (a dense-row pivot, no admissible pivot) must be the first in the fronts' order, as the reference
+    // meets it column by column; the batched levels run the lower fronts of later subtrees first.  Redo it front by
+    // front: this happens on a pattern's first factorization (before its dense-chain start is known) or on failure.
+    if (bs_on && (h.code == ST_BORDER || h.code == ST_SINGULAR) && !h.tc_err)
+        return run_fronts<T>(P, D, N, pivot_rel, border_front, err, errlen, false);
     if (h.tc_err) { errf(err, errlen, "factorization: a tensor-core Schur update timed out (status %u)", h.tc_err); return FPLUS_ERR_GPU; }
     if (h.code == ST_WAIT) { errf(err, errlen, "factorization: a multi-CTA pivot search in front %ld timed out", (long)h.idx); return FPLUS_ERR_GPU; }
     if (h.code == ST_BORDER) { *border_front = h.idx; return FPLUS_OK; }

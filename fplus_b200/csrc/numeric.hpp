@@ -50,6 +50,20 @@ struct DevPlan {
     std::vector<int64_t> sv_brows_ptr, sv_bcols_ptr;
     std::vector<int64_t> brows_maxnr, brows_maxnp, brows_maxm, bcols_maxnp, bcols_maxnch;
     int64_t part_need = 0;
+    // the batched fronts of the factorization: every interior front whose whole subtree fits the one-CTA pivot-block LU
+    // and the fused tail (at most 128 rows and 64 pivots).  They run first, level by level, three launches per level
+    // (assembly, LU, tail), each front with its own working block (wofs, within the level's workspace) and its
+    // contribution block in a separate arena (cbofs); the other fronts follow front by front.  Device descriptors and
+    // children, lists by level with host ranges and the level's largest sizes and algorithmic counts; host flags and
+    // contribution-block offsets
+    FcFront *fc = nullptr;
+    int64_t *children = nullptr;
+    int *bs_list = nullptr;
+    std::vector<int64_t> bs_ptr, bs_maxnr, bs_maxnp, bs_maxtiles, bs_wsz;
+    std::vector<double> bs_lu_flops, bs_tail_flops, bs_asm_bytes, bs_lu_bytes, bs_tail_bytes;
+    std::vector<char> is_bs;
+    std::vector<int64_t> bs_cbofs;
+    int64_t bs_ws = 0, bs_cb = 0;
     int64_t *rsp = nullptr, *rsi = nullptr, *csp = nullptr, *csi = nullptr, *iota = nullptr;
     int64_t vrow = 0, vcol = 0;              // the plan's total front rows, total front columns
     ~DevPlan();
@@ -76,6 +90,8 @@ struct DevNum {
     size_t cap_permall = 0;
     void *vbuf = nullptr;          // the level-scheduled solve's contribution vectors
     size_t cap_vb = 0;
+    void *bsw = nullptr, *bscb = nullptr;   // the batched fronts' working blocks (one level) and contribution blocks
+    size_t cap_bsw = 0, cap_bscb = 0;
     // the look-ahead over chain fronts: a second working block and row order, the critical stream and its events
     void *work2 = nullptr;
     int *perm2 = nullptr;
@@ -92,7 +108,8 @@ struct DevNum {
     void *coopbuf = nullptr;       // the multi-CTA pivot-block LU: the CTAs' posts, the ticket, the choices, U12, row scratch
     size_t cap_coop = 0;
     int lu_variant = 2;            // the small fronts' pivot-block LU (2: k_front_lu2, 3: k_front_lu3); + 4: the tall
-                                   // blocks by one CTA per 32-column panel instead of k_block_lu_mc
+                                   // blocks by one CTA per 32-column panel instead of k_block_lu_mc; + 8: no batched
+                                   // fronts (every front on its own)
     int capture = 0;               // the launches are being captured into a CUDA graph: no host copies, waits or decisions
     void *gm_buf = nullptr;        // GMRES-IR: the Krylov basis and its vectors
     size_t cap_gm = 0;

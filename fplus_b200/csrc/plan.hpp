@@ -67,6 +67,14 @@ struct SvFront {
     long long nch, poff;           // the U sweep of a larger front: CB-column chunks, first partial sum (per right-hand side)
 };
 
+// a front as the batched factorization kernels read it: its shape, arenas and row / column entries, its assembly entries
+// and children, its working block (wofs, within its level's workspace) and contribution block (cbofs, in the batched
+// fronts' contribution-block arena)
+struct FcFront {
+    long long f, np, nr, nri, nc, L_off, U_off, row_off, relcol_off, asm_begin, asm_end, child_begin, child_end, slot,
+        tau_base, wofs, cbofs;
+};
+
 struct fplus_symbolic_view {
     int64_t n, ntr, ntc;
     const int64_t *Bp, *Bi;

@@ -267,3 +267,30 @@ def test_tall_pivot_blocks_match_oracle(gpu, cplx, variant):
     b = W.rhs(n, 1, cplx, 4)[0]
     x = N.solve(b)
     assert O.backward_error(n, Ap, Ai, Ax, x, b) <= 1e-14
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_batched_small_fronts_match_front_by_front(gpu, cplx):
+    """The small fronts at the bottom of the tree factored level by level (one launch per level for assembly, LU and
+    tail) give bit for bit the factors of the front-by-front path (set_front_shape variant + 8), and the oracle's pivots."""
+    g = 14 if cplx else 18
+    n, Ap, Ai, Ax = W.convdiff3d(g, 3)
+    if cplx:
+        Ax = Ax + 0.25j * np.random.default_rng(23).uniform(-1, 1, Ax.size)
+    Ns = []
+    for variant in (2, 10):
+        S = F.analyze(n, Ap, Ai)
+        S.set_front_shape(256, 64, variant)
+        Ns.append((S, S.factor(Ax)))
+    (S1, N1), (S2, N2) = Ns
+    assert np.array_equal(N1.p, N2.p)
+    L1, U1, _ = N1.factors()
+    L2, U2, _ = N2.factors()
+    assert np.array_equal(L1.data, L2.data) and np.array_equal(U1.data, U2.data), "batched factors differ from front by front"
+    orc = O.OracleLU(n, Ap, Ai, Ax, S1.row_perm, S1.col_perm)
+    assert np.array_equal(N1.p, orc.p)
+    b = W.rhs(n, 2, cplx, 6).T.copy(order="F")
+    for trans in ((0, 1, 2) if cplx else (0, 1)):
+        X = N1.solve(b, trans)
+        for r in range(2):
+            assert O.backward_error(n, Ap, Ai, Ax, X[:, r], b[:, r], trans) <= 1e-14
