@@ -99,6 +99,26 @@ __device__ __forceinline__ unsigned long long warp_max_key(unsigned long long ke
     return ((unsigned long long)hi << 32) | lo;
 }
 
+// the smallest 64-bit value over the warp (two 32-bit reductions)
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
+{
+    const unsigned vhi = (unsigned)(v >> 32);
+    const unsigned hi = __reduce_min_sync(0xffffffffu, vhi);
+    const unsigned lo = __reduce_min_sync(0xffffffffu, vhi == hi ? (unsigned)v : 0xffffffffu);
+    return ((unsigned long long)hi << 32) | lo;
+}
+// the lane holding the best candidate of the warp: the largest key (>= 0; -1: no candidate), ties to the smaller row id
+// (ids are distinct and >= 0); -1 when no lane holds one
+__device__ __forceinline__ int warp_argbest(long long key, long long rid)
+{
+    const unsigned long long k = key >= 0 ? (unsigned long long)key + 1ull : 0ull;
+    const unsigned long long m = warp_max_key(k);
+    if (m == 0ull) return -1;
+    const unsigned long long rmin = warp_min_u64(k == m ? (unsigned long long)rid : ~0ull);
+    const unsigned bal = __ballot_sync(0xffffffffu, k == m && (unsigned long long)rid == rmin);
+    return __ffs(bal) - 1;
+}
+
 // 1 / p for the pivot: conj(p) / |p|^2 with the components scaled by max(|re|, |im|) first (no overflow or underflow of the
 // squares); real: 1 / p
 // (__drcp_rn: the correctly rounded reciprocal, the same value as the IEEE quotient 1.0 / q)

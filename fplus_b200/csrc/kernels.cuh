@@ -395,8 +395,8 @@ __global__ void __launch_bounds__(MC_THREADS) k_block_lu_mc(T *W, int64_t ld, in
         if (tid == 0) s_stop = *cg::this_cluster().map_shared_rank(&s_stop, 0);
     }
     __syncthreads();
-    auto better = [](long long k, long long r, long long bk, long long br) { return k > bk || (k == bk && r < br); };
-    for (int p0 = 0; p0 < npr && !s_stop; p0 += MC_PW) {
+    bool stopped = s_stop != 0;                          // the same in every thread (every decision below is)
+    for (int p0 = 0; p0 < npr && !stopped; p0 += MC_PW) {
         const int w = npr - p0 < MC_PW ? npr - p0 : MC_PW;
         if (tid < w) s_thr[tid] = pivot_rel * colmax[fcol + p0 + tid];
         for (int e = tid; e < w * nmine; e += MC_THREADS) {
@@ -404,29 +404,28 @@ __global__ void __launch_bounds__(MC_THREADS) k_block_lu_mc(T *W, int64_t ld, in
             S[c * per + r] = W[(r_lo + r) + (int64_t)(p0 + c) * ld];
         }
         __syncthreads();
+        // every thread owns row tid of this CTA's rows for the whole panel (per <= MC_THREADS): its key, its multiplier
+        // and its update need no block barrier
+        bool mine = tid < nmine && live[tid];
         for (int kk = 0; kk < w; kk++) {
             const int j = p0 + kk, par = j & 1;
             // 1. the best of this CTA's live rows in column j, posted
-            long long bk = -1, brid = LLONG_MAX, brow = -1;
-            for (int r = tid; r < nmine; r += MC_THREADS) {
-                if (!live[r]) continue;
-                const long long key = (long long)pivkey(S[kk * per + r]);
-                if (better(key, rid_s[r], bk, brid)) { bk = key; brid = rid_s[r]; brow = r; }
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                const long long ok = __shfl_xor_sync(0xffffffffu, bk, o), orr = __shfl_xor_sync(0xffffffffu, brid, o),
-                                ow = __shfl_xor_sync(0xffffffffu, brow, o);
-                if (better(ok, orr, bk, brid)) { bk = ok; brid = orr; brow = ow; }
+            long long bk = mine ? (long long)pivkey(S[kk * per + tid]) : -1, brid = mine ? rid_s[tid] : LLONG_MAX;
+            long long brow = mine ? tid : -1;
+            {
+                const int src = warp_argbest(bk, brid);
+                bk = src >= 0 ? __shfl_sync(0xffffffffu, bk, src) : -1;
+                brid = src >= 0 ? __shfl_sync(0xffffffffu, brid, src) : LLONG_MAX;
+                brow = src >= 0 ? __shfl_sync(0xffffffffu, brow, src) : -1;
             }
             if (lane == 0) { s_k[warp] = bk; s_r[warp] = brid; s_p[warp] = brow; }
             __syncthreads();
             if (warp == 0) {
                 bk = lane < nw ? s_k[lane] : -1; brid = lane < nw ? s_r[lane] : LLONG_MAX; brow = lane < nw ? s_p[lane] : -1;
-                for (int o = 16; o > 0; o >>= 1) {
-                    const long long ok = __shfl_xor_sync(0xffffffffu, bk, o), orr = __shfl_xor_sync(0xffffffffu, brid, o),
-                                    ow = __shfl_xor_sync(0xffffffffu, brow, o);
-                    if (better(ok, orr, bk, brid)) { bk = ok; brid = orr; brow = ow; }
-                }
+                const int src = warp_argbest(bk, brid);
+                bk = src >= 0 ? __shfl_sync(0xffffffffu, bk, src) : -1;
+                brid = src >= 0 ? __shfl_sync(0xffffffffu, brid, src) : LLONG_MAX;
+                brow = src >= 0 ? __shfl_sync(0xffffffffu, brow, src) : -1;
                 const T v = (lane < w && brow >= 0) ? S[lane * per + brow] : VT<T>::zero();
                 const long long pos = brow >= 0 ? r_lo + brow : -1;
                 if constexpr (CL) {
@@ -441,97 +440,87 @@ __global__ void __launch_bounds__(MC_THREADS) k_block_lu_mc(T *W, int64_t ld, in
                     if (lane < w) my->v[lane] = v;
                     if (lane == 0) { my->key = bk; my->rid = brid; my->pos = pos; }
                     __syncwarp();
-                    if (lane == 0) red_release_add_u32(sync + 1, 1u);
+                    if (lane == 0) {
+                        red_release_add_u32(sync + 1, 1u);
+                        const unsigned target = (unsigned)G * (unsigned)(j + 1);
+                        unsigned it = 0;
+                        while (ld_acquire_u32(sync + 1) < target && ++it < MC_SPIN) {}
+                        if (it >= MC_SPIN) s_wait = 1;
+                    }
                 }
             }
-            // 2. the barrier, then the same winner in every CTA
+            // 2. the barrier, then the same winner in every warp
             long long gk = -1, gr = LLONG_MAX, gp = -1;
             int gq = -1;
+            const T *wv;                                 // the winner's panel values
             if constexpr (CL) {
                 cg::this_cluster().sync();
-            } else {
-                if (tid == 0) {
-                    const unsigned target = (unsigned)G * (unsigned)(j + 1);
-                    unsigned it = 0;
-                    while (ld_acquire_u32(sync + 1) < target && ++it < MC_SPIN) {}
-                    if (it >= MC_SPIN) s_wait = 1;
+                if (lane < G) {
+                    const McSlot<T> *c = cs + par * MC_CMAX + lane;
+                    gk = c->key; gr = c->rid; gp = c->pos; gq = lane;
                 }
+                const int src = warp_argbest(gk, gr);
+                gp = src >= 0 ? __shfl_sync(0xffffffffu, gp, src) : -1;
+                gq = src >= 0 ? __shfl_sync(0xffffffffu, gq, src) : -1;
+                gk = src >= 0 ? __shfl_sync(0xffffffffu, gk, src) : -1;
+                wv = gq >= 0 ? cs[par * MC_CMAX + gq].v : Lb + kk * MC_LB;
+            } else {
                 __syncthreads();
                 if (tid < G && !s_wait) {
                     const McSlot<T> *c = gslots + (size_t)par * G + tid;
                     gk = __ldcg(&c->key); gr = __ldcg(&c->rid); gp = __ldcg(&c->pos); gq = tid;
                 }
-                for (int o = 16; o > 0; o >>= 1) {
-                    const long long ok = __shfl_xor_sync(0xffffffffu, gk, o), orr = __shfl_xor_sync(0xffffffffu, gr, o),
-                                    op = __shfl_xor_sync(0xffffffffu, gp, o);
-                    const int oq = __shfl_xor_sync(0xffffffffu, gq, o);
-                    if (op >= 0 && (gp < 0 || better(ok, orr, gk, gr))) { gk = ok; gr = orr; gp = op; gq = oq; }
+                {
+                    const int src = warp_argbest(gk, gr);
+                    gk = src >= 0 ? __shfl_sync(0xffffffffu, gk, src) : -1;
+                    gr = src >= 0 ? __shfl_sync(0xffffffffu, gr, src) : LLONG_MAX;
+                    gp = src >= 0 ? __shfl_sync(0xffffffffu, gp, src) : -1;
+                    gq = src >= 0 ? __shfl_sync(0xffffffffu, gq, src) : -1;
                 }
                 if (lane == 0) { s_k[warp] = gk; s_r[warp] = gr; s_p[warp] = gp; s_q[warp] = gq; }
                 __syncthreads();
+                gk = lane < nw ? s_k[lane] : -1; gr = lane < nw ? s_r[lane] : LLONG_MAX;
+                gp = lane < nw ? s_p[lane] : -1; gq = lane < nw ? s_q[lane] : -1;
+                const int src = warp_argbest(gk, gr);
+                gp = src >= 0 ? __shfl_sync(0xffffffffu, gp, src) : -1;
+                gq = src >= 0 ? __shfl_sync(0xffffffffu, gq, src) : -1;
+                gk = src >= 0 ? __shfl_sync(0xffffffffu, gk, src) : -1;
+                // warp 0 brings the winner's values into Lb for every warp
+                if (warp == 0 && lane < w)
+                    Lb[kk * MC_LB + lane] = gq >= 0 ? ldcg_v(&gslots[(size_t)par * G + gq].v[lane]) : VT<T>::zero();
+                __syncthreads();
+                wv = Lb + kk * MC_LB;
             }
-            if (warp == 0) {
-                if constexpr (CL) {
-                    if (lane < G) {
-                        const McSlot<T> *c = cs + par * MC_CMAX + lane;
-                        gk = c->key; gr = c->rid; gp = c->pos; gq = lane;
-                    }
-                } else {
-                    gk = lane < nw ? s_k[lane] : -1; gr = lane < nw ? s_r[lane] : LLONG_MAX;
-                    gp = lane < nw ? s_p[lane] : -1; gq = lane < nw ? s_q[lane] : -1;
-                }
-                for (int o = 16; o > 0; o >>= 1) {
-                    const long long ok = __shfl_xor_sync(0xffffffffu, gk, o), orr = __shfl_xor_sync(0xffffffffu, gr, o),
-                                    op = __shfl_xor_sync(0xffffffffu, gp, o);
-                    const int oq = __shfl_xor_sync(0xffffffffu, gq, o);
-                    if (op >= 0 && (gp < 0 || better(ok, orr, gk, gr))) { gk = ok; gr = orr; gp = op; gq = oq; }
-                }
-                // the winner's panel values: row j of L11 \ U11
-                T v = VT<T>::zero();
-                if (gq >= 0 && lane < w) {
-                    if constexpr (CL) v = cs[par * MC_CMAX + gq].v[lane];
-                    else v = ldcg_v(&gslots[(size_t)par * G + gq].v[lane]);
-                }
-                if (lane < w) Lb[kk * MC_LB + lane] = v;
-                T pv;
-                if constexpr (VT<T>::cplx_) pv = T{__shfl_sync(0xffffffffu, v.x, kk), __shfl_sync(0xffffffffu, v.y, kk)};
-                else pv = __shfl_sync(0xffffffffu, v, kk);
-                if (lane == 0) {
-                    int stop = 0;
-                    if (s_wait) {
-                        set_status(st, ST_WAIT, front, 0.0, 0.0);
-                        stop = 1;
-                    } else {
-                        const double t = s_thr[kk];
-                        if (gp < 0 || gk <= 0 || ((unsigned long long)gk < pivkey_of_modulus<T>(2.0 * t) && vabs(pv) < t)) {
-                            if (b == 0) set_status(st, ST_SINGULAR, fcol + j, gp >= 0 ? vabs(pv) : 0.0, t);
-                            stop = 1;
-                        } else if (gp >= nri) {
-                            if (b == 0) set_status(st, ST_BORDER, front, vabs(pv), t);
-                            stop = 1;
-                        }
-                    }
-                    s_stop = stop;
-                    if (!stop) {
-                        if (b == 0) chosen[j] = gp;
-                        if (gp >= r_lo && gp < r_hi) live[gp - r_lo] = 0;     // its owner takes it out of the search
-                        s_piv[kk] = (int)gp;
-                    }
+            const T pv = gq >= 0 ? wv[kk] : VT<T>::zero();
+            // the decision, the same in every thread
+            const double t = s_thr[kk];
+            int stop = 0;
+            if (!CL && s_wait) stop = 2;
+            else if (gp < 0 || gk <= 0 || ((unsigned long long)gk < pivkey_of_modulus<T>(2.0 * t) && vabs(pv) < t)) stop = 1;
+            else if (gp >= nri) stop = 3;
+            if (tid == 0) {
+                if (stop == 2) set_status(st, ST_WAIT, front, 0.0, 0.0);
+                else if (stop == 1 && b == 0) set_status(st, ST_SINGULAR, fcol + j, gp >= 0 ? vabs(pv) : 0.0, t);
+                else if (stop == 3 && b == 0) set_status(st, ST_BORDER, front, vabs(pv), t);
+                if (!stop) { if (b == 0) chosen[j] = gp; s_piv[kk] = (int)gp; }
+            }
+            if (stop) { stopped = true; break; }
+            if (CL && warp == 0 && lane < w) Lb[kk * MC_LB + lane] = wv[lane];
+            // 3. this thread's row: the pivot row leaves the search; a live row takes its multiplier and the update of
+            // the panel's later columns
+            if (mine) {
+                if (r_lo + tid == gp) mine = false;
+                else {
+                    const T inv = recip(pv);
+                    const T l = mul(S[kk * per + tid], inv);
+                    S[kk * per + tid] = l;
+                    for (int c = kk + 1; c < w; c++) S[c * per + tid] = sub(S[c * per + tid], mul(l, wv[c]));
                 }
             }
-            __syncthreads();
-            if (s_stop) break;
-            // 3. this CTA's live rows: the multiplier, then the update of the panel's later columns
-            const T inv = recip(Lb[kk * MC_LB + kk]);
-            for (int r = tid; r < nmine; r += MC_THREADS) {
-                if (!live[r]) continue;
-                const T l = mul(S[kk * per + r], inv);
-                S[kk * per + r] = l;
-                for (int c = kk + 1; c < w; c++) S[c * per + r] = sub(S[c * per + r], mul(l, Lb[kk * MC_LB + c]));
-            }
-            __syncthreads();
         }
-        if (s_stop) break;
+        if (tid < per) live[tid] = mine ? 1 : 0;
+        if (stopped) break;
+        __syncthreads();
         for (int e = tid; e < w * nmine; e += MC_THREADS) {
             const int c = e / nmine, r = e - c * nmine;
             W[(r_lo + r) + (int64_t)(p0 + c) * ld] = S[c * per + r];
