@@ -206,11 +206,13 @@ __global__ void k_colmax(const int64_t *__restrict__ seg, int64_t nseg, const T 
 template <typename T>
 __global__ void k_assemble(T *__restrict__ W, const T *__restrict__ Bx, const int64_t *__restrict__ src,
                            const int64_t *__restrict__ dst, int64_t cnt, int64_t *__restrict__ rowid,
-                           const int64_t *__restrict__ rowinit, int64_t nrows, const DevStatus *st)
+                           const int64_t *__restrict__ rowinit, int64_t nrows, const DevStatus *st, int addto = 0)
 {
+    // addto: the block already holds the child's contribution block (written by its Schur update), the entries add to it
     if (st->code) return;
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e = tid; e < cnt; e += stride) W[dst[e]] = Bx[src[e]];
+    if (addto) for (int64_t e = tid; e < cnt; e += stride) W[dst[e]] = add(W[dst[e]], Bx[src[e]]);
+    else for (int64_t e = tid; e < cnt; e += stride) W[dst[e]] = Bx[src[e]];
     for (int64_t i = tid; i < nrows; i += stride) if (rowinit[i] >= 0) rowid[i] = rowinit[i];
 }
 
@@ -719,7 +721,8 @@ constexpr int GBM = 64, GBN = 64, GBK = 16, GPAD = 68, GBP = 20;   // A staged [
 template <typename T>
 __global__ void __launch_bounds__(256) k_gemm_sub(int64_t M, int64_t N, int64_t K, const T *__restrict__ A, int64_t lda,
                                                  const T *__restrict__ B, int64_t ldb, const T *Cin, int64_t ldci,
-                                                 const int *__restrict__ rmap, T *Cout, int64_t ldco, const DevStatus *st)
+                                                 const int *__restrict__ rmap, T *Cout, int64_t ldco, const DevStatus *st,
+                                                 OutMap om)
 {
     constexpr bool CP = VT<T>::cplx_;
     __shared__ double As[CP ? 2 : 1][GBK][GPAD];
@@ -811,7 +814,8 @@ __global__ void __launch_bounds__(256) k_gemm_sub(int64_t M, int64_t N, int64_t 
                     T v = Cin[gi + gn * ldci];
                     if constexpr (CP) { v.x -= acc[0][a][b][h]; v.y -= acc[1][a][b][h]; }
                     else v -= acc[0][a][b][h];
-                    Cout[gm + gn * ldco] = v;
+                    if (om.col) Cout[(gm < om.nslot ? om.slot + gm : om.tau + (gm - om.nslot)) + om.col[gn] * ldco] = v;
+                    else Cout[gm + gn * ldco] = v;
                 }
             }
 }

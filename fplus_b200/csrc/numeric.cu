@@ -678,24 +678,28 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     auto cb_of = [&](int64_t gi) -> T * { return bs_on && D.is_bs[(size_t)gi] ? CBA + D.bs_cbofs[(size_t)gi] : CB + P.fronts[(size_t)gi].cb_off; };
 
     // the assembly of columns [0, npiv) (part 1), the others (part 2), or all (part 0)
+    // (part 3: every column, with the single child's contribution block already written into W by its Schur update and
+    // the entering rows zeroed: the original entries add to it, the child gives its row ids only)
     auto assemble = [&](int64_t fi, T *W, cudaStream_t st, int part) {
         const Front &F = P.fronts[fi];
         const int64_t nr = F.nrows, nc = F.ncols, np = F.npiv, ld = nr;
+        const bool pre = part == 3;
         const int64_t e0 = part == 2 ? F.asm_mid : F.asm_begin, e1 = part == 1 ? F.asm_mid : F.asm_end;
-        const int64_t z0 = part == 2 ? nr * np : 0, z1 = part == 1 ? nr * np : nr * nc;
+        const int64_t z0 = part == 2 ? nr * np : 0, z1 = pre ? 0 : part == 1 ? nr * np : nr * nc;
         prof.begin(st, PROF_ASM, 0.0, (double)((z1 - z0) + 2 * (e1 - e0)) * vs);
         if (z1 > z0) CK(cudaMemsetAsync(W + z0, 0, (size_t)(z1 - z0) * vs, st));
         const int64_t cnt = e1 - e0, nri = part == 2 ? 0 : nr;
         if (cnt > 0 || nri > 0)
             k_assemble<T><<<nblk(std::max(cnt, nri)), 256, 0, st>>>(W, Bx, D.asm_src + e0, D.asm_dst + e0, cnt,
-                                                                    N.rowid + F.row_off, D.rowinit + F.row_off, nri, N.st), note_launch();
+                                                                    N.rowid + F.row_off, D.rowinit + F.row_off, nri, N.st,
+                                                                    pre ? 1 : 0), note_launch();
         for (int64_t k = F.child_begin; k < F.child_end; k++) {
             const int64_t gi = P.children[k];
             const Front &G = P.fronts[gi];
             const int64_t cbr = std::max<int64_t>(0, G.nrows - G.npiv), cbc = G.ncols - G.npiv;
             const int64_t nslot = std::max<int64_t>(0, G.nri - G.npiv);
             if (cbr == 0) continue;
-            const int64_t c0 = part == 2 ? hc[gi] : 0, c1 = part == 1 ? hc[gi] : cbc;
+            const int64_t c0 = part == 2 ? hc[gi] : 0, c1 = pre ? 0 : part == 1 ? hc[gi] : cbc;
             const int rowids = part != 2;
             if (c1 <= c0 && !rowids) continue;
             k_extend_add<T><<<nblk(std::max(cbr * std::max<int64_t>(c1 - c0, 0), nslot)), 256, 0, st>>>(
@@ -797,7 +801,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
                             dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((Nn + GBN - 1) / GBN));
                             T *C = W + (k0 + w) + (k0 + w) * ld;
                             k_gemm_sub<T><<<g, 256, 0, st>>>(M, Nn, w, W + (k0 + w) + k0 * ld, ld, W + k0 + (k0 + w) * ld, ld,
-                                                             C, ld, nullptr, C, ld, N.st), note_launch();
+                                                             C, ld, nullptr, C, ld, N.st, OutMap{}), note_launch();
                         }
                     }
                 }
@@ -861,6 +865,26 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         }
     }
 
+    // A front whose parent is the next front, takes no other child, and whose contribution block covers every row of the
+    // parent's working block but its entering rows, and every column: its Schur update writes straight into the
+    // parent's working block (through the extend-add maps; the two working blocks alternate), whose entering rows are
+    // zeroed first and whose original entries are added after.  The contribution block never goes through the stack.
+    std::vector<char> direct((size_t)nf, 0);
+    bool any_direct = false;
+    for (int64_t fi = 0; fi + 1 < nf; fi++) {
+        const Front &F = P.fronts[(size_t)fi], &Q = P.fronts[(size_t)fi + 1];
+        if (pipe[(size_t)fi] || pipe[(size_t)fi + 1] || F.parent != fi + 1 || Q.child_end - Q.child_begin != 1) continue;
+        if (bs_on && (D.is_bs[(size_t)fi] || D.is_bs[(size_t)fi + 1])) continue;
+        const int64_t np = F.npiv, nr = F.nrows, ncb = F.ncols - np, M = nr - np;
+        if (np == 0 || np > nr || M <= 0 || ncb <= 0 || (np <= FT_NP && nr <= FT_NR)) continue;
+        const int64_t nslot = std::max<int64_t>(0, F.nri - np);
+        if (ncb != Q.ncols || F.slot + nslot != Q.tau_base || M - nslot != Q.nrows - Q.tau_base) continue;
+        direct[(size_t)fi] = 1;
+        any_direct = true;
+    }
+    if (any_direct && (rc = ensure_async(N, (void **)&N.work2, &N.cap_work2, (size_t)P.work_size * vs, err, errlen))) return rc;
+    T *next_W = nullptr;                 // the working block a direct child has written into, for the next front
+
     bool in_pipe = false;
     int wsel = 0;
     for (int64_t fi = 0; fi < nf; fi++) {
@@ -908,10 +932,12 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             continue;
         }
         if (in_pipe) { CK(cudaEventRecord(N.ev_lu, A)); CK(cudaStreamWaitEvent(s, N.ev_lu, 0)); in_pipe = false; }
-        T *W = (T *)N.work;
+        T *W = next_W ? next_W : (T *)N.work;
+        const bool pre = next_W != nullptr;
+        next_W = nullptr;
         T *Lf = La + F.L_off;
         const int64_t ld = nr;
-        if ((rc = assemble(fi, W, s, 0))) return rc;
+        if ((rc = assemble(fi, W, s, pre ? 3 : 0))) return rc;
         if (np == 0) continue;
         if (nr == 0) { k_set_singular<<<1, 1, 0, s>>>(N.st, F.f), note_launch(); continue; }     // no row can take pivot step f
         if ((rc = factor_block(fi, W, N.permall + F.row_off, s, PivotAsm{}))) return rc;
@@ -943,7 +969,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             if (M > 0) {
                 dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((ncb + GBN - 1) / GBN));
                 T *C = Uf + k0 + w;
-                k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, w, Lf + (k0 + w) + k0 * ld, ld, Uf + k0, np, C, np, nullptr, C, np, N.st), note_launch();
+                k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, w, Lf + (k0 + w) + k0 * ld, ld, Uf + k0, np, C, np, nullptr, C, np, N.st, OutMap{}), note_launch();
             }
         }
         }
@@ -952,6 +978,20 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         // cores in reduced precision for the large updates; FP64 DMMA otherwise)
         const int64_t M = nr - np;
         if (M > 0) {
+            // the output: the stack, or (direct) the parent's working block, the other of the two, its entering rows zeroed
+            T *Cout = CB + F.cb_off;
+            int64_t ldco = M;
+            OutMap om{};
+            if (direct[(size_t)fi]) {
+                const Front &Q = P.fronts[(size_t)fi + 1];
+                T *Wq = W == (T *)N.work ? (T *)N.work2 : (T *)N.work;
+                if (F.slot > 0)
+                    CK(cudaMemset2DAsync(Wq, (size_t)Q.nrows * vs, 0, (size_t)F.slot * vs, (size_t)Q.ncols, s));
+                Cout = Wq;
+                ldco = Q.nrows;
+                om = OutMap{D.relcol + F.relcol_off, std::max<int64_t>(0, F.nri - np), F.slot, Q.tau_base};
+                next_W = Wq;
+            }
             prof.begin(s, PROF_SCHUR, fm * (double)M * (double)ncb * (double)np, (double)(2 * M * ncb + M * np + np * ncb) * vs);
             const bool tc = N.prec != PREC_FP64 && M >= TC_MIN_ROWS && ncb >= TC_MIN_COLS &&
                             (double)M * (double)ncb * (double)np >= TC_MIN_MADDS && schur_tc_supported(M, ncb, np, VT<T>::cplx_);
@@ -960,13 +1000,14 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
                 const size_t wsb = schur_tc_workspace(N.prec, M, ncb, np, VT<T>::cplx_);
                 if ((rc = ensure_async(N, &N.tcws, &N.cap_tcws, wsb, err, errlen))) return rc;
                 trc = schur_tc(N.prec, VT<T>::cplx_, M, ncb, np, (const double *)(Lf + np), ld, (const double *)Uf, np,
-                               (const double *)(W + np * ld), ld, N.permall + F.row_off + np, (double *)(CB + F.cb_off), M, N.tcws, N.cap_tcws,
-                               &N.st->tc_err, s);
+                               (const double *)(W + np * ld), ld, N.permall + F.row_off + np, (double *)Cout, ldco, N.tcws, N.cap_tcws,
+                               &N.st->tc_err, s, om);
                 if (trc == 0) { note_launch(); add_launches(2); N.tc_updates++; N.tc_flops += fm * (double)M * (double)ncb * (double)np; }
             }
             if (trc != 0) {
                 dim3 g((unsigned)((M + GBM - 1) / GBM), (unsigned)((ncb + GBN - 1) / GBN));
-                k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, np, Lf + np, ld, Uf, np, W + np * ld, ld, N.permall + F.row_off + np, CB + F.cb_off, M, N.st), note_launch();
+                k_gemm_sub<T><<<g, 256, 0, s>>>(M, ncb, np, Lf + np, ld, Uf, np, W + np * ld, ld, N.permall + F.row_off + np, Cout,
+                                                ldco, N.st, om), note_launch();
             }
             prof.end(s);
         }

@@ -60,6 +60,14 @@ struct FrontPlan {
     int nlevels = 0;
 };
 
+// Where a Schur update's output element (i, j) goes: identity when col is null, else row i < nslot -> slot + i, row
+// i >= nslot -> tau + (i - nslot), column j -> col[j] (a child's contribution block written straight into its parent's
+// working block, through the extend-add maps)
+struct OutMap {
+    const int64_t *col;
+    int64_t nslot, slot, tau;
+};
+
 // a front as the level-scheduled solve kernels read it (pivot columns [f, f + np), nr rows of which nri above the border,
 // nc columns; its L block, its U12 block, its first entry in the plan's row and column arrays)
 struct SvFront {

@@ -136,7 +136,7 @@ template <bool BF16, bool CPLX>
 __global__ void __launch_bounds__(THREADS, 1) k_schur_tc(const __grid_constant__ CUtensorMap tmA,
                                                         const __grid_constant__ CUtensorMap tmB, int M, int Nd, int kb128,
                                                         const double *Cin, int64_t ldci, const int *__restrict__ rmap,
-                                                        double *Cout, int64_t ldco, unsigned *err)
+                                                        double *Cout, int64_t ldco, unsigned *err, OutMap om)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     unsigned char *sm = (unsigned char *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);   // 1024-byte aligned ring
@@ -232,6 +232,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_schur_tc(const __grid_constant__
             const int row = m0 + q * 32 + lane;
             const bool live = row < M;
             const int64_t src = live ? (int64_t)(rmap ? rmap[row] : row) : 0;
+            const int64_t orow = om.col ? (row < om.nslot ? om.slot + row : om.tau + (row - om.nslot)) : row;
             for (int c0 = half * (BN / 2); c0 < (half + 1) * (BN / 2); c0 += 32) {
                 float v[32];
                 __syncwarp();
@@ -244,7 +245,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_schur_tc(const __grid_constant__
                     for (int j = 0; j < 32; j++) cin[j] = d0 + j < Nd ? Cin[src + (int64_t)(d0 + j) * ldci] : 0.0;
 #pragma unroll
                     for (int j = 0; j < 32; j++)
-                        if (d0 + j < Nd) Cout[row + (int64_t)(d0 + j) * ldco] = cin[j] - (double)v[j];
+                        if (d0 + j < Nd) Cout[orow + (om.col ? om.col[d0 + j] : (int64_t)(d0 + j)) * ldco] = cin[j] - (double)v[j];
                 } else {
                     const cplx_t *ci = (const cplx_t *)Cin;
                     cplx_t *co = (cplx_t *)Cout;
@@ -255,7 +256,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_schur_tc(const __grid_constant__
 #pragma unroll
                     for (int j = 0; j < 16; j++)
                         if (d0 + 2 * j < Nd)
-                            co[row + (int64_t)(c + j) * ldco] = cplx_t{cin[j].x - (double)v[2 * j], cin[j].y - (double)v[2 * j + 1]};
+                            co[orow + (om.col ? om.col[c + j] : (int64_t)(c + j)) * ldco] =
+                                cplx_t{cin[j].x - (double)v[2 * j], cin[j].y - (double)v[2 * j + 1]};
                 }
             }
             tc_fence_before();
@@ -390,7 +392,7 @@ bool make_map(CUtensorMap *m, const void *base, int64_t rows, int64_t Kp, int es
 template <bool BF16, bool CPLX>
 int run(int P, int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B, int64_t ldb, const double *Cin,
         int64_t ldci, const int *rmap, double *Cout, int64_t ldco, void *ws, size_t ws_bytes, unsigned *err, cudaStream_t s,
-        int nsm)
+        int nsm, OutMap om)
 {
     using E = typename SplitT<BF16>::E;
     const int64_t esz = sizeof(E), per = ROWB / esz;
@@ -413,7 +415,7 @@ int run(int P, int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, co
     const int64_t tiles = ((M + BM - 1) / BM) * ((Nd + BN - 1) / BN);
     const int grid = (int)std::min<int64_t>(tiles, nsm);
     k_schur_tc<BF16, CPLX><<<grid, THREADS, SMEM_BYTES, s>>>(ma, mb, (int)M, (int)Nd, (int)(Kp * esz / ROWB), Cin, ldci, rmap,
-                                                             Cout, ldco, err);
+                                                             Cout, ldco, err, om);
     return cudaGetLastError() == cudaSuccess ? 0 : -4;
 }
 
@@ -436,7 +438,7 @@ bool schur_tc_supported(int64_t M, int64_t N, int64_t K, int cplx)
 
 int schur_tc(int prec, int cplx, int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B, int64_t ldb,
              const double *Cin, int64_t ldci, const int *rmap, double *Cout, int64_t ldco, void *ws, size_t ws_bytes,
-             unsigned *err, cudaStream_t s)
+             unsigned *err, cudaStream_t s, OutMap om)
 {
     static int nsm = 0;
     if (!nsm) {
@@ -447,10 +449,10 @@ int schur_tc(int prec, int cplx, int64_t M, int64_t N, int64_t K, const double *
     }
     const int P = prec == PREC_TF32 ? 1 : 3;
     if (prec == PREC_BF16X3)
-        return cplx ? run<true, true>(P, M, N, K, A, lda, B, ldb, Cin, ldci, rmap, Cout, ldco, ws, ws_bytes, err, s, nsm)
-                    : run<true, false>(P, M, N, K, A, lda, B, ldb, Cin, ldci, rmap, Cout, ldco, ws, ws_bytes, err, s, nsm);
-    return cplx ? run<false, true>(P, M, N, K, A, lda, B, ldb, Cin, ldci, rmap, Cout, ldco, ws, ws_bytes, err, s, nsm)
-                : run<false, false>(P, M, N, K, A, lda, B, ldb, Cin, ldci, rmap, Cout, ldco, ws, ws_bytes, err, s, nsm);
+        return cplx ? run<true, true>(P, M, N, K, A, lda, B, ldb, Cin, ldci, rmap, Cout, ldco, ws, ws_bytes, err, s, nsm, om)
+                    : run<true, false>(P, M, N, K, A, lda, B, ldb, Cin, ldci, rmap, Cout, ldco, ws, ws_bytes, err, s, nsm, om);
+    return cplx ? run<false, true>(P, M, N, K, A, lda, B, ldb, Cin, ldci, rmap, Cout, ldco, ws, ws_bytes, err, s, nsm, om)
+                : run<false, false>(P, M, N, K, A, lda, B, ldb, Cin, ldci, rmap, Cout, ldco, ws, ws_bytes, err, s, nsm, om);
 }
 
 }  // namespace fpl

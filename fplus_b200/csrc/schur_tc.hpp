@@ -3,6 +3,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
+#include "plan.hpp"
 
 namespace fpl {
 
@@ -23,8 +24,9 @@ bool schur_tc_supported(int64_t M, int64_t N, int64_t K, int cplx);
 // PREC_BF16X3 or PREC_TF32.  ws: at least schur_tc_workspace() bytes of device memory.  A wait in the kernel that runs
 // out of time sets bit 0 (or 1) of *err (device memory).  Returns 0, or a negative value when the launch could not be
 // made (workspace too small, no tensor-map encoder, a launch error).
+// om: where each output element goes (OutMap; identity when om.col is null).
 int schur_tc(int prec, int cplx, int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B, int64_t ldb,
              const double *Cin, int64_t ldci, const int *rmap, double *Cout, int64_t ldco, void *ws, size_t ws_bytes,
-             unsigned *err, cudaStream_t s);
+             unsigned *err, cudaStream_t s, OutMap om = OutMap{});
 
 }  // namespace fpl
