@@ -422,7 +422,8 @@ __global__ void __launch_bounds__(MC_THREADS) k_block_lu_mc(T *W, int64_t ld, in
             }
             if (lane == 0) { s_k[warp] = bk; s_r[warp] = brid; s_p[warp] = brow; }
             __syncthreads();
-            if (warp == 0) {
+            if (CL ? warp < G : warp == 0) {
+                // the CTA's best (cluster form: every pushing warp takes it; warp d pushes it into CTA d)
                 bk = lane < nw ? s_k[lane] : -1; brid = lane < nw ? s_r[lane] : LLONG_MAX; brow = lane < nw ? s_p[lane] : -1;
                 const int src = warp_argbest(bk, brid);
                 bk = src >= 0 ? __shfl_sync(0xffffffffu, bk, src) : -1;
@@ -431,12 +432,9 @@ __global__ void __launch_bounds__(MC_THREADS) k_block_lu_mc(T *W, int64_t ld, in
                 const T v = (lane < w && brow >= 0) ? S[lane * per + brow] : VT<T>::zero();
                 const long long pos = brow >= 0 ? r_lo + brow : -1;
                 if constexpr (CL) {
-                    cg::cluster_group cl = cg::this_cluster();
-                    for (int d = 0; d < G; d++) {
-                        McSlot<T> *dst = cl.map_shared_rank(cs + par * MC_CMAX + b, d);
-                        if (lane < w) dst->v[lane] = v;
-                        if (lane == 0) { dst->key = bk; dst->rid = brid; dst->pos = pos; }
-                    }
+                    McSlot<T> *dst = cg::this_cluster().map_shared_rank(cs + par * MC_CMAX + b, warp);
+                    if (lane < w) dst->v[lane] = v;
+                    if (lane == 0) { dst->key = bk; dst->rid = brid; dst->pos = pos; }
                 } else {
                     McSlot<T> *my = gslots + (size_t)par * G + b;
                     if (lane < w) my->v[lane] = v;
@@ -516,6 +514,7 @@ __global__ void __launch_bounds__(MC_THREADS) k_block_lu_mc(T *W, int64_t ld, in
                     const T inv = recip(pv);
                     const T l = mul(S[kk * per + tid], inv);
                     S[kk * per + tid] = l;
+#pragma unroll 4
                     for (int c = kk + 1; c < w; c++) S[c * per + tid] = sub(S[c * per + tid], mul(l, wv[c]));
                 }
             }
@@ -530,9 +529,18 @@ __global__ void __launch_bounds__(MC_THREADS) k_block_lu_mc(T *W, int64_t ld, in
         // the trailing columns [p0 + w, npiv) by chunks
         for (int c0 = p0 + w; c0 < npiv; c0 += CW) {
             const int cw = npiv - c0 < CW ? npiv - c0 : CW;
-            for (int e = tid; e < w * cw; e += MC_THREADS) {
-                const int k = e % w, c = e / w;
-                Uc[k * CW + c] = ldcg_v(W + s_piv[k] + (int64_t)(c0 + c) * ld);
+            for (int e0 = tid; e0 < w * cw; e0 += 8 * MC_THREADS) {        // eight loads in flight per thread
+                T u[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const int e = e0 + q * MC_THREADS;
+                    u[q] = e < w * cw ? ldcg_v(W + s_piv[e % w] + (int64_t)(c0 + e / w) * ld) : VT<T>::zero();
+                }
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const int e = e0 + q * MC_THREADS;
+                    if (e < w * cw) Uc[(e % w) * CW + e / w] = u[q];
+                }
             }
             __syncthreads();
             // U12 = L11^-1 A12: a thread per column, 8-row blocks in registers (the order of a forward substitution)
