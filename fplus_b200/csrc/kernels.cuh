@@ -1892,23 +1892,33 @@ __device__ void blk_trisolve(const T *__restrict__ L, int64_t ld, int np, T *x, 
         }
         __syncthreads();
         const int o0 = UPPER ? 0 : r0 + w, o1 = UPPER ? r0 : np;
-        if (o1 > o0)
-            for (int64_t e = tid; e < (int64_t)(o1 - o0) * nrhs; e += blockDim.x) {
-                const int row = o0 + (int)(e % (o1 - o0));
-                const int64_t r = e / (o1 - o0);
+        if (o1 > o0) {
+            // a thread per (row, block of 8 right-hand sides): L's row loaded once for the 8, sixteen loads in flight;
+            // each sum in k order
+            const int nrb = (int)((nrhs + 7) / 8);
+            for (int e = tid; e < (o1 - o0) * nrb; e += blockDim.x) {
+                const int row = o0 + e % (o1 - o0), rb0 = 8 * (e / (o1 - o0));
+                const int rb = nrhs - rb0 < 8 ? (int)(nrhs - rb0) : 8;
                 const T *Lr = L + row + (int64_t)r0 * ld;
-                const T *xr = x + r * np + r0;
-                T acc = VT<T>::zero();
-                for (int k0 = 0; k0 < w; k0 += 16) {         // sixteen loads of L in flight, the sum in k order
+                T acc[8];
+#pragma unroll
+                for (int r = 0; r < 8; r++) acc[r] = VT<T>::zero();
+                for (int k0 = 0; k0 < w; k0 += 16) {
                     T lv[16];
 #pragma unroll
                     for (int q = 0; q < 16; q++) lv[q] = k0 + q < w ? Lr[(int64_t)(k0 + q) * ld] : VT<T>::zero();
 #pragma unroll
                     for (int q = 0; q < 16; q++)
-                        if (k0 + q < w) acc = add(acc, mul(lv[q], xr[k0 + q]));
+                        if (k0 + q < w)
+#pragma unroll
+                            for (int r = 0; r < 8; r++)
+                                if (r < rb) acc[r] = add(acc[r], mul(lv[q], x[(int64_t)(rb0 + r) * np + r0 + k0 + q]));
                 }
-                x[r * np + row] = sub(x[r * np + row], acc);
+#pragma unroll
+                for (int r = 0; r < 8; r++)
+                    if (r < rb) x[(int64_t)(rb0 + r) * np + row] = sub(x[(int64_t)(rb0 + r) * np + row], acc[r]);
             }
+        }
         __syncthreads();
     }
 }
@@ -2941,6 +2951,7 @@ __global__ void k_vupdate(const T *__restrict__ V, int64_t n, int nv, const T *_
 // the children's order, the children's contribution entries that land on it (the lists rsp/rsi over the plan's rows,
 // csp/csi over its columns).
 constexpr int SV_RC = 8;              // right-hand sides per pass of the one-CTA sweep kernels
+constexpr int SVB_RC = 16;            // right-hand sides per pass over a larger front's L21 or U12
 constexpr int SV_THREADS = 256;
 
 // L sweep (trans 0) of a level's small fronts, a CTA each: the front's vector in its final row order (position k holds
@@ -3272,7 +3283,8 @@ __global__ void __launch_bounds__(256) k_svb_L11(const SvFront *__restrict__ fr,
     if (np == 0) return;
     T *x = reinterpret_cast<T *>(smem_raw);          // np x rcb
     T *sT = x + (int64_t)np * rcb;                   // 64 x 64
-    for (int r0 = 0; r0 < nrhs; r0 += rcb) {
+    // blockIdx.y: the group of right-hand sides [y * rcb, y * rcb + rcb) (the groups are independent)
+    for (int r0 = blockIdx.y * rcb; r0 < nrhs && r0 < (int)(blockIdx.y + 1) * rcb; r0 += rcb) {
         const int rc = nrhs - r0 < rcb ? nrhs - r0 : rcb;
         for (int e = tid; e < np * rc; e += blockDim.x) x[e] = VB[F.row_off + e % np + (int64_t)(r0 + e / np) * vstride];
         __syncthreads();
@@ -3305,9 +3317,9 @@ __global__ void __launch_bounds__(256) k_svb_L21(const SvFront *__restrict__ fr,
         for (int e = tid; e < np * rc; e += blockDim.x) xs[e] = VB[F.row_off + e % np + (int64_t)(r0 + e / np) * vstride];
         __syncthreads();
         if (rr < F.nr) {
-            T acc[SV_RC];
+            T acc[SVB_RC];
 #pragma unroll
-            for (int r = 0; r < SV_RC; r++) acc[r] = VT<T>::zero();
+            for (int r = 0; r < SVB_RC; r++) acc[r] = VT<T>::zero();
             for (int k0 = 0; k0 < np; k0 += 8) {
                 T lv[8];
 #pragma unroll
@@ -3316,11 +3328,11 @@ __global__ void __launch_bounds__(256) k_svb_L21(const SvFront *__restrict__ fr,
                 for (int q = 0; q < 8; q++)
                     if (k0 + q < np)
 #pragma unroll
-                        for (int r = 0; r < SV_RC; r++)
+                        for (int r = 0; r < SVB_RC; r++)
                             if (r < rc) acc[r] = add(acc[r], mul(lv[q], xs[k0 + q + r * np]));
             }
 #pragma unroll
-            for (int r = 0; r < SV_RC; r++)
+            for (int r = 0; r < SVB_RC; r++)
                 if (r < rc) {
                     T *o = VB + F.row_off + rr + (int64_t)(r0 + r) * vstride;
                     *o = sub(*o, acc[r]);
@@ -3331,53 +3343,83 @@ __global__ void __launch_bounds__(256) k_svb_L21(const SvFront *__restrict__ fr,
 }
 
 // U sweep, 1: the partial products U12 x[CB columns] of chunk blockIdx.x of a front's CB columns (F.nch chunks), a
-// thread per row of U12, into part (the front's partial sums start at F.poff * nrhs)
+// thread per row of U12, into part (the front's partial sums start at F.poff * nrhs); the chunk's x values staged in
+// shared memory, SVB_RC right-hand sides per pass over U12
 template <typename T>
 __global__ void __launch_bounds__(256) k_svb_u12(const SvFront *__restrict__ fr, const int *__restrict__ list,
                                                  const T *__restrict__ Ua, const int64_t *__restrict__ cols,
                                                  const T *__restrict__ X, int64_t n, int nrhs, T *__restrict__ part)
 {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *Xs = reinterpret_cast<T *>(smem_raw);         // chunk x SVB_RC: Xs[k * SVB_RC + r]
     const SvFront F = fr[list[blockIdx.y]];
     if (blockIdx.x >= F.nch || F.np == 0) return;
     const int64_t np = F.np, ncb = F.nc - F.np, chunk = (ncb + F.nch - 1) / F.nch;
     const int64_t c0 = blockIdx.x * chunk, c1 = c0 + chunk < ncb ? c0 + chunk : ncb;
+    const int cc = (int)(c1 - c0);
     const T *U12 = Ua + F.U_off;
     const int64_t *cb = cols + F.col_off + np;
     T *pp = part + F.poff * nrhs + (int64_t)blockIdx.x * np * nrhs;
-    for (int r0 = 0; r0 < nrhs; r0 += SV_RC) {
-        const int rc = nrhs - r0 < SV_RC ? nrhs - r0 : SV_RC;
+    for (int r0 = 0; r0 < nrhs; r0 += SVB_RC) {
+        const int rc = nrhs - r0 < SVB_RC ? nrhs - r0 : SVB_RC;
+        for (int e = threadIdx.x; e < cc * rc; e += blockDim.x) {
+            const int k = e / rc, r = e - k * rc;
+            Xs[k * SVB_RC + r] = X[cb[c0 + k] + (int64_t)(r0 + r) * n];
+        }
+        __syncthreads();
         for (int64_t i = threadIdx.x; i < np; i += blockDim.x) {
-            T acc[SV_RC];
+            T acc[SVB_RC];
 #pragma unroll
-            for (int r = 0; r < SV_RC; r++) acc[r] = VT<T>::zero();
-            for (int64_t k0 = c0; k0 < c1; k0 += 8) {
+            for (int r = 0; r < SVB_RC; r++) acc[r] = VT<T>::zero();
+            for (int k0 = 0; k0 < cc; k0 += 8) {
                 T uv[8];
-                int64_t cc[8];
 #pragma unroll
-                for (int q = 0; q < 8; q++) {
-                    const bool ok = k0 + q < c1;
-                    uv[q] = ok ? U12[i + (k0 + q) * np] : VT<T>::zero();
-                    cc[q] = ok ? cb[k0 + q] : 0;
-                }
+                for (int q = 0; q < 8; q++) uv[q] = k0 + q < cc ? U12[i + (c0 + k0 + q) * np] : VT<T>::zero();
 #pragma unroll
                 for (int q = 0; q < 8; q++)
-                    if (k0 + q < c1)
+                    if (k0 + q < cc)
 #pragma unroll
-                        for (int r = 0; r < SV_RC; r++)
-                            if (r < rc) acc[r] = add(acc[r], mul(uv[q], X[cc[q] + (int64_t)(r0 + r) * n]));
+                        for (int r = 0; r < SVB_RC; r++)
+                            if (r < rc) acc[r] = add(acc[r], mul(uv[q], Xs[(k0 + q) * SVB_RC + r]));
             }
 #pragma unroll
-            for (int r = 0; r < SV_RC; r++)
+            for (int r = 0; r < SVB_RC; r++)
                 if (r < rc) pp[i + (int64_t)(r0 + r) * np] = acc[r];
         }
+        __syncthreads();
     }
 }
 
-// U sweep, 2: x = U11^-1 (y - the partial products, in chunk order), a CTA per front, rcb right-hand sides per pass
+// U sweep, 2: y - the partial products (in chunk order) for every front of the level, over many CTAs, into the front's
+// first partial sum
+template <typename T>
+__global__ void k_svb_psum(const SvFront *__restrict__ fr, const int *__restrict__ list, T *__restrict__ part,
+                           const T *__restrict__ Y, int64_t n, int nrhs)
+{
+    const SvFront F = fr[list[blockIdx.y]];
+    if (F.np == 0 || F.nch == 0) return;              // (no partial sums: k_svb_bwdU reads y itself)
+    const int64_t np = F.np, E = np * nrhs;
+    T *pp = part + F.poff * nrhs;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+        T v = Y[F.f + e % np + (e / np) * n];
+        for (int64_t q0 = 0; q0 < F.nch; q0 += 8) {          // eight loads in flight
+            T pv[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) pv[q] = q0 + q < F.nch ? pp[(q0 + q) * E + e] : VT<T>::zero();
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (q0 + q < F.nch) v = sub(v, pv[q]);
+        }
+        pp[e] = v;
+    }
+}
+
+// U sweep, 3: x = U11^-1 (y - the partial products, in chunk order), a CTA per front, rcb right-hand sides per pass
+// (presummed: k_svb_psum left y - the products in the front's first partial sum)
 template <typename T>
 __global__ void __launch_bounds__(256) k_svb_bwdU(const SvFront *__restrict__ fr, const int *__restrict__ list,
                                                   const T *__restrict__ La, const T *__restrict__ part, const T *__restrict__ Y,
-                                                  T *__restrict__ X, int64_t n, int nrhs, int rcb, DevStatus *st)
+                                                  T *__restrict__ X, int64_t n, int nrhs, int rcb, DevStatus *st, int presummed)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_zero;
@@ -3388,13 +3430,25 @@ __global__ void __launch_bounds__(256) k_svb_bwdU(const SvFront *__restrict__ fr
     T *sT = x + (int64_t)np * rcb;                   // 64 x 64
     T *dinv = sT + 64 * 64;                          // 64
     const T *pp = part + F.poff * nrhs;
-    for (int r0 = 0; r0 < nrhs; r0 += rcb) {
+    // blockIdx.y: the group of right-hand sides [y * rcb, y * rcb + rcb) (the groups are independent)
+    for (int r0 = blockIdx.y * rcb; r0 < nrhs && r0 < (int)(blockIdx.y + 1) * rcb; r0 += rcb) {
         const int rc = nrhs - r0 < rcb ? nrhs - r0 : rcb;
         for (int e = tid; e < np * rc; e += blockDim.x) {
             const int i = e % np;
             const int64_t r = r0 + e / np;
-            T v = Y[F.f + i + r * n];
-            for (int64_t q = 0; q < F.nch; q++) v = sub(v, pp[q * np * nrhs + i + r * np]);
+            T v;
+            if (presummed && F.nch > 0) v = pp[i + r * np];
+            else {
+                v = Y[F.f + i + r * n];
+                for (int64_t q0 = 0; q0 < F.nch; q0 += 8) {      // eight loads in flight, the sum in chunk order
+                    T pv[8];
+#pragma unroll
+                    for (int q = 0; q < 8; q++) pv[q] = q0 + q < F.nch ? pp[(q0 + q) * np * nrhs + i + r * np] : VT<T>::zero();
+#pragma unroll
+                    for (int q = 0; q < 8; q++)
+                        if (q0 + q < F.nch) v = sub(v, pv[q]);
+                }
+            }
             x[e] = v;
         }
         if (tid == 0) s_zero = 0;

@@ -143,7 +143,7 @@ static int upload_solve_levels(const FrontPlan &P, DevPlan &D, char *err, size_t
     std::vector<int> brows_list, bcols_list;
     D.sv_brows_ptr.assign(1, 0); D.sv_bcols_ptr.assign(1, 0);
     D.brows_maxnr.assign((size_t)nlev, 0); D.brows_maxnp.assign((size_t)nlev, 0); D.brows_maxm.assign((size_t)nlev, 0);
-    D.bcols_maxnp.assign((size_t)nlev, 0); D.bcols_maxnch.assign((size_t)nlev, 0);
+    D.bcols_maxnp.assign((size_t)nlev, 0); D.bcols_maxnch.assign((size_t)nlev, 0); D.bcols_maxchunk.assign((size_t)nlev, 0);
     D.part_need = 1;
     for (int64_t L = 0; L < nlev; L++) {
         for (int64_t fi : D.big_rows[(size_t)L]) {
@@ -168,6 +168,7 @@ static int upload_solve_levels(const FrontPlan &P, DevPlan &D, char *err, size_t
             bcols_list.push_back((int)fi);
             D.bcols_maxnp[(size_t)L] = std::max(D.bcols_maxnp[(size_t)L], F.npiv);
             D.bcols_maxnch[(size_t)L] = std::max(D.bcols_maxnch[(size_t)L], nch);
+            if (nch > 0) D.bcols_maxchunk[(size_t)L] = std::max(D.bcols_maxchunk[(size_t)L], (ncb + nch - 1) / nch);
         }
         D.part_need = std::max(D.part_need, poff);
         D.sv_brows_ptr.push_back((int64_t)brows_list.size());
@@ -175,6 +176,7 @@ static int upload_solve_levels(const FrontPlan &P, DevPlan &D, char *err, size_t
     }
     if (brows_list.empty()) brows_list.push_back(0);
     if (bcols_list.empty()) bcols_list.push_back(0);
+    D.sv_brows_host.assign(brows_list.begin(), brows_list.end());
     std::vector<int> rows_list, cols_list;
     D.sv_rows_ptr.assign(1, 0); D.sv_cols_ptr.assign(1, 0);
     for (int64_t L = 0; L < nlev; L++) {
@@ -882,6 +884,16 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         direct[(size_t)fi] = 1;
         any_direct = true;
     }
+    // the second working block only where it fits a quarter of the free device memory (a pattern whose largest front is
+    // a sizable share of HBM keeps the contribution blocks on the stack)
+    if (any_direct && N.cap_work2 < (size_t)P.work_size * vs) {
+        size_t fr = 0, tot = 0;
+        if (N.capture || cudaMemGetInfo(&fr, &tot) != cudaSuccess || (size_t)P.work_size * vs > fr / 4) {
+            (void)cudaGetLastError();
+            std::fill(direct.begin(), direct.end(), 0);
+            any_direct = false;
+        }
+    }
     if (any_direct && (rc = ensure_async(N, (void **)&N.work2, &N.cap_work2, (size_t)P.work_size * vs, err, errlen))) return rc;
     T *next_W = nullptr;                 // the working block a direct child has written into, for the next front
 
@@ -1122,6 +1134,7 @@ static int run_solve_block(const FrontPlan &P, const DevPlan &D, DevNum &N, T *x
             CK(cudaFuncSetAttribute(k_svb_L11<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
             CK(cudaFuncSetAttribute(k_svb_L21<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
             CK(cudaFuncSetAttribute(k_svb_bwdU<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+            CK(cudaFuncSetAttribute(k_svb_u12<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
             sv_attr = true;
         }
     }
@@ -1177,12 +1190,23 @@ static int run_solve_block(const FrontPlan &P, const DevPlan &D, DevNum &N, T *x
                 k_svb_gatherL<T><<<dim3(gx, nb), 256, 0, s>>>(D.sv, bl, D.rowinit, N.permall, D.rsp, D.rsi, R, VB, D.vrow, n,
                                                               nrhs), note_launch();
                 if (mnp > 0) {
-                    const int rcb = (int)std::max<int64_t>(1, std::min<int64_t>(nrhs, (int64_t)((SMEM_MAX - 64 * 64 * sizeof(T)) /
-                                                                                                 ((size_t)mnp * sizeof(T)))));
-                    k_svb_L11<T><<<nb, 256, ((size_t)mnp * rcb + 64 * 64) * sizeof(T), s>>>(D.sv, bl, La, VB, D.vrow, S2, n,
-                                                                                              (int)nrhs, rcb), note_launch();
-                    if (mm > 0) {
-                        const int rc2 = (int)std::max<int64_t>(1, std::min<int64_t>(SV_RC, (int64_t)(SMEM_MAX / ((size_t)mnp * sizeof(T)))));
+                    // the L11 solves: at most 8 right-hand sides per CTA (the groups in parallel)
+                    const int rcb = (int)std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(nrhs, 8),
+                        (int64_t)((SMEM_MAX - 64 * 64 * sizeof(T)) / ((size_t)mnp * sizeof(T)))));
+                    k_svb_L11<T><<<dim3(nb, (unsigned)((nrhs + rcb - 1) / rcb)), 256, ((size_t)mnp * rcb + 64 * 64) * sizeof(T), s>>>(
+                        D.sv, bl, La, VB, D.vrow, S2, n, (int)nrhs, rcb), note_launch();
+                    if (mm > 0 && nrhs >= 8 && nb == 1) {
+                        // one front and several right-hand sides: u = v[np:] - L21 x as an FP64 tensor-core GEMM, in place
+                        const Front &F1 = P.fronts[(size_t)D.sv_brows_host[(size_t)b0]];
+                        const int64_t np1 = std::min(F1.npiv, F1.nrows), M1 = F1.nrows - np1;
+                        if (M1 > 0) {
+                            T *C = VB + F1.row_off + np1;
+                            dim3 g((unsigned)((M1 + GBM - 1) / GBM), (unsigned)((nrhs + GBN - 1) / GBN));
+                            k_gemm_sub<T><<<g, 256, 0, s>>>(M1, nrhs, np1, La + F1.L_off + np1, F1.nrows, VB + F1.row_off, D.vrow, C,
+                                                            D.vrow, nullptr, C, D.vrow, N.st, OutMap{}), note_launch();
+                        }
+                    } else if (mm > 0) {
+                        const int rc2 = (int)std::max<int64_t>(1, std::min<int64_t>(SVB_RC, (int64_t)(SMEM_MAX / ((size_t)mnp * sizeof(T)))));
                         k_svb_L21<T><<<dim3((unsigned)((mm + 255) / 256), nb), 256, (size_t)mnp * rc2 * sizeof(T), s>>>(
                             D.sv, bl, La, VB, D.vrow, (int)nrhs, rc2), note_launch();
                     }
@@ -1268,12 +1292,22 @@ static int run_solve_block(const FrontPlan &P, const DevPlan &D, DevNum &N, T *x
                 const unsigned nb = (unsigned)(b1 - b0);
                 const int *bl = D.sv_bcols + b0;
                 const int64_t mnp = D.bcols_maxnp[(size_t)lv], mch = D.bcols_maxnch[(size_t)lv];
-                if (mch > 0)
-                    k_svb_u12<T><<<dim3((unsigned)mch, nb), 256, 0, s>>>(D.sv, bl, Ua, D.cols, R, n, (int)nrhs, part), note_launch();
-                const int rcb = (int)std::max<int64_t>(1, std::min<int64_t>(nrhs, (int64_t)((SMEM_MAX - (64 * 64 + 64) * sizeof(T)) /
-                                                                                             ((size_t)mnp * sizeof(T)))));
-                k_svb_bwdU<T><<<nb, 256, ((size_t)mnp * rcb + 64 * 64 + 64) * sizeof(T), s>>>(D.sv, bl, La, part, S2, R, n,
-                                                                                               (int)nrhs, rcb, N.st), note_launch();
+                if (mch > 0) {
+                    const size_t xsm = (size_t)D.bcols_maxchunk[(size_t)lv] * SVB_RC * sizeof(T);
+                    k_svb_u12<T><<<dim3((unsigned)mch, nb), 256, xsm, s>>>(D.sv, bl, Ua, D.cols, R, n, (int)nrhs, part), note_launch();
+                    // the partial sums over many CTAs when a front's right-hand sides are more than its CTA's threads
+                    if (mnp * nrhs > 256) {
+                        const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((mnp * nrhs + 255) / 256, 148));
+                        k_svb_psum<T><<<dim3(gx, nb), 256, 0, s>>>(D.sv, bl, part, S2, n, (int)nrhs), note_launch();
+                    }
+                }
+                const int rcb = (int)std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(nrhs, 8),
+                    (int64_t)((SMEM_MAX - (64 * 64 + 64) * sizeof(T)) / ((size_t)mnp * sizeof(T)))));
+                k_svb_bwdU<T><<<dim3(nb, (unsigned)((nrhs + rcb - 1) / rcb)), 256, ((size_t)mnp * rcb + 64 * 64 + 64) * sizeof(T), s>>>(
+                    D.sv, bl, La, part, S2, R, n,
+                                                                                               (int)nrhs, rcb, N.st,
+                                                                                               mch > 0 && mnp * nrhs > 256 ? 1 : 0),
+                    note_launch();
             }
         }
         // x[col_perm[k]] = Dcp[k] * R[k]  (raw: x[k] = R[k])

@@ -47,8 +47,9 @@ struct DevPlan {
     // the trans-0 sweeps' larger fronts as device lists by level (brows: the L sweep; bcols: the U sweep below the dense
     // chain), with host ranges and the level's largest sizes; the partial sums a level's U sweep needs (per right-hand side)
     int *sv_brows = nullptr, *sv_bcols = nullptr;
+    std::vector<int> sv_brows_host;
     std::vector<int64_t> sv_brows_ptr, sv_bcols_ptr;
-    std::vector<int64_t> brows_maxnr, brows_maxnp, brows_maxm, bcols_maxnp, bcols_maxnch;
+    std::vector<int64_t> brows_maxnr, brows_maxnp, brows_maxm, bcols_maxnp, bcols_maxnch, bcols_maxchunk;
     int64_t part_need = 0;
     // the batched fronts of the factorization: every interior front whose whole subtree fits the one-CTA pivot-block LU
     // and the fused tail (at most 128 rows and 64 pivots).  They run first, level by level, three launches per level
