@@ -191,25 +191,46 @@ def allreduce_max(value: float, device) -> float:
 
 # ------------------------------------------------------------------------------------------------------------- arms
 def run_profile_once(args):
-    """One factor + solve inside a profiler range (after a warm factorization that caches the plan), then the per-class
-    algorithmic flops and bytes of that factorization (the library's own counts) as one JSON line."""
+    """One factorization and solve inside a profiler range (after a warm factorization and solve that size every buffer),
+    then the per-class algorithmic flops and bytes of that factorization (the library's own counts) as one JSON line.
+    --profile-workload: the benchmark workload (--workload), the 3D stencil (stencil3d, --precision-grid), or the
+    17-decade random configuration (random, --random-n); --profile-part solve puts only the solve, with --profile-nrhs
+    right-hand sides, in the range; --profile-precision the Schur-update arithmetic (FPLUS_B200_PREC_*)."""
     import torch
     import fplus_b200 as F
+    from fplus_b200 import workloads as W
     torch.cuda.init()
-    n, Ap, Ai, Ax, b, desc = workload(args.workload, args.modes)
+    if args.profile_workload == "stencil3d":
+        n, Ap, Ai, Ax = W.convdiff3d(args.precision_grid, 3)
+        desc = {"workload": f"3D convection-diffusion 7-point, {args.precision_grid}^3 grid (n={n}), float64"}
+    elif args.profile_workload == "random":
+        n, Ap, Ai, Ax = W.random_scaled(n=args.random_n)
+        desc = {"workload": f"random complex base, scales over 17 decades (n={n})"}
+    else:
+        n, Ap, Ai, Ax, _, desc = workload(args.workload, args.modes)
+    nrhs = args.profile_nrhs
+    B = torch.from_numpy(W.rhs(n, nrhs, np.iscomplexobj(Ax), 2)).cuda()
+    Ad = torch.from_numpy(np.ascontiguousarray(Ax)).cuda()
     S = F.analyze(n, Ap, Ai)
-    N = S.factor(Ax)
-    N.solve(b)
+    N = S.factor(Ad, device=True, precision=args.profile_precision)
+    N.solve_device(B.clone(), 0)
     del N
     torch.cuda.synchronize()
     F.profile(True)
-    torch.cuda.cudart().cudaProfilerStart()
-    N = S.factor(Ax)
-    N.solve(b)
+    solve_only = args.profile_part == "solve"
+    if not solve_only:
+        torch.cuda.cudart().cudaProfilerStart()
+    N = S.factor(Ad, device=True, precision=args.profile_precision)
+    Bc = B.clone()
+    torch.cuda.synchronize()
+    if solve_only:
+        torch.cuda.cudart().cudaProfilerStart()
+    N.solve_device(Bc, 0)
     torch.cuda.synchronize()
     torch.cuda.cudart().cudaProfilerStop()
     prof = {F.PROFILE_CLASSES[c]: F.profile_read(c) for c in F.PROFILE_CLASSES}
     F.profile(False)
+    desc.update({"n": n, "nrhs": nrhs, "part": args.profile_part, "precision": args.profile_precision})
     print(json.dumps({"profile_once": desc, "classes": prof}))
 
 
@@ -287,6 +308,56 @@ def run_precision_form(stream, dev, g=80, reps=2):
         v["speedup_vs_fp64"] = base / v["total_ms"] if v["berr"] <= 1e-14 else None
     ok = [v["total_ms"] for k, v in out["forms"].items() if k != "fp64" and v["berr"] <= 1e-14]
     out["best_mixed_speedup_vs_plain"] = base / min(ok) if ok else None
+    return out
+
+
+def run_random_form(stream, dev, n=40000, nrhs=256, reps=1):
+    """C5, the ill-conditioned stress configuration, at n = `n`: the seeded well-conditioned random complex base (12
+    entries per column) scaled by row and column factors over 17 decades, Ruiz on, `nrhs` right-hand sides solved
+    together.  The plain form (FP64 Schur updates) against the FP32 form (split TF32x3 on the tensor cores) with FP64
+    refinement (classic, GMRES-IR where it stalls) to a componentwise backward error of 1e-14 for every right-hand side.
+    Device time of the factorization (values in HBM) and of the refined solve (host right-hand sides in, solutions out),
+    CUDA events on the library's stream, median of `reps` after one warm-up.  The specified n = 300,000 does not fit:
+    the static front structure of this random pattern holds about 0.85 n^2 entries."""
+    import torch
+    import fplus_b200 as F
+    import oracle as O
+    from fplus_b200 import workloads as W
+    nn, Ap, Ai, Ax = W.random_scaled(n=n)
+    S = F.analyze(nn, Ap, Ai)
+    B = W.rhs(nn, nrhs, True, 5).T.copy(order="F")
+    Ad = torch.from_numpy(Ax).to(dev)
+    out = {"workload": f"random complex base, 12 entries per column, row / column scales over 17 decades (n={nn}, "
+                       f"{int(Ap[-1])} entries), {nrhs} right-hand sides", "forms": {}}
+    X64 = None
+    for prec, name in ((F.PREC_FP64, "fp64"), (F.PREC_FP32, "fp32_split_tf32x3")):
+        fms, sms = [], []
+        for r in range(reps + 1):
+            torch.cuda.synchronize()
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            N = S.factor(Ad, device=True, precision=prec)
+            e1.record(stream)
+            X, berr, it = N.solve_refine(B, 0, max_iter=40, tol=1e-14)
+            e2.record(stream)
+            e2.synchronize()
+            if r > 0:
+                fms.append(e0.elapsed_time(e1)); sms.append(e1.elapsed_time(e2))
+            info = N.info
+            del N
+        be = max(O.backward_error(nn, Ap, Ai, Ax, X[:, c], B[:, c]) for c in (0, nrhs // 2, nrhs - 1))
+        if prec == F.PREC_FP64:
+            X64 = X.copy()
+        f_ms, s_ms = float(np.median(fms)), float(np.median(sms))
+        out["forms"][name] = {"factor_ms": f_ms, "refined_solve_ms": s_ms, "total_ms": f_ms + s_ms,
+                              "corrections_max": int(it.max()), "berr_componentwise_max": float(berr.max()),
+                              "berr_normwise_sampled": be,
+                              "forward_diff_vs_fp64": float(np.linalg.norm(X - X64) / np.linalg.norm(X64)),
+                              "tc_flop_share": float(info["tc_flops"] / max(info["front_flops"], 1.0)),
+                              "device_GB": round(info["device_bytes"] / 1e9, 2)}
+    f = out["forms"]
+    ok = f["fp32_split_tf32x3"]["berr_componentwise_max"] <= 1e-14
+    out["speedup_fp32_vs_fp64"] = f["fp64"]["total_ms"] / f["fp32_split_tf32x3"]["total_ms"] if ok else None
     return out
 
 
@@ -673,6 +744,9 @@ def run_b200_arm(args, rank, world):
     precision = None
     if world == 1 and args.precision_grid > 0:
         precision = run_precision_form(stream, dev, args.precision_grid)
+    random_form = None
+    if world == 1 and args.random_n > 0:
+        random_form = run_random_form(stream, dev, args.random_n)
 
     if rank != 0:
         return
@@ -705,7 +779,7 @@ def run_b200_arm(args, rank, world):
                     "d2h_bytes_per_step": n * vsz},
             "gpu_launches": int(launches),
             "clocks": clocks, "roofline": roof, "cpu_baseline": cpu, "solve_nrhs16": solve16, "batch": batch,
-            "batch_pencils": batch_pencils, "c1_pair": c1_pair, "precision_form": precision}
+            "batch_pencils": batch_pencils, "c1_pair": c1_pair, "precision_form": precision, "random_form": random_form}
     print(json.dumps(line))
 
 
@@ -722,9 +796,15 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default front shape (no fplus_b200_autotune)")
     ap.add_argument("--precision-grid", type=int, default=80,
                     help="grid of the 3D stencil of the precision-form measurement (80: n = 512,000; 0: none)")
+    ap.add_argument("--random-n", type=int, default=40000,
+                    help="n of the 17-decade random configuration with 256 right-hand sides (0: none)")
     ap.add_argument("--batch", type=int, default=64, help="shifts of the pencil in the batch measurement (0: none)")
     ap.add_argument("--batch-pencils", type=int, default=512,
                     help="independent uneven pencils in the second batch measurement (0: none)")
+    ap.add_argument("--profile-workload", default="bench", choices=["bench", "stencil3d", "random"])
+    ap.add_argument("--profile-part", default="all", choices=["all", "solve"])
+    ap.add_argument("--profile-nrhs", type=int, default=1)
+    ap.add_argument("--profile-precision", type=int, default=0)
     ap.add_argument("--profile-once", action="store_true",
                     help="for ncu --profile-from-start off: one warm factorization, then exactly one factor + solve "
                          "between cudaProfilerStart / Stop; prints that factorization's algorithmic work per class")
