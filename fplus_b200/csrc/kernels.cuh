@@ -1672,28 +1672,50 @@ template <typename T, int RPL>
 __global__ void __launch_bounds__(256) k_trsm_warp(T *__restrict__ X, int64_t ldx, int w, int64_t ncols,
                                                    const T *__restrict__ Lb, int64_t ldl, const DevStatus *st)
 {
+    constexpr int CPW = 4;                            // columns per warp at once (independent chains through one loop)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *sL = reinterpret_cast<T *>(smem_raw);          // w x w, column-major, ld w
     if (st->code) return;
-    for (int e = threadIdx.x; e < w * w; e += blockDim.x) sL[e] = Lb[(e % w) + (int64_t)(e / w) * ldl];
+    for (int e0 = threadIdx.x; e0 < w * w; e0 += 8 * blockDim.x) {       // eight loads in flight per thread
+        T v[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) { const int e = e0 + q * blockDim.x; v[q] = e < w * w ? Lb[(e % w) + (int64_t)(e / w) * ldl] : VT<T>::zero(); }
+#pragma unroll
+        for (int q = 0; q < 8; q++) { const int e = e0 + q * blockDim.x; if (e < w * w) sL[e] = v[q]; }
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5, nwarp = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t c = wid; c < ncols; c += nwarp) {
-        T *col = X + c * ldx;
-        T x[RPL];
+    for (int64_t c0 = wid * CPW; c0 < ncols; c0 += nwarp * CPW) {
+        T x[CPW][RPL];
 #pragma unroll
-        for (int q = 0; q < RPL; q++) { const int r = lane + 32 * q; x[q] = r < w ? col[r] : VT<T>::zero(); }
-        for (int i = 0; i < w; i++) {
-            const T xi = shfl_v<T>(x[i >> 5], i & 31);
+        for (int j = 0; j < CPW; j++)
 #pragma unroll
             for (int q = 0; q < RPL; q++) {
                 const int r = lane + 32 * q;
-                if (r > i && r < w) x[q] = sub(x[q], mul(sL[r + i * w], xi));
+                x[j][q] = (r < w && c0 + j < ncols) ? X[r + (c0 + j) * ldx] : VT<T>::zero();
+            }
+        for (int i = 0; i < w; i++) {
+            T xi[CPW];
+#pragma unroll
+            for (int j = 0; j < CPW; j++) xi[j] = shfl_v<T>(RPL > 1 && i >= 32 ? x[j][RPL > 1 ? 1 : 0] : x[j][0], i & 31);
+#pragma unroll
+            for (int q = 0; q < RPL; q++) {
+                const int r = lane + 32 * q;
+                if (r > i && r < w) {
+                    const T l = sL[r + i * w];
+#pragma unroll
+                    for (int j = 0; j < CPW; j++) x[j][q] = sub(x[j][q], mul(l, xi[j]));
+                }
             }
         }
 #pragma unroll
-        for (int q = 0; q < RPL; q++) { const int r = lane + 32 * q; if (r < w) col[r] = x[q]; }
+        for (int j = 0; j < CPW; j++)
+#pragma unroll
+            for (int q = 0; q < RPL; q++) {
+                const int r = lane + 32 * q;
+                if (r < w && c0 + j < ncols) X[r + (c0 + j) * ldx] = x[j][q];
+            }
     }
 }
 

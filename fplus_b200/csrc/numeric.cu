@@ -888,7 +888,8 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     // a sizable share of HBM keeps the contribution blocks on the stack)
     if (any_direct && N.cap_work2 < (size_t)P.work_size * vs) {
         size_t fr = 0, tot = 0;
-        if (N.capture || cudaMemGetInfo(&fr, &tot) != cudaSuccess || (size_t)P.work_size * vs > fr / 4) {
+        const bool big = (size_t)P.work_size * vs > ((size_t)1 << 30);        // (small blocks: no device query)
+        if (N.capture || (big && (cudaMemGetInfo(&fr, &tot) != cudaSuccess || (size_t)P.work_size * vs > fr / 4))) {
             (void)cudaGetLastError();
             std::fill(direct.begin(), direct.end(), 0);
             any_direct = false;
@@ -973,7 +974,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         for (int64_t k0 = 0; k0 < npr; k0 += TB) {
             const int w = (int)std::min<int64_t>(TB, npr - k0);
             const size_t tsm = (size_t)w * w * vs;
-            const int nwarps = (int)std::min<int64_t>(ncb, 148 * 64);
+            const int nwarps = (int)std::min<int64_t>((ncb + 3) / 4, 148 * 32);     // four columns per warp at once
             const int blocks = (nwarps + 7) / 8;
             if (w <= 32) k_trsm_warp<T, 1><<<blocks, 256, tsm, s>>>(Uf + k0, np, w, ncb, Lf + k0 + k0 * ld, ld, N.st), note_launch();
             else k_trsm_warp<T, 2><<<blocks, 256, tsm, s>>>(Uf + k0, np, w, ncb, Lf + k0 + k0 * ld, ld, N.st), note_launch();
