@@ -380,6 +380,7 @@ __global__ void __launch_bounds__(MC_THREADS) k_block_lu_mc(T *W, int64_t ld, in
     __shared__ long long s_k[16], s_r[16], s_p[16];
     __shared__ int s_q[16];
     __shared__ int s_piv[MC_PW];
+    __shared__ T s_wc[16 * MC_PW];                      // cluster form: each warp's candidate row, fully updated
     __shared__ double s_thr[MC_PW];
     __shared__ int s_stop, s_wait;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = MC_THREADS / 32;
@@ -420,6 +421,17 @@ __global__ void __launch_bounds__(MC_THREADS) k_block_lu_mc(T *W, int64_t ld, in
                 brid = src >= 0 ? __shfl_sync(0xffffffffu, brid, src) : LLONG_MAX;
                 brow = src >= 0 ? __shfl_sync(0xffffffffu, brow, src) : -1;
             }
+            if constexpr (CL) {
+                // the warp's candidate row in full: its later columns still lack the previous pivot's update (applied
+                // to every row during the cluster barrier below), so it is applied here, with the same arithmetic
+                __syncwarp();
+                if (lane < w) {
+                    T v = brow >= 0 ? S[lane * per + brow] : VT<T>::zero();
+                    if (brow >= 0 && kk >= 1 && lane > kk)
+                        v = sub(v, mul(S[(kk - 1) * per + brow], Lb[(kk - 1) * MC_LB + lane]));
+                    s_wc[warp * MC_PW + lane] = v;
+                }
+            }
             if (lane == 0) { s_k[warp] = bk; s_r[warp] = brid; s_p[warp] = brow; }
             __syncthreads();
             if (CL ? warp < G : warp == 0) {
@@ -429,7 +441,7 @@ __global__ void __launch_bounds__(MC_THREADS) k_block_lu_mc(T *W, int64_t ld, in
                 bk = src >= 0 ? __shfl_sync(0xffffffffu, bk, src) : -1;
                 brid = src >= 0 ? __shfl_sync(0xffffffffu, brid, src) : LLONG_MAX;
                 brow = src >= 0 ? __shfl_sync(0xffffffffu, brow, src) : -1;
-                const T v = (lane < w && brow >= 0) ? S[lane * per + brow] : VT<T>::zero();
+                const T v = (lane < w && brow >= 0) ? (CL ? s_wc[src * MC_PW + lane] : S[lane * per + brow]) : VT<T>::zero();
                 const long long pos = brow >= 0 ? r_lo + brow : -1;
                 if constexpr (CL) {
                     McSlot<T> *dst = cg::this_cluster().map_shared_rank(cs + par * MC_CMAX + b, warp);
@@ -454,7 +466,13 @@ __global__ void __launch_bounds__(MC_THREADS) k_block_lu_mc(T *W, int64_t ld, in
             int gq = -1;
             const T *wv;                                 // the winner's panel values
             if constexpr (CL) {
-                cg::this_cluster().sync();
+                asm volatile("barrier.cluster.arrive.release;" ::: "memory");
+                // while the other CTAs arrive: the previous pivot's update of this row's later columns
+                if (mine && kk >= 1) {
+                    const T l = S[(kk - 1) * per + tid];
+                    for (int c = kk + 1; c < w; c++) S[c * per + tid] = sub(S[c * per + tid], mul(l, Lb[(kk - 1) * MC_LB + c]));
+                }
+                asm volatile("barrier.cluster.wait.acquire;" ::: "memory");
                 if (lane < G) {
                     const McSlot<T> *c = cs + par * MC_CMAX + lane;
                     gk = c->key; gr = c->rid; gp = c->pos; gq = lane;
@@ -505,7 +523,10 @@ __global__ void __launch_bounds__(MC_THREADS) k_block_lu_mc(T *W, int64_t ld, in
                 if (!stop) { if (b == 0) chosen[j] = gp; s_piv[kk] = (int)gp; }
             }
             if (stop) { stopped = true; break; }
-            if (CL && warp == 0 && lane < w) Lb[kk * MC_LB + lane] = wv[lane];
+            if constexpr (CL) {             // every warp keeps the winner's row (the same values) for its deferred update
+                if (lane < w) Lb[kk * MC_LB + lane] = wv[lane];
+                __syncwarp();
+            }
             // 3. this thread's row: the pivot row leaves the search; a live row takes its multiplier and the update of
             // the panel's later columns
             if (mine) {
@@ -514,8 +535,12 @@ __global__ void __launch_bounds__(MC_THREADS) k_block_lu_mc(T *W, int64_t ld, in
                     const T inv = recip(pv);
                     const T l = mul(S[kk * per + tid], inv);
                     S[kk * per + tid] = l;
+                    if constexpr (CL) {         // the next column now; the others during the next column's barrier
+                        if (kk + 1 < w) S[(kk + 1) * per + tid] = sub(S[(kk + 1) * per + tid], mul(l, wv[kk + 1]));
+                    } else {
 #pragma unroll 4
-                    for (int c = kk + 1; c < w; c++) S[c * per + tid] = sub(S[c * per + tid], mul(l, wv[c]));
+                        for (int c = kk + 1; c < w; c++) S[c * per + tid] = sub(S[c * per + tid], mul(l, wv[c]));
+                    }
                 }
             }
         }
