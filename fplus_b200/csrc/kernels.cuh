@@ -910,22 +910,14 @@ struct PivotAsm {
     const int64_t *rowinit;                  // the entering rows' ids (-1 for rows from children)
 };
 
+// A front's pivot block into shared memory (A: npiv x nrows, column-major, A[c * nrows + i]) with its row ids (rid): read
+// from the working block, or (pa.on) assembled here from the original entries and at most one child's contribution
+// block.  Every thread of the CTA takes part; the caller synchronises before reading A.
 template <typename T>
-__device__ __forceinline__ void front_lu2_body(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
-                                               int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
-                                               int64_t *__restrict__ rowid, T *__restrict__ Lout, int *__restrict__ perm,
-                                               int64_t *__restrict__ p_lu, DevStatus *st, int64_t front, const PivotAsm &pa)
+__device__ __forceinline__ void stage_pivot_block(T *__restrict__ A, int64_t *__restrict__ rid, const T *__restrict__ W, int64_t ld,
+                                                  int nrows, int npiv, const int64_t *__restrict__ rowid, const PivotAsm &pa,
+                                                  int tid, int nt)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *A = reinterpret_cast<T *>(smem_raw);                        // npiv x nrows, column-major: A[c * nrows + i]
-    T *lcol = A + (size_t)npiv * nrows;                            // 2 x nrows: multipliers of steps j (j & 1)
-    int64_t *rid = reinterpret_cast<int64_t *>(lcol + 2 * nrows);
-    double *thr = reinterpret_cast<double *>(rid + nrows);         // npiv: pivot_rel * max |B(:, column)|
-    int *tag = reinterpret_cast<int *>(thr + npiv);
-    int *pos = tag + nrows;
-    __shared__ int s_bi[2], s_stv[2], s_stop;                      // s_stv: the stop decision of steps j (j & 1)
-    __shared__ T s_inv[2];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
     const int ne = npiv * nrows;
     if (!pa.on) {
         pdl_wait();
@@ -960,6 +952,26 @@ __device__ __forceinline__ void front_lu2_body(const T *__restrict__ W, int64_t 
             *a = add(*a, cb[t + (int64_t)c * cbr]);
         }
     }
+}
+
+template <typename T>
+__device__ __forceinline__ void front_lu2_body(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
+                                               int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
+                                               int64_t *__restrict__ rowid, T *__restrict__ Lout, int *__restrict__ perm,
+                                               int64_t *__restrict__ p_lu, DevStatus *st, int64_t front, const PivotAsm &pa)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *A = reinterpret_cast<T *>(smem_raw);                        // npiv x nrows, column-major: A[c * nrows + i]
+    T *lcol = A + (size_t)npiv * nrows;                            // 2 x nrows: multipliers of steps j (j & 1)
+    int64_t *rid = reinterpret_cast<int64_t *>(lcol + 2 * nrows);
+    double *thr = reinterpret_cast<double *>(rid + nrows);         // npiv: pivot_rel * max |B(:, column)|
+    int *tag = reinterpret_cast<int *>(thr + npiv);
+    int *pos = tag + nrows;
+    __shared__ int s_bi[2], s_stv[2], s_stop;                      // s_stv: the stop decision of steps j (j & 1)
+    __shared__ T s_inv[2];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
+    const int ne = npiv * nrows;
+    stage_pivot_block<T>(A, rid, W, ld, nrows, npiv, rowid, pa, tid, nt);
     for (int i = tid; i < nrows; i += nt) tag[i] = INT_MAX;
     for (int c = tid; c < npiv; c += nt) thr[c] = pivot_rel * colmax[fcol + c];
     if (tid == 0) s_stop = st->code != 0 ? 3 : 0;
@@ -1217,6 +1229,178 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
                                                     int64_t *__restrict__ p_lu, DevStatus *st, int64_t front, PivotAsm pa)
 {
     front_lu2_body<T>(W, ld, nrows, npiv, nri, fcol, colmax, pivot_rel, rowid, Lout, perm, p_lu, st, front, pa);
+}
+
+// Partial-pivot LU of a front's pivot block with the block in registers (nrows <= 128, npiv <= 64; one CTA of 512
+// threads).  Thread (g, i) -- column group g = warp / 4, row i = 32 (warp % 4) + lane -- holds row i's entries of the
+// columns g, g + 4, .., g + 60 in registers for the whole elimination.  Per pivot step j (two block barriers):
+//   B  every thread reads the four warp candidates of column j (posted before the first barrier), takes the winner (the
+//      largest pivot key, ties to the smaller row of B) and makes the same stop decision (singular, dense row); the
+//      threads of column j form the multipliers l = a_ij / a_pj in their registers (the entries of L) and post them; the
+//      pivot row's threads post its later entries (u).
+//   C  every row not yet pivoted updates its later columns, a_ik -= l_i u_k, from its registers; the warps of column
+//      j + 1 update that column first and post their candidates for step j + 1 (key, row of B, value, 1 / value).
+// Rows never move: a row pivoted at step j is tagged j, and the block goes out in the final row order at the end.  The
+// arithmetic per entry is that of k_front_lu2 (l = a * (1 / p), a - l u), and so are the pivots.
+constexpr int LU4_THREADS = 512, LU4_NR = 128, LU4_NP = 64, LU4_G = 4, LU4_M = LU4_NP / LU4_G;
+
+template <typename T> struct Lu4Cand {
+    unsigned long long key;    // pivot key (0: no candidate)
+    long long rid;             // row of B (ties: the smaller)
+    T val, inv;                // the candidate value and its reciprocal
+    int row;                   // row in the block (-1: no candidate)
+    int pad[3];
+};
+
+// dynamic shared memory: the staged block (reused for the output), row ids, thresholds and their keys
+static inline size_t front_lu4_smem(int64_t nrows, int64_t npiv, int64_t vs)
+{
+    return (size_t)(nrows * npiv * vs + nrows * 8 + npiv * 16);
+}
+
+template <typename T>
+__device__ __forceinline__ void front_lu4_body(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
+                                               int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
+                                               int64_t *__restrict__ rowid, T *__restrict__ Lout, int *__restrict__ perm,
+                                               int64_t *__restrict__ p_lu, DevStatus *st, int64_t front, const PivotAsm &pa)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *A = reinterpret_cast<T *>(smem_raw);                        // npiv x nrows, column-major: A[c * nrows + i]
+    int64_t *rid = reinterpret_cast<int64_t *>(A + (size_t)npiv * nrows);
+    double *thr = reinterpret_cast<double *>(rid + nrows);         // npiv: pivot_rel * max |B(:, column)|
+    unsigned long long *thk = reinterpret_cast<unsigned long long *>(thr + npiv);   // the key of 2 thr
+    __shared__ Lu4Cand<T> cand[4];
+    __shared__ T ubuf[LU4_NP], lbuf[LU4_NR];
+    __shared__ int wcnt[4], s_stop;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = warp >> 2, wr = warp & 3, i = wr * 32 + lane;
+    if (tid == 0) s_stop = st->code != 0;                          // an earlier front stopped the factorization
+    stage_pivot_block<T>(A, rid, W, ld, nrows, npiv, rowid, pa, tid, LU4_THREADS);
+    for (int c = tid; c < npiv; c += LU4_THREADS) {
+        thr[c] = pivot_rel * colmax[fcol + c];
+        thk[c] = pivkey_of_modulus<T>(2.0 * thr[c]);
+    }
+    for (int c = tid; c < LU4_NP; c += LU4_THREADS) ubuf[c] = VT<T>::zero();
+    __syncthreads();
+    if (s_stop) return;
+    T a[LU4_M];
+#pragma unroll
+    for (int m = 0; m < LU4_M; m++) {
+        const int c = g + LU4_G * m;
+        a[m] = i < nrows && c < npiv ? A[c * nrows + i] : VT<T>::zero();
+    }
+    const long long myrid = i < nrows ? (long long)rid[i] : LLONG_MAX;
+    bool live = i < nrows;                                         // not pivoted yet
+    int mytag = INT_MAX;                                           // the step at which this row was pivoted
+    // the warp's candidate for a column (x: this lane's entry, ok: the row is a candidate) into cand[wr]
+    auto post = [&](T x, bool ok) {
+        const unsigned long long key = ok ? pivkey(x) : 0ull;
+        const T xinv = key != 0ull ? recip(x) : VT<T>::zero();
+        const unsigned long long mk = warp_max_key(key);
+        unsigned cnd = __ballot_sync(0xffffffffu, key != 0ull && key == mk);
+        if (cnd == 0u) {
+            if (lane == 0) { cand[wr].key = 0ull; cand[wr].rid = LLONG_MAX; cand[wr].row = -1; }
+            return;
+        }
+        if ((cnd & (cnd - 1u)) != 0u) {
+            long long r2 = (cnd >> lane) & 1u ? myrid : LLONG_MAX;
+            for (int o = 16; o > 0; o >>= 1) { const long long t = __shfl_xor_sync(0xffffffffu, r2, o); r2 = t < r2 ? t : r2; }
+            cnd = __ballot_sync(0xffffffffu, ((cnd >> lane) & 1u) && myrid == r2);
+        }
+        if (lane == __ffs(cnd) - 1) {
+            cand[wr].key = mk; cand[wr].rid = myrid; cand[wr].val = x; cand[wr].inv = xinv; cand[wr].row = i;
+        }
+    };
+    if (g == 0) post(a[0], live);
+    __syncthreads();
+#pragma unroll
+    for (int jj = 0; jj < LU4_M; jj++) {
+        for (int gg = 0; gg < LU4_G; gg++) {
+            const int j = LU4_G * jj + gg;
+            if (j >= npiv) goto done;
+            // B: the winner of column j (every thread the same), the stop decision, the multipliers and the pivot row
+            int bs = 0;
+            unsigned long long bk = cand[0].key;
+            long long br = cand[0].rid;
+#pragma unroll
+            for (int s = 1; s < 4; s++) {
+                const unsigned long long k = cand[s].key;
+                const long long r = cand[s].rid;
+                if (k > bk || (k == bk && r < br)) { bk = k; br = r; bs = s; }
+            }
+            const int bi = cand[bs].row;
+            const T pv = cand[bs].val, inv = cand[bs].inv;
+            {
+                // the singular test of the reference (FPLUS src/factor_sn_panel.inc:232-233): no candidate, a zero
+                // modulus, or a modulus below pivot_rel * max |B(:, column)| (the modulus itself only near it)
+                int stop = 0;
+                if (bi < 0 || bk == 0ull || (bk < thk[j] && vabs(pv) < thr[j])) stop = 1;
+                else if (bi >= nri) stop = 2;
+                if (stop) {
+                    if (tid == 0) {
+                        if (stop == 1) set_status(st, ST_SINGULAR, fcol + j, bi >= 0 ? vabs(pv) : 0.0, thr[j]);
+                        else set_status(st, ST_BORDER, front, vabs(pv), thr[j]);
+                    }
+                    return;                                      // every thread leaves here
+                }
+            }
+            const bool piv = i == bi;
+            if (piv) { mytag = j; live = false; }
+            if (g == gg && live) { const T l = mul(a[jj], inv); a[jj] = l; lbuf[i] = l; }
+            if (piv) {
+#pragma unroll
+                for (int m = jj; m < LU4_M; m++)
+                    if (m > jj || g > gg) ubuf[g + LU4_G * m] = a[m];
+            }
+            __syncthreads();
+            // C: the update of every live row; the warps of column j + 1 post its candidates once it is updated
+            const T l = g == gg ? a[jj] : (live ? lbuf[i] : VT<T>::zero());
+            if (live && g > gg) a[jj] = sub(a[jj], mul(l, ubuf[g + LU4_G * jj]));
+            if (jj + 1 < LU4_M && live) a[jj + 1] = sub(a[jj + 1], mul(l, ubuf[g + LU4_G * (jj + 1)]));
+            if (j + 1 < npiv && g == ((gg + 1) & 3)) post(gg == 3 ? a[jj + 1 < LU4_M ? jj + 1 : jj] : a[jj], live);
+            if (live) {
+#pragma unroll
+                for (int m = jj + 2; m < LU4_M; m++) a[m] = sub(a[m], mul(l, ubuf[g + LU4_G * m]));
+            }
+            __syncthreads();
+        }
+    }
+done:
+    // the final order: pivot rows at their step, the others after them in block order
+    {
+        const bool un = i < nrows && mytag == INT_MAX;
+        const unsigned bal = __ballot_sync(0xffffffffu, un);
+        if (g == 0 && lane == 0) wcnt[wr] = __popc(bal);
+        __syncthreads();
+        int base = npiv;
+        for (int w = 0; w < wr; w++) base += wcnt[w];
+        const int k = un ? base + __popc(bal & ((1u << lane) - 1u)) : mytag;
+        if (i < nrows) {
+#pragma unroll
+            for (int m = 0; m < LU4_M; m++) {
+                const int c = g + LU4_G * m;
+                if (c < npiv) A[c * nrows + k] = a[m];
+            }
+            if (g == 0) {
+                perm[k] = i;
+                rowid[k] = myrid;
+                if (k < npiv) p_lu[fcol + k] = myrid;
+            }
+        }
+    }
+    __syncthreads();
+    const int ne = npiv * nrows;
+    for (int e = tid; e < ne; e += LU4_THREADS) Lout[e] = A[e];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(LU4_THREADS, 1) k_front_lu4(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
+                                                               int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
+                                                               int64_t *__restrict__ rowid, T *__restrict__ Lout,
+                                                               int *__restrict__ perm, int64_t *__restrict__ p_lu, DevStatus *st,
+                                                               int64_t front, PivotAsm pa)
+{
+    front_lu4_body<T>(W, ld, nrows, npiv, nri, fcol, colmax, pivot_rel, rowid, Lout, perm, p_lu, st, front, pa);
 }
 
 // Blocked partial-pivot LU of a front's pivot block in shared memory (nrows <= 128, npiv <= 64; one CTA of LU3_THREADS):
@@ -2402,152 +2586,6 @@ __global__ void __launch_bounds__(512) k_chain_bwd(const T *__restrict__ Ua, con
     }
 }
 
-// The backward sweep through the dense chain by blocks of CHB fronts (the fronts [k0, k1), chain indices), two launches
-// per block, the blocks from the last one up.  Rows and columns are relative to the chain's first column f0; front j
-// owns rows [j nb, (j + 1) nb) and its U12 row i, column c sits at Ua[cU_off[j] + i + (c - j nb - nb) nb].
-//   k_chain_diag (one CTA)   for k = k1 - 1 down to k0: y_k -= U[front k rows, columns of fronts (k, k1)] x, then
-//                            x_k = U11_k^-1 y_k (U11 in the top rows of front k's L block, scaled by the reciprocal
-//                            diagonal; a warp per right-hand side, as in k_chain_bwd's last CTA)
-//   k_chain_bulk (full grid) every row above the block: y_r -= U[r, the block's columns] x_block, four lanes per row
-//                            (each a quarter of the columns, 16 loads in flight), combined by shuffles in a fixed order
-// Every entry of U12 in the chain is read once per group of right-hand sides, and the serial part per block is only the
-// block's own triangle.
-constexpr int CHB = 4;
-
-template <typename T>
-__global__ void __launch_bounds__(512) k_chain_diag(const T *__restrict__ Ua, const int64_t *__restrict__ cU_off,
-                                                    const int64_t *__restrict__ cL_off, const int64_t *__restrict__ cnrow,
-                                                    const T *__restrict__ La, int64_t f0, int64_t nb, int64_t k0, int64_t k1,
-                                                    int64_t ncols_chain, T *__restrict__ Y, T *__restrict__ X, int64_t n,
-                                                    int64_t nrhs, DevStatus *st)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *s = reinterpret_cast<T *>(smem_raw);          // nb x nrhs: y_k
-    T *dinv = s + nb * nrhs;                          // nb
-    T *sU = dinv + nb;                                // nb x nb: sU[j + i * nb] = U[j, i] / U[i, i]
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    pdl_wait();
-    pdl_trigger();
-    if (st->code) return;
-    for (int64_t k = k1 - 1; k >= k0; k--) {
-        const int64_t fk = k * nb, npk = (fk + nb <= ncols_chain ? nb : ncols_chain - fk);
-        const T *Lk = La + cL_off[k];
-        const int64_t nrk = cnrow[k];
-        // the rows of front k against the block's solved columns after it, (k, k1): four lanes per row
-        const int64_t ca = fk + nb, cb = (k1 * nb < ncols_chain ? k1 * nb : ncols_chain), nc = cb > ca ? cb - ca : 0;
-        if (nc > 0) {
-            const int64_t tot = (npk * 4 + 31) / 32 * 32;     // whole warps: every lane takes part in the shuffles
-            for (int64_t e = tid; e < tot; e += blockDim.x) {
-                const bool on = e < npk * 4;
-                const int64_t i = on ? e >> 2 : 0;
-                const int qq = (int)(e & 3);
-                const T *u = Ua + cU_off[k] + i;
-                for (int64_t r0 = 0; r0 < nrhs; r0 += 8) {     // eight right-hand sides per pass: each u entry used 8 times
-                    const int rb = nrhs - r0 < 8 ? (int)(nrhs - r0) : 8;
-                    T acc[8];
-#pragma unroll
-                    for (int t = 0; t < 8; t++) acc[t] = VT<T>::zero();
-                    if (on)
-                        for (int64_t c = ca + qq; c < cb; c += 4) {
-                            const T uv = u[(c - fk - nb) * nb];
-#pragma unroll
-                            for (int t = 0; t < 8; t++)
-                                if (t < rb) acc[t] = add(acc[t], mul(uv, X[f0 + c + (r0 + t) * n]));
-                        }
-#pragma unroll
-                    for (int t = 0; t < 8; t++) {
-                        acc[t] = add(acc[t], shfl_xor_v<T>(acc[t], 1));
-                        acc[t] = add(acc[t], shfl_xor_v<T>(acc[t], 2));
-                        if (on && qq == 0 && t < rb) { T *y = Y + f0 + fk + i + (r0 + t) * n; *y = sub(*y, acc[t]); }
-                    }
-                }
-            }
-            __syncthreads();
-        }
-        // x_k = U11^-1 y_k
-        for (int e = tid; e < npk * npk; e += blockDim.x) sU[e] = Lk[(e % npk) + (int64_t)(e / npk) * nrk];
-        for (int64_t e = tid; e < npk * nrhs; e += blockDim.x) s[e] = Y[f0 + fk + e % npk + (e / npk) * n];
-        for (int i = tid; i < npk; i += blockDim.x) {
-            const T d = Lk[i + (int64_t)i * nrk];
-            if (is_zero(d)) set_status(st, ST_SOLVE_ZERO, f0 + fk + i, 0, 0);
-            dinv[i] = is_zero(d) ? VT<T>::zero() : recip(d);
-        }
-        __syncthreads();
-        if (st->code == ST_SOLVE_ZERO) return;
-        for (int e = tid; e < npk * npk; e += blockDim.x) sU[e] = mul(sU[e], dinv[e / npk]);
-        __syncthreads();
-        for (int64_t r = warp; r < nrhs; r += nw) {
-            T a = lane < npk ? s[lane + r * npk] : VT<T>::zero();
-            T b = lane + 32 < npk ? s[lane + 32 + r * npk] : VT<T>::zero();
-            for (int ii = (int)npk - 1; ii >= 0; ii--) {
-                const T *col = sU + ii * npk;
-                const T si = shfl_v<T>(ii < 32 ? a : b, ii & 31);
-                if (ii >= 32) {
-                    if (lane < ii - 32) b = sub(b, mul(col[lane + 32], si));
-                    a = sub(a, mul(col[lane], si));
-                } else if (lane < ii) a = sub(a, mul(col[lane], si));
-            }
-            if (lane < npk) X[f0 + fk + lane + r * n] = mul(a, dinv[lane]);
-            if (lane + 32 < npk) X[f0 + fk + lane + 32 + r * n] = mul(b, dinv[lane + 32]);
-        }
-        __syncthreads();
-    }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256) k_chain_bulk(const T *__restrict__ Ua, const int64_t *__restrict__ cU_off, int64_t f0,
-                                                    int64_t nb, int64_t k0, int64_t k1, int64_t ncols_chain,
-                                                    T *__restrict__ Y, const T *__restrict__ X, int64_t n, int64_t nrhs)
-{
-    constexpr int RB = 8;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *xs = reinterpret_cast<T *>(smem_raw);          // the block's x: column c (relative) of rhs t at c + t * nc
-    const int tid = threadIdx.x, lane = tid & 31, q = lane & 3;
-    const int64_t ca = k0 * nb, cb = (k1 * nb < ncols_chain ? k1 * nb : ncols_chain), nc = cb - ca;
-    const int64_t R = k0 * nb;                        // every row above the block
-    pdl_wait();
-    pdl_trigger();
-    for (int64_t e = tid; e < nc * nrhs; e += blockDim.x) xs[e] = X[f0 + ca + e % nc + (e / nc) * n];
-    __syncthreads();
-    const int64_t r = blockIdx.x * (int64_t)(blockDim.x >> 2) + (tid >> 2);
-    const bool on = r < R;
-    const int64_t j = on ? r / nb : 0, i = on ? r % nb : 0;
-    const T *u = Ua + (on ? cU_off[j] : 0) + i + (ca - j * nb - nb) * nb;      // U12_j[i, column ca]
-    // 64 columns per round (16 per lane, all loaded at once, then used for every right-hand side); the row's partial
-    // sums of a round go into y after it (y stays in L2)
-    for (int64_t cr = 0; cr < nc; cr += 64) {
-        const int64_t c0 = cr + q * 16;
-        T uv[16];
-#pragma unroll
-        for (int c = 0; c < 16; c++) uv[c] = on && c0 + c < nc ? u[(c0 + c) * nb] : VT<T>::zero();
-        for (int64_t r0 = 0; r0 < nrhs; r0 += RB) {
-            const int rb = nrhs - r0 < RB ? (int)(nrhs - r0) : RB;
-            T acc[RB];
-#pragma unroll
-            for (int t = 0; t < RB; t++) acc[t] = VT<T>::zero();
-            if (on) {
-#pragma unroll
-                for (int c = 0; c < 16; c++) {
-                    if (c0 + c >= nc) break;
-#pragma unroll
-                    for (int t = 0; t < RB; t++)
-                        if (t < rb) acc[t] = add(acc[t], mul(uv[c], xs[c0 + c + (r0 + t) * nc]));
-                }
-            }
-#pragma unroll
-            for (int t = 0; t < RB; t++) {
-                acc[t] = add(acc[t], shfl_xor_v<T>(acc[t], 1));
-                acc[t] = add(acc[t], shfl_xor_v<T>(acc[t], 2));
-            }
-            if (on && q == 0) {
-#pragma unroll
-                for (int t = 0; t < RB; t++)
-                    if (t < rb) { T *y = Y + f0 + r + (r0 + t) * n; *y = sub(*y, acc[t]); }
-            }
-        }
-    }
-}
-
 // the sum over a warp by a fixed butterfly (every lane gets the same result)
 template <typename T> __device__ __forceinline__ T shfl_sum(T v)
 {
@@ -3557,6 +3595,21 @@ __global__ void __launch_bounds__(640) k_bat_lu2(const FcFront *__restrict__ fc,
     PivotAsm pa;
     pa.on = 0;
     front_lu2_body<T>(Wbase + F.wofs, F.nr, (int)F.nr, (int)F.np, (int)F.nri, F.f, colmax, pivot_rel, rowid_all + F.row_off,
+                      La + F.L_off, permall + F.row_off, p_lu, st, fi, pa);
+}
+
+// the same with the register-resident pivot-block LU (the body of k_front_lu4)
+template <typename T>
+__global__ void __launch_bounds__(LU4_THREADS, 1) k_bat_lu4(const FcFront *__restrict__ fc, const int *__restrict__ list,
+                                                             const T *__restrict__ Wbase, const double *__restrict__ colmax,
+                                                             double pivot_rel, int64_t *__restrict__ rowid_all, T *__restrict__ La,
+                                                             int *__restrict__ permall, int64_t *__restrict__ p_lu, DevStatus *st)
+{
+    const int fi = list[blockIdx.x];
+    const FcFront F = fc[fi];
+    PivotAsm pa;
+    pa.on = 0;
+    front_lu4_body<T>(Wbase + F.wofs, F.nr, (int)F.nr, (int)F.np, (int)F.nri, F.f, colmax, pivot_rel, rowid_all + F.row_off,
                       La + F.L_off, permall + F.row_off, p_lu, st, fi, pa);
 }
 

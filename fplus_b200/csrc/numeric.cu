@@ -87,8 +87,7 @@ template <typename T> static int upload(const std::vector<T> &h, T **d, char *er
 DevPlan::~DevPlan()
 {
     for (void *p : {(void *)cols, (void *)relcol, (void *)rowinit, (void *)asm_src, (void *)asm_dst, (void *)Bp, (void *)Bi,
-                    (void *)Bsrc, (void *)row_perm, (void *)col_perm, (void *)seg, (void *)chain_uoff, (void *)chain_loff,
-                    (void *)chain_nrow, (void *)sv, (void *)sv_rows, (void *)sv_cols, (void *)rsp, (void *)rsi, (void *)csp,
+                    (void *)Bsrc, (void *)row_perm, (void *)col_perm, (void *)seg, (void *)chain_uoff, (void *)sv, (void *)sv_rows, (void *)sv_cols, (void *)rsp, (void *)rsi, (void *)csp,
                     (void *)csi, (void *)iota, (void *)sv_brows, (void *)sv_bcols, (void *)fc, (void *)children, (void *)bs_list})
         if (p) cudaFree(p);
 }
@@ -313,21 +312,17 @@ int dev_upload_plan(const fplus_symbolic *S, const FrontPlan &P, DevPlan &D, cha
         int64_t c0 = nf;
         while (c0 > 0 && P.fronts[c0 - 1].dense) c0--;
         bool ok = nf - c0 >= 2 && nb > 0 && nb <= 64;
-        std::vector<int64_t> uoff, loff, nrow;
+        std::vector<int64_t> uoff;
         for (int64_t j = c0; ok && j < nf; j++) {
             const Front &F = P.fronts[j];
             const bool lastf = j == nf - 1;
             ok = F.f == P.fronts[c0].f + (j - c0) * nb && (lastf ? F.npiv <= nb : F.npiv == nb) && F.npiv <= F.nrows &&
                  F.ncols == S->n - F.f;
             uoff.push_back(F.U_off);
-            loff.push_back(F.L_off);
-            nrow.push_back(F.nrows);
         }
         if (ok) {
             D.chain_begin = c0; D.chain_nb = nb; D.chain_f0 = P.fronts[c0].f;
             if ((rc = upload(uoff, &D.chain_uoff, err, errlen))) return rc;
-            if ((rc = upload(loff, &D.chain_loff, err, errlen))) return rc;
-            if ((rc = upload(nrow, &D.chain_nrow, err, errlen))) return rc;
         }
     }
     if ((rc = upload_solve_levels(P, D, err, errlen))) return rc;
@@ -567,6 +562,8 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     static thread_local int attr_set = 0;
     if (!attr_set) {
         CK(cudaFuncSetAttribute(k_front_lu2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_front_lu4<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_bat_lu4<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_front_lu3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
@@ -731,6 +728,15 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             } else
                 k_front_lu3<T><<<1, LU3_THREADS, sm3, st>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel,
                                                             N.rowid + F.row_off, Lf, perm, N.p_lu, N.st, fi, pa), note_launch();
+        } else if ((N.lu_variant & 3) == 1 && nr <= LU4_NR && np <= LU4_NP && front_lu4_smem(nr, np, vs) <= SMEM_MAX) {
+            const size_t sm4 = front_lu4_smem(nr, np, vs);
+            if (pa.on) {      // right after the child's tail head on the critical stream: overlap the launch
+                CK(launch_pdl(k_front_lu4<T>, 1, LU4_THREADS, sm4, st, (const T *)W, ld, (int)nr, (int)np, (int)F.nri, F.f,
+                              (const double *)N.colmax, pivot_rel, N.rowid + F.row_off, Lf, perm, N.p_lu, N.st, fi, pa));
+                note_launch();
+            } else
+                k_front_lu4<T><<<1, LU4_THREADS, sm4, st>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel,
+                                                            N.rowid + F.row_off, Lf, perm, N.p_lu, N.st, fi, pa), note_launch();
         } else if (sm <= SMEM_MAX) {
             const int R = (int)((nr + 31) & ~31);
             int nt = 32 + (R <= 128 ? 4 * R : R);   // the pivot warp + the update warps
@@ -857,8 +863,12 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             int nt = 32 + (R <= 128 ? 4 * R : R);
             if (nt > 640) nt = 640;
             prof.begin(s, PROF_LU, fm * D.bs_lu_flops[(size_t)lv], D.bs_lu_bytes[(size_t)lv] * (double)vs);
-            k_bat_lu2<T><<<cnt, nt, front_lu_smem(D.bs_maxnr[(size_t)lv], D.bs_maxnp[(size_t)lv], vs), s>>>(
-                D.fc, bl, Wb, N.colmax, pivot_rel, N.rowid, La, N.permall, N.p_lu, N.st), note_launch();
+            if ((N.lu_variant & 3) == 1)
+                k_bat_lu4<T><<<cnt, LU4_THREADS, front_lu4_smem(D.bs_maxnr[(size_t)lv], D.bs_maxnp[(size_t)lv], vs), s>>>(
+                    D.fc, bl, Wb, N.colmax, pivot_rel, N.rowid, La, N.permall, N.p_lu, N.st), note_launch();
+            else
+                k_bat_lu2<T><<<cnt, nt, front_lu_smem(D.bs_maxnr[(size_t)lv], D.bs_maxnp[(size_t)lv], vs), s>>>(
+                    D.fc, bl, Wb, N.colmax, pivot_rel, N.rowid, La, N.permall, N.p_lu, N.st), note_launch();
             prof.end(s);
             if (D.bs_maxtiles[(size_t)lv] > 0) {
                 prof.begin(s, PROF_SCHUR, fm * D.bs_tail_flops[(size_t)lv], D.bs_tail_bytes[(size_t)lv] * (double)vs);
@@ -1254,27 +1264,19 @@ static int run_solve_block(const FrontPlan &P, const DevPlan &D, DevNum &N, T *x
             const int64_t cb = D.chain_begin, nb = D.chain_nb;
             const size_t csm = std::max((size_t)(nb + (nb + 15) / 16) * nrhs, (size_t)(nb * (nrhs + 1) + nb * nb)) * sizeof(T);
             if (csm > 48 * 1024) CK(cudaFuncSetAttribute(k_chain_bwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
-            // blocks of CHB fronts from the last: the block's own triangle on one CTA (k_chain_diag), then every row above
-            // it against the block's columns on the whole GPU (k_chain_bulk)
-            const int64_t nch = nf - cb, ncc = n - D.chain_f0;
-            const size_t dsm = (size_t)(nb * (nrhs + 1) + nb * nb) * sizeof(T);
-            const size_t bsm = (size_t)(CHB * nb) * (size_t)nrhs * sizeof(T);
-            CK(cudaFuncSetAttribute(k_chain_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(dsm, (size_t)48 * 1024)));
-            CK(cudaFuncSetAttribute(k_chain_bulk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(bsm, (size_t)48 * 1024)));
-            for (int64_t k1 = nch; k1 > 0; k1 -= CHB) {
-                const int64_t k0 = std::max<int64_t>(0, k1 - CHB);
-                CK(launch_pdl(k_chain_diag<T>, 1, 512, dsm, s, (const T *)Ua, (const int64_t *)D.chain_uoff,
-                              (const int64_t *)D.chain_loff, (const int64_t *)D.chain_nrow, (const T *)La, D.chain_f0, nb, k0, k1,
-                              ncc, S2, R, n, nrhs, N.st));
+            // front by front from the last: each launch subtracts front k + 1's solution from every chain row above it
+            // (U read once for all right-hand sides), and its last CTA solves front k's U11 block
+            for (int64_t fi = nf - 1; fi >= cb; fi--) {
+                const Front &F = P.fronts[fi];
+                const int64_t jk1 = fi + 1 < nf ? fi + 1 - cb : -1;
+                const int npk1 = jk1 >= 0 ? (int)P.fronts[fi + 1].npiv : 0;
+                const int64_t rows = jk1 >= 0 ? jk1 * nb : 0;
+                const int cbt = nrhs > 8 ? 512 : 256;      // a warp per right-hand side in the U11 sweep
+                const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((rows + cbt / 4 - 1) / (cbt / 4), 296));
+                CK(launch_pdl(k_chain_bwd<T>, grid, cbt, csm, s, (const T *)Ua, (const int64_t *)D.chain_uoff, D.chain_f0, nb,
+                              jk1, npk1, (const T *)(La + F.L_off), F.nrows, F.f, (int)F.npiv, S2, R, n, nrhs, N.st));
                 note_launch();
-                if (k0 > 0) {
-                    const int64_t rows = k0 * nb;
-                    CK(launch_pdl(k_chain_bulk<T>, (int)((rows + 63) / 64), 256, bsm, s, (const T *)Ua, (const int64_t *)D.chain_uoff,
-                                  D.chain_f0, nb, k0, k1, ncc, S2, (const T *)R, n, nrhs));
-                    note_launch();
-                }
             }
-            (void)csm;
             fi_end = cb;
         }
         CK(cudaFuncSetAttribute(k_bwdU_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));

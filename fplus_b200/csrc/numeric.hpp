@@ -34,7 +34,6 @@ struct DevPlan {
     // (the last one at most), first column chain_f0, their U offsets; chain_begin < 0 when the fronts do not qualify
     int64_t chain_begin = -1, chain_nb = 0, chain_f0 = 0;
     int64_t *chain_uoff = nullptr;
-    int64_t *chain_loff = nullptr, *chain_nrow = nullptr;     // each chain front's L block (U11 in its top rows), rows
     // the level-scheduled solve: every front's descriptor; per level (ascending height) the fronts the one-CTA kernels
     // take, as device lists (sv_rows: the L and L^T sweeps; sv_cols: the U and U^T sweeps) with host ranges and the
     // level's largest sizes, and the others as host lists; the lists of the children's contribution entries landing on
@@ -108,7 +107,7 @@ struct DevNum {
     int prec = 0;
     void *coopbuf = nullptr;       // the multi-CTA pivot-block LU: the CTAs' posts, the ticket, the choices, U12, row scratch
     size_t cap_coop = 0;
-    int lu_variant = 2;            // the small fronts' pivot-block LU (2: k_front_lu2, 3: k_front_lu3); + 4: the tall
+    int lu_variant = 1;            // the small fronts' pivot-block LU (1: k_front_lu4, 2: k_front_lu2, 3: k_front_lu3); + 4: the tall
                                    // blocks by one CTA per 32-column panel instead of k_block_lu_mc; + 8: no batched
                                    // fronts (every front on its own)
     int capture = 0;               // the launches are being captured into a CUDA graph: no host copies, waits or decisions

@@ -233,12 +233,14 @@ def test_large_fronts_all_solve_directions(gpu, cplx):
             assert be <= 1e-14, f"trans {trans} rhs {r}: backward error {be:.2e}"
 
 
+@pytest.mark.parametrize("variant", [2, 3])
 @pytest.mark.parametrize("name", ["pencil_1x64", "pencil_2x256", "banded_cplx_1200", "convdiff3d_g12", "hard_cplx_300"])
-def test_blocked_pivot_block_lu_matches_oracle(gpu, name):
-    """The blocked pivot-block LU (k_front_lu3, the autotuner's other choice) gives the oracle's pivots and factors."""
+def test_other_pivot_block_lus_match_oracle(gpu, name, variant):
+    """The other pivot-block LU kernels of the small fronts (k_front_lu2: the block in shared memory, the autotuner's other
+    choice; k_front_lu3: blocked panels) give the oracle's pivots and factors."""
     n, Ap, Ai, Ax = CASES[name]()
     S = F.analyze(n, Ap, Ai)
-    S.set_front_shape(256, 64, 3)
+    S.set_front_shape(256, 64, variant)
     N = S.factor(Ax)
     orc = O.OracleLU(n, Ap, Ai, Ax, S.row_perm, S.col_perm)
     assert np.array_equal(N.p, orc.p)
@@ -246,11 +248,11 @@ def test_blocked_pivot_block_lu_matches_oracle(gpu, name):
     assert _rel(L, orc.L) <= FACTOR_TOL and _rel(U, orc.U) <= FACTOR_TOL
 
 
-@pytest.mark.parametrize("variant", [2, 6])
+@pytest.mark.parametrize("variant", [1, 5])
 @pytest.mark.parametrize("cplx", [False, True])
 def test_tall_pivot_blocks_match_oracle(gpu, cplx, variant):
     """Pivot blocks too large for one CTA (a 20^3 / 16^3 stencil: 256 pivots, hundreds to thousands of rows), pivoted by
-    all SMs in one launch (k_block_lu_mc, variant 2) and by one CTA per 32-column panel (variant 6): the oracle's pivots,
+    all SMs in one launch (k_block_lu_mc, variant 1) and by one CTA per 32-column panel (variant 5): the oracle's pivots,
     and L and U within 1e-12."""
     g = 16 if cplx else 20
     n, Ap, Ai, Ax = W.convdiff3d(g, 3)
@@ -269,16 +271,18 @@ def test_tall_pivot_blocks_match_oracle(gpu, cplx, variant):
     assert O.backward_error(n, Ap, Ai, Ax, x, b) <= 1e-14
 
 
+@pytest.mark.parametrize("lu", [1, 2])
 @pytest.mark.parametrize("cplx", [False, True])
-def test_batched_small_fronts_match_front_by_front(gpu, cplx):
+def test_batched_small_fronts_match_front_by_front(gpu, cplx, lu):
     """The small fronts at the bottom of the tree factored level by level (one launch per level for assembly, LU and
-    tail) give bit for bit the factors of the front-by-front path (set_front_shape variant + 8), and the oracle's pivots."""
+    tail) give bit for bit the factors of the front-by-front path (set_front_shape variant + 8), and the oracle's pivots,
+    with either pivot-block LU kernel (1: the block in registers, 2: in shared memory)."""
     g = 14 if cplx else 18
     n, Ap, Ai, Ax = W.convdiff3d(g, 3)
     if cplx:
         Ax = Ax + 0.25j * np.random.default_rng(23).uniform(-1, 1, Ax.size)
     Ns = []
-    for variant in (2, 10):
+    for variant in (lu, lu + 8):
         S = F.analyze(n, Ap, Ai)
         S.set_front_shape(256, 64, variant)
         Ns.append((S, S.factor(Ax)))

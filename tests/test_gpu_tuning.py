@@ -25,7 +25,7 @@ def test_autotune_keeps_the_pivots(gpu, case):
     S = F.analyze(n, Ap, Ai)
     p0 = S.factor(Ax).p
     w, nb, lu, ms = S.autotune(Ax)
-    assert w in (128, 256, 512) and nb in (32, 64) and lu in (2, 3) and ms > 0
+    assert w in (128, 256, 512) and nb in (32, 64) and lu in (1, 2) and ms > 0
     N = S.factor(Ax)
     assert np.array_equal(N.p, p0)
     b = W.rhs(n, 1, np.iscomplexobj(Ax), 1)[0]
