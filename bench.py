@@ -610,7 +610,9 @@ def run_b200_arm(args, rank, world):
     F.lib().fplus_b200_use_stream(ctypes.c_void_p(stream.cuda_stream))
     # the front shape for this pattern, picked once by the library's autotuner (untimed, like the analysis)
     t0 = time.perf_counter()
-    tuned = S.autotune(Ax) if not args.no_autotune else None
+    if args.front_variant:
+        S.set_front_shape(256, 64, args.front_variant)
+    tuned = S.autotune(Ax) if not (args.no_autotune or args.front_variant) else None
     autotune_ms = (time.perf_counter() - t0) * 1e3
     Ad = torch.from_numpy(Ax).to(dev)
     bd0 = torch.from_numpy(np.ascontiguousarray(b)).to(dev)
@@ -769,6 +771,7 @@ def run_b200_arm(args, rank, world):
             "scaling": "weak", "vs_baseline": None, "dtype": "c128" if cplx else "f64", "data": "synthetic",
             "config": dict(desc, **{"parallelism": f"replicas{world}" if world > 1 else "1 GPU",
                                     "l2": "flushed between steps (512 MiB write)", "analyze_ms": round(analyze_ms, 2),
+                                    "front_variant": args.front_variant or None,
                                     "front_shape": None if tuned is None else {"max_width": tuned[0], "nb_chain": tuned[1],
                                                                                 "lu_kernel": tuned[2],
                                                                                 "autotune_ms": round(autotune_ms, 1)},
@@ -794,6 +797,8 @@ def main():
                     help="Fourier modes of the pencil workload (8: n = 32768, the benchmark; 1: n = 4096, for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default front shape (no fplus_b200_autotune)")
+    ap.add_argument("--front-variant", type=int, default=0,
+                    help="fplus_b200_set_front_shape variant for the benchmark pattern instead of the autotuner (0: autotune)")
     ap.add_argument("--precision-grid", type=int, default=80,
                     help="grid of the 3D stencil of the precision-form measurement (80: n = 512,000; 0: none)")
     ap.add_argument("--random-n", type=int, default=40000,

@@ -272,7 +272,7 @@ class Symbolic:
         out["f_dense"] = fd.value
         return out
 
-    def set_front_shape(self, max_width=256, nb_chain=64, lu_variant=1):
+    def set_front_shape(self, max_width=256, nb_chain=64, lu_variant=2):
         """fplus_b200_set_front_shape."""
         _check(lib().fplus_b200_set_front_shape(self._h, int(max_width), int(nb_chain), int(lu_variant)), None)
 

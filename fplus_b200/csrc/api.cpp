@@ -281,7 +281,7 @@ extern "C" int fplus_b200_schur_update(int precision, int is_complex, int64_t M,
 extern "C" int fplus_b200_set_front_shape(fplus_symbolic *sym, int64_t max_width, int64_t nb_chain, int lu_variant)
 {
     if (!sym || max_width < 16 || max_width > 4096 || nb_chain < 8 || nb_chain > 64 ||
-        (lu_variant & 3) == 0 || (lu_variant & ~15) != 0)
+        (lu_variant & 3) == 0 || (lu_variant & ~63) != 0)
         return FPLUS_ERR_BADARG;
     std::lock_guard<std::mutex> lk(sym->mu);
     sym->max_width = max_width;
@@ -306,7 +306,7 @@ extern "C" int fplus_b200_autotune(fplus_symbolic *sym, const int64_t *Ap, const
     int bl = l0;
     double bms = -1.0;
     bool chain = false;
-    // the front shapes with the register-resident pivot-block LU, then the best shape with the shared-memory LU
+    // the front shapes with the shared-memory pivot-block LU, then the best shape with the register-resident LU
     for (int ci = 0; ci < 7; ci++) {
         const int wi = ci < 6 ? ci / 2 : -1, bi = ci < 6 ? ci % 2 : -1;
         if (ci < 6 && bi == 0 && !chain && wi > 0) continue;      // the chain size matters only with a dense chain
@@ -314,7 +314,7 @@ extern "C" int fplus_b200_autotune(fplus_symbolic *sym, const int64_t *Ap, const
             std::lock_guard<std::mutex> lk(sym->mu);
             sym->max_width = ci < 6 ? widths[wi] : bw;
             sym->nb_chain = ci < 6 ? nbs[bi] : bb;
-            sym->lu_variant = ci < 6 ? 1 : 2;
+            sym->lu_variant = ci < 6 ? 2 : 1;
         }
         {
             double t = -1.0;
@@ -333,7 +333,7 @@ extern "C" int fplus_b200_autotune(fplus_symbolic *sym, const int64_t *Ap, const
             }
             if (bms < 0 || t < bms) {
                 bms = t;
-                if (ci < 6) { bw = widths[wi]; bb = nbs[bi]; bl = 1; } else bl = 2;
+                if (ci < 6) { bw = widths[wi]; bb = nbs[bi]; bl = 2; } else bl = 1;
             }
         }
     }

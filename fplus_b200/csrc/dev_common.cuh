@@ -82,6 +82,7 @@ __device__ __forceinline__ unsigned long long pivkey(cplx a)
 {
     const double q = __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y));
     if (q >= 0x1p-1000 && q <= 0x1p1000) return ((unsigned long long)__double_as_longlong(q) >> 2) + (PIVKEY_OFF << 50);
+    if (a.x == 0.0 && a.y == 0.0) return 0ull;                     // exact zeros (common in a front) stay off the slow path
     return pivkey_wide(a.x, a.y);
 }
 // the key of a value of modulus t >= 0

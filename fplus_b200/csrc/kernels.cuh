@@ -965,7 +965,8 @@ __device__ __forceinline__ void front_lu2_body(const T *__restrict__ W, int64_t 
     T *lcol = A + (size_t)npiv * nrows;                            // 2 x nrows: multipliers of steps j (j & 1)
     int64_t *rid = reinterpret_cast<int64_t *>(lcol + 2 * nrows);
     double *thr = reinterpret_cast<double *>(rid + nrows);         // npiv: pivot_rel * max |B(:, column)|
-    int *tag = reinterpret_cast<int *>(thr + npiv);
+    unsigned long long *thk = reinterpret_cast<unsigned long long *>(thr + npiv);   // npiv: the pivot key of 2 thr
+    int *tag = reinterpret_cast<int *>(thk + npiv);
     int *pos = tag + nrows;
     __shared__ int s_bi[2], s_stv[2], s_stop;                      // s_stv: the stop decision of steps j (j & 1)
     __shared__ T s_inv[2];
@@ -973,7 +974,7 @@ __device__ __forceinline__ void front_lu2_body(const T *__restrict__ W, int64_t 
     const int ne = npiv * nrows;
     stage_pivot_block<T>(A, rid, W, ld, nrows, npiv, rowid, pa, tid, nt);
     for (int i = tid; i < nrows; i += nt) tag[i] = INT_MAX;
-    for (int c = tid; c < npiv; c += nt) thr[c] = pivot_rel * colmax[fcol + c];
+    for (int c = tid; c < npiv; c += nt) { thr[c] = pivot_rel * colmax[fcol + c]; thk[c] = pivkey_of_modulus<T>(2.0 * thr[c]); }
     if (tid == 0) s_stop = st->code != 0 ? 3 : 0;
     __syncthreads();
     if (s_stop) return;
@@ -990,11 +991,11 @@ __device__ __forceinline__ void front_lu2_body(const T *__restrict__ W, int64_t 
     const int my_i = ut >= 0 ? (nu >= R ? ut % R : ut) : 0, my_g = ut >= 0 ? (nu >= R ? ut / R : 0) : G;
     const bool upd = ut >= 0 && my_g < G;
     // The singular test of the reference (FPLUS src/factor_sn_panel.inc:232-233): no candidate, a zero modulus, or a
-    // modulus below t = pivot_rel * max |B(:, column)|.  A key at or above the key of 2t is clear of the threshold; below
-    // it the modulus itself is compared.
-    auto singular = [&](int bi, unsigned long long key, double t, T pv) -> bool {
+    // modulus below t = pivot_rel * max |B(:, column)|.  A key at or above the key of 2t (tk, staged) is clear of the
+    // threshold; below it the modulus itself is compared.
+    auto singular = [&](int bi, unsigned long long key, double t, unsigned long long tk, T pv) -> bool {
         if (bi < 0 || key == 0ull) return true;
-        return key < pivkey_of_modulus<T>(2.0 * t) && vabs(pv) < t;
+        return key < tk && vabs(pv) < t;
     };
     // warp 0: decide on the winner (bi, pivot key) of column j, publish into slot
     auto decide = [&](int j, int bi, unsigned long long key, int slot) {
@@ -1002,7 +1003,7 @@ __device__ __forceinline__ void front_lu2_body(const T *__restrict__ W, int64_t 
         const double t = thr[j];
         int stop = 0;
         const T pv = bi >= 0 ? A[(size_t)j * nrows + bi] : VT<T>::zero();
-        if (singular(bi, key, t, pv)) { set_status(st, ST_SINGULAR, fcol + j, bi >= 0 ? vabs(pv) : 0.0, t); stop = 1; }
+        if (singular(bi, key, t, thk[j], pv)) { set_status(st, ST_SINGULAR, fcol + j, bi >= 0 ? vabs(pv) : 0.0, t); stop = 1; }
         else if (bi >= nri) { set_status(st, ST_BORDER, front, vabs(pv), t); stop = 1; }
         s_bi[slot] = bi;
         s_stv[slot] = stop;
@@ -1067,7 +1068,7 @@ __device__ __forceinline__ void front_lu2_body(const T *__restrict__ W, int64_t 
             if (lane == 0) {
                 const double t = thr[j];
                 int stop = 0;
-                if (singular(bi, key, t, pv)) { set_status(st, ST_SINGULAR, fcol + j, bi >= 0 ? vabs(pv) : 0.0, t); stop = 1; }
+                if (singular(bi, key, t, thk[j], pv)) { set_status(st, ST_SINGULAR, fcol + j, bi >= 0 ? vabs(pv) : 0.0, t); stop = 1; }
                 else if (bi >= nri) { set_status(st, ST_BORDER, front, vabs(pv), t); stop = 1; }
                 s_bi[slot] = bi;
                 s_stv[slot] = stop;
@@ -1232,17 +1233,19 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
 }
 
 // Partial-pivot LU of a front's pivot block with the block in registers (nrows <= 128, npiv <= 64; one CTA of 512
-// threads).  Thread (g, i) -- column group g = warp / 4, row i = 32 (warp % 4) + lane -- holds row i's entries of the
-// columns g, g + 4, .., g + 60 in registers for the whole elimination.  Per pivot step j (two block barriers):
-//   B  every thread reads the four warp candidates of column j (posted before the first barrier), takes the winner (the
-//      largest pivot key, ties to the smaller row of B) and makes the same stop decision (singular, dense row); the
-//      threads of column j form the multipliers l = a_ij / a_pj in their registers (the entries of L) and post them; the
-//      pivot row's threads post its later entries (u).
-//   C  every row not yet pivoted updates its later columns, a_ik -= l_i u_k, from its registers; the warps of column
-//      j + 1 update that column first and post their candidates for step j + 1 (key, row of B, value, 1 / value).
-// Rows never move: a row pivoted at step j is tagged j, and the block goes out in the final row order at the end.  The
-// arithmetic per entry is that of k_front_lu2 (l = a * (1 / p), a - l u), and so are the pivots.
-constexpr int LU4_THREADS = 512, LU4_NR = 128, LU4_NP = 64, LU4_G = 4, LU4_M = LU4_NP / LU4_G;
+// threads, 16 warps).  Warp w owns rows 8w .. 8w + 7; lane 4r + q holds row 8w + r's entries of the columns q, q + 4, ..,
+// q + 60 (16 values) in registers for the whole elimination.  One block barrier per pivot step j:
+//   before it  every warp has applied step j - 1 to its live rows, found its candidate for column j among its 8 rows (the
+//              largest pivot key, ties to the smaller row of B) and posted it (key, row of B, value, 1 / value) together
+//              with the candidate row's 64 entries (double-buffered by step parity);
+//   after it   every thread reads the 16 candidates and makes the same pivot and stop decision; the lane holding a row's
+//              column-j entry forms its multiplier (l = a * (1 / p)) and hands it to the row's other three lanes by a
+//              shuffle; every live row updates its later columns from the winner's posted row (a - l u).
+// Rows never move: a row pivoted at step j is tagged j.  Once a group of four columns is final (after its last step) it
+// leaves the registers for the shared-memory copy of the block and the others shift down, so that the register indices
+// are compile-time constants in a loop that is not unrolled.  The arithmetic per entry and the pivots are those of
+// k_front_lu2.
+constexpr int LU4_THREADS = 512, LU4_NR = 128, LU4_NP = 64, LU4_M = 16, LU4_W = 16;
 
 template <typename T> struct Lu4Cand {
     unsigned long long key;    // pivot key (0: no candidate)
@@ -1252,10 +1255,10 @@ template <typename T> struct Lu4Cand {
     int pad[3];
 };
 
-// dynamic shared memory: the staged block (reused for the output), row ids, thresholds and their keys
+// dynamic shared memory: the staged block (reused for the output), row ids, thresholds and their keys, the final order
 static inline size_t front_lu4_smem(int64_t nrows, int64_t npiv, int64_t vs)
 {
-    return (size_t)(nrows * npiv * vs + nrows * 8 + npiv * 16);
+    return (size_t)(nrows * npiv * vs + nrows * 8 + npiv * 16 + nrows * 4);
 }
 
 template <typename T>
@@ -1269,37 +1272,40 @@ __device__ __forceinline__ void front_lu4_body(const T *__restrict__ W, int64_t 
     int64_t *rid = reinterpret_cast<int64_t *>(A + (size_t)npiv * nrows);
     double *thr = reinterpret_cast<double *>(rid + nrows);         // npiv: pivot_rel * max |B(:, column)|
     unsigned long long *thk = reinterpret_cast<unsigned long long *>(thr + npiv);   // the key of 2 thr
-    __shared__ Lu4Cand<T> cand[4];
-    __shared__ T ubuf[LU4_NP], lbuf[LU4_NR];
-    __shared__ int wcnt[4], s_stop;
+    int *sperm = reinterpret_cast<int *>(thk + npiv);              // final position -> block row
+    __shared__ Lu4Cand<T> cand[2][LU4_W];
+    __shared__ T rowbuf[2][LU4_W][LU4_NP];
+    __shared__ int wcnt[LU4_W], s_stop;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int g = warp >> 2, wr = warp & 3, i = wr * 32 + lane;
+    const int q = lane & 3, i = 8 * warp + (lane >> 2);
     if (tid == 0) s_stop = st->code != 0;                          // an earlier front stopped the factorization
     stage_pivot_block<T>(A, rid, W, ld, nrows, npiv, rowid, pa, tid, LU4_THREADS);
     for (int c = tid; c < npiv; c += LU4_THREADS) {
         thr[c] = pivot_rel * colmax[fcol + c];
         thk[c] = pivkey_of_modulus<T>(2.0 * thr[c]);
     }
-    for (int c = tid; c < LU4_NP; c += LU4_THREADS) ubuf[c] = VT<T>::zero();
+    for (int e = tid; e < 2 * LU4_W * LU4_NP; e += LU4_THREADS) (&rowbuf[0][0][0])[e] = VT<T>::zero();
     __syncthreads();
     if (s_stop) return;
     T a[LU4_M];
 #pragma unroll
     for (int m = 0; m < LU4_M; m++) {
-        const int c = g + LU4_G * m;
+        const int c = q + 4 * m;
         a[m] = i < nrows && c < npiv ? A[c * nrows + i] : VT<T>::zero();
     }
     const long long myrid = i < nrows ? (long long)rid[i] : LLONG_MAX;
     bool live = i < nrows;                                         // not pivoted yet
     int mytag = INT_MAX;                                           // the step at which this row was pivoted
-    // the warp's candidate for a column (x: this lane's entry, ok: the row is a candidate) into cand[wr]
-    auto post = [&](T x, bool ok) {
-        const unsigned long long key = ok ? pivkey(x) : 0ull;
+    int base = 0;                                                  // groups of four columns retired from the registers
+    // the warp's candidate for column 4 base + cq (this lane's entry a[0] when q == cq) and its row, into parity par
+    auto post = [&](int par, int cq) {
+        const T x = a[0];
+        const unsigned long long key = live && q == cq ? pivkey(x) : 0ull;
         const T xinv = key != 0ull ? recip(x) : VT<T>::zero();
         const unsigned long long mk = warp_max_key(key);
         unsigned cnd = __ballot_sync(0xffffffffu, key != 0ull && key == mk);
         if (cnd == 0u) {
-            if (lane == 0) { cand[wr].key = 0ull; cand[wr].rid = LLONG_MAX; cand[wr].row = -1; }
+            if (lane == 0) { cand[par][warp].key = 0ull; cand[par][warp].rid = LLONG_MAX; cand[par][warp].row = -1; }
             return;
         }
         if ((cnd & (cnd - 1u)) != 0u) {
@@ -1307,90 +1313,93 @@ __device__ __forceinline__ void front_lu4_body(const T *__restrict__ W, int64_t 
             for (int o = 16; o > 0; o >>= 1) { const long long t = __shfl_xor_sync(0xffffffffu, r2, o); r2 = t < r2 ? t : r2; }
             cnd = __ballot_sync(0xffffffffu, ((cnd >> lane) & 1u) && myrid == r2);
         }
-        if (lane == __ffs(cnd) - 1) {
-            cand[wr].key = mk; cand[wr].rid = myrid; cand[wr].val = x; cand[wr].inv = xinv; cand[wr].row = i;
+        const int wl = __ffs(cnd) - 1;
+        if (lane == wl) {
+            cand[par][warp].key = mk; cand[par][warp].rid = myrid; cand[par][warp].val = x; cand[par][warp].inv = xinv;
+            cand[par][warp].row = i;
         }
-    };
-    if (g == 0) post(a[0], live);
-    __syncthreads();
-#pragma unroll
-    for (int jj = 0; jj < LU4_M; jj++) {
-        for (int gg = 0; gg < LU4_G; gg++) {
-            const int j = LU4_G * jj + gg;
-            if (j >= npiv) goto done;
-            // B: the winner of column j (every thread the same), the stop decision, the multipliers and the pivot row
-            int bs = 0;
-            unsigned long long bk = cand[0].key;
-            long long br = cand[0].rid;
-#pragma unroll
-            for (int s = 1; s < 4; s++) {
-                const unsigned long long k = cand[s].key;
-                const long long r = cand[s].rid;
-                if (k > bk || (k == bk && r < br)) { bk = k; br = r; bs = s; }
-            }
-            const int bi = cand[bs].row;
-            const T pv = cand[bs].val, inv = cand[bs].inv;
-            {
-                // the singular test of the reference (FPLUS src/factor_sn_panel.inc:232-233): no candidate, a zero
-                // modulus, or a modulus below pivot_rel * max |B(:, column)| (the modulus itself only near it)
-                int stop = 0;
-                if (bi < 0 || bk == 0ull || (bk < thk[j] && vabs(pv) < thr[j])) stop = 1;
-                else if (bi >= nri) stop = 2;
-                if (stop) {
-                    if (tid == 0) {
-                        if (stop == 1) set_status(st, ST_SINGULAR, fcol + j, bi >= 0 ? vabs(pv) : 0.0, thr[j]);
-                        else set_status(st, ST_BORDER, front, vabs(pv), thr[j]);
-                    }
-                    return;                                      // every thread leaves here
-                }
-            }
-            const bool piv = i == bi;
-            if (piv) { mytag = j; live = false; }
-            if (g == gg && live) { const T l = mul(a[jj], inv); a[jj] = l; lbuf[i] = l; }
-            if (piv) {
-#pragma unroll
-                for (int m = jj; m < LU4_M; m++)
-                    if (m > jj || g > gg) ubuf[g + LU4_G * m] = a[m];
-            }
-            __syncthreads();
-            // C: the update of every live row; the warps of column j + 1 post its candidates once it is updated
-            const T l = g == gg ? a[jj] : (live ? lbuf[i] : VT<T>::zero());
-            if (live && g > gg) a[jj] = sub(a[jj], mul(l, ubuf[g + LU4_G * jj]));
-            if (jj + 1 < LU4_M && live) a[jj + 1] = sub(a[jj + 1], mul(l, ubuf[g + LU4_G * (jj + 1)]));
-            if (j + 1 < npiv && g == ((gg + 1) & 3)) post(gg == 3 ? a[jj + 1 < LU4_M ? jj + 1 : jj] : a[jj], live);
-            if (live) {
-#pragma unroll
-                for (int m = jj + 2; m < LU4_M; m++) a[m] = sub(a[m], mul(l, ubuf[g + LU4_G * m]));
-            }
-            __syncthreads();
-        }
-    }
-done:
-    // the final order: pivot rows at their step, the others after them in block order
-    {
-        const bool un = i < nrows && mytag == INT_MAX;
-        const unsigned bal = __ballot_sync(0xffffffffu, un);
-        if (g == 0 && lane == 0) wcnt[wr] = __popc(bal);
-        __syncthreads();
-        int base = npiv;
-        for (int w = 0; w < wr; w++) base += wcnt[w];
-        const int k = un ? base + __popc(bal & ((1u << lane) - 1u)) : mytag;
-        if (i < nrows) {
+        if ((lane >> 2) == (wl >> 2)) {                             // the candidate row's four lanes post its entries
 #pragma unroll
             for (int m = 0; m < LU4_M; m++) {
-                const int c = g + LU4_G * m;
-                if (c < npiv) A[c * nrows + k] = a[m];
-            }
-            if (g == 0) {
-                perm[k] = i;
-                rowid[k] = myrid;
-                if (k < npiv) p_lu[fcol + k] = myrid;
+                const int c = q + 4 * (m + base);
+                if (m + base < LU4_M && c < npiv) rowbuf[par][warp][c] = a[m];
             }
         }
+    };
+    if (npiv > 0) post(0, 0);
+    for (int j = 0; j < npiv; j++) {
+        const int par = j & 1, qj = j & 3;
+        __syncthreads();                                           // the candidates of column j are posted
+        // the winner: lane s % 16 reads candidate s; the largest key, ties to the smaller row of B
+        const unsigned long long ck = cand[par][lane & 15].key;
+        const long long cr = cand[par][lane & 15].rid;
+        const unsigned long long bk = warp_max_key(ck);
+        unsigned cw = __ballot_sync(0xffffffffu, ck != 0ull && ck == bk);
+        if (cw != 0u && (cw & (cw - 1u) & 0xffffu) != 0u) {
+            long long r2 = (cw >> lane) & 1u ? cr : LLONG_MAX;
+            for (int o = 16; o > 0; o >>= 1) { const long long t = __shfl_xor_sync(0xffffffffu, r2, o); r2 = t < r2 ? t : r2; }
+            cw = __ballot_sync(0xffffffffu, ((cw >> lane) & 1u) && cr == r2);
+        }
+        const int bw = cw != 0u ? (__ffs(cw) - 1) & 15 : 0;
+        const int bi = cw != 0u ? cand[par][bw].row : -1;
+        const T pv = cand[par][bw].val, inv = cand[par][bw].inv;
+        {
+            // the singular test of the reference (FPLUS src/factor_sn_panel.inc:232-233): no candidate, a zero modulus,
+            // or a modulus below pivot_rel * max |B(:, column)| (the modulus itself only near it)
+            int stop = 0;
+            if (bi < 0 || bk == 0ull || (bk < thk[j] && vabs(pv) < thr[j])) stop = 1;
+            else if (bi >= nri) stop = 2;
+            if (stop) {
+                if (tid == 0) {
+                    if (stop == 1) set_status(st, ST_SINGULAR, fcol + j, bi >= 0 ? vabs(pv) : 0.0, thr[j]);
+                    else set_status(st, ST_BORDER, front, vabs(pv), thr[j]);
+                }
+                return;                                          // every thread leaves here
+            }
+        }
+        const T l = shfl_v<T>(mul(a[0], inv), (lane & ~3) | qj);     // this row's multiplier (from its column-j lane)
+        if (i == bi) { mytag = j; live = false; }
+        if (live) {
+            const T *u = rowbuf[par][bw];
+            if (q == qj) a[0] = l;                                 // the entry of L
+            else if (q > qj) a[0] = sub(a[0], mul(l, u[q + 4 * base]));
+#pragma unroll
+            for (int m = 1; m < LU4_M; m++)
+                if (m + base < LU4_M) a[m] = sub(a[m], mul(l, u[q + 4 * (m + base)]));
+        }
+        if (qj == 3) {                                             // columns 4 base .. 4 base + 3 are final
+            const int c = q + 4 * base;
+            if (i < nrows && c < npiv) A[c * nrows + i] = a[0];
+#pragma unroll
+            for (int m = 0; m + 1 < LU4_M; m++) a[m] = a[m + 1];
+            a[LU4_M - 1] = VT<T>::zero();
+            base++;
+        }
+        if (j + 1 < npiv) post(par ^ 1, (j + 1) & 3);
+    }
+    // the columns still in registers to the shared copy; the final order: pivot rows at their step, the others after them
+    // in block order
+#pragma unroll
+    for (int m = 0; m < LU4_M; m++) {
+        const int c = q + 4 * (m + base);
+        if (m + base < LU4_M && i < nrows && c < npiv) A[c * nrows + i] = a[m];
+    }
+    const bool un = i < nrows && mytag == INT_MAX;
+    const unsigned bal = __ballot_sync(0xffffffffu, un && q == 0);
+    if (lane == 0) wcnt[warp] = __popc(bal);
+    __syncthreads();
+    int k0 = npiv;
+    for (int w = 0; w < warp; w++) k0 += wcnt[w];
+    const int k = un ? k0 + __popc(bal & ((1u << lane) - 1u)) : mytag;
+    if (q == 0 && i < nrows) {
+        sperm[k] = i;
+        perm[k] = i;
+        rowid[k] = myrid;
+        if (k < npiv) p_lu[fcol + k] = myrid;
     }
     __syncthreads();
     const int ne = npiv * nrows;
-    for (int e = tid; e < ne; e += LU4_THREADS) Lout[e] = A[e];
+    for (int e = tid; e < ne; e += LU4_THREADS) { const int kk = e % nrows, c = e / nrows; Lout[e] = A[c * nrows + sperm[kk]]; }
 }
 
 template <typename T>
@@ -1873,6 +1882,279 @@ __global__ void __launch_bounds__(FT_THREADS) k_front_tail(const T *__restrict__
                                                            const DevStatus *st)
 {
     front_tail_body<T, TN>(W, ld, perm, npiv, nrows, ncb, cb0, cb1, Lb, U, CB, st, (int)blockIdx.x, (int)gridDim.x);
+}
+
+// d += a b on the FP64 tensor cores (mma m8n8k4), free for the compiler to schedule
+__device__ __forceinline__ void dmma_s(double &d0, double &d1, double a, double b)
+{
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n" : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
+// The tail's multipliers with the diagonal blocks folded in, formed in shared memory from the front's L block (sL: L[m, k]
+// at k * FT_LD + m): for each 16-column block b of the pivot columns (rows and columns [16b, 16b + w)), D_b = L_bb^-1
+// (unit lower, zero above the diagonal) replaces the block's rows, and every row r below the block holds
+// M[r, block b] = L[r, block b] D_b.  Then the blocked forward substitution X_b <- D_b X_b, X_r -= L[r, b] X_b becomes, per
+// block, one product M[rows >= 16b, block b] X_b with no serial step: X_b = D_b X_b and X_r -= M[r, b] X_b.  Every thread of
+// the CTA (FT_THREADS) takes part; ends with a block barrier.
+template <bool CP>
+__device__ __forceinline__ void tail_prep_m(double *__restrict__ sLr, double *__restrict__ sLi, int npiv, int nrows, int tid)
+{
+    const int lane = tid & 31, warp = tid >> 5, half = lane >> 4, hl = lane & 15;
+    const int nbk = (npiv + 15) >> 4;
+    // (1) the columns of every D_b: the half-warp (warp, half) solves L_bb x = e for columns 2 warp + half and that + 32
+    // (both halves of a warp are in the same block, so the shuffles see the same trip count)
+    double dr[2], di[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const int c = 2 * warp + half + 32 * q, k0 = c & ~15, cb = c & 15;
+        const int w = npiv - k0 < 16 ? npiv - k0 : 16;
+        double xr = hl == cb ? 1.0 : 0.0, xi = 0.0;
+        for (int i = 0; i < w; i++) {
+            const double pr = __shfl_sync(0xffffffffu, xr, i, 16);
+            const double pi = CP ? __shfl_sync(0xffffffffu, xi, i, 16) : 0.0;
+            if (hl > i && hl < w) {
+                const double lr = sLr[(k0 + i) * FT_LD + k0 + hl];
+                if constexpr (CP) {
+                    const double li = sLi[(k0 + i) * FT_LD + k0 + hl];
+                    const cplx x = sub(cplx{xr, xi}, mul(cplx{lr, li}, cplx{pr, pi}));
+                    xr = x.x; xi = x.y;
+                } else xr = xr - lr * pr;
+            }
+        }
+        dr[q] = xr; di[q] = xi;
+    }
+    // (2) the products M[r, block b] = L[r, block b] D_b of the rows below each block (D_b read from the registers of
+    // step 1 through shared memory after the barrier): items (b, 8-row fragment), two 8-column fragments each, at most
+    // 14 + 12 + 10 + 8 = 44 items, three per warp
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const int c = 2 * warp + half + 32 * q, k0 = c & ~15, cb = c & 15;
+        const int w = npiv - k0 < 16 ? npiv - k0 : 16;
+        if (cb < w && hl < w) { sLr[(k0 + cb) * FT_LD + k0 + hl] = dr[q]; if constexpr (CP) sLi[(k0 + cb) * FT_LD + k0 + hl] = di[q]; }
+    }
+    __syncthreads();
+    int rs[4], nf[4], pre[5];
+    pre[0] = 0;
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+        const int k0 = 16 * b, w = b < nbk ? (npiv - k0 < 16 ? npiv - k0 : 16) : 0;
+        rs[b] = (k0 + w) & ~7;
+        nf[b] = b < nbk && nrows > k0 + w ? (nrows - rs[b] + 7) >> 3 : 0;
+        pre[b + 1] = pre[b] + nf[b];
+    }
+    double res[3][2][4];
+    int rb[3], rr0[3];
+#pragma unroll
+    for (int s = 0; s < 3; s++) {
+        const int p = warp + 16 * s;
+        rb[s] = -1;
+        if (p >= pre[4]) continue;                                   // warp-uniform
+        int b = 0, rsb = rs[0], preb = 0;
+#pragma unroll
+        for (int q = 1; q < 4; q++) if (p >= pre[q]) { b = q; rsb = rs[q]; preb = pre[q]; }
+        const int k0 = 16 * b, w = npiv - k0 < 16 ? npiv - k0 : 16;
+        const int r0 = rsb + 8 * (p - preb);
+        rb[s] = b; rr0[s] = r0;
+        const int am = r0 + (lane >> 2);
+#pragma unroll
+        for (int cf = 0; cf < 2; cf++) { res[s][cf][0] = res[s][cf][1] = res[s][cf][2] = res[s][cf][3] = 0.0; }
+        for (int ks = 0; ks < w; ks += 4) {
+            const int kk = ks + (lane & 3), k = k0 + kk;
+            const bool kin = kk < w;
+            const double ar = kin && am < nrows ? sLr[k * FT_LD + am] : 0.0;
+            const double ai = CP && kin && am < nrows ? sLi[k * FT_LD + am] : 0.0;
+#pragma unroll
+            for (int cf = 0; cf < 2; cf++) {
+                const int nn = 8 * cf + (lane >> 2);                    // column of D_b
+                const bool bok = kin && nn < w;
+                const double br = bok ? sLr[(k0 + nn) * FT_LD + k] : 0.0;
+                dmma_s(res[s][cf][0], res[s][cf][1], ar, br);
+                if constexpr (CP) {
+                    const double bi = bok ? sLi[(k0 + nn) * FT_LD + k] : 0.0;
+                    dmma_s(res[s][cf][0], res[s][cf][1], ai, -bi);
+                    dmma_s(res[s][cf][2], res[s][cf][3], ar, bi);
+                    dmma_s(res[s][cf][2], res[s][cf][3], ai, br);
+                }
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < 3; s++) {
+        if (rb[s] < 0) continue;
+        const int k0 = 16 * rb[s], w = npiv - k0 < 16 ? npiv - k0 : 16;
+        const int cr = rr0[s] + (lane >> 2);
+        if (cr < k0 + w || cr >= nrows) continue;
+#pragma unroll
+        for (int cf = 0; cf < 2; cf++) {
+            const int cc = 8 * cf + 2 * (lane & 3);
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                if (cc + h >= w) continue;
+                sLr[(k0 + cc + h) * FT_LD + cr] = res[s][cf][h];
+                if constexpr (CP) sLi[(k0 + cc + h) * FT_LD + cr] = res[s][cf][2 + h];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Where a front's tail writes its contribution block: the stack (W null), or straight into its parent's working block W
+// (leading dimension ld): CB row t to parent row slot + t (t < nslot) or tau_base + t - nslot, CB column c to parent column
+// relcol[c]; the parent's first `slot` rows (its entering rows) of those columns are written as zeros.
+struct TailOut {
+    void *W;
+    int64_t ld, nslot, slot, tau_base;
+    const int64_t *relcol;
+};
+
+// The tail of a front with npiv <= 64 and nrows <= 128 (the successor of front_tail_body): the same U12 and contribution
+// block, X = [L11; L21]-forward-substitution of the gathered columns A[perm, npiv + c], with the multipliers M of
+// tail_prep_m (formed once per CTA): per tile of TN columns and per 16-column block b of the pivots, one FP64 tensor-core
+// product over the rows at and below the block (warp w takes rows 16b + 8w .. + 7 and every column of the tile, so the
+// M fragment is loaded once for all of them): rows below the block leave as X_r -= M[r, b] X_b at once, the block's own
+// rows as X_b = D_b X_b after the block barrier (no later block reads them).  One barrier per pivot block, no serial
+// diagonal solve.
+template <typename T, int TN>
+__device__ __forceinline__ void front_tail2_body(const T *__restrict__ W, int64_t ld, const int *__restrict__ perm, int npiv,
+                                                 int nrows, int64_t ncb, int64_t cb0, int64_t cb1, const T *__restrict__ Lb,
+                                                 T *__restrict__ U, T *__restrict__ CB, const DevStatus *st, int bid, int nbk,
+                                                 const TailOut &to)
+{
+    constexpr bool CP = VT<T>::cplx_;
+    constexpr int PER = FT_NR * TN / FT_THREADS;                   // tile values per thread
+    constexpr int NCF = TN / 8;                                     // 8-column fragments per tile
+    extern __shared__ __align__(16) double ft_smem[];
+    double *sLr = ft_smem;                                          // M[m, k] at k * FT_LD + m
+    double *sLi = sLr + (CP ? FT_NP * FT_LD : 0);
+    double *sXr = sLr + (CP ? 2 : 1) * FT_NP * FT_LD;               // X[r, c] at c * FT_LD + r
+    double *sXi = sXr + (CP ? TN * FT_LD : 0);
+    __shared__ int sperm[FT_NR];
+    pdl_trigger();                                   // the next pivot block's LU may start its own set-up
+    if (st->code) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int M = nrows - npiv;
+    for (int i = tid; i < nrows; i += FT_THREADS) sperm[i] = perm[i];
+    __syncthreads();
+    const int64_t t0 = cb0 / TN, ntile = (cb1 + TN - 1) / TN;
+    T pre[PER];
+    auto fetch = [&](int64_t t) {
+        const int64_t c0 = t * TN;
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            const int e = tid + q * FT_THREADS, r = e % FT_NR, c = e / FT_NR;
+            pre[q] = (t < ntile && r < nrows && c0 + c < cb1) ? W[sperm[r] + (npiv + c0 + c) * ld] : VT<T>::zero();
+        }
+    };
+    if (t0 + bid < ntile) fetch(t0 + bid);                          // in flight while M is formed
+    for (int e0 = tid; e0 < npiv * nrows; e0 += 8 * FT_THREADS) {     // 8 loads in flight per thread
+        T v[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) { const int e = e0 + q * FT_THREADS; v[q] = e < npiv * nrows ? Lb[e] : VT<T>::zero(); }
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int e = e0 + q * FT_THREADS, m = e % nrows, k = e / nrows;
+            if (e < npiv * nrows) {
+                if constexpr (CP) { sLr[k * FT_LD + m] = v[q].x; sLi[k * FT_LD + m] = v[q].y; } else sLr[k * FT_LD + m] = v[q];
+            }
+        }
+    }
+    __syncthreads();
+    tail_prep_m<CP>(sLr, sLi, npiv, nrows, tid);
+    const int nb16 = (npiv + 15) >> 4;
+    for (int64_t t = t0 + bid; t < ntile; t += nbk) {
+        const int64_t c0 = t * TN;
+        const int tn = (int)(cb1 - c0 < TN ? cb1 - c0 : TN);
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            const int e = tid + q * FT_THREADS, r = e % FT_NR, c = e / FT_NR;
+            if constexpr (CP) { sXr[c * FT_LD + r] = pre[q].x; sXi[c * FT_LD + r] = pre[q].y; } else sXr[c * FT_LD + r] = pre[q];
+        }
+        __syncthreads();
+        fetch(t + nbk);                                       // in flight during this tile
+        for (int b = 0; b < nb16; b++) {
+            const int k0 = 16 * b, w = npiv - k0 < 16 ? npiv - k0 : 16;
+            const int r0 = k0 + 8 * warp;                            // this warp's 8 rows
+            const bool act = r0 < nrows;                             // warp-uniform
+            double acc[NCF][4];
+#pragma unroll
+            for (int cf = 0; cf < NCF; cf++) acc[cf][0] = acc[cf][1] = acc[cf][2] = acc[cf][3] = 0.0;
+            const int am = r0 + (lane >> 2);
+            if (act) {
+                for (int ks = 0; ks < w; ks += 4) {
+                    const int kk = ks + (lane & 3), k = k0 + kk;
+                    const bool kin = kk < w;
+                    const double ar = kin && am < nrows ? sLr[k * FT_LD + am] : 0.0;
+                    const double ai = CP && kin && am < nrows ? sLi[k * FT_LD + am] : 0.0;
+#pragma unroll
+                    for (int cf = 0; cf < NCF; cf++) {
+                        const int bn = 8 * cf + (lane >> 2);
+                        const double br = kin ? sXr[bn * FT_LD + k] : 0.0;
+                        dmma_s(acc[cf][0], acc[cf][1], ar, br);
+                        if constexpr (CP) {
+                            const double bi = kin ? sXi[bn * FT_LD + k] : 0.0;
+                            dmma_s(acc[cf][0], acc[cf][1], ai, -bi);
+                            dmma_s(acc[cf][2], acc[cf][3], ar, bi);
+                            dmma_s(acc[cf][2], acc[cf][3], ai, br);
+                        }
+                    }
+                }
+            }
+            // the output fragment: row cr, columns cc and cc + 1 of each 8-column fragment
+            const int cr = r0 + (lane >> 2);
+            const bool yrow = cr < k0 + w;                           // a row of block b: X_b = D_b X_b after the barrier
+            if (act && !yrow && cr < nrows) {
+#pragma unroll
+                for (int cf = 0; cf < NCF; cf++) {
+                    const int cc = 8 * cf + 2 * (lane & 3);
+                    sXr[cc * FT_LD + cr] -= acc[cf][0];
+                    sXr[(cc + 1) * FT_LD + cr] -= acc[cf][1];
+                    if constexpr (CP) { sXi[cc * FT_LD + cr] -= acc[cf][2]; sXi[(cc + 1) * FT_LD + cr] -= acc[cf][3]; }
+                }
+            }
+            __syncthreads();
+            if (act && yrow && cr < nrows) {
+#pragma unroll
+                for (int cf = 0; cf < NCF; cf++) {
+                    const int cc = 8 * cf + 2 * (lane & 3);
+                    sXr[cc * FT_LD + cr] = acc[cf][0];
+                    sXr[(cc + 1) * FT_LD + cr] = acc[cf][1];
+                    if constexpr (CP) { sXi[cc * FT_LD + cr] = acc[cf][2]; sXi[(cc + 1) * FT_LD + cr] = acc[cf][3]; }
+                }
+            }
+        }
+        __syncthreads();
+        T *Wo = reinterpret_cast<T *>(to.W);
+        for (int e = tid; e < nrows * tn; e += FT_THREADS) {
+            const int r = e % nrows, c = e / nrows;
+            T v;
+            if constexpr (CP) v = T{sXr[c * FT_LD + r], sXi[c * FT_LD + r]}; else v = sXr[c * FT_LD + r];
+            if (r < npiv) U[r + (c0 + c) * (int64_t)npiv] = v;
+            else if (!Wo) CB[(r - npiv) + (c0 + c) * (int64_t)M] = v;
+            else {
+                const int64_t t = r - npiv, pr = t < to.nslot ? to.slot + t : to.tau_base + (t - to.nslot);
+                Wo[pr + to.relcol[c0 + c] * to.ld] = v;
+            }
+        }
+        if (Wo) {
+            const int sl = (int)to.slot;
+            for (int e = tid; e < sl * tn; e += FT_THREADS) {
+                const int r = e % sl, c = e / sl;
+                Wo[r + to.relcol[c0 + c] * to.ld] = VT<T>::zero();
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, int TN>
+__global__ void __launch_bounds__(FT_THREADS) k_front_tail2(const T *__restrict__ W, int64_t ld, const int *__restrict__ perm,
+                                                            int npiv, int nrows, int64_t ncb, int64_t cb0, int64_t cb1,
+                                                            const T *__restrict__ Lb, T *__restrict__ U, T *__restrict__ CB,
+                                                            const DevStatus *st, TailOut to)
+{
+    front_tail2_body<T, TN>(W, ld, perm, npiv, nrows, ncb, cb0, cb1, Lb, U, CB, st, (int)blockIdx.x, (int)gridDim.x, to);
 }
 
 // X <- L^-1 X for a unit lower w x w block (w <= 32 RPL) and every column of X (rows [0, w) of each column, ld ldx):
@@ -3628,6 +3910,23 @@ __global__ void __launch_bounds__(FT_THREADS) k_bat_tail(const FcFront *__restri
     const int nbk = (int)(gridDim.x < ntile ? gridDim.x : ntile);
     front_tail_body<T, TN>(Wbase + F.wofs, F.nr, permall + F.row_off, (int)F.np, (int)F.nr, ncb, 0, ncb, La + F.L_off,
                            Ua + F.U_off, CBA + F.cbofs, st, (int)blockIdx.x, nbk);
+}
+
+// the same with the tail of k_front_tail2 (blockIdx.y: the front; blockIdx.x: its CTAs over the
+// 32-column tiles; the body of k_front_tail2)
+template <typename T, int TN>
+__global__ void __launch_bounds__(FT_THREADS) k_bat_tail2(const FcFront *__restrict__ fc, const int *__restrict__ list,
+                                                         const T *__restrict__ Wbase, const int *__restrict__ permall,
+                                                         const T *__restrict__ La, T *__restrict__ Ua, T *__restrict__ CBA,
+                                                         const DevStatus *st)
+{
+    const FcFront F = fc[list[blockIdx.y]];
+    const int64_t ncb = F.nc - F.np;
+    const int64_t ntile = (ncb + TN - 1) / TN;
+    if (ncb <= 0 || blockIdx.x >= ntile) return;
+    const int nbk = (int)(gridDim.x < ntile ? gridDim.x : ntile);
+    front_tail2_body<T, TN>(Wbase + F.wofs, F.nr, permall + F.row_off, (int)F.np, (int)F.nr, ncb, 0, ncb, La + F.L_off,
+                            Ua + F.U_off, CBA + F.cbofs, st, (int)blockIdx.x, nbk, TailOut{});
 }
 
 }  // namespace fpl

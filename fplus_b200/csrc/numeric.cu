@@ -528,7 +528,7 @@ static int run_equil(const DevPlan &D, DevNum &N, int equilibrate, int max_iter,
 
 // ---------------------------------------------------------------------------------------------------------------------
 // the fronts, in order.  Returns FPLUS_OK, or ST_BORDER through *border_front (>= 0) for a restart with a dense chain.
-static size_t front_lu_smem(int64_t nrows, int64_t npiv, int64_t vs) { return (size_t)(nrows * npiv * vs + nrows * (2 * vs + 16) + npiv * 8); }
+static size_t front_lu_smem(int64_t nrows, int64_t npiv, int64_t vs) { return (size_t)(nrows * npiv * vs + nrows * (2 * vs + 16) + npiv * 16); }
 // k_front_lu3: the block, two panels of masked multipliers, row ids, tags, positions, thresholds and pivot rows
 static size_t front_lu3_smem(int64_t nrows, int64_t npiv, int64_t vs)
 {
@@ -562,8 +562,9 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     static thread_local int attr_set = 0;
     if (!attr_set) {
         CK(cudaFuncSetAttribute(k_front_lu2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
-        CK(cudaFuncSetAttribute(k_front_lu4<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
-        CK(cudaFuncSetAttribute(k_bat_lu4<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        // (k_front_lu4 has 35 KB of static shared memory beside its block: the opt-in is its largest block's need)
+        CK(cudaFuncSetAttribute(k_front_lu4<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_lu4_smem(LU4_NR, LU4_NP, sizeof(T))));
+        CK(cudaFuncSetAttribute(k_bat_lu4<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_lu4_smem(LU4_NR, LU4_NP, sizeof(T))));
         CK(cudaFuncSetAttribute(k_front_lu3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
@@ -572,6 +573,8 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         CK(cudaFuncSetAttribute(k_front_tail<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_bat_lu2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_bat_tail<T, FT_TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_front_tail2<T, FT_TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
+        CK(cudaFuncSetAttribute(k_bat_tail2<T, FT_TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         attr_set = 1;
     }
     // (captured: the status was cleared where the captured equilibration began, and must keep what it reported)
@@ -664,6 +667,22 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         }
     }
     cudaStream_t A = N.crit;
+    // A pipelined front whose parent is the next pipelined front, takes no other child, and whose contribution block has
+    // the parent's every column and every row but its entering rows: the bulk of its tail (the columns after the ones
+    // the parent's pivot block takes from the stack) writes straight into the parent's working block, the other of the
+    // two, entering rows as zeros; the parent then adds only its original entries to those columns (part 4).
+    std::vector<char> pdirect((size_t)nf, 0);
+    if (any_pipe && !(N.lu_variant & 48)) {
+        for (int64_t fi = 0; fi + 1 < nf; fi++) {
+            const Front &F = P.fronts[(size_t)fi], &Q = P.fronts[(size_t)fi + 1];
+            if (!pipe[(size_t)fi] || !pipe[(size_t)fi + 1] || F.parent != fi + 1 || Q.child_end - Q.child_begin != 1) continue;
+            const int64_t np = F.npiv, M = F.nrows - np, ncb = F.ncols - np, nslot = std::max<int64_t>(0, F.nri - np);
+            const int64_t h = std::min<int64_t>(ncb, (hc[(size_t)fi] + FT_TN - 1) / FT_TN * FT_TN);
+            if (M <= 0 || h != hc[(size_t)fi] || h >= ncb || ncb != Q.ncols || hc[(size_t)fi] != Q.npiv) continue;
+            if (F.slot + nslot != Q.tau_base || M - nslot != Q.nrows - Q.tau_base) continue;
+            pdirect[(size_t)fi] = 1;
+        }
+    }
 
     // the batched fronts (variant + 8 or the blocked small-front LU turn them off): their contribution blocks live in
     // their own arena
@@ -678,11 +697,21 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
 
     // the assembly of columns [0, npiv) (part 1), the others (part 2), or all (part 0)
     // (part 3: every column, with the single child's contribution block already written into W by its Schur update and
-    // the entering rows zeroed: the original entries add to it, the child gives its row ids only)
+    // the entering rows zeroed: the original entries add to it, the child gives its row ids only; part 4: the same for
+    // the columns of part 2, written by the child's tail)
     auto assemble = [&](int64_t fi, T *W, cudaStream_t st, int part) {
         const Front &F = P.fronts[fi];
         const int64_t nr = F.nrows, nc = F.ncols, np = F.npiv, ld = nr;
-        const bool pre = part == 3;
+        const bool pre = part == 3 || part == 4;
+        if (part == 4) {
+            const int64_t e0 = F.asm_mid, cnt = F.asm_end - F.asm_mid;
+            prof.begin(st, PROF_ASM, 0.0, (double)(2 * cnt) * vs);
+            if (cnt > 0)
+                k_assemble<T><<<nblk(cnt), 256, 0, st>>>(W, Bx, D.asm_src + e0, D.asm_dst + e0, cnt, N.rowid + F.row_off,
+                                                         D.rowinit + F.row_off, 0, N.st, 1), note_launch();
+            prof.end(st);
+            return FPLUS_OK;
+        }
         const int64_t e0 = part == 2 ? F.asm_mid : F.asm_begin, e1 = part == 1 ? F.asm_mid : F.asm_end;
         const int64_t z0 = part == 2 ? nr * np : 0, z1 = pre ? 0 : part == 1 ? nr * np : nr * nc;
         prof.begin(st, PROF_ASM, 0.0, (double)((z1 - z0) + 2 * (e1 - e0)) * vs);
@@ -824,7 +853,8 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         return FPLUS_OK;
     };
     // U12 and the CB for CB columns [c0, c1) by the fused tail kernel (at most `cap` CTAs)
-    auto tail = [&](int64_t fi, T *W, const int *perm, cudaStream_t st, int64_t c0, int64_t c1, int cap, bool narrow) {
+    auto tail = [&](int64_t fi, T *W, const int *perm, cudaStream_t st, int64_t c0, int64_t c1, int cap, bool narrow,
+                    const TailOut &to = TailOut{}) {
         const Front &F = P.fronts[fi];
         const int64_t nr = F.nrows, np = F.npiv, ncb = F.ncols - F.npiv, M = nr - np;
         if (c1 <= c0) return FPLUS_OK;
@@ -833,7 +863,12 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         const int tn = narrow ? 8 : FT_TN;
         const size_t fsm = (size_t)(VT<T>::cplx_ ? 2 : 1) * (FT_NP + tn) * FT_LD * sizeof(double);
         const int blocks = (int)std::min<int64_t>((c1 - c0 + tn - 1) / tn, cap);
-        if (narrow)
+        // (the narrow tiles of a pipelined front's head, which the next pivot block waits for, by forward substitution:
+        // eight CTAs, each forming the block-inverse multipliers first, would take longer)
+        if (!(N.lu_variant & 16) && !narrow)
+            k_front_tail2<T, FT_TN><<<blocks, FT_THREADS, fsm, st>>>(W, nr, perm, (int)np, (int)nr, ncb, c0, c1, La + F.L_off,
+                                                                    Ua + F.U_off, CB + F.cb_off, N.st, to), note_launch();
+        else if (narrow)
             k_front_tail<T, 8><<<blocks, FT_THREADS, fsm, st>>>(W, nr, perm, (int)np, (int)nr, ncb, c0, c1, La + F.L_off,
                                                                Ua + F.U_off, CB + F.cb_off, N.st), note_launch();
         else
@@ -872,8 +907,11 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             prof.end(s);
             if (D.bs_maxtiles[(size_t)lv] > 0) {
                 prof.begin(s, PROF_SCHUR, fm * D.bs_tail_flops[(size_t)lv], D.bs_tail_bytes[(size_t)lv] * (double)vs);
-                k_bat_tail<T, FT_TN><<<dim3((unsigned)std::min<int64_t>(D.bs_maxtiles[(size_t)lv], 148), cnt), FT_THREADS, fsm, s>>>(
-                    D.fc, bl, Wb, N.permall, La, Ua, CBA, N.st), note_launch();
+                const dim3 tg((unsigned)std::min<int64_t>(D.bs_maxtiles[(size_t)lv], 148), cnt);
+                if (!(N.lu_variant & 16))
+                    k_bat_tail2<T, FT_TN><<<tg, FT_THREADS, fsm, s>>>(D.fc, bl, Wb, N.permall, La, Ua, CBA, N.st), note_launch();
+                else
+                    k_bat_tail<T, FT_TN><<<tg, FT_THREADS, fsm, s>>>(D.fc, bl, Wb, N.permall, La, Ua, CBA, N.st), note_launch();
                 prof.end(s);
             }
         }
@@ -944,12 +982,22 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             if ((rc = factor_block(fi, W, perm, A, pa))) return rc;
             CK(cudaEventRecord(N.ev_lu, A));
             if (ncb > 0) {
-                if ((rc = assemble(fi, W, s, 2))) return rc;
+                if ((rc = assemble(fi, W, s, fi > 0 && pdirect[(size_t)fi - 1] ? 4 : 2))) return rc;
                 CK(cudaEventRecord(N.ev_head, s));
                 CK(cudaStreamWaitEvent(s, N.ev_lu, 0));
                 const int64_t h = std::min<int64_t>(ncb, (hc[fi] + FT_TN - 1) / FT_TN * FT_TN);
+                TailOut to{};
+                if (pdirect[(size_t)fi]) {
+                    const Front &Q = P.fronts[(size_t)fi + 1];
+                    to.W = wsel ? N.work2 : N.work;                    // the parent's working block (the next in turn)
+                    to.ld = Q.nrows;
+                    to.nslot = std::max<int64_t>(0, F.nri - np);
+                    to.slot = F.slot;
+                    to.tau_base = Q.tau_base;
+                    to.relcol = D.relcol + F.relcol_off;
+                }
                 // at most 139 CTAs: one SM stays free for the next LU and eight for the next tail head
-                if ((rc = tail(fi, W, perm, s, h, ncb, 139, false))) return rc;
+                if ((rc = tail(fi, W, perm, s, h, ncb, 139, false, to))) return rc;
                 CK(cudaStreamWaitEvent(A, N.ev_head, 0));
                 if ((rc = tail(fi, W, perm, A, 0, h, 148, true))) return rc;
             }

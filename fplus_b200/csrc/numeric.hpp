@@ -107,9 +107,12 @@ struct DevNum {
     int prec = 0;
     void *coopbuf = nullptr;       // the multi-CTA pivot-block LU: the CTAs' posts, the ticket, the choices, U12, row scratch
     size_t cap_coop = 0;
-    int lu_variant = 1;            // the small fronts' pivot-block LU (1: k_front_lu4, 2: k_front_lu2, 3: k_front_lu3); + 4: the tall
+    int lu_variant = 2;            // the small fronts' pivot-block LU (2: k_front_lu2, 1: k_front_lu4, 3: k_front_lu3); + 4: the tall
                                    // blocks by one CTA per 32-column panel instead of k_block_lu_mc; + 8: no batched
-                                   // fronts (every front on its own)
+                                   // fronts (every front on its own); + 16: the small fronts' tails by forward
+                                   // substitution (k_front_tail) instead of the block-inverse products (k_front_tail2);
+                                   // + 32: the pipelined chain's contribution blocks through the stack and the
+                                   // extend-add instead of straight into the parent's working block
     int capture = 0;               // the launches are being captured into a CUDA graph: no host copies, waits or decisions
     void *gm_buf = nullptr;        // GMRES-IR: the Krylov basis and its vectors
     size_t cap_gm = 0;

@@ -151,11 +151,13 @@ int fplus_b200_autotune(fplus_symbolic *sym, const int64_t *Ap, const int64_t *A
 
 /* The front shape of every later factorization on sym, chosen by the caller instead of the autotuner: at most max_width
  * pivot columns per front (16 .. 4096), nb_chain pivots per dense-chain front (8 .. 64), and the pivot-block LU of the
- * small fronts (1: the block in registers, the default; 2: the block in shared memory, one barrier per pivot step;
- * 3: blocked 8-column panels), plus 4 to pivot the pivot blocks too large
- * for one CTA by one CTA per 32-column panel instead of all SMs in one launch, plus 8 to factor every front on its own
- * instead of the small fronts at the bottom of the tree level by level (variant 3 also turns that off).  The pivots do
- * not depend on these.  No counterpart in FPLUS. */
+ * small fronts (2: the block in shared memory, one barrier per pivot step, the default; 1: the block in registers;
+ * 3: blocked 8-column panels), plus 4 to pivot the pivot blocks too large for one CTA by one CTA per 32-column panel
+ * instead of all SMs in one launch, plus 8 to factor every front on its own instead of the small fronts at the bottom of
+ * the tree level by level (variant 3 also turns that off), plus 16 to form the small fronts' U12 and contribution blocks
+ * by 16-row forward-substitution steps instead of products with the inverted diagonal blocks, plus 32 to pass the
+ * pipelined fronts' contribution blocks through the stack instead of writing them into the parent's working block.  The
+ * pivots do not depend on these.  No counterpart in FPLUS. */
 int fplus_b200_set_front_shape(fplus_symbolic *sym, int64_t max_width, int64_t nb_chain, int lu_variant);
 
 /* The device time of a batch: from the earliest start of the factorizations nums[0 .. count) (their first operation) to

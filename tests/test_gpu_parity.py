@@ -298,3 +298,25 @@ def test_batched_small_fronts_match_front_by_front(gpu, cplx, lu):
         X = N1.solve(b, trans)
         for r in range(2):
             assert O.backward_error(n, Ap, Ai, Ax, X[:, r], b[:, r], trans) <= 1e-14
+
+
+@pytest.mark.parametrize("name", ["pencil_1x64", "pencil_2x256", "banded_cplx_1200"])
+def test_chain_tail_forms(gpu, name):
+    """The dense chain's tails: the block-inverse products writing the contribution blocks straight into the next
+    front's working block (the default), the same through the stack and the extend-add (variant + 32: bit for bit the
+    same factors, as the sums are the same), and the 16-row forward substitution (variant + 16): the oracle's pivots and
+    L and U within 1e-12 for each."""
+    n, Ap, Ai, Ax = CASES[name]()
+    S0 = F.analyze(n, Ap, Ai)
+    orc = O.OracleLU(n, Ap, Ai, Ax, S0.row_perm, S0.col_perm)
+    got = {}
+    for variant in (1, 33, 17):
+        S = F.analyze(n, Ap, Ai)
+        S.set_front_shape(256, 64, variant)
+        N = S.factor(Ax)
+        assert np.array_equal(N.p, orc.p), f"variant {variant}: pivots differ from the oracle"
+        L, U, _ = N.factors()
+        assert _rel(L, orc.L) <= FACTOR_TOL and _rel(U, orc.U) <= FACTOR_TOL, f"variant {variant}"
+        got[variant] = (L, U)
+    assert np.array_equal(got[1][0].data, got[33][0].data) and np.array_equal(got[1][1].data, got[33][1].data), \
+        "the direct write changed the factors"
