@@ -692,24 +692,33 @@ def run_b200_arm(args, rank, world):
     F.profile(False)
     dom = max(prof, key=lambda k: prof[k]["ms"])
     peaks, psrc = measured_peaks()
-    p = prof[dom]
-    if dom == "assemble":
-        achieved = p["bytes"] / (p["ms"] * 1e-3) / 1e9
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "peak_source": f"hbm_gbs ({psrc})"}
-    else:
-        achieved = p["flops"] / (p["ms"] * 1e-3) / 1e12
-        peak = fp64_peak_tflops(torch, cplx) if rank == 0 else float("nan")
-        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "peak_source": ("cuBLAS " + ("ZGEMM" if cplx else "DGEMM") + " 8192^3 measured in bench.py (FP64 tensor "
-                                "path; the measured-peaks file has bf16 and HBM only)")}
-    ratio, rsrc = traffic_ratio(dom)
-    roof.update({"kernel_class": dom, "launches": p["count"], "avg_launch_us": 1e3 * p["ms"] / max(p["count"], 1),
-                 "algorithmic_per_launch": (p["flops"] if dom != "assemble" else p["bytes"]) / max(p["count"], 1),
-                 "algorithmic_bytes_per_launch": p["bytes"] / max(p["count"], 1),
-                 "traffic": None if ratio is None else ratio * p["bytes"] / max(p["count"], 1),
-                 "traffic_source": rsrc,
-                 "classes_ms": {k: round(v["ms"], 3) for k, v in prof.items()}})
+    fp64_peak = fp64_peak_tflops(torch, cplx) if rank == 0 else float("nan")
+
+    def class_roofline(cls):
+        p = prof[cls]
+        if cls == "assemble":
+            achieved = p["bytes"] / (p["ms"] * 1e-3) / 1e9
+            r = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                 "frac": achieved / peaks["hbm_gbs"], "peak_source": f"hbm_gbs ({psrc})"}
+        else:
+            achieved = p["flops"] / (p["ms"] * 1e-3) / 1e12
+            r = {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                 "peak_source": ("cuBLAS " + ("ZGEMM" if cplx else "DGEMM") + " 8192^3 measured in bench.py (FP64 tensor "
+                                 "path; the measured-peaks file has bf16 and HBM only)")}
+        ratio, rsrc = traffic_ratio(cls)
+        r.update({"kernel_class": cls, "launches": p["count"], "avg_launch_us": 1e3 * p["ms"] / max(p["count"], 1),
+                  "algorithmic_per_launch": (p["flops"] if cls != "assemble" else p["bytes"]) / max(p["count"], 1),
+                  "algorithmic_bytes_per_launch": p["bytes"] / max(p["count"], 1),
+                  "traffic": None if ratio is None else ratio * p["bytes"] / max(p["count"], 1),
+                  "traffic_source": rsrc})
+        return r
+    roof = class_roofline(dom)
+    roof["classes_ms"] = {k: round(v["ms"], 3) for k, v in prof.items()}
+    if dom == "front_lu":
+        # the pivot-block LU is bound by the latency of its dependent pivot steps, not by a throughput; the Schur
+        # updates' roofline beside it
+        roof["bound_note"] = "latency of np dependent pivot steps per front (one CTA); no throughput roofline applies"
+    roof_schur = class_roofline("schur_gemm") if dom != "schur_gemm" and prof["schur_gemm"]["count"] > 0 else None
 
     # the solve with 16 right-hand sides (the configuration's second nrhs)
     solve16 = None
@@ -781,7 +790,7 @@ def run_b200_arm(args, rank, world):
             "e2e": {"value": ms_e2e / world, "unit": "ms", "h2d_bytes_per_step": int(Ap[-1]) * vsz + n * vsz,
                     "d2h_bytes_per_step": n * vsz},
             "gpu_launches": int(launches),
-            "clocks": clocks, "roofline": roof, "cpu_baseline": cpu, "solve_nrhs16": solve16, "batch": batch,
+            "clocks": clocks, "roofline": roof, "roofline_schur": roof_schur, "cpu_baseline": cpu, "solve_nrhs16": solve16, "batch": batch,
             "batch_pencils": batch_pencils, "c1_pair": c1_pair, "precision_form": precision, "random_form": random_form}
     print(json.dumps(line))
 
