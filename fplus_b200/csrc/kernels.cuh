@@ -2087,17 +2087,24 @@ __device__ __forceinline__ void front_tail2_body(const T *__restrict__ W, int64_
                     const bool kin = kk < w;
                     const double ar = kin && am < nrows ? sLr[k * FT_LD + am] : 0.0;
                     const double ai = CP && kin && am < nrows ? sLi[k * FT_LD + am] : 0.0;
+                    double br[NCF], bi[NCF];
 #pragma unroll
                     for (int cf = 0; cf < NCF; cf++) {
                         const int bn = 8 * cf + (lane >> 2);
-                        const double br = kin ? sXr[bn * FT_LD + k] : 0.0;
-                        dmma_s(acc[cf][0], acc[cf][1], ar, br);
-                        if constexpr (CP) {
-                            const double bi = kin ? sXi[bn * FT_LD + k] : 0.0;
-                            dmma_s(acc[cf][0], acc[cf][1], ai, -bi);
-                            dmma_s(acc[cf][2], acc[cf][3], ar, bi);
-                            dmma_s(acc[cf][2], acc[cf][3], ai, br);
-                        }
+                        br[cf] = kin ? sXr[bn * FT_LD + k] : 0.0;
+                        bi[cf] = CP && kin ? sXi[bn * FT_LD + k] : 0.0;
+                    }
+                    // the products grouped so that consecutive tensor-core instructions are independent (2 NCF - 1
+                    // others between two on the same accumulator)
+#pragma unroll
+                    for (int cf = 0; cf < NCF; cf++) dmma_s(acc[cf][0], acc[cf][1], ar, br[cf]);
+                    if constexpr (CP) {
+#pragma unroll
+                        for (int cf = 0; cf < NCF; cf++) dmma_s(acc[cf][2], acc[cf][3], ar, bi[cf]);
+#pragma unroll
+                        for (int cf = 0; cf < NCF; cf++) dmma_s(acc[cf][0], acc[cf][1], ai, -bi[cf]);
+#pragma unroll
+                        for (int cf = 0; cf < NCF; cf++) dmma_s(acc[cf][2], acc[cf][3], ai, br[cf]);
                     }
                 }
             }

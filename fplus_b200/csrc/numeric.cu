@@ -453,14 +453,11 @@ static int run_equil(const DevPlan &D, DevNum &N, int equilibrate, int max_iter,
         CK(cudaGetLastError());
         return FPLUS_OK;
     }
-    DevStatus h0;
-    std::memset(&h0, 0, sizeof(h0));
-    h0.amin_bits = 0x7ff0000000000000ull;       // +inf
-    h0.idx = INT64_MAX;                         // the smallest failing index wins
-    CK(cudaMemcpyAsync(N.st, &h0, sizeof(h0), cudaMemcpyHostToDevice, s));
-    std::vector<double> ones((size_t)(n > 0 ? n : 1), 1.0);
-    CK(cudaMemcpyAsync(N.Drp, ones.data(), (size_t)n * 8, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(N.Dcp, ones.data(), (size_t)n * 8, cudaMemcpyHostToDevice, s));
+    // the status (the smallest failing index wins; the range's minimum starts at +inf) and the unit scalings, set on the
+    // device (no pageable host copies)
+    k_clear_status<<<1, 1, 0, s>>>(N.st, 1), note_launch();
+    k_fill<<<nblk(n), 256, 0, s>>>(N.Drp, n, 1.0), note_launch();
+    k_fill<<<nblk(n), 256, 0, s>>>(N.Dcp, n, 1.0), note_launch();
     if (equilibrate) {
         // range guard (FPLUS src/equil.c:197-241)
         const int64_t m = (N.cplx ? 2 : 1) * nnz;
