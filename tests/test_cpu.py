@@ -321,6 +321,22 @@ def test_batch_argument_checks_on_host():
     assert L.fplus_b200_solve_batch(2, None, None, None, None, 0, 2, None, err, 256) == F.FPLUS_ERR_BADARG
 
 
+def test_front_shape_checks_on_host():
+    """fplus_b200_set_front_shape (host only): the pivot-block LU kernel 1, 2 or 3, plus 4 (tall blocks by panels), 8 (no
+    batched levels), 16 (forward-substitution tails) and 32 (no direct write of the chain's contribution blocks); widths
+    16 .. 4096 and chain fronts of 8 .. 64 pivots; anything else is refused and leaves the shape as it was."""
+    n, Ap, Ai, _ = W.convdiff2d(12, 1)
+    S = F.analyze(n, Ap, Ai)
+    L = F.lib()
+    for v in (1, 2, 3, 5, 10, 18, 33, 63):
+        assert L.fplus_b200_set_front_shape(S._h, 256, 64, v) == F.FPLUS_OK, v
+    for v in (0, 4, 8, 64, 66, -1):
+        assert L.fplus_b200_set_front_shape(S._h, 256, 64, v) == F.FPLUS_ERR_BADARG, v
+    assert L.fplus_b200_set_front_shape(S._h, 8, 64, 2) == F.FPLUS_ERR_BADARG
+    assert L.fplus_b200_set_front_shape(S._h, 256, 65, 2) == F.FPLUS_ERR_BADARG
+    assert L.fplus_b200_set_front_shape(None, 256, 64, 2) == F.FPLUS_ERR_BADARG
+
+
 def test_lowlevel_argument_checks_on_host():
     """The low-level entry points refuse bad arguments, and a zero or missing diagonal of U, on the host before any
     GPU work (FPLUS src/pipeline.c:91-99, src/solve_plan.c:664-673, src/solve.c:62-66); a plan on factors this library
