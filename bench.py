@@ -212,6 +212,8 @@ def run_profile_once(args):
     B = torch.from_numpy(W.rhs(n, nrhs, np.iscomplexobj(Ax), 2)).cuda()
     Ad = torch.from_numpy(np.ascontiguousarray(Ax)).cuda()
     S = F.analyze(n, Ap, Ai)
+    if args.front_variant:
+        S.set_front_shape(256, 64, args.front_variant)
     N = S.factor(Ad, device=True, precision=args.profile_precision)
     N.solve_device(B.clone(), 0)
     del N

@@ -306,7 +306,7 @@ extern "C" int fplus_b200_autotune(fplus_symbolic *sym, const int64_t *Ap, const
     int bl = l0;
     double bms = -1.0;
     bool chain = false;
-    // the front shapes with the shared-memory pivot-block LU, then the best shape with the register-resident LU
+    // the front shapes with the shared-memory pivot-block LU, then the best shape with the panel LU (tensor-core updates)
     for (int ci = 0; ci < 7; ci++) {
         const int wi = ci < 6 ? ci / 2 : -1, bi = ci < 6 ? ci % 2 : -1;
         if (ci < 6 && bi == 0 && !chain && wi > 0) continue;      // the chain size matters only with a dense chain

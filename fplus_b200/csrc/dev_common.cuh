@@ -27,6 +27,12 @@ __device__ __forceinline__ double sub(double a, double b) { return a - b; }
 __device__ __forceinline__ cplx sub(cplx a, cplx b) { return cplx{a.x - b.x, a.y - b.y}; }
 __device__ __forceinline__ double mul(double a, double b) { return a * b; }
 __device__ __forceinline__ cplx mul(cplx a, cplx b) { return cplx{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
+// a - l p in fused multiply-adds (complex: four)
+__device__ __forceinline__ double msub(double a, double l, double p) { return fma(-l, p, a); }
+__device__ __forceinline__ cplx msub(cplx a, cplx l, cplx p)
+{
+    return cplx{fma(l.y, p.y, fma(-l.x, p.x, a.x)), fma(-l.y, p.x, fma(-l.x, p.y, a.y))};
+}
 __device__ __forceinline__ double conjv(double a) { return a; }
 __device__ __forceinline__ cplx conjv(cplx a) { return cplx{a.x, -a.y}; }
 __device__ __forceinline__ double scal(double a, double s) { return a * s; }

@@ -57,8 +57,8 @@ struct fplus_symbolic {
     // the front structure's shape: at most max_width pivot columns per front, nb_chain per dense-chain front (the
     // autotuner, fplus_b200_autotune, may change them)
     mutable int64_t max_width = 256, nb_chain = 64;
-    // the pivot-block LU kernel of the small fronts: 2 (the block in shared memory, a barrier per pivot step), 1 (the
-    // block in registers) or 3 (blocked panels); autotuned
+    // the pivot-block LU kernel of the small fronts: 2 (the block in shared memory, a barrier per pivot step), 1 (8-column
+    // panels, the later columns' updates on the FP64 tensor cores) or 3 (blocked panels); autotuned
     mutable int lu_variant = 2;
     mutable std::shared_ptr<fpl::FrontPlan> plan;
     mutable std::shared_ptr<fpl::DevPlan> dplan;

@@ -1172,26 +1172,24 @@ __device__ __forceinline__ void front_lu2_body(const T *__restrict__ W, int64_t 
             if (upd) {
                 T *lc = lcol + (j & 1) * nrows;
                 const T *lp = lcol + ((j + 1) & 1) * nrows;
+                // (32-bit offsets, one per column for the row and the pivot row; a - l p in fused multiply-adds)
+                const int gs = G * nrows;                             // from one of this thread's columns to the next
                 for (int i = my_i; i < nrows; i += rstep) {
-                    if (my_g == 0 && j > 0 && tag[i] >= j) A[(size_t)(j - 1) * nrows + i] = lp[i];   // step j - 1's multiplier
+                    if (my_g == 0 && j > 0 && tag[i] >= j) A[(j - 1) * nrows + i] = lp[i];   // step j - 1's multiplier
                     if (tag[i] <= j) continue;
-                    const T l = mul(A[(size_t)j * nrows + i], inv);
+                    const T l = mul(A[j * nrows + i], inv);
                     if (my_g == 0) lc[i] = l;
                     int c = j + 2 + my_g;
-                    for (; c + 3 * G < npiv; c += 4 * G) {          // 4 independent columns per round, loads first
+                    T *xa = A + c * nrows + i;
+                    const T *pa_ = A + c * nrows + bi;
+                    for (; c + 3 * G < npiv; c += 4 * G, xa += 4 * gs, pa_ += 4 * gs) {   // 4 independent columns, loads first
                         T xv[4], pv[4];
 #pragma unroll
-                        for (int q = 0; q < 4; q++) {
-                            xv[q] = A[(size_t)(c + q * G) * nrows + i];
-                            pv[q] = A[(size_t)(c + q * G) * nrows + bi];
-                        }
+                        for (int q = 0; q < 4; q++) { xv[q] = xa[q * gs]; pv[q] = pa_[q * gs]; }
 #pragma unroll
-                        for (int q = 0; q < 4; q++) A[(size_t)(c + q * G) * nrows + i] = sub(xv[q], mul(l, pv[q]));
+                        for (int q = 0; q < 4; q++) xa[q * gs] = msub(xv[q], l, pv[q]);
                     }
-                    for (; c < npiv; c += G) {
-                        T *x = A + (size_t)c * nrows + i;
-                        *x = sub(*x, mul(l, A[(size_t)c * nrows + bi]));
-                    }
+                    for (; c < npiv; c += G, xa += gs, pa_ += gs) *xa = msub(*xa, l, *pa_);
                 }
             }
             named_bar(1, nact);
@@ -1232,184 +1230,218 @@ __global__ void __launch_bounds__(640) k_front_lu2(const T *__restrict__ W, int6
     front_lu2_body<T>(W, ld, nrows, npiv, nri, fcol, colmax, pivot_rel, rowid, Lout, perm, p_lu, st, front, pa);
 }
 
-// Partial-pivot LU of a front's pivot block with the block in registers (nrows <= 128, npiv <= 64; one CTA of 512
-// threads, 16 warps).  Warp w owns rows 8w .. 8w + 7; lane 4r + q holds row 8w + r's entries of the columns q, q + 4, ..,
-// q + 60 (16 values) in registers for the whole elimination.  One block barrier per pivot step j:
-//   before it  every warp has applied step j - 1 to its live rows, found its candidate for column j among its 8 rows (the
-//              largest pivot key, ties to the smaller row of B) and posted it (key, row of B, value, 1 / value) together
-//              with the candidate row's 64 entries (double-buffered by step parity);
-//   after it   every thread reads the 16 candidates and makes the same pivot and stop decision; the lane holding a row's
-//              column-j entry forms its multiplier (l = a * (1 / p)) and hands it to the row's other three lanes by a
-//              shuffle; every live row updates its later columns from the winner's posted row (a - l u).
-// Rows never move: a row pivoted at step j is tagged j.  Once a group of four columns is final (after its last step) it
-// leaves the registers for the shared-memory copy of the block and the others shift down, so that the register indices
-// are compile-time constants in a loop that is not unrolled.  The arithmetic per entry and the pivots are those of
-// k_front_lu2.
-constexpr int LU4_THREADS = 512, LU4_NR = 128, LU4_NP = 64, LU4_M = 16, LU4_W = 16;
+// Blocked partial-pivot LU of a front's pivot block (nrows <= 128, npiv <= 64; one CTA of 256 threads): 8-column panels
+// pivoted by warps 0-3 (thread i < 128 holds row i's eight panel entries in registers; per pivot step every warp posts its
+// candidate with the candidate row's panel entries, one 128-thread barrier, and every thread makes the same decision),
+// then the panel's pivot rows' U for the later columns by an 8-step forward substitution (a thread per column), then
+// the rank-8 update of every later column as FP64 tensor-core products (mma m8n8k4) of the masked multipliers (rows
+// already pivoted read zero) and the pivot rows' U.  Rows never move: a row pivoted at step j is tagged j, and the block
+// goes out in the final order at the end.  The pivots are those of the step-by-step elimination (the update of a later
+// column sums the panel's eight products in another order, so the values agree to rounding).
+constexpr int LU5_THREADS = 256, LU5_PB = 8, LU5_LMLD = 132;
 
-template <typename T> struct Lu4Cand {
-    unsigned long long key;    // pivot key (0: no candidate)
-    long long rid;             // row of B (ties: the smaller)
-    T val, inv;                // the candidate value and its reciprocal
-    int row;                   // row in the block (-1: no candidate)
-    int pad[3];
+template <typename T> struct Lu5Cand {
+    unsigned long long key;
+    long long rid;
+    int row, pad;
+    T val, inv;
+    T u[LU5_PB];
 };
 
-// dynamic shared memory: the staged block (reused for the output), row ids, thresholds and their keys, the final order
-static inline size_t front_lu4_smem(int64_t nrows, int64_t npiv, int64_t vs)
+// dynamic shared memory: the block, row ids, thresholds and their keys, the masked multipliers (two planes for complex),
+// the final order
+static inline size_t front_lu5_smem(int64_t nrows, int64_t npiv, int64_t vs)
 {
-    return (size_t)(nrows * npiv * vs + nrows * 8 + npiv * 16 + nrows * 4);
+    return (size_t)(nrows * npiv * vs + nrows * 8 + npiv * 16 + (vs / 8) * LU5_PB * LU5_LMLD * 8 + nrows * 4);
 }
 
 template <typename T>
-__device__ __forceinline__ void front_lu4_body(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
+__device__ __forceinline__ void front_lu5_body(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
                                                int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
                                                int64_t *__restrict__ rowid, T *__restrict__ Lout, int *__restrict__ perm,
                                                int64_t *__restrict__ p_lu, DevStatus *st, int64_t front, const PivotAsm &pa)
 {
+    constexpr bool CP = VT<T>::cplx_;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *A = reinterpret_cast<T *>(smem_raw);                        // npiv x nrows, column-major: A[c * nrows + i]
     int64_t *rid = reinterpret_cast<int64_t *>(A + (size_t)npiv * nrows);
-    double *thr = reinterpret_cast<double *>(rid + nrows);         // npiv: pivot_rel * max |B(:, column)|
-    unsigned long long *thk = reinterpret_cast<unsigned long long *>(thr + npiv);   // the key of 2 thr
-    int *sperm = reinterpret_cast<int *>(thk + npiv);              // final position -> block row
-    __shared__ Lu4Cand<T> cand[2][LU4_W];
-    __shared__ T rowbuf[2][LU4_W][LU4_NP];
-    __shared__ int wcnt[LU4_W], s_stop;
+    double *thr = reinterpret_cast<double *>(rid + nrows);
+    unsigned long long *thk = reinterpret_cast<unsigned long long *>(thr + npiv);
+    double *Lmr = reinterpret_cast<double *>(thk + npiv);         // masked multipliers: Lm[k][row] at k * LU5_LMLD + row
+    double *Lmi = Lmr + (CP ? LU5_PB * LU5_LMLD : 0);
+    int *sperm = reinterpret_cast<int *>(Lmr + (CP ? 2 : 1) * LU5_PB * LU5_LMLD);
+    __shared__ Lu5Cand<T> cand[2][4];
+    __shared__ int prow[LU5_PB], s_stop, wcnt[4];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int q = lane & 3, i = 8 * warp + (lane >> 2);
-    if (tid == 0) s_stop = st->code != 0;                          // an earlier front stopped the factorization
-    stage_pivot_block<T>(A, rid, W, ld, nrows, npiv, rowid, pa, tid, LU4_THREADS);
-    for (int c = tid; c < npiv; c += LU4_THREADS) {
+    if (tid == 0) s_stop = st->code != 0;
+    stage_pivot_block<T>(A, rid, W, ld, nrows, npiv, rowid, pa, tid, LU5_THREADS);
+    for (int c = tid; c < npiv; c += LU5_THREADS) {
         thr[c] = pivot_rel * colmax[fcol + c];
         thk[c] = pivkey_of_modulus<T>(2.0 * thr[c]);
     }
-    for (int e = tid; e < 2 * LU4_W * LU4_NP; e += LU4_THREADS) (&rowbuf[0][0][0])[e] = VT<T>::zero();
     __syncthreads();
     if (s_stop) return;
-    T a[LU4_M];
+    const bool pg = tid < 128;                                     // the panel group: thread i holds row i
+    const int i = tid;
+    const long long myrid = pg && i < nrows ? (long long)rid[i] : LLONG_MAX;
+    bool live = pg && i < nrows;
+    int mytag = INT_MAX;
+    for (int c0 = 0; c0 < npiv; c0 += LU5_PB) {
+        const int w = npiv - c0 < LU5_PB ? npiv - c0 : LU5_PB;   // pivot steps of this panel
+        if (pg) {
+            T pv[LU5_PB];
 #pragma unroll
-    for (int m = 0; m < LU4_M; m++) {
-        const int c = q + 4 * m;
-        a[m] = i < nrows && c < npiv ? A[c * nrows + i] : VT<T>::zero();
-    }
-    const long long myrid = i < nrows ? (long long)rid[i] : LLONG_MAX;
-    bool live = i < nrows;                                         // not pivoted yet
-    int mytag = INT_MAX;                                           // the step at which this row was pivoted
-    int base = 0;                                                  // groups of four columns retired from the registers
-    // the warp's candidate for column 4 base + cq (this lane's entry a[0] when q == cq) and its row, into parity par
-    auto post = [&](int par, int cq) {
-        const T x = a[0];
-        const unsigned long long key = live && q == cq ? pivkey(x) : 0ull;
-        const T xinv = key != 0ull ? recip(x) : VT<T>::zero();
-        const unsigned long long mk = warp_max_key(key);
-        unsigned cnd = __ballot_sync(0xffffffffu, key != 0ull && key == mk);
-        if (cnd == 0u) {
-            if (lane == 0) { cand[par][warp].key = 0ull; cand[par][warp].rid = LLONG_MAX; cand[par][warp].row = -1; }
-            return;
-        }
-        if ((cnd & (cnd - 1u)) != 0u) {
-            long long r2 = (cnd >> lane) & 1u ? myrid : LLONG_MAX;
-            for (int o = 16; o > 0; o >>= 1) { const long long t = __shfl_xor_sync(0xffffffffu, r2, o); r2 = t < r2 ? t : r2; }
-            cnd = __ballot_sync(0xffffffffu, ((cnd >> lane) & 1u) && myrid == r2);
-        }
-        const int wl = __ffs(cnd) - 1;
-        if (lane == wl) {
-            cand[par][warp].key = mk; cand[par][warp].rid = myrid; cand[par][warp].val = x; cand[par][warp].inv = xinv;
-            cand[par][warp].row = i;
-        }
-        if ((lane >> 2) == (wl >> 2)) {                             // the candidate row's four lanes post its entries
+            for (int s = 0; s < LU5_PB; s++) pv[s] = i < nrows && s < w ? A[(c0 + s) * nrows + i] : VT<T>::zero();
 #pragma unroll
-            for (int m = 0; m < LU4_M; m++) {
-                const int c = q + 4 * (m + base);
-                if (m + base < LU4_M && c < npiv) rowbuf[par][warp][c] = a[m];
-            }
-        }
-    };
-    if (npiv > 0) post(0, 0);
-    for (int j = 0; j < npiv; j++) {
-        const int par = j & 1, qj = j & 3;
-        __syncthreads();                                           // the candidates of column j are posted
-        // the winner: lane s % 16 reads candidate s; the largest key, ties to the smaller row of B
-        const unsigned long long ck = cand[par][lane & 15].key;
-        const long long cr = cand[par][lane & 15].rid;
-        const unsigned long long bk = warp_max_key(ck);
-        unsigned cw = __ballot_sync(0xffffffffu, ck != 0ull && ck == bk);
-        if (cw != 0u && (cw & (cw - 1u) & 0xffffu) != 0u) {
-            long long r2 = (cw >> lane) & 1u ? cr : LLONG_MAX;
-            for (int o = 16; o > 0; o >>= 1) { const long long t = __shfl_xor_sync(0xffffffffu, r2, o); r2 = t < r2 ? t : r2; }
-            cw = __ballot_sync(0xffffffffu, ((cw >> lane) & 1u) && cr == r2);
-        }
-        const int bw = cw != 0u ? (__ffs(cw) - 1) & 15 : 0;
-        const int bi = cw != 0u ? cand[par][bw].row : -1;
-        const T pv = cand[par][bw].val, inv = cand[par][bw].inv;
-        {
-            // the singular test of the reference (FPLUS src/factor_sn_panel.inc:232-233): no candidate, a zero modulus,
-            // or a modulus below pivot_rel * max |B(:, column)| (the modulus itself only near it)
-            int stop = 0;
-            if (bi < 0 || bk == 0ull || (bk < thk[j] && vabs(pv) < thr[j])) stop = 1;
-            else if (bi >= nri) stop = 2;
-            if (stop) {
-                if (tid == 0) {
-                    if (stop == 1) set_status(st, ST_SINGULAR, fcol + j, bi >= 0 ? vabs(pv) : 0.0, thr[j]);
-                    else set_status(st, ST_BORDER, front, vabs(pv), thr[j]);
+            for (int s = 0; s < LU5_PB; s++) {
+                if (s >= w) break;
+                const int par = s & 1, j = c0 + s;
+                // this warp's candidate for column j, posted with its row's panel entries
+                const unsigned long long key = live ? pivkey(pv[s]) : 0ull;
+                const T xinv = key != 0ull ? recip(pv[s]) : VT<T>::zero();
+                const unsigned long long mk = warp_max_key(key);
+                unsigned cnd = __ballot_sync(0xffffffffu, key != 0ull && key == mk);
+                if (cnd != 0u && (cnd & (cnd - 1u)) != 0u) {
+                    long long r2 = (cnd >> lane) & 1u ? myrid : LLONG_MAX;
+                    for (int o = 16; o > 0; o >>= 1) { const long long t = __shfl_xor_sync(0xffffffffu, r2, o); r2 = t < r2 ? t : r2; }
+                    cnd = __ballot_sync(0xffffffffu, ((cnd >> lane) & 1u) && myrid == r2);
                 }
-                return;                                          // every thread leaves here
+                const int wl = cnd != 0u ? __ffs(cnd) - 1 : 0;
+                if (lane == wl) {
+                    Lu5Cand<T> &cd = cand[par][warp];
+                    cd.key = cnd != 0u ? mk : 0ull; cd.rid = cnd != 0u ? myrid : LLONG_MAX; cd.row = cnd != 0u ? i : -1;
+                    cd.val = pv[s]; cd.inv = xinv;
+#pragma unroll
+                    for (int q = 0; q < LU5_PB; q++) cd.u[q] = pv[q];
+                }
+                named_bar(1, 128);
+                // the winner (every thread of the group the same): the largest key, ties to the smaller row of B
+                int bs = 0;
+                unsigned long long bk = cand[par][0].key;
+                long long br = cand[par][0].rid;
+#pragma unroll
+                for (int q = 1; q < 4; q++) {
+                    const unsigned long long k = cand[par][q].key;
+                    const long long r = cand[par][q].rid;
+                    if (k > bk || (k == bk && r < br)) { bk = k; br = r; bs = q; }
+                }
+                const int bi = cand[par][bs].row;
+                const T pvw = cand[par][bs].val, inv = cand[par][bs].inv;
+                int stop = 0;
+                if (bi < 0 || bk == 0ull || (bk < thk[j] && vabs(pvw) < thr[j])) stop = 1;
+                else if (bi >= nri) stop = 2;
+                if (stop) {
+                    if (tid == 0) {
+                        if (stop == 1) set_status(st, ST_SINGULAR, fcol + j, bi >= 0 ? vabs(pvw) : 0.0, thr[j]);
+                        else set_status(st, ST_BORDER, front, vabs(pvw), thr[j]);
+                        s_stop = 1;
+                    }
+                    break;                                         // (every thread of the group the same)
+                }
+                if (i == bi) { mytag = j; live = false; prow[s] = i; }
+                if (live) {
+                    const T l = mul(pv[s], inv);
+                    pv[s] = l;
+#pragma unroll
+                    for (int q = s + 1; q < LU5_PB; q++) pv[q] = sub(pv[q], mul(l, cand[par][bs].u[q]));
+                }
+            }
+            // the panel back into the block; the masked multipliers (zero for every row pivoted so far)
+#pragma unroll
+            for (int s = 0; s < LU5_PB; s++) {
+                if (i < nrows && s < w) A[(c0 + s) * nrows + i] = pv[s];
+                const T lm = live && s < w ? pv[s] : VT<T>::zero();
+                if constexpr (CP) { Lmr[s * LU5_LMLD + i] = lm.x; Lmi[s * LU5_LMLD + i] = lm.y; } else Lmr[s * LU5_LMLD + i] = lm;
             }
         }
-        const T l = shfl_v<T>(mul(a[0], inv), (lane & ~3) | qj);     // this row's multiplier (from its column-j lane)
-        if (i == bi) { mytag = j; live = false; }
-        if (live) {
-            const T *u = rowbuf[par][bw];
-            if (q == qj) a[0] = l;                                 // the entry of L
-            else if (q > qj) a[0] = sub(a[0], mul(l, u[q + 4 * base]));
+        __syncthreads();
+        if (s_stop) return;
+        const int t0 = c0 + w, T_ = npiv - t0;                     // the later columns
+        if (T_ <= 0) continue;
+        // the pivot rows' U for the later columns: forward substitution with the panel's unit-lower L (a thread per column)
+        for (int c = t0 + tid; c < npiv; c += LU5_THREADS) {
+            T u[LU5_PB];
 #pragma unroll
-            for (int m = 1; m < LU4_M; m++)
-                if (m + base < LU4_M) a[m] = sub(a[m], mul(l, u[q + 4 * (m + base)]));
+            for (int k = 0; k < LU5_PB; k++) u[k] = k < w ? A[c * nrows + prow[k]] : VT<T>::zero();
+#pragma unroll
+            for (int k = 1; k < LU5_PB; k++) {
+                if (k >= w) break;
+                T acc = u[k];
+#pragma unroll
+                for (int q = 0; q < k; q++) acc = sub(acc, mul(A[(c0 + q) * nrows + prow[k]], u[q]));
+                u[k] = acc;
+                A[c * nrows + prow[k]] = acc;
+            }
         }
-        if (qj == 3) {                                             // columns 4 base .. 4 base + 3 are final
-            const int c = q + 4 * base;
-            if (i < nrows && c < npiv) A[c * nrows + i] = a[0];
+        __syncthreads();
+        // the rank-w update of every later column on the FP64 tensor cores: A[r, c] -= sum_k Lm[k][r] U[k, c]
+        // (item = an 8-row x 8-column fragment; rows already pivoted have zero multipliers and stay as they are)
+        {
+            const int rf = (nrows + 7) >> 3, cf = (T_ + 7) >> 3;
+            for (int p = warp; p < rf * cf; p += LU5_THREADS / 32) {
+                const int r0 = 8 * (p % rf), cb = t0 + 8 * (p / rf);
+                double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+                const int am = r0 + (lane >> 2), bn = cb + (lane >> 2);
 #pragma unroll
-            for (int m = 0; m + 1 < LU4_M; m++) a[m] = a[m + 1];
-            a[LU4_M - 1] = VT<T>::zero();
-            base++;
+                for (int ks = 0; ks < LU5_PB; ks += 4) {
+                    const int k = ks + (lane & 3);
+                    const bool kin = k < w;
+                    const double ar = kin && am < nrows ? Lmr[k * LU5_LMLD + am] : 0.0;
+                    const double ai = CP && kin && am < nrows ? Lmi[k * LU5_LMLD + am] : 0.0;
+                    T bv = kin && bn < npiv ? A[bn * nrows + prow[k < w ? k : 0]] : VT<T>::zero();
+                    double brr, bii;
+                    if constexpr (CP) { brr = bv.x; bii = bv.y; } else { brr = bv; bii = 0.0; }
+                    dmma(a0, a1, ar, brr);
+                    if constexpr (CP) {
+                        dmma(b0, b1, ar, bii);
+                        dmma(a0, a1, ai, -bii);
+                        dmma(b0, b1, ai, brr);
+                    }
+                }
+                const int cr = r0 + (lane >> 2), cc = cb + 2 * (lane & 3);
+                if (cr < nrows) {
+                    if (cc < npiv) {
+                        T *x = A + cc * nrows + cr;
+                        if constexpr (CP) *x = cplx{x->x - a0, x->y - b0}; else *x = *x - a0;
+                    }
+                    if (cc + 1 < npiv) {
+                        T *x = A + (cc + 1) * nrows + cr;
+                        if constexpr (CP) *x = cplx{x->x - a1, x->y - b1}; else *x = *x - a1;
+                    }
+                }
+            }
         }
-        if (j + 1 < npiv) post(par ^ 1, (j + 1) & 3);
+        __syncthreads();
     }
-    // the columns still in registers to the shared copy; the final order: pivot rows at their step, the others after them
-    // in block order
-#pragma unroll
-    for (int m = 0; m < LU4_M; m++) {
-        const int c = q + 4 * (m + base);
-        if (m + base < LU4_M && i < nrows && c < npiv) A[c * nrows + i] = a[m];
-    }
-    const bool un = i < nrows && mytag == INT_MAX;
-    const unsigned bal = __ballot_sync(0xffffffffu, un && q == 0);
-    if (lane == 0) wcnt[warp] = __popc(bal);
-    __syncthreads();
-    int k0 = npiv;
-    for (int w = 0; w < warp; w++) k0 += wcnt[w];
-    const int k = un ? k0 + __popc(bal & ((1u << lane) - 1u)) : mytag;
-    if (q == 0 && i < nrows) {
-        sperm[k] = i;
-        perm[k] = i;
-        rowid[k] = myrid;
-        if (k < npiv) p_lu[fcol + k] = myrid;
+    // the final order: pivot rows at their step, the others after them in block order (warps 0-3, a row each)
+    if (pg) {
+        const bool un = i < nrows && mytag == INT_MAX;
+        const unsigned bal = __ballot_sync(0xffffffffu, un);
+        if (lane == 0) wcnt[warp] = __popc(bal);
+        named_bar(1, 128);
+        int k0 = npiv;
+        for (int q = 0; q < warp; q++) k0 += wcnt[q];
+        const int k = un ? k0 + __popc(bal & ((1u << lane) - 1u)) : mytag;
+        if (i < nrows) {
+            sperm[k] = i;
+            perm[k] = i;
+            rowid[k] = myrid;
+            if (k < npiv) p_lu[fcol + k] = myrid;
+        }
     }
     __syncthreads();
     const int ne = npiv * nrows;
-    for (int e = tid; e < ne; e += LU4_THREADS) { const int kk = e % nrows, c = e / nrows; Lout[e] = A[c * nrows + sperm[kk]]; }
+    for (int e = tid; e < ne; e += LU5_THREADS) { const int kk = e % nrows, c = e / nrows; Lout[e] = A[c * nrows + sperm[kk]]; }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(LU4_THREADS, 1) k_front_lu4(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
-                                                               int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
-                                                               int64_t *__restrict__ rowid, T *__restrict__ Lout,
-                                                               int *__restrict__ perm, int64_t *__restrict__ p_lu, DevStatus *st,
-                                                               int64_t front, PivotAsm pa)
+__global__ void __launch_bounds__(LU5_THREADS) k_front_lu5(const T *__restrict__ W, int64_t ld, int nrows, int npiv, int nri,
+                                                            int64_t fcol, const double *__restrict__ colmax, double pivot_rel,
+                                                            int64_t *__restrict__ rowid, T *__restrict__ Lout,
+                                                            int *__restrict__ perm, int64_t *__restrict__ p_lu, DevStatus *st,
+                                                            int64_t front, PivotAsm pa)
 {
-    front_lu4_body<T>(W, ld, nrows, npiv, nri, fcol, colmax, pivot_rel, rowid, Lout, perm, p_lu, st, front, pa);
+    front_lu5_body<T>(W, ld, nrows, npiv, nri, fcol, colmax, pivot_rel, rowid, Lout, perm, p_lu, st, front, pa);
 }
 
 // Blocked partial-pivot LU of a front's pivot block in shared memory (nrows <= 128, npiv <= 64; one CTA of LU3_THREADS):
@@ -3887,18 +3919,18 @@ __global__ void __launch_bounds__(640) k_bat_lu2(const FcFront *__restrict__ fc,
                       La + F.L_off, permall + F.row_off, p_lu, st, fi, pa);
 }
 
-// the same with the register-resident pivot-block LU (the body of k_front_lu4)
+// the same with the blocked pivot-block LU (the body of k_front_lu5)
 template <typename T>
-__global__ void __launch_bounds__(LU4_THREADS, 1) k_bat_lu4(const FcFront *__restrict__ fc, const int *__restrict__ list,
-                                                             const T *__restrict__ Wbase, const double *__restrict__ colmax,
-                                                             double pivot_rel, int64_t *__restrict__ rowid_all, T *__restrict__ La,
-                                                             int *__restrict__ permall, int64_t *__restrict__ p_lu, DevStatus *st)
+__global__ void __launch_bounds__(LU5_THREADS) k_bat_lu5(const FcFront *__restrict__ fc, const int *__restrict__ list,
+                                                          const T *__restrict__ Wbase, const double *__restrict__ colmax,
+                                                          double pivot_rel, int64_t *__restrict__ rowid_all, T *__restrict__ La,
+                                                          int *__restrict__ permall, int64_t *__restrict__ p_lu, DevStatus *st)
 {
     const int fi = list[blockIdx.x];
     const FcFront F = fc[fi];
     PivotAsm pa;
     pa.on = 0;
-    front_lu4_body<T>(Wbase + F.wofs, F.nr, (int)F.nr, (int)F.np, (int)F.nri, F.f, colmax, pivot_rel, rowid_all + F.row_off,
+    front_lu5_body<T>(Wbase + F.wofs, F.nr, (int)F.nr, (int)F.np, (int)F.nri, F.f, colmax, pivot_rel, rowid_all + F.row_off,
                       La + F.L_off, permall + F.row_off, p_lu, st, fi, pa);
 }
 

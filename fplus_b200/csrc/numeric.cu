@@ -559,9 +559,8 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
     static thread_local int attr_set = 0;
     if (!attr_set) {
         CK(cudaFuncSetAttribute(k_front_lu2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
-        // (k_front_lu4 has 35 KB of static shared memory beside its block: the opt-in is its largest block's need)
-        CK(cudaFuncSetAttribute(k_front_lu4<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_lu4_smem(LU4_NR, LU4_NP, sizeof(T))));
-        CK(cudaFuncSetAttribute(k_bat_lu4<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_lu4_smem(LU4_NR, LU4_NP, sizeof(T))));
+        CK(cudaFuncSetAttribute(k_front_lu5<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_lu5_smem(128, 64, sizeof(T))));
+        CK(cudaFuncSetAttribute(k_bat_lu5<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_lu5_smem(128, 64, sizeof(T))));
         CK(cudaFuncSetAttribute(k_front_lu3<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
         CK(cudaFuncSetAttribute(k_trsm_warp<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX));
@@ -754,14 +753,14 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             } else
                 k_front_lu3<T><<<1, LU3_THREADS, sm3, st>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel,
                                                             N.rowid + F.row_off, Lf, perm, N.p_lu, N.st, fi, pa), note_launch();
-        } else if ((N.lu_variant & 3) == 1 && nr <= LU4_NR && np <= LU4_NP && front_lu4_smem(nr, np, vs) <= SMEM_MAX) {
-            const size_t sm4 = front_lu4_smem(nr, np, vs);
+        } else if ((N.lu_variant & 3) == 1 && nr <= 128 && np <= 64) {
+            const size_t sm5 = front_lu5_smem(nr, np, vs);
             if (pa.on) {      // right after the child's tail head on the critical stream: overlap the launch
-                CK(launch_pdl(k_front_lu4<T>, 1, LU4_THREADS, sm4, st, (const T *)W, ld, (int)nr, (int)np, (int)F.nri, F.f,
+                CK(launch_pdl(k_front_lu5<T>, 1, LU5_THREADS, sm5, st, (const T *)W, ld, (int)nr, (int)np, (int)F.nri, F.f,
                               (const double *)N.colmax, pivot_rel, N.rowid + F.row_off, Lf, perm, N.p_lu, N.st, fi, pa));
                 note_launch();
             } else
-                k_front_lu4<T><<<1, LU4_THREADS, sm4, st>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel,
+                k_front_lu5<T><<<1, LU5_THREADS, sm5, st>>>(W, ld, (int)nr, (int)np, (int)F.nri, F.f, N.colmax, pivot_rel,
                                                             N.rowid + F.row_off, Lf, perm, N.p_lu, N.st, fi, pa), note_launch();
         } else if (sm <= SMEM_MAX) {
             const int R = (int)((nr + 31) & ~31);
@@ -896,7 +895,7 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
             if (nt > 640) nt = 640;
             prof.begin(s, PROF_LU, fm * D.bs_lu_flops[(size_t)lv], D.bs_lu_bytes[(size_t)lv] * (double)vs);
             if ((N.lu_variant & 3) == 1)
-                k_bat_lu4<T><<<cnt, LU4_THREADS, front_lu4_smem(D.bs_maxnr[(size_t)lv], D.bs_maxnp[(size_t)lv], vs), s>>>(
+                k_bat_lu5<T><<<cnt, LU5_THREADS, front_lu5_smem(D.bs_maxnr[(size_t)lv], D.bs_maxnp[(size_t)lv], vs), s>>>(
                     D.fc, bl, Wb, N.colmax, pivot_rel, N.rowid, La, N.permall, N.p_lu, N.st), note_launch();
             else
                 k_bat_lu2<T><<<cnt, nt, front_lu_smem(D.bs_maxnr[(size_t)lv], D.bs_maxnp[(size_t)lv], vs), s>>>(

@@ -107,7 +107,7 @@ struct DevNum {
     int prec = 0;
     void *coopbuf = nullptr;       // the multi-CTA pivot-block LU: the CTAs' posts, the ticket, the choices, U12, row scratch
     size_t cap_coop = 0;
-    int lu_variant = 2;            // the small fronts' pivot-block LU (2: k_front_lu2, 1: k_front_lu4, 3: k_front_lu3); + 4: the tall
+    int lu_variant = 2;            // the small fronts' pivot-block LU (2: k_front_lu2, 1: k_front_lu5, 3: k_front_lu3); + 4: the tall
                                    // blocks by one CTA per 32-column panel instead of k_block_lu_mc; + 8: no batched
                                    // fronts (every front on its own); + 16: the small fronts' tails by forward
                                    // substitution (k_front_tail) instead of the block-inverse products (k_front_tail2);

@@ -151,8 +151,8 @@ int fplus_b200_autotune(fplus_symbolic *sym, const int64_t *Ap, const int64_t *A
 
 /* The front shape of every later factorization on sym, chosen by the caller instead of the autotuner: at most max_width
  * pivot columns per front (16 .. 4096), nb_chain pivots per dense-chain front (8 .. 64), and the pivot-block LU of the
- * small fronts (2: the block in shared memory, one barrier per pivot step, the default; 1: the block in registers;
- * 3: blocked 8-column panels), plus 4 to pivot the pivot blocks too large for one CTA by one CTA per 32-column panel
+ * small fronts (2: the block in shared memory, one barrier per pivot step, the default; 1: 8-column panels with the
+ * later columns' rank-8 updates on the FP64 tensor cores; 3: blocked 8-column panels in FP64 lanes), plus 4 to pivot the pivot blocks too large for one CTA by one CTA per 32-column panel
  * instead of all SMs in one launch, plus 8 to factor every front on its own instead of the small fronts at the bottom of
  * the tree level by level (variant 3 also turns that off), plus 16 to form the small fronts' U12 and contribution blocks
  * by 16-row forward-substitution steps instead of products with the inverted diagonal blocks, plus 32 to pass the

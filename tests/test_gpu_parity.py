@@ -233,11 +233,12 @@ def test_large_fronts_all_solve_directions(gpu, cplx):
             assert be <= 1e-14, f"trans {trans} rhs {r}: backward error {be:.2e}"
 
 
-@pytest.mark.parametrize("variant", [2, 3])
+@pytest.mark.parametrize("variant", [1, 3])
 @pytest.mark.parametrize("name", ["pencil_1x64", "pencil_2x256", "banded_cplx_1200", "convdiff3d_g12", "hard_cplx_300"])
 def test_other_pivot_block_lus_match_oracle(gpu, name, variant):
-    """The other pivot-block LU kernels of the small fronts (k_front_lu2: the block in shared memory, the autotuner's other
-    choice; k_front_lu3: blocked panels) give the oracle's pivots and factors."""
+    """The other pivot-block LU kernels of the small fronts (k_front_lu5: 8-column panels with the later columns' rank-8
+    updates on the FP64 tensor cores, the autotuner's other choice; k_front_lu3: blocked panels in FP64 lanes) give the
+    oracle's pivots and factors."""
     n, Ap, Ai, Ax = CASES[name]()
     S = F.analyze(n, Ap, Ai)
     S.set_front_shape(256, 64, variant)
@@ -276,7 +277,7 @@ def test_tall_pivot_blocks_match_oracle(gpu, cplx, variant):
 def test_batched_small_fronts_match_front_by_front(gpu, cplx, lu):
     """The small fronts at the bottom of the tree factored level by level (one launch per level for assembly, LU and
     tail) give bit for bit the factors of the front-by-front path (set_front_shape variant + 8), and the oracle's pivots,
-    with either pivot-block LU kernel (1: the block in registers, 2: in shared memory)."""
+    with either pivot-block LU kernel (1: blocked with tensor-core updates, 2: the block in shared memory)."""
     g = 14 if cplx else 18
     n, Ap, Ai, Ax = W.convdiff3d(g, 3)
     if cplx:
