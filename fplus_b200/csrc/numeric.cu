@@ -594,7 +594,9 @@ static int run_fronts(const FrontPlan &P, const DevPlan &D, DevNum &N, double pi
         (void)cudaGetLastError();
         mc_sms = k >= 1 ? sms : 0;
         // the largest cluster the device places with the cluster form's largest shared memory
-        if (cudaFuncSetAttribute(k_block_lu_mc<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX) == cudaSuccess &&
+        // (the opt-in is the largest request of the cluster form: with the 220 KB cap its static posts would pass the 227 KB
+        // limit for complex values)
+        if (cudaFuncSetAttribute(k_block_lu_mc<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mc_smem<T>(per_max, true)) == cudaSuccess &&
             cudaFuncSetAttribute(k_block_lu_mc<T, true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
             for (int csz = MC_CMAX; csz >= 4 && mc_cl == 0; csz /= 2) {
                 cudaLaunchConfig_t oc = {};
