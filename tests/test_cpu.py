@@ -531,3 +531,26 @@ def test_lpt_sharding_over_two_gloo_ranks():
     assert set(r0[0]["jobs"]).isdisjoint(r0[1]["jobs"])
     assert abs(r0[0]["load"] - r0[1]["load"]) <= max(costs)
     assert shard.lpt_partition(costs, 2) == [r0[0]["jobs"], r0[1]["jobs"]]
+
+
+@pytest.mark.skipif(not O.have_reference(), reason="the reference build (oracle/_ref) is not present")
+def test_reference_arm_json_line():
+    """bench.py --impl reference on the CPU-runnable stencil: one JSON line with the arm's metric, a measured value, a
+    cpu_baseline of kind "reference" and an e2e with no host-device bytes; libfplus.so is not loaded by that arm."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    # the arm run as __main__, then whether the process mapped libfplus.so (printed after the arm's own line)
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'convdiff2d', '--steps', '1', "
+            "'--warmup', '1']; runpy.run_path('bench.py', run_name='__main__'); "
+            "print('LIBFPLUS_MAPPED', any('libfplus.so' in l for l in open('/proc/self/maps')))")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = out.stdout.strip().splitlines()
+    assert lines[-1] == "LIBFPLUS_MAPPED False", lines[-1]
+    line = json.loads(lines[-2])
+    assert line["impl"] == "reference" and line["unit"] == "ms" and line["higher_is_better"] is False
+    assert line["value"] > 0 and line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert line["config"]["n"] == 10000
