@@ -4,6 +4,8 @@
 #include <algorithm>
 #include <cstring>
 #include <cmath>
+#include <thread>
+#include <vector>
 
 namespace fpl {
 
@@ -37,11 +39,49 @@ int check_compressed(int64_t n, const int64_t *ptr, const int64_t *idx, int cano
     return FPLUS_OK;
 }
 
+// whether any of d[0 .. m) is infinite or NaN (its exponent bits all ones), without an early exit
+static bool any_nonfinite(const double *d, int64_t m)
+{
+    const uint64_t E = 0x7ff0000000000000ull;
+    uint64_t f0 = 0, f1 = 0, f2 = 0, f3 = 0;
+    int64_t k = 0;
+    for (; k + 4 <= m; k += 4) {
+        uint64_t b[4];
+        std::memcpy(b, d + k, sizeof b);
+        f0 |= (uint64_t)((b[0] & E) == E); f1 |= (uint64_t)((b[1] & E) == E);
+        f2 |= (uint64_t)((b[2] & E) == E); f3 |= (uint64_t)((b[3] & E) == E);
+    }
+    for (; k < m; k++) { uint64_t b; std::memcpy(&b, d + k, 8); f0 |= (uint64_t)((b & E) == E); }
+    return (f0 | f1 | f2 | f3) != 0;
+}
+
+// Every value finite, else the first entry that is not (the error names it).  Large arrays are first scanned for any
+// non-finite value by up to 8 host threads; only then is the first one located, serially.
 int check_finite(int64_t nnz, const void *x, int is_complex, char *err, size_t errlen)
 {
     const double *d = (const double *)x;
     const int64_t m = is_complex ? 2 * nnz : nnz;
     if (m > 0 && !d) { errf(err, errlen, "NULL value array"); return FPLUS_ERR_BADARG; }
+    bool bad = false;
+    const unsigned hc = std::thread::hardware_concurrency();
+    const int nt = m >= (int64_t)1 << 20 ? (int)std::min<unsigned>(8u, hc > 1 ? hc : 1u) : 1;
+    if (nt > 1) {
+        std::vector<char> r((size_t)nt, 0);
+        std::vector<std::thread> th;
+        bool all = true;                                   // every chunk has its thread
+        try {
+            for (int t = 1; t < nt; t++)
+                th.emplace_back([&r, d, m, nt, t]() { const int64_t a = m * t / nt, b = m * (t + 1) / nt; r[(size_t)t] = any_nonfinite(d + a, b - a); });
+        } catch (...) {
+            all = false;
+        }
+        r[0] = any_nonfinite(d, m / nt);                   // chunk 0 on this thread
+        for (std::thread &x : th) x.join();
+        if (!all) bad = any_nonfinite(d, m);               // (threads could not be had: one pass over everything)
+        else for (char v : r) bad = bad || v;
+    } else
+        bad = any_nonfinite(d, m);
+    if (!bad) return FPLUS_OK;
     for (int64_t k = 0; k < m; k++)
         if (!std::isfinite(d[k])) { errf(err, errlen, "non-finite value in entry %ld", (long)(is_complex ? k / 2 : k)); return FPLUS_ERR_BADARG; }
     return FPLUS_OK;

@@ -87,6 +87,23 @@ def test_factor_argument_checks_on_host():
     assert rc == F.FPLUS_ERR_BADARG and "nonzeros" in msg
 
 
+def test_non_finite_values_found_in_large_arrays():
+    """The host check of the values (several threads over arrays of a million values or more): the first non-finite
+    entry is named, real and complex, wherever it lies; finite values pass."""
+    n, Ap, Ai, Ax = W.convdiff2d(1100, 1)                  # 6 million entries
+    assert Ax.size >= 1 << 20
+    S = F.analyze(n, Ap, Ai)
+    for pos in (3, Ax.size // 2 + 7, Ax.size - 1):
+        for val in (np.nan, np.inf, -np.inf):
+            bad = Ax.copy(); bad[pos] = val; bad[-1 if pos != Ax.size - 1 else 0] = np.nan
+            first = min(pos, Ax.size - 1 if pos != Ax.size - 1 else 0)
+            rc, msg = _factor_rc(S, bad, 0)
+            assert rc == F.FPLUS_ERR_BADARG and f"non-finite value in entry {first}" in msg, (pos, val, msg)
+    cx = Ax.astype(np.complex128); cx[11] = complex(1.0, np.nan)
+    rc, msg = _factor_rc(S, cx, 1)
+    assert rc == F.FPLUS_ERR_BADARG and "non-finite value in entry 11" in msg
+
+
 def test_analyze_argument_checks():
     with pytest.raises(F.FplusError) as e:
         F.analyze(2, np.array([0, 2, 3]), np.array([1, 0, 1]))       # unsorted: not canonical
